@@ -1,0 +1,340 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+The oracle restates OPAL's space-charge step in sequential FP64 C
+(``oracle/sc_oracle.c``; every function there cites the reference file and
+line it follows).  Only the tests, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` import this module -- as the checker, never as
+the thing that is measured or shipped.
+
+``use_reference_fft()`` switches the oracle's 1-D FFT engine to the
+reference's own FFTPACK (``ippl/src/FFT/fftpack.cpp``) compiled from source
+into ``oracle/_ref/libfftpack_ref.so`` by ``oracle/Makefile``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libscoracle.so")
+REF_FFT_PATH = os.path.join(HERE, "_ref", "libfftpack_ref.so")
+
+_dp = C.POINTER(C.c_double)
+
+
+class Mesh(C.Structure):
+    _fields_ = [("nr", C.c_int * 3), ("hr", C.c_double * 3), ("origin", C.c_double * 3),
+                ("rmin", C.c_double * 3), ("rmax", C.c_double * 3)]
+
+
+class Trafo(C.Structure):
+    _fields_ = [("origin", C.c_double * 3), ("quat", C.c_double * 4), ("M", C.c_double * 9)]
+
+
+class Params(C.Structure):
+    _fields_ = [("nr", C.c_int * 3), ("pad_", C.c_int), ("dh", C.c_double), ("dT", C.c_double),
+                ("mass", C.c_double), ("charge", C.c_double), ("coupling", C.c_double),
+                ("bz_ext", C.c_double), ("ref_pz", C.c_double)]
+
+
+class Tracker(C.Structure):
+    _fields_ = [("prm", Params), ("Q", C.c_double), ("t", C.c_double), ("path_length", C.c_double),
+                ("ref_R", C.c_double * 3), ("ref_P", C.c_double * 3), ("ref_to_lab", Trafo),
+                ("step", C.c_longlong)]
+
+
+class Debug(C.Structure):
+    _fields_ = [("rho", _dp), ("phi", _dp), ("E", _dp), ("Ef", _dp), ("Bf", _dp), ("mesh", Mesh),
+                ("gammaz", C.c_double), ("hr_scaled", C.c_double * 3), ("pmean", C.c_double * 3),
+                ("rot_beam_to_ref", C.c_double * 9), ("update_origin", C.c_double * 3)]
+
+
+class BeamParams(C.Structure):
+    _fields_ = [(name, C.c_double * 3) for name in
+                ("rmin", "rmax", "rmean", "pmean", "rrms", "prms", "eps_norm", "eps", "rprms")] + \
+               [("gamma", C.c_double), ("moments", C.c_double * 27)]
+
+    def as_dict(self):
+        out = {name: np.array(getattr(self, name)) for name, _ in self._fields_ if name != "gamma"}
+        out["gamma"] = float(self.gamma)
+        return out
+
+
+def build():
+    """Compile the oracle (and oracle/_ref when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+_ref_fft = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.sco_const_c.restype = C.c_double
+        L.sco_const_electron_mass_ev.restype = C.c_double
+        L.sco_const_coupling.restype = C.c_double
+        L.sco_sum_gamma.restype = C.c_double
+        assert L.sco_sizeof_tracker() == C.sizeof(Tracker)
+        assert L.sco_sizeof_debug() == C.sizeof(Debug)
+        assert L.sco_sizeof_beam_params() == C.sizeof(BeamParams)
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def reference_fft_available():
+    return os.path.exists(REF_FFT_PATH)
+
+
+def use_reference_fft(on=True):
+    """Route the oracle's 1-D transforms through the reference's FFTPACK."""
+    global _ref_fft
+    L = lib()
+    if not on:
+        L.sco_set_fft_engine(None, None, None, None, None, None)
+        return
+    if _ref_fft is None:
+        _ref_fft = C.CDLL(REF_FFT_PATH)
+    fn = [C.cast(getattr(_ref_fft, name), C.c_void_p) for name in
+          ("cffti", "cfftf", "cfftb", "rffti", "rfftf", "rfftb")]
+    L.sco_set_fft_engine(*fn)
+
+
+def fft_engine_is_own():
+    return bool(lib().sco_fft_engine_is_own())
+
+
+# ---------------------------------------------------------------- constants
+def c_light():
+    return lib().sco_const_c()
+
+
+def electron_mass_ev():
+    return lib().sco_const_electron_mass_ev()
+
+
+def coupling():
+    return lib().sco_const_coupling()
+
+
+# ---------------------------------------------------------------- functions
+def fft1d(kind, data):
+    """kind: 0 cfftf, 1 cfftb, 2 rfftf, 3 rfftb (FFTPACK semantics)."""
+    d = _f64(data).copy()
+    n = d.size // 2 if kind < 2 else d.size
+    lib().sco_fft1d(C.c_int(kind), C.c_longlong(n), _ptr(d))
+    return d
+
+
+def fft3d_r2c(real):
+    """real: array [L2, L1, L0] (x fastest) -> complex [L2, L1, L0//2+1]."""
+    r = _f64(real)
+    L = (C.c_int * 3)(r.shape[2], r.shape[1], r.shape[0])
+    out = np.empty((r.shape[0], r.shape[1], r.shape[2] // 2 + 1), dtype=np.complex128)
+    lib().sco_fft3d_r2c(L, _ptr(r), out.ctypes.data_as(_dp))
+    return out
+
+
+def fft3d_c2r(spec, L0):
+    s = np.ascontiguousarray(spec, dtype=np.complex128).copy()
+    L = (C.c_int * 3)(L0, s.shape[1], s.shape[0])
+    out = np.empty((s.shape[0], s.shape[1], L0), dtype=np.float64)
+    lib().sco_fft3d_c2r(L, s.ctypes.data_as(_dp), _ptr(out))
+    return out
+
+
+def igf(nr, hr):
+    """Doubled, mirrored integrated Green's function, array [2nz, 2ny, 2nx]."""
+    G = np.empty((2 * nr[2], 2 * nr[1], 2 * nr[0]), dtype=np.float64)
+    lib().sco_igf((C.c_int * 3)(*nr), (C.c_double * 3)(*hr), _ptr(G))
+    return G
+
+
+def compute_potential(rho, hr):
+    """FFTPoissonSolver::computePotential: rho [nz, ny, nx] -> convolution."""
+    r = _f64(rho).copy()
+    nr = (C.c_int * 3)(r.shape[2], r.shape[1], r.shape[0])
+    rc = lib().sco_compute_potential(nr, _ptr(r), (C.c_double * 3)(*hr))
+    if rc:
+        raise RuntimeError(f"sco_compute_potential failed: {rc}")
+    return r
+
+
+def neg_grad_scaled(phi, h, gammaz):
+    p = _f64(phi)
+    nr = (C.c_int * 3)(p.shape[2], p.shape[1], p.shape[0])
+    E = np.empty(p.shape + (3,), dtype=np.float64)
+    lib().sco_neg_grad_scaled(nr, _ptr(p), (C.c_double * 3)(*h), C.c_double(gammaz), _ptr(E))
+    return E
+
+
+def boundp(R, nr, dh):
+    R = _f64(R)
+    m = Mesh()
+    rc = lib().sco_boundp(C.c_longlong(R.shape[0]), _ptr(R), (C.c_int * 3)(*nr), C.c_double(dh), C.byref(m))
+    if rc:
+        raise RuntimeError(f"boundp failed: {rc}")
+    return m
+
+
+def scatter_cic(R, q, mesh):
+    R = _f64(R)
+    nr = list(mesh.nr)
+    rho = np.zeros((nr[2], nr[1], nr[0]), dtype=np.float64)
+    rc = lib().sco_scatter_cic(C.c_longlong(R.shape[0]), _ptr(R), C.c_double(q), C.byref(mesh), _ptr(rho))
+    if rc:
+        raise RuntimeError(f"scatter failed: {rc}")
+    return rho
+
+
+def gather_cic(R, mesh, E):
+    R = _f64(R)
+    E = _f64(E)
+    Ef = np.empty_like(R)
+    rc = lib().sco_gather_cic(C.c_longlong(R.shape[0]), _ptr(R), C.byref(mesh), _ptr(E), _ptr(Ef))
+    if rc:
+        raise RuntimeError(f"gather failed: {rc}")
+    return Ef
+
+
+def push(R, P, dt):
+    R = _f64(R).copy()
+    P = _f64(P)
+    lib().sco_push(C.c_longlong(R.shape[0]), _ptr(R), _ptr(P), C.c_double(dt))
+    return R
+
+
+def kick(P, Ef, Bf, dt, mass, charge):
+    P = _f64(P).copy()
+    lib().sco_kick(C.c_longlong(P.shape[0]), _ptr(P), _ptr(_f64(Ef)), _ptr(_f64(Bf)), C.c_double(dt),
+                   C.c_double(mass), C.c_double(charge))
+    return P
+
+
+def beam_parameters(R, P):
+    bp = BeamParams()
+    R = _f64(R)
+    P = _f64(P)
+    lib().sco_beam_parameters(C.c_longlong(R.shape[0]), _ptr(R), _ptr(P), C.byref(bp))
+    return bp.as_dict()
+
+
+def make_params(nr, dT, dh=0.02, bz_ext=0.0, ref_pz=10.0, mass=None, charge=-1.0):
+    p = Params()
+    p.nr = (C.c_int * 3)(*nr)
+    p.dh = dh
+    p.dT = dT
+    p.mass = electron_mass_ev() if mass is None else mass
+    p.charge = charge
+    p.coupling = coupling()
+    p.bz_ext = bz_ext
+    p.ref_pz = ref_pz
+    return p
+
+
+def compute_self_fields(params, Q, R, P, want_grids=True):
+    """PartBunch::computeSelfFields on a bunch in the beam frame.
+    Returns (Ef, Bf, Q_after, debug dict)."""
+    R = _f64(R)
+    P = _f64(P)
+    n = R.shape[0]
+    nr = list(params.nr)
+    M = nr[0] * nr[1] * nr[2]
+    Ef = np.empty_like(R)
+    Bf = np.empty_like(R)
+    dbg = Debug()
+    grids = {}
+    if want_grids:
+        grids = {"rho": np.empty(M), "phi": np.empty(M), "E": np.empty(3 * M)}
+        dbg.rho, dbg.phi, dbg.E = _ptr(grids["rho"]), _ptr(grids["phi"]), _ptr(grids["E"])
+    q = C.c_double(Q)
+    rc = lib().sco_compute_self_fields(C.byref(params), C.byref(q), C.c_longlong(n), _ptr(R), _ptr(P),
+                                       _ptr(Ef), _ptr(Bf), C.byref(dbg))
+    if rc:
+        raise RuntimeError(f"compute_self_fields failed: {rc}")
+    return Ef, Bf, q.value, _debug_dict(dbg, grids, nr)
+
+
+def _debug_dict(dbg, grids, nr):
+    out = {
+        "hr": np.array(dbg.mesh.hr), "origin": np.array(dbg.mesh.origin),
+        "rmin": np.array(dbg.mesh.rmin), "rmax": np.array(dbg.mesh.rmax),
+        "gammaz": float(dbg.gammaz), "hr_scaled": np.array(dbg.hr_scaled),
+        "pmean": np.array(dbg.pmean), "rot_beam_to_ref": np.array(dbg.rot_beam_to_ref).reshape(3, 3),
+    }
+    shape = (nr[2], nr[1], nr[0])
+    for k, v in grids.items():
+        out[k] = v.reshape(shape + ((3,) if k == "E" else ()))
+    return out
+
+
+class OracleTracker:
+    """ParallelTTracker step loop restated on the CPU (sequential FP64)."""
+
+    def __init__(self, params, Q):
+        self.tr = Tracker()
+        lib().sco_tracker_init(C.byref(self.tr), C.byref(params), C.c_double(Q))
+
+    @property
+    def Q(self):
+        return self.tr.Q
+
+    @property
+    def t(self):
+        return self.tr.t
+
+    @property
+    def path_length(self):
+        return self.tr.path_length
+
+    @property
+    def ref_R(self):
+        return np.array(self.tr.ref_R)
+
+    @property
+    def ref_P(self):
+        return np.array(self.tr.ref_P)
+
+    def track(self, R, P, nsteps, want_debug=False):
+        """Advance R, P (N x 3, updated in place) by nsteps.  With want_debug
+        the last step's grids and fields are returned."""
+        assert R.dtype == np.float64 and R.flags.c_contiguous
+        assert P.dtype == np.float64 and P.flags.c_contiguous
+        n = R.shape[0]
+        dbgp = None
+        grids = {}
+        nr = list(self.tr.prm.nr)
+        if want_debug:
+            M = nr[0] * nr[1] * nr[2]
+            grids = {"rho": np.empty(M), "phi": np.empty(M), "E": np.empty(3 * M),
+                     "Ef": np.empty(3 * n), "Bf": np.empty(3 * n)}
+            dbg = Debug()
+            dbg.rho, dbg.phi, dbg.E = _ptr(grids["rho"]), _ptr(grids["phi"]), _ptr(grids["E"])
+            dbg.Ef, dbg.Bf = _ptr(grids["Ef"]), _ptr(grids["Bf"])
+            dbgp = C.byref(dbg)
+        rc = lib().sco_track(C.byref(self.tr), C.c_longlong(n), _ptr(R), _ptr(P), C.c_int(nsteps), dbgp)
+        if rc:
+            raise RuntimeError(f"sco_track failed: {rc}")
+        if not want_debug:
+            return None
+        ef = grids.pop("Ef").reshape(n, 3)
+        bf = grids.pop("Bf").reshape(n, 3)
+        out = _debug_dict(dbg, grids, nr)
+        out["Ef"], out["Bf"] = ef, bf
+        out["update_origin"] = np.array(dbg.update_origin)
+        return out

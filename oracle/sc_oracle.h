@@ -1,0 +1,125 @@
+/*
+ * sc_oracle.h -- CPU restatement of OPAL's space-charge step (test
+ * infrastructure: the checker and the timed CPU baseline, never the product).
+ */
+#ifndef SC_ORACLE_H
+#define SC_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCO_ERR_ARG (-1)
+#define SCO_ERR_OOM (-2)
+#define SCO_ERR_MESH (-3)   /* boundp: h <= 0 (PartBunchBase.hpp:870-872) */
+#define SCO_ERR_GUARD (-4)  /* a CIC stencil reached a guard cell */
+#define SCO_ERR_FRAME (-5)  /* getQuaternion on an anti-parallel or null vector */
+
+typedef struct {
+    int nr[3];
+    double hr[3];
+    double origin[3];
+    double rmin[3];
+    double rmax[3];
+} sco_mesh;
+
+typedef struct {
+    double origin[3];
+    double quat[4];
+    double M[9]; /* row-major rotation matrix */
+} sco_trafo;
+
+typedef struct {
+    int nr[3];       /* MX, MY, MT: mesh cells per axis */
+    int pad_;
+    double dh;       /* BBOXINCR / 100 */
+    double dT;       /* time step [s] */
+    double mass;     /* rest energy [eV] */
+    double charge;   /* particle charge [e] */
+    double coupling; /* 1 / (4 pi eps0) */
+    double bz_ext;   /* uniform external B_z [T] (0: drift) */
+    double ref_pz;   /* reference particle beta*gamma along z at start */
+} sco_params;
+
+typedef struct {
+    sco_params prm;
+    double Q; /* macro-particle charge [C] */
+    double t;
+    double path_length;
+    double ref_R[3];
+    double ref_P[3];
+    sco_trafo ref_to_lab;
+    long long step;
+} sco_tracker;
+
+typedef struct {
+    /* optional caller-owned outputs (NULL to skip) */
+    double* rho; /* n^3: charge density fed to the solver [C/m^3] */
+    double* phi; /* n^3: potential [V] */
+    double* E;   /* 3 n^3 interleaved: -grad phi scaled by (g, g, 1/g) */
+    double* Ef;  /* 3 N: E at particles, reference frame */
+    double* Bf;  /* 3 N: B at particles, reference frame */
+    /* filled by the call */
+    sco_mesh mesh;
+    double gammaz;
+    double hr_scaled[3];
+    double pmean[3];
+    double rot_beam_to_ref[9];
+    double update_origin[3];
+} sco_debug;
+
+typedef struct {
+    double rmin[3], rmax[3];
+    double rmean[3], pmean[3];
+    double rrms[3], prms[3];
+    double eps_norm[3], eps[3];
+    double rprms[3];
+    double gamma;
+    double moments[27];
+} sco_beam_params;
+
+double sco_const_c(void);
+double sco_const_electron_mass_ev(void);
+double sco_const_coupling(void);
+
+int sco_get_quaternion(const double* u, const double* ref, double* q);
+void sco_trafo_make(sco_trafo* t, const double* origin, const double* quat);
+void sco_trafo_invert(sco_trafo* t);
+void sco_trafo_compose(sco_trafo* t, const sco_trafo* right);
+
+void sco_push(long long n, double* R, const double* P, double dt);
+void sco_kick(long long n, double* P, const double* Ef, const double* Bf, double dt, double mass, double charge);
+
+void sco_bounds(long long n, const double* R, double* rmin, double* rmax);
+void sco_moments(long long n, const double* R, const double* P, double* m27);
+double sco_sum_gamma(long long n, const double* P);
+void sco_beam_parameters_from_sums(const double* m27, double gsum, double N, sco_beam_params* bp);
+int sco_beam_parameters(long long n, const double* R, const double* P, sco_beam_params* bp);
+
+int sco_boundp(long long n, const double* R, const int* nr, double dh, sco_mesh* mesh);
+int sco_scatter_cic(long long n, const double* R, double q, const sco_mesh* m, double* rho);
+int sco_gather_cic(long long n, const double* R, const sco_mesh* m, const double* E, double* Ef);
+
+void sco_set_fft_engine(void* cffti, void* cfftf, void* cfftb, void* rffti, void* rfftf, void* rfftb);
+int sco_fft_engine_is_own(void);
+void sco_fft1d(int kind, long long n, double* data);
+void sco_fft3d_r2c(const int* L, const double* in, double* out);
+void sco_fft3d_c2r(const int* L, double* spec, double* out);
+
+void sco_igf(const int* nr, const double* hr, double* G2);
+int sco_compute_potential(const int* nr, double* rho, const double* hr);
+void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, double gammaz, double* E);
+int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const double* R, const double* P,
+                            double* Ef, double* Bf, sco_debug* dbg);
+
+int sco_tracker_init(sco_tracker* tr, const sco_params* prm, double Q);
+int sco_track(sco_tracker* tr, long long n, double* R, double* P, int nsteps, sco_debug* dbg);
+
+int sco_sizeof_tracker(void);
+int sco_sizeof_debug(void);
+int sco_sizeof_beam_params(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,99 @@
+"""Seeded synthetic electron bunches (host side, numpy).
+
+The reference draws its initial distributions with GSL
+(src/Distribution/Distribution.cpp); no public dataset is involved.  The
+bunches used here are Gaussian in position and momentum about a reference
+particle at the origin moving along +z, drawn from a counter-based
+Philox4x32-10 stream (Salmon et al., SC'11) with one stream per bunch id, and
+turned into normals by the Box-Muller transform in FP64.  The same host
+arrays feed the CUDA path and the oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+DEFAULT_SEED = 20261203
+
+_M0 = np.uint64(0xD2511F53)
+_M1 = np.uint64(0xCD9E8D57)
+_W0 = np.uint32(0x9E3779B9)
+_W1 = np.uint32(0xBB67AE85)
+_MASK = np.uint64(0xFFFFFFFF)
+
+
+def philox4x32(counter, key, rounds=10):
+    """counter: 4 uint32 arrays; key: 2 uint32 scalars.  Returns 4 uint32 arrays."""
+    c0, c1, c2, c3 = (np.asarray(c, dtype=np.uint32) for c in counter)
+    k0, k1 = np.uint32(key[0]), np.uint32(key[1])
+    with np.errstate(over="ignore"):
+        for r in range(rounds):
+            p0 = _M0 * c0.astype(np.uint64)
+            p1 = _M1 * c2.astype(np.uint64)
+            hi0 = (p0 >> np.uint64(32)).astype(np.uint32)
+            lo0 = (p0 & _MASK).astype(np.uint32)
+            hi1 = (p1 >> np.uint64(32)).astype(np.uint32)
+            lo1 = (p1 & _MASK).astype(np.uint32)
+            c0, c1, c2, c3 = hi1 ^ c1 ^ k0, lo1, hi0 ^ c3 ^ k1, lo0
+            if r != rounds - 1:
+                k0 = np.uint32(k0 + _W0)
+                k1 = np.uint32(k1 + _W1)
+    return c0, c1, c2, c3
+
+
+def _uniform53(a, b):
+    """Two uint32 -> double in (0, 1): 53 random bits, centred in their bin."""
+    x = (a.astype(np.uint64) >> np.uint64(5)) * np.uint64(67108864) + (b.astype(np.uint64) >> np.uint64(6))
+    return (x.astype(np.float64) + 0.5) / 9007199254740992.0
+
+
+def standard_normals(n, seed=DEFAULT_SEED, stream=0, block=0):
+    """2n standard normals for particles 0..n-1 (two per particle) from
+    counter (i, stream, block, 0) and key (seed low, seed high)."""
+    i = np.arange(n, dtype=np.uint64)
+    key = (np.uint32(seed & 0xFFFFFFFF), np.uint32((seed >> 32) & 0xFFFFFFFF))
+    ctr = ((i & _MASK).astype(np.uint32), np.full(n, stream & 0xFFFFFFFF, dtype=np.uint32),
+           np.full(n, block, dtype=np.uint32), (i >> np.uint64(32)).astype(np.uint32))
+    r0, r1, r2, r3 = philox4x32(ctr, key)
+    u1 = _uniform53(r0, r1)
+    u2 = _uniform53(r2, r3)
+    rad = np.sqrt(-2.0 * np.log(u1))
+    ang = 2.0 * np.pi * u2
+    return rad * np.cos(ang), rad * np.sin(ang)
+
+
+def gaussian_bunch(n, sigma=(1e-3, 1e-3, 2e-3), bg_z=10.0, rel_spread=1e-3, bg_perp=1e-3,
+                   seed=DEFAULT_SEED, bunch_id=0):
+    """Electron bunch about the reference particle.
+
+    Positions: x, y, z ~ N(0, sigma) [m].  Momenta (beta*gamma):
+    p_z = bg_z * (1 + rel_spread * N(0,1)), p_x, p_y = bg_perp * N(0,1).
+    Returns R, P as (n, 3) float64 arrays (x, y, z per particle, like OPAL's
+    Vector_t attributes).
+    """
+    n = int(n)
+    g0, g1 = standard_normals(n, seed, bunch_id, 0)
+    g2, g3 = standard_normals(n, seed, bunch_id, 1)
+    g4, g5 = standard_normals(n, seed, bunch_id, 2)
+    R = np.empty((n, 3), dtype=np.float64)
+    P = np.empty((n, 3), dtype=np.float64)
+    R[:, 0] = sigma[0] * g0
+    R[:, 1] = sigma[1] * g1
+    R[:, 2] = sigma[2] * g2
+    P[:, 0] = bg_perp * g3
+    P[:, 1] = bg_perp * g4
+    P[:, 2] = bg_z * (1.0 + rel_spread * g5)
+    return R, P
+
+
+def config_bunch(name, n=None, seed=DEFAULT_SEED, bunch_id=0):
+    """The fixed Gaussian recipe of the single-bunch workloads:
+    1 nC electrons, sigma = (1, 1, 2) mm, beta*gamma_z = 10 with 1e-3 relative
+    spread, transverse beta*gamma sigma 1e-3, dt = 1 ps."""
+    sizes = {"c1": (100_000, 32, 100, 0.0), "c2": (1_000_000, 64, 1000, 0.0),
+             "c3": (10_000_000, 128, 1000, 0.2)}
+    N, mesh, steps, bz = sizes[name]
+    if n is not None:
+        N = int(n)
+    R, P = gaussian_bunch(N, seed=seed, bunch_id=bunch_id)
+    return dict(R=R, P=P, N=N, nr=(mesh, mesh, mesh), steps=steps, bz_ext=bz, dT=1e-12,
+                Q=-1e-9 / N, ref_pz=10.0, dh=0.02)

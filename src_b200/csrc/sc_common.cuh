@@ -1,0 +1,407 @@
+// sc_common.cuh -- types and scalar math shared by the host and the device.
+//
+// The scalar frame arithmetic below (quaternions, coordinate-system
+// transformations, the Boris pusher) follows OPAL's expressions operand for
+// operand so that, compiled without fused multiply-add contraction, the
+// device computes the same doubles as the reference's CPU code:
+//   Quaternion.cpp:34-150, CoordinateSystemTrafo.{h:77-85,cpp:18-43},
+//   BorisPusher.h:56-124, PartBunchBase.hpp:468-513.
+// Only +, -, *, / and sqrt appear; all are correctly rounded on both sides.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define SC_HD __host__ __device__ __forceinline__
+
+namespace sc {
+
+constexpr double kC = 299792458.0;          // Physics.h:52
+constexpr double kPi = 3.14159265358979323846;  // Physics.h:31
+
+// status codes (mirrored by include/scgpu.h)
+enum : int {
+    kOk = 0,
+    kErrArg = -1,
+    kErrOom = -2,
+    kErrMesh = -3,
+    kErrGuard = -4,
+    kErrFrame = -5,
+    kErrCuda = -6,
+    kErrState = -7,
+    kErrUnsupported = -8,
+};
+
+// device-side error bits (StepState::err)
+enum : int {
+    kFlagMesh = 1,
+    kFlagGuard = 2,
+    kFlagFrame = 4,
+};
+
+struct Trafo {
+    double origin[3];
+    double quat[4];
+    double M[9];  // row-major
+};
+
+// Device-resident state of one bunch: the ParallelTTracker members that the
+// step loop updates, and the per-step scalars that one kernel derives and
+// later kernels read.  Kernels read it through a pointer so that a captured
+// CUDA graph replays correctly for any number of steps.
+struct StepState {
+    // tracker state
+    double t;
+    double path_length;
+    double ref_R[3];
+    double ref_P[3];
+    Trafo ref_to_lab;
+    double Q;  // macro-particle charge after the Q*=dt ... Q/=dt round trip
+    long long step;
+    unsigned int gen;  // deposit generation stamp (never 0 once a step ran)
+    int err;
+    // reductions of the particle state at the end of the previous step
+    double psum[3];
+    double moments[27];
+    double gsum;
+    // per-step scalars
+    Trafo r2b;  // reference -> beam frame (inverse of b2r)
+    Trafo b2r;  // beam -> reference frame
+    double bmin[3], bmax[3];
+    double mesh_rmin[3], mesh_rmax[3];
+    double hr[3], origin[3];
+    double gammaz;
+    double hr_scaled[3];
+    double tmp2;   // 1/hx * 1/hy * 1/hz_scaled
+    double hvol;   // hx * hy * hz_scaled
+    double betaC;  // sqrt(gz^2-1)/gz/c
+    double qdt;    // Q * dt (the scattered charge)
+    Trafo upd;     // reference-particle update of this step
+};
+
+struct BunchConst {
+    int n[3];       // mesh cells per axis (MX, MY, MT)
+    int key_bits;
+    long long N;    // particles
+    double dT;
+    double mass;    // eV
+    double charge;  // e
+    double coupling;
+    double bz_ext;
+    double dh;
+};
+
+// ---------------------------------------------------------------- vectors
+SC_HD double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+SC_HD void cross3(const double* a, const double* b, double* r) {
+    double r0 = a[1] * b[2] - a[2] * b[1];
+    double r1 = a[2] * b[0] - a[0] * b[2];
+    double r2 = a[0] * b[1] - a[1] * b[0];
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+}
+SC_HD void matvec(const double* M, const double* v, double* r) {
+    double r0 = M[0] * v[0] + M[1] * v[1] + M[2] * v[2];
+    double r1 = M[3] * v[0] + M[4] * v[1] + M[5] * v[2];
+    double r2 = M[6] * v[0] + M[7] * v[1] + M[8] * v[2];
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+}
+
+// ---------------------------------------------------------------- quaternions
+SC_HD void quat_mul(const double* a, const double* b, double* r) {
+    double ai[3] = {a[1], a[2], a[3]}, bi[3] = {b[1], b[2], b[3]}, c[3];
+    cross3(ai, bi, c);
+    double r0 = a[0] * b[0] - dot3(ai, bi);
+    double r1 = a[0] * bi[0] + b[0] * ai[0] + c[0];
+    double r2 = a[0] * bi[1] + b[0] * ai[1] + c[1];
+    double r3 = a[0] * bi[2] + b[0] * ai[2] + c[2];
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+    r[3] = r3;
+}
+SC_HD void quat_normalize(double* q) {
+    double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    q[0] /= len;
+    q[1] /= len;
+    q[2] /= len;
+    q[3] /= len;
+}
+SC_HD void quat_rotate(const double* q, const double* v, double* r) {
+    double qv[4] = {0.0, v[0], v[1], v[2]};
+    double qc[4] = {q[0], -q[1], -q[2], -q[3]};
+    double t[4], u[4];
+    quat_mul(qv, qc, t);
+    quat_mul(q, t, u);
+    r[0] = u[1];
+    r[1] = u[2];
+    r[2] = u[3];
+}
+SC_HD void quat_rotmat(const double* qin, double* M) {
+    double q[4] = {qin[0], qin[1], qin[2], qin[3]};
+    quat_normalize(q);
+    M[0] = 1 - 2 * (q[2] * q[2] + q[3] * q[3]);
+    M[1] = 2 * (-q[0] * q[3] + q[1] * q[2]);
+    M[2] = 2 * (q[0] * q[2] + q[1] * q[3]);
+    M[3] = 2 * (q[0] * q[3] + q[1] * q[2]);
+    M[4] = 1 - 2 * (q[1] * q[1] + q[3] * q[3]);
+    M[5] = 2 * (-q[0] * q[1] + q[2] * q[3]);
+    M[6] = 2 * (-q[0] * q[2] + q[1] * q[3]);
+    M[7] = 2 * (q[0] * q[1] + q[2] * q[3]);
+    M[8] = 1 - 2 * (q[1] * q[1] + q[2] * q[2]);
+}
+// getQuaternion(u, ref); false for anti-parallel or null input.
+SC_HD bool get_quaternion(const double* uin, const double* refin, double* q) {
+    const double tol = 1e-12;
+    double u[3] = {uin[0], uin[1], uin[2]}, ref[3] = {refin[0], refin[1], refin[2]};
+    double lu = sqrt(dot3(u, u)), lr = sqrt(dot3(ref, ref));
+    if (!(lu >= 1e-12) || !(lr >= 1e-12)) return false;
+    u[0] /= lu;
+    u[1] /= lu;
+    u[2] /= lu;
+    ref[0] /= lr;
+    ref[1] /= lr;
+    ref[2] /= lr;
+    double axis[3];
+    cross3(u, ref, axis);
+    double normAxis = sqrt(dot3(axis, axis));
+    if (normAxis < tol) {
+        double d = dot3(u, ref) - 1.0;
+        if ((d < 0 ? -d : d) < tol) {
+            q[0] = 1.0;
+            q[1] = q[2] = q[3] = 0.0;
+            return true;
+        }
+        return false;
+    }
+    axis[0] /= normAxis;
+    axis[1] /= normAxis;
+    axis[2] /= normAxis;
+    double cosAngle = sqrt(0.5 * (1 + dot3(u, ref)));
+    double sinAngle = sqrt(1 - cosAngle * cosAngle);
+    q[0] = cosAngle;
+    q[1] = sinAngle * axis[0];
+    q[2] = sinAngle * axis[1];
+    q[3] = sinAngle * axis[2];
+    return true;
+}
+
+// ---------------------------------------------------------------- trafos
+SC_HD void trafo_make(Trafo& t, const double* origin, const double* quat) {
+    for (int i = 0; i < 3; ++i) t.origin[i] = origin[i];
+    for (int i = 0; i < 4; ++i) t.quat[i] = quat[i];
+    quat_rotmat(t.quat, t.M);
+}
+SC_HD void trafo_invert(Trafo& t) {
+    double r[3];
+    quat_rotate(t.quat, t.origin, r);
+    t.origin[0] = -r[0];
+    t.origin[1] = -r[1];
+    t.origin[2] = -r[2];
+    t.quat[1] = -t.quat[1];
+    t.quat[2] = -t.quat[2];
+    t.quat[3] = -t.quat[3];
+    double M[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) M[i * 3 + j] = t.M[j * 3 + i];
+    for (int i = 0; i < 9; ++i) t.M[i] = M[i];
+}
+SC_HD void trafo_compose(Trafo& t, const Trafo& right) {
+    double rc[4] = {right.quat[0], -right.quat[1], -right.quat[2], -right.quat[3]};
+    double r[3];
+    quat_rotate(rc, t.origin, r);
+    t.origin[0] = r[0] + right.origin[0];
+    t.origin[1] = r[1] + right.origin[1];
+    t.origin[2] = r[2] + right.origin[2];
+    double q[4];
+    quat_mul(t.quat, right.quat, q);
+    for (int i = 0; i < 4; ++i) t.quat[i] = q[i];
+    quat_normalize(t.quat);
+    quat_rotmat(t.quat, t.M);
+}
+SC_HD void trafo_transform_to(const Trafo& t, const double* r, double* out) {
+    double d[3] = {r[0] - t.origin[0], r[1] - t.origin[1], r[2] - t.origin[2]};
+    matvec(t.M, d, out);
+}
+SC_HD void trafo_rotate_to(const Trafo& t, const double* r, double* out) { matvec(t.M, r, out); }
+
+// ---------------------------------------------------------------- pusher
+// BorisPusher::push between switchToUnitlessPositions / switchOff...
+SC_HD void push_one(double* R, const double* P, double dt) {
+    const double s = kC * dt;
+    double r0 = R[0] / s, r1 = R[1] / s, r2 = R[2] / s;
+    double g = sqrt(1.0 + dot3(P, P));
+    r0 += 0.5 * P[0] / g;
+    r1 += 0.5 * P[1] / g;
+    r2 += 0.5 * P[2] / g;
+    R[0] = r0 * s;
+    R[1] = r1 * s;
+    R[2] = r2 * s;
+}
+// BorisPusher::kick
+SC_HD void kick_one(double* P, const double* Ef, const double* Bf, double dt, double mass, double charge) {
+    const double ke = 0.5 * dt * charge * kC / mass;
+    P[0] += ke * Ef[0];
+    P[1] += ke * Ef[1];
+    P[2] += ke * Ef[2];
+    const double gamma = sqrt(1.0 + dot3(P, P));
+    const double kt = 0.5 * dt * charge * kC * kC / (gamma * mass);
+    double t[3] = {kt * Bf[0], kt * Bf[1], kt * Bf[2]};
+    double w[3], c[3];
+    cross3(P, t, c);
+    w[0] = P[0] + c[0];
+    w[1] = P[1] + c[1];
+    w[2] = P[2] + c[2];
+    const double ks = 2.0 / (1.0 + dot3(t, t));
+    double s[3] = {ks * t[0], ks * t[1], ks * t[2]};
+    cross3(w, s, c);
+    P[0] += c[0];
+    P[1] += c[1];
+    P[2] += c[2];
+    P[0] += ke * Ef[0];
+    P[1] += ke * Ef[1];
+    P[2] += ke * Ef[2];
+}
+
+// ---------------------------------------------------------------- CIC
+// Lower grid point and normalised offset of a particle (IntCIC.h:818-858 with
+// getVertexBelow, UniformCartesian.hpp:1025-1039, and getCellPosition,
+// :1084-1097).  Returns false when a stencil point would leave the n^3 field.
+SC_HD bool cic_locate(const double* hr, const double* origin, const int* n, const double* x, int* lgp,
+                      double* dpos) {
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+        int i = (int)((x[d] - origin[d]) / hr[d]);
+        int ngp = (x[d] >= origin[d]) ? i : i - 1;
+        double gpos = (ngp + 0.5) * hr[d] + origin[d];
+        double delta = hr[d];
+        int l = ngp;
+        if (gpos > x[d]) {
+            l = ngp - 1;
+            gpos = gpos - delta;
+        }
+        double dp = x[d] - gpos;
+        dp /= delta;
+        if (l < 0) {
+            ok = false;
+            l = 0;
+        }
+        if (l > n[d] - 2) {
+            ok = false;
+            l = n[d] - 2;
+        }
+        lgp[d] = l;
+        dpos[d] = dp;
+    }
+    return ok;
+}
+
+// ---------------------------------------------------------------- mesh
+// boundp (PartBunchBase.hpp:802-884) from the beam-frame bounds, then the
+// scalars of computeSelfFields (PartBunch.cpp:493-511, 541-547, 641).
+// Returns false when h <= 0.
+SC_HD bool derive_mesh(StepState& s, const BunchConst& bc) {
+    double rmin[3] = {s.bmin[0], s.bmin[1], s.bmin[2]};
+    double rmax[3] = {s.bmax[0], s.bmax[1], s.bmax[2]};
+    for (int i = 0; i < 3; ++i) {
+        double length = rmax[i] - rmin[i];
+        if (length < 0) length = -length;
+        if (length < 1e-10) {
+            rmax[i] += 1e-10;
+            rmin[i] -= 1e-10;
+        } else {
+            rmax[i] += bc.dh * length;
+            rmin[i] -= bc.dh * length;
+        }
+        s.hr[i] = (rmax[i] - rmin[i]) / (bc.n[i] - 1);
+        s.mesh_rmin[i] = rmin[i];
+        s.mesh_rmax[i] = rmax[i];
+    }
+    bool ok = s.hr[0] * s.hr[1] * s.hr[2] > 0;
+    for (int i = 0; i < 3; ++i) s.origin[i] = rmin[i] - s.hr[i] / 2.0;
+    double gz = s.psum[2] / (double)bc.N;
+    gz *= gz;
+    gz = sqrt(gz + 1.0);
+    s.gammaz = gz;
+    s.hr_scaled[0] = s.hr[0] * 1.0;
+    s.hr_scaled[1] = s.hr[1] * 1.0;
+    s.hr_scaled[2] = s.hr[2] * 1.0;
+    s.hr_scaled[2] *= gz;
+    s.tmp2 = 1 / s.hr_scaled[0] * 1 / s.hr_scaled[1] * 1 / s.hr_scaled[2];
+    s.hvol = s.hr_scaled[0] * s.hr_scaled[1] * s.hr_scaled[2];
+    s.betaC = sqrt(gz * gz - 1.0) / gz / kC;
+    return ok;
+}
+
+// Beam-frame trafos of computeSpaceChargeFields (ParallelTTracker.cpp:550-554)
+// from the momentum sum and the path length.  Returns false for an
+// anti-parallel mean momentum.
+SC_HD bool derive_beam_frame(StepState& s, const BunchConst& bc) {
+    const double N = (double)bc.N;
+    double pmean[3] = {s.psum[0] / N, s.psum[1] / N, s.psum[2] / N};
+    double zhat[3] = {0.0, 0.0, 1.0}, q[4];
+    bool ok = get_quaternion(pmean, zhat, q);
+    if (!ok) {
+        q[0] = 1.0;
+        q[1] = q[2] = q[3] = 0.0;
+    }
+    double qc[4] = {q[0], -q[1], -q[2], -q[3]};
+    double org[3] = {0.0, 0.0, s.path_length};
+    trafo_make(s.b2r, org, qc);
+    s.r2b = s.b2r;
+    trafo_invert(s.r2b);
+    return ok;
+}
+
+// updateReferenceParticle + updateRefToLabCSTrafo (ParallelTTracker.cpp:1123-1212)
+// for a beamline with no elements except an optional uniform B_z.
+SC_HD bool advance_reference(StepState& s, const BunchConst& bc) {
+    s.t += bc.dT;
+    const double dt = s.t < bc.dT ? s.t : bc.dT;
+    const double scaleFactor = kC * dt;
+    double* rr = s.ref_R;
+    double* rp = s.ref_P;
+    double zero[3] = {0.0, 0.0, 0.0}, bref[3] = {0.0, 0.0, 0.0};
+    for (int pass = 0; pass < 2; ++pass) {
+        rr[0] /= scaleFactor;
+        rr[1] /= scaleFactor;
+        rr[2] /= scaleFactor;
+        double g = sqrt(1.0 + dot3(rp, rp));
+        rr[0] += 0.5 * rp[0] / g;
+        rr[1] += 0.5 * rp[1] / g;
+        rr[2] += 0.5 * rp[2] / g;
+        rr[0] *= scaleFactor;
+        rr[1] *= scaleFactor;
+        rr[2] *= scaleFactor;
+        if (pass == 0) {
+            if (bc.bz_ext != 0.0) bref[2] += bc.bz_ext;
+            kick_one(rp, zero, bref, dt, bc.mass, bc.charge);
+        }
+    }
+    s.path_length += sqrt(dot3(rr, rr));
+    double zhat[3] = {0.0, 0.0, 1.0}, qu[4];
+    bool ok = get_quaternion(rp, zhat, qu);
+    if (!ok) {
+        qu[0] = 1.0;
+        qu[1] = qu[2] = qu[3] = 0.0;
+    }
+    trafo_make(s.upd, rr, qu);
+    double v[3];
+    trafo_transform_to(s.upd, rr, v);
+    rr[0] = v[0];
+    rr[1] = v[1];
+    rr[2] = v[2];
+    trafo_rotate_to(s.upd, rp, v);
+    rp[0] = v[0];
+    rp[1] = v[1];
+    rp[2] = v[2];
+    Trafo inv = s.upd;
+    trafo_invert(inv);
+    trafo_compose(s.ref_to_lab, inv);
+    return ok;
+}
+
+}  // namespace sc

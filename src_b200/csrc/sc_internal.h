@@ -1,0 +1,94 @@
+// sc_internal.h -- launchers shared between the translation units of libscgpu.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sc_common.cuh"
+
+namespace sc {
+
+// Device buffers of one bunch + solver instance.  All grid arrays use
+// x-fastest order: index = x + n0 * (y + n1 * z).
+struct DevBunch {
+    BunchConst bc;
+    int precision;  // 0 = plain FP64, 1 = mixed
+    // particle state (SoA, beam or reference frame depending on the phase)
+    double* x;
+    double* y;
+    double* z;
+    double* px;
+    double* py;
+    double* pz;
+    // sort
+    uint32_t* keys;
+    uint32_t* keys_alt;
+    uint32_t* vals;
+    uint32_t* vals_alt;
+    int* hist;        // radix digit table [bins][tiles]
+    int* hist_scan;   // exclusive scan of hist
+    int* scan_blocks; // block sums of the scan
+    int sort_tiles;
+    // deposit
+    void* seg;        // per-cell corner sums S[cell][8] (double or float2 pairs)
+    uint32_t* stamp;  // per-cell generation stamp
+    void* carry_first;
+    void* carry_last;
+    int* wflag;
+    long long nwin;
+    // grids
+    void* rho;        // n^3 real (T)
+    void* phi;        // n^3 real (T)
+    void* E4;         // n^3 x 4 (T): (-grad phi) * (g, g, 1/g), w unused
+    void* spec;       // (n2+1) x L1 x L0 complex (T)
+    double* gtmp;     // (n0+2)(n1+2)(n2+2) IGF antiderivative
+    double* gline;    // (n0+1)(n1+1)(n2+1) G then its cosine transforms (FP64)
+    void* ghat;       // (n0+1)(n1+1)(n2+1) real spectrum of G (T)
+    void* tw[3];      // twiddles exp(-2 pi i e / L_d), complex T, per axis
+    // reductions
+    double* partials;
+    unsigned* ticket;
+    StepState* st;
+    int red_blocks;
+    // per-launch scratch for optional outputs
+    double* Ef;
+    double* Bf;
+};
+
+struct FftPlan {
+    int L;
+    int nst;
+    int r[12];
+};
+
+FftPlan make_plan(int L);
+int particle_grid(const DevBunch& b);
+
+// particle TU (sc_particles.cu)
+void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s);
+void launch_drift_to_beam(const DevBunch& b, bool drift, bool advance_ref, cudaStream_t s);
+void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s);
+void launch_deposit(const DevBunch& b, cudaStream_t s);
+void launch_assemble_rho(const DevBunch& b, cudaStream_t s);
+void launch_igf(const DevBunch& b, const double* hr_host, cudaStream_t s);
+void launch_grad(const DevBunch& b, cudaStream_t s);
+void launch_gather_kick_push(const DevBunch& b, bool stats, cudaStream_t s);
+void launch_gather_fields(const DevBunch& b, cudaStream_t s);
+
+// sort TU (sc_sort.cu)
+int sort_tile_elems();
+void launch_sort(const DevBunch& b, cudaStream_t s);
+
+// FFT TU (sc_fft.cu)
+void launch_green_transform(const DevBunch& b, cudaStream_t s);
+void launch_convolution(const DevBunch& b, int mode, cudaStream_t s);
+size_t fft_smem_bytes(const DevBunch& b);
+void upload_twiddles(DevBunch& b, cudaStream_t s);
+
+// convolution modes
+enum : int {
+    kConvSelfField = 0,  // phi = conv * normFact * hvol * coupling (computeSelfFields)
+    kConvPotential = 1,  // phi = conv * normFact (PoissonSolver::computePotential)
+};
+
+}  // namespace sc
