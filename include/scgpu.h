@@ -1,0 +1,177 @@
+/*
+ * scgpu.h -- C ABI of the B200 space-charge step for OPAL's time-domain
+ * tracker.  Plain C types only (pointers, sizes, doubles); no CUDA or torch
+ * types cross this boundary.  Every entry point returns an int status
+ * (SCGPU_OK or a negative SCGPU_ERR_*) and never aborts; the text of the
+ * last failure is available from scgpu_last_error().
+ *
+ * Which reference interface each entry point replaces (paths relative to
+ * the OPAL source tree):
+ *
+ *   scgpu_create / scgpu_destroy
+ *       FieldSolver::initSolver -> new FFTPoissonSolver(mesh, layout,
+ *       "INTEGRATED", bcz)  (src/Structure/FieldSolver.cpp:440-532, :486) and
+ *       PartBunchBase::setSolver (src/Classic/Algorithms/PartBunchBase.hpp:1739-1754);
+ *       device set-up of the DKS path ParallelTTracker::setupDKS /
+ *       allocateDeviceMemory (src/Algorithms/ParallelTTracker.h:468-499)
+ *   scgpu_compute_potential, scgpu_compute_potential_device
+ *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr)
+ *       (src/Solvers/PoissonSolver.h:28; FFTPoissonSolver.cpp:337-382)
+ *   scgpu_compute_self_fields
+ *       PartBunch::computeSelfFields()  (src/Classic/Algorithms/PartBunch.cpp:482-647,
+ *       declared PartBunchBase.h:372, called ParallelTTracker.cpp:583),
+ *       preceded by boundp() (PartBunchBase.hpp:802-884)
+ *   scgpu_bunch_upload / scgpu_bunch_download
+ *       DKS writeDataAsync / readData of R, P  (ParallelTTracker.h:501-512, :514-529)
+ *   scgpu_register_host / scgpu_unregister_host
+ *       DKS registerHostMemory / unregisterHostMemory (ParallelTTracker.h:490-496)
+ *   scgpu_track
+ *       the ParallelTTracker::execute step loop (src/Algorithms/ParallelTTracker.cpp:343-388):
+ *       timeIntegration1 (pushParticles / pushParticlesDKS, :434-447,
+ *       ParallelTTracker.h:448-455, :514-529), computeSpaceChargeFields (:546-592),
+ *       timeIntegration2 (kickParticles+pushParticles / kickParticlesDKS, :450-491,
+ *       ParallelTTracker.h:442-446, :531-562), updateRefToLabCSTrafo (:1199-1212)
+ *   scgpu_beam_parameters
+ *       PartBunchBase::calcBeamParameters (PartBunchBase.hpp:1529-1614) with
+ *       calcMoments (:2185-2259)
+ *
+ * Layouts: particle vectors are N x 3 doubles, x, y, z per particle (OPAL's
+ * ParticleAttrib<Vector_t>).  Grids are nx*ny*nz doubles with x fastest:
+ * index = i + nx*(j + ny*k), the cell-centred field of the reference without
+ * its guard layer.
+ *
+ * Threading: one context per host thread; a context is not re-entrant.
+ */
+#ifndef SCGPU_H
+#define SCGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCGPU_ABI_VERSION 1
+
+#define SCGPU_OK 0
+#define SCGPU_ERR_ARG (-1)          /* invalid argument or size */
+#define SCGPU_ERR_OOM (-2)          /* device or host allocation failed */
+#define SCGPU_ERR_MESH (-3)         /* boundp: h <= 0, cannot build a mesh */
+#define SCGPU_ERR_GUARD (-4)        /* a CIC stencil left the mesh */
+#define SCGPU_ERR_FRAME (-5)        /* getQuaternion of an anti-parallel or null vector */
+#define SCGPU_ERR_CUDA (-6)         /* CUDA runtime error */
+#define SCGPU_ERR_STATE (-7)        /* call order (e.g. tracking without a bunch) */
+#define SCGPU_ERR_UNSUPPORTED (-8)  /* mesh size or option this build does not support */
+
+#define SCGPU_PLAIN_FP64 0  /* FP64 throughout */
+#define SCGPU_MIXED 1       /* FP32 grid work, FP64 particles / Green's function / boost */
+
+#define SCGPU_NSTATS 28     /* per-step statistics record: 27 moment sums + sum of gamma */
+
+#define SCGPU_FIELD_RHO 0   /* charge density fed to the solver [C/m^3], nx*ny*nz */
+#define SCGPU_FIELD_PHI 1   /* potential [V], nx*ny*nz */
+#define SCGPU_FIELD_E 2     /* -grad(phi) scaled by (gz, gz, 1/gz) [V/m], 3*nx*ny*nz interleaved */
+
+typedef struct scgpu_ctx scgpu_ctx;
+
+/* FIELDSOLVER attributes (src/Structure/FieldSolver.cpp:127-165) */
+typedef struct scgpu_solver_params {
+    int mx, my, mt;          /* MX, MY, MT: mesh cells per axis (2n must factor into 2, 3, 5) */
+    int precision;           /* SCGPU_PLAIN_FP64 or SCGPU_MIXED */
+    double bboxincr;         /* BBOXINCR in percent (OPAL default 2.0) */
+} scgpu_solver_params;
+
+/* bunch constants and tracker state at upload */
+typedef struct scgpu_bunch_params {
+    double dT;               /* time step [s] */
+    double mass;             /* rest energy [eV] (PartData::getM) */
+    double charge;           /* particle charge [e] (PartData::getQ) */
+    double q_macro;          /* charge per macro-particle [C] (PartBunch Q) */
+    double coupling;         /* 1/(4 pi eps0) (TrackRun.cpp:423) */
+    double bz_ext;           /* uniform external B_z [T] in the reference frame, 0 for a drift */
+    double t;                /* time [s] */
+    double path_length;      /* s-position of the reference particle [m] */
+    double ref_R[3];         /* reference particle position (reference frame) */
+    double ref_P[3];         /* reference particle beta*gamma */
+} scgpu_bunch_params;
+
+typedef struct scgpu_tracker_state {
+    double t;
+    double path_length;
+    double ref_R[3];
+    double ref_P[3];
+    double q_macro;
+    double ref_to_lab_origin[3];
+    double ref_to_lab_quat[4];
+    long long step;
+} scgpu_tracker_state;
+
+/* calcBeamParameters outputs */
+typedef struct scgpu_beam_params {
+    double rmean[3], pmean[3];
+    double rrms[3], prms[3];
+    double eps_norm[3], eps[3];
+    double rprms[3];
+    double gamma;
+    double moments[27];      /* x, px, y, py, z, pz sums, then the lower triangle of products */
+} scgpu_beam_params;
+
+typedef struct scgpu_mesh {
+    double hr[3];            /* mesh spacing of the last solve [m] */
+    double origin[3];
+    double rmin[3], rmax[3]; /* enlarged beam-frame bounds */
+    double gammaz;
+    double hr_scaled[3];     /* rest-frame spacing passed to the Poisson solve */
+} scgpu_mesh;
+
+int scgpu_abi_version(void);
+
+int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* params, int device);
+void scgpu_destroy(scgpu_ctx* ctx);
+const char* scgpu_last_error(const scgpu_ctx* ctx);
+/* run on a caller-owned cudaStream_t (passed as void*); NULL = the context's own stream */
+int scgpu_set_stream(scgpu_ctx* ctx, void* cuda_stream);
+int scgpu_synchronize(scgpu_ctx* ctx);
+
+/* PoissonSolver::computePotential: rho (nx*ny*nz, x fastest) in, the open-
+ * boundary convolution with the integrated Green's function out (in place),
+ * i.e. phi * 4 pi eps0 / (hx hy hz) in the reference's units.  hr is the
+ * rest-frame mesh spacing. */
+int scgpu_compute_potential(scgpu_ctx* ctx, double* rho_inout, const double hr[3]);
+int scgpu_compute_potential_device(scgpu_ctx* ctx, double* rho_inout_device, const double hr[3]);
+
+/* PartBunch::computeSelfFields on a bunch already in the beam frame: boundp,
+ * CIC deposit of q_macro*dT ... /dT, Poisson solve, -grad, CIC gather; writes
+ * Ef, Bf (N x 3, beam frame).  *q_macro is updated by the reference's
+ * Q *= dt ... Q /= dt round trip. */
+int scgpu_compute_self_fields(scgpu_ctx* ctx, long long n, const double* R, const double* P, double* q_macro, double dT,
+                              double* Ef, double* Bf);
+
+int scgpu_register_host(scgpu_ctx* ctx, void* ptr, long long bytes);
+int scgpu_unregister_host(scgpu_ctx* ctx, void* ptr);
+
+/* Bunch state (reference frame, coordinates relative to the reference
+ * particle).  Upload resets the tracker state from *bp. */
+int scgpu_bunch_upload(scgpu_ctx* ctx, long long n, const double* R, const double* P, const scgpu_bunch_params* bp);
+int scgpu_bunch_download(scgpu_ctx* ctx, double* R, double* P);
+
+/* Advance the device-resident bunch by nsteps ParallelTTracker steps.  When
+ * stats is not NULL it receives nsteps records of SCGPU_NSTATS doubles: the
+ * moment sums of the state at the end of each step (asynchronous copies;
+ * pinned memory keeps them off the critical path). */
+int scgpu_track(scgpu_ctx* ctx, int nsteps, double* stats);
+
+int scgpu_get_tracker_state(scgpu_ctx* ctx, scgpu_tracker_state* out);
+int scgpu_beam_parameters(scgpu_ctx* ctx, scgpu_beam_params* out);
+/* beam parameters from one SCGPU_NSTATS record of scgpu_track */
+int scgpu_beam_parameters_from_stats(const double* record, long long n, scgpu_beam_params* out);
+
+/* diagnostics of the last solve: SCGPU_FIELD_* grids and the mesh */
+int scgpu_get_field(scgpu_ctx* ctx, int which, double* out);
+int scgpu_get_mesh(scgpu_ctx* ctx, scgpu_mesh* out);
+
+/* device-side elapsed time of the last scgpu_track call [ms] */
+double scgpu_last_track_ms(const scgpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,638 @@
+// sc_api.cu -- the C ABI (include/scgpu.h): contexts, device memory, the step
+// sequence and its CUDA graph.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "scgpu.h"
+#include "sc_internal.h"
+
+using namespace sc;
+
+struct scgpu_ctx {
+    int device = 0;
+    scgpu_solver_params sp{};
+    DevBunch b{};
+    cudaStream_t stream = nullptr;   // work stream (own or the caller's)
+    cudaStream_t own = nullptr;
+    cudaStream_t side = nullptr;     // Green's function branch
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+    long long capacity = 0;
+    long long n = 0;
+    bool have_bunch = false;
+    bool have_solve = false;
+    int digit_bits = 0;
+    std::string err;
+    double last_ms = 0.0;
+    cudaGraphExec_t g_step = nullptr;
+    cudaGraphExec_t g_step_stats = nullptr;
+    bool use_graphs = true;
+    size_t smem_fft = 0;
+};
+
+namespace {
+
+int fail(scgpu_ctx* c, int code, const std::string& what) {
+    if (c) c->err = what;
+    return code;
+}
+
+int cuda_fail(scgpu_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, SCGPU_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                          \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+    } while (0)
+
+template <typename P>
+int dalloc(scgpu_ctx* c, P** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(c, SCGPU_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return SCGPU_OK;
+}
+
+template <typename P>
+void dfree(P*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+bool length_ok(int n) {
+    if (n < 3 || 2 * n > 256) return false;
+    return make_plan(2 * n).nst > 0;
+}
+
+void free_particles(scgpu_ctx* c) {
+    DevBunch& b = c->b;
+    dfree(b.x); dfree(b.y); dfree(b.z); dfree(b.px); dfree(b.py); dfree(b.pz);
+    dfree(b.keys); dfree(b.keys_alt); dfree(b.vals); dfree(b.vals_alt);
+    dfree(b.hist); dfree(b.hist_scan); dfree(b.scan_blocks);
+    dfree(b.carry_first); dfree(b.carry_last); dfree(b.wflag);
+    dfree(b.Ef); dfree(b.Bf);
+    c->capacity = 0;
+}
+
+void drop_graphs(scgpu_ctx* c) {
+    if (c->g_step) cudaGraphExecDestroy(c->g_step);
+    if (c->g_step_stats) cudaGraphExecDestroy(c->g_step_stats);
+    c->g_step = c->g_step_stats = nullptr;
+}
+
+int ensure_particles(scgpu_ctx* c, long long n) {
+    if (n <= 0 || n > 0x7fffffffLL) return fail(c, SCGPU_ERR_ARG, "particle count must be in [1, 2^31)");
+    DevBunch& b = c->b;
+    if (n > c->capacity) {
+        drop_graphs(c);
+        free_particles(c);
+        int rc;
+        const size_t d = (size_t)n * sizeof(double);
+        const size_t u = (size_t)n * sizeof(uint32_t);
+        if ((rc = dalloc(c, &b.x, d)) || (rc = dalloc(c, &b.y, d)) || (rc = dalloc(c, &b.z, d)) ||
+            (rc = dalloc(c, &b.px, d)) || (rc = dalloc(c, &b.py, d)) || (rc = dalloc(c, &b.pz, d)))
+            return rc;
+        if ((rc = dalloc(c, &b.keys, u)) || (rc = dalloc(c, &b.keys_alt, u)) || (rc = dalloc(c, &b.vals, u)) ||
+            (rc = dalloc(c, &b.vals_alt, u)))
+            return rc;
+        if ((rc = dalloc(c, &b.Ef, 3 * d)) || (rc = dalloc(c, &b.Bf, 3 * d))) return rc;
+        const long long tiles = (n + sort_tile_elems() - 1) / sort_tile_elems();
+        const long long table = tiles * 512;
+        if ((rc = dalloc(c, &b.hist, table * sizeof(int))) || (rc = dalloc(c, &b.hist_scan, table * sizeof(int))) ||
+            (rc = dalloc(c, &b.scan_blocks, (2 * (table / 8192 + 2)) * sizeof(int))))
+            return rc;
+        const long long nwin = (n + 31) / 32;
+        if ((rc = dalloc(c, (double**)&b.carry_first, nwin * 8 * sizeof(double))) ||
+            (rc = dalloc(c, (double**)&b.carry_last, nwin * 8 * sizeof(double))) ||
+            (rc = dalloc(c, &b.wflag, nwin * sizeof(int))))
+            return rc;
+        c->capacity = n;
+    }
+    if (n != c->n) drop_graphs(c);
+    c->n = n;
+    b.bc.N = n;
+    b.sort_tiles = (int)((n + sort_tile_elems() - 1) / sort_tile_elems());
+    b.nwin = (n + 31) / 32;
+    long long g = (n + 255) / 256;
+    if (g < 1) g = 1;
+    if (g > 148 * 4) g = 148 * 4;
+    b.red_blocks = (int)g;
+    return SCGPU_OK;
+}
+
+// one ParallelTTracker step on the context's stream
+void enqueue_step(scgpu_ctx* c, bool stats, cudaStream_t s) {
+    DevBunch& b = c->b;
+    launch_drift_to_beam(b, true, true, s);
+    // Green's function branch depends only on the mesh
+    cudaEventRecord(c->ev_fork, s);
+    cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+    launch_igf(b, nullptr, c->side);
+    launch_green_transform(b, c->side);
+    cudaEventRecord(c->ev_join, c->side);
+    launch_cell_keys(b, c->digit_bits, s);
+    launch_sort(b, s);
+    launch_deposit(b, s);
+    launch_assemble_rho(b, s);
+    cudaStreamWaitEvent(s, c->ev_join, 0);
+    launch_convolution(b, kConvSelfField, s);
+    launch_grad(b, s);
+    launch_gather_kick_push(b, stats, s);
+}
+
+int build_graph(scgpu_ctx* c, bool stats, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c, stats, c->own);
+    cudaError_t e = cudaStreamEndCapture(c->own, &g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+    return SCGPU_OK;
+}
+
+int check_device_err(scgpu_ctx* c) {
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, &c->b.st->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (err) {
+        int zero = 0;
+        cudaMemcpyAsync(&c->b.st->err, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream);
+        cudaStreamSynchronize(c->stream);
+        if (err & kFlagMesh) return fail(c, SCGPU_ERR_MESH, "boundp: h <= 0, cannot build a mesh");
+        if (err & kFlagFrame) return fail(c, SCGPU_ERR_FRAME, "getQuaternion: anti-parallel or null vector");
+        if (err & kFlagGuard) return fail(c, SCGPU_ERR_GUARD, "a CIC stencil left the mesh");
+        if (err & kFlagSort) return fail(c, SCGPU_ERR_CUDA, "cell sort: scatter position out of range");
+        return fail(c, SCGPU_ERR_CUDA, "unknown device error flag");
+    }
+    return SCGPU_OK;
+}
+
+// calcBeamParameters from the moment sums (PartBunchBase.hpp:1529-1614)
+int mom_idx(int i, int j) {
+    if (i < j) {
+        int t = i;
+        i = j;
+        j = t;
+    }
+    return 6 + i * (i + 1) / 2 + j;
+}
+
+void beam_params_from_sums(const double* m27, double gsum, double N, scgpu_beam_params* bp) {
+    double rsqsum[3], psqsum[3], rpsum[3], eps2[3];
+    for (int i = 0; i < 3; ++i) {
+        bp->rmean[i] = m27[2 * i] / N;
+        bp->pmean[i] = m27[2 * i + 1] / N;
+        rsqsum[i] = m27[mom_idx(2 * i, 2 * i)] - N * bp->rmean[i] * bp->rmean[i];
+        psqsum[i] = m27[mom_idx(2 * i + 1, 2 * i + 1)] - N * bp->pmean[i] * bp->pmean[i];
+        if (psqsum[i] < 0) psqsum[i] = 0;
+        rpsum[i] = m27[mom_idx(2 * i, 2 * i + 1)] - N * bp->rmean[i] * bp->pmean[i];
+    }
+    for (int i = 0; i < 3; ++i) eps2[i] = (rsqsum[i] * psqsum[i] - rpsum[i] * rpsum[i]) / (N * N);
+    for (int i = 0; i < 3; ++i) rpsum[i] /= N;
+    for (int i = 0; i < 3; ++i) {
+        bp->rrms[i] = std::sqrt(rsqsum[i] / N);
+        bp->prms[i] = std::sqrt(psqsum[i] / N);
+        bp->eps_norm[i] = std::sqrt(eps2[i] > 0.0 ? eps2[i] : 0.0);
+        double tmp = bp->rrms[i] * bp->prms[i];
+        double fac = (tmp == 0) ? 0.0 : 1.0 / tmp;
+        bp->rprms[i] = rpsum[i] * fac;
+    }
+    double gamma = gsum / N;
+    bp->gamma = gamma;
+    double den = gamma * std::sqrt(1.0 - 1.0 / (gamma * gamma));
+    for (int i = 0; i < 3; ++i) bp->eps[i] = bp->eps_norm[i] / den;
+    for (int k = 0; k < 27; ++k) bp->moments[k] = m27[k];
+}
+
+// With SCGPU_SYNC_CHECK set, every stage of the synchronous entry points is
+// synchronised and checked, so a device error names the kernel that raised it.
+bool sync_check_enabled() {
+    static const bool on = std::getenv("SCGPU_SYNC_CHECK") != nullptr;
+    return on;
+}
+
+int stage_check(scgpu_ctx* c, cudaStream_t s, const char* name) {
+    if (!sync_check_enabled()) return SCGPU_OK;
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, name);
+    return SCGPU_OK;
+}
+
+#define STAGE(name)                                  \
+    do {                                             \
+        int rc_ = stage_check(c, s, name);           \
+        if (rc_) return rc_;                         \
+    } while (0)
+
+// the solve shared by compute_potential and compute_self_fields
+void enqueue_green(scgpu_ctx* c, cudaStream_t s) {
+    launch_igf(c->b, nullptr, s);
+    launch_green_transform(c->b, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int scgpu_abi_version(void) { return SCGPU_ABI_VERSION; }
+
+int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
+    if (!out || !p) return SCGPU_ERR_ARG;
+    *out = nullptr;
+    if (p->precision != SCGPU_PLAIN_FP64 && p->precision != SCGPU_MIXED) return SCGPU_ERR_ARG;
+    if (!length_ok(p->mx) || !length_ok(p->my) || !length_ok(p->mt)) return SCGPU_ERR_UNSUPPORTED;
+    if (!(p->bboxincr >= 0.0)) return SCGPU_ERR_ARG;
+    scgpu_ctx* c = new scgpu_ctx();
+    c->device = device;
+    c->sp = *p;
+    c->use_graphs = std::getenv("SCGPU_NO_GRAPH") == nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        return SCGPU_ERR_CUDA;
+    }
+    DevBunch& b = c->b;
+    b.precision = p->precision;
+    b.bc.n[0] = p->mx;
+    b.bc.n[1] = p->my;
+    b.bc.n[2] = p->mt;
+    b.bc.dh = p->bboxincr / 100.0;
+    const long long n0 = p->mx, n1 = p->my, n2 = p->mt;
+    const long long M = n0 * n1 * n2;
+    int bits = 0;
+    while ((1LL << bits) < M) ++bits;
+    b.bc.key_bits = bits < 1 ? 1 : bits;
+    c->digit_bits = sort_digit_bits(b.bc.key_bits);
+    const size_t rs = p->precision == SCGPU_PLAIN_FP64 ? sizeof(double) : sizeof(float);
+    int rc = SCGPU_OK;
+    const long long S = (n2 + 1) * (2 * n1) * (2 * n0);
+    const long long T3 = (n0 + 2) * (n1 + 2) * (n2 + 2);
+    const long long G3 = (n0 + 1) * (n1 + 1) * (n2 + 1);
+    if ((rc = dalloc(c, (double**)&b.seg, M * 8 * sizeof(double))) || (rc = dalloc(c, &b.stamp, M * sizeof(uint32_t))) ||
+        (rc = dalloc(c, (char**)&b.rho, M * rs)) || (rc = dalloc(c, (char**)&b.phi, M * rs)) ||
+        (rc = dalloc(c, (char**)&b.E4, 4 * M * rs)) || (rc = dalloc(c, (char**)&b.spec, S * 2 * rs)) ||
+        (rc = dalloc(c, &b.gtmp, T3 * sizeof(double))) || (rc = dalloc(c, &b.gline, G3 * sizeof(double))) ||
+        (rc = dalloc(c, (char**)&b.ghat, G3 * rs)) || (rc = dalloc(c, &b.st, sizeof(StepState))) ||
+        (rc = dalloc(c, &b.partials, 148 * 4 * 32 * sizeof(double))) || (rc = dalloc(c, &b.ticket, 64))) {
+        scgpu_destroy(c);
+        return rc;
+    }
+    for (int d = 0; d < 3; ++d) {
+        const int L = 2 * b.bc.n[d];
+        if ((rc = dalloc(c, (char**)&b.tw[d], L * (sizeof(double2) + sizeof(float2))))) {
+            scgpu_destroy(c);
+            return rc;
+        }
+    }
+    cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+    c->stream = c->own;
+    cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    cudaEventCreate(&c->ev_t0);
+    cudaEventCreate(&c->ev_t1);
+    cudaMemsetAsync(b.stamp, 0, M * sizeof(uint32_t), c->own);
+    cudaMemsetAsync(b.ticket, 0, 64, c->own);
+    cudaMemsetAsync(b.st, 0, sizeof(StepState), c->own);
+    fft_set_smem_limits();
+    upload_twiddles(b, c->own);
+    e = cudaStreamSynchronize(c->own);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        scgpu_destroy(c);
+        return SCGPU_ERR_CUDA;
+    }
+    *out = c;
+    return SCGPU_OK;
+}
+
+void scgpu_destroy(scgpu_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->own) cudaStreamSynchronize(c->own);
+    if (c->stream && c->stream != c->own) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    free_particles(c);
+    DevBunch& b = c->b;
+    dfree(b.seg); dfree(b.stamp); dfree(b.rho); dfree(b.phi); dfree(b.E4); dfree(b.spec);
+    dfree(b.gtmp); dfree(b.gline); dfree(b.ghat); dfree(b.st); dfree(b.partials); dfree(b.ticket);
+    for (int d = 0; d < 3; ++d) dfree(b.tw[d]);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->ev_t0) cudaEventDestroy(c->ev_t0);
+    if (c->ev_t1) cudaEventDestroy(c->ev_t1);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+}
+
+const char* scgpu_last_error(const scgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int scgpu_set_stream(scgpu_ctx* c, void* stream) {
+    if (!c) return SCGPU_ERR_ARG;
+    c->stream = stream ? (cudaStream_t)stream : c->own;
+    return SCGPU_OK;
+}
+
+int scgpu_synchronize(scgpu_ctx* c) {
+    if (!c) return SCGPU_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    return SCGPU_OK;
+}
+
+int scgpu_register_host(scgpu_ctx* c, void* ptr, long long bytes) {
+    if (!c || !ptr || bytes <= 0) return SCGPU_ERR_ARG;
+    CK(cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault));
+    return SCGPU_OK;
+}
+
+int scgpu_unregister_host(scgpu_ctx* c, void* ptr) {
+    if (!c || !ptr) return SCGPU_ERR_ARG;
+    CK(cudaHostUnregister(ptr));
+    return SCGPU_OK;
+}
+
+static int compute_potential_impl(scgpu_ctx* c, double* rho, const double hr[3], bool device_ptr) {
+    if (!c || !rho || !hr) return fail(c, SCGPU_ERR_ARG, "null argument");
+    for (int d = 0; d < 3; ++d)
+        if (!(hr[d] > 0.0) || !std::isfinite(hr[d])) return fail(c, SCGPU_ERR_ARG, "hr must be positive and finite");
+    CK(cudaSetDevice(c->device));
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    const long long M = (long long)b.bc.n[0] * b.bc.n[1] * b.bc.n[2];
+    const cudaMemcpyKind in_kind = device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out_kind = device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CK(cudaMemcpyAsync(b.st->hr_scaled, hr, 3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (b.precision == SCGPU_PLAIN_FP64) {
+        CK(cudaMemcpyAsync(b.rho, rho, M * sizeof(double), in_kind, s));
+    } else {
+        double* stage = c->capacity * 3 >= M ? b.Ef : nullptr;
+        bool tmp_alloc = false;
+        if (!stage) {
+            CK(cudaMalloc(&stage, M * sizeof(double)));
+            tmp_alloc = true;
+        }
+        CK(cudaMemcpyAsync(stage, rho, M * sizeof(double), in_kind, s));
+        launch_f64_to_f32(stage, (float*)b.rho, M, s);
+        if (tmp_alloc) {
+            CK(cudaStreamSynchronize(s));
+            cudaFree(stage);
+        }
+    }
+    enqueue_green(c, s);
+    launch_convolution(b, kConvPotential, s);
+    if (b.precision == SCGPU_PLAIN_FP64) {
+        CK(cudaMemcpyAsync(rho, b.phi, M * sizeof(double), out_kind, s));
+    } else {
+        double* stage = nullptr;
+        CK(cudaMalloc(&stage, M * sizeof(double)));
+        launch_f32_to_f64((const float*)b.phi, stage, M, s);
+        CK(cudaMemcpyAsync(rho, stage, M * sizeof(double), out_kind, s));
+        CK(cudaStreamSynchronize(s));
+        cudaFree(stage);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    c->have_solve = false;
+    return SCGPU_OK;
+}
+
+int scgpu_compute_potential(scgpu_ctx* c, double* rho, const double hr[3]) { return compute_potential_impl(c, rho, hr, false); }
+
+int scgpu_compute_potential_device(scgpu_ctx* c, double* rho, const double hr[3]) {
+    return compute_potential_impl(c, rho, hr, true);
+}
+
+int scgpu_compute_self_fields(scgpu_ctx* c, long long n, const double* R, const double* P, double* q_macro, double dT,
+                              double* Ef, double* Bf) {
+    if (!c || !R || !P || !q_macro || !Ef || !Bf) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!(dT > 0.0)) return fail(c, SCGPU_ERR_ARG, "dT must be positive");
+    CK(cudaSetDevice(c->device));
+    int rc = ensure_particles(c, n);
+    if (rc) return rc;
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    b.bc.dT = dT;
+    if (b.bc.coupling == 0.0) b.bc.coupling = 1.0 / (4 * kPi * 8.854187817e-12);
+    CK(cudaMemcpyAsync(b.Ef, R, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(b.Bf, P, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_aos_to_soa(b.Ef, b.x, b.y, b.z, n, s);
+    launch_aos_to_soa(b.Bf, b.px, b.py, b.pz, n, s);
+    CK(cudaMemcpyAsync(&b.st->Q, q_macro, sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(b.stamp, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(uint32_t), s));
+    CK(cudaMemsetAsync(&b.st->gen, 0, sizeof(unsigned), s));
+    launch_reduce_state(b, false, s);
+    STAGE("reduce_state");
+    launch_drift_to_beam(b, false, false, s);
+    STAGE("bounds");
+    enqueue_green(c, s);
+    STAGE("green");
+    launch_cell_keys(b, c->digit_bits, s);
+    STAGE("cell_keys");
+    launch_sort(b, s);
+    STAGE("sort");
+    launch_deposit(b, s);
+    STAGE("deposit");
+    launch_assemble_rho(b, s);
+    STAGE("assemble");
+    launch_convolution(b, kConvSelfField, s);
+    STAGE("convolution");
+    launch_grad(b, s);
+    STAGE("grad");
+    launch_gather_fields(b, s);
+    STAGE("gather");
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(Ef, b.Ef, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(Bf, b.Bf, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(q_macro, &b.st->Q, sizeof(double), cudaMemcpyDeviceToHost, s));
+    rc = check_device_err(c);
+    c->have_bunch = false;  // the particle buffers now hold a beam-frame bunch
+    c->have_solve = (rc == SCGPU_OK);
+    return rc;
+}
+
+int scgpu_bunch_upload(scgpu_ctx* c, long long n, const double* R, const double* P, const scgpu_bunch_params* bp) {
+    if (!c || !R || !P || !bp) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!(bp->dT > 0.0) || !(bp->mass > 0.0)) return fail(c, SCGPU_ERR_ARG, "dT and mass must be positive");
+    CK(cudaSetDevice(c->device));
+    int rc = ensure_particles(c, n);
+    if (rc) return rc;
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    const bool consts_changed = b.bc.dT != bp->dT || b.bc.mass != bp->mass || b.bc.charge != bp->charge ||
+                                b.bc.coupling != bp->coupling || b.bc.bz_ext != bp->bz_ext;
+    if (consts_changed) drop_graphs(c);
+    b.bc.dT = bp->dT;
+    b.bc.mass = bp->mass;
+    b.bc.charge = bp->charge;
+    b.bc.coupling = bp->coupling;
+    b.bc.bz_ext = bp->bz_ext;
+    StepState h{};
+    h.t = bp->t;
+    h.path_length = bp->path_length;
+    for (int k = 0; k < 3; ++k) {
+        h.ref_R[k] = bp->ref_R[k];
+        h.ref_P[k] = bp->ref_P[k];
+    }
+    const double o[3] = {0.0, 0.0, 0.0}, q[4] = {1.0, 0.0, 0.0, 0.0};
+    trafo_make(h.ref_to_lab, o, q);
+    h.Q = bp->q_macro;
+    h.step = 0;
+    h.gen = 0;
+    CK(cudaMemcpyAsync(b.st, &h, sizeof(StepState), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(b.stamp, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(uint32_t), s));
+    CK(cudaMemcpyAsync(b.Ef, R, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(b.Bf, P, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_aos_to_soa(b.Ef, b.x, b.y, b.z, n, s);
+    launch_aos_to_soa(b.Bf, b.px, b.py, b.pz, n, s);
+    launch_reduce_state(b, true, s);
+    CK(cudaGetLastError());
+    rc = check_device_err(c);
+    c->have_bunch = (rc == SCGPU_OK);
+    return rc;
+}
+
+int scgpu_bunch_download(scgpu_ctx* c, double* R, double* P) {
+    if (!c || !R || !P) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    CK(cudaSetDevice(c->device));
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    const long long n = c->n;
+    launch_soa_to_aos(b.x, b.y, b.z, b.Ef, n, s);
+    launch_soa_to_aos(b.px, b.py, b.pz, b.Bf, n, s);
+    CK(cudaMemcpyAsync(R, b.Ef, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(P, b.Bf, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return SCGPU_OK;
+}
+
+int scgpu_track(scgpu_ctx* c, int nsteps, double* stats) {
+    if (!c || nsteps < 0) return fail(c, SCGPU_ERR_ARG, "bad argument");
+    if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    CK(cudaSetDevice(c->device));
+    const bool want = stats != nullptr;
+    cudaGraphExec_t* gx = want ? &c->g_step_stats : &c->g_step;
+    if (c->use_graphs && !*gx) {
+        int rc = build_graph(c, want, gx);
+        if (rc) return rc;
+    }
+    cudaStream_t s = c->stream;
+    CK(cudaEventRecord(c->ev_t0, s));
+    for (int k = 0; k < nsteps; ++k) {
+        if (c->use_graphs)
+            CK(cudaGraphLaunch(*gx, s));
+        else
+            enqueue_step(c, want, s);
+        if (want)
+            CK(cudaMemcpyAsync(stats + (size_t)k * SCGPU_NSTATS, c->b.st->moments, SCGPU_NSTATS * sizeof(double),
+                               cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaEventRecord(c->ev_t1, s));
+    CK(cudaGetLastError());
+    int rc = check_device_err(c);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev_t0, c->ev_t1);
+    c->last_ms = ms;
+    c->have_solve = (rc == SCGPU_OK && nsteps > 0);
+    return rc;
+}
+
+int scgpu_get_tracker_state(scgpu_ctx* c, scgpu_tracker_state* out) {
+    if (!c || !out) return fail(c, SCGPU_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->device));
+    StepState h;
+    CK(cudaMemcpyAsync(&h, c->b.st, sizeof(StepState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out->t = h.t;
+    out->path_length = h.path_length;
+    for (int k = 0; k < 3; ++k) {
+        out->ref_R[k] = h.ref_R[k];
+        out->ref_P[k] = h.ref_P[k];
+        out->ref_to_lab_origin[k] = h.ref_to_lab.origin[k];
+    }
+    for (int k = 0; k < 4; ++k) out->ref_to_lab_quat[k] = h.ref_to_lab.quat[k];
+    out->q_macro = h.Q;
+    out->step = h.step;
+    return SCGPU_OK;
+}
+
+int scgpu_beam_parameters(scgpu_ctx* c, scgpu_beam_params* out) {
+    if (!c || !out) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    CK(cudaSetDevice(c->device));
+    launch_reduce_stats(c->b, c->stream);
+    double rec[SCGPU_NSTATS];
+    CK(cudaMemcpyAsync(rec, c->b.st->moments, sizeof(rec), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return scgpu_beam_parameters_from_stats(rec, c->n, out);
+}
+
+int scgpu_beam_parameters_from_stats(const double* rec, long long n, scgpu_beam_params* out) {
+    if (!rec || !out || n <= 0) return SCGPU_ERR_ARG;
+    std::memset(out, 0, sizeof(*out));
+    beam_params_from_sums(rec, rec[27], (double)n, out);
+    return SCGPU_OK;
+}
+
+int scgpu_get_field(scgpu_ctx* c, int which, double* out) {
+    if (!c || !out) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!c->have_solve) return fail(c, SCGPU_ERR_STATE, "no self-field solve has run");
+    CK(cudaSetDevice(c->device));
+    DevBunch& b = c->b;
+    const long long M = (long long)b.bc.n[0] * b.bc.n[1] * b.bc.n[2];
+    const bool f64 = b.precision == SCGPU_PLAIN_FP64;
+    const size_t rs = f64 ? sizeof(double) : sizeof(float);
+    if (which == SCGPU_FIELD_RHO || which == SCGPU_FIELD_PHI) {
+        const void* src = which == SCGPU_FIELD_RHO ? b.rho : b.phi;
+        std::vector<unsigned char> h(M * rs);
+        CK(cudaMemcpyAsync(h.data(), src, M * rs, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (long long i = 0; i < M; ++i)
+            out[i] = f64 ? ((const double*)h.data())[i] : (double)((const float*)h.data())[i];
+        return SCGPU_OK;
+    }
+    if (which == SCGPU_FIELD_E) {
+        std::vector<unsigned char> h(4 * M * rs);
+        CK(cudaMemcpyAsync(h.data(), b.E4, 4 * M * rs, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (long long i = 0; i < M; ++i)
+            for (int k = 0; k < 3; ++k)
+                out[3 * i + k] = f64 ? ((const double*)h.data())[4 * i + k] : (double)((const float*)h.data())[4 * i + k];
+        return SCGPU_OK;
+    }
+    return fail(c, SCGPU_ERR_ARG, "unknown field");
+}
+
+int scgpu_get_mesh(scgpu_ctx* c, scgpu_mesh* out) {
+    if (!c || !out) return fail(c, SCGPU_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->device));
+    StepState h;
+    CK(cudaMemcpyAsync(&h, c->b.st, sizeof(StepState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 3; ++k) {
+        out->hr[k] = h.hr[k];
+        out->origin[k] = h.origin[k];
+        out->rmin[k] = h.mesh_rmin[k];
+        out->rmax[k] = h.mesh_rmax[k];
+        out->hr_scaled[k] = h.hr_scaled[k];
+    }
+    out->gammaz = h.gammaz;
+    return SCGPU_OK;
+}
+
+double scgpu_last_track_ms(const scgpu_ctx* c) { return c ? c->last_ms : 0.0; }
+
+}  // extern "C"

@@ -37,6 +37,7 @@ enum : int {
     kFlagMesh = 1,
     kFlagGuard = 2,
     kFlagFrame = 4,
+    kFlagSort = 8,  // a sort position fell outside [0, N): inconsistent histogram
 };
 
 struct Trafo {

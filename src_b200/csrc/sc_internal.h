@@ -74,9 +74,15 @@ void launch_igf(const DevBunch& b, const double* hr_host, cudaStream_t s);
 void launch_grad(const DevBunch& b, cudaStream_t s);
 void launch_gather_kick_push(const DevBunch& b, bool stats, cudaStream_t s);
 void launch_gather_fields(const DevBunch& b, cudaStream_t s);
+void launch_reduce_stats(const DevBunch& b, cudaStream_t s);
+void launch_aos_to_soa(const double* aos, double* a, double* b, double* c, long long n, cudaStream_t s);
+void launch_soa_to_aos(const double* a, const double* b, const double* c, double* aos, long long n, cudaStream_t s);
+void launch_f64_to_f32(const double* in, float* out, long long n, cudaStream_t s);
+void launch_f32_to_f64(const float* in, double* out, long long n, cudaStream_t s);
 
 // sort TU (sc_sort.cu)
 int sort_tile_elems();
+int sort_digit_bits(int key_bits);
 void launch_sort(const DevBunch& b, cudaStream_t s);
 
 // FFT TU (sc_fft.cu)
@@ -84,6 +90,7 @@ void launch_green_transform(const DevBunch& b, cudaStream_t s);
 void launch_convolution(const DevBunch& b, int mode, cudaStream_t s);
 size_t fft_smem_bytes(const DevBunch& b);
 void upload_twiddles(DevBunch& b, cudaStream_t s);
+void fft_set_smem_limits();
 
 // convolution modes
 enum : int {

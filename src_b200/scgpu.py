@@ -1,0 +1,237 @@
+"""ctypes binding of the C ABI in include/scgpu.h (libscgpu.so, sm_100a).
+
+The names follow the reference's call surface: ``FFTPoissonSolver``
+(PoissonSolver::computePotential), ``PartBunch`` (computeSelfFields,
+calcBeamParameters) and ``ParallelTTracker`` (the step loop).  There is no
+CPU fallback: importing works anywhere, but creating a solver needs the
+built library and a CUDA device, and fails loudly otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libscgpu.so")
+
+PLAIN_FP64 = 0
+MIXED = 1
+NSTATS = 28
+FIELD_RHO, FIELD_PHI, FIELD_E = 0, 1, 2
+
+ERRORS = {
+    -1: "SCGPU_ERR_ARG", -2: "SCGPU_ERR_OOM", -3: "SCGPU_ERR_MESH", -4: "SCGPU_ERR_GUARD",
+    -5: "SCGPU_ERR_FRAME", -6: "SCGPU_ERR_CUDA", -7: "SCGPU_ERR_STATE", -8: "SCGPU_ERR_UNSUPPORTED",
+}
+
+_dp = C.POINTER(C.c_double)
+
+
+class SolverParams(C.Structure):
+    _fields_ = [("mx", C.c_int), ("my", C.c_int), ("mt", C.c_int), ("precision", C.c_int), ("bboxincr", C.c_double)]
+
+
+class BunchParams(C.Structure):
+    _fields_ = [("dT", C.c_double), ("mass", C.c_double), ("charge", C.c_double), ("q_macro", C.c_double),
+                ("coupling", C.c_double), ("bz_ext", C.c_double), ("t", C.c_double), ("path_length", C.c_double),
+                ("ref_R", C.c_double * 3), ("ref_P", C.c_double * 3)]
+
+
+class TrackerState(C.Structure):
+    _fields_ = [("t", C.c_double), ("path_length", C.c_double), ("ref_R", C.c_double * 3), ("ref_P", C.c_double * 3),
+                ("q_macro", C.c_double), ("ref_to_lab_origin", C.c_double * 3), ("ref_to_lab_quat", C.c_double * 4),
+                ("step", C.c_longlong)]
+
+
+class BeamParams(C.Structure):
+    _fields_ = [(name, C.c_double * 3) for name in ("rmean", "pmean", "rrms", "prms", "eps_norm", "eps", "rprms")] + \
+               [("gamma", C.c_double), ("moments", C.c_double * 27)]
+
+    def as_dict(self):
+        out = {name: np.array(getattr(self, name)) for name, _ in self._fields_ if name != "gamma"}
+        out["gamma"] = float(self.gamma)
+        return out
+
+
+class Mesh(C.Structure):
+    _fields_ = [("hr", C.c_double * 3), ("origin", C.c_double * 3), ("rmin", C.c_double * 3),
+                ("rmax", C.c_double * 3), ("gammaz", C.c_double), ("hr_scaled", C.c_double * 3)]
+
+
+class ScgpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libscgpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C src_b200/csrc` "
+                               "(or __graft_entry__.build()); there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        L.scgpu_last_error.restype = C.c_char_p
+        L.scgpu_last_track_ms.restype = C.c_double
+        L.scgpu_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(SolverParams), C.c_int]
+        for name in ("scgpu_destroy", "scgpu_last_error", "scgpu_synchronize", "scgpu_last_track_ms"):
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.scgpu_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+        L.scgpu_compute_potential.argtypes = [C.c_void_p, _dp, _dp]
+        L.scgpu_compute_potential_device.argtypes = [C.c_void_p, C.c_void_p, _dp]
+        L.scgpu_compute_self_fields.argtypes = [C.c_void_p, C.c_longlong, _dp, _dp, _dp, C.c_double, _dp, _dp]
+        L.scgpu_register_host.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong]
+        L.scgpu_unregister_host.argtypes = [C.c_void_p, C.c_void_p]
+        L.scgpu_bunch_upload.argtypes = [C.c_void_p, C.c_longlong, _dp, _dp, C.POINTER(BunchParams)]
+        L.scgpu_bunch_download.argtypes = [C.c_void_p, _dp, _dp]
+        L.scgpu_track.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.scgpu_get_tracker_state.argtypes = [C.c_void_p, C.POINTER(TrackerState)]
+        L.scgpu_beam_parameters.argtypes = [C.c_void_p, C.POINTER(BeamParams)]
+        L.scgpu_beam_parameters_from_stats.argtypes = [_dp, C.c_longlong, C.POINTER(BeamParams)]
+        L.scgpu_get_field.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.scgpu_get_mesh.argtypes = [C.c_void_p, C.POINTER(Mesh)]
+        _lib = L
+    return _lib
+
+
+EXPORTED = [
+    "scgpu_abi_version", "scgpu_create", "scgpu_destroy", "scgpu_last_error", "scgpu_set_stream",
+    "scgpu_synchronize", "scgpu_compute_potential", "scgpu_compute_potential_device",
+    "scgpu_compute_self_fields", "scgpu_register_host", "scgpu_unregister_host", "scgpu_bunch_upload",
+    "scgpu_bunch_download", "scgpu_track", "scgpu_get_tracker_state", "scgpu_beam_parameters",
+    "scgpu_beam_parameters_from_stats", "scgpu_get_field", "scgpu_get_mesh", "scgpu_last_track_ms",
+]
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _f64c(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+class Context:
+    """One solver instance on one device (FieldSolver + FFTPoissonSolver)."""
+
+    def __init__(self, nr, precision=PLAIN_FP64, bboxincr=2.0, device=0):
+        self.nr = tuple(int(v) for v in nr)
+        self.precision = precision
+        sp = SolverParams(self.nr[0], self.nr[1], self.nr[2], precision, float(bboxincr))
+        h = C.c_void_p()
+        rc = lib().scgpu_create(C.byref(h), C.byref(sp), int(device))
+        if rc != 0:
+            raise ScgpuError(rc, f"scgpu_create(nr={self.nr}, precision={precision}) failed")
+        self.h = h
+        self.n = 0
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = lib().scgpu_last_error(self.h)
+            raise ScgpuError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().scgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- PoissonSolver::computePotential
+    def compute_potential(self, rho, hr):
+        """rho: array [nz, ny, nx] (x fastest).  Returns the convolution."""
+        r = _f64c(rho).copy()
+        assert r.shape == (self.nr[2], self.nr[1], self.nr[0])
+        self._check(lib().scgpu_compute_potential(self.h, _p(r), (C.c_double * 3)(*hr)), "compute_potential")
+        return r
+
+    # ---- PartBunch::computeSelfFields
+    def compute_self_fields(self, R, P, q_macro, dT):
+        R = _f64c(R)
+        P = _f64c(P)
+        n = R.shape[0]
+        Ef = np.empty_like(R)
+        Bf = np.empty_like(R)
+        q = C.c_double(q_macro)
+        self._check(lib().scgpu_compute_self_fields(self.h, n, _p(R), _p(P), C.byref(q), float(dT), _p(Ef), _p(Bf)),
+                    "compute_self_fields")
+        return Ef, Bf, q.value
+
+    # ---- bunch state
+    def upload(self, R, P, dT, q_macro, mass, charge=-1.0, coupling=None, bz_ext=0.0, t=0.0, path_length=0.0,
+               ref_R=(0.0, 0.0, 0.0), ref_P=(0.0, 0.0, 10.0)):
+        R = _f64c(R)
+        P = _f64c(P)
+        if coupling is None:
+            coupling = 1.0 / (4 * 3.14159265358979323846 * 8.854187817e-12)
+        bp = BunchParams(dT, mass, charge, q_macro, coupling, bz_ext, t, path_length, (C.c_double * 3)(*ref_R),
+                         (C.c_double * 3)(*ref_P))
+        self._check(lib().scgpu_bunch_upload(self.h, R.shape[0], _p(R), _p(P), C.byref(bp)), "bunch_upload")
+        self.n = R.shape[0]
+
+    def download(self):
+        R = np.empty((self.n, 3))
+        P = np.empty((self.n, 3))
+        self._check(lib().scgpu_bunch_download(self.h, _p(R), _p(P)), "bunch_download")
+        return R, P
+
+    def track(self, nsteps, stats=None):
+        """stats: optional float64 array [nsteps, NSTATS] (pinned for best overlap)."""
+        sp = None
+        if stats is not None:
+            assert stats.dtype == np.float64 and stats.flags.c_contiguous and stats.size >= nsteps * NSTATS
+            sp = _p(stats)
+        self._check(lib().scgpu_track(self.h, int(nsteps), sp), "track")
+        return lib().scgpu_last_track_ms(self.h)
+
+    def tracker_state(self):
+        s = TrackerState()
+        self._check(lib().scgpu_get_tracker_state(self.h, C.byref(s)), "get_tracker_state")
+        return {"t": s.t, "path_length": s.path_length, "ref_R": np.array(s.ref_R), "ref_P": np.array(s.ref_P),
+                "q_macro": s.q_macro, "step": s.step, "ref_to_lab_origin": np.array(s.ref_to_lab_origin),
+                "ref_to_lab_quat": np.array(s.ref_to_lab_quat)}
+
+    def beam_parameters(self):
+        bp = BeamParams()
+        self._check(lib().scgpu_beam_parameters(self.h, C.byref(bp)), "beam_parameters")
+        return bp.as_dict()
+
+    def field(self, which):
+        nx, ny, nz = self.nr
+        out = np.empty((nz, ny, nx, 3) if which == FIELD_E else (nz, ny, nx))
+        self._check(lib().scgpu_get_field(self.h, which, _p(out)), "get_field")
+        return out
+
+    def mesh(self):
+        m = Mesh()
+        self._check(lib().scgpu_get_mesh(self.h, C.byref(m)), "get_mesh")
+        return {"hr": np.array(m.hr), "origin": np.array(m.origin), "rmin": np.array(m.rmin),
+                "rmax": np.array(m.rmax), "gammaz": m.gammaz, "hr_scaled": np.array(m.hr_scaled)}
+
+
+def beam_parameters_from_stats(record, n):
+    bp = BeamParams()
+    rec = _f64c(record)
+    rc = lib().scgpu_beam_parameters_from_stats(_p(rec), int(n), C.byref(bp))
+    if rc != 0:
+        raise ScgpuError(rc, "beam_parameters_from_stats")
+    return bp.as_dict()

@@ -1,0 +1,71 @@
+"""Generate the golden fixtures in tests/golden/ (run in a tree that has the
+reference sources, after `make -C oracle`).
+
+fftpack_kat.npz
+    Inputs and outputs of the reference's own FFTPACK (ippl/src/FFT/fftpack.cpp,
+    compiled from source into oracle/_ref/libfftpack_ref.so): cfftf, cfftb,
+    rfftf, rfftb at the doubled-grid lengths of the supported meshes.  The
+    oracle's project-written FFT engine is checked against these.
+convolution_n8.npz
+    rho, hr and the open-boundary convolution of FFTPoissonSolver::computePotential
+    computed by the oracle with the reference's FFTPACK engine, plus the
+    mirrored integrated Green's function G2 (n = 8, non-cubic spacing).
+step_n8.npz
+    A 2000-particle bunch tracked 3 steps on an 8^3 mesh by the oracle with the
+    reference's FFTPACK engine: final R, P and the last step's rho, phi, E.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from src_b200.bunch import gaussian_bunch  # noqa: E402
+
+LENGTHS = (16, 32, 48, 64, 96, 128, 256)
+
+
+def main():
+    O.build()
+    if not O.reference_fft_available():
+        raise SystemExit("oracle/_ref/libfftpack_ref.so is missing: the reference tree is needed")
+    O.use_reference_fft(True)
+    rng = np.random.default_rng(20261203)
+    kat = {}
+    for n in LENGTHS:
+        c = rng.standard_normal(2 * n)
+        r = rng.standard_normal(n)
+        kat[f"c_in_{n}"] = c
+        kat[f"r_in_{n}"] = r
+        kat[f"cfftf_{n}"] = O.fft1d(0, c)
+        kat[f"cfftb_{n}"] = O.fft1d(1, c)
+        kat[f"rfftf_{n}"] = O.fft1d(2, r)
+        kat[f"rfftb_{n}"] = O.fft1d(3, r)
+    np.savez_compressed(os.path.join(HERE, "fftpack_kat.npz"), **kat)
+
+    nr = (8, 8, 8)
+    hr = (2.5e-4, 3.0e-4, 4.0e-3)
+    rho = rng.standard_normal((nr[2], nr[1], nr[0]))
+    phi = O.compute_potential(rho, hr)
+    G2 = O.igf(nr, hr)
+    np.savez_compressed(os.path.join(HERE, "convolution_n8.npz"), rho=rho, hr=np.array(hr), phi=phi, G2=G2)
+
+    R, P = gaussian_bunch(2000, bunch_id=7)
+    R0, P0 = R.copy(), P.copy()
+    prm = O.make_params(nr, 1e-12)
+    tr = O.OracleTracker(prm, -1e-9 / 2000)
+    dbg = tr.track(R, P, 3, want_debug=True)
+    np.savez_compressed(os.path.join(HERE, "step_n8.npz"), R0=R0, P0=P0, R=R, P=P, rho=dbg["rho"], phi=dbg["phi"],
+                        E=dbg["E"], Q=tr.Q, path_length=tr.path_length, t=tr.t)
+    O.use_reference_fft(False)
+    print("wrote fftpack_kat.npz, convolution_n8.npz, step_n8.npz")
+
+
+if __name__ == "__main__":
+    main()
