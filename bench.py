@@ -1,0 +1,368 @@
+"""Benchmark of the space-charge tracking step (one JSON line on stdout).
+
+Workload (default): one Gaussian electron bunch of 1,000,000 macro-particles
+on a 64^3 mesh (128^3 doubled grid), 1 nC, dt = 1 ps, plain FP64 form --
+the single-GPU configuration the reference metric is quoted on.  A "step" is
+one ParallelTTracker step: half drift, space-charge fields (deposit, Hockney
+FFT convolution with the integrated Green's function, gather), Boris kick,
+half drift, reference-frame update.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--precision fp64|mixed]
+
+value    particle-steps/s, device time (CUDA events) of K steps, the bunch
+         resident in HBM; L2 flushed before every timed step.
+e2e      the same metric through the C ABI with host buffers: every step
+         uploads R, P from pinned host memory, runs scgpu_track(1) and
+         downloads R, P (the DKS offload seam of the reference,
+         ParallelTTracker.h:514-562).
+Multi-GPU: independent replicas (one bunch per rank); no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_PARTICLES = 1_000_000
+MESH = 64
+DT = 1e-12
+WORKLOAD = "gaussian bunch 1e6 e-, 64^3 mesh (128^3 doubled), 1 nC, dt 1 ps, drift"
+
+
+def algorithmic_bytes(N, n, precision):
+    """Per-step algorithmic HBM bytes of the whole step and of each phase.
+    FP64 step model: 96 N + 32 M + 48 S + 16 G3 (M = n^3, S = (n+1)(2n)^2,
+    G3 = (n+1)^3); mixed halves the grid terms except the FP64 G build."""
+    M = n ** 3
+    S = (n + 1) * (2 * n) ** 2
+    G3 = (n + 1) ** 3
+    r = 8 if precision == "fp64" else 4
+    step = 96 * N + 4 * r * M + 6 * r * S + 16 * G3
+    phases = {
+        "drift_bounds": 72 * N,                    # read R, P; write R (beam frame)
+        "cell_keys": 28 * N,                       # read R; write 32-bit key
+        "sort": 32 * N,                            # 2 radix passes over (key, index)
+        "deposit": 32 * N,                         # sorted (key, index), gathered R
+        "assemble_rho": r * M,                     # write rho
+        "green": 16 * G3,                          # G write + read
+        "convolution": 2 * r * M + 6 * r * S,      # rho in, phi out, spectrum traffic
+        "grad": r * M + 3 * r * M,                 # phi in, 3-component E out
+        "gather_kick_push": 96 * N + 3 * r * M,    # R, P in and out; E read
+    }
+    return step, phases
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel):
+    """DRAM bytes per launch of a kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    v = t.get(kernel)
+    return None if v is None else float(v)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = str(device_index)
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9 or parts[0] != self.idx:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU path (the oracle restatement with the reference's own
+    FFTPACK engine), all host threads, on the same workload."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from src_b200.bunch import config_bunch
+
+    threads = O.lib().sco_max_threads()
+    O.lib().sco_set_threads(threads)
+    if O.reference_fft_available():
+        O.use_reference_fft(True)
+    b = config_bunch("c2")
+    tr = O.OracleTracker(O.make_params(b["nr"], b["dT"]), b["Q"])
+    R, P = b["R"].copy(), b["P"].copy()
+    t0 = time.perf_counter()
+    tr.track(R, P, args.warmup)
+    per_step = (time.perf_counter() - t0) / args.warmup
+    # bound the run to about two minutes of host time
+    timed = max(1, min(args.steps, int(120.0 / max(per_step, 1e-6))))
+    t0 = time.perf_counter()
+    tr.track(R, P, timed)
+    el = time.perf_counter() - t0
+    value = b["N"] * timed / el
+    sample = (f"{timed} of {args.steps} requested full tracking steps of the 1e6-particle / 64^3 workload, "
+              f"{threads} host threads ({'reference FFTPACK' if not O.fft_engine_is_own() else 'oracle FFT'} engine)")
+    el = el * args.steps / timed
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": b["N"], "mesh": MESH, "precision": "fp64",
+                   "l2": "n/a (host)"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_single(target_s=12.0):
+    """Oracle port, 1 thread, bounded sample of the same workload."""
+    from oracle import oracle as O
+    from src_b200.bunch import config_bunch
+
+    O.lib().sco_set_threads(1)
+    if O.reference_fft_available():
+        O.use_reference_fft(True)
+    b = config_bunch("c2")
+    tr = O.OracleTracker(O.make_params(b["nr"], b["dT"]), b["Q"])
+    R, P = b["R"].copy(), b["P"].copy()
+    t0 = time.perf_counter()
+    tr.track(R, P, 1)
+    one = time.perf_counter() - t0
+    steps = max(1, int(target_s / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    tr.track(R, P, steps)
+    el = time.perf_counter() - t0
+    return {"value": b["N"] * steps / el, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} full tracking steps of the 1e6-particle / 64^3 workload on 1 core "
+                      f"({'reference FFTPACK' if not O.fft_engine_is_own() else 'oracle FFT'} engine)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from src_b200 import scgpu
+    from src_b200.bunch import gaussian_bunch
+
+    prec = scgpu.PLAIN_FP64 if args.precision == "fp64" else scgpu.MIXED
+    R, P = gaussian_bunch(N_PARTICLES, bunch_id=rank)
+    Q = -1e-9 / N_PARTICLES
+    mass = 0.51099892e-03 * 1.0e9
+    ctx = scgpu.Context((MESH, MESH, MESH), precision=prec, device=local)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload(R, P, DT, Q, mass)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    # warm-up (also builds the step's CUDA graph)
+    ctx.track(args.warmup)
+    kernels = ctx.kernels_per_step()
+    torch.cuda.synchronize(dev)
+
+    # ---- timed region: K steps, device time, L2 flushed before each step
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        ctx.track(1)
+        ends[k].record(stream)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * N_PARTICLES * args.steps / (ms_max * 1e-3)
+
+    # ---- per-phase device times (serialised phases), the dominant kernel's roofline
+    nprof = min(max(args.steps // 10, 20), 200)
+    phases = ctx.profile(nprof)
+    step_bytes, phase_bytes = algorithmic_bytes(N_PARTICLES, MESH, args.precision)
+    peak, peak_kind = measured_peaks()
+    dom = max(phases, key=phases.get)
+    dom_ms = phases[dom] / nprof
+    achieved = phase_bytes[dom] / (dom_ms * 1e-3) / 1e9
+    traffic = committed_traffic(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "algorithmic_bytes": phase_bytes[dom], "avg_launch_ms": dom_ms}
+    step_ms = ms_max / args.steps
+    step_roofline = {"achieved": step_bytes / (step_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak, "algorithmic_bytes": step_bytes}
+
+    # ---- e2e through the C ABI with host buffers (per-step offload)
+    e2e_steps = max(5, min(args.steps // 20, 50))
+    Rh = torch.empty((N_PARTICLES, 3), dtype=torch.float64, pin_memory=True).numpy()
+    Ph = torch.empty((N_PARTICLES, 3), dtype=torch.float64, pin_memory=True).numpy()
+    Rh[:] = R
+    Ph[:] = P
+    st = ctx.tracker_state()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        ctx.upload(Rh, Ph, DT, Q, mass, t=st["t"], path_length=st["path_length"], ref_R=st["ref_R"],
+                   ref_P=st["ref_P"])
+        ctx.track(1)
+        ctx.download(Rh, Ph)
+        st = ctx.tracker_state()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * N_PARTICLES * e2e_steps / (float(t.item()) * 1e-3)
+
+    # ---- e2e of a resident tracking job: upload once, per-step statistics
+    # records to pinned host memory, download at the end
+    job_steps = max(10, min(args.steps // 5, 200))
+    stats = torch.empty((job_steps, scgpu.NSTATS), dtype=torch.float64, pin_memory=True).numpy()
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    ctx.upload(Rh, Ph, DT, Q, mass)
+    ctx.track(job_steps, stats)
+    ctx.download(Rh, Ph)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    job_value = N_PARTICLES * job_steps / (e0.elapsed_time(e1) * 1e-3)
+
+    ctx.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_single()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": N_PARTICLES * world, "particles_per_gpu": N_PARTICLES,
+                   "mesh": MESH, "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "l2": "flushed before every timed step (256 MiB write)"},
+        "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 48 * N_PARTICLES,
+                "d2h_bytes_per_step": 48 * N_PARTICLES + 8 * 13, "steps": e2e_steps,
+                "mode": "per-step upload / scgpu_track(1) / download of R, P (pinned host)"},
+        "e2e_resident_job": {"value": job_value, "unit": "particle-steps/s", "steps": job_steps,
+                             "h2d_bytes_per_step": 48 * N_PARTICLES / job_steps,
+                             "d2h_bytes_per_step": 8 * scgpu.NSTATS + 48 * N_PARTICLES / job_steps},
+        "roofline": roofline,
+        "step_roofline": step_roofline,
+        "phases_ms_per_step": {k: v / nprof for k, v in phases.items()},
+        "gpu_launches": kernels * args.steps,
+        "kernels_per_step": kernels,
+        "clocks": clk,
+        "wall_s_timed_region": wall,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

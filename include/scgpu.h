@@ -171,6 +171,26 @@ int scgpu_get_mesh(scgpu_ctx* ctx, scgpu_mesh* out);
 /* device-side elapsed time of the last scgpu_track call [ms] */
 double scgpu_last_track_ms(const scgpu_ctx* ctx);
 
+/* Per-phase device timers, the counterpart of the reference's IpplTimings
+ * ("SelfField total", "SF: GreensFTotal", "ComputePotential",
+ * "TIntegration1/2", "Boundingbox"; ippl/src/Utility/IpplTimings.h:172-215,
+ * PartBunchBase.hpp:2393-2397, FFTPoissonSolver.cpp:65-66).  Runs nsteps
+ * tracking steps with the phases serialised on one stream and CUDA events
+ * between them; phase_ms[SCGPU_NPHASES] receives the summed milliseconds. */
+#define SCGPU_NPHASES 9
+#define SCGPU_PHASE_DRIFT_BOUNDS 0   /* half drift, beam frame, bounds, mesh */
+#define SCGPU_PHASE_CELL_KEYS 1
+#define SCGPU_PHASE_SORT 2
+#define SCGPU_PHASE_DEPOSIT 3        /* segmented reduction + cell joins */
+#define SCGPU_PHASE_ASSEMBLE 4       /* corner sums -> rho */
+#define SCGPU_PHASE_GREEN 5          /* integrated Green's function + its spectrum */
+#define SCGPU_PHASE_CONVOLUTION 6    /* pruned FFT convolution */
+#define SCGPU_PHASE_GRAD 7
+#define SCGPU_PHASE_GATHER_KICK 8    /* gather, frames, kick, drift, reference update */
+int scgpu_profile_track(scgpu_ctx* ctx, int nsteps, double* phase_ms);
+/* number of kernels one tracking step launches (from the step's CUDA graph) */
+int scgpu_kernels_per_step(scgpu_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif

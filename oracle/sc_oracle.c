@@ -54,6 +54,23 @@
 #define SCO_C 299792458.0
 #define SCO_EPS0 8.854187817e-12
 
+/* Host threads for the timed multi-core baseline (1 = the sequential
+ * restatement).  With more threads, particle loops, FFT strips and the
+ * Green's function run in parallel; the deposit goes to per-thread grids
+ * merged in thread order and sums are combined in thread order, so a run is
+ * reproducible for a fixed thread count. */
+static int g_threads = 1;
+#define SCO_PAR _Pragma("omp parallel for num_threads(g_threads) if(g_threads > 1) schedule(static)")
+void sco_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+int sco_get_threads(void) { return g_threads; }
+int sco_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_num_procs();
+#else
+    return 1;
+#endif
+}
+
 double sco_const_c(void) { return SCO_C; }
 double sco_const_electron_mass_ev(void) { return 0.51099892e-03 * 1.0e9; }
 double sco_const_coupling(void) { return 1.0 / (4 * SCO_PI * SCO_EPS0); }
@@ -224,11 +241,13 @@ static inline void kick_one(double* P, const double* Ef, const double* Bf, doubl
 }
 
 void sco_push(long long n, double* R, const double* P, double dt) {
+    SCO_PAR
     for (long long i = 0; i < n; ++i) push_one(R + 3 * i, P + 3 * i, dt);
 }
 
 void sco_kick(long long n, double* P, const double* Ef, const double* Bf, double dt,
               double mass, double charge) {
+    SCO_PAR
     for (long long i = 0; i < n; ++i) kick_one(P + 3 * i, Ef + 3 * i, Bf + 3 * i, dt, mass, charge);
 }
 
@@ -241,6 +260,28 @@ void sco_bounds(long long n, const double* R, double* rmin, double* rmax) {
         for (int d = 0; d < 3; ++d) rmin[d] = rmax[d] = 0.0;
         return;
     }
+    if (g_threads > 1 && n > 1) {
+        /* min / max are exact: the split does not change the result */
+        double lo[3] = {R[0], R[1], R[2]}, hi[3] = {R[0], R[1], R[2]};
+#pragma omp parallel num_threads(g_threads)
+        {
+            double tl[3] = {R[0], R[1], R[2]}, th[3] = {R[0], R[1], R[2]};
+#pragma omp for schedule(static) nowait
+            for (long long i = 1; i < n; ++i)
+                for (int d = 0; d < 3; ++d) {
+                    const double v = R[3 * i + d];
+                    if (tl[d] > v) tl[d] = v;
+                    else if (th[d] < v) th[d] = v;
+                }
+#pragma omp critical
+            for (int d = 0; d < 3; ++d) {
+                if (lo[d] > tl[d]) lo[d] = tl[d];
+                if (hi[d] < th[d]) hi[d] = th[d];
+            }
+        }
+        for (int d = 0; d < 3; ++d) { rmin[d] = lo[d]; rmax[d] = hi[d]; }
+        return;
+    }
     for (int d = 0; d < 3; ++d) rmin[d] = rmax[d] = R[d];
     for (long long i = 1; i < n; ++i)
         for (int d = 0; d < 3; ++d) {
@@ -249,11 +290,37 @@ void sco_bounds(long long n, const double* R, double* rmin, double* rmax) {
         }
 }
 
+static void moments_range(long long k0, long long k1, const double* R, const double* P, double* m27);
+
 /* 6 first moments + 21 second moments in OPAL's order (x,px,y,py,z,pz). */
 void sco_moments(long long n, const double* R, const double* P, double* m27) {
+    if (g_threads > 1) {
+        const int T = g_threads;
+        double* part = (double*)calloc((size_t)T * 27, sizeof(double));
+#pragma omp parallel num_threads(T)
+        {
+#ifdef _OPENMP
+            const int t = omp_get_thread_num();
+#else
+            const int t = 0;
+#endif
+            const long long k0 = n * t / T, k1 = n * (t + 1) / T;
+            moments_range(k0, k1, R, P, part + 27 * t);
+        }
+        for (int i = 0; i < 27; ++i) m27[i] = 0.0;
+        for (int t = 0; t < T; ++t)
+            for (int i = 0; i < 27; ++i) m27[i] += part[27 * t + i];
+        free(part);
+        return;
+    }
+    moments_range(0, n, R, P, m27);
+}
+
+static void moments_range(long long k0, long long k1, const double* R, const double* P, double* m27) {
+    const long long n = k1;
     for (int i = 0; i < 27; ++i) m27[i] = 0.0;
     double part[6];
-    for (long long k = 0; k < n; ++k) {
+    for (long long k = k0; k < n; ++k) {
         part[1] = P[3 * k + 0]; part[3] = P[3 * k + 1]; part[5] = P[3 * k + 2];
         part[0] = R[3 * k + 0]; part[2] = R[3 * k + 1]; part[4] = R[3 * k + 2];
         int l = 6;
@@ -370,10 +437,37 @@ static inline int cic_locate(const sco_mesh* m, const double* x, int* lgp, doubl
     return 0;
 }
 
+static int scatter_range(long long p0, long long p1, const double* R, double q, const sco_mesh* m, double* rho);
+
 int sco_scatter_cic(long long n, const double* R, double q, const sco_mesh* m, double* rho) {
+    if (g_threads > 1) {
+        const int T = g_threads;
+        const long long M = (long long)m->nr[0] * m->nr[1] * m->nr[2];
+        double* grids = (double*)calloc((size_t)T * M, sizeof(double));
+        int bad = 0;
+#pragma omp parallel num_threads(T) reduction(| : bad)
+        {
+#ifdef _OPENMP
+            const int t = omp_get_thread_num();
+#else
+            const int t = 0;
+#endif
+            bad |= scatter_range(n * t / T, n * (t + 1) / T, R, q, m, grids + (size_t)t * M) != 0;
+        }
+#pragma omp parallel for num_threads(T) schedule(static)
+        for (long long c = 0; c < M; ++c)
+            for (int t = 0; t < T; ++t) rho[c] += grids[(size_t)t * M + c];
+        free(grids);
+        return bad ? SCO_ERR_GUARD : 0;
+    }
+    return scatter_range(0, n, R, q, m, rho);
+}
+
+static int scatter_range(long long p0, long long p1, const double* R, double q, const sco_mesh* m, double* rho) {
     const long long nx = m->nr[0], nxy = (long long)m->nr[0] * m->nr[1];
+    const long long n = p1;
     int bad = 0;
-    for (long long p = 0; p < n; ++p) {
+    for (long long p = p0; p < n; ++p) {
         int l[3];
         double d[3];
         if (cic_locate(m, R + 3 * p, l, d)) { bad = 1; continue; }
@@ -394,6 +488,7 @@ int sco_scatter_cic(long long n, const double* R, double q, const sco_mesh* m, d
 int sco_gather_cic(long long n, const double* R, const sco_mesh* m, const double* E, double* Ef) {
     const long long nx = m->nr[0], nxy = (long long)m->nr[0] * m->nr[1];
     int bad = 0;
+#pragma omp parallel for num_threads(g_threads) if(g_threads > 1) schedule(static) reduction(| : bad)
     for (long long p = 0; p < n; ++p) {
         int l[3];
         double d[3];
@@ -571,107 +666,109 @@ void sco_fft1d(int kind, long long n, double* data) {
 /* Inverse: backward complex along z and y, then complex-to-real along x,     */
 /* then multiply by normFact = 1/L0/L1/L2 (FFT.hpp:726-732, :1706).           */
 /* ------------------------------------------------------------------------ */
+typedef struct {
+    double *wr, *w1, *w2, *strip;
+} fft_ws;
+
+static void fft_ws_init(fft_ws* w, long long L0, long long L1, long long L2) {
+    w->wr = (double*)calloc(4 * L0 + 15 + 2 * L0 + 8, sizeof(double));
+    w->w1 = (double*)calloc(4 * L1 + 15 + 2 * L1 + 8, sizeof(double));
+    w->w2 = (double*)calloc(4 * L2 + 15 + 2 * L2 + 8, sizeof(double));
+    long long Lmax = L0 > L1 ? L0 : L1;
+    if (L2 > Lmax) Lmax = L2;
+    w->strip = (double*)malloc((2 * Lmax + 4) * sizeof(double));
+    g_rffti((size_t)L0, w->wr);
+    g_cffti((size_t)L1, w->w1);
+    g_cffti((size_t)L2, w->w2);
+}
+
+static void fft_ws_free(fft_ws* w) {
+    free(w->wr); free(w->w1); free(w->w2); free(w->strip);
+}
+
+/* complex transforms of the columns along y (axis 1) or z (axis 2) */
+static void fft_columns(double* spec, long long C0, long long L1, long long L2, int axis, int forward) {
+    const long long outer = axis == 1 ? L2 : L1;
+    const long long len = axis == 1 ? L1 : L2;
+    const long long stride = axis == 1 ? C0 : C0 * L1;
+#pragma omp parallel num_threads(g_threads) if(g_threads > 1)
+    {
+        fft_ws ws;
+        fft_ws_init(&ws, 2, L1, L2);
+        double* strip = ws.strip;
+        double* w = axis == 1 ? ws.w1 : ws.w2;
+#pragma omp for schedule(static)
+        for (long long o = 0; o < outer; ++o) {
+            const long long base = axis == 1 ? C0 * L1 * o : C0 * o;
+            for (long long kx = 0; kx < C0; ++kx) {
+                double* c = spec + 2 * (base + kx);
+                for (long long e = 0; e < len; ++e) {
+                    strip[2 * e] = c[2 * stride * e];
+                    strip[2 * e + 1] = c[2 * stride * e + 1];
+                }
+                if (forward) g_cfftf((size_t)len, strip, w);
+                else g_cfftb((size_t)len, strip, w);
+                for (long long e = 0; e < len; ++e) {
+                    c[2 * stride * e] = strip[2 * e];
+                    c[2 * stride * e + 1] = strip[2 * e + 1];
+                }
+            }
+        }
+        fft_ws_free(&ws);
+    }
+}
+
 void sco_fft3d_r2c(const int* L, const double* in, double* out) {
     engine_defaults();
     const long long L0 = L[0], L1 = L[1], L2 = L[2], C0 = L0 / 2 + 1;
-    double* wr = (double*)calloc(4 * L0 + 15 + 2 * L0 + 8, sizeof(double));
-    double* w1 = (double*)calloc(4 * L1 + 15 + 2 * L1 + 8, sizeof(double));
-    double* w2 = (double*)calloc(4 * L2 + 15 + 2 * L2 + 8, sizeof(double));
-    long long Lmax = L0 > L1 ? L0 : L1;
-    if (L2 > Lmax) Lmax = L2;
-    double* strip = (double*)malloc((2 * Lmax + 4) * sizeof(double));
-    g_rffti((size_t)L0, wr);
-    g_cffti((size_t)L1, w1);
-    g_cffti((size_t)L2, w2);
-    for (long long k = 0; k < L2; ++k)
-        for (long long j = 0; j < L1; ++j) {
-            memcpy(strip, in + L0 * (j + L1 * k), L0 * sizeof(double));
-            g_rfftf((size_t)L0, strip, wr);
-            double* o = out + 2 * C0 * (j + L1 * k);
+#pragma omp parallel num_threads(g_threads) if(g_threads > 1)
+    {
+        fft_ws ws;
+        fft_ws_init(&ws, L0, 2, 2);
+        double* strip = ws.strip;
+#pragma omp for schedule(static)
+        for (long long r = 0; r < L1 * L2; ++r) {
+            memcpy(strip, in + L0 * r, L0 * sizeof(double));
+            g_rfftf((size_t)L0, strip, ws.wr);
+            double* o = out + 2 * C0 * r;
             o[0] = strip[0]; o[1] = 0.0;
             for (long long m = 1; 2 * m < L0; ++m) { o[2 * m] = strip[2 * m - 1]; o[2 * m + 1] = strip[2 * m]; }
             if (L0 % 2 == 0) { o[2 * (C0 - 1)] = strip[L0 - 1]; o[2 * (C0 - 1) + 1] = 0.0; }
         }
-    for (long long k = 0; k < L2; ++k)
-        for (long long kx = 0; kx < C0; ++kx) {
-            for (long long j = 0; j < L1; ++j) {
-                strip[2 * j] = out[2 * (kx + C0 * (j + L1 * k))];
-                strip[2 * j + 1] = out[2 * (kx + C0 * (j + L1 * k)) + 1];
-            }
-            g_cfftf((size_t)L1, strip, w1);
-            for (long long j = 0; j < L1; ++j) {
-                out[2 * (kx + C0 * (j + L1 * k))] = strip[2 * j];
-                out[2 * (kx + C0 * (j + L1 * k)) + 1] = strip[2 * j + 1];
-            }
-        }
-    for (long long j = 0; j < L1; ++j)
-        for (long long kx = 0; kx < C0; ++kx) {
-            for (long long k = 0; k < L2; ++k) {
-                strip[2 * k] = out[2 * (kx + C0 * (j + L1 * k))];
-                strip[2 * k + 1] = out[2 * (kx + C0 * (j + L1 * k)) + 1];
-            }
-            g_cfftf((size_t)L2, strip, w2);
-            for (long long k = 0; k < L2; ++k) {
-                out[2 * (kx + C0 * (j + L1 * k))] = strip[2 * k];
-                out[2 * (kx + C0 * (j + L1 * k)) + 1] = strip[2 * k + 1];
-            }
-        }
-    free(wr); free(w1); free(w2); free(strip);
+        fft_ws_free(&ws);
+    }
+    fft_columns(out, C0, L1, L2, 1, 1);
+    fft_columns(out, C0, L1, L2, 2, 1);
 }
 
 /* inverse; `spec` is overwritten. `out` receives the normalised real field. */
 void sco_fft3d_c2r(const int* L, double* spec, double* out) {
     engine_defaults();
     const long long L0 = L[0], L1 = L[1], L2 = L[2], C0 = L0 / 2 + 1;
-    double* wr = (double*)calloc(4 * L0 + 15 + 2 * L0 + 8, sizeof(double));
-    double* w1 = (double*)calloc(4 * L1 + 15 + 2 * L1 + 8, sizeof(double));
-    double* w2 = (double*)calloc(4 * L2 + 15 + 2 * L2 + 8, sizeof(double));
-    long long Lmax = L0 > L1 ? L0 : L1;
-    if (L2 > Lmax) Lmax = L2;
-    double* strip = (double*)malloc((2 * Lmax + 4) * sizeof(double));
-    g_rffti((size_t)L0, wr);
-    g_cffti((size_t)L1, w1);
-    g_cffti((size_t)L2, w2);
-    for (long long j = 0; j < L1; ++j)
-        for (long long kx = 0; kx < C0; ++kx) {
-            for (long long k = 0; k < L2; ++k) {
-                strip[2 * k] = spec[2 * (kx + C0 * (j + L1 * k))];
-                strip[2 * k + 1] = spec[2 * (kx + C0 * (j + L1 * k)) + 1];
-            }
-            g_cfftb((size_t)L2, strip, w2);
-            for (long long k = 0; k < L2; ++k) {
-                spec[2 * (kx + C0 * (j + L1 * k))] = strip[2 * k];
-                spec[2 * (kx + C0 * (j + L1 * k)) + 1] = strip[2 * k + 1];
-            }
-        }
-    for (long long k = 0; k < L2; ++k)
-        for (long long kx = 0; kx < C0; ++kx) {
-            for (long long j = 0; j < L1; ++j) {
-                strip[2 * j] = spec[2 * (kx + C0 * (j + L1 * k))];
-                strip[2 * j + 1] = spec[2 * (kx + C0 * (j + L1 * k)) + 1];
-            }
-            g_cfftb((size_t)L1, strip, w1);
-            for (long long j = 0; j < L1; ++j) {
-                spec[2 * (kx + C0 * (j + L1 * k))] = strip[2 * j];
-                spec[2 * (kx + C0 * (j + L1 * k)) + 1] = strip[2 * j + 1];
-            }
-        }
+    fft_columns(spec, C0, L1, L2, 2, 0);
+    fft_columns(spec, C0, L1, L2, 1, 0);
     double normFact = 1.0;
     normFact /= L0;
     normFact /= L1;
     normFact /= L2;
-    for (long long k = 0; k < L2; ++k)
-        for (long long j = 0; j < L1; ++j) {
-            const double* c = spec + 2 * C0 * (j + L1 * k);
+#pragma omp parallel num_threads(g_threads) if(g_threads > 1)
+    {
+        fft_ws ws;
+        fft_ws_init(&ws, L0, 2, 2);
+        double* strip = ws.strip;
+#pragma omp for schedule(static)
+        for (long long r = 0; r < L1 * L2; ++r) {
+            const double* c = spec + 2 * C0 * r;
             /* netlib repack (fftpack_FFT.h:229-233) */
             strip[0] = c[0];
             for (long long m = 1; 2 * m < L0; ++m) { strip[2 * m - 1] = c[2 * m]; strip[2 * m] = c[2 * m + 1]; }
             if (L0 % 2 == 0) strip[L0 - 1] = c[2 * (C0 - 1)];
-            g_rfftb((size_t)L0, strip, wr);
-            double* o = out + L0 * (j + L1 * k);
+            g_rfftb((size_t)L0, strip, ws.wr);
+            double* o = out + L0 * r;
             for (long long i = 0; i < L0; ++i) o[i] = strip[i] * normFact;
         }
-    free(wr); free(w1); free(w2); free(strip);
+        fft_ws_free(&ws);
+    }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -698,6 +795,7 @@ void sco_igf(const int* nr, const double* hr, double* G2) {
     const long long L0 = 2 * n0, L1 = 2 * n1, L2 = 2 * n2;
     double cellVolume = hr[0] * hr[1] * hr[2];
     double* tmp = (double*)malloc(t0 * t1 * t2 * sizeof(double));
+    SCO_PAR
     for (long long k = 0; k < t2; ++k)
         for (long long j = 0; j < t1; ++j)
             for (long long i = 0; i < t0; ++i) {
@@ -708,6 +806,7 @@ void sco_igf(const int* nr, const double* hr, double* G2) {
             }
 #define TG(a, b, c) tmp[(a) + t0 * ((b) + t1 * (c))]
     memset(G2, 0, L0 * L1 * L2 * sizeof(double));
+    SCO_PAR
     for (long long k = 0; k <= n2; ++k)
         for (long long j = 0; j <= n1; ++j)
             for (long long i = 0; i <= n0; ++i) {
@@ -783,6 +882,7 @@ void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, doub
     const long long st[3] = {1, n0, n0 * n1};
     const long long nn[3] = {n0, n1, n2};
     const double sc[3] = {gammaz / 1.0, gammaz / 1.0, 1.0 / (1.0 * gammaz)};
+    SCO_PAR
     for (long long k = 0; k < n2; ++k)
         for (long long j = 0; j < n1; ++j)
             for (long long i = 0; i < n0; ++i) {
@@ -824,28 +924,39 @@ int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const
     rc = sco_scatter_cic(n, R, qdt, &mesh, rho);
     *Q = qdt / dt;
     if (rc) { free(rho); free(E); return rc; }
+    SCO_PAR
     for (long long c = 0; c < M; ++c) rho[c] /= prm->dT;
     /* gamma_z from the mean longitudinal momentum (:499-502) */
     double psum2 = 0.0;
-    for (long long i = 0; i < n; ++i) psum2 += P[3 * i + 2];
+    if (g_threads > 1) {
+        double m27[27];
+        sco_moments(n, R, P, m27); /* thread-ordered partial sums; pz sum is m27[5] */
+        psum2 = m27[5];
+    } else {
+        for (long long i = 0; i < n; ++i) psum2 += P[3 * i + 2];
+    }
     double gammaz = psum2 / (double)n;
     gammaz *= gammaz;
     gammaz = sqrt(gammaz + 1.0);
     double hr_scaled[3] = {mesh.hr[0] * 1.0, mesh.hr[1] * 1.0, mesh.hr[2] * 1.0};
     hr_scaled[2] *= gammaz;
     double tmp2 = 1 / hr_scaled[0] * 1 / hr_scaled[1] * 1 / hr_scaled[2];
+    SCO_PAR
     for (long long c = 0; c < M; ++c) rho[c] *= tmp2;
     if (dbg && dbg->rho) memcpy(dbg->rho, rho, M * sizeof(double));
     rc = sco_compute_potential(prm->nr, rho, hr_scaled);
     if (rc) { free(rho); free(E); return rc; }
     const double hvol = hr_scaled[0] * hr_scaled[1] * hr_scaled[2];
+    SCO_PAR
     for (long long c = 0; c < M; ++c) rho[c] *= hvol;
+    SCO_PAR
     for (long long c = 0; c < M; ++c) rho[c] *= prm->coupling;
     if (dbg && dbg->phi) memcpy(dbg->phi, rho, M * sizeof(double));
     sco_neg_grad_scaled(prm->nr, rho, mesh.hr, gammaz, E);
     if (dbg && dbg->E) memcpy(dbg->E, E, 3 * M * sizeof(double));
     rc = sco_gather_cic(n, R, &mesh, E, Ef);
     const double betaC = sqrt(gammaz * gammaz - 1.0) / gammaz / SCO_C;
+    SCO_PAR
     for (long long i = 0; i < n; ++i) {
         Bf[3 * i + 0] = 0.0 - betaC * Ef[3 * i + 1];
         Bf[3 * i + 1] = 0.0 + betaC * Ef[3 * i + 0];
@@ -888,6 +999,7 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
     sco_trafo_make(&b2r, org, qc);
     r2b = b2r;
     sco_trafo_invert(&r2b);
+    SCO_PAR
     for (long long i = 0; i < n; ++i) {
         double v[3];
         trafo_transform_to(&r2b, R + 3 * i, v);
@@ -895,6 +1007,7 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
     }
     int rc = sco_compute_self_fields(prm, &tr->Q, n, R, P, Ef, Bf, dbg);
     if (rc) return rc;
+    SCO_PAR
     for (long long i = 0; i < n; ++i) {
         double v[3];
         trafo_transform_to(&b2r, R + 3 * i, v);
@@ -909,8 +1022,10 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
         dbg->pmean[0] = pmean[0]; dbg->pmean[1] = pmean[1]; dbg->pmean[2] = pmean[2];
     }
     /* computeExternalFields (:356): a uniform solenoid field along z */
-    if (prm->bz_ext != 0.0)
+    if (prm->bz_ext != 0.0) {
+        SCO_PAR
         for (long long i = 0; i < n; ++i) Bf[3 * i + 2] += prm->bz_ext;
+    }
     if (dbg && dbg->Ef) memcpy(dbg->Ef, Ef, 3 * n * sizeof(double));
     if (dbg && dbg->Bf) memcpy(dbg->Bf, Bf, 3 * n * sizeof(double));
     /* timeIntegration2: kick + push (:450-491) */
@@ -942,11 +1057,13 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
         rr[0] = v[0]; rr[1] = v[1]; rr[2] = v[2];
         trafo_rotate_to(&upd, rp, v);
         rp[0] = v[0]; rp[1] = v[1]; rp[2] = v[2];
+        SCO_PAR
         for (long long i = 0; i < n; ++i) {
-            trafo_transform_to(&upd, R + 3 * i, v);
-            R[3 * i] = v[0]; R[3 * i + 1] = v[1]; R[3 * i + 2] = v[2];
-            trafo_rotate_to(&upd, P + 3 * i, v);
-            P[3 * i] = v[0]; P[3 * i + 1] = v[1]; P[3 * i + 2] = v[2];
+            double w[3];
+            trafo_transform_to(&upd, R + 3 * i, w);
+            R[3 * i] = w[0]; R[3 * i + 1] = w[1]; R[3 * i + 2] = w[2];
+            trafo_rotate_to(&upd, P + 3 * i, w);
+            P[3 * i] = w[0]; P[3 * i + 1] = w[1]; P[3 * i + 2] = w[2];
         }
         sco_trafo inv = upd;
         sco_trafo_invert(&inv);

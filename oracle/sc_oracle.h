@@ -78,6 +78,10 @@ typedef struct {
     double moments[27];
 } sco_beam_params;
 
+void sco_set_threads(int n);
+int sco_get_threads(void);
+int sco_max_threads(void);
+
 double sco_const_c(void);
 double sco_const_electron_mass_ev(void);
 double sco_const_coupling(void);

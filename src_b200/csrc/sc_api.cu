@@ -635,4 +635,73 @@ int scgpu_get_mesh(scgpu_ctx* c, scgpu_mesh* out) {
 
 double scgpu_last_track_ms(const scgpu_ctx* c) { return c ? c->last_ms : 0.0; }
 
+int scgpu_profile_track(scgpu_ctx* c, int nsteps, double* phase_ms) {
+    if (!c || nsteps < 0 || !phase_ms) return fail(c, SCGPU_ERR_ARG, "bad argument");
+    if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    CK(cudaSetDevice(c->device));
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    cudaEvent_t ev[SCGPU_NPHASES + 1];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int p = 0; p < SCGPU_NPHASES; ++p) phase_ms[p] = 0.0;
+    int rc = SCGPU_OK;
+    for (int k = 0; k < nsteps && rc == SCGPU_OK; ++k) {
+        cudaEventRecord(ev[0], s);
+        launch_drift_to_beam(b, true, true, s);
+        cudaEventRecord(ev[1], s);
+        launch_cell_keys(b, c->digit_bits, s);
+        cudaEventRecord(ev[2], s);
+        launch_sort(b, s);
+        cudaEventRecord(ev[3], s);
+        launch_deposit(b, s);
+        cudaEventRecord(ev[4], s);
+        launch_assemble_rho(b, s);
+        cudaEventRecord(ev[5], s);
+        enqueue_green(c, s);
+        cudaEventRecord(ev[6], s);
+        launch_convolution(b, kConvSelfField, s);
+        cudaEventRecord(ev[7], s);
+        launch_grad(b, s);
+        cudaEventRecord(ev[8], s);
+        launch_gather_kick_push(b, false, s);
+        cudaEventRecord(ev[9], s);
+        cudaError_t e = cudaEventSynchronize(ev[9]);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(c, e, "profile step");
+            break;
+        }
+        for (int p = 0; p < SCGPU_NPHASES; ++p) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[p], ev[p + 1]);
+            phase_ms[p] += ms;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    return check_device_err(c);
+}
+
+int scgpu_kernels_per_step(scgpu_ctx* c) {
+    if (!c) return SCGPU_ERR_ARG;
+    if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    CK(cudaSetDevice(c->device));
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c, false, c->own);
+    CK(cudaStreamEndCapture(c->own, &g));
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    cudaGraphGetNodes(g, nodes.data(), &nn);
+    int kernels = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nd, &t);
+        if (t == cudaGraphNodeTypeKernel) ++kernels;
+    }
+    cudaGraphDestroy(g);
+    return kernels;
+}
+
 }  // extern "C"

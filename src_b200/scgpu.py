@@ -96,6 +96,8 @@ def lib():
         L.scgpu_beam_parameters_from_stats.argtypes = [_dp, C.c_longlong, C.POINTER(BeamParams)]
         L.scgpu_get_field.argtypes = [C.c_void_p, C.c_int, _dp]
         L.scgpu_get_mesh.argtypes = [C.c_void_p, C.POINTER(Mesh)]
+        L.scgpu_profile_track.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.scgpu_kernels_per_step.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -106,7 +108,11 @@ EXPORTED = [
     "scgpu_compute_self_fields", "scgpu_register_host", "scgpu_unregister_host", "scgpu_bunch_upload",
     "scgpu_bunch_download", "scgpu_track", "scgpu_get_tracker_state", "scgpu_beam_parameters",
     "scgpu_beam_parameters_from_stats", "scgpu_get_field", "scgpu_get_mesh", "scgpu_last_track_ms",
+    "scgpu_profile_track", "scgpu_kernels_per_step",
 ]
+
+PHASES = ["drift_bounds", "cell_keys", "sort", "deposit", "assemble_rho", "green", "convolution", "grad",
+          "gather_kick_push"]
 
 
 def _p(a):
@@ -188,9 +194,12 @@ class Context:
         self._check(lib().scgpu_bunch_upload(self.h, R.shape[0], _p(R), _p(P), C.byref(bp)), "bunch_upload")
         self.n = R.shape[0]
 
-    def download(self):
-        R = np.empty((self.n, 3))
-        P = np.empty((self.n, 3))
+    def download(self, R=None, P=None):
+        """Returns R, P (n x 3); pass pinned arrays to receive them in place."""
+        R = np.empty((self.n, 3)) if R is None else R
+        P = np.empty((self.n, 3)) if P is None else P
+        assert R.dtype == np.float64 and R.flags.c_contiguous and R.shape == (self.n, 3)
+        assert P.dtype == np.float64 and P.flags.c_contiguous and P.shape == (self.n, 3)
         self._check(lib().scgpu_bunch_download(self.h, _p(R), _p(P)), "bunch_download")
         return R, P
 
@@ -220,6 +229,21 @@ class Context:
         out = np.empty((nz, ny, nx, 3) if which == FIELD_E else (nz, ny, nx))
         self._check(lib().scgpu_get_field(self.h, which, _p(out)), "get_field")
         return out
+
+    def profile(self, nsteps):
+        """Per-phase device milliseconds summed over nsteps serialised steps."""
+        out = np.zeros(len(PHASES))
+        self._check(lib().scgpu_profile_track(self.h, int(nsteps), _p(out)), "profile_track")
+        return dict(zip(PHASES, out))
+
+    def kernels_per_step(self):
+        k = lib().scgpu_kernels_per_step(self.h)
+        if k < 0:
+            self._check(k, "kernels_per_step")
+        return k
+
+    def set_stream(self, stream_handle):
+        self._check(lib().scgpu_set_stream(self.h, C.c_void_p(stream_handle)), "set_stream")
 
     def mesh(self):
         m = Mesh()

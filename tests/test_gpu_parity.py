@@ -1,0 +1,201 @@
+"""GPU parity of the plain FP64 form against the CPU oracle, through the C ABI.
+
+Tolerances are norm-wise, max|gpu - oracle| / max|oracle|:
+
+* per-particle state (R, P) after tracking, CIC charge density: 1e-13.  The
+  particle arithmetic rounds like the reference; only summation order differs.
+* potential and fields: 1e-12 (FIELD_TOL).  The integrated Green's function
+  cancels 8 antiderivative values per point, which amplifies 1-ulp
+  differences between device and glibc atan/log.
+* raw phase-space moment sums: 1e-12.  Derived rms emittances inherit the
+  cancellation of the reference's one-pass formula (PartBunchBase.hpp:1549-1557):
+  the tolerance is 1e-12 times the condition number sum(p^2)/(sum(p^2) - N pmean^2).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from src_b200.bunch import config_bunch, gaussian_bunch
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-12
+STATE_TOL = 1e-13
+RHO_TOL = 1e-13
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+def run_pair(oracle, gpu, N, nr, steps, bunch_id=0, bz=0.0, precision=0):
+    R, P = gaussian_bunch(N, bunch_id=bunch_id)
+    Q = -1e-9 / N
+    prm = oracle.make_params(nr, 1e-12, bz_ext=bz)
+    tr = oracle.OracleTracker(prm, Q)
+    Ro, Po = R.copy(), P.copy()
+    dbg = tr.track(Ro, Po, steps, want_debug=True)
+    with gpu.Context(nr, precision=precision) as c:
+        c.upload(R, P, 1e-12, Q, oracle.electron_mass_ev(), bz_ext=bz)
+        c.track(steps)
+        Rg, Pg = c.download()
+        out = dict(R=Rg, P=Pg, st=c.tracker_state(), rho=c.field(gpu.FIELD_RHO), phi=c.field(gpu.FIELD_PHI),
+                   E=c.field(gpu.FIELD_E), bp=c.beam_parameters(), mesh=c.mesh())
+    return dict(R=Ro, P=Po, tr=tr, dbg=dbg), out
+
+
+def test_compute_potential_golden(gpu):
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "convolution_n8.npz"))
+    with gpu.Context((8, 8, 8)) as c:
+        phi = c.compute_potential(g["rho"], g["hr"])
+    assert rel(phi, g["phi"]) < FIELD_TOL
+
+
+@pytest.mark.parametrize("nr", [(16, 16, 16), (24, 24, 24), (16, 24, 32), (48, 48, 48), (32, 32, 96)])
+def test_compute_potential_vs_oracle(oracle, gpu, nr):
+    rng = np.random.default_rng(sum(nr))
+    rho = np.abs(rng.standard_normal((nr[2], nr[1], nr[0])))
+    hr = (2.7e-4, 2.9e-4, 5.1e-3)
+    with gpu.Context(nr) as c:
+        phi = c.compute_potential(rho, hr)
+    assert rel(phi, oracle.compute_potential(rho, hr)) < FIELD_TOL
+
+
+def test_compute_self_fields_vs_oracle(oracle, gpu):
+    b = config_bunch("c1", n=50_000)
+    prm = oracle.make_params((32, 32, 32), b["dT"])
+    Ef_o, Bf_o, q_o, dbg = oracle.compute_self_fields(prm, b["Q"], b["R"], b["P"])
+    with gpu.Context((32, 32, 32)) as c:
+        Ef, Bf, q = c.compute_self_fields(b["R"], b["P"], b["Q"], b["dT"])
+        rho, phi, E, m = c.field(gpu.FIELD_RHO), c.field(gpu.FIELD_PHI), c.field(gpu.FIELD_E), c.mesh()
+    assert q == q_o
+    np.testing.assert_array_equal(m["hr"], dbg["hr"])
+    np.testing.assert_array_equal(m["origin"], dbg["origin"])
+    assert m["gammaz"] == dbg["gammaz"]
+    assert rel(rho, dbg["rho"]) < RHO_TOL
+    assert rel(phi, dbg["phi"]) < FIELD_TOL
+    assert rel(E, dbg["E"]) < FIELD_TOL
+    assert rel(Ef, Ef_o) < FIELD_TOL
+    assert rel(Bf, Bf_o) < FIELD_TOL
+
+
+@pytest.mark.parametrize("N,nr,steps", [(20_000, (16, 16, 16), 5), (100_000, (32, 32, 32), 10),
+                                        (30_001, (16, 24, 48), 3)])
+def test_tracking_vs_oracle(oracle, gpu, N, nr, steps):
+    o, g = run_pair(oracle, gpu, N, nr, steps)
+    assert rel(g["R"], o["R"]) < STATE_TOL
+    assert rel(g["P"], o["P"]) < STATE_TOL
+    assert rel(g["rho"], o["dbg"]["rho"]) < RHO_TOL
+    assert rel(g["phi"], o["dbg"]["phi"]) < FIELD_TOL
+    assert rel(g["E"], o["dbg"]["E"]) < FIELD_TOL
+    st, tr = g["st"], o["tr"]
+    assert st["path_length"] == tr.path_length and st["t"] == tr.t and st["q_macro"] == tr.Q
+    assert st["step"] == steps
+    bo = oracle.beam_parameters(o["R"], o["P"])
+    assert rel(g["bp"]["moments"], bo["moments"]) < 1e-12
+    for d in range(3):
+        s = bo["moments"][6 + (2 * d + 1) * (2 * d + 2) // 2 + 2 * d + 1]   # sum p_d^2
+        cond = s / max(s - N * bo["pmean"][d] ** 2, 1e-300)
+        assert abs(g["bp"]["eps_norm"][d] - bo["eps_norm"][d]) <= 1e-12 * cond * bo["eps_norm"][d]
+        assert math.isclose(g["bp"]["rrms"][d], bo["rrms"][d], rel_tol=1e-12)
+
+
+def test_tracking_golden(gpu):
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "step_n8.npz"))
+    with gpu.Context((8, 8, 8)) as c:
+        c.upload(g["R0"], g["P0"], 1e-12, -1e-9 / 2000, 0.51099892e-03 * 1.0e9)
+        c.track(3)
+        R, P = c.download()
+        E = c.field(gpu.FIELD_E)
+        st = c.tracker_state()
+    assert rel(R, g["R"]) < STATE_TOL and rel(P, g["P"]) < STATE_TOL
+    assert rel(E, g["E"]) < FIELD_TOL
+    assert st["q_macro"] == float(g["Q"]) and st["path_length"] == float(g["path_length"])
+
+
+def test_solenoid_field_tracking(oracle, gpu):
+    o, g = run_pair(oracle, gpu, 20_000, (16, 16, 16), 5, bz=0.2)
+    assert rel(g["R"], o["R"]) < STATE_TOL and rel(g["P"], o["P"]) < STATE_TOL
+
+
+def test_deterministic_bitwise(gpu, oracle):
+    R, P = gaussian_bunch(200_000, bunch_id=5)
+    outs = []
+    for _ in range(2):
+        with gpu.Context((32, 32, 32)) as c:
+            c.upload(R, P, 1e-12, -1e-9 / 200_000, oracle.electron_mass_ev())
+            c.track(4)
+            outs.append((*c.download(), c.field(gpu.FIELD_RHO), c.field(gpu.FIELD_E)))
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_stats_records_match_beam_parameters(gpu, oracle):
+    R, P = gaussian_bunch(50_000, bunch_id=6)
+    with gpu.Context((16, 16, 16)) as c:
+        c.upload(R, P, 1e-12, -1e-9 / 50_000, oracle.electron_mass_ev())
+        stats = np.zeros((4, gpu.NSTATS))
+        c.track(4, stats)
+        bp = c.beam_parameters()
+    last = gpu.beam_parameters_from_stats(stats[-1], 50_000)
+    np.testing.assert_array_equal(last["moments"], bp["moments"])
+    assert np.all(np.diff(stats[:, 4]) != 0)
+
+
+def test_edge_cases(gpu, oracle):
+    m = oracle.electron_mass_ev()
+    # a single particle: every bound has zero length (the 1e-10 branch of boundp)
+    with gpu.Context((8, 8, 8)) as c:
+        c.upload(np.zeros((1, 3)), np.array([[0.0, 0.0, 10.0]]), 1e-12, -1e-9, m)
+        c.track(2)
+        R, P = c.download()
+    R1, P1 = np.zeros((1, 3)), np.array([[0.0, 0.0, 10.0]])
+    tr = oracle.OracleTracker(oracle.make_params((8, 8, 8), 1e-12), -1e-9)
+    tr.track(R1, P1, 2)
+    assert rel(R + 1e-30, R1 + 1e-30) < STATE_TOL and rel(P, P1) < STATE_TOL
+    # particle counts off every tile / window boundary
+    for N in (31, 33, 4095, 4097):
+        o, g = run_pair(oracle, gpu, N, (8, 8, 8), 2, bunch_id=N)
+        assert rel(g["R"], o["R"]) < STATE_TOL and rel(g["P"], o["P"]) < STATE_TOL
+
+
+def test_errors_are_reported(gpu, oracle):
+    m = oracle.electron_mass_ev()
+    R, P = gaussian_bunch(1000, bunch_id=8)
+    with gpu.Context((8, 8, 8)) as c:
+        with pytest.raises(gpu.ScgpuError) as e:
+            c.track(1)
+        assert e.value.code == -7
+        # mean momentum anti-parallel to z: getQuaternion has no defined rotation
+        with pytest.raises(gpu.ScgpuError) as e:
+            c.upload(R, -P, 1e-12, -1e-12, m)
+        assert e.value.code == -5
+        with pytest.raises(gpu.ScgpuError) as e:
+            c.upload(R, P, -1.0, -1e-12, m)
+        assert e.value.code == -1
+        # the context stays usable after errors
+        c.upload(R, P, 1e-12, -1e-12, m)
+        c.track(1)
+
+
+def test_c2_size_properties(gpu, oracle):
+    """Full single-bunch size (1M particles, 64^3 mesh): charge conservation,
+    two steps against the oracle, bitwise determinism."""
+    b = config_bunch("c2")
+    N = b["N"]
+    with gpu.Context((64, 64, 64)) as c:
+        c.upload(b["R"], b["P"], b["dT"], b["Q"], oracle.electron_mass_ev())
+        c.track(2)
+        Rg, Pg = c.download()
+        rho = c.field(gpu.FIELD_RHO)
+        m = c.mesh()
+        st = c.tracker_state()
+    hv = m["hr_scaled"][0] * m["hr_scaled"][1] * m["hr_scaled"][2]
+    assert math.isclose(rho.sum() * hv * b["dT"], N * st["q_macro"] * b["dT"], rel_tol=1e-12)
+    tr = oracle.OracleTracker(oracle.make_params((64, 64, 64), b["dT"]), b["Q"])
+    Ro, Po = b["R"].copy(), b["P"].copy()
+    tr.track(Ro, Po, 2)
+    assert rel(Rg, Ro) < STATE_TOL and rel(Pg, Po) < STATE_TOL
