@@ -2,11 +2,13 @@
 
 Tolerances are norm-wise, max|gpu - oracle| / max|oracle|:
 
-* per-particle state (R, P) after tracking, CIC charge density: 1e-13.  The
-  particle arithmetic rounds like the reference; only summation order differs.
-* potential and fields: 1e-12 (FIELD_TOL).  The integrated Green's function
-  cancels 8 antiderivative values per point, which amplifies 1-ulp
-  differences between device and glibc atan/log.
+* CIC charge density: 1e-13.  The particle arithmetic rounds like the
+  reference; only the summation order of the deposit differs.
+* potential and fields: FIELD_TOL.  The integrated Green's function cancels
+  8 antiderivative values per point (up to n^3-fold), which amplifies 1-ulp
+  differences between device and glibc atan/log into ~1e-11 of the field.
+* per-particle state (R, P) after tracking: STATE_TOL, driven by the field
+  differences above through the kicks.
 * raw phase-space moment sums: 1e-12.  Derived rms emittances inherit the
   cancellation of the reference's one-pass formula (PartBunchBase.hpp:1549-1557):
   the tolerance is 1e-12 times the condition number sum(p^2)/(sum(p^2) - N pmean^2).
@@ -20,8 +22,8 @@ from src_b200.bunch import config_bunch, gaussian_bunch
 
 pytestmark = pytest.mark.gpu
 
-FIELD_TOL = 1e-12
-STATE_TOL = 1e-13
+FIELD_TOL = 2e-11
+STATE_TOL = 1e-12
 RHO_TOL = 1e-13
 
 
@@ -71,9 +73,11 @@ def test_compute_self_fields_vs_oracle(oracle, gpu):
         Ef, Bf, q = c.compute_self_fields(b["R"], b["P"], b["Q"], b["dT"])
         rho, phi, E, m = c.field(gpu.FIELD_RHO), c.field(gpu.FIELD_PHI), c.field(gpu.FIELD_E), c.mesh()
     assert q == q_o
+    # bounds are exact (min / max), so the mesh is bitwise the oracle's
     np.testing.assert_array_equal(m["hr"], dbg["hr"])
     np.testing.assert_array_equal(m["origin"], dbg["origin"])
-    assert m["gammaz"] == dbg["gammaz"]
+    # gamma_z comes from a sum of p_z: tree order vs sequential order
+    assert math.isclose(m["gammaz"], dbg["gammaz"], rel_tol=1e-13)
     assert rel(rho, dbg["rho"]) < RHO_TOL
     assert rel(phi, dbg["phi"]) < FIELD_TOL
     assert rel(E, dbg["E"]) < FIELD_TOL
@@ -147,15 +151,21 @@ def test_stats_records_match_beam_parameters(gpu, oracle):
 
 def test_edge_cases(gpu, oracle):
     m = oracle.electron_mass_ev()
-    # a single particle: every bound has zero length (the 1e-10 branch of boundp)
+    # a single uncharged particle: every bound has zero length (the 1e-10
+    # branch of boundp) and the step reduces to the drift, bit for bit
+    R0 = np.array([[1e-4, -2e-4, 3e-4]])
+    P0 = np.array([[1e-3, 2e-3, 10.0]])
     with gpu.Context((8, 8, 8)) as c:
-        c.upload(np.zeros((1, 3)), np.array([[0.0, 0.0, 10.0]]), 1e-12, -1e-9, m)
+        c.upload(R0, P0, 1e-12, 0.0, m)
         c.track(2)
         R, P = c.download()
-    R1, P1 = np.zeros((1, 3)), np.array([[0.0, 0.0, 10.0]])
-    tr = oracle.OracleTracker(oracle.make_params((8, 8, 8), 1e-12), -1e-9)
+        mesh = c.mesh()
+    R1, P1 = R0.copy(), P0.copy()
+    tr = oracle.OracleTracker(oracle.make_params((8, 8, 8), 1e-12), 0.0)
     tr.track(R1, P1, 2)
-    assert rel(R + 1e-30, R1 + 1e-30) < STATE_TOL and rel(P, P1) < STATE_TOL
+    np.testing.assert_array_equal(R, R1)
+    np.testing.assert_array_equal(P, P1)
+    assert math.isclose(mesh["rmax"][0] - mesh["rmin"][0], 2e-10, rel_tol=1e-6)
     # particle counts off every tile / window boundary
     for N in (31, 33, 4095, 4097):
         o, g = run_pair(oracle, gpu, N, (8, 8, 8), 2, bunch_id=N)
@@ -170,8 +180,10 @@ def test_errors_are_reported(gpu, oracle):
             c.track(1)
         assert e.value.code == -7
         # mean momentum anti-parallel to z: getQuaternion has no defined rotation
+        Pa = np.zeros_like(P)
+        Pa[:, 2] = -10.0
         with pytest.raises(gpu.ScgpuError) as e:
-            c.upload(R, -P, 1e-12, -1e-12, m)
+            c.upload(R, Pa, 1e-12, -1e-12, m)
         assert e.value.code == -5
         with pytest.raises(gpu.ScgpuError) as e:
             c.upload(R, P, -1.0, -1e-12, m)
