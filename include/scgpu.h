@@ -191,6 +191,25 @@ int scgpu_profile_track(scgpu_ctx* ctx, int nsteps, double* phase_ms);
 /* number of kernels one tracking step launches (from the step's CUDA graph) */
 int scgpu_kernels_per_step(scgpu_ctx* ctx);
 
+/* The open-boundary Poisson solve of scgpu_compute_potential_device for
+ * callers that cannot allocate device memory -- hosts whose device memory is
+ * owned by their own pool allocator, or loops that cannot afford the device
+ * synchronisation of cudaMalloc / cudaFree.  It has no counterpart in the
+ * reference.  No context is needed and nothing is allocated: rho_dev
+ * (nx*ny*nz doubles, x fastest) and phi_dev (same size; may equal rho_dev)
+ * are the caller's device buffers on the current device, and the scratch is
+ * a 4 MiB array inside the library that every GPU loading the library keeps
+ * until the process exits.  Limits: at most 32 cells per axis (and 2n
+ * factoring into 2, 3, 5); larger meshes return SCGPU_ERR_UNSUPPORTED.  The
+ * first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current; make that first call before
+ * any stream capture.  Every call shares the one array, so calls that overlap
+ * on the GPU (different streams, or several host threads) race; serialise
+ * them on one stream.  The work is enqueued on cuda_stream (a cudaStream_t,
+ * NULL for the default stream) and returns without synchronising. */
+int scgpu_compute_potential_noalloc(const double* rho_dev, double* phi_dev, int nx, int ny, int nz,
+                                    const double hr[3], void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
