@@ -51,14 +51,13 @@ def algorithmic_bytes(N, n, precision):
     step = 96 * N + 4 * r * M + 6 * r * S + 16 * G3
     phases = {
         "drift_bounds": 72 * N,                    # read R, P; write R (beam frame)
-        "cell_keys": 28 * N,                       # read R; write 32-bit key
-        "sort": 32 * N,                            # 2 radix passes over (key, index)
-        "deposit": 32 * N,                         # sorted (key, index), gathered R
-        "assemble_rho": r * M,                     # write rho
+        "deposit": 24 * N + 16 * M,                # read R; 128-bit node accumulators
+        "assemble_rho": 16 * M + r * M,            # node accumulators in, rho out
         "green": 16 * G3,                          # G write + read
         "convolution": 2 * r * M + 6 * r * S,      # rho in, phi out, spectrum traffic
         "grad": r * M + 3 * r * M,                 # phi in, 3-component E out
         "gather_kick_push": 96 * N + 3 * r * M,    # R, P in and out; E read
+        "reorder": 0,                              # amortised cell-order sort (no algorithmic bytes)
     }
     return step, phases
 

@@ -177,16 +177,15 @@ double scgpu_last_track_ms(const scgpu_ctx* ctx);
  * PartBunchBase.hpp:2393-2397, FFTPoissonSolver.cpp:65-66).  Runs nsteps
  * tracking steps with the phases serialised on one stream and CUDA events
  * between them; phase_ms[SCGPU_NPHASES] receives the summed milliseconds. */
-#define SCGPU_NPHASES 9
-#define SCGPU_PHASE_DRIFT_BOUNDS 0   /* half drift, beam frame, bounds, mesh */
-#define SCGPU_PHASE_CELL_KEYS 1
-#define SCGPU_PHASE_SORT 2
-#define SCGPU_PHASE_DEPOSIT 3        /* segmented reduction + cell joins */
-#define SCGPU_PHASE_ASSEMBLE 4       /* corner sums -> rho */
-#define SCGPU_PHASE_GREEN 5          /* integrated Green's function + its spectrum */
-#define SCGPU_PHASE_CONVOLUTION 6    /* pruned FFT convolution */
-#define SCGPU_PHASE_GRAD 7
-#define SCGPU_PHASE_GATHER_KICK 8    /* gather, frames, kick, drift, reference update */
+#define SCGPU_NPHASES 8
+#define SCGPU_PHASE_DRIFT_BOUNDS 0   /* half drift, beam frame, bounds, mesh; reference particle */
+#define SCGPU_PHASE_DEPOSIT 1        /* CIC charge deposit (exact node sums) */
+#define SCGPU_PHASE_ASSEMBLE 2       /* node sums -> rho */
+#define SCGPU_PHASE_GREEN 3          /* integrated Green's function + its spectrum */
+#define SCGPU_PHASE_CONVOLUTION 4    /* pruned FFT convolution */
+#define SCGPU_PHASE_GRAD 5
+#define SCGPU_PHASE_GATHER_KICK 6    /* gather, frames, kick, drift, reference update */
+#define SCGPU_PHASE_REORDER 7        /* cell-order sort of the particle arrays (every few steps) */
 int scgpu_profile_track(scgpu_ctx* ctx, int nsteps, double* phase_ms);
 /* number of kernels one tracking step launches (from the step's CUDA graph) */
 int scgpu_kernels_per_step(scgpu_ctx* ctx);

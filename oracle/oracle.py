@@ -119,6 +119,30 @@ def fft_engine_is_own():
     return bool(lib().sco_fft_engine_is_own())
 
 
+def set_exact_math(on=True):
+    """Correctly rounded atan / log in the Green's function (quad precision)
+    instead of the host libm's; returns the previous setting."""
+    L = lib()
+    prev = bool(L.sco_get_exact_math())
+    L.sco_set_exact_math(C.c_int(1 if on else 0))
+    return prev
+
+
+class exact_math:
+    """Context manager: correctly rounded Green's-function math inside."""
+
+    def __init__(self, on=True):
+        self.on = on
+
+    def __enter__(self):
+        self.prev = set_exact_math(self.on)
+        return self
+
+    def __exit__(self, *exc):
+        set_exact_math(self.prev)
+        return False
+
+
 # ---------------------------------------------------------------- constants
 def c_light():
     return lib().sco_const_c()

@@ -45,6 +45,7 @@
 
 #ifdef _OPENMP
 #include <omp.h>
+#include <quadmath.h>
 #endif
 
 /* ------------------------------------------------------------------------ */
@@ -778,14 +779,26 @@ void sco_fft3d_c2r(const int* L, double* spec, double* out) {
 /* in the reference and never reaches the physical n^3 block of phi; here it  */
 /* holds the value of the same closed form.                                   */
 /* ------------------------------------------------------------------------ */
+/* Elementary functions of the antiderivative.  By default the host libm,
+ * as the reference calls std::atan / std::log.  With sco_set_exact_math(1)
+ * they are evaluated in quad precision (libquadmath) and rounded once, i.e.
+ * correctly rounded: the field then no longer depends on which libm rounds
+ * which argument (the eight-corner difference turns a one-ulp change of one
+ * value into ~1e-11 of the field). */
+static int g_exact_math = 0;
+void sco_set_exact_math(int on) { g_exact_math = on != 0; }
+int sco_get_exact_math(void) { return g_exact_math; }
+static double igf_atan(double v) { return g_exact_math ? (double)atanq((__float128)v) : atan(v); }
+static double igf_log(double v) { return g_exact_math ? (double)logq((__float128)v) : log(v); }
+
 static double igf_antiderivative(double x, double y, double z, double cellVolume) {
     double r = sqrt(x * x + y * y + z * z);
-    double tmpgrn = -z * z * atan(x * y / (z * r)) / 2;
-    tmpgrn += -y * y * atan(x * z / (y * r)) / 2;
-    tmpgrn += -x * x * atan(y * z / (x * r)) / 2;
-    tmpgrn += y * z * log(x + r);
-    tmpgrn += x * z * log(y + r);
-    tmpgrn += x * y * log(z + r);
+    double tmpgrn = -z * z * igf_atan(x * y / (z * r)) / 2;
+    tmpgrn += -y * y * igf_atan(x * z / (y * r)) / 2;
+    tmpgrn += -x * x * igf_atan(y * z / (x * r)) / 2;
+    tmpgrn += y * z * igf_log(x + r);
+    tmpgrn += x * z * igf_log(y + r);
+    tmpgrn += x * y * igf_log(z + r);
     return tmpgrn / cellVolume;
 }
 

@@ -110,6 +110,10 @@ void sco_fft1d(int kind, long long n, double* data);
 void sco_fft3d_r2c(const int* L, const double* in, double* out);
 void sco_fft3d_c2r(const int* L, double* spec, double* out);
 
+/* 0: host libm for the Green's function's atan / log (the reference's
+ * behaviour); 1: correctly rounded (quad precision, rounded once). */
+void sco_set_exact_math(int on);
+int sco_get_exact_math(void);
 void sco_igf(const int* nr, const double* hr, double* G2);
 int sco_compute_potential(const int* nr, double* rho, const double* hr);
 void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, double gammaz, double* E);

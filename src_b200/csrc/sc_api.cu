@@ -27,9 +27,10 @@ struct scgpu_ctx {
     int digit_bits = 0;
     std::string err;
     double last_ms = 0.0;
-    cudaGraphExec_t g_step = nullptr;
-    cudaGraphExec_t g_step_stats = nullptr;
+    cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [stats][reorder]
     bool use_graphs = true;
+    int reorder_every = 16;   // put the particle arrays in cell order every k steps (0: never)
+    long long steps_done = 0; // steps since the last upload
     size_t smem_fft = 0;
 };
 
@@ -75,18 +76,18 @@ bool length_ok(int n) {
 
 void free_particles(scgpu_ctx* c) {
     DevBunch& b = c->b;
-    dfree(b.x); dfree(b.y); dfree(b.z); dfree(b.px); dfree(b.py); dfree(b.pz);
+    dfree(b.x); dfree(b.y); dfree(b.z); dfree(b.px); dfree(b.py); dfree(b.pz); dfree(b.id);
     dfree(b.keys); dfree(b.keys_alt); dfree(b.vals); dfree(b.vals_alt);
-    dfree(b.hist); dfree(b.hist_scan); dfree(b.scan_blocks);
-    dfree(b.carry_first); dfree(b.carry_last); dfree(b.wflag);
     dfree(b.Ef); dfree(b.Bf);
     c->capacity = 0;
 }
 
 void drop_graphs(scgpu_ctx* c) {
-    if (c->g_step) cudaGraphExecDestroy(c->g_step);
-    if (c->g_step_stats) cudaGraphExecDestroy(c->g_step_stats);
-    c->g_step = c->g_step_stats = nullptr;
+    for (auto& row : c->graphs)
+        for (auto& g : row) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
 }
 
 int ensure_particles(scgpu_ctx* c, long long n) {
@@ -102,57 +103,56 @@ int ensure_particles(scgpu_ctx* c, long long n) {
             (rc = dalloc(c, &b.px, d)) || (rc = dalloc(c, &b.py, d)) || (rc = dalloc(c, &b.pz, d)))
             return rc;
         if ((rc = dalloc(c, &b.keys, u)) || (rc = dalloc(c, &b.keys_alt, u)) || (rc = dalloc(c, &b.vals, u)) ||
-            (rc = dalloc(c, &b.vals_alt, u)))
+            (rc = dalloc(c, &b.vals_alt, u)) || (rc = dalloc(c, &b.id, u)))
             return rc;
         if ((rc = dalloc(c, &b.Ef, 3 * d)) || (rc = dalloc(c, &b.Bf, 3 * d))) return rc;
-        const long long tiles = (n + sort_tile_elems() - 1) / sort_tile_elems();
-        const long long table = tiles * 512;
-        if ((rc = dalloc(c, &b.hist, table * sizeof(int))) || (rc = dalloc(c, &b.hist_scan, table * sizeof(int))) ||
-            (rc = dalloc(c, &b.scan_blocks, (2 * (table / 8192 + 2)) * sizeof(int))))
-            return rc;
-        const long long nwin = (n + 31) / 32;
-        if ((rc = dalloc(c, (double**)&b.carry_first, nwin * 8 * sizeof(double))) ||
-            (rc = dalloc(c, (double**)&b.carry_last, nwin * 8 * sizeof(double))) ||
-            (rc = dalloc(c, &b.wflag, nwin * sizeof(int))))
-            return rc;
         c->capacity = n;
     }
     if (n != c->n) drop_graphs(c);
     c->n = n;
     b.bc.N = n;
-    b.sort_tiles = (int)((n + sort_tile_elems() - 1) / sort_tile_elems());
-    b.nwin = (n + 31) / 32;
     long long g = (n + 255) / 256;
     if (g < 1) g = 1;
-    if (g > 148 * 4) g = 148 * 4;
+    if (g > 148 * 8) g = 148 * 8;
     b.red_blocks = (int)g;
     return SCGPU_OK;
 }
 
-// one ParallelTTracker step on the context's stream
-void enqueue_step(scgpu_ctx* c, bool stats, cudaStream_t s) {
+// Puts the particle arrays in cell order: counting sort (keys, ranks, cell
+// starts, scatter) and a gather of the particle arrays.
+void enqueue_reorder(scgpu_ctx* c, cudaStream_t s) {
     DevBunch& b = c->b;
-    launch_drift_to_beam(b, true, true, s);
-    // Green's function branch depends only on the mesh
+    launch_cell_keys(b, 0, s);
+    launch_sort(b, s);
+    launch_reorder(b, s);
+    cudaMemsetAsync(b.hist, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(int), s);
+}
+
+// one ParallelTTracker step on the context's stream
+void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
+    DevBunch& b = c->b;
+    launch_drift_to_beam(b, true, s);
+    // the reference particle and the Green's function depend only on the
+    // mesh and the tracker state: a side branch beside sort and deposit
     cudaEventRecord(c->ev_fork, s);
     cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+    launch_advance_reference(b, c->side);
     launch_igf(b, nullptr, c->side);
     launch_green_transform(b, c->side);
     cudaEventRecord(c->ev_join, c->side);
-    launch_cell_keys(b, c->digit_bits, s);
-    launch_sort(b, s);
     launch_deposit(b, s);
     launch_assemble_rho(b, s);
+    if (reorder) enqueue_reorder(c, s);
     cudaStreamWaitEvent(s, c->ev_join, 0);
     launch_convolution(b, kConvSelfField, s);
     launch_grad(b, s);
     launch_gather_kick_push(b, stats, s);
 }
 
-int build_graph(scgpu_ctx* c, bool stats, cudaGraphExec_t* out) {
+int build_graph(scgpu_ctx* c, bool stats, bool reorder, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(c, stats, c->own);
+    enqueue_step(c, stats, reorder, c->own);
     cudaError_t e = cudaStreamEndCapture(c->own, &g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
     e = cudaGraphInstantiate(out, g, 0);
@@ -258,6 +258,7 @@ int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
     c->device = device;
     c->sp = *p;
     c->use_graphs = std::getenv("SCGPU_NO_GRAPH") == nullptr;
+    if (const char* r = std::getenv("SCGPU_REORDER_EVERY")) c->reorder_every = std::atoi(r);
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
         delete c;
@@ -274,18 +275,20 @@ int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
     int bits = 0;
     while ((1LL << bits) < M) ++bits;
     b.bc.key_bits = bits < 1 ? 1 : bits;
-    c->digit_bits = sort_digit_bits(b.bc.key_bits);
     const size_t rs = p->precision == SCGPU_PLAIN_FP64 ? sizeof(double) : sizeof(float);
     int rc = SCGPU_OK;
     const long long S = (n2 + 1) * (2 * n1) * (2 * n0);
     const long long T3 = (n0 + 2) * (n1 + 2) * (n2 + 2);
     const long long G3 = (n0 + 1) * (n1 + 1) * (n2 + 1);
-    if ((rc = dalloc(c, (double**)&b.seg, M * 8 * sizeof(double))) || (rc = dalloc(c, &b.stamp, M * sizeof(uint32_t))) ||
-        (rc = dalloc(c, (char**)&b.rho, M * rs)) || (rc = dalloc(c, (char**)&b.phi, M * rs)) ||
-        (rc = dalloc(c, (char**)&b.E4, 4 * M * rs)) || (rc = dalloc(c, (char**)&b.spec, S * 2 * rs)) ||
+    if ((rc = dalloc(c, &b.nacc, M * 2 * sizeof(unsigned long long))) ||
+        (rc = dalloc(c, (char**)&b.rho, M * rs)) || (rc = dalloc(c, (char**)&b.phi, M * sizeof(double))) ||
+        (rc = dalloc(c, (char**)&b.E4, 4 * M * rs)) || (rc = dalloc(c, (char**)&b.spec, S * sizeof(double2))) ||
+        (p->precision != SCGPU_PLAIN_FP64 && (rc = dalloc(c, (char**)&b.spec_lo, S * sizeof(float2)))) ||
         (rc = dalloc(c, &b.gtmp, T3 * sizeof(double))) || (rc = dalloc(c, &b.gline, G3 * sizeof(double))) ||
         (rc = dalloc(c, (char**)&b.ghat, G3 * rs)) || (rc = dalloc(c, &b.st, sizeof(StepState))) ||
-        (rc = dalloc(c, &b.partials, 148 * 4 * 32 * sizeof(double))) || (rc = dalloc(c, &b.ticket, 64))) {
+        (rc = dalloc(c, &b.partials, 148 * 8 * 32 * 16)) || (rc = dalloc(c, &b.ticket, 64)) ||
+        (rc = dalloc(c, &b.hist, M * sizeof(int))) || (rc = dalloc(c, &b.hist_scan, M * sizeof(int))) ||
+        (rc = dalloc(c, &b.scan_blocks, scan_scratch_ints(M) * sizeof(int)))) {
         scgpu_destroy(c);
         return rc;
     }
@@ -303,7 +306,8 @@ int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
     cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     cudaEventCreate(&c->ev_t0);
     cudaEventCreate(&c->ev_t1);
-    cudaMemsetAsync(b.stamp, 0, M * sizeof(uint32_t), c->own);
+    cudaMemsetAsync(b.nacc, 0, M * 2 * sizeof(unsigned long long), c->own);
+    cudaMemsetAsync(b.hist, 0, M * sizeof(int), c->own);
     cudaMemsetAsync(b.ticket, 0, 64, c->own);
     cudaMemsetAsync(b.st, 0, sizeof(StepState), c->own);
     fft_set_smem_limits();
@@ -326,8 +330,9 @@ void scgpu_destroy(scgpu_ctx* c) {
     drop_graphs(c);
     free_particles(c);
     DevBunch& b = c->b;
-    dfree(b.seg); dfree(b.stamp); dfree(b.rho); dfree(b.phi); dfree(b.E4); dfree(b.spec);
+    dfree(b.nacc); dfree(b.rho); dfree(b.phi); dfree(b.E4); dfree(b.spec); dfree(b.spec_lo);
     dfree(b.gtmp); dfree(b.gline); dfree(b.ghat); dfree(b.st); dfree(b.partials); dfree(b.ticket);
+    dfree(b.hist); dfree(b.hist_scan); dfree(b.scan_blocks);
     for (int d = 0; d < 3; ++d) dfree(b.tw[d]);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -393,16 +398,7 @@ static int compute_potential_impl(scgpu_ctx* c, double* rho, const double hr[3],
     }
     enqueue_green(c, s);
     launch_convolution(b, kConvPotential, s);
-    if (b.precision == SCGPU_PLAIN_FP64) {
-        CK(cudaMemcpyAsync(rho, b.phi, M * sizeof(double), out_kind, s));
-    } else {
-        double* stage = nullptr;
-        CK(cudaMalloc(&stage, M * sizeof(double)));
-        launch_f32_to_f64((const float*)b.phi, stage, M, s);
-        CK(cudaMemcpyAsync(rho, stage, M * sizeof(double), out_kind, s));
-        CK(cudaStreamSynchronize(s));
-        cudaFree(stage);
-    }
+    CK(cudaMemcpyAsync(rho, b.phi, M * sizeof(double), out_kind, s));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
     c->have_solve = false;
@@ -426,23 +422,22 @@ int scgpu_compute_self_fields(scgpu_ctx* c, long long n, const double* R, const 
     cudaStream_t s = c->stream;
     b.bc.dT = dT;
     if (b.bc.coupling == 0.0) b.bc.coupling = 1.0 / (4 * kPi * 8.854187817e-12);
+    if (b.bc.mass == 0.0) b.bc.mass = 0.51099892e-03 * 1.0e9;
+    bunch_constants(b.bc);
     CK(cudaMemcpyAsync(b.Ef, R, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(b.Bf, P, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     launch_aos_to_soa(b.Ef, b.x, b.y, b.z, n, s);
     launch_aos_to_soa(b.Bf, b.px, b.py, b.pz, n, s);
     CK(cudaMemcpyAsync(&b.st->Q, q_macro, sizeof(double), cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(b.stamp, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(uint32_t), s));
+    CK(cudaMemsetAsync(b.nacc, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * 2 * sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(b.hist, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(int), s));
     CK(cudaMemsetAsync(&b.st->gen, 0, sizeof(unsigned), s));
     launch_reduce_state(b, false, s);
     STAGE("reduce_state");
-    launch_drift_to_beam(b, false, false, s);
+    launch_drift_to_beam(b, false, s);
     STAGE("bounds");
     enqueue_green(c, s);
     STAGE("green");
-    launch_cell_keys(b, c->digit_bits, s);
-    STAGE("cell_keys");
-    launch_sort(b, s);
-    STAGE("sort");
     launch_deposit(b, s);
     STAGE("deposit");
     launch_assemble_rho(b, s);
@@ -479,6 +474,7 @@ int scgpu_bunch_upload(scgpu_ctx* c, long long n, const double* R, const double*
     b.bc.charge = bp->charge;
     b.bc.coupling = bp->coupling;
     b.bc.bz_ext = bp->bz_ext;
+    bunch_constants(b.bc);
     StepState h{};
     h.t = bp->t;
     h.path_length = bp->path_length;
@@ -492,11 +488,14 @@ int scgpu_bunch_upload(scgpu_ctx* c, long long n, const double* R, const double*
     h.step = 0;
     h.gen = 0;
     CK(cudaMemcpyAsync(b.st, &h, sizeof(StepState), cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(b.stamp, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(uint32_t), s));
+    CK(cudaMemsetAsync(b.nacc, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * 2 * sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(b.hist, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(int), s));
     CK(cudaMemcpyAsync(b.Ef, R, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(b.Bf, P, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     launch_aos_to_soa(b.Ef, b.x, b.y, b.z, n, s);
     launch_aos_to_soa(b.Bf, b.px, b.py, b.pz, n, s);
+    launch_iota(b.id, n, s);
+    c->steps_done = 0;
     launch_reduce_state(b, true, s);
     CK(cudaGetLastError());
     rc = check_device_err(c);
@@ -511,8 +510,8 @@ int scgpu_bunch_download(scgpu_ctx* c, double* R, double* P) {
     DevBunch& b = c->b;
     cudaStream_t s = c->stream;
     const long long n = c->n;
-    launch_soa_to_aos(b.x, b.y, b.z, b.Ef, n, s);
-    launch_soa_to_aos(b.px, b.py, b.pz, b.Bf, n, s);
+    launch_soa_to_aos_by_id(b.x, b.y, b.z, b.id, b.Ef, n, s);
+    launch_soa_to_aos_by_id(b.px, b.py, b.pz, b.id, b.Bf, n, s);
     CK(cudaMemcpyAsync(R, b.Ef, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(P, b.Bf, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -524,18 +523,21 @@ int scgpu_track(scgpu_ctx* c, int nsteps, double* stats) {
     if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
     CK(cudaSetDevice(c->device));
     const bool want = stats != nullptr;
-    cudaGraphExec_t* gx = want ? &c->g_step_stats : &c->g_step;
-    if (c->use_graphs && !*gx) {
-        int rc = build_graph(c, want, gx);
-        if (rc) return rc;
-    }
     cudaStream_t s = c->stream;
     CK(cudaEventRecord(c->ev_t0, s));
     for (int k = 0; k < nsteps; ++k) {
-        if (c->use_graphs)
-            CK(cudaGraphLaunch(*gx, s));
-        else
-            enqueue_step(c, want, s);
+        const bool reorder = c->reorder_every > 0 && (c->steps_done % c->reorder_every) == 0;
+        if (c->use_graphs) {
+            cudaGraphExec_t& gx = c->graphs[want ? 1 : 0][reorder ? 1 : 0];
+            if (!gx) {
+                int rc = build_graph(c, want, reorder, &gx);
+                if (rc) return rc;
+            }
+            CK(cudaGraphLaunch(gx, s));
+        } else {
+            enqueue_step(c, want, reorder, s);
+        }
+        ++c->steps_done;
         if (want)
             CK(cudaMemcpyAsync(stats + (size_t)k * SCGPU_NSTATS, c->b.st->moments, SCGPU_NSTATS * sizeof(double),
                                cudaMemcpyDeviceToHost, s));
@@ -595,10 +597,14 @@ int scgpu_get_field(scgpu_ctx* c, int which, double* out) {
     const long long M = (long long)b.bc.n[0] * b.bc.n[1] * b.bc.n[2];
     const bool f64 = b.precision == SCGPU_PLAIN_FP64;
     const size_t rs = f64 ? sizeof(double) : sizeof(float);
-    if (which == SCGPU_FIELD_RHO || which == SCGPU_FIELD_PHI) {
-        const void* src = which == SCGPU_FIELD_RHO ? b.rho : b.phi;
+    if (which == SCGPU_FIELD_PHI) {
+        CK(cudaMemcpyAsync(out, b.phi, M * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return SCGPU_OK;
+    }
+    if (which == SCGPU_FIELD_RHO) {
         std::vector<unsigned char> h(M * rs);
-        CK(cudaMemcpyAsync(h.data(), src, M * rs, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(h.data(), b.rho, M * rs, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         for (long long i = 0; i < M; ++i)
             out[i] = f64 ? ((const double*)h.data())[i] : (double)((const float*)h.data())[i];
@@ -647,33 +653,38 @@ int scgpu_profile_track(scgpu_ctx* c, int nsteps, double* phase_ms) {
     int rc = SCGPU_OK;
     for (int k = 0; k < nsteps && rc == SCGPU_OK; ++k) {
         cudaEventRecord(ev[0], s);
-        launch_drift_to_beam(b, true, true, s);
+        launch_drift_to_beam(b, true, s);
+        launch_advance_reference(b, s);
         cudaEventRecord(ev[1], s);
-        launch_cell_keys(b, c->digit_bits, s);
-        cudaEventRecord(ev[2], s);
-        launch_sort(b, s);
-        cudaEventRecord(ev[3], s);
         launch_deposit(b, s);
-        cudaEventRecord(ev[4], s);
+        cudaEventRecord(ev[2], s);
         launch_assemble_rho(b, s);
-        cudaEventRecord(ev[5], s);
+        cudaEventRecord(ev[3], s);
+        // the reorder sorts beam-frame positions: it runs where the step runs it
+        if (c->reorder_every > 0 && (c->steps_done % c->reorder_every) == 0) enqueue_reorder(c, s);
+        ++c->steps_done;
+        cudaEventRecord(ev[4], s);
         enqueue_green(c, s);
-        cudaEventRecord(ev[6], s);
+        cudaEventRecord(ev[5], s);
         launch_convolution(b, kConvSelfField, s);
-        cudaEventRecord(ev[7], s);
+        cudaEventRecord(ev[6], s);
         launch_grad(b, s);
-        cudaEventRecord(ev[8], s);
+        cudaEventRecord(ev[7], s);
         launch_gather_kick_push(b, false, s);
-        cudaEventRecord(ev[9], s);
-        cudaError_t e = cudaEventSynchronize(ev[9]);
+        cudaEventRecord(ev[8], s);
+        cudaError_t e = cudaEventSynchronize(ev[8]);
         if (e != cudaSuccess) {
             rc = cuda_fail(c, e, "profile step");
             break;
         }
+        // event interval i -> phase index (the reorder runs between assemble and green)
+        static const int phase_of_interval[SCGPU_NPHASES] = {
+            SCGPU_PHASE_DRIFT_BOUNDS, SCGPU_PHASE_DEPOSIT, SCGPU_PHASE_ASSEMBLE,    SCGPU_PHASE_REORDER,
+            SCGPU_PHASE_GREEN,        SCGPU_PHASE_CONVOLUTION, SCGPU_PHASE_GRAD, SCGPU_PHASE_GATHER_KICK};
         for (int p = 0; p < SCGPU_NPHASES; ++p) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[p], ev[p + 1]);
-            phase_ms[p] += ms;
+            phase_ms[phase_of_interval[p]] += ms;
         }
     }
     for (auto& e : ev) cudaEventDestroy(e);
@@ -688,7 +699,7 @@ int scgpu_kernels_per_step(scgpu_ctx* c) {
     CK(cudaSetDevice(c->device));
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(c, false, c->own);
+    enqueue_step(c, false, false, c->own);
     CK(cudaStreamEndCapture(c->own, &g));
     size_t nn = 0;
     cudaGraphGetNodes(g, nullptr, &nn);

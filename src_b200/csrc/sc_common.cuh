@@ -71,6 +71,7 @@ struct StepState {
     double bmin[3], bmax[3];
     double mesh_rmin[3], mesh_rmax[3];
     double hr[3], origin[3];
+    double rhr[3];  // RN(1 / hr)
     double gammaz;
     double hr_scaled[3];
     double tmp2;   // 1/hx * 1/hy * 1/hz_scaled
@@ -90,7 +91,20 @@ struct BunchConst {
     double coupling;
     double bz_ext;
     double dh;
+    // per-bunch constants of the pusher, evaluated in the reference's order
+    double s_cdt;   // c * dT                      (PartBunchBase.hpp:481)
+    double rs_cdt;  // RN(1 / (c * dT))
+    double ke;      // 0.5 * dT * charge * c / mass (BorisPusher.h:88)
+    double ktn;     // 0.5 * dT * charge * c * c    (BorisPusher.h:99, numerator)
 };
+
+// fill the derived pusher constants of bc (host side)
+inline void bunch_constants(BunchConst& bc) {
+    bc.s_cdt = kC * bc.dT;
+    bc.rs_cdt = 1.0 / bc.s_cdt;
+    bc.ke = 0.5 * bc.dT * bc.charge * kC / bc.mass;
+    bc.ktn = 0.5 * bc.dT * bc.charge * kC * kC;
+}
 
 // ---------------------------------------------------------------- vectors
 SC_HD double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
@@ -267,6 +281,21 @@ SC_HD void kick_one(double* P, const double* Ef, const double* Bf, double dt, do
     P[2] += ke * Ef[2];
 }
 
+// ---------------------------------------------------------------- division
+// a / b, correctly rounded, from rb = RN(1/b): one product, then the
+// remainder a - q0 b (exact with an FMA) corrects q0 (Markstein, IBM J. Res.
+// Dev. 34(1), 1990).  With rb correctly rounded the result equals the IEEE
+// quotient; operands near the ends of the exponent range take the division.
+// Callers pass divisors in the normal range (mesh spacings, c dt, gamma), so
+// only the quotient is checked: a tiny, zero or huge q0 takes the division.
+SC_HD double div_rcp(double a, double b, double rb) {
+    const double q0 = a * rb;
+    const double aq = q0 < 0 ? -q0 : q0;
+    if (!(aq > 0x1p-900 && aq < 0x1p900)) return a / b;
+    const double r = fma(-q0, b, a);
+    return fma(r, rb, q0);
+}
+
 // ---------------------------------------------------------------- CIC
 // Lower grid point and normalised offset of a particle (IntCIC.h:818-858 with
 // getVertexBelow, UniformCartesian.hpp:1025-1039, and getCellPosition,
@@ -300,6 +329,73 @@ SC_HD bool cic_locate(const double* hr, const double* origin, const int* n, cons
     return ok;
 }
 
+// cic_locate with the reciprocals rhr[d] = RN(1 / hr[d]): same results.
+SC_HD bool cic_locate_r(const double* hr, const double* rhr, const double* origin, const int* n, const double* x,
+                        int* lgp, double* dpos) {
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+        int i = (int)div_rcp(x[d] - origin[d], hr[d], rhr[d]);
+        int ngp = (x[d] >= origin[d]) ? i : i - 1;
+        double gpos = (ngp + 0.5) * hr[d] + origin[d];
+        double delta = hr[d];
+        int l = ngp;
+        if (gpos > x[d]) {
+            l = ngp - 1;
+            gpos = gpos - delta;
+        }
+        double dp = x[d] - gpos;
+        dp = div_rcp(dp, delta, rhr[d]);
+        if (l < 0) {
+            ok = false;
+            l = 0;
+        }
+        if (l > n[d] - 2) {
+            ok = false;
+            l = n[d] - 2;
+        }
+        lgp[d] = l;
+        dpos[d] = dp;
+    }
+    return ok;
+}
+
+// push_one with s = c dt and rs = RN(1/s) precomputed: same results.
+SC_HD void push_r(double* R, const double* P, double s, double rs) {
+    double r0 = div_rcp(R[0], s, rs), r1 = div_rcp(R[1], s, rs), r2 = div_rcp(R[2], s, rs);
+    const double g = sqrt(1.0 + dot3(P, P));
+    const double rg = 1.0 / g;
+    r0 += div_rcp(0.5 * P[0], g, rg);
+    r1 += div_rcp(0.5 * P[1], g, rg);
+    r2 += div_rcp(0.5 * P[2], g, rg);
+    R[0] = r0 * s;
+    R[1] = r1 * s;
+    R[2] = r2 * s;
+}
+
+// kick_one with ke = 0.5 dt q c / m and ktn = 0.5 dt q c c precomputed.
+SC_HD void kick_r(double* P, const double* Ef, const double* Bf, double ke, double ktn, double mass) {
+    P[0] += ke * Ef[0];
+    P[1] += ke * Ef[1];
+    P[2] += ke * Ef[2];
+    const double gamma = sqrt(1.0 + dot3(P, P));
+    const double kt = ktn / (gamma * mass);
+    double t[3] = {kt * Bf[0], kt * Bf[1], kt * Bf[2]};
+    double w[3], c[3];
+    cross3(P, t, c);
+    w[0] = P[0] + c[0];
+    w[1] = P[1] + c[1];
+    w[2] = P[2] + c[2];
+    const double ks = 2.0 / (1.0 + dot3(t, t));
+    double s[3] = {ks * t[0], ks * t[1], ks * t[2]};
+    cross3(w, s, c);
+    P[0] += c[0];
+    P[1] += c[1];
+    P[2] += c[2];
+    P[0] += ke * Ef[0];
+    P[1] += ke * Ef[1];
+    P[2] += ke * Ef[2];
+}
+
 // ---------------------------------------------------------------- mesh
 // boundp (PartBunchBase.hpp:802-884) from the beam-frame bounds, then the
 // scalars of computeSelfFields (PartBunch.cpp:493-511, 541-547, 641).
@@ -323,6 +419,7 @@ SC_HD bool derive_mesh(StepState& s, const BunchConst& bc) {
     }
     bool ok = s.hr[0] * s.hr[1] * s.hr[2] > 0;
     for (int i = 0; i < 3; ++i) s.origin[i] = rmin[i] - s.hr[i] / 2.0;
+    for (int i = 0; i < 3; ++i) s.rhr[i] = 1.0 / s.hr[i];
     double gz = s.psum[2] / (double)bc.N;
     gz *= gz;
     gz = sqrt(gz + 1.0);

@@ -84,6 +84,62 @@ __device__ __forceinline__ void dft(Cx<T>* v) {
         v[0] = cadd(v[0], t1);
         v[1] = C{t2.x - s * d.y, t2.y + s * d.x};
         v[2] = C{t2.x + s * d.y, t2.y - s * d.x};
+    } else if constexpr (R == 8) {
+        // 2 x 4: a_k = x_k + x_{k+4}, b_k = (x_k - x_{k+4}) W8^k; X_{2m} = DFT4(a), X_{2m+1} = DFT4(b)
+        const T h = (T)0.70710678118654752440;
+        C a[4], b[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            a[k] = cadd(v[k], v[k + 4]);
+            b[k] = csub(v[k], v[k + 4]);
+        }
+        // W8^1 = (1 - i)/sqrt2 (forward), W8^2 = -i, W8^3 = -(1 + i)/sqrt2; conjugates for the inverse
+        if constexpr (!INV) {
+            b[1] = C{h * (b[1].x + b[1].y), h * (b[1].y - b[1].x)};
+            b[2] = C{b[2].y, -b[2].x};
+            b[3] = C{h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y)};
+        } else {
+            b[1] = C{h * (b[1].x - b[1].y), h * (b[1].y + b[1].x)};
+            b[2] = C{-b[2].y, b[2].x};
+            b[3] = C{-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y)};
+        }
+        dft<T, 4, INV>(a);
+        dft<T, 4, INV>(b);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            v[2 * m] = a[m];
+            v[2 * m + 1] = b[m];
+        }
+    } else if constexpr (R == 16) {
+        // 4 x 4: y_q = DFT4 over p of x_{q + 4p}; y_q[s] *= W16^{q s}; X_{s + 4t} = DFT4 over q of y_q[s]
+        C y[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            C t[4] = {v[q], v[q + 4], v[q + 8], v[q + 12]};
+            dft<T, 4, INV>(t);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) y[q][s] = t[s];
+        }
+        const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173;  // cos, sin of 2 pi / 16
+        const T c2 = (T)0.70710678118654752440;
+        // W16^j = cos(2 pi j/16) - i sin(2 pi j/16) (forward), j = q s in {1, 2, 3, 4, 6, 9}
+        const C w[10] = {C{(T)1, (T)0},  C{c1, -s1},       C{c2, -c2},      C{s1, -c1},  C{(T)0, (T)-1},
+                         C{-s1, -c1},    C{-c2, -c2},      C{-c1, -s1},     C{(T)-1, (T)0}, C{-c1, s1}};
+#pragma unroll
+        for (int q = 1; q < 4; ++q)
+#pragma unroll
+            for (int s = 1; s < 4; ++s) {
+                C tw = w[q * s];
+                if (INV) tw.y = -tw.y;
+                y[q][s] = cmul(y[q][s], tw);
+            }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            C t[4] = {y[0][s], y[1][s], y[2][s], y[3][s]};
+            dft<T, 4, INV>(t);
+#pragma unroll
+            for (int tt = 0; tt < 4; ++tt) v[s + 4 * tt] = t[tt];
+        }
     } else if constexpr (R == 5) {
         const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
         const T s1 = INV ? (T)0.95105651629515357212 : (T)-0.95105651629515357212;
@@ -140,7 +196,11 @@ __device__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, int ncols, const FftPlan& pl
     Cx<T>* b = tmp;
     for (int s = 0; s < pl.nst; ++s) {
         const int R = pl.r[s];
-        if (R == 4)
+        if (R == 16)
+            stage<T, 16, INV>(a, b, pl.L, Ns, ncols, tw);
+        else if (R == 8)
+            stage<T, 8, INV>(a, b, pl.L, Ns, ncols, tw);
+        else if (R == 4)
             stage<T, 4, INV>(a, b, pl.L, Ns, ncols, tw);
         else if (R == 2)
             stage<T, 2, INV>(a, b, pl.L, Ns, ncols, tw);
@@ -232,28 +292,41 @@ __global__ void __launch_bounds__(kThreads) k_fft_y(Cx<T>* __restrict__ spec, in
 }
 
 // ---------------------------------------------------------------- pass C
+// The forward transform and the multiplication run in TI, the inverse in TO.
+// The mixed form takes TI = float, TO = double: rounding in the forward half
+// is white noise in the spectrum, which the derivative of phi does not
+// amplify, while rounding after the multiplication would be noise relative
+// to phi itself and is kept at FP64.  `in` and `out` alias in the plain form;
+// every block reads its rows before it writes them.
 constexpr int kRowsC = 8;
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_fft_x_conv(Cx<T>* __restrict__ spec, const T* __restrict__ ghat, int n0, int n1,
-                                                         int L1, long long rows, FftPlan px, const Cx<T>* __restrict__ twx) {
-    using C = Cx<T>;
+template <typename TI, typename TO>
+__global__ void __launch_bounds__(kThreads) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0,
+                                                         int n1, int L1, long long rows, FftPlan px,
+                                                         const Cx<TI>* __restrict__ twi, const Cx<TO>* __restrict__ two) {
+    using CI = Cx<TI>;
+    using CO = Cx<TO>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L0 = px.L;
-    C* tw = reinterpret_cast<C*>(smem_raw);
-    C* buf = tw + L0;
-    C* tmp = buf + kRowsC * L0;
-    load_twiddles<T>(tw, twx, L0);
+    CO* tw_o = reinterpret_cast<CO*>(smem_raw);
+    CI* tw_i = reinterpret_cast<CI*>(tw_o + L0);
+    CO* bufo = reinterpret_cast<CO*>(tw_i + L0);
+    CO* tmpo = bufo + kRowsC * L0;
+    load_twiddles<TO>(tw_o, two, L0);
+    load_twiddles<TI>(tw_i, twi, L0);
+    CI* bufi = reinterpret_cast<CI*>(bufo);
+    CI* tmpi = reinterpret_cast<CI*>(tmpo);
     const long long r0 = (long long)blockIdx.x * kRowsC;
     for (int e = threadIdx.x; e < kRowsC * L0; e += blockDim.x) {
         const int ri = e / L0, x = e - ri * L0;
         const long long r = r0 + ri;
-        C v = C{(T)0, (T)0};
-        if (r < rows && x < n0) v = spec[(size_t)r * L0 + x];
-        buf[ri * L0 + x] = v;
+        CI v = CI{(TI)0, (TI)0};
+        if (r < rows && x < n0) v = in[(size_t)r * L0 + x];
+        bufi[ri * L0 + x] = v;
     }
     __syncthreads();
-    C* f = block_fft<T, false>(buf, tmp, kRowsC, px, tw);
-    C* g = (f == buf) ? tmp : buf;
+    const CI* f = block_fft<TI, false>(bufi, tmpi, kRowsC, px, tw_i);
+    CO* g = (f == bufi) ? tmpo : bufo;
+    CO* h = (f == bufi) ? bufo : tmpo;
     for (int e = threadIdx.x; e < kRowsC * L0; e += blockDim.x) {
         const int ri = e / L0, kx = e - ri * L0;
         const long long r = r0 + ri;
@@ -262,22 +335,22 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_conv(Cx<T>* __restrict__ spe
         const int ky = (int)(r - (long long)kz * L1);
         const int gy = ky <= n1 ? ky : L1 - ky;
         const int gx = kx <= n0 ? kx : L0 - kx;
-        const T gv = ghat[((size_t)kz * (n1 + 1) + gy) * (n0 + 1) + gx];
-        C v = f[e];
-        f[e] = C{v.x * gv, v.y * gv};
+        const TI gv = ghat[((size_t)kz * (n1 + 1) + gy) * (n0 + 1) + gx];
+        const CI v = f[e];
+        g[e] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
     }
     __syncthreads();
-    const C* out = block_fft<T, true>(f, g, kRowsC, px, tw);
+    const CO* o = block_fft<TO, true>(g, h, kRowsC, px, tw_o);
     for (int e = threadIdx.x; e < kRowsC * n0; e += blockDim.x) {
         const int ri = e / n0, x = e - ri * n0;
         const long long r = r0 + ri;
-        if (r < rows) spec[(size_t)r * L0 + x] = out[ri * L0 + x];
+        if (r < rows) out[(size_t)r * L0 + x] = o[ri * L0 + x];
     }
 }
 
 // ---------------------------------------------------------------- pass E
 template <typename T, bool SELF>
-__global__ void __launch_bounds__(kThreads) k_fft_z_c2r(const Cx<T>* __restrict__ spec, T* __restrict__ phi, int n0, int n1,
+__global__ void __launch_bounds__(kThreads) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
                                                         int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz,
                                                         const StepState* __restrict__ st, double normFact, double coupling) {
     using C = Cx<T>;
@@ -327,7 +400,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_c2r(const Cx<T>* __restrict_
             r = r * hvol;
             r = r * coupling;
         }
-        phi[((size_t)zz * n1 + y) * n0 + x] = (T)r;
+        phi[((size_t)zz * n1 + y) * n0 + x] = r;
     }
 }
 
@@ -382,6 +455,14 @@ FftPlan make_plan(int L) {
     p.L = L;
     int m = L;
     int ns = 0;
+    while (m % 16 == 0) {
+        p.r[ns++] = 16;
+        m /= 16;
+    }
+    if (m % 8 == 0) {
+        p.r[ns++] = 8;
+        m /= 8;
+    }
     while (m % 4 == 0) {
         p.r[ns++] = 4;
         m /= 4;
@@ -410,7 +491,7 @@ size_t fft_smem_bytes(const DevBunch& b) {
         m = std::max(m, cs * (size_t)(L[d] + 2 * (16 * L[d] + 32)));
         m = std::max(m, sizeof(double2) * (size_t)(L[d] + 2 * (16 * L[d] + 32)));
     }
-    m = std::max(m, cs * (size_t)(L[0] + 2 * (kRowsC * L[0] + 32)));
+    m = std::max(m, (sizeof(double2) + cs) * (size_t)L[0] + 2 * sizeof(double2) * (size_t)(kRowsC * L[0]));
     return m;
 }
 
@@ -465,6 +546,12 @@ void launch_green_transform(const DevBunch& b, cudaStream_t s) {
         k_dct_lines<float><<<gx, kThreads, sm0, s>>>(b.gline, (float*)b.ghat, (int)g0, (int)g1, g0, g0 * g1, 1, p0, tw0);
 }
 
+static size_t smem_conv(int L0, size_t in_bytes) {
+    return (sizeof(double2) + in_bytes) * (size_t)L0 + 2 * sizeof(double2) * (size_t)(kRowsC * L0);
+}
+
+// T is the type of the forward half (A, B and the forward x transform of C);
+// the inverse half (C's inverse, D, E) is FP64 in both forms.
 template <typename T>
 static void convolution_t(const DevBunch& b, int mode, cudaStream_t s) {
     using C = Cx<T>;
@@ -474,30 +561,34 @@ static void convolution_t(const DevBunch& b, int mode, cudaStream_t s) {
     const C* twx = reinterpret_cast<const C*>(tw_for(b, 0));
     const C* twy = reinterpret_cast<const C*>(tw_for(b, 1));
     const C* twz = reinterpret_cast<const C*>(tw_for(b, 2));
-    C* spec = reinterpret_cast<C*>(b.spec);
+    const double2* twx_d = reinterpret_cast<const double2*>(b.tw[0]);
+    const double2* twy_d = reinterpret_cast<const double2*>(b.tw[1]);
+    const double2* twz_d = reinterpret_cast<const double2*>(b.tw[2]);
+    C* fwd = reinterpret_cast<C*>(b.precision == 0 ? b.spec : b.spec_lo);
+    double2* inv = reinterpret_cast<double2*>(b.spec);
     double normFact = 1.0;
     normFact /= L0;
     normFact /= L1;
     normFact /= L2;
     // A
     dim3 ga((unsigned)((n0 + 31) / 32), (unsigned)n1);
-    k_fft_z_r2c<T><<<ga, kThreads, smem_tile<T>(L2, 16), s>>>((const T*)b.rho, spec, n0, n1, n2, L0, L1, pz, twz);
+    k_fft_z_r2c<T><<<ga, kThreads, smem_tile<T>(L2, 16), s>>>((const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz);
     // B
     dim3 gb((unsigned)((n0 + 15) / 16), (unsigned)(n2 + 1));
-    k_fft_y<T, false><<<gb, kThreads, smem_tile<T>(L1, 16), s>>>(spec, n0, L0, n1, L1, py, twy);
+    k_fft_y<T, false><<<gb, kThreads, smem_tile<T>(L1, 16), s>>>(fwd, n0, L0, n1, L1, py, twy);
     // C
     const long long rows = (long long)(n2 + 1) * L1;
-    k_fft_x_conv<T><<<(unsigned)((rows + kRowsC - 1) / kRowsC), kThreads, smem_tile<T>(L0, kRowsC), s>>>(
-        spec, (const T*)b.ghat, n0, n1, L1, rows, px, twx);
+    k_fft_x_conv<T, double><<<(unsigned)((rows + kRowsC - 1) / kRowsC), kThreads, smem_conv(L0, sizeof(C)), s>>>(
+        fwd, inv, (const T*)b.ghat, n0, n1, L1, rows, px, twx, twx_d);
     // D
-    k_fft_y<T, true><<<gb, kThreads, smem_tile<T>(L1, 16), s>>>(spec, n0, L0, L1, n1, py, twy);
+    k_fft_y<double, true><<<gb, kThreads, smem_tile<double>(L1, 16), s>>>(inv, n0, L0, L1, n1, py, twy_d);
     // E
     if (mode == kConvSelfField)
-        k_fft_z_c2r<T, true><<<ga, kThreads, smem_tile<T>(L2, 16), s>>>(spec, (T*)b.phi, n0, n1, n2, L0, L1, pz, twz, b.st,
-                                                                         normFact, b.bc.coupling);
+        k_fft_z_c2r<double, true><<<ga, kThreads, smem_tile<double>(L2, 16), s>>>(inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d,
+                                                                                   b.st, normFact, b.bc.coupling);
     else
-        k_fft_z_c2r<T, false><<<ga, kThreads, smem_tile<T>(L2, 16), s>>>(spec, (T*)b.phi, n0, n1, n2, L0, L1, pz, twz, b.st,
-                                                                          normFact, b.bc.coupling);
+        k_fft_z_c2r<double, false><<<ga, kThreads, smem_tile<double>(L2, 16), s>>>(inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d,
+                                                                                    b.st, normFact, b.bc.coupling);
 }
 
 void launch_convolution(const DevBunch& b, int mode, cudaStream_t s) {
@@ -514,13 +605,10 @@ void fft_set_smem_limits() {
     cudaFuncSetAttribute(k_fft_y<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_fft_y<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_fft_y<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_y<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_x_conv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_x_conv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_fft_x_conv<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_fft_x_conv<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_fft_z_c2r<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_fft_z_c2r<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_z_c2r<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_z_c2r<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_dct_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_dct_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
 }

@@ -20,27 +20,24 @@ struct DevBunch {
     double* px;
     double* py;
     double* pz;
+    uint32_t* id;     // original index of the particle in each slot
     // sort
     uint32_t* keys;
     uint32_t* keys_alt;
     uint32_t* vals;
     uint32_t* vals_alt;
-    int* hist;        // radix digit table [bins][tiles]
-    int* hist_scan;   // exclusive scan of hist
-    int* scan_blocks; // block sums of the scan
-    int sort_tiles;
-    // deposit
-    void* seg;        // per-cell corner sums S[cell][8] (double or float2 pairs)
-    uint32_t* stamp;  // per-cell generation stamp
-    void* carry_first;
-    void* carry_last;
-    int* wflag;
-    long long nwin;
+    int* hist;        // particles per cell (counting sort), zero between steps
+    int* hist_scan;   // first sorted position of every cell
+    int* scan_blocks; // chunk sums of the scan
+    // deposit: 128-bit fixed-point charge per node (lo, hi), zero between steps
+    unsigned long long* nacc;
     // grids
+    // T is double in the plain form and float in the mixed form.
     void* rho;        // n^3 real (T)
-    void* phi;        // n^3 real (T)
+    double* phi;      // n^3 real, FP64 in both forms
     void* E4;         // n^3 x 4 (T): (-grad phi) * (g, g, 1/g), w unused
-    void* spec;       // (n2+1) x L1 x L0 complex (T)
+    void* spec;       // (n2+1) x L1 x L0 complex, FP64: the inverse half of the convolution
+    void* spec_lo;    // same shape, complex float: forward half in the mixed form (null in the plain form)
     double* gtmp;     // (n0+2)(n1+2)(n2+2) IGF antiderivative
     double* gline;    // (n0+1)(n1+1)(n2+1) G then its cosine transforms (FP64)
     void* ghat;       // (n0+1)(n1+1)(n2+1) real spectrum of G (T)
@@ -66,7 +63,8 @@ int particle_grid(const DevBunch& b);
 
 // particle TU (sc_particles.cu)
 void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s);
-void launch_drift_to_beam(const DevBunch& b, bool drift, bool advance_ref, cudaStream_t s);
+void launch_drift_to_beam(const DevBunch& b, bool drift, cudaStream_t s);
+void launch_advance_reference(const DevBunch& b, cudaStream_t s);
 void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s);
 void launch_deposit(const DevBunch& b, cudaStream_t s);
 void launch_assemble_rho(const DevBunch& b, cudaStream_t s);
@@ -77,12 +75,16 @@ void launch_gather_fields(const DevBunch& b, cudaStream_t s);
 void launch_reduce_stats(const DevBunch& b, cudaStream_t s);
 void launch_aos_to_soa(const double* aos, double* a, double* b, double* c, long long n, cudaStream_t s);
 void launch_soa_to_aos(const double* a, const double* b, const double* c, double* aos, long long n, cudaStream_t s);
+void launch_reorder(const DevBunch& b, cudaStream_t s);
+void launch_iota(uint32_t* id, long long n, cudaStream_t s);
+void launch_soa_to_aos_by_id(const double* a, const double* b, const double* c, const uint32_t* id, double* aos,
+                             long long n, cudaStream_t s);
 void launch_f64_to_f32(const double* in, float* out, long long n, cudaStream_t s);
 void launch_f32_to_f64(const float* in, double* out, long long n, cudaStream_t s);
 
 // sort TU (sc_sort.cu)
-int sort_tile_elems();
-int sort_digit_bits(int key_bits);
+long long scan_scratch_ints(long long n);
+void exclusive_scan(const int* in, int* out, long long n, int* blocks, cudaStream_t s);
 void launch_sort(const DevBunch& b, cudaStream_t s);
 
 // FFT TU (sc_fft.cu)

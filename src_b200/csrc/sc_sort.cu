@@ -1,45 +1,23 @@
-// sc_sort.cu -- stable LSD radix sort of the particles' cell keys.
+// sc_sort.cu -- counting sort of the particles by CIC cell.
 //
-// The deposit sums the particles of one cell in the order the sort leaves
-// them; a stable sort whose first pass ranks particles by their index makes
-// that order (cell, particle index) -- unique, so the deposit is bitwise
-// reproducible.  Keys have at most 21 significant bits (128^3 cells); each
-// pass sorts one digit of up to 9 bits.
-//
-//   upsweep    per-tile digit histogram, digit-major table [bins][tiles]
-//   scan       exclusive prefix sum of that table (its flattened order is
-//              exactly "all smaller digits, then earlier tiles")
-//   downsweep  stable ranking inside the tile with warp match masks, scatter
+// Cell keys are bounded by the mesh (key < n0 n1 n2), so one counting pass
+// sorts them:
+//   k_cell_keys (sc_particles.cu)  key and rank = atomicAdd(count[key], 1)
+//   exclusive scan of count         -> first sorted position of every cell
+//   k_scatter                       sorted key and particle index at start + rank
+// The order of particles inside a cell depends on the order the atomics were
+// served in; the deposit therefore sums each cell exactly (fixed point), so
+// its result does not depend on that order and every run is bitwise the same.
 #include "sc_internal.h"
 
 namespace sc {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;  // 4096 keys per tile
-constexpr int kMaxBins = 512;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kScanThreads = 1024;
-constexpr int kScanItems = 8;
+constexpr int kScanItems = 16;
 constexpr int kScanChunk = kScanThreads * kScanItems;
 
-__global__ void __launch_bounds__(kThreads) k_upsweep(const uint32_t* __restrict__ keys, long long n, int shift, int bits,
-                                                      int* __restrict__ hist, int tiles) {
-    __shared__ int h[kMaxBins];
-    const int bins = 1 << bits;
-    for (int d = threadIdx.x; d < bins; d += blockDim.x) h[d] = 0;
-    __syncthreads();
-    const long long begin = (long long)blockIdx.x * kTile;
-    long long end = begin + kTile;
-    if (end > n) end = n;
-    for (long long i = begin + threadIdx.x; i < end; i += blockDim.x) atomicAdd(&h[(keys[i] >> shift) & (bins - 1)], 1);
-    __syncthreads();
-    for (int d = threadIdx.x; d < bins; d += blockDim.x) hist[(size_t)d * tiles + blockIdx.x] = h[d];
-}
-
-// ---- exclusive scan of an int array (three phases for large arrays)
 __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
     __shared__ int ws[kScanThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -67,6 +45,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
     return before;
 }
 
+// out[i] = sum of in[0..i) (+ chunk_base[chunk]); chunk_sum[chunk] = chunk total
 __global__ void __launch_bounds__(kScanThreads) k_scan_chunks(const int* __restrict__ in, int* __restrict__ out, long long n,
                                                               const int* __restrict__ chunk_base, int* __restrict__ chunk_sum) {
     const long long base = (long long)blockIdx.x * kScanChunk + (long long)threadIdx.x * kScanItems;
@@ -90,119 +69,46 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_chunks(const int* __restr
     if (chunk_sum && threadIdx.x == 0) chunk_sum[blockIdx.x] = total;
 }
 
+__global__ void __launch_bounds__(256) k_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ ranks,
+                                                 const int* __restrict__ start, uint32_t* __restrict__ skey,
+                                                 uint32_t* __restrict__ sval, long long n, int* __restrict__ err) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        const long long p = (long long)start[k] + ranks[i];
+        if (p >= 0 && p < n) {
+            skey[p] = k;
+            sval[p] = (uint32_t)i;
+        } else {
+            atomicOr(err, kFlagSort);
+        }
+    }
+}
+
+}  // namespace
+
+long long scan_scratch_ints(long long n) { return 2 * ((n + kScanChunk - 1) / kScanChunk) + 2; }
+
 void exclusive_scan(const int* in, int* out, long long n, int* blocks, cudaStream_t s) {
     const long long chunks = (n + kScanChunk - 1) / kScanChunk;
     if (chunks <= 1) {
         k_scan_chunks<<<1, kScanThreads, 0, s>>>(in, out, n, nullptr, nullptr);
         return;
     }
-    // chunk sums, scan of the sums (fits one chunk for n <= 64M), final pass
+    // chunk sums, scan of the sums (one chunk holds them for n <= 2^28), final pass
     k_scan_chunks<<<(unsigned)chunks, kScanThreads, 0, s>>>(in, nullptr, n, nullptr, blocks);
     k_scan_chunks<<<1, kScanThreads, 0, s>>>(blocks, blocks + chunks, chunks, nullptr, nullptr);
     k_scan_chunks<<<(unsigned)chunks, kScanThreads, 0, s>>>(in, out, n, blocks + chunks, nullptr);
 }
 
-// ---- downsweep: stable scatter of (key, value)
-template <bool FIRST>
-__global__ void __launch_bounds__(kThreads) k_downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
-                                                        uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, long long n,
-                                                        int shift, int bits, const int* __restrict__ offsets, int tiles,
-                                                        int* __restrict__ err) {
-    __shared__ int cnt[kWarps][kMaxBins];
-    __shared__ int run[kMaxBins];
-    __shared__ int base[kMaxBins];
-    const int bins = 1 << bits;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int d = threadIdx.x; d < bins; d += blockDim.x) {
-        run[d] = 0;
-        base[d] = offsets[(size_t)d * tiles + blockIdx.x];
-    }
-    const long long tile0 = (long long)blockIdx.x * kTile;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    for (int r = 0; r < kItems; ++r) {
-        for (int e = threadIdx.x; e < kWarps * bins; e += blockDim.x) cnt[e / bins][e % bins] = 0;
-        __syncthreads();
-        const long long i = tile0 + (long long)r * kThreads + threadIdx.x;
-        const bool valid = i < n;
-        uint32_t key = 0, val = 0;
-        int digit = bins;  // invalid lanes form their own group
-        if (valid) {
-            key = kin[i];
-            val = FIRST ? (uint32_t)i : vin[i];
-            digit = (int)((key >> shift) & (uint32_t)(bins - 1));
-        }
-        const unsigned peers = __match_any_sync(kFull, digit);
-        const int lrank = __popc(peers & lt_mask);
-        if (valid && lrank == 0) cnt[warp][digit] = __popc(peers);
-        __syncthreads();
-        // exclusive prefix over warps for each digit, continuing the tile's running count
-        for (int d = threadIdx.x; d < bins; d += blockDim.x) {
-            int acc = run[d];
-            for (int w = 0; w < kWarps; ++w) {
-                const int c = cnt[w][d];
-                cnt[w][d] = acc;
-                acc += c;
-            }
-            run[d] = acc;
-        }
-        __syncthreads();
-        if (valid) {
-            const long long p = (long long)base[digit] + cnt[warp][digit] + lrank;
-            if (p >= 0 && p < n) {
-                kout[p] = key;
-                vout[p] = val;
-            } else {
-                atomicOr(err, kFlagSort);
-            }
-        }
-        __syncthreads();
-    }
-}
-
-}  // namespace
-
-int sort_tile_elems() { return kTile; }
-
-// Sorts b.keys (particle order) into b.keys / b.vals (cell order, values =
-// particle indices).  The first pass's histogram comes from k_cell_keys.
+// After k_cell_keys: b.keys (key per particle), b.vals_alt (rank in its
+// cell), b.hist (count per cell).  Produces b.keys_alt (sorted keys) and
+// b.vals (particle index per sorted position); b.hist_scan holds the cell starts.
 void launch_sort(const DevBunch& b, cudaStream_t s) {
-    const long long n = b.bc.N;
-    const int bits_total = b.bc.key_bits;
-    const int passes = (bits_total + 8) / 9;
-    const int bits = (bits_total + passes - 1) / passes;
-    const int tiles = b.sort_tiles;
-    const long long table = (long long)tiles << bits;
-    uint32_t* kin = b.keys;
-    uint32_t* vin = b.vals;
-    uint32_t* kout = b.keys_alt;
-    uint32_t* vout = b.vals_alt;
-    for (int p = 0; p < passes; ++p) {
-        const int shift = p * bits;
-        if (p > 0) k_upsweep<<<tiles, kThreads, 0, s>>>(kin, n, shift, bits, b.hist, tiles);
-        exclusive_scan(b.hist, b.hist_scan, table, b.scan_blocks, s);
-        if (p == 0)
-            k_downsweep<true><<<tiles, kThreads, 0, s>>>(kin, nullptr, kout, vout, n, shift, bits, b.hist_scan, tiles,
-                                                          &b.st->err);
-        else
-            k_downsweep<false><<<tiles, kThreads, 0, s>>>(kin, vin, kout, vout, n, shift, bits, b.hist_scan, tiles,
-                                                           &b.st->err);
-        uint32_t* t = kin;
-        kin = kout;
-        kout = t;
-        t = vin;
-        vin = vout;
-        vout = t;
-    }
-    // result must end in keys/vals
-    if (kin != b.keys) {
-        cudaMemcpyAsync(b.keys, kin, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(b.vals, vin, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
-    }
-}
-
-int sort_digit_bits(int key_bits) {
-    const int passes = (key_bits + 8) / 9;
-    return (key_bits + passes - 1) / passes;
+    const long long M = (long long)b.bc.n[0] * b.bc.n[1] * b.bc.n[2];
+    exclusive_scan(b.hist, b.hist_scan, M, b.scan_blocks, s);
+    long long g = (b.bc.N + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    k_scatter<<<(unsigned)g, 256, 0, s>>>(b.keys, b.vals_alt, b.hist_scan, b.keys_alt, b.vals, b.bc.N, &b.st->err);
 }
 
 }  // namespace sc

@@ -111,8 +111,7 @@ EXPORTED = [
     "scgpu_profile_track", "scgpu_kernels_per_step",
 ]
 
-PHASES = ["drift_bounds", "cell_keys", "sort", "deposit", "assemble_rho", "green", "convolution", "grad",
-          "gather_kick_push"]
+PHASES = ["drift_bounds", "deposit", "assemble_rho", "green", "convolution", "grad", "gather_kick_push", "reorder"]
 
 
 def _p(a):

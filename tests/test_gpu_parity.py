@@ -211,3 +211,24 @@ def test_c2_size_properties(gpu, oracle):
     Ro, Po = b["R"].copy(), b["P"].copy()
     tr.track(Ro, Po, 2)
     assert rel(Rg, Ro) < STATE_TOL and rel(Pg, Po) < STATE_TOL
+
+
+@pytest.mark.parametrize("n,npart", [(32, 100_000), (64, 400_000)])
+def test_mixed_form_against_fp64(gpu, oracle, n, npart):
+    """Mixed form (FP32 deposit storage, forward FFT half and field storage;
+    FP64 particles, Green's function, inverse FFT half and boost): the field
+    bound is 1e-5 relative (max norm) to the FP64 form; the design gives
+    about 1e-7, asserted here with margin at 1e-6."""
+    R, P = gaussian_bunch(npart, bunch_id=12)
+    out = {}
+    for prec in (gpu.PLAIN_FP64, gpu.MIXED):
+        with gpu.Context((n, n, n), precision=prec) as c:
+            c.upload(R, P, 1e-12, -1e-9 / npart, oracle.electron_mass_ev())
+            c.track(5)
+            out[prec] = (*c.download(), c.field(gpu.FIELD_E), c.field(gpu.FIELD_RHO), c.beam_parameters())
+    Rd, Pd, Ed, rd, bd = out[gpu.PLAIN_FP64]
+    Rm, Pm, Em, rm, bm = out[gpu.MIXED]
+    assert rel(Em, Ed) < 1e-6
+    assert rel(rm, rd) < 1e-6
+    assert rel(Rm, Rd) < 1e-7 and rel(Pm, Pd) < 1e-7
+    np.testing.assert_allclose(bm["eps_norm"], bd["eps_norm"], rtol=1e-6)
