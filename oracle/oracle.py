@@ -119,27 +119,30 @@ def fft_engine_is_own():
     return bool(lib().sco_fft_engine_is_own())
 
 
-def set_exact_math(on=True):
-    """Correctly rounded atan / log in the Green's function (quad precision)
-    instead of the host libm's; returns the previous setting."""
+def set_exact(on=True):
+    """Exact mode: correctly rounded atan / log in the Green's function
+    (quad precision) and order-independent exact particle sums (terms
+    truncated at 2^-72, 128-bit integer addition, one rounding) instead of
+    the reference's libm calls and storage-order sums.  Returns the previous
+    setting."""
     L = lib()
-    prev = bool(L.sco_get_exact_math())
-    L.sco_set_exact_math(C.c_int(1 if on else 0))
+    prev = bool(L.sco_get_exact())
+    L.sco_set_exact(C.c_int(1 if on else 0))
     return prev
 
 
-class exact_math:
-    """Context manager: correctly rounded Green's-function math inside."""
+class exact:
+    """Context manager: the oracle in exact mode inside."""
 
     def __init__(self, on=True):
         self.on = on
 
     def __enter__(self):
-        self.prev = set_exact_math(self.on)
+        self.prev = set_exact(self.on)
         return self
 
     def __exit__(self, *exc):
-        set_exact_math(self.prev)
+        set_exact(self.prev)
         return False
 
 

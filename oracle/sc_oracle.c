@@ -61,6 +61,39 @@
  * merged in thread order and sums are combined in thread order, so a run is
  * reproducible for a fixed thread count. */
 static int g_threads = 1;
+
+/* Exact mode (off by default, i.e. the reference's own arithmetic):
+ *  - the Green's function's atan / log correctly rounded (quad precision);
+ *  - the particle sums (moments, the mean momentum behind gamma_z and the
+ *    beam frame, the sum of gamma) order-independent: every term v becomes
+ *    the integer trunc(v 2^72) (|v| < 2^55), the integers are added exactly
+ *    in 128 bits and the total is rounded to a double once.
+ * The reference sums particles in storage order on each rank and then across
+ * ranks (MPI_Allreduce), so its last bits depend on the rank count; through
+ * gamma_z and the eight-corner cancellation of the Green's function one ulp
+ * of such a sum moves the field by ~1e-11.  The exact mode fixes one answer. */
+static int g_exact = 0;
+void sco_set_exact(int on) { g_exact = on != 0; }
+int sco_get_exact(void) { return g_exact; }
+
+typedef __int128 sco_i128;
+#define SCO_EX_FRAC 72
+static sco_i128 ex_from(double v) {
+    uint64_t bits;
+    memcpy(&bits, &v, sizeof bits);
+    const int e = (int)((bits >> 52) & 0x7ff);
+    if (e == 0) return 0; /* zero or subnormal */
+    const uint64_t m = (bits & 0xfffffffffffffull) | (1ull << 52);
+    const int sh = e - 1075 + SCO_EX_FRAC;
+    unsigned __int128 mag;
+    if (sh >= 0)
+        mag = sh < 75 ? ((unsigned __int128)m << sh) : ((unsigned __int128)m << 74);
+    else
+        mag = sh > -53 ? (unsigned __int128)(m >> (-sh)) : 0;
+    return (bits >> 63) ? -(sco_i128)mag : (sco_i128)mag;
+}
+/* (double) of a 128-bit integer rounds to nearest-even; the scaling is exact */
+static double ex_to_double(sco_i128 x) { return ldexp((double)x, -SCO_EX_FRAC); }
 #define SCO_PAR _Pragma("omp parallel for num_threads(g_threads) if(g_threads > 1) schedule(static)")
 void sco_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
 int sco_get_threads(void) { return g_threads; }
@@ -294,7 +327,41 @@ void sco_bounds(long long n, const double* R, double* rmin, double* rmax) {
 static void moments_range(long long k0, long long k1, const double* R, const double* P, double* m27);
 
 /* 6 first moments + 21 second moments in OPAL's order (x,px,y,py,z,pz). */
+static void moments_exact_range(long long k0, long long k1, const double* R, const double* P, sco_i128* acc) {
+    for (int i = 0; i < 27; ++i) acc[i] = 0;
+    double part[6];
+    for (long long k = k0; k < k1; ++k) {
+        part[1] = P[3 * k + 0]; part[3] = P[3 * k + 1]; part[5] = P[3 * k + 2];
+        part[0] = R[3 * k + 0]; part[2] = R[3 * k + 1]; part[4] = R[3 * k + 2];
+        int l = 6;
+        for (int i = 0; i < 6; ++i) {
+            acc[i] += ex_from(part[i]);
+            for (int j = 0; j <= i; ++j) acc[l++] += ex_from(part[i] * part[j]);
+        }
+    }
+}
+
 void sco_moments(long long n, const double* R, const double* P, double* m27) {
+    if (g_exact) {
+        const int T = g_threads > 1 ? g_threads : 1;
+        sco_i128* part = (sco_i128*)calloc((size_t)T * 27, sizeof(sco_i128));
+#pragma omp parallel num_threads(T)
+        {
+#ifdef _OPENMP
+            const int t = omp_get_thread_num();
+#else
+            const int t = 0;
+#endif
+            moments_exact_range(n * t / T, n * (t + 1) / T, R, P, part + 27 * t);
+        }
+        for (int i = 0; i < 27; ++i) {
+            sco_i128 a = 0;
+            for (int t = 0; t < T; ++t) a += part[27 * t + i];
+            m27[i] = ex_to_double(a);
+        }
+        free(part);
+        return;
+    }
     if (g_threads > 1) {
         const int T = g_threads;
         double* part = (double*)calloc((size_t)T * 27, sizeof(double));
@@ -333,6 +400,11 @@ static void moments_range(long long k0, long long k1, const double* R, const dou
 }
 
 double sco_sum_gamma(long long n, const double* P) {
+    if (g_exact) {
+        sco_i128 a = 0;
+        for (long long i = 0; i < n; ++i) a += ex_from(sqrt(1.0 + dot3(P + 3 * i, P + 3 * i)));
+        return ex_to_double(a);
+    }
     double g = 0.0;
     for (long long i = 0; i < n; ++i) g += sqrt(1.0 + dot3(P + 3 * i, P + 3 * i));
     return g;
@@ -780,16 +852,13 @@ void sco_fft3d_c2r(const int* L, double* spec, double* out) {
 /* holds the value of the same closed form.                                   */
 /* ------------------------------------------------------------------------ */
 /* Elementary functions of the antiderivative.  By default the host libm,
- * as the reference calls std::atan / std::log.  With sco_set_exact_math(1)
- * they are evaluated in quad precision (libquadmath) and rounded once, i.e.
- * correctly rounded: the field then no longer depends on which libm rounds
- * which argument (the eight-corner difference turns a one-ulp change of one
- * value into ~1e-11 of the field). */
-static int g_exact_math = 0;
-void sco_set_exact_math(int on) { g_exact_math = on != 0; }
-int sco_get_exact_math(void) { return g_exact_math; }
-static double igf_atan(double v) { return g_exact_math ? (double)atanq((__float128)v) : atan(v); }
-static double igf_log(double v) { return g_exact_math ? (double)logq((__float128)v) : log(v); }
+ * as the reference calls std::atan / std::log.  In exact mode they are
+ * evaluated in quad precision (libquadmath) and rounded once, i.e. correctly
+ * rounded: the field then no longer depends on which libm rounds which
+ * argument (the eight-corner difference turns a one-ulp change of one value
+ * into ~1e-11 of the field). */
+static double igf_atan(double v) { return g_exact ? (double)atanq((__float128)v) : atan(v); }
+static double igf_log(double v) { return g_exact ? (double)logq((__float128)v) : log(v); }
 
 static double igf_antiderivative(double x, double y, double z, double cellVolume) {
     double r = sqrt(x * x + y * y + z * z);
@@ -941,7 +1010,7 @@ int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const
     for (long long c = 0; c < M; ++c) rho[c] /= prm->dT;
     /* gamma_z from the mean longitudinal momentum (:499-502) */
     double psum2 = 0.0;
-    if (g_threads > 1) {
+    if (g_threads > 1 || g_exact) {
         double m27[27];
         sco_moments(n, R, P, m27); /* thread-ordered partial sums; pz sum is m27[5] */
         psum2 = m27[5];

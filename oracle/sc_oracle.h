@@ -110,10 +110,12 @@ void sco_fft1d(int kind, long long n, double* data);
 void sco_fft3d_r2c(const int* L, const double* in, double* out);
 void sco_fft3d_c2r(const int* L, double* spec, double* out);
 
-/* 0: host libm for the Green's function's atan / log (the reference's
- * behaviour); 1: correctly rounded (quad precision, rounded once). */
-void sco_set_exact_math(int on);
-int sco_get_exact_math(void);
+/* 0 (default): the reference's arithmetic -- host libm atan / log in the
+ * Green's function, particle sums in storage order.  1: correctly rounded
+ * atan / log (quad precision) and order-independent exact particle sums
+ * (terms truncated at 2^-72, added as 128-bit integers, rounded once). */
+void sco_set_exact(int on);
+int sco_get_exact(void);
 void sco_igf(const int* nr, const double* hr, double* G2);
 int sco_compute_potential(const int* nr, double* rho, const double* hr);
 void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, double gammaz, double* E);

@@ -36,6 +36,11 @@ def main():
         h, l = dd(mp.log(mp.mpf(j) / 64))
         out.append(f"    {{{fmt(h)}, {fmt(l)}}},  // j = {j}")
     out.append("};")
+    out.append("// 64 / j rounded to double, j = 45 .. 91 (reciprocals of the log table's centres)")
+    out.append("SC_DDM_TABLE double kLogRcp[kLogJ1 - kLogJ0 + 1] = {")
+    for j in range(45, 92):
+        out.append(f"    {fmt(float(mp.mpf(64) / j))},  // j = {j}")
+    out.append("};")
     out.append("// atan(j / 64), j = 0 .. 64: {hi, lo}")
     out.append("SC_DDM_TABLE double kAtanTab[65][2] = {")
     for j in range(0, 65):

@@ -13,6 +13,9 @@
 #include <cuda_runtime.h>
 
 #define SC_HD __host__ __device__ __forceinline__
+// once-per-step scalar work run by one thread of a last block: kept out of line
+// so that it does not raise the register budget of the particle loops
+#define SC_HD_COLD inline __host__ __device__ __noinline__
 
 namespace sc {
 
@@ -400,7 +403,7 @@ SC_HD void kick_r(double* P, const double* Ef, const double* Bf, double ke, doub
 // boundp (PartBunchBase.hpp:802-884) from the beam-frame bounds, then the
 // scalars of computeSelfFields (PartBunch.cpp:493-511, 541-547, 641).
 // Returns false when h <= 0.
-SC_HD bool derive_mesh(StepState& s, const BunchConst& bc) {
+SC_HD_COLD bool derive_mesh(StepState& s, const BunchConst& bc) {
     double rmin[3] = {s.bmin[0], s.bmin[1], s.bmin[2]};
     double rmax[3] = {s.bmax[0], s.bmax[1], s.bmax[2]};
     for (int i = 0; i < 3; ++i) {
@@ -437,7 +440,7 @@ SC_HD bool derive_mesh(StepState& s, const BunchConst& bc) {
 // Beam-frame trafos of computeSpaceChargeFields (ParallelTTracker.cpp:550-554)
 // from the momentum sum and the path length.  Returns false for an
 // anti-parallel mean momentum.
-SC_HD bool derive_beam_frame(StepState& s, const BunchConst& bc) {
+SC_HD_COLD bool derive_beam_frame(StepState& s, const BunchConst& bc) {
     const double N = (double)bc.N;
     double pmean[3] = {s.psum[0] / N, s.psum[1] / N, s.psum[2] / N};
     double zhat[3] = {0.0, 0.0, 1.0}, q[4];

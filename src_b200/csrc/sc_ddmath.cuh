@@ -28,10 +28,10 @@
 #include <cstring>
 
 #ifdef __CUDACC__
-#define SC_HD __host__ __device__ __forceinline__
+#define SC_DDM_HD __host__ __device__ __forceinline__
 #define SC_DDM_TABLE static __device__ const
 #else
-#define SC_HD static inline
+#define SC_DDM_HD static inline
 #define SC_DDM_TABLE static const
 #endif
 
@@ -44,7 +44,7 @@ struct dd {
     double hi, lo;
 };
 
-SC_HD dd two_sum(double a, double b) {
+SC_DDM_HD dd two_sum(double a, double b) {
     const double s = a + b;
     const double bb = s - a;
     const double e = (a - (s - bb)) + (b - bb);
@@ -52,20 +52,20 @@ SC_HD dd two_sum(double a, double b) {
 }
 
 // requires |a| >= |b| (or a == 0)
-SC_HD dd fast_two_sum(double a, double b) {
+SC_DDM_HD dd fast_two_sum(double a, double b) {
     const double s = a + b;
     const double e = b - (s - a);
     return dd{s, e};
 }
 
-SC_HD dd two_prod(double a, double b) {
+SC_DDM_HD dd two_prod(double a, double b) {
     const double p = a * b;
     return dd{p, fma(a, b, -p)};
 }
 
-SC_HD dd neg(dd a) { return dd{-a.hi, -a.lo}; }
+SC_DDM_HD dd neg(dd a) { return dd{-a.hi, -a.lo}; }
 
-SC_HD dd add(dd a, dd b) {
+SC_DDM_HD dd add(dd a, dd b) {
     dd s = two_sum(a.hi, b.hi);
     const dd t = two_sum(a.lo, b.lo);
     s.lo += t.hi;
@@ -74,31 +74,35 @@ SC_HD dd add(dd a, dd b) {
     return fast_two_sum(s.hi, s.lo);
 }
 
-SC_HD dd mul(dd a, dd b) {
+SC_DDM_HD dd mul(dd a, dd b) {
     dd p = two_prod(a.hi, b.hi);
     p.lo += a.hi * b.lo + a.lo * b.hi;
     return fast_two_sum(p.hi, p.lo);
 }
 
-SC_HD dd mul_d(dd a, double b) {
+SC_DDM_HD dd mul_d(dd a, double b) {
     dd p = two_prod(a.hi, b);
     p.lo += a.lo * b;
     return fast_two_sum(p.hi, p.lo);
 }
 
-SC_HD dd div(dd a, dd b) {
-    const double q1 = a.hi / b.hi;
+// a / b from one hardware division: q1 = a.hi (1 / b.hi) is within a few ulp
+// of the quotient, and two correction terms from the exact residuals
+// a - b (q1 + q2) bring the result to about 2^-100 relative.
+SC_DDM_HD dd div(dd a, dd b) {
+    const double inv = 1.0 / b.hi;
+    const double q1 = a.hi * inv;
     dd r = add(a, neg(mul_d(b, q1)));
-    const double q2 = r.hi / b.hi;
+    const double q2 = r.hi * inv;
     r = add(r, neg(mul_d(b, q2)));
-    const double q3 = r.hi / b.hi;
+    const double q3 = r.hi * inv;
     return add(fast_two_sum(q1, q2), dd{q3, 0.0});
 }
 
-SC_HD dd tab(const double (*t)[2], int i) { return dd{t[i][0], t[i][1]}; }
+SC_DDM_HD dd tab(const double (*t)[2], int i) { return dd{t[i][0], t[i][1]}; }
 
 // log(x) for finite normal x > 0; other inputs go to the library function.
-SC_HD double log_dd(double x) {
+SC_DDM_HD double log_dd(double x) {
     if (!(x >= 2.2250738585072014e-308) || !(x <= 1.7976931348623157e308)) return log(x);
     uint64_t bits;
     memcpy(&bits, &x, sizeof bits);
@@ -113,8 +117,10 @@ SC_HD double log_dd(double x) {
     const int j = (int)rint(m * 64.0);  // 45 .. 91
     const double c = (double)j / 64.0;
     const double u = m - c;  // exact (Sterbenz)
-    const double th = u / c;
-    const double tl = fma(-th, c, u) / c;  // the remainder u - th c is exact
+    // t = u / c: th from the tabulated reciprocal, tl from the exact residual
+    const double rc = kLogRcp[j - kLogJ0];
+    const double th = u * rc;
+    const double tl = fma(-th, c, u) * rc;
     const dd t = fast_two_sum(th, tl);     // |t| < 0.0112
     // log1p t = t - t^2/2 + t^3/3 + t^4 (-1/4 + t/5 - ... - t^8/12)
     const double h = t.hi;
@@ -142,22 +148,27 @@ SC_HD double log_dd(double x) {
 }
 
 // atan(x) for finite x; NaN and infinities go to the library function.
-SC_HD double atan_dd(double x) {
+SC_DDM_HD double atan_dd(double x) {
     const double a = fabs(x);
     if (!(a <= 1.7976931348623157e308)) return atan(x);
     if (a < 9.3132257461547852e-10) return x;  // |x| < 2^-30: x^3/3 is below half an ulp of x
+    // s = min(a, 1/a); c = j/64 near s; atan s = atan c + atan t with
+    //   a <= 1: t = (a - c) / (1 + a c)
+    //   a >  1: t = (1/a - c) / (1 + c/a) = (1 - a c) / (a + c)
+    // numerator and denominator are exact double-doubles (TwoProd, TwoSum).
     const bool inv = a > 1.0;
-    dd s;
-    if (inv) {
-        const double sh = 1.0 / a;
-        s = fast_two_sum(sh, fma(-sh, a, 1.0) / a);
-    } else {
-        s = dd{a, 0.0};
-    }
-    const int j = (int)rint(s.hi * 64.0);  // 0 .. 64
+    const double s = inv ? 1.0 / a : a;
+    const int j = (int)rint(s * 64.0);  // 0 .. 64
     const double c = (double)j / 64.0;
-    const dd num = two_sum(s.hi - c, s.lo);  // s.hi - c is exact
-    const dd den = add(dd{1.0, 0.0}, mul_d(s, c));
+    dd num, den;
+    if (inv) {
+        const dd ac = two_prod(a, c);
+        num = add(dd{1.0, 0.0}, neg(ac));
+        den = two_sum(a, c);
+    } else {
+        num = dd{a - c, 0.0};  // exact (Sterbenz, or c = 0)
+        den = add(dd{1.0, 0.0}, two_prod(a, c));
+    }
     const dd t = div(num, den);  // |t| < 2^-7
     // atan t = t - t^3/3 + t^5 (1/5 - t^2/7 + t^4/9 - t^6/11)
     const double h = t.hi, h2 = h * h;

@@ -20,6 +20,14 @@
 // transform is real and is the product of three cosine (DCT-I) transforms of
 // G on (n0+1)(n1+1)(n2+1) points; it is built here from G with the same FFT
 // stages applied to the even extension of each line.
+//
+// Every kernel stages its lines global -> shared with cp.async (all copies of
+// a block in flight at once, no register round trip), runs Stockham radix
+// stages in shared memory and writes the pruned output.  The transform
+// lengths of the common meshes (2n = 32, 64, 96, 128, 256) are template
+// constants, so the stage loops unroll and the index arithmetic folds; other
+// lengths take the same kernels with the length read at run time.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -27,8 +35,6 @@
 
 namespace sc {
 namespace {
-
-constexpr int kThreads = 256;
 
 template <typename T>
 struct CT;
@@ -56,6 +62,90 @@ __device__ __forceinline__ C cmul(C a, C b) {
     return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }
 
+// ---------------------------------------------------------------- cp.async
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+template <typename V>
+__device__ __forceinline__ void cp_elem(V* smem, const V* gmem) {
+    cp_async<(int)sizeof(V)>(smem, gmem);
+}
+
+// ---------------------------------------------------------------- plans
+// Radix sequence of a length L = 2^p 3^a 5^b: radix-8 stages for the power of
+// two (a remainder of 2 with an 8 becomes 4 x 4, so no radix-2 stage runs
+// beside radix 8), then 3s and 5s.  nst = -1 when L has another factor.
+struct RadixPlan {
+    int nst;
+    int r[12];
+};
+__host__ __device__ constexpr RadixPlan radix_plan(int L) {
+    RadixPlan p{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+    if (L < 2) {
+        p.nst = -1;
+        return p;
+    }
+    int m = L, twos = 0;
+    while (m % 2 == 0) {
+        m /= 2;
+        ++twos;
+    }
+    int e8 = twos / 3;
+    const int rem = twos % 3;
+    if (rem == 1 && e8 > 0) {
+        e8 -= 1;
+        p.r[p.nst++] = 4;
+        p.r[p.nst++] = 4;
+    } else if (rem == 1) {
+        p.r[p.nst++] = 2;
+    } else if (rem == 2) {
+        p.r[p.nst++] = 4;
+    }
+    for (int i = 0; i < e8; ++i) p.r[p.nst++] = 8;
+    while (m % 3 == 0 && p.nst < 12) {
+        p.r[p.nst++] = 3;
+        m /= 3;
+    }
+    while (m % 5 == 0 && p.nst < 12) {
+        p.r[p.nst++] = 5;
+        m /= 5;
+    }
+    if (m != 1) p.nst = -1;
+    return p;
+}
+__host__ __device__ constexpr int min_radix(int L) {
+    const RadixPlan p = radix_plan(L);
+    int r = 16;
+    for (int i = 0; i < p.nst; ++i) r = p.r[i] < r ? p.r[i] : r;
+    return r;
+}
+// Complex transforms per block for a template length: the widest stage
+// (L / min radix butterflies per transform) fills at most 256 threads, and
+// at most 16 transforms share a block.  Length 0 (read at run time): 16.
+__host__ __device__ constexpr int cols_for(int LT) {
+    if (LT == 0) return 16;
+    const int per = LT / min_radix(LT);
+    int nc = 256 / per;
+    if (nc > 16) nc = 16;
+    if (nc < 1) nc = 1;
+    return nc;
+}
+__host__ __device__ constexpr int threads_for(int LT) {
+    if (LT == 0) return 256;
+    const int t = cols_for(LT) * (LT / min_radix(LT));
+    return t < 32 ? 32 : t;
+}
+
+// ---------------------------------------------------------------- butterflies
 // R-point DFT in registers; forward uses exp(-2 pi i / R).
 template <typename T, int R, bool INV>
 __device__ __forceinline__ void dft(Cx<T>* v) {
@@ -110,36 +200,6 @@ __device__ __forceinline__ void dft(Cx<T>* v) {
             v[2 * m] = a[m];
             v[2 * m + 1] = b[m];
         }
-    } else if constexpr (R == 16) {
-        // 4 x 4: y_q = DFT4 over p of x_{q + 4p}; y_q[s] *= W16^{q s}; X_{s + 4t} = DFT4 over q of y_q[s]
-        C y[4][4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            C t[4] = {v[q], v[q + 4], v[q + 8], v[q + 12]};
-            dft<T, 4, INV>(t);
-#pragma unroll
-            for (int s = 0; s < 4; ++s) y[q][s] = t[s];
-        }
-        const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173;  // cos, sin of 2 pi / 16
-        const T c2 = (T)0.70710678118654752440;
-        // W16^j = cos(2 pi j/16) - i sin(2 pi j/16) (forward), j = q s in {1, 2, 3, 4, 6, 9}
-        const C w[10] = {C{(T)1, (T)0},  C{c1, -s1},       C{c2, -c2},      C{s1, -c1},  C{(T)0, (T)-1},
-                         C{-s1, -c1},    C{-c2, -c2},      C{-c1, -s1},     C{(T)-1, (T)0}, C{-c1, s1}};
-#pragma unroll
-        for (int q = 1; q < 4; ++q)
-#pragma unroll
-            for (int s = 1; s < 4; ++s) {
-                C tw = w[q * s];
-                if (INV) tw.y = -tw.y;
-                y[q][s] = cmul(y[q][s], tw);
-            }
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            C t[4] = {y[0][s], y[1][s], y[2][s], y[3][s]};
-            dft<T, 4, INV>(t);
-#pragma unroll
-            for (int tt = 0; tt < 4; ++tt) v[s + 4 * tt] = t[tt];
-        }
     } else if constexpr (R == 5) {
         const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
         const T s1 = INV ? (T)0.95105651629515357212 : (T)-0.95105651629515357212;
@@ -159,99 +219,143 @@ __device__ __forceinline__ void dft(Cx<T>* v) {
     }
 }
 
-// One Stockham autosort stage (radix R) over ncols columns of length L.
+// One Stockham autosort butterfly (radix R): butterfly j of a column reads
+// src[j + r nb], r < R, applies the twiddles W^(r k step), k = j mod Ns, and
+// writes dst[(j / Ns) Ns R + k + r Ns].
 template <typename T, int R, bool INV>
-__device__ __forceinline__ void stage(const Cx<T>* __restrict__ in, Cx<T>* __restrict__ out, int L, int Ns, int ncols,
-                                      const Cx<T>* __restrict__ tw) {
+__device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst, int j, int nb, int Ns,
+                                          int step, const Cx<T>* __restrict__ tw) {
     using C = Cx<T>;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
+    const int k = j % Ns;
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+        C t = tw[r * k * step];
+        if (INV) t.y = -t.y;
+        v[r] = cmul(v[r], t);
+    }
+    dft<T, R, INV>(v);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+}
+
+// compile-time stage: length L, Ns, NC columns, NT threads
+template <typename T, int R, bool INV, int L, int NS, int NC, int NT>
+__device__ __forceinline__ void stage_c(const Cx<T>* in, Cx<T>* out, const Cx<T>* tw) {
+    constexpr int NB = L / R;
+    constexpr int STEP = L / (NS * R);
+#pragma unroll
+    for (int w0 = 0; w0 < NC * NB; w0 += NT) {
+        const int w = w0 + (int)threadIdx.x;
+        if ((NC * NB) % NT != 0 && w >= NC * NB) break;
+        const int col = w / NB;
+        const int j = w - col * NB;
+        butterfly<T, R, INV>(in + col * L, out + col * L, j, NB, NS, STEP, tw);
+    }
+}
+
+template <typename T, bool INV, int L, int S, int NS, int NC, int NT>
+__device__ __forceinline__ Cx<T>* stages_c(Cx<T>* a, Cx<T>* b, const Cx<T>* tw) {
+    constexpr RadixPlan P = radix_plan(L);
+    if constexpr (S == P.nst) {
+        return a;
+    } else {
+        constexpr int R = P.r[S];
+        stage_c<T, R, INV, L, NS, NC, NT>(a, b, tw);
+        __syncthreads();
+        return stages_c<T, INV, L, S + 1, NS * R, NC, NT>(b, a, tw);
+    }
+}
+
+// run-time stage (lengths without a template instance)
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void stage_r(const Cx<T>* in, Cx<T>* out, int L, int Ns, int ncols, const Cx<T>* tw) {
     const int nb = L / R;
     const int step = L / (Ns * R);
     for (int w = threadIdx.x; w < ncols * nb; w += blockDim.x) {
         const int col = w / nb;
         const int j = w - col * nb;
-        const C* src = in + col * L;
-        C* dst = out + col * L;
-        C v[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
-        const int k = j % Ns;
-#pragma unroll
-        for (int r = 1; r < R; ++r) {
-            C t = tw[r * k * step];
-            if (INV) t.y = -t.y;
-            v[r] = cmul(v[r], t);
+        butterfly<T, R, INV>(in + col * L, out + col * L, j, nb, Ns, step, tw);
+    }
+}
+
+// Complex FFT of NC columns (buf[col * L + i]); returns the buffer holding
+// the result (buf or tmp).  The caller synchronises before the call.
+template <typename T, bool INV, int LT, int NC, int NT>
+__device__ __forceinline__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, const FftPlan& pl, const Cx<T>* tw) {
+    if constexpr (LT > 0) {
+        return stages_c<T, INV, LT, 0, 1, NC, NT>(buf, tmp, tw);
+    } else {
+        int Ns = 1;
+        Cx<T>* a = buf;
+        Cx<T>* b = tmp;
+        for (int s = 0; s < pl.nst; ++s) {
+            const int R = pl.r[s];
+            if (R == 8)
+                stage_r<T, 8, INV>(a, b, pl.L, Ns, NC, tw);
+            else if (R == 4)
+                stage_r<T, 4, INV>(a, b, pl.L, Ns, NC, tw);
+            else if (R == 2)
+                stage_r<T, 2, INV>(a, b, pl.L, Ns, NC, tw);
+            else if (R == 3)
+                stage_r<T, 3, INV>(a, b, pl.L, Ns, NC, tw);
+            else
+                stage_r<T, 5, INV>(a, b, pl.L, Ns, NC, tw);
+            __syncthreads();
+            Cx<T>* t = a;
+            a = b;
+            b = t;
+            Ns *= R;
         }
-        dft<T, R, INV>(v);
-        const int base = (j / Ns) * Ns * R + k;
-#pragma unroll
-        for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+        return a;
     }
 }
 
-// Complex FFT of ncols columns (buf[col * L + i]); result returned (buf or tmp).
-template <typename T, bool INV>
-__device__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, int ncols, const FftPlan& pl, const Cx<T>* tw) {
-    int Ns = 1;
-    Cx<T>* a = buf;
-    Cx<T>* b = tmp;
-    for (int s = 0; s < pl.nst; ++s) {
-        const int R = pl.r[s];
-        if (R == 16)
-            stage<T, 16, INV>(a, b, pl.L, Ns, ncols, tw);
-        else if (R == 8)
-            stage<T, 8, INV>(a, b, pl.L, Ns, ncols, tw);
-        else if (R == 4)
-            stage<T, 4, INV>(a, b, pl.L, Ns, ncols, tw);
-        else if (R == 2)
-            stage<T, 2, INV>(a, b, pl.L, Ns, ncols, tw);
-        else if (R == 3)
-            stage<T, 3, INV>(a, b, pl.L, Ns, ncols, tw);
-        else
-            stage<T, 5, INV>(a, b, pl.L, Ns, ncols, tw);
-        __syncthreads();
-        Cx<T>* t = a;
-        a = b;
-        b = t;
-        Ns *= R;
-    }
-    return a;
+template <typename V, int NT>
+__device__ __forceinline__ void stage_twiddles(V* dst, const V* __restrict__ src, int L) {
+    for (int e = threadIdx.x; e < L; e += NT) cp_elem(dst + e, src + e);
 }
 
-template <typename T>
-__device__ __forceinline__ void load_twiddles(Cx<T>* dst, const Cx<T>* __restrict__ src, int L) {
-    for (int e = threadIdx.x; e < L; e += blockDim.x) dst[e] = src[e];
-}
+// elements of one tile: twiddles (L), buf and tmp (NC L + 2 NC each)
+__host__ __device__ constexpr size_t tile_elems(int L, int nc) { return (size_t)L + 2 * ((size_t)nc * L + 2 * nc); }
 
 // ---------------------------------------------------------------- pass A
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_fft_z_r2c(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1,
-                                                        int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz) {
+// 2 NC real columns (x) of one y per block, packed two per complex FFT.
+template <typename T, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1, int n2,
+                                                  int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz) {
     using C = Cx<T>;
+    constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int L2 = pz.L;
+    const int L2 = LT > 0 ? LT : pz.L;
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L2;
-    C* tmp = buf + 16 * L2 + 32;
-    load_twiddles<T>(tw, twz, L2);
+    C* tmp = buf + NC * L2 + RC;
+    stage_twiddles<C, NT>(tw, twz, L2);
     const int y = blockIdx.y;
-    const int x0 = blockIdx.x * 32;
-    for (int e = threadIdx.x; e < 32 * L2; e += blockDim.x) {
-        const int xi = e & 31, z = e >> 5;
+    const int x0 = blockIdx.x * RC;
+    for (int e = threadIdx.x; e < RC * L2; e += NT) {
+        const int xi = e % RC, z = e / RC;
         const int x = x0 + xi;
-        T v = (T)0;
-        if (z < n2 && x < n0) v = rho[((size_t)z * n1 + y) * n0 + x];
-        T* slot = reinterpret_cast<T*>(&buf[(xi >> 1) * L2 + z]);
-        slot[xi & 1] = v;
+        T* slot = reinterpret_cast<T*>(&buf[(xi >> 1) * L2 + z]) + (xi & 1);
+        if (z < n2 && x < n0)
+            cp_elem(slot, &rho[((size_t)z * n1 + y) * n0 + x]);
+        else
+            *slot = (T)0;
     }
+    cp_async_wait_all();
     __syncthreads();
-    const C* out = block_fft<T, false>(buf, tmp, 16, pz, tw);
-    for (int e = threadIdx.x; e < 32 * (n2 + 1); e += blockDim.x) {
-        const int xi = e & 31, k = e >> 5;
+    const C* out = block_fft<T, false, LT, NC, NT>(buf, tmp, pz, tw);
+    for (int e = threadIdx.x; e < RC * (n2 + 1); e += NT) {
+        const int xi = e % RC, k = e / RC;
         const int x = x0 + xi;
         if (x >= n0) continue;
         const int q = xi >> 1;
         const C Z = out[q * L2 + k];
-        const C Zm = out[q * L2 + ((L2 - k) % L2)];
+        const C Zm = out[q * L2 + (k == 0 ? 0 : L2 - k)];
         C r;
         if ((xi & 1) == 0)
             r = C{(T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y)};
@@ -262,30 +366,34 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_r2c(const T* __restrict__ rh
 }
 
 // ---------------------------------------------------------------- pass B / D
-template <typename T, bool INV>
-__global__ void __launch_bounds__(kThreads) k_fft_y(Cx<T>* __restrict__ spec, int n0, int L0, int n_in, int n_out, FftPlan py,
-                                                    const Cx<T>* __restrict__ twy) {
+// NC x-columns of one kz plane per block; rows y < n_in in, y < n_out out.
+template <typename T, bool INV, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, int L0, int n_in, int n_out, FftPlan py,
+                                              const Cx<T>* __restrict__ twy) {
     using C = Cx<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int L1 = py.L;
+    const int L1 = LT > 0 ? LT : py.L;
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L1;
-    C* tmp = buf + 16 * L1;
-    load_twiddles<T>(tw, twy, L1);
+    C* tmp = buf + NC * L1 + 2 * NC;
+    stage_twiddles<C, NT>(tw, twy, L1);
     const int kz = blockIdx.y;
-    const int x0 = blockIdx.x * 16;
+    const int x0 = blockIdx.x * NC;
     C* plane = spec + (size_t)kz * L1 * L0;
-    for (int e = threadIdx.x; e < 16 * L1; e += blockDim.x) {
-        const int xi = e & 15, yy = e >> 4;
+    for (int e = threadIdx.x; e < NC * L1; e += NT) {
+        const int xi = e % NC, yy = e / NC;
         const int x = x0 + xi;
-        C v = C{(T)0, (T)0};
-        if (yy < n_in && x < n0) v = plane[(size_t)yy * L0 + x];
-        buf[xi * L1 + yy] = v;
+        C* slot = &buf[xi * L1 + yy];
+        if (yy < n_in && x < n0)
+            cp_elem(slot, &plane[(size_t)yy * L0 + x]);
+        else
+            *slot = C{(T)0, (T)0};
     }
+    cp_async_wait_all();
     __syncthreads();
-    const C* out = block_fft<T, INV>(buf, tmp, 16, py, tw);
-    for (int e = threadIdx.x; e < 16 * n_out; e += blockDim.x) {
-        const int xi = e & 15, yy = e >> 4;
+    const C* out = block_fft<T, INV, LT, NC, NT>(buf, tmp, py, tw);
+    for (int e = threadIdx.x; e < NC * n_out; e += NT) {
+        const int xi = e % NC, yy = e / NC;
         const int x = x0 + xi;
         if (x < n0) plane[(size_t)yy * L0 + x] = out[xi * L1 + yy];
     }
@@ -298,41 +406,43 @@ __global__ void __launch_bounds__(kThreads) k_fft_y(Cx<T>* __restrict__ spec, in
 // amplify, while rounding after the multiplication would be noise relative
 // to phi itself and is kept at FP64.  `in` and `out` alias in the plain form;
 // every block reads its rows before it writes them.
-constexpr int kRowsC = 8;
-template <typename TI, typename TO>
-__global__ void __launch_bounds__(kThreads) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0,
-                                                         int n1, int L1, long long rows, FftPlan px,
-                                                         const Cx<TI>* __restrict__ twi, const Cx<TO>* __restrict__ two) {
+template <typename TI, typename TO, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0, int n1,
+                                                   int L1, int rows, FftPlan px, const Cx<TI>* __restrict__ twi,
+                                                   const Cx<TO>* __restrict__ two) {
     using CI = Cx<TI>;
     using CO = Cx<TO>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int L0 = px.L;
+    const int L0 = LT > 0 ? LT : px.L;
     CO* tw_o = reinterpret_cast<CO*>(smem_raw);
     CI* tw_i = reinterpret_cast<CI*>(tw_o + L0);
     CO* bufo = reinterpret_cast<CO*>(tw_i + L0);
-    CO* tmpo = bufo + kRowsC * L0;
-    load_twiddles<TO>(tw_o, two, L0);
-    load_twiddles<TI>(tw_i, twi, L0);
+    CO* tmpo = bufo + NC * L0;
+    stage_twiddles<CO, NT>(tw_o, two, L0);
+    stage_twiddles<CI, NT>(tw_i, twi, L0);
     CI* bufi = reinterpret_cast<CI*>(bufo);
     CI* tmpi = reinterpret_cast<CI*>(tmpo);
-    const long long r0 = (long long)blockIdx.x * kRowsC;
-    for (int e = threadIdx.x; e < kRowsC * L0; e += blockDim.x) {
+    const int r0 = blockIdx.x * NC;
+    for (int e = threadIdx.x; e < NC * L0; e += NT) {
         const int ri = e / L0, x = e - ri * L0;
-        const long long r = r0 + ri;
-        CI v = CI{(TI)0, (TI)0};
-        if (r < rows && x < n0) v = in[(size_t)r * L0 + x];
-        bufi[ri * L0 + x] = v;
+        const int r = r0 + ri;
+        CI* slot = &bufi[ri * L0 + x];
+        if (r < rows && x < n0)
+            cp_elem(slot, &in[(size_t)r * L0 + x]);
+        else
+            *slot = CI{(TI)0, (TI)0};
     }
+    cp_async_wait_all();
     __syncthreads();
-    const CI* f = block_fft<TI, false>(bufi, tmpi, kRowsC, px, tw_i);
+    const CI* f = block_fft<TI, false, LT, NC, NT>(bufi, tmpi, px, tw_i);
     CO* g = (f == bufi) ? tmpo : bufo;
     CO* h = (f == bufi) ? bufo : tmpo;
-    for (int e = threadIdx.x; e < kRowsC * L0; e += blockDim.x) {
+    for (int e = threadIdx.x; e < NC * L0; e += NT) {
         const int ri = e / L0, kx = e - ri * L0;
-        const long long r = r0 + ri;
+        const int r = r0 + ri;
         if (r >= rows) continue;
-        const int kz = (int)(r / L1);
-        const int ky = (int)(r - (long long)kz * L1);
+        const int kz = r / L1;
+        const int ky = r - kz * L1;
         const int gy = ky <= n1 ? ky : L1 - ky;
         const int gx = kx <= n0 ? kx : L0 - kx;
         const TI gv = ghat[((size_t)kz * (n1 + 1) + gy) * (n0 + 1) + gx];
@@ -340,45 +450,52 @@ __global__ void __launch_bounds__(kThreads) k_fft_x_conv(const Cx<TI>* in, Cx<TO
         g[e] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
     }
     __syncthreads();
-    const CO* o = block_fft<TO, true>(g, h, kRowsC, px, tw_o);
-    for (int e = threadIdx.x; e < kRowsC * n0; e += blockDim.x) {
+    const CO* o = block_fft<TO, true, LT, NC, NT>(g, h, px, tw_o);
+    for (int e = threadIdx.x; e < NC * n0; e += NT) {
         const int ri = e / n0, x = e - ri * n0;
-        const long long r = r0 + ri;
+        const int r = r0 + ri;
         if (r < rows) out[(size_t)r * L0 + x] = o[ri * L0 + x];
     }
 }
 
 // ---------------------------------------------------------------- pass E
-template <typename T, bool SELF>
-__global__ void __launch_bounds__(kThreads) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
-                                                        int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz,
-                                                        const StepState* __restrict__ st, double normFact, double coupling) {
+template <typename T, bool SELF, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
+                                                  int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz,
+                                                  const StepState* __restrict__ st, double normFact, double coupling) {
     using C = Cx<T>;
+    constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int L2 = pz.L;
+    const int L2 = LT > 0 ? LT : pz.L;
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L2;
-    C* tmp = buf + 16 * L2 + 32;
-    load_twiddles<T>(tw, twz, L2);
+    C* tmp = buf + NC * L2 + RC;
+    stage_twiddles<C, NT>(tw, twz, L2);
     const int y = blockIdx.y;
-    const int x0 = blockIdx.x * 32;
-    // stage the half spectra of the 32 columns in tmp: [xi][k], k <= n2
-    for (int e = threadIdx.x; e < 32 * (n2 + 1); e += blockDim.x) {
-        const int xi = e & 31, k = e >> 5;
+    const int x0 = blockIdx.x * RC;
+    // the half spectra of the 2 NC columns in tmp: [xi][k], k <= n2
+    for (int e = threadIdx.x; e < RC * (n2 + 1); e += NT) {
+        const int xi = e % RC, k = e / RC;
         const int x = x0 + xi;
-        C v = C{(T)0, (T)0};
-        if (x < n0) v = spec[((size_t)k * L1 + y) * L0 + x];
-        if (k == 0 || k == n2) v.y = (T)0;  // the half-complex format holds no imaginary part there
-        tmp[xi * (n2 + 1) + k] = v;
+        C* slot = &tmp[xi * (n2 + 1) + k];
+        if (x < n0)
+            cp_elem(slot, &spec[((size_t)k * L1 + y) * L0 + x]);
+        else
+            *slot = C{(T)0, (T)0};
     }
+    cp_async_wait_all();
     __syncthreads();
-    for (int e = threadIdx.x; e < 16 * L2; e += blockDim.x) {
+    for (int e = threadIdx.x; e < NC * L2; e += NT) {
         const int q = e / L2, k = e - q * L2;
         const C* A = tmp + (2 * q) * (n2 + 1);
         const C* B = tmp + (2 * q + 1) * (n2 + 1);
         C z;
         if (k <= n2) {
-            const C a = A[k], b = B[k];
+            C a = A[k], b = B[k];
+            if (k == 0 || k == n2) {  // the half-complex format holds no imaginary part there
+                a.y = (T)0;
+                b.y = (T)0;
+            }
             z = C{a.x - b.y, a.y + b.x};
         } else {
             const C a = A[L2 - k], b = B[L2 - k];
@@ -387,10 +504,10 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_c2r(const Cx<T>* __restrict_
         buf[q * L2 + k] = z;
     }
     __syncthreads();
-    const C* out = block_fft<T, true>(buf, tmp, 16, pz, tw);
+    const C* out = block_fft<T, true, LT, NC, NT>(buf, tmp, pz, tw);
     const double hvol = SELF ? st->hvol : 1.0;
-    for (int e = threadIdx.x; e < 32 * n2; e += blockDim.x) {
-        const int xi = e & 31, zz = e >> 5;
+    for (int e = threadIdx.x; e < RC * n2; e += NT) {
+        const int xi = e % RC, zz = e / RC;
         const int x = x0 + xi;
         if (x >= n0) continue;
         const C v = out[(xi >> 1) * L2 + zz];
@@ -406,36 +523,41 @@ __global__ void __launch_bounds__(kThreads) k_fft_z_c2r(const Cx<T>* __restrict_
 
 // ---------------------------------------------------------------- G spectrum
 // Cosine transform of every line along one axis: Y[m] = sum over the even
-// extension (length 2(len-1)) of g, m in [0, len-1].  Lines are addressed as
-// in[b * sb + o * so + e * se]; 32 lines per block (two per complex FFT).
-template <typename TO>
-__global__ void __launch_bounds__(kThreads) k_dct_lines(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
-                                                        long long sb, long long so, long long se, FftPlan pl,
-                                                        const double2* __restrict__ twd) {
+// extension (length L = 2(len-1)) of g, m in [0, len-1].  Lines are addressed
+// as in[b * sb + o * so + e * se]; 2 NC lines per block (two per complex FFT).
+template <typename TO, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
+                                                  long long sb, long long so, long long se, FftPlan pl,
+                                                  const double2* __restrict__ twd) {
+    constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int L = pl.L;  // 2 (len - 1)
+    const int L = LT > 0 ? LT : pl.L;
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double2* buf = tw + L;
-    double2* tmp = buf + 16 * L;
-    load_twiddles<double>(tw, twd, L);
-    const int b0 = blockIdx.x * 32;
+    double2* tmp = buf + NC * L + RC;
+    stage_twiddles<double2, NT>(tw, twd, L);
+    const int b0 = blockIdx.x * RC;
     const long long obase = (long long)blockIdx.y * so;
-    for (int e = threadIdx.x; e < 32 * len; e += blockDim.x) {
-        const int li = e & 31, m = e >> 5;
+    for (int e = threadIdx.x; e < RC * len; e += NT) {
+        const int li = e % RC, m = e / RC;
         const int b = b0 + li;
-        double g = 0.0;
-        if (b < nb) g = in[(long long)b * sb + obase + (long long)m * se];
-        double* slot = reinterpret_cast<double*>(&buf[(li >> 1) * L + m]);
-        slot[li & 1] = g;
-        if (m >= 1 && m <= len - 2) {
-            double* mir = reinterpret_cast<double*>(&buf[(li >> 1) * L + (L - m)]);
-            mir[li & 1] = g;
+        double* slot = reinterpret_cast<double*>(&buf[(li >> 1) * L + m]) + (li & 1);
+        const bool inner = m >= 1 && m <= len - 2;
+        double* mir = reinterpret_cast<double*>(&buf[(li >> 1) * L + (inner ? L - m : m)]) + (li & 1);
+        if (b < nb) {
+            const double* src = in + (long long)b * sb + obase + (long long)m * se;
+            cp_elem(slot, src);
+            if (inner) cp_elem(mir, src);
+        } else {
+            *slot = 0.0;
+            if (inner) *mir = 0.0;
         }
     }
+    cp_async_wait_all();
     __syncthreads();
-    const double2* o = block_fft<double, false>(buf, tmp, 16, pl, tw);
-    for (int e = threadIdx.x; e < 32 * len; e += blockDim.x) {
-        const int li = e & 31, m = e >> 5;
+    const double2* o = block_fft<double, false, LT, NC, NT>(buf, tmp, pl, tw);
+    for (int e = threadIdx.x; e < RC * len; e += NT) {
+        const int li = e % RC, m = e / RC;
         const int b = b0 + li;
         if (b >= nb) continue;
         const double2 v = o[(li >> 1) * L + m];
@@ -443,55 +565,162 @@ __global__ void __launch_bounds__(kThreads) k_dct_lines(const double* __restrict
     }
 }
 
-template <typename T>
-size_t smem_tile(int L, int cols) {
-    return sizeof(Cx<T>) * (size_t)(L + 2 * (cols * L + 32));
+// ---------------------------------------------------------------- dispatch
+template <int LT>
+struct Geo {
+    static constexpr int NC = cols_for(LT);
+    static constexpr int NT = threads_for(LT);
+};
+
+template <typename C>
+size_t smem_of(int L, int nc) {
+    return sizeof(C) * tile_elems(L, nc);
 }
+
+template <typename TI>
+size_t smem_conv(int L, int nc) {
+    return (sizeof(double2) + sizeof(Cx<TI>)) * (size_t)L + 2 * sizeof(double2) * (size_t)nc * L;
+}
+
+// Calls f.template run<LT>() with LT the template length for L, or 0.
+template <typename F>
+void with_length(int L, F&& f) {
+    switch (L) {
+        case 32: f.template run<32>(); break;
+        case 64: f.template run<64>(); break;
+        case 96: f.template run<96>(); break;
+        case 128: f.template run<128>(); break;
+        case 256: f.template run<256>(); break;
+        default: f.template run<0>(); break;
+    }
+}
+
+template <typename T>
+struct LaunchA {
+    const T* rho;
+    Cx<T>* spec;
+    int n0, n1, n2, L0, L1;
+    FftPlan pz;
+    const Cx<T>* twz;
+    cudaStream_t s;
+    template <int LT>
+    void run() {
+        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        dim3 g((unsigned)((n0 + 2 * NC - 1) / (2 * NC)), (unsigned)n1);
+        k_fft_z_r2c<T, LT, NC, NT><<<g, NT, smem_of<Cx<T>>(pz.L, NC), s>>>(rho, spec, n0, n1, n2, L0, L1, pz, twz);
+    }
+};
+
+template <typename T, bool INV>
+struct LaunchY {
+    Cx<T>* spec;
+    int n0, L0, n_in, n_out, planes;
+    FftPlan py;
+    const Cx<T>* twy;
+    cudaStream_t s;
+    template <int LT>
+    void run() {
+        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        dim3 g((unsigned)((n0 + NC - 1) / NC), (unsigned)planes);
+        k_fft_y<T, INV, LT, NC, NT><<<g, NT, smem_of<Cx<T>>(py.L, NC), s>>>(spec, n0, L0, n_in, n_out, py, twy);
+    }
+};
+
+template <typename TI>
+struct LaunchC {
+    const Cx<TI>* in;
+    double2* out;
+    const TI* ghat;
+    int n0, n1, L1, rows;
+    FftPlan px;
+    const Cx<TI>* twi;
+    const double2* two;
+    cudaStream_t s;
+    template <int LT>
+    void run() {
+        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        k_fft_x_conv<TI, double, LT, NC, NT><<<(unsigned)((rows + NC - 1) / NC), NT, smem_conv<TI>(px.L, NC), s>>>(
+            in, out, ghat, n0, n1, L1, rows, px, twi, two);
+    }
+};
+
+template <bool SELF>
+struct LaunchE {
+    const double2* spec;
+    double* phi;
+    int n0, n1, n2, L0, L1;
+    FftPlan pz;
+    const double2* twz;
+    const StepState* st;
+    double normFact, coupling;
+    cudaStream_t s;
+    template <int LT>
+    void run() {
+        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        dim3 g((unsigned)((n0 + 2 * NC - 1) / (2 * NC)), (unsigned)n1);
+        k_fft_z_c2r<double, SELF, LT, NC, NT><<<g, NT, smem_of<double2>(pz.L, NC), s>>>(spec, phi, n0, n1, n2, L0, L1, pz,
+                                                                                          twz, st, normFact, coupling);
+    }
+};
+
+template <typename TO>
+struct LaunchDct {
+    const double* in;
+    TO* out;
+    int len, nb, outer;
+    long long sb, so, se;
+    FftPlan pl;
+    const double2* tw;
+    cudaStream_t s;
+    template <int LT>
+    void run() {
+        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        dim3 g((unsigned)((nb + 2 * NC - 1) / (2 * NC)), (unsigned)outer);
+        k_dct_lines<TO, LT, NC, NT><<<g, NT, smem_of<double2>(pl.L, NC), s>>>(in, out, len, nb, sb, so, se, pl, tw);
+    }
+};
+
+// Raises the dynamic shared-memory limit of every instance of one length.
+struct SetLimits {
+    template <typename K>
+    static void allow(K kernel) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    }
+    template <int LT>
+    void run() {
+        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        allow(k_fft_z_r2c<double, LT, NC, NT>);
+        allow(k_fft_z_r2c<float, LT, NC, NT>);
+        allow(k_fft_y<double, false, LT, NC, NT>);
+        allow(k_fft_y<float, false, LT, NC, NT>);
+        allow(k_fft_y<double, true, LT, NC, NT>);
+        allow(k_fft_x_conv<double, double, LT, NC, NT>);
+        allow(k_fft_x_conv<float, double, LT, NC, NT>);
+        allow(k_fft_z_c2r<double, true, LT, NC, NT>);
+        allow(k_fft_z_c2r<double, false, LT, NC, NT>);
+        allow(k_dct_lines<double, LT, NC, NT>);
+        allow(k_dct_lines<float, LT, NC, NT>);
+    }
+};
 
 }  // namespace
 
 FftPlan make_plan(int L) {
+    const RadixPlan r = radix_plan(L);
     FftPlan p{};
     p.L = L;
-    int m = L;
-    int ns = 0;
-    while (m % 16 == 0) {
-        p.r[ns++] = 16;
-        m /= 16;
-    }
-    if (m % 8 == 0) {
-        p.r[ns++] = 8;
-        m /= 8;
-    }
-    while (m % 4 == 0) {
-        p.r[ns++] = 4;
-        m /= 4;
-    }
-    while (m % 2 == 0) {
-        p.r[ns++] = 2;
-        m /= 2;
-    }
-    while (m % 3 == 0) {
-        p.r[ns++] = 3;
-        m /= 3;
-    }
-    while (m % 5 == 0) {
-        p.r[ns++] = 5;
-        m /= 5;
-    }
-    p.nst = (m == 1) ? ns : -1;
+    p.nst = r.nst;
+    for (int i = 0; i < 12; ++i) p.r[i] = r.r[i];
     return p;
 }
 
 size_t fft_smem_bytes(const DevBunch& b) {
-    const int L[3] = {2 * b.bc.n[0], 2 * b.bc.n[1], 2 * b.bc.n[2]};
-    const size_t cs = b.precision == 0 ? sizeof(double2) : sizeof(float2);
     size_t m = 0;
     for (int d = 0; d < 3; ++d) {
-        m = std::max(m, cs * (size_t)(L[d] + 2 * (16 * L[d] + 32)));
-        m = std::max(m, sizeof(double2) * (size_t)(L[d] + 2 * (16 * L[d] + 32)));
+        const int L = 2 * b.bc.n[d];
+        m = std::max(m, smem_of<double2>(L, cols_for(0)));
+        m = std::max(m, smem_conv<double>(L, cols_for(0)));
     }
-    m = std::max(m, (sizeof(double2) + cs) * (size_t)L[0] + 2 * sizeof(double2) * (size_t)(kRowsC * L[0]));
     return m;
 }
 
@@ -528,26 +757,18 @@ void launch_green_transform(const DevBunch& b, cudaStream_t s) {
     const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
     const long long g0 = n0 + 1, g1 = n1 + 1, g2 = n2 + 1;
     const FftPlan p0 = make_plan(2 * n0), p1 = make_plan(2 * n1), p2 = make_plan(2 * n2);
-    const size_t sm0 = smem_tile<double>(2 * n0, 16), sm1 = smem_tile<double>(2 * n1, 16), sm2 = smem_tile<double>(2 * n2, 16);
     const double2* tw0 = reinterpret_cast<const double2*>(b.tw[0]);
     const double2* tw1 = reinterpret_cast<const double2*>(b.tw[1]);
     const double2* tw2 = reinterpret_cast<const double2*>(b.tw[2]);
     // z lines: batch x (stride 1), outer y
-    dim3 gz((unsigned)((g0 + 31) / 32), (unsigned)g1);
-    k_dct_lines<double><<<gz, kThreads, sm2, s>>>(b.gline, b.gtmp, (int)g2, (int)g0, 1, g0, g0 * g1, p2, tw2);
+    with_length(2 * n2, LaunchDct<double>{b.gline, b.gtmp, (int)g2, (int)g0, (int)g1, 1, g0, g0 * g1, p2, tw2, s});
     // y lines: batch x, outer z
-    dim3 gy((unsigned)((g0 + 31) / 32), (unsigned)g2);
-    k_dct_lines<double><<<gy, kThreads, sm1, s>>>(b.gtmp, b.gline, (int)g1, (int)g0, 1, g0 * g1, g0, p1, tw1);
+    with_length(2 * n1, LaunchDct<double>{b.gtmp, b.gline, (int)g1, (int)g0, (int)g2, 1, g0 * g1, g0, p1, tw1, s});
     // x lines: batch y (stride g0), outer z
-    dim3 gx((unsigned)((g1 + 31) / 32), (unsigned)g2);
     if (b.precision == 0)
-        k_dct_lines<double><<<gx, kThreads, sm0, s>>>(b.gline, (double*)b.ghat, (int)g0, (int)g1, g0, g0 * g1, 1, p0, tw0);
+        with_length(2 * n0, LaunchDct<double>{b.gline, (double*)b.ghat, (int)g0, (int)g1, (int)g2, g0, g0 * g1, 1, p0, tw0, s});
     else
-        k_dct_lines<float><<<gx, kThreads, sm0, s>>>(b.gline, (float*)b.ghat, (int)g0, (int)g1, g0, g0 * g1, 1, p0, tw0);
-}
-
-static size_t smem_conv(int L0, size_t in_bytes) {
-    return (sizeof(double2) + in_bytes) * (size_t)L0 + 2 * sizeof(double2) * (size_t)(kRowsC * L0);
+        with_length(2 * n0, LaunchDct<float>{b.gline, (float*)b.ghat, (int)g0, (int)g1, (int)g2, g0, g0 * g1, 1, p0, tw0, s});
 }
 
 // T is the type of the forward half (A, B and the forward x transform of C);
@@ -570,25 +791,14 @@ static void convolution_t(const DevBunch& b, int mode, cudaStream_t s) {
     normFact /= L0;
     normFact /= L1;
     normFact /= L2;
-    // A
-    dim3 ga((unsigned)((n0 + 31) / 32), (unsigned)n1);
-    k_fft_z_r2c<T><<<ga, kThreads, smem_tile<T>(L2, 16), s>>>((const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz);
-    // B
-    dim3 gb((unsigned)((n0 + 15) / 16), (unsigned)(n2 + 1));
-    k_fft_y<T, false><<<gb, kThreads, smem_tile<T>(L1, 16), s>>>(fwd, n0, L0, n1, L1, py, twy);
-    // C
-    const long long rows = (long long)(n2 + 1) * L1;
-    k_fft_x_conv<T, double><<<(unsigned)((rows + kRowsC - 1) / kRowsC), kThreads, smem_conv(L0, sizeof(C)), s>>>(
-        fwd, inv, (const T*)b.ghat, n0, n1, L1, rows, px, twx, twx_d);
-    // D
-    k_fft_y<double, true><<<gb, kThreads, smem_tile<double>(L1, 16), s>>>(inv, n0, L0, L1, n1, py, twy_d);
-    // E
+    with_length(L2, LaunchA<T>{(const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz, s});
+    with_length(L1, LaunchY<T, false>{fwd, n0, L0, n1, L1, n2 + 1, py, twy, s});
+    with_length(L0, LaunchC<T>{fwd, inv, (const T*)b.ghat, n0, n1, L1, (n2 + 1) * L1, px, twx, twx_d, s});
+    with_length(L1, LaunchY<double, true>{inv, n0, L0, L1, n1, n2 + 1, py, twy_d, s});
     if (mode == kConvSelfField)
-        k_fft_z_c2r<double, true><<<ga, kThreads, smem_tile<double>(L2, 16), s>>>(inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d,
-                                                                                   b.st, normFact, b.bc.coupling);
+        with_length(L2, LaunchE<true>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact, b.bc.coupling, s});
     else
-        k_fft_z_c2r<double, false><<<ga, kThreads, smem_tile<double>(L2, 16), s>>>(inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d,
-                                                                                    b.st, normFact, b.bc.coupling);
+        with_length(L2, LaunchE<false>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact, b.bc.coupling, s});
 }
 
 void launch_convolution(const DevBunch& b, int mode, cudaStream_t s) {
@@ -599,18 +809,13 @@ void launch_convolution(const DevBunch& b, int mode, cudaStream_t s) {
 }
 
 void fft_set_smem_limits() {
-    const int big = 227 * 1024;
-    cudaFuncSetAttribute(k_fft_z_r2c<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_z_r2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_y<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_y<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_y<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_x_conv<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_x_conv<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_z_c2r<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_fft_z_c2r<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_dct_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_dct_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    SetLimits sl;
+    sl.run<32>();
+    sl.run<64>();
+    sl.run<96>();
+    sl.run<128>();
+    sl.run<256>();
+    sl.run<0>();
 }
 
 }  // namespace sc

@@ -29,7 +29,7 @@ struct DevBunch {
     int* hist;        // particles per cell (counting sort), zero between steps
     int* hist_scan;   // first sorted position of every cell
     int* scan_blocks; // chunk sums of the scan
-    // deposit: 128-bit fixed-point charge per node (lo, hi), zero between steps
+    // deposit: fixed-point charge per node as (L, H), value H 2^32 + L; zero between steps
     unsigned long long* nacc;
     // grids
     // T is double in the plain form and float in the mixed form.

@@ -276,48 +276,44 @@ __device__ __forceinline__ void cic_charge(const double* d, double q, double* v)
 }
 
 // Exact sums of the scattered charges: each charge v (|v| <= |q dt|) becomes
-// the integer t = trunc(v * 2^(56 - E)) with 2^E > 2 |q dt| (|t| < 2^55); the
-// sums are integer additions, exact, so any order gives the same total,
-// which is rounded to a double once.  The part below 2^(E - 56), about 2^-54
-// of one particle's charge, is dropped.  Inside a warp window the sum of at
-// most 32 values stays below 2^60 (int64); pieces of a cell that continue
-// across windows are joined as 96-bit integers (Fx).
-constexpr int kFxFrac = 56;
+// the integer t = rint(v * 2^(52 - E)) with 2^E > 2 |q dt|, so |t| < 2^51;
+// the sums are integer additions, exact, so any order gives the same total,
+// which is rounded to a double once.  The rounding of t is at most 2^-52 of
+// one particle's charge.
+constexpr int kFxFrac = 52;
 
 __device__ __forceinline__ int fx_exponent(double qdt) { return qdt != 0.0 ? ilogb(qdt) + 2 : 0; }
 
-// Exact sum of t (|t| < 2^55) over the lanes of `group` (every lane of the
-// group calls it with the same mask): the biased value t + 2^57 < 2^58 is
-// split into limbs of 20, 20 and 18 bits, each limb summed with redux.sync
-// (at most 32 x 2^20 < 2^32), and the limbs recombined.
-__device__ __forceinline__ long long group_sum(unsigned group, long long t) {
-    const unsigned long long b = (unsigned long long)t + (1ull << 57);
-    const unsigned l0 = __reduce_add_sync(group, (unsigned)(b & 0xfffffull));
-    const unsigned l1 = __reduce_add_sync(group, (unsigned)((b >> 20) & 0xfffffull));
-    const unsigned l2 = __reduce_add_sync(group, (unsigned)(b >> 40));
-    const unsigned long long x = (unsigned long long)l0 + ((unsigned long long)l1 << 20) + ((unsigned long long)l2 << 40) -
-                                 ((unsigned long long)__popc(group) << 57);
-    return (long long)x;
+// Exact sum of t (an integer-valued double, |t| < 2^51) over the lanes of
+// `group` (every lane of the group calls it with the same mask): t is split
+// exactly into hi = floor(t / 2^26) in [-2^25, 2^25) and lo = t - hi 2^26 in
+// [0, 2^26); the two 32-bit limbs are summed with redux.sync (at most 32
+// terms: |sum hi| < 2^30, sum lo < 2^31) and recombined in 64 bits.
+__device__ __forceinline__ long long group_sum(unsigned group, double t) {
+    const double hi = floor(t * 0x1p-26);
+    const double lo = fma(-hi, 0x1p26, t);
+    const int shi = __reduce_add_sync(group, __double2int_rz(hi));
+    const unsigned slo = __reduce_add_sync(group, __double2uint_rz(lo));
+    return (long long)shi * (1ll << 26) + (long long)slo;
 }
 
-// 128-bit two's-complement accumulator add: the low word's carry (and the
-// sign extension of a negative addend) goes to the high word.  Integer
-// addition commutes, so the final value does not depend on the order the
-// atomics are served in.
-__device__ __forceinline__ void acc_add(unsigned long long* a, long long t) {
-    const unsigned long long u = (unsigned long long)t;
-    const unsigned long long old = atomicAdd(a, u);
-    const unsigned long long carry = (old + u < old) ? 1ull : 0ull;
-    const unsigned long long ext = t < 0 ? ~0ull : 0ull;
-    if (carry + ext != 0ull) atomicAdd(a + 1, carry + ext);
+// Node accumulator: two 64-bit words (L, H) holding the value H 2^32 + L.
+// A group sum v (|v| < 2^56) adds its low 32 bits to L and its arithmetic
+// high part v >> 32 to H, both as fire-and-forget atomics (no returned value
+// is waited for).  L stays below 2^64 for fewer than 2^32 additions; H is a
+// signed sum of terms below 2^24.  Integer additions commute, so the value
+// is the same in any order.
+__device__ __forceinline__ void acc_add(unsigned long long* a, long long v) {
+    atomicAdd(a, (unsigned long long)v & 0xffffffffull);
+    atomicAdd(a + 1, (unsigned long long)(v >> 32));
 }
 
 // Charge deposit.  Each warp takes 32 consecutive particles (the arrays are
 // kept in cell order, so they share few cells), locates them (IntCIC.h:818-858),
 // groups the lanes by cell (match.any) and sums each of the 8 corner charges
-// over the group exactly (fixed point, redux.sync).  The group's leader adds
-// the 8 sums to the 128-bit integer accumulators of the 8 nodes.  No
-// floating-point value is accumulated by an atomic.
+// over the group exactly (fixed point, redux.sync).  The group's first lane
+// adds the 8 sums to the node accumulators.  No floating-point value is
+// accumulated by an atomic.
 __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
                                                       const double* __restrict__ z, StepState* st,
                                                       unsigned long long* __restrict__ acc) {
@@ -354,7 +350,7 @@ __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const doubl
         const unsigned group = __match_any_sync(kFull, key);
         long long v[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = group_sum(group, __double2ll_rz(c[k] * to_int));
+        for (int k = 0; k < 8; ++k) v[k] = group_sum(group, rint(c[k] * to_int));
         if (valid && lane == __ffs(group) - 1) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
@@ -396,7 +392,8 @@ __global__ void __launch_bounds__(kThreads) k_assemble_rho(BunchConst bc, const 
     const double unit = ldexp(1.0, fx_exponent(st->qdt) - kFxFrac);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x) {
         const ulonglong2 a = reinterpret_cast<const ulonglong2*>(acc)[c];
-        double s = acc_to_double(a.x, a.y, unit);
+        const i128 w = (i128)(long long)a.y * (i128)4294967296 + (i128)a.x;  // H 2^32 + L
+        double s = acc_to_double((unsigned long long)w, (unsigned long long)(w >> 64), unit);
         s /= dT;
         s *= tmp2;
         rho[c] = (T)s;

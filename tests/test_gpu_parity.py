@@ -1,14 +1,21 @@
 """GPU parity of the plain FP64 form against the CPU oracle, through the C ABI.
 
+The oracle runs in its exact mode here (``oracle.exact``): correctly rounded
+atan / log in the Green's function and order-independent exact particle sums
+-- the same definitions the device uses.  With the reference's own
+arithmetic (host libm, storage-order sums) the last bits of gamma_z and of
+the Green's function depend on the library and on the summation order, and
+the eight-corner cancellation of the integrated Green's function turns those
+into ~1e-11 of the field; ``test_reference_arithmetic_spread`` measures that
+spread and the golden-vector tests (made with the reference's arithmetic)
+use GOLDEN_TOL for it.
+
 Tolerances are norm-wise, max|gpu - oracle| / max|oracle|:
 
-* CIC charge density: 1e-13.  The particle arithmetic rounds like the
+* CIC charge density: RHO_TOL.  The particle arithmetic rounds like the
   reference; only the summation order of the deposit differs.
-* potential and fields: FIELD_TOL.  The integrated Green's function cancels
-  8 antiderivative values per point (up to n^3-fold), which amplifies 1-ulp
-  differences between device and glibc atan/log into ~1e-11 of the field.
-* per-particle state (R, P) after tracking: STATE_TOL, driven by the field
-  differences above through the kicks.
+* potential and fields: FIELD_TOL = 1e-12.
+* per-particle state (R, P) after tracking: STATE_TOL.
 * raw phase-space moment sums: 1e-12.  Derived rms emittances inherit the
   cancellation of the reference's one-pass formula (PartBunchBase.hpp:1549-1557):
   the tolerance is 1e-12 times the condition number sum(p^2)/(sum(p^2) - N pmean^2).
@@ -22,9 +29,16 @@ from src_b200.bunch import config_bunch, gaussian_bunch
 
 pytestmark = pytest.mark.gpu
 
-FIELD_TOL = 2e-11
+FIELD_TOL = 1e-12
 STATE_TOL = 1e-12
 RHO_TOL = 1e-13
+GOLDEN_TOL = 2e-11
+
+
+@pytest.fixture(autouse=True)
+def _oracle_exact(oracle):
+    with oracle.exact():
+        yield
 
 
 def rel(a, b):
@@ -52,7 +66,7 @@ def test_compute_potential_golden(gpu):
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "convolution_n8.npz"))
     with gpu.Context((8, 8, 8)) as c:
         phi = c.compute_potential(g["rho"], g["hr"])
-    assert rel(phi, g["phi"]) < FIELD_TOL
+    assert rel(phi, g["phi"]) < GOLDEN_TOL
 
 
 @pytest.mark.parametrize("nr", [(16, 16, 16), (24, 24, 24), (16, 24, 32), (48, 48, 48), (32, 32, 96)])
@@ -63,6 +77,16 @@ def test_compute_potential_vs_oracle(oracle, gpu, nr):
     with gpu.Context(nr) as c:
         phi = c.compute_potential(rho, hr)
     assert rel(phi, oracle.compute_potential(rho, hr)) < FIELD_TOL
+
+
+def test_reference_arithmetic_spread(oracle, gpu):
+    """The device against the oracle with the reference's own arithmetic
+    (host libm, storage-order sums): agreement to GOLDEN_TOL, the size of the
+    reference's dependence on its libm and summation order."""
+    with oracle.exact(False):
+        o, g = run_pair(oracle, gpu, 100_000, (32, 32, 32), 5)
+    assert rel(g["E"], o["dbg"]["E"]) < GOLDEN_TOL
+    assert rel(g["R"], o["R"]) < STATE_TOL and rel(g["P"], o["P"]) < STATE_TOL
 
 
 def test_compute_self_fields_vs_oracle(oracle, gpu):
@@ -116,7 +140,7 @@ def test_tracking_golden(gpu):
         E = c.field(gpu.FIELD_E)
         st = c.tracker_state()
     assert rel(R, g["R"]) < STATE_TOL and rel(P, g["P"]) < STATE_TOL
-    assert rel(E, g["E"]) < FIELD_TOL
+    assert rel(E, g["E"]) < GOLDEN_TOL
     assert st["q_macro"] == float(g["Q"]) and st["path_length"] == float(g["path_length"])
 
 
