@@ -299,6 +299,17 @@ SC_HD double div_rcp(double a, double b, double rb) {
     return fma(r, rb, q0);
 }
 
+// div_rcp without the branch: `fast` is cleared when q0 is outside the range
+// in which the result is the IEEE quotient.  Callers check `fast` once after
+// a group of quotients and redo the group with divisions if it was cleared.
+SC_HD double div_rcp_nc(double a, double b, double rb, bool& fast) {
+    const double q0 = a * rb;
+    const double aq = q0 < 0 ? -q0 : q0;
+    fast = fast && (aq > 0x1p-900 && aq < 0x1p900);
+    const double r = fma(-q0, b, a);
+    return fma(r, rb, q0);
+}
+
 // ---------------------------------------------------------------- CIC
 // Lower grid point and normalised offset of a particle (IntCIC.h:818-858 with
 // getVertexBelow, UniformCartesian.hpp:1025-1039, and getCellPosition,
@@ -335,9 +346,9 @@ SC_HD bool cic_locate(const double* hr, const double* origin, const int* n, cons
 // cic_locate with the reciprocals rhr[d] = RN(1 / hr[d]): same results.
 SC_HD bool cic_locate_r(const double* hr, const double* rhr, const double* origin, const int* n, const double* x,
                         int* lgp, double* dpos) {
-    bool ok = true;
+    bool ok = true, fast = true;
     for (int d = 0; d < 3; ++d) {
-        int i = (int)div_rcp(x[d] - origin[d], hr[d], rhr[d]);
+        int i = (int)div_rcp_nc(x[d] - origin[d], hr[d], rhr[d], fast);
         int ngp = (x[d] >= origin[d]) ? i : i - 1;
         double gpos = (ngp + 0.5) * hr[d] + origin[d];
         double delta = hr[d];
@@ -347,7 +358,7 @@ SC_HD bool cic_locate_r(const double* hr, const double* rhr, const double* origi
             gpos = gpos - delta;
         }
         double dp = x[d] - gpos;
-        dp = div_rcp(dp, delta, rhr[d]);
+        dp = div_rcp_nc(dp, delta, rhr[d], fast);
         if (l < 0) {
             ok = false;
             l = 0;
@@ -359,17 +370,24 @@ SC_HD bool cic_locate_r(const double* hr, const double* rhr, const double* origi
         lgp[d] = l;
         dpos[d] = dp;
     }
+    if (!fast) return cic_locate(hr, origin, n, x, lgp, dpos);
     return ok;
 }
 
 // push_one with s = c dt and rs = RN(1/s) precomputed: same results.
 SC_HD void push_r(double* R, const double* P, double s, double rs) {
-    double r0 = div_rcp(R[0], s, rs), r1 = div_rcp(R[1], s, rs), r2 = div_rcp(R[2], s, rs);
+    bool fast = true;
+    double r0 = div_rcp_nc(R[0], s, rs, fast), r1 = div_rcp_nc(R[1], s, rs, fast), r2 = div_rcp_nc(R[2], s, rs, fast);
     const double g = sqrt(1.0 + dot3(P, P));
     const double rg = 1.0 / g;
-    r0 += div_rcp(0.5 * P[0], g, rg);
-    r1 += div_rcp(0.5 * P[1], g, rg);
-    r2 += div_rcp(0.5 * P[2], g, rg);
+    r0 += div_rcp_nc(0.5 * P[0], g, rg, fast);
+    r1 += div_rcp_nc(0.5 * P[1], g, rg, fast);
+    r2 += div_rcp_nc(0.5 * P[2], g, rg, fast);
+    if (!fast) {
+        r0 = R[0] / s + 0.5 * P[0] / g;
+        r1 = R[1] / s + 0.5 * P[1] / g;
+        r2 = R[2] / s + 0.5 * P[2] / g;
+    }
     R[0] = r0 * s;
     R[1] = r1 * s;
     R[2] = r2 * s;

@@ -242,18 +242,23 @@ __device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* 
     for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
 }
 
+// Columns are stored with stride L + 1 elements, so that the columns of a
+// block start in different shared-memory banks.
+__host__ __device__ constexpr int col_stride(int L) { return L + 1; }
+
 // compile-time stage: length L, Ns, NC columns, NT threads
 template <typename T, int R, bool INV, int L, int NS, int NC, int NT>
 __device__ __forceinline__ void stage_c(const Cx<T>* in, Cx<T>* out, const Cx<T>* tw) {
     constexpr int NB = L / R;
     constexpr int STEP = L / (NS * R);
+    constexpr int CS = col_stride(L);
 #pragma unroll
     for (int w0 = 0; w0 < NC * NB; w0 += NT) {
         const int w = w0 + (int)threadIdx.x;
         if ((NC * NB) % NT != 0 && w >= NC * NB) break;
         const int col = w / NB;
         const int j = w - col * NB;
-        butterfly<T, R, INV>(in + col * L, out + col * L, j, NB, NS, STEP, tw);
+        butterfly<T, R, INV>(in + col * CS, out + col * CS, j, NB, NS, STEP, tw);
     }
 }
 
@@ -275,14 +280,15 @@ template <typename T, int R, bool INV>
 __device__ __forceinline__ void stage_r(const Cx<T>* in, Cx<T>* out, int L, int Ns, int ncols, const Cx<T>* tw) {
     const int nb = L / R;
     const int step = L / (Ns * R);
+    const int cs = col_stride(L);
     for (int w = threadIdx.x; w < ncols * nb; w += blockDim.x) {
         const int col = w / nb;
         const int j = w - col * nb;
-        butterfly<T, R, INV>(in + col * L, out + col * L, j, nb, Ns, step, tw);
+        butterfly<T, R, INV>(in + col * cs, out + col * cs, j, nb, Ns, step, tw);
     }
 }
 
-// Complex FFT of NC columns (buf[col * L + i]); returns the buffer holding
+// Complex FFT of NC columns (buf[col * (L + 1) + i]); returns the buffer holding
 // the result (buf or tmp).  The caller synchronises before the call.
 template <typename T, bool INV, int LT, int NC, int NT>
 __device__ __forceinline__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, const FftPlan& pl, const Cx<T>* tw) {
@@ -319,8 +325,10 @@ __device__ __forceinline__ void stage_twiddles(V* dst, const V* __restrict__ src
     for (int e = threadIdx.x; e < L; e += NT) cp_elem(dst + e, src + e);
 }
 
-// elements of one tile: twiddles (L), buf and tmp (NC L + 2 NC each)
-__host__ __device__ constexpr size_t tile_elems(int L, int nc) { return (size_t)L + 2 * ((size_t)nc * L + 2 * nc); }
+// elements of one tile: twiddles (L), buf and tmp (NC (L + 1) + 2 NC each)
+__host__ __device__ constexpr size_t tile_elems(int L, int nc) {
+    return (size_t)L + 2 * ((size_t)nc * col_stride(L) + 2 * nc);
+}
 
 // ---------------------------------------------------------------- pass A
 // 2 NC real columns (x) of one y per block, packed two per complex FFT.
@@ -331,16 +339,17 @@ __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<
     constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L2 = LT > 0 ? LT : pz.L;
+    const int CS = col_stride(L2);
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L2;
-    C* tmp = buf + NC * L2 + RC;
+    C* tmp = buf + NC * CS + RC;
     stage_twiddles<C, NT>(tw, twz, L2);
     const int y = blockIdx.y;
     const int x0 = blockIdx.x * RC;
     for (int e = threadIdx.x; e < RC * L2; e += NT) {
         const int xi = e % RC, z = e / RC;
         const int x = x0 + xi;
-        T* slot = reinterpret_cast<T*>(&buf[(xi >> 1) * L2 + z]) + (xi & 1);
+        T* slot = reinterpret_cast<T*>(&buf[(xi >> 1) * CS + z]) + (xi & 1);
         if (z < n2 && x < n0)
             cp_elem(slot, &rho[((size_t)z * n1 + y) * n0 + x]);
         else
@@ -354,8 +363,8 @@ __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<
         const int x = x0 + xi;
         if (x >= n0) continue;
         const int q = xi >> 1;
-        const C Z = out[q * L2 + k];
-        const C Zm = out[q * L2 + (k == 0 ? 0 : L2 - k)];
+        const C Z = out[q * CS + k];
+        const C Zm = out[q * CS + (k == 0 ? 0 : L2 - k)];
         C r;
         if ((xi & 1) == 0)
             r = C{(T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y)};
@@ -373,9 +382,10 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
     using C = Cx<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L1 = LT > 0 ? LT : py.L;
+    const int CS = col_stride(L1);
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L1;
-    C* tmp = buf + NC * L1 + 2 * NC;
+    C* tmp = buf + NC * CS + 2 * NC;
     stage_twiddles<C, NT>(tw, twy, L1);
     const int kz = blockIdx.y;
     const int x0 = blockIdx.x * NC;
@@ -383,7 +393,7 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
     for (int e = threadIdx.x; e < NC * L1; e += NT) {
         const int xi = e % NC, yy = e / NC;
         const int x = x0 + xi;
-        C* slot = &buf[xi * L1 + yy];
+        C* slot = &buf[xi * CS + yy];
         if (yy < n_in && x < n0)
             cp_elem(slot, &plane[(size_t)yy * L0 + x]);
         else
@@ -395,7 +405,7 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
     for (int e = threadIdx.x; e < NC * n_out; e += NT) {
         const int xi = e % NC, yy = e / NC;
         const int x = x0 + xi;
-        if (x < n0) plane[(size_t)yy * L0 + x] = out[xi * L1 + yy];
+        if (x < n0) plane[(size_t)yy * L0 + x] = out[xi * CS + yy];
     }
 }
 
@@ -414,10 +424,11 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
     using CO = Cx<TO>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L0 = LT > 0 ? LT : px.L;
+    const int CS = col_stride(L0);
     CO* tw_o = reinterpret_cast<CO*>(smem_raw);
     CI* tw_i = reinterpret_cast<CI*>(tw_o + L0);
     CO* bufo = reinterpret_cast<CO*>(tw_i + L0);
-    CO* tmpo = bufo + NC * L0;
+    CO* tmpo = bufo + NC * CS;
     stage_twiddles<CO, NT>(tw_o, two, L0);
     stage_twiddles<CI, NT>(tw_i, twi, L0);
     CI* bufi = reinterpret_cast<CI*>(bufo);
@@ -426,7 +437,7 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
     for (int e = threadIdx.x; e < NC * L0; e += NT) {
         const int ri = e / L0, x = e - ri * L0;
         const int r = r0 + ri;
-        CI* slot = &bufi[ri * L0 + x];
+        CI* slot = &bufi[ri * CS + x];
         if (r < rows && x < n0)
             cp_elem(slot, &in[(size_t)r * L0 + x]);
         else
@@ -446,15 +457,15 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
         const int gy = ky <= n1 ? ky : L1 - ky;
         const int gx = kx <= n0 ? kx : L0 - kx;
         const TI gv = ghat[((size_t)kz * (n1 + 1) + gy) * (n0 + 1) + gx];
-        const CI v = f[e];
-        g[e] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
+        const CI v = f[ri * CS + kx];
+        g[ri * CS + kx] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
     }
     __syncthreads();
     const CO* o = block_fft<TO, true, LT, NC, NT>(g, h, px, tw_o);
     for (int e = threadIdx.x; e < NC * n0; e += NT) {
         const int ri = e / n0, x = e - ri * n0;
         const int r = r0 + ri;
-        if (r < rows) out[(size_t)r * L0 + x] = o[ri * L0 + x];
+        if (r < rows) out[(size_t)r * L0 + x] = o[ri * CS + x];
     }
 }
 
@@ -467,9 +478,10 @@ __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec
     constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L2 = LT > 0 ? LT : pz.L;
+    const int CS = col_stride(L2);
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L2;
-    C* tmp = buf + NC * L2 + RC;
+    C* tmp = buf + NC * CS + RC;
     stage_twiddles<C, NT>(tw, twz, L2);
     const int y = blockIdx.y;
     const int x0 = blockIdx.x * RC;
@@ -501,7 +513,7 @@ __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec
             const C a = A[L2 - k], b = B[L2 - k];
             z = C{a.x + b.y, b.x - a.y};
         }
-        buf[q * L2 + k] = z;
+        buf[q * CS + k] = z;
     }
     __syncthreads();
     const C* out = block_fft<T, true, LT, NC, NT>(buf, tmp, pz, tw);
@@ -510,7 +522,7 @@ __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec
         const int xi = e % RC, zz = e / RC;
         const int x = x0 + xi;
         if (x >= n0) continue;
-        const C v = out[(xi >> 1) * L2 + zz];
+        const C v = out[(xi >> 1) * CS + zz];
         double r = (double)((xi & 1) ? v.y : v.x);
         r = r * normFact;
         if (SELF) {
@@ -532,18 +544,19 @@ __global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in,
     constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L = LT > 0 ? LT : pl.L;
+    const int CS = col_stride(L);
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double2* buf = tw + L;
-    double2* tmp = buf + NC * L + RC;
+    double2* tmp = buf + NC * CS + RC;
     stage_twiddles<double2, NT>(tw, twd, L);
     const int b0 = blockIdx.x * RC;
     const long long obase = (long long)blockIdx.y * so;
     for (int e = threadIdx.x; e < RC * len; e += NT) {
         const int li = e % RC, m = e / RC;
         const int b = b0 + li;
-        double* slot = reinterpret_cast<double*>(&buf[(li >> 1) * L + m]) + (li & 1);
+        double* slot = reinterpret_cast<double*>(&buf[(li >> 1) * CS + m]) + (li & 1);
         const bool inner = m >= 1 && m <= len - 2;
-        double* mir = reinterpret_cast<double*>(&buf[(li >> 1) * L + (inner ? L - m : m)]) + (li & 1);
+        double* mir = reinterpret_cast<double*>(&buf[(li >> 1) * CS + (inner ? L - m : m)]) + (li & 1);
         if (b < nb) {
             const double* src = in + (long long)b * sb + obase + (long long)m * se;
             cp_elem(slot, src);
@@ -560,7 +573,7 @@ __global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in,
         const int li = e % RC, m = e / RC;
         const int b = b0 + li;
         if (b >= nb) continue;
-        const double2 v = o[(li >> 1) * L + m];
+        const double2 v = o[(li >> 1) * CS + m];
         out[(long long)b * sb + obase + (long long)m * se] = (TO)((li & 1) ? v.y : v.x);
     }
 }
@@ -579,7 +592,7 @@ size_t smem_of(int L, int nc) {
 
 template <typename TI>
 size_t smem_conv(int L, int nc) {
-    return (sizeof(double2) + sizeof(Cx<TI>)) * (size_t)L + 2 * sizeof(double2) * (size_t)nc * L;
+    return (sizeof(double2) + sizeof(Cx<TI>)) * (size_t)L + 2 * sizeof(double2) * (size_t)nc * col_stride(L);
 }
 
 // Calls f.template run<LT>() with LT the template length for L, or 0.

@@ -28,6 +28,27 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
 
+// Per-step constants (mesh, frames) are staged once per block in shared
+// memory.  Reading them through fresh() inside a particle loop keeps the
+// compiler from hoisting all of them into registers for the whole loop
+// (which spills); each value is re-read from shared memory where it is used.
+template <typename P>
+__device__ __forceinline__ const P* fresh(const P* p) {
+    asm volatile("" : "+l"(p));
+    return p;
+}
+
+struct MeshConsts {
+    double hr[3], rhr[3], org[3];
+};
+__device__ __forceinline__ void load_mesh_consts(MeshConsts& m, const StepState* st) {
+    if (threadIdx.x < 3) {
+        m.hr[threadIdx.x] = st->hr[threadIdx.x];
+        m.rhr[threadIdx.x] = st->rhr[threadIdx.x];
+        m.org[threadIdx.x] = st->origin[threadIdx.x];
+    }
+}
+
 // ------------------------------------------------------------ reductions
 // Last-block-done: true in exactly one block, after every block's partials
 // are visible.  The caller resets the ticket.
@@ -156,8 +177,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, do
                                                             double* __restrict__ z, const double* __restrict__ px,
                                                             const double* __restrict__ py, const double* __restrict__ pz,
                                                             StepState* st, double* partials, unsigned* ticket) {
-    __shared__ Trafo r2b;
-    if (threadIdx.x == 0) r2b = st->r2b;
+    __shared__ Trafo r2b_s;
+    if (threadIdx.x == 0) r2b_s = st->r2b;
     __syncthreads();
     double v[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};  // min x,y,z, -max x,y,z
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)gridDim.x * blockDim.x) {
@@ -166,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, do
             const double P[3] = {px[i], py[i], pz[i]};
             push_r(R, P, bc.s_cdt, bc.rs_cdt);
             double b[3];
-            trafo_transform_to(r2b, R, b);
+            trafo_transform_to(*fresh(&r2b_s), R, b);
             R[0] = b[0];
             R[1] = b[1];
             R[2] = b[2];
@@ -228,12 +249,8 @@ __global__ void __launch_bounds__(kThreads) k_cell_keys(BunchConst bc, const dou
                                                         const double* __restrict__ y, const double* __restrict__ z,
                                                         StepState* st, uint32_t* __restrict__ keys,
                                                         uint32_t* __restrict__ ranks, int* __restrict__ count) {
-    __shared__ double hr[3], rhr[3], org[3];
-    if (threadIdx.x < 3) {
-        hr[threadIdx.x] = st->hr[threadIdx.x];
-        rhr[threadIdx.x] = st->rhr[threadIdx.x];
-        org[threadIdx.x] = st->origin[threadIdx.x];
-    }
+    __shared__ MeshConsts ms;
+    load_mesh_consts(ms, st);
     __syncthreads();
     bool bad = false;
     const int lane = threadIdx.x & 31;
@@ -246,7 +263,8 @@ __global__ void __launch_bounds__(kThreads) k_cell_keys(BunchConst bc, const dou
             double X[3] = {x[i], y[i], z[i]};
             int l[3];
             double d[3];
-            if (!cic_locate_r(hr, rhr, org, bc.n, X, l, d)) bad = true;
+            const MeshConsts* m = fresh(&ms);
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
             key = (uint32_t)l[0] + (uint32_t)bc.n[0] * ((uint32_t)l[1] + (uint32_t)bc.n[1] * (uint32_t)l[2]);
             keys[i] = key;
         }
@@ -317,15 +335,12 @@ __device__ __forceinline__ void acc_add(unsigned long long* a, long long v) {
 __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
                                                       const double* __restrict__ z, StepState* st,
                                                       unsigned long long* __restrict__ acc) {
-    __shared__ double hr[3], rhr[3], org[3], qdt, to_int;
-    if (threadIdx.x < 3) {
-        hr[threadIdx.x] = st->hr[threadIdx.x];
-        rhr[threadIdx.x] = st->rhr[threadIdx.x];
-        org[threadIdx.x] = st->origin[threadIdx.x];
-    }
+    __shared__ MeshConsts ms;
+    __shared__ double qdt_s, to_int_s;
+    load_mesh_consts(ms, st);
     if (threadIdx.x == 0) {
-        qdt = st->qdt;
-        to_int = ldexp(1.0, kFxFrac - fx_exponent(st->qdt));
+        qdt_s = st->qdt;
+        to_int_s = ldexp(1.0, kFxFrac - fx_exponent(st->qdt));
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -340,8 +355,9 @@ __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const doubl
             double X[3] = {x[i], y[i], z[i]};
             int l[3];
             double d[3];
-            if (!cic_locate_r(hr, rhr, org, bc.n, X, l, d)) bad = true;
-            cic_charge(d, qdt, c);
+            const MeshConsts* m = fresh(&ms);
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
+            cic_charge(d, *fresh(&qdt_s), c);
             key = (uint32_t)(l[0] + nx * l[1] + nxy * l[2]);
         } else {
 #pragma unroll
@@ -349,6 +365,8 @@ __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const doubl
         }
         const unsigned group = __match_any_sync(kFull, key);
         long long v[8];
+#pragma unroll
+        const double to_int = *fresh(&to_int_s);
 #pragma unroll
         for (int k = 0; k < 8; ++k) v[k] = group_sum(group, rint(c[k] * to_int));
         if (valid && lane == __ffs(group) - 1) {
@@ -504,7 +522,18 @@ __device__ __forceinline__ void cic_gather(const T* __restrict__ E4, const int* 
         const int a0 = k & 1, a1 = (k >> 1) & 1, a2 = (k >> 2) & 1;
         const double w = (a0 ? d[0] : u[0]) * (a1 ? d[1] : u[1]) * (a2 ? d[2] : u[2]);
         const T* p = E4 + 4 * (size_t)(b + a0 + a1 * nx + a2 * nxy);
-        const double e0 = (double)p[0], e1 = (double)p[1], e2 = (double)p[2];
+        double e0, e1, e2;
+        if constexpr (sizeof(T) == sizeof(double)) {
+            const double2 a = *reinterpret_cast<const double2*>(p);  // nodes are 32-byte aligned
+            e0 = a.x;
+            e1 = a.y;
+            e2 = (double)p[2];
+        } else {
+            const float4 a = *reinterpret_cast<const float4*>(p);  // nodes are 16-byte aligned
+            e0 = (double)a.x;
+            e1 = (double)a.y;
+            e2 = (double)a.z;
+        }
         if (k == 0) {
             Ef[0] = w * e0;
             Ef[1] = w * e1;
@@ -523,17 +552,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
                                                                   double* __restrict__ py, double* __restrict__ pz,
                                                                   const T* __restrict__ E4, StepState* st, double* partials,
                                                                   unsigned* ticket) {
-    __shared__ Trafo b2r, upd;
-    __shared__ double hr[3], rhr[3], org[3], betaC;
+    __shared__ Trafo b2r_s, upd_s;
+    __shared__ MeshConsts ms;
+    __shared__ double betaC_s;
+    load_mesh_consts(ms, st);
     if (threadIdx.x == 0) {
-        b2r = st->b2r;
-        upd = st->upd;
-        betaC = st->betaC;
-        for (int k = 0; k < 3; ++k) {
-            hr[k] = st->hr[k];
-            rhr[k] = st->rhr[k];
-            org[k] = st->origin[k];
-        }
+        b2r_s = st->b2r;
+        upd_s = st->upd;
+        betaC_s = st->betaC;
     }
     __syncthreads();
     i128 acc[3] = {0, 0, 0};
@@ -543,20 +569,24 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
         double P[3] = {px[i], py[i], pz[i]};
         int l[3];
         double d[3];
-        if (!cic_locate_r(hr, rhr, org, bc.n, X, l, d)) bad = true;
+        const MeshConsts* m = fresh(&ms);
+        if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
         double Eb[3];
         cic_gather(E4, bc.n, l, d, Eb);
+        const double betaC = *fresh(&betaC_s);
         const double Bb[3] = {0.0 - betaC * Eb[1], 0.0 + betaC * Eb[0], 0.0};
         double R[3], Ef[3], Bf[3];
-        trafo_transform_to(b2r, X, R);
-        trafo_rotate_to(b2r, Eb, Ef);
-        trafo_rotate_to(b2r, Bb, Bf);
+        const Trafo* b2r = fresh(&b2r_s);
+        trafo_transform_to(*b2r, X, R);
+        trafo_rotate_to(*b2r, Eb, Ef);
+        trafo_rotate_to(*b2r, Bb, Bf);
         if (bc.bz_ext != 0.0) Bf[2] += bc.bz_ext;
         kick_r(P, Ef, Bf, bc.ke, bc.ktn, bc.mass);
         push_r(R, P, bc.s_cdt, bc.rs_cdt);
         double Ru[3], Pu[3];
-        trafo_transform_to(upd, R, Ru);
-        trafo_rotate_to(upd, P, Pu);
+        const Trafo* upd = fresh(&upd_s);
+        trafo_transform_to(*upd, R, Ru);
+        trafo_rotate_to(*upd, P, Pu);
         x[i] = Ru[0];
         y[i] = Ru[1];
         z[i] = Ru[2];
