@@ -219,16 +219,22 @@ __device__ __forceinline__ void dft(Cx<T>* v) {
     }
 }
 
+// Shared-memory position of element i of a column: one empty slot after every
+// 8 elements.  The first Stockham stages write with strides of R elements
+// (R = 4 or 8, i.e. 64 or 128 bytes of complex double), which would put a
+// warp's stores into one or two bank groups; the skew spreads them over all.
+__host__ __device__ constexpr int sk(int i) { return i + (i >> 3); }
+
 // One Stockham autosort butterfly (radix R): butterfly j of a column reads
-// src[j + r nb], r < R, applies the twiddles W^(r k step), k = j mod Ns, and
-// writes dst[(j / Ns) Ns R + k + r Ns].
+// element j + r nb, r < R, applies the twiddles W^(r k step), k = j mod Ns,
+// and writes element (j / Ns) Ns R + k + r Ns (positions through sk()).
 template <typename T, int R, bool INV>
 __device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst, int j, int nb, int Ns,
                                           int step, const Cx<T>* __restrict__ tw) {
     using C = Cx<T>;
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
+    for (int r = 0; r < R; ++r) v[r] = src[sk(j + r * nb)];
     const int k = j % Ns;
 #pragma unroll
     for (int r = 1; r < R; ++r) {
@@ -239,12 +245,12 @@ __device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* 
     dft<T, R, INV>(v);
     const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+    for (int r = 0; r < R; ++r) dst[sk(base + r * Ns)] = v[r];
 }
 
-// Columns are stored with stride L + 1 elements, so that the columns of a
-// block start in different shared-memory banks.
-__host__ __device__ constexpr int col_stride(int L) { return L + 1; }
+// Column stride: the L skewed elements (sk(L - 1) < L + L/8) plus one, so
+// that the columns of a block also start in different banks.
+__host__ __device__ constexpr int col_stride(int L) { return L + (L >> 3) + 1; }
 
 // compile-time stage: length L, Ns, NC columns, NT threads
 template <typename T, int R, bool INV, int L, int NS, int NC, int NT>
@@ -288,7 +294,7 @@ __device__ __forceinline__ void stage_r(const Cx<T>* in, Cx<T>* out, int L, int 
     }
 }
 
-// Complex FFT of NC columns (buf[col * (L + 1) + i]); returns the buffer holding
+// Complex FFT of NC columns (element i of column col at buf[col * col_stride(L) + sk(i)]); returns the buffer holding
 // the result (buf or tmp).  The caller synchronises before the call.
 template <typename T, bool INV, int LT, int NC, int NT>
 __device__ __forceinline__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, const FftPlan& pl, const Cx<T>* tw) {
@@ -325,7 +331,7 @@ __device__ __forceinline__ void stage_twiddles(V* dst, const V* __restrict__ src
     for (int e = threadIdx.x; e < L; e += NT) cp_elem(dst + e, src + e);
 }
 
-// elements of one tile: twiddles (L), buf and tmp (NC (L + 1) + 2 NC each)
+// elements of one tile: twiddles (L), buf and tmp (NC col_stride(L) + 2 NC each)
 __host__ __device__ constexpr size_t tile_elems(int L, int nc) {
     return (size_t)L + 2 * ((size_t)nc * col_stride(L) + 2 * nc);
 }
@@ -349,7 +355,7 @@ __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<
     for (int e = threadIdx.x; e < RC * L2; e += NT) {
         const int xi = e % RC, z = e / RC;
         const int x = x0 + xi;
-        T* slot = reinterpret_cast<T*>(&buf[(xi >> 1) * CS + z]) + (xi & 1);
+        T* slot = reinterpret_cast<T*>(&buf[(xi >> 1) * CS + sk(z)]) + (xi & 1);
         if (z < n2 && x < n0)
             cp_elem(slot, &rho[((size_t)z * n1 + y) * n0 + x]);
         else
@@ -363,8 +369,8 @@ __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<
         const int x = x0 + xi;
         if (x >= n0) continue;
         const int q = xi >> 1;
-        const C Z = out[q * CS + k];
-        const C Zm = out[q * CS + (k == 0 ? 0 : L2 - k)];
+        const C Z = out[q * CS + sk(k)];
+        const C Zm = out[q * CS + sk(k == 0 ? 0 : L2 - k)];
         C r;
         if ((xi & 1) == 0)
             r = C{(T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y)};
@@ -393,7 +399,7 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
     for (int e = threadIdx.x; e < NC * L1; e += NT) {
         const int xi = e % NC, yy = e / NC;
         const int x = x0 + xi;
-        C* slot = &buf[xi * CS + yy];
+        C* slot = &buf[xi * CS + sk(yy)];
         if (yy < n_in && x < n0)
             cp_elem(slot, &plane[(size_t)yy * L0 + x]);
         else
@@ -405,7 +411,7 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
     for (int e = threadIdx.x; e < NC * n_out; e += NT) {
         const int xi = e % NC, yy = e / NC;
         const int x = x0 + xi;
-        if (x < n0) plane[(size_t)yy * L0 + x] = out[xi * CS + yy];
+        if (x < n0) plane[(size_t)yy * L0 + x] = out[xi * CS + sk(yy)];
     }
 }
 
@@ -437,7 +443,7 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
     for (int e = threadIdx.x; e < NC * L0; e += NT) {
         const int ri = e / L0, x = e - ri * L0;
         const int r = r0 + ri;
-        CI* slot = &bufi[ri * CS + x];
+        CI* slot = &bufi[ri * CS + sk(x)];
         if (r < rows && x < n0)
             cp_elem(slot, &in[(size_t)r * L0 + x]);
         else
@@ -457,15 +463,15 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
         const int gy = ky <= n1 ? ky : L1 - ky;
         const int gx = kx <= n0 ? kx : L0 - kx;
         const TI gv = ghat[((size_t)kz * (n1 + 1) + gy) * (n0 + 1) + gx];
-        const CI v = f[ri * CS + kx];
-        g[ri * CS + kx] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
+        const CI v = f[ri * CS + sk(kx)];
+        g[ri * CS + sk(kx)] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
     }
     __syncthreads();
     const CO* o = block_fft<TO, true, LT, NC, NT>(g, h, px, tw_o);
     for (int e = threadIdx.x; e < NC * n0; e += NT) {
         const int ri = e / n0, x = e - ri * n0;
         const int r = r0 + ri;
-        if (r < rows) out[(size_t)r * L0 + x] = o[ri * CS + x];
+        if (r < rows) out[(size_t)r * L0 + x] = o[ri * CS + sk(x)];
     }
 }
 
@@ -513,7 +519,7 @@ __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec
             const C a = A[L2 - k], b = B[L2 - k];
             z = C{a.x + b.y, b.x - a.y};
         }
-        buf[q * CS + k] = z;
+        buf[q * CS + sk(k)] = z;
     }
     __syncthreads();
     const C* out = block_fft<T, true, LT, NC, NT>(buf, tmp, pz, tw);
@@ -522,7 +528,7 @@ __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec
         const int xi = e % RC, zz = e / RC;
         const int x = x0 + xi;
         if (x >= n0) continue;
-        const C v = out[(xi >> 1) * CS + zz];
+        const C v = out[(xi >> 1) * CS + sk(zz)];
         double r = (double)((xi & 1) ? v.y : v.x);
         r = r * normFact;
         if (SELF) {
@@ -554,9 +560,9 @@ __global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in,
     for (int e = threadIdx.x; e < RC * len; e += NT) {
         const int li = e % RC, m = e / RC;
         const int b = b0 + li;
-        double* slot = reinterpret_cast<double*>(&buf[(li >> 1) * CS + m]) + (li & 1);
+        double* slot = reinterpret_cast<double*>(&buf[(li >> 1) * CS + sk(m)]) + (li & 1);
         const bool inner = m >= 1 && m <= len - 2;
-        double* mir = reinterpret_cast<double*>(&buf[(li >> 1) * CS + (inner ? L - m : m)]) + (li & 1);
+        double* mir = reinterpret_cast<double*>(&buf[(li >> 1) * CS + sk(inner ? L - m : m)]) + (li & 1);
         if (b < nb) {
             const double* src = in + (long long)b * sb + obase + (long long)m * se;
             cp_elem(slot, src);
@@ -573,7 +579,7 @@ __global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in,
         const int li = e % RC, m = e / RC;
         const int b = b0 + li;
         if (b >= nb) continue;
-        const double2 v = o[(li >> 1) * CS + m];
+        const double2 v = o[(li >> 1) * CS + sk(m)];
         out[(long long)b * sb + obase + (long long)m * se] = (TO)((li & 1) ? v.y : v.x);
     }
 }

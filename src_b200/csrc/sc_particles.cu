@@ -302,18 +302,22 @@ constexpr int kFxFrac = 52;
 
 __device__ __forceinline__ int fx_exponent(double qdt) { return qdt != 0.0 ? ilogb(qdt) + 2 : 0; }
 
-// Exact sum of t (an integer-valued double, |t| < 2^51) over the lanes of
-// `group` (every lane of the group calls it with the same mask): t is split
-// exactly into hi = floor(t / 2^26) in [-2^25, 2^25) and lo = t - hi 2^26 in
-// [0, 2^26); the two 32-bit limbs are summed with redux.sync (at most 32
-// terms: |sum hi| < 2^30, sum lo < 2^31) and recombined in 64 bits.
-__device__ __forceinline__ long long group_sum(unsigned group, double t) {
-    const double hi = floor(t * 0x1p-26);
-    const double lo = fma(-hi, 0x1p26, t);
-    const int shi = __reduce_add_sync(group, __double2int_rz(hi));
-    const unsigned slo = __reduce_add_sync(group, __double2uint_rz(lo));
-    return (long long)shi * (1ll << 26) + (long long)slo;
+// A fixed-point charge t (an integer-valued double, |t| < 2^51) as two exact
+// 32-bit limbs: hi = floor(t / 2^26) in [-2^25, 2^25), lo = t - hi 2^26 in
+// [0, 2^26).  Sums of up to 32 limbs fit 32 bits (|sum hi| < 2^30,
+// sum lo < 2^31) and recombine exactly in 64 bits.
+struct Limbs {
+    int hi;
+    unsigned lo;
+};
+__device__ __forceinline__ Limbs limbs_of(double t) {
+    const double h = floor(t * 0x1p-26);
+    return Limbs{__double2int_rz(h), __double2uint_rz(fma(-h, 0x1p26, t))};
 }
+__device__ __forceinline__ long long join(long long hi, long long lo) { return hi * (1ll << 26) + lo; }
+
+// Group passes per warp before a warp falls back to per-lane additions.
+constexpr int kMaxGroupPasses = 4;
 
 // Node accumulator: two 64-bit words (L, H) holding the value H 2^32 + L.
 // A group sum v (|v| < 2^56) adds its low 32 bits to L and its arithmetic
@@ -329,9 +333,12 @@ __device__ __forceinline__ void acc_add(unsigned long long* a, long long v) {
 // Charge deposit.  Each warp takes 32 consecutive particles (the arrays are
 // kept in cell order, so they share few cells), locates them (IntCIC.h:818-858),
 // groups the lanes by cell (match.any) and sums each of the 8 corner charges
-// over the group exactly (fixed point, redux.sync).  The group's first lane
-// adds the 8 sums to the node accumulators.  No floating-point value is
-// accumulated by an atomic.
+// over the group exactly (fixed point, full-warp redux.sync, one pass per
+// group of two or more lanes).  The group's first lane adds the 8 sums to the
+// node accumulators.  A sorted warp spans 2-3 cells on average at 1M
+// particles / 64^3; warps with more than kMaxGroupPasses multi-lane groups
+// (sparse regions) add per lane.  No floating-point value is accumulated by
+// an atomic.
 __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
                                                       const double* __restrict__ z, StepState* st,
                                                       unsigned long long* __restrict__ acc) {
@@ -363,17 +370,41 @@ __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const doubl
 #pragma unroll
             for (int k = 0; k < 8; ++k) c[k] = 0.0;
         }
-        const unsigned group = __match_any_sync(kFull, key);
-        long long v[8];
-#pragma unroll
         const double to_int = *fresh(&to_int_s);
+        Limbs t[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = group_sum(group, rint(c[k] * to_int));
-        if (valid && lane == __ffs(group) - 1) {
+        for (int k = 0; k < 8; ++k) t[k] = limbs_of(rint(c[k] * to_int));
+        const unsigned group = __match_any_sync(kFull, key);
+        const int gsize = __popc(group);
+        const bool leader = lane == __ffs(group) - 1;
+        // Groups of two or more lanes are summed one group per pass with
+        // full-warp redux.sync (lanes outside the group add zero); a redux
+        // whose mask differs between lanes would run once per distinct mask.
+        unsigned multi = __ballot_sync(kFull, leader && gsize > 1);
+        const bool passes = __popc(multi) <= kMaxGroupPasses;
+        // single lanes, and every lane of a warp with many small groups,
+        // add their own charges
+        if (valid && (gsize == 1 || !passes)) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const int node = (int)key + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
-                acc_add(acc + 2 * (size_t)node, v[k]);
+                acc_add(acc + 2 * (size_t)node, join(t[k].hi, t[k].lo));
+            }
+        }
+        while (passes && multi) {
+            const int ld = __ffs(multi) - 1;
+            multi &= multi - 1;
+            const bool in = (__shfl_sync(kFull, group, ld) >> lane) & 1u;
+            long long s[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                s[k] = join(__reduce_add_sync(kFull, in ? t[k].hi : 0), __reduce_add_sync(kFull, in ? t[k].lo : 0u));
+            if (valid && lane == ld) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int node = (int)key + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
+                    acc_add(acc + 2 * (size_t)node, s[k]);
+                }
             }
         }
     }
