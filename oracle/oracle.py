@@ -119,6 +119,19 @@ def fft_engine_is_own():
     return bool(lib().sco_fft_engine_is_own())
 
 
+def set_threads(n):
+    """OpenMP threads of the oracle's particle and grid loops; returns the
+    previous count."""
+    L = lib()
+    prev = int(L.sco_get_threads())
+    L.sco_set_threads(C.c_int(int(n)))
+    return prev
+
+
+def max_threads():
+    return int(lib().sco_max_threads())
+
+
 def set_exact(on=True):
     """Exact mode: correctly rounded atan / log in the Green's function
     (quad precision) and order-independent exact particle sums (terms

@@ -132,16 +132,16 @@ void enqueue_reorder(scgpu_ctx* c, cudaStream_t s) {
 void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
     DevBunch& b = c->b;
     launch_drift_to_beam(b, true, s);
-    // the reference particle and the Green's function depend only on the
-    // mesh and the tracker state: a side branch beside sort and deposit
+    // the Green's function depends only on the mesh: a side branch beside
+    // deposit, reference-particle update and reorder
     cudaEventRecord(c->ev_fork, s);
     cudaStreamWaitEvent(c->side, c->ev_fork, 0);
-    launch_advance_reference(b, c->side);
     launch_igf(b, nullptr, c->side);
     launch_green_transform(b, c->side);
     cudaEventRecord(c->ev_join, c->side);
     launch_deposit(b, s);
     launch_assemble_rho(b, s);
+    launch_advance_reference(b, s);
     if (reorder) enqueue_reorder(c, s);
     cudaStreamWaitEvent(s, c->ev_join, 0);
     launch_convolution(b, kConvSelfField, s);

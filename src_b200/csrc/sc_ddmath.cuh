@@ -65,12 +65,12 @@ SC_DDM_HD dd two_prod(double a, double b) {
 
 SC_DDM_HD dd neg(dd a) { return dd{-a.hi, -a.lo}; }
 
+// "Sloppy" double-double addition: relative error about 2^-105 (|a| + |b|) /
+// |a + b|.  Every sum below either has no cancellation, or (the residuals of
+// div) only needs its result to 2^-53 relative.
 SC_DDM_HD dd add(dd a, dd b) {
     dd s = two_sum(a.hi, b.hi);
-    const dd t = two_sum(a.lo, b.lo);
-    s.lo += t.hi;
-    s = fast_two_sum(s.hi, s.lo);
-    s.lo += t.lo;
+    s.lo += a.lo + b.lo;
     return fast_two_sum(s.hi, s.lo);
 }
 

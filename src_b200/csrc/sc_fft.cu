@@ -225,35 +225,95 @@ __device__ __forceinline__ void dft(Cx<T>* v) {
 // warp's stores into one or two bank groups; the skew spreads them over all.
 __host__ __device__ constexpr int sk(int i) { return i + (i >> 3); }
 
+// R-point DFT of inputs whose upper half v[R/2 .. R-1] is zero (the
+// zero-padded half of a forward transform's first stage).
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void dft_half(Cx<T>* v) {
+    using C = Cx<T>;
+    if constexpr (R == 2) {
+        v[1] = v[0];
+    } else if constexpr (R == 4) {
+        const C a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[2] = csub(a, b);
+        if constexpr (!INV) {
+            v[1] = C{a.x + b.y, a.y - b.x};
+            v[3] = C{a.x - b.y, a.y + b.x};
+        } else {
+            v[1] = C{a.x - b.y, a.y + b.x};
+            v[3] = C{a.x + b.y, a.y - b.x};
+        }
+    } else {
+        static_assert(R == 8, "half-input DFT for radix 2, 4, 8");
+        const T h = (T)0.70710678118654752440;
+        C a[4], b[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a[k] = b[k] = v[k];
+        if constexpr (!INV) {
+            b[1] = C{h * (b[1].x + b[1].y), h * (b[1].y - b[1].x)};
+            b[2] = C{b[2].y, -b[2].x};
+            b[3] = C{h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y)};
+        } else {
+            b[1] = C{h * (b[1].x - b[1].y), h * (b[1].y + b[1].x)};
+            b[2] = C{-b[2].y, b[2].x};
+            b[3] = C{-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y)};
+        }
+        dft<T, 4, INV>(a);
+        dft<T, 4, INV>(b);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            v[2 * m] = a[m];
+            v[2 * m + 1] = b[m];
+        }
+    }
+}
+
 // One Stockham autosort butterfly (radix R): butterfly j of a column reads
 // element j + r nb, r < R, applies the twiddles W^(r k step), k = j mod Ns,
 // and writes element (j / Ns) Ns R + k + r Ns (positions through sk()).
-template <typename T, int R, bool INV>
+// NZ < R: inputs r >= NZ are known zeros (NZ = R/2 only); NO < R: only
+// outputs r < NO are needed; FIRST: Ns = 1, all twiddles are 1.
+template <typename T, int R, bool INV, int NZ = R, int NO = R, bool FIRST = false>
 __device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst, int j, int nb, int Ns,
                                           int step, const Cx<T>* __restrict__ tw) {
     using C = Cx<T>;
+    static_assert(NZ == R || (2 * NZ == R && FIRST), "zero inputs only in a first stage");
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[sk(j + r * nb)];
-    const int k = j % Ns;
+    for (int r = 0; r < NZ; ++r) v[r] = src[sk(j + r * nb)];
+    const int k = FIRST ? 0 : j % Ns;
+    if constexpr (!FIRST) {
 #pragma unroll
-    for (int r = 1; r < R; ++r) {
-        C t = tw[r * k * step];
-        if (INV) t.y = -t.y;
-        v[r] = cmul(v[r], t);
+        for (int r = 1; r < R; ++r) {
+            C t = tw[r * k * step];
+            if (INV) t.y = -t.y;
+            v[r] = cmul(v[r], t);
+        }
     }
-    dft<T, R, INV>(v);
+    if constexpr (NZ == R)
+        dft<T, R, INV>(v);
+    else
+        dft_half<T, R, INV>(v);
     const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[sk(base + r * Ns)] = v[r];
+    for (int r = 0; r < NO; ++r) dst[sk(base + r * Ns)] = v[r];
 }
 
 // Column stride: the L skewed elements (sk(L - 1) < L + L/8) plus one, so
 // that the columns of a block also start in different banks.
 __host__ __device__ constexpr int col_stride(int L) { return L + (L >> 3) + 1; }
 
+// Pruning of a transform whose length is a template constant:
+//   kPruneNone  full transform;
+//   kPruneIn    the upper half of the input is zero (forward transforms of
+//               the zero-padded doubled grid): the first stage reads half;
+//   kPruneOut   only the lower half of the output is used (inverse
+//               transforms back to the physical octant): the last stage
+//               writes half.
+constexpr int kPruneNone = 0, kPruneIn = 1, kPruneOut = 2;
+
 // compile-time stage: length L, Ns, NC columns, NT threads
-template <typename T, int R, bool INV, int L, int NS, int NC, int NT>
+template <typename T, int R, bool INV, int L, int NS, int NC, int NT, int NZ, int NO>
 __device__ __forceinline__ void stage_c(const Cx<T>* in, Cx<T>* out, const Cx<T>* tw) {
     constexpr int NB = L / R;
     constexpr int STEP = L / (NS * R);
@@ -264,20 +324,23 @@ __device__ __forceinline__ void stage_c(const Cx<T>* in, Cx<T>* out, const Cx<T>
         if ((NC * NB) % NT != 0 && w >= NC * NB) break;
         const int col = w / NB;
         const int j = w - col * NB;
-        butterfly<T, R, INV>(in + col * CS, out + col * CS, j, NB, NS, STEP, tw);
+        butterfly<T, R, INV, NZ, NO, NS == 1>(in + col * CS, out + col * CS, j, NB, NS, STEP, tw);
     }
 }
 
-template <typename T, bool INV, int L, int S, int NS, int NC, int NT>
+template <typename T, bool INV, int L, int S, int NS, int NC, int NT, int PR>
 __device__ __forceinline__ Cx<T>* stages_c(Cx<T>* a, Cx<T>* b, const Cx<T>* tw) {
     constexpr RadixPlan P = radix_plan(L);
     if constexpr (S == P.nst) {
         return a;
     } else {
         constexpr int R = P.r[S];
-        stage_c<T, R, INV, L, NS, NC, NT>(a, b, tw);
+        constexpr bool even = R % 2 == 0;
+        constexpr int NZ = (PR == kPruneIn && S == 0 && even && R <= 8) ? R / 2 : R;
+        constexpr int NO = (PR == kPruneOut && S == P.nst - 1 && even) ? R / 2 : R;
+        stage_c<T, R, INV, L, NS, NC, NT, NZ, NO>(a, b, tw);
         __syncthreads();
-        return stages_c<T, INV, L, S + 1, NS * R, NC, NT>(b, a, tw);
+        return stages_c<T, INV, L, S + 1, NS * R, NC, NT, PR>(b, a, tw);
     }
 }
 
@@ -296,10 +359,13 @@ __device__ __forceinline__ void stage_r(const Cx<T>* in, Cx<T>* out, int L, int 
 
 // Complex FFT of NC columns (element i of column col at buf[col * col_stride(L) + sk(i)]); returns the buffer holding
 // the result (buf or tmp).  The caller synchronises before the call.
-template <typename T, bool INV, int LT, int NC, int NT>
+// With a template length the transform is pruned as PR says (the caller
+// then stages only the nonzero half, or reads only the lower half); with a
+// run-time length it is always full.
+template <typename T, bool INV, int LT, int NC, int NT, int PR = kPruneNone>
 __device__ __forceinline__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, const FftPlan& pl, const Cx<T>* tw) {
     if constexpr (LT > 0) {
-        return stages_c<T, INV, LT, 0, 1, NC, NT>(buf, tmp, tw);
+        return stages_c<T, INV, LT, 0, 1, NC, NT, PR>(buf, tmp, tw);
     } else {
         int Ns = 1;
         Cx<T>* a = buf;
@@ -352,7 +418,7 @@ __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<
     stage_twiddles<C, NT>(tw, twz, L2);
     const int y = blockIdx.y;
     const int x0 = blockIdx.x * RC;
-    for (int e = threadIdx.x; e < RC * L2; e += NT) {
+    for (int e = threadIdx.x; e < RC * (LT > 0 ? n2 : L2); e += NT) {  // the zero half is not staged when pruned
         const int xi = e % RC, z = e / RC;
         const int x = x0 + xi;
         T* slot = reinterpret_cast<T*>(&buf[(xi >> 1) * CS + sk(z)]) + (xi & 1);
@@ -363,7 +429,7 @@ __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<
     }
     cp_async_wait_all();
     __syncthreads();
-    const C* out = block_fft<T, false, LT, NC, NT>(buf, tmp, pz, tw);
+    const C* out = block_fft<T, false, LT, NC, NT, kPruneIn>(buf, tmp, pz, tw);
     for (int e = threadIdx.x; e < RC * (n2 + 1); e += NT) {
         const int xi = e % RC, k = e / RC;
         const int x = x0 + xi;
@@ -396,7 +462,7 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
     const int kz = blockIdx.y;
     const int x0 = blockIdx.x * NC;
     C* plane = spec + (size_t)kz * L1 * L0;
-    for (int e = threadIdx.x; e < NC * L1; e += NT) {
+    for (int e = threadIdx.x; e < NC * ((LT > 0 && !INV) ? n_in : L1); e += NT) {
         const int xi = e % NC, yy = e / NC;
         const int x = x0 + xi;
         C* slot = &buf[xi * CS + sk(yy)];
@@ -407,7 +473,7 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
     }
     cp_async_wait_all();
     __syncthreads();
-    const C* out = block_fft<T, INV, LT, NC, NT>(buf, tmp, py, tw);
+    const C* out = block_fft<T, INV, LT, NC, NT, INV ? kPruneOut : kPruneIn>(buf, tmp, py, tw);
     for (int e = threadIdx.x; e < NC * n_out; e += NT) {
         const int xi = e % NC, yy = e / NC;
         const int x = x0 + xi;
@@ -440,8 +506,9 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
     CI* bufi = reinterpret_cast<CI*>(bufo);
     CI* tmpi = reinterpret_cast<CI*>(tmpo);
     const int r0 = blockIdx.x * NC;
-    for (int e = threadIdx.x; e < NC * L0; e += NT) {
-        const int ri = e / L0, x = e - ri * L0;
+    const int xs = LT > 0 ? n0 : L0;  // staged length: the zero half is not staged when pruned
+    for (int e = threadIdx.x; e < NC * xs; e += NT) {
+        const int ri = e / xs, x = e - ri * xs;
         const int r = r0 + ri;
         CI* slot = &bufi[ri * CS + sk(x)];
         if (r < rows && x < n0)
@@ -451,7 +518,7 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
     }
     cp_async_wait_all();
     __syncthreads();
-    const CI* f = block_fft<TI, false, LT, NC, NT>(bufi, tmpi, px, tw_i);
+    const CI* f = block_fft<TI, false, LT, NC, NT, kPruneIn>(bufi, tmpi, px, tw_i);
     CO* g = (f == bufi) ? tmpo : bufo;
     CO* h = (f == bufi) ? bufo : tmpo;
     for (int e = threadIdx.x; e < NC * L0; e += NT) {
@@ -467,7 +534,7 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
         g[ri * CS + sk(kx)] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
     }
     __syncthreads();
-    const CO* o = block_fft<TO, true, LT, NC, NT>(g, h, px, tw_o);
+    const CO* o = block_fft<TO, true, LT, NC, NT, kPruneOut>(g, h, px, tw_o);
     for (int e = threadIdx.x; e < NC * n0; e += NT) {
         const int ri = e / n0, x = e - ri * n0;
         const int r = r0 + ri;
@@ -522,7 +589,7 @@ __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec
         buf[q * CS + sk(k)] = z;
     }
     __syncthreads();
-    const C* out = block_fft<T, true, LT, NC, NT>(buf, tmp, pz, tw);
+    const C* out = block_fft<T, true, LT, NC, NT, kPruneOut>(buf, tmp, pz, tw);
     const double hvol = SELF ? st->hvol : 1.0;
     for (int e = threadIdx.x; e < RC * n2; e += NT) {
         const int xi = e % RC, zz = e / RC;

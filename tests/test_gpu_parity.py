@@ -37,8 +37,10 @@ GOLDEN_TOL = 2e-11
 
 @pytest.fixture(autouse=True)
 def _oracle_exact(oracle):
+    prev = oracle.set_threads(oracle.max_threads())
     with oracle.exact():
         yield
+    oracle.set_threads(prev)
 
 
 def rel(a, b):
@@ -69,7 +71,8 @@ def test_compute_potential_golden(gpu):
     assert rel(phi, g["phi"]) < GOLDEN_TOL
 
 
-@pytest.mark.parametrize("nr", [(16, 16, 16), (24, 24, 24), (16, 24, 32), (48, 48, 48), (32, 32, 96)])
+@pytest.mark.parametrize("nr", [(16, 16, 16), (24, 24, 24), (16, 24, 32), (48, 48, 48), (32, 32, 96), (64, 64, 64),
+                                (128, 128, 128), (40, 20, 60)])
 def test_compute_potential_vs_oracle(oracle, gpu, nr):
     rng = np.random.default_rng(sum(nr))
     rho = np.abs(rng.standard_normal((nr[2], nr[1], nr[0])))
