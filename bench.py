@@ -34,10 +34,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_PARTICLES = 1_000_000
-MESH = 64
 DT = 1e-12
-WORKLOAD = "gaussian bunch 1e6 e-, 64^3 mesh (128^3 doubled), 1 nC, dt 1 ps, drift"
+# name -> (particles, mesh cells per axis, uniform B_z [T], description)
+WORKLOADS = {
+    "c2": (1_000_000, 64, 0.0, "gaussian bunch 1e6 e-, 64^3 mesh (128^3 doubled), 1 nC, dt 1 ps, drift"),
+    "c3": (10_000_000, 128, 0.2, "gaussian bunch 1e7 e-, 128^3 mesh (256^3 doubled), 1 nC, dt 1 ps, "
+                                 "uniform solenoid B_z = 0.2 T"),
+}
+N_PARTICLES, MESH, BZ, WORKLOAD = WORKLOADS["c2"]
 
 
 def algorithmic_bytes(N, n, precision):
@@ -213,9 +217,19 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS),
+                    help="c2: 1e6 particles / 64^3 (the default bench line); c3: 1e7 / 128^3 with B_z = 0.2 T")
+    ap.add_argument("--compare-precision", action="store_true",
+                    help="run the plain and the mixed form on the same bunch for --steps steps and report "
+                         "the mixed form's field and emittance error against FP64 (one JSON line)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global N_PARTICLES, MESH, BZ, WORKLOAD
+    N_PARTICLES, MESH, BZ, WORKLOAD = WORKLOADS[args.workload]
     world, rank, local = dist_setup()
+    if args.compare_precision:
+        compare_precision(args, local)
+        return
 
     if args.impl == "reference":
         run_reference(args, world, rank)
@@ -239,7 +253,7 @@ def main():
     ctx = scgpu.Context((MESH, MESH, MESH), precision=prec, device=local)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
-    ctx.upload(R, P, DT, Q, mass)
+    ctx.upload(R, P, DT, Q, mass, bz_ext=BZ)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
     # warm-up (also builds the step's CUDA graph)
@@ -304,7 +318,7 @@ def main():
     e0.record(stream)
     for _ in range(e2e_steps):
         ctx.upload(Rh, Ph, DT, Q, mass, t=st["t"], path_length=st["path_length"], ref_R=st["ref_R"],
-                   ref_P=st["ref_P"])
+                   ref_P=st["ref_P"], bz_ext=BZ)
         ctx.track(1)
         ctx.download(Rh, Ph)
         st = ctx.tracker_state()
@@ -322,7 +336,7 @@ def main():
     stats = torch.empty((job_steps, scgpu.NSTATS), dtype=torch.float64, pin_memory=True).numpy()
     torch.cuda.synchronize(dev)
     e0.record(stream)
-    ctx.upload(Rh, Ph, DT, Q, mass)
+    ctx.upload(Rh, Ph, DT, Q, mass, bz_ext=BZ)
     ctx.track(job_steps, stats)
     ctx.download(Rh, Ph)
     e1.record(stream)
@@ -331,7 +345,7 @@ def main():
 
     ctx.close()
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c2":
         cpu = cpu_baseline_single()
     if world > 1:
         dist.destroy_process_group()
@@ -359,6 +373,64 @@ def main():
         "clocks": clk,
         "wall_s_timed_region": wall,
         "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def compare_precision(args, local):
+    """Mixed form against the plain FP64 form on the same bunch: the field
+    error of the first solve (identical inputs), the field error after
+    --steps steps, and the largest relative difference of the normalised rms
+    emittances over all steps (per-step statistics records)."""
+    import torch
+
+    from src_b200 import scgpu
+    from src_b200.bunch import gaussian_bunch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    R0, P0 = gaussian_bunch(N_PARTICLES, bunch_id=0)
+    Q = -1e-9 / N_PARTICLES
+    mass = 0.51099892e-03 * 1.0e9
+    out = {}
+    for name, prec in (("fp64", scgpu.PLAIN_FP64), ("mixed", scgpu.MIXED)):
+        with scgpu.Context((MESH, MESH, MESH), precision=prec, device=local) as c:
+            stream = torch.cuda.current_stream(dev)
+            c.set_stream(stream.cuda_stream)
+            c.upload(R0, P0, DT, Q, mass, bz_ext=BZ)
+            first = np.zeros((1, scgpu.NSTATS))
+            c.track(1, first)
+            E1 = c.field(scgpu.FIELD_E)
+            stats = np.zeros((args.steps, scgpu.NSTATS))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            c.track(args.steps, stats)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1)
+            E = c.field(scgpu.FIELD_E)
+            R, P = c.download()
+            eps = np.array([scgpu.beam_parameters_from_stats(r, N_PARTICLES)["eps_norm"] for r in stats])
+            out[name] = dict(E1=E1, E=E, R=R, P=P, eps=eps, ms_per_step=ms / args.steps)
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+    d, m = out["fp64"], out["mixed"]
+    drift = np.abs(m["eps"] - d["eps"]) / np.abs(d["eps"])
+    line = {
+        "metric": "mixed-form error vs FP64", "workload": WORKLOAD, "steps": args.steps + 1,
+        "field_rel_err_first_solve": rel(m["E1"], d["E1"]),
+        "field_rel_err_final": rel(m["E"], d["E"]),
+        "emittance_rel_drift_max": float(drift.max()),
+        "emittance_rel_drift_final": [float(v) for v in drift[-1]],
+        "eps_norm_final_fp64": [float(v) for v in d["eps"][-1]],
+        "R_rel_err_final": rel(m["R"], d["R"]), "P_rel_err_final": rel(m["P"], d["P"]),
+        "ms_per_step": {"fp64": d["ms_per_step"], "mixed": m["ms_per_step"]},
+        "speedup_mixed_over_fp64": d["ms_per_step"] / m["ms_per_step"],
+        "bounds": {"field": 1e-5, "emittance_drift": 1e-6},
+        "norms": "max|mixed - fp64| / max|fp64| over all mesh points (E) or particles (R, P)",
     }
     print(json.dumps(line), flush=True)
 

@@ -259,3 +259,23 @@ def test_mixed_form_against_fp64(gpu, oracle, n, npart):
     assert rel(rm, rd) < 1e-6
     assert rel(Rm, Rd) < 1e-7 and rel(Pm, Pd) < 1e-7
     np.testing.assert_allclose(bm["eps_norm"], bd["eps_norm"], rtol=1e-6)
+
+
+def test_mixed_form_long_run_bounds(gpu, oracle):
+    """Mixed form over 200 steps with the uniform solenoid field: the field
+    stays within 1e-5 and the normalised emittances within 1e-6 (relative)
+    of the FP64 form at every step."""
+    N, n, steps = 200_000, 32, 200
+    R, P = gaussian_bunch(N, bunch_id=21)
+    out = {}
+    for prec in (gpu.PLAIN_FP64, gpu.MIXED):
+        with gpu.Context((n, n, n), precision=prec) as c:
+            c.upload(R, P, 1e-12, -1e-9 / N, oracle.electron_mass_ev(), bz_ext=0.2)
+            stats = np.zeros((steps, gpu.NSTATS))
+            c.track(steps, stats)
+            eps = np.array([gpu.beam_parameters_from_stats(r, N)["eps_norm"] for r in stats])
+            out[prec] = (c.field(gpu.FIELD_E), eps)
+    Ed, epsd = out[gpu.PLAIN_FP64]
+    Em, epsm = out[gpu.MIXED]
+    assert rel(Em, Ed) < 1e-5
+    assert np.max(np.abs(epsm - epsd) / np.abs(epsd)) < 1e-6
