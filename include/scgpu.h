@@ -190,6 +190,46 @@ int scgpu_profile_track(scgpu_ctx* ctx, int nsteps, double* phase_ms);
 /* number of kernels one tracking step launches (from the step's CUDA graph) */
 int scgpu_kernels_per_step(scgpu_ctx* ctx);
 
+/* ------------------------------------------------------------------ batches
+ * Many independent bunches that step together: every batched step launches
+ * each kernel of the step once for all bunches (blocks index a device work
+ * table of (bunch, block)), grouped by transform length for the FFT passes,
+ * and the whole step is one CUDA graph launch while the membership is
+ * unchanged.  This replaces running one tracker per design point, as the
+ * reference's optimizer does (optimizer/Pilot/Worker.h:31-190 calling
+ * OpalSimulation::run, src/Optimize/OpalSimulation.cpp:232); the reference
+ * has no batched step.  Each bunch lives in its own context (a slot), so the
+ * single-bunch calls (scgpu_bunch_download, scgpu_get_tracker_state,
+ * scgpu_beam_parameters, scgpu_get_field) work on scgpu_batch_member().
+ * Results do not depend on the batch's membership or tuning: all sums are
+ * exact and no kernel mixes bunches.  A batch is not thread-safe. */
+typedef struct scgpu_batch scgpu_batch;
+/* precision: SCGPU_PLAIN_FP64 or SCGPU_MIXED for every bunch of the batch */
+int scgpu_batch_create(scgpu_batch** out, int device, int precision);
+void scgpu_batch_destroy(scgpu_batch* batch);
+const char* scgpu_batch_last_error(const scgpu_batch* batch);
+/* Adds a bunch (mesh from p; p->precision is ignored) and uploads it as
+ * scgpu_bunch_upload does; returns its slot (>= 0) or a negative status. */
+int scgpu_batch_add(scgpu_batch* batch, const scgpu_solver_params* p, long long n, const double* R, const double* P,
+                    const scgpu_bunch_params* bp);
+int scgpu_batch_remove(scgpu_batch* batch, int slot);
+/* the context of an occupied slot (NULL otherwise); owned by the batch */
+scgpu_ctx* scgpu_batch_member(scgpu_batch* batch, int slot);
+int scgpu_batch_size(const scgpu_batch* batch);
+/* every occupied slot advances nsteps ParallelTTracker steps */
+int scgpu_batch_track(scgpu_batch* batch, int nsteps);
+double scgpu_batch_last_track_ms(const scgpu_batch* batch);
+/* Tuning of the batched launches: threads per block of the deposit (128,
+ * 256 or 512) and, per transform length L, the FFT tile shape (0: the
+ * single-bunch shape, 1: half as many columns per block). */
+int scgpu_batch_set_tuning(scgpu_batch* batch, int deposit_threads, int L, int fft_variant);
+int scgpu_batch_get_tuning(const scgpu_batch* batch, int L, int* deposit_threads, int* fft_variant);
+/* The autotuner: times trial_steps batched steps per candidate (deposit block
+ * size, then the FFT tile shape of every transform length present) and keeps
+ * the fastest.  The trial steps advance the bunches like scgpu_batch_track
+ * (tuning never changes results); the number of steps taken is returned. */
+int scgpu_batch_autotune(scgpu_batch* batch, int trial_steps);
+
 /* The open-boundary Poisson solve of scgpu_compute_potential_device for
  * callers that cannot allocate device memory -- hosts whose device memory is
  * owned by their own pool allocator, or loops that cannot afford the device

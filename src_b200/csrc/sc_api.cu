@@ -7,32 +7,9 @@
 #include <string>
 #include <vector>
 
-#include "scgpu.h"
-#include "sc_internal.h"
+#include "sc_ctx.h"
 
 using namespace sc;
-
-struct scgpu_ctx {
-    int device = 0;
-    scgpu_solver_params sp{};
-    DevBunch b{};
-    cudaStream_t stream = nullptr;   // work stream (own or the caller's)
-    cudaStream_t own = nullptr;
-    cudaStream_t side = nullptr;     // Green's function branch
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
-    long long capacity = 0;
-    long long n = 0;
-    bool have_bunch = false;
-    bool have_solve = false;
-    int digit_bits = 0;
-    std::string err;
-    double last_ms = 0.0;
-    cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [stats][reorder]
-    bool use_graphs = true;
-    int reorder_every = 16;   // put the particle arrays in cell order every k steps (0: never)
-    long long steps_done = 0; // steps since the last upload
-    size_t smem_fft = 0;
-};
 
 namespace {
 
@@ -161,6 +138,15 @@ int build_graph(scgpu_ctx* c, bool stats, bool reorder, cudaGraphExec_t* out) {
     return SCGPU_OK;
 }
 
+int status_from_flags(scgpu_ctx* c, int err) {
+    if (!err) return SCGPU_OK;
+    if (err & kFlagMesh) return fail(c, SCGPU_ERR_MESH, "boundp: h <= 0, cannot build a mesh");
+    if (err & kFlagFrame) return fail(c, SCGPU_ERR_FRAME, "getQuaternion: anti-parallel or null vector");
+    if (err & kFlagGuard) return fail(c, SCGPU_ERR_GUARD, "a CIC stencil left the mesh");
+    if (err & kFlagSort) return fail(c, SCGPU_ERR_CUDA, "cell sort: scatter position out of range");
+    return fail(c, SCGPU_ERR_CUDA, "unknown device error flag");
+}
+
 int check_device_err(scgpu_ctx* c) {
     int err = 0;
     CK(cudaMemcpyAsync(&err, &c->b.st->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -169,13 +155,8 @@ int check_device_err(scgpu_ctx* c) {
         int zero = 0;
         cudaMemcpyAsync(&c->b.st->err, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream);
         cudaStreamSynchronize(c->stream);
-        if (err & kFlagMesh) return fail(c, SCGPU_ERR_MESH, "boundp: h <= 0, cannot build a mesh");
-        if (err & kFlagFrame) return fail(c, SCGPU_ERR_FRAME, "getQuaternion: anti-parallel or null vector");
-        if (err & kFlagGuard) return fail(c, SCGPU_ERR_GUARD, "a CIC stencil left the mesh");
-        if (err & kFlagSort) return fail(c, SCGPU_ERR_CUDA, "cell sort: scatter position out of range");
-        return fail(c, SCGPU_ERR_CUDA, "unknown device error flag");
     }
-    return SCGPU_OK;
+    return status_from_flags(c, err);
 }
 
 // calcBeamParameters from the moment sums (PartBunchBase.hpp:1529-1614)
@@ -243,6 +224,12 @@ void enqueue_green(scgpu_ctx* c, cudaStream_t s) {
 }
 
 }  // namespace
+
+namespace sc {
+int ctx_fail(scgpu_ctx* c, int code, const std::string& what) { return fail(c, code, what); }
+void ctx_enqueue_reorder(scgpu_ctx* c, cudaStream_t s) { enqueue_reorder(c, s); }
+int ctx_status_from_flags(scgpu_ctx* c, int flags) { return status_from_flags(c, flags); }
+}  // namespace sc
 
 extern "C" {
 

@@ -1,0 +1,42 @@
+// sc_ctx.h -- the context behind an scgpu_ctx handle, shared by the C ABI
+// translation units (sc_api.cu: one bunch; sc_batch.cu: many bunches that
+// step together, each held in its own context).
+#pragma once
+
+#include <string>
+
+#include "scgpu.h"
+#include "sc_internal.h"
+
+struct scgpu_ctx {
+    int device = 0;
+    scgpu_solver_params sp{};
+    sc::DevBunch b{};
+    cudaStream_t stream = nullptr;   // work stream (own or the caller's)
+    cudaStream_t own = nullptr;
+    cudaStream_t side = nullptr;     // Green's function branch
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+    long long capacity = 0;
+    long long n = 0;
+    bool have_bunch = false;
+    bool have_solve = false;
+    int digit_bits = 0;
+    std::string err;
+    double last_ms = 0.0;
+    cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [stats][reorder]
+    bool use_graphs = true;
+    int reorder_every = 16;   // put the particle arrays in cell order every k steps (0: never)
+    long long steps_done = 0; // steps since the last upload
+    size_t smem_fft = 0;
+};
+
+namespace sc {
+
+// Records `what` as the context's last error and returns `code`.
+int ctx_fail(scgpu_ctx* c, int code, const std::string& what);
+// Counting sort of the particle arrays into cell order (enqueued on s).
+void ctx_enqueue_reorder(scgpu_ctx* c, cudaStream_t s);
+// Turns a device error flag word into a status code (and clears the flag).
+int ctx_status_from_flags(scgpu_ctx* c, int flags);
+
+}  // namespace sc

@@ -405,8 +405,9 @@ __host__ __device__ constexpr size_t tile_elems(int L, int nc) {
 // ---------------------------------------------------------------- pass A
 // 2 NC real columns (x) of one y per block, packed two per complex FFT.
 template <typename T, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1, int n2,
-                                                  int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz) {
+__device__ __forceinline__ void fft_z_r2c_body(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1, int n2,
+                                               int L0, int L1, const FftPlan& pz, const Cx<T>* __restrict__ twz, int bx,
+                                               int by) {
     using C = Cx<T>;
     constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -416,8 +417,8 @@ __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<
     C* buf = tw + L2;
     C* tmp = buf + NC * CS + RC;
     stage_twiddles<C, NT>(tw, twz, L2);
-    const int y = blockIdx.y;
-    const int x0 = blockIdx.x * RC;
+    const int y = by;
+    const int x0 = bx * RC;
     for (int e = threadIdx.x; e < RC * (LT > 0 ? n2 : L2); e += NT) {  // the zero half is not staged when pruned
         const int xi = e % RC, z = e / RC;
         const int x = x0 + xi;
@@ -445,12 +446,17 @@ __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<
         spec[((size_t)k * L1 + y) * L0 + x] = r;
     }
 }
+template <typename T, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1, int n2,
+                                                  int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz) {
+    fft_z_r2c_body<T, LT, NC, NT>(rho, spec, n0, n1, n2, L0, L1, pz, twz, blockIdx.x, blockIdx.y);
+}
 
 // ---------------------------------------------------------------- pass B / D
 // NC x-columns of one kz plane per block; rows y < n_in in, y < n_out out.
 template <typename T, bool INV, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, int L0, int n_in, int n_out, FftPlan py,
-                                              const Cx<T>* __restrict__ twy) {
+__device__ __forceinline__ void fft_y_body(Cx<T>* __restrict__ spec, int n0, int L0, int n_in, int n_out, const FftPlan& py,
+                                           const Cx<T>* __restrict__ twy, int bx, int by) {
     using C = Cx<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L1 = LT > 0 ? LT : py.L;
@@ -459,8 +465,8 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
     C* buf = tw + L1;
     C* tmp = buf + NC * CS + 2 * NC;
     stage_twiddles<C, NT>(tw, twy, L1);
-    const int kz = blockIdx.y;
-    const int x0 = blockIdx.x * NC;
+    const int kz = by;
+    const int x0 = bx * NC;
     C* plane = spec + (size_t)kz * L1 * L0;
     for (int e = threadIdx.x; e < NC * ((LT > 0 && !INV) ? n_in : L1); e += NT) {
         const int xi = e % NC, yy = e / NC;
@@ -480,6 +486,11 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
         if (x < n0) plane[(size_t)yy * L0 + x] = out[xi * CS + sk(yy)];
     }
 }
+template <typename T, bool INV, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, int L0, int n_in, int n_out, FftPlan py,
+                                              const Cx<T>* __restrict__ twy) {
+    fft_y_body<T, INV, LT, NC, NT>(spec, n0, L0, n_in, n_out, py, twy, blockIdx.x, blockIdx.y);
+}
 
 // ---------------------------------------------------------------- pass C
 // The forward transform and the multiplication run in TI, the inverse in TO.
@@ -489,9 +500,9 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
 // to phi itself and is kept at FP64.  `in` and `out` alias in the plain form;
 // every block reads its rows before it writes them.
 template <typename TI, typename TO, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0, int n1,
-                                                   int L1, int rows, FftPlan px, const Cx<TI>* __restrict__ twi,
-                                                   const Cx<TO>* __restrict__ two) {
+__device__ __forceinline__ void fft_x_conv_body(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0, int n1,
+                                                int L1, int rows, const FftPlan& px, const Cx<TI>* __restrict__ twi,
+                                                const Cx<TO>* __restrict__ two, int bx) {
     using CI = Cx<TI>;
     using CO = Cx<TO>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -505,7 +516,7 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
     stage_twiddles<CI, NT>(tw_i, twi, L0);
     CI* bufi = reinterpret_cast<CI*>(bufo);
     CI* tmpi = reinterpret_cast<CI*>(tmpo);
-    const int r0 = blockIdx.x * NC;
+    const int r0 = bx * NC;
     const int xs = LT > 0 ? n0 : L0;  // staged length: the zero half is not staged when pruned
     for (int e = threadIdx.x; e < NC * xs; e += NT) {
         const int ri = e / xs, x = e - ri * xs;
@@ -541,12 +552,19 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
         if (r < rows) out[(size_t)r * L0 + x] = o[ri * CS + sk(x)];
     }
 }
+template <typename TI, typename TO, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0, int n1,
+                                                   int L1, int rows, FftPlan px, const Cx<TI>* __restrict__ twi,
+                                                   const Cx<TO>* __restrict__ two) {
+    fft_x_conv_body<TI, TO, LT, NC, NT>(in, out, ghat, n0, n1, L1, rows, px, twi, two, blockIdx.x);
+}
 
 // ---------------------------------------------------------------- pass E
 template <typename T, bool SELF, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
-                                                  int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz,
-                                                  const StepState* __restrict__ st, double normFact, double coupling) {
+__device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
+                                               int n2, int L0, int L1, const FftPlan& pz, const Cx<T>* __restrict__ twz,
+                                               const StepState* __restrict__ st, double normFact, double coupling, int bx,
+                                               int by) {
     using C = Cx<T>;
     constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -556,8 +574,8 @@ __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec
     C* buf = tw + L2;
     C* tmp = buf + NC * CS + RC;
     stage_twiddles<C, NT>(tw, twz, L2);
-    const int y = blockIdx.y;
-    const int x0 = blockIdx.x * RC;
+    const int y = by;
+    const int x0 = bx * RC;
     // the half spectra of the 2 NC columns in tmp: [xi][k], k <= n2
     for (int e = threadIdx.x; e < RC * (n2 + 1); e += NT) {
         const int xi = e % RC, k = e / RC;
@@ -605,15 +623,22 @@ __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec
         phi[((size_t)zz * n1 + y) * n0 + x] = r;
     }
 }
+template <typename T, bool SELF, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
+                                                  int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz,
+                                                  const StepState* __restrict__ st, double normFact, double coupling) {
+    fft_z_c2r_body<T, SELF, LT, NC, NT>(spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling, blockIdx.x,
+                                        blockIdx.y);
+}
 
 // ---------------------------------------------------------------- G spectrum
 // Cosine transform of every line along one axis: Y[m] = sum over the even
 // extension (length L = 2(len-1)) of g, m in [0, len-1].  Lines are addressed
 // as in[b * sb + o * so + e * se]; 2 NC lines per block (two per complex FFT).
 template <typename TO, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
-                                                  long long sb, long long so, long long se, FftPlan pl,
-                                                  const double2* __restrict__ twd) {
+__device__ __forceinline__ void dct_lines_body(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
+                                               long long sb, long long so, long long se, const FftPlan& pl,
+                                               const double2* __restrict__ twd, int bx, int by) {
     constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L = LT > 0 ? LT : pl.L;
@@ -622,8 +647,8 @@ __global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in,
     double2* buf = tw + L;
     double2* tmp = buf + NC * CS + RC;
     stage_twiddles<double2, NT>(tw, twd, L);
-    const int b0 = blockIdx.x * RC;
-    const long long obase = (long long)blockIdx.y * so;
+    const int b0 = bx * RC;
+    const long long obase = (long long)by * so;
     for (int e = threadIdx.x; e < RC * len; e += NT) {
         const int li = e % RC, m = e / RC;
         const int b = b0 + li;
@@ -649,6 +674,12 @@ __global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in,
         const double2 v = o[(li >> 1) * CS + sk(m)];
         out[(long long)b * sb + obase + (long long)m * se] = (TO)((li & 1) ? v.y : v.x);
     }
+}
+template <typename TO, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
+                                                  long long sb, long long so, long long se, FftPlan pl,
+                                                  const double2* __restrict__ twd) {
+    dct_lines_body<TO, LT, NC, NT>(in, out, len, nb, sb, so, se, pl, twd, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------- dispatch
@@ -789,7 +820,188 @@ struct SetLimits {
     }
 };
 
+// ---------------------------------------------------------------- batches
+// Tile-shape variants of a length for batched launches: V = 0 is the
+// single-bunch shape (cols_for), V = 1 half as many columns per block (more,
+// smaller blocks; the autotuner picks per length).
+__host__ __device__ constexpr int cols_v(int LT, int V) {
+    const int c = cols_for(LT);
+    return V == 0 ? c : (c > 1 ? c / 2 : 1);
+}
+__host__ __device__ constexpr int threads_v(int LT, int V) {
+    if (LT == 0) return 256;
+    const int t = cols_v(LT, V) * (LT / min_radix(LT));
+    return t < 32 ? 32 : t;
+}
+
+__device__ __forceinline__ FftPlan plan_dev(int L) {
+    const RadixPlan r = radix_plan(L);
+    FftPlan p;
+    p.L = L;
+    p.nst = r.nst;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) p.r[i] = r.r[i];
+    return p;
+}
+
+// twiddles of axis a as complex T (the float table follows the double one)
+template <typename T>
+__device__ __forceinline__ const Cx<T>* tw_dev(const DevBunch& d, int a) {
+    const double2* p = reinterpret_cast<const double2*>(d.tw[a]);
+    if constexpr (sizeof(T) == sizeof(double))
+        return reinterpret_cast<const Cx<T>*>(p);
+    else
+        return reinterpret_cast<const Cx<T>*>(p + 2 * d.bc.n[a]);
+}
+
+// One kernel per pass: block i runs the single-bunch body for bunch work[i].x
+// at block coordinates (work[i].y, work[i].z), with that bunch's sizes and
+// buffers (T: the forward-half type, as in convolution_t).
+template <typename T, int PASS, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_fft_pass_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    const int n0 = d.bc.n[0], n1 = d.bc.n[1], n2 = d.bc.n[2];
+    const int L0 = 2 * n0, L1 = 2 * n1, L2 = 2 * n2;
+    Cx<T>* fwd = reinterpret_cast<Cx<T>*>(d.precision == 0 ? d.spec : d.spec_lo);
+    double2* inv = reinterpret_cast<double2*>(d.spec);
+    if constexpr (PASS == kPassZR2C) {
+        fft_z_r2c_body<T, LT, NC, NT>((const T*)d.rho, fwd, n0, n1, n2, L0, L1, plan_dev(L2), tw_dev<T>(d, 2), w.y, w.z);
+    } else if constexpr (PASS == kPassYFwd) {
+        fft_y_body<T, false, LT, NC, NT>(fwd, n0, L0, n1, L1, plan_dev(L1), tw_dev<T>(d, 1), w.y, w.z);
+    } else if constexpr (PASS == kPassXConv) {
+        fft_x_conv_body<T, double, LT, NC, NT>(fwd, inv, (const T*)d.ghat, n0, n1, L1, (n2 + 1) * L1, plan_dev(L0),
+                                               tw_dev<T>(d, 0), tw_dev<double>(d, 0), w.y);
+    } else if constexpr (PASS == kPassYInv) {
+        fft_y_body<double, true, LT, NC, NT>(inv, n0, L0, L1, n1, plan_dev(L1), tw_dev<double>(d, 1), w.y, w.z);
+    } else if constexpr (PASS == kPassZC2R) {
+        double normFact = 1.0;
+        normFact /= L0;
+        normFact /= L1;
+        normFact /= L2;
+        fft_z_c2r_body<double, true, LT, NC, NT>(inv, d.phi, n0, n1, n2, L0, L1, plan_dev(L2), tw_dev<double>(d, 2), d.st,
+                                                 normFact, d.bc.coupling, w.y, w.z);
+    } else {
+        const long long g0 = n0 + 1, g1 = n1 + 1, g2 = n2 + 1;
+        if constexpr (PASS == kPassDctZ)
+            dct_lines_body<double, LT, NC, NT>(d.gline, d.gtmp, (int)g2, (int)g0, 1, g0, g0 * g1, plan_dev(L2),
+                                               tw_dev<double>(d, 2), w.y, w.z);
+        else if constexpr (PASS == kPassDctY)
+            dct_lines_body<double, LT, NC, NT>(d.gtmp, d.gline, (int)g1, (int)g0, 1, g0 * g1, g0, plan_dev(L1),
+                                               tw_dev<double>(d, 1), w.y, w.z);
+        else
+            dct_lines_body<T, LT, NC, NT>(d.gline, (T*)d.ghat, (int)g0, (int)g1, g0, g0 * g1, 1, plan_dev(L0),
+                                          tw_dev<double>(d, 0), w.y, w.z);
+    }
+}
+
+template <typename T, int PASS>
+size_t pass_smem(int L, int nc) {
+    if constexpr (PASS == kPassXConv) return smem_conv<T>(L, nc);
+    if constexpr (PASS == kPassZR2C || PASS == kPassYFwd) return smem_of<Cx<T>>(L, nc);
+    return smem_of<double2>(L, nc);
+}
+
+template <typename T, int PASS, int V>
+struct LaunchPassBatch {
+    const DevBunch* tab;
+    const int4* work;
+    int n, L;
+    cudaStream_t s;
+    template <int LT>
+    void run() {
+        constexpr int NC = cols_v(LT, V), NT = threads_v(LT, V);
+        auto k = k_fft_pass_batch<T, PASS, LT, NC, NT>;
+        const size_t sm = pass_smem<T, PASS>(L, NC);
+        static bool limits = [&] {
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+            return true;
+        }();
+        (void)limits;
+        k<<<n, NT, sm, s>>>(tab, work);
+    }
+};
+
+template <typename T, int PASS>
+void pass_batch_t(int L, int variant, const DevBunch* tab, const int4* work, int n, cudaStream_t s) {
+    if (variant == 0)
+        with_length(L, LaunchPassBatch<T, PASS, 0>{tab, work, n, L, s});
+    else
+        with_length(L, LaunchPassBatch<T, PASS, 1>{tab, work, n, L, s});
+}
+
+template <typename T>
+void pass_batch(int pass, int L, int variant, const DevBunch* tab, const int4* work, int n, cudaStream_t s) {
+    switch (pass) {
+        case kPassZR2C: pass_batch_t<T, kPassZR2C>(L, variant, tab, work, n, s); break;
+        case kPassYFwd: pass_batch_t<T, kPassYFwd>(L, variant, tab, work, n, s); break;
+        case kPassXConv: pass_batch_t<T, kPassXConv>(L, variant, tab, work, n, s); break;
+        case kPassYInv: pass_batch_t<T, kPassYInv>(L, variant, tab, work, n, s); break;
+        case kPassZC2R: pass_batch_t<T, kPassZC2R>(L, variant, tab, work, n, s); break;
+        case kPassDctZ: pass_batch_t<T, kPassDctZ>(L, variant, tab, work, n, s); break;
+        case kPassDctY: pass_batch_t<T, kPassDctY>(L, variant, tab, work, n, s); break;
+        default: pass_batch_t<T, kPassDctX>(L, variant, tab, work, n, s); break;
+    }
+}
+
+inline bool special_length(int L) { return L == 32 || L == 64 || L == 96 || L == 128 || L == 256; }
+
 }  // namespace
+
+int fft_pass_length(int pass, const DevBunch& b) {
+    switch (pass) {
+        case kPassZR2C:
+        case kPassZC2R:
+        case kPassDctZ: return 2 * b.bc.n[2];
+        case kPassYFwd:
+        case kPassYInv:
+        case kPassDctY: return 2 * b.bc.n[1];
+        default: return 2 * b.bc.n[0];
+    }
+}
+
+void fft_pass_grid(int pass, const DevBunch& b, int variant, int* gx, int* gy) {
+    const int L = fft_pass_length(pass, b);
+    const int nc = cols_v(special_length(L) ? L : 0, variant);
+    const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    switch (pass) {
+        case kPassZR2C:
+        case kPassZC2R:
+            *gx = (n0 + 2 * nc - 1) / (2 * nc);
+            *gy = n1;
+            break;
+        case kPassYFwd:
+        case kPassYInv:
+            *gx = (n0 + nc - 1) / nc;
+            *gy = n2 + 1;
+            break;
+        case kPassXConv:
+            *gx = ((n2 + 1) * 2 * n1 + nc - 1) / nc;
+            *gy = 1;
+            break;
+        case kPassDctZ:
+            *gx = (n0 + 1 + 2 * nc - 1) / (2 * nc);
+            *gy = n1 + 1;
+            break;
+        case kPassDctY:
+            *gx = (n0 + 1 + 2 * nc - 1) / (2 * nc);
+            *gy = n2 + 1;
+            break;
+        default:
+            *gx = (n1 + 1 + 2 * nc - 1) / (2 * nc);
+            *gy = n2 + 1;
+            break;
+    }
+}
+
+void launch_fft_pass_batch(int pass, int L, int precision, int variant, const DevBunch* tab, const int4* work, int n,
+                           cudaStream_t s) {
+    if (n <= 0) return;
+    if (precision == 0)
+        pass_batch<double>(pass, L, variant, tab, work, n, s);
+    else
+        pass_batch<float>(pass, L, variant, tab, work, n, s);
+}
 
 FftPlan make_plan(int L) {
     const RadixPlan r = radix_plan(L);

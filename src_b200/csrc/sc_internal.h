@@ -82,6 +82,45 @@ void launch_soa_to_aos_by_id(const double* a, const double* b, const double* c, 
 void launch_f64_to_f32(const double* in, float* out, long long n, cudaStream_t s);
 void launch_f32_to_f64(const float* in, double* out, long long n, cudaStream_t s);
 
+// Batched launches (many bunches, one kernel): `tab` is a device array of
+// DevBunch, `work` a device array of n work items; item i = (bunch, block x,
+// block y, blocks of that bunch) drives block i.
+enum : int {
+    kBatchDrift = 0,
+    kBatchPsum,
+    kBatchStats,
+    kBatchDeposit,
+    kBatchAssemble,
+    kBatchAdvance,
+    kBatchIgfTmp,
+    kBatchIgfG,
+    kBatchGrad,
+    kBatchGather,
+};
+void launch_batch(int kind, int precision, int threads, const DevBunch* tab, const int4* work, int n, cudaStream_t s);
+
+// FFT passes of a batch: every bunch of one launch has the same transform
+// length L on the pass's axis; `variant` picks the tile shape (columns per
+// block) the autotuner chose for that length.
+enum : int {
+    kPassZR2C = 0,   // A
+    kPassYFwd,       // B
+    kPassXConv,      // C
+    kPassYInv,       // D
+    kPassZC2R,       // E (self-field scaling)
+    kPassDctZ,
+    kPassDctY,
+    kPassDctX,
+    kNumPasses
+};
+constexpr int kFftVariants = 2;
+// Blocks of one pass for one bunch (grid x, y) with a tile-shape variant.
+void fft_pass_grid(int pass, const DevBunch& b, int variant, int* gx, int* gy);
+// Transform length of a pass's axis for a bunch.
+int fft_pass_length(int pass, const DevBunch& b);
+void launch_fft_pass_batch(int pass, int L, int precision, int variant, const DevBunch* tab, const int4* work, int n,
+                           cudaStream_t s);
+
 // sort TU (sc_sort.cu)
 long long scan_scratch_ints(long long n);
 void exclusive_scan(const int* in, int* out, long long n, int* blocks, cudaStream_t s);

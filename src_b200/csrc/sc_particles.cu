@@ -38,6 +38,14 @@ __device__ __forceinline__ const P* fresh(const P* p) {
     return p;
 }
 
+// The block a kernel body works on and the number of blocks working on the
+// same bunch: blockIdx.x / gridDim.x of a single-bunch launch, or an entry of
+// the work table of a batched launch.
+struct VB {
+    int blk, nblk;
+};
+__device__ __forceinline__ VB vb_grid() { return VB{(int)blockIdx.x, (int)gridDim.x}; }
+
 struct MeshConsts {
     double hr[3], rhr[3], org[3];
 };
@@ -50,20 +58,20 @@ __device__ __forceinline__ void load_mesh_consts(MeshConsts& m, const StepState*
 }
 
 // ------------------------------------------------------------ reductions
-// Last-block-done: true in exactly one block, after every block's partials
-// are visible.  The caller resets the ticket.
-__device__ __forceinline__ bool last_block(unsigned* ticket) {
+// Last-block-done: true in exactly one of the nblk blocks working on a bunch,
+// after every block's partials are visible.  The caller resets the ticket.
+__device__ __forceinline__ bool last_block(unsigned* ticket, int nblk) {
     __shared__ bool am_last;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) am_last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    if (threadIdx.x == 0) am_last = (atomicAdd(ticket, 1u) == (unsigned)nblk - 1u);
     __syncthreads();
     return am_last;
 }
 
 // Exact block sum of NV fixed-point values per thread into partials[block][NV].
 template <int NV>
-__device__ __forceinline__ void block_sum_ex(i128 (&v)[NV], i128* __restrict__ partials) {
+__device__ __forceinline__ void block_sum_ex(i128 (&v)[NV], i128* __restrict__ partials, int blk) {
     __shared__ i128 sm[NV][kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -77,7 +85,7 @@ __device__ __forceinline__ void block_sum_ex(i128 (&v)[NV], i128* __restrict__ p
     for (int k = threadIdx.x; k < NV; k += blockDim.x) {
         i128 s = 0;
         for (int w = 0; w < kWarps; ++w) s += sm[k][w];
-        partials[(size_t)blockIdx.x * NV + k] = s;
+        partials[(size_t)blk * NV + k] = s;
     }
 }
 
@@ -131,16 +139,16 @@ __device__ __forceinline__ void accumulate_moments(i128 (&m)[28], const double* 
 // st->moments / st->gsum.  Otherwise the momentum sums into st->psum (and,
 // with init_frame, the beam frame of the next step).
 template <bool STATS>
-__global__ void __launch_bounds__(kThreads) k_reduce_state(BunchConst bc, const double* __restrict__ x,
-                                                           const double* __restrict__ y, const double* __restrict__ z,
-                                                           const double* __restrict__ px, const double* __restrict__ py,
-                                                           const double* __restrict__ pz, StepState* st,
-                                                           double* partials, unsigned* ticket, bool init_frame) {
+__device__ __forceinline__ void reduce_state_body(const BunchConst& bc, const double* __restrict__ x,
+                                                  const double* __restrict__ y, const double* __restrict__ z,
+                                                  const double* __restrict__ px, const double* __restrict__ py,
+                                                  const double* __restrict__ pz, StepState* st, double* partials,
+                                                  unsigned* ticket, bool init_frame, VB g) {
     constexpr int NV = STATS ? 28 : 3;
     i128 v[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) v[k] = 0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
         double P[3] = {px[i], py[i], pz[i]};
         if constexpr (STATS) {
             double R[3] = {x[i], y[i], z[i]};
@@ -152,10 +160,10 @@ __global__ void __launch_bounds__(kThreads) k_reduce_state(BunchConst bc, const 
         }
     }
     i128* xpart = reinterpret_cast<i128*>(partials);
-    block_sum_ex<NV>(v, xpart);
-    if (!last_block(ticket)) return;
+    block_sum_ex<NV>(v, xpart, g.blk);
+    if (!last_block(ticket, g.nblk)) return;
     __shared__ double tot[NV];
-    final_sum_ex<NV>(xpart, gridDim.x, tot);
+    final_sum_ex<NV>(xpart, g.nblk, tot);
     __syncthreads();
     if (threadIdx.x == 0) {
         if constexpr (STATS) {
@@ -170,18 +178,26 @@ __global__ void __launch_bounds__(kThreads) k_reduce_state(BunchConst bc, const 
         *ticket = 0u;
     }
 }
+template <bool STATS>
+__global__ void __launch_bounds__(kThreads) k_reduce_state(BunchConst bc, const double* __restrict__ x,
+                                                           const double* __restrict__ y, const double* __restrict__ z,
+                                                           const double* __restrict__ px, const double* __restrict__ py,
+                                                           const double* __restrict__ pz, StepState* st,
+                                                           double* partials, unsigned* ticket, bool init_frame) {
+    reduce_state_body<STATS>(bc, x, y, z, px, py, pz, st, partials, ticket, init_frame, vb_grid());
+}
 
 // ------------------------------------------------------------ drift + frame
 template <bool DRIFT>
-__global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
-                                                            double* __restrict__ z, const double* __restrict__ px,
-                                                            const double* __restrict__ py, const double* __restrict__ pz,
-                                                            StepState* st, double* partials, unsigned* ticket) {
+__device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
+                                           double* __restrict__ z, const double* __restrict__ px,
+                                           const double* __restrict__ py, const double* __restrict__ pz, StepState* st,
+                                           double* partials, unsigned* ticket, VB g) {
     __shared__ Trafo r2b_s;
     if (threadIdx.x == 0) r2b_s = st->r2b;
     __syncthreads();
     double v[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};  // min x,y,z, -max x,y,z
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
         double R[3] = {x[i], y[i], z[i]};
         if constexpr (DRIFT) {
             const double P[3] = {px[i], py[i], pz[i]};
@@ -214,11 +230,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, do
     if (threadIdx.x < 6) {
         double m = INFINITY;
         for (int w = 0; w < kWarps; ++w) m = fmin(m, sm[threadIdx.x][w]);
-        partials[(size_t)blockIdx.x * 6 + threadIdx.x] = m;
+        partials[(size_t)g.blk * 6 + threadIdx.x] = m;
     }
-    if (!last_block(ticket)) return;
+    if (!last_block(ticket, g.nblk)) return;
     __shared__ double tot[6];
-    final_min<6>(partials, gridDim.x, tot);
+    final_min<6>(partials, g.nblk, tot);
     __syncthreads();
     if (threadIdx.x == 0) {
         StepState& s = *st;
@@ -235,12 +251,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, do
         *ticket = 0u;
     }
 }
+template <bool DRIFT>
+__global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
+                                                            double* __restrict__ z, const double* __restrict__ px,
+                                                            const double* __restrict__ py, const double* __restrict__ pz,
+                                                            StepState* st, double* partials, unsigned* ticket) {
+    drift_body<DRIFT>(bc, x, y, z, px, py, pz, st, partials, ticket, vb_grid());
+}
 
 // The reference particle needs no particle data: it runs beside the deposit.
-__global__ void k_advance_reference(BunchConst bc, StepState* st) {
-    if (threadIdx.x == 0 && blockIdx.x == 0)
+__device__ __forceinline__ void advance_reference_body(const BunchConst& bc, StepState* st, VB g) {
+    if (threadIdx.x == 0 && g.blk == 0)
         if (!advance_reference(*st, bc)) atomicOr(&st->err, kFlagFrame);
 }
+__global__ void k_advance_reference(BunchConst bc, StepState* st) { advance_reference_body(bc, st, vb_grid()); }
 
 // ------------------------------------------------------------ cell keys
 // key = lgp_x + n0 * (lgp_y + n1 * lgp_z) and the particle's rank among the
@@ -339,9 +363,9 @@ __device__ __forceinline__ void acc_add(unsigned long long* a, long long v) {
 // particles / 64^3; warps with more than kMaxGroupPasses multi-lane groups
 // (sparse regions) add per lane.  No floating-point value is accumulated by
 // an atomic.
-__global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
-                                                      const double* __restrict__ z, StepState* st,
-                                                      unsigned long long* __restrict__ acc) {
+__device__ __forceinline__ void deposit_body(const BunchConst& bc, const double* __restrict__ x,
+                                             const double* __restrict__ y, const double* __restrict__ z, StepState* st,
+                                             unsigned long long* __restrict__ acc, VB g) {
     __shared__ MeshConsts ms;
     __shared__ double qdt_s, to_int_s;
     load_mesh_consts(ms, st);
@@ -353,7 +377,7 @@ __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const doubl
     const int lane = threadIdx.x & 31;
     const int nx = bc.n[0], nxy = bc.n[0] * bc.n[1];
     bool bad = false;
-    for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < bc.N; i0 += (long long)gridDim.x * blockDim.x) {
+    for (long long i0 = (long long)g.blk * blockDim.x; i0 < bc.N; i0 += (long long)g.nblk * blockDim.x) {
         const long long i = i0 + threadIdx.x;
         const bool valid = i < bc.N;
         uint32_t key = 0xffffffffu;
@@ -410,6 +434,11 @@ __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const doubl
     }
     if (bad) atomicOr(&st->err, kFlagGuard);
 }
+__global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
+                                                      const double* __restrict__ z, StepState* st,
+                                                      unsigned long long* __restrict__ acc) {
+    deposit_body(bc, x, y, z, st, acc, vb_grid());
+}
 
 // correctly rounded double of the 128-bit accumulator (lo, hi), times unit
 __device__ __forceinline__ double acc_to_double(unsigned long long lo, unsigned long long hi, double unit) {
@@ -434,12 +463,12 @@ __device__ __forceinline__ double acc_to_double(unsigned long long lo, unsigned 
 // rho = (exact node sum) / dT * tmp2   (PartBunch.cpp:496, :510-511); the
 // accumulators are cleared for the next deposit.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_assemble_rho(BunchConst bc, const StepState* __restrict__ st,
-                                                           unsigned long long* __restrict__ acc, T* __restrict__ rho) {
+__device__ __forceinline__ void assemble_body(const BunchConst& bc, const StepState* __restrict__ st,
+                                              unsigned long long* __restrict__ acc, T* __restrict__ rho, VB g) {
     const int M = bc.n[0] * bc.n[1] * bc.n[2];
     const double dT = bc.dT, tmp2 = st->tmp2;
     const double unit = ldexp(1.0, fx_exponent(st->qdt) - kFxFrac);
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x) {
+    for (int c = g.blk * blockDim.x + threadIdx.x; c < M; c += g.nblk * blockDim.x) {
         const ulonglong2 a = reinterpret_cast<const ulonglong2*>(acc)[c];
         const i128 w = (i128)(long long)a.y * (i128)4294967296 + (i128)a.x;  // H 2^32 + L
         double s = acc_to_double((unsigned long long)w, (unsigned long long)(w >> 64), unit);
@@ -448,6 +477,11 @@ __global__ void __launch_bounds__(kThreads) k_assemble_rho(BunchConst bc, const 
         rho[c] = (T)s;
         reinterpret_cast<ulonglong2*>(acc)[c] = make_ulonglong2(0ull, 0ull);
     }
+}
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_assemble_rho(BunchConst bc, const StepState* __restrict__ st,
+                                                           unsigned long long* __restrict__ acc, T* __restrict__ rho) {
+    assemble_body<T>(bc, st, acc, rho, vb_grid());
 }
 
 // ------------------------------------------------------------ Green's function
@@ -467,12 +501,12 @@ __device__ __forceinline__ double igf_antiderivative(double x, double y, double 
     return tmpgrn / cellVolume;
 }
 
-__global__ void __launch_bounds__(kThreads) k_igf_tmp(int n0, int n1, int n2, const StepState* __restrict__ st,
-                                                      double* __restrict__ tmp) {
+__device__ __forceinline__ void igf_tmp_body(int n0, int n1, int n2, const StepState* __restrict__ st,
+                                             double* __restrict__ tmp, VB g) {
     const int t0 = n0 + 2, t1 = n1 + 2, t2 = n2 + 2;
     const double h0 = st->hr_scaled[0], h1 = st->hr_scaled[1], h2 = st->hr_scaled[2];
     const double cellVolume = h0 * h1 * h2;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < t0 * t1 * t2; c += gridDim.x * blockDim.x) {
+    for (int c = g.blk * blockDim.x + threadIdx.x; c < t0 * t1 * t2; c += g.nblk * blockDim.x) {
         const int i = c % t0, j = (c / t0) % t1, k = c / (t0 * t1);
         const double vx = i * h0 - h0 / 2;
         const double vy = j * h1 - h1 / 2;
@@ -480,14 +514,18 @@ __global__ void __launch_bounds__(kThreads) k_igf_tmp(int n0, int n1, int n2, co
         tmp[c] = igf_antiderivative(vx, vy, vz, cellVolume);
     }
 }
+__global__ void __launch_bounds__(kThreads) k_igf_tmp(int n0, int n1, int n2, const StepState* __restrict__ st,
+                                                      double* __restrict__ tmp) {
+    igf_tmp_body(n0, n1, n2, st, tmp, vb_grid());
+}
 
 // G on (n0+1)(n1+1)(n2+1) points, 8-corner difference (:508-516), then
 // G[0,0,0] <- G[0,0,1] (mirrorRhoField, :657).
-__global__ void __launch_bounds__(kThreads) k_igf_G(int n0, int n1, int n2, const double* __restrict__ tmp,
-                                                    double* __restrict__ G) {
+__device__ __forceinline__ void igf_G_body(int n0, int n1, int n2, const double* __restrict__ tmp,
+                                           double* __restrict__ G, VB g) {
     const int g0 = n0 + 1, g1 = n1 + 1, g2 = n2 + 1;
     const int t0 = n0 + 2, t1 = n1 + 2;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g0 * g1 * g2; c += gridDim.x * blockDim.x) {
+    for (int c = g.blk * blockDim.x + threadIdx.x; c < g0 * g1 * g2; c += g.nblk * blockDim.x) {
         int i = c % g0, j = (c / g0) % g1, k = c / (g0 * g1);
         if (c == 0) k = 1;
 #define TG(a, b, e) tmp[(a) + t0 * ((b) + t1 * (e))]
@@ -503,12 +541,16 @@ __global__ void __launch_bounds__(kThreads) k_igf_G(int n0, int n1, int n2, cons
         G[c] = g;
     }
 }
+__global__ void __launch_bounds__(kThreads) k_igf_G(int n0, int n1, int n2, const double* __restrict__ tmp,
+                                                    double* __restrict__ G) {
+    igf_G_body(n0, n1, n2, tmp, G, vb_grid());
+}
 
 // ------------------------------------------------------------ gradient
 // phi is FP64 in both forms; T is the storage type of the field.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_grad(BunchConst bc, const StepState* __restrict__ st,
-                                                   const double* __restrict__ phi, T* __restrict__ E4) {
+__device__ __forceinline__ void grad_body(const BunchConst& bc, const StepState* __restrict__ st,
+                                          const double* __restrict__ phi, T* __restrict__ E4, VB g) {
     const int n[3] = {bc.n[0], bc.n[1], bc.n[2]};
     const int M = n[0] * n[1] * n[2];
     const int stv[3] = {1, n[0], n[0] * n[1]};
@@ -516,7 +558,7 @@ __global__ void __launch_bounds__(kThreads) k_grad(BunchConst bc, const StepStat
     const double id[3] = {0.5 / h[0], 0.5 / h[1], 0.5 / h[2]};
     const double gz = st->gammaz;
     const double sc[3] = {gz / 1.0, gz / 1.0, 1.0 / (1.0 * gz)};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x) {
+    for (int c = g.blk * blockDim.x + threadIdx.x; c < M; c += g.nblk * blockDim.x) {
         const int idx[3] = {c % n[0], (c / n[0]) % n[1], c / (n[0] * n[1])};
         double e[3];
 #pragma unroll
@@ -537,6 +579,11 @@ __global__ void __launch_bounds__(kThreads) k_grad(BunchConst bc, const StepStat
         E4[4 * (size_t)c + 2] = (T)e[2];
         E4[4 * (size_t)c + 3] = (T)0;
     }
+}
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_grad(BunchConst bc, const StepState* __restrict__ st,
+                                                   const double* __restrict__ phi, T* __restrict__ E4) {
+    grad_body<T>(bc, st, phi, E4, vb_grid());
 }
 
 // ------------------------------------------------------------ gather, kick, push
@@ -578,11 +625,10 @@ __device__ __forceinline__ void cic_gather(const T* __restrict__ E4, const int* 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
-                                                                  double* __restrict__ z, double* __restrict__ px,
-                                                                  double* __restrict__ py, double* __restrict__ pz,
-                                                                  const T* __restrict__ E4, StepState* st, double* partials,
-                                                                  unsigned* ticket) {
+__device__ __forceinline__ void gather_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
+                                            double* __restrict__ z, double* __restrict__ px, double* __restrict__ py,
+                                            double* __restrict__ pz, const T* __restrict__ E4, StepState* st,
+                                            double* partials, unsigned* ticket, VB g) {
     __shared__ Trafo b2r_s, upd_s;
     __shared__ MeshConsts ms;
     __shared__ double betaC_s;
@@ -595,7 +641,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
     __syncthreads();
     i128 acc[3] = {0, 0, 0};
     bool bad = false;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
         const double X[3] = {x[i], y[i], z[i]};
         double P[3] = {px[i], py[i], pz[i]};
         int l[3];
@@ -630,10 +676,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
     }
     if (bad) atomicOr(&st->err, kFlagGuard);
     i128* xpart = reinterpret_cast<i128*>(partials);
-    block_sum_ex<3>(acc, xpart);
-    if (!last_block(ticket)) return;
+    block_sum_ex<3>(acc, xpart, g.blk);
+    if (!last_block(ticket, g.nblk)) return;
     __shared__ double tot[3];
-    final_sum_ex<3>(xpart, gridDim.x, tot);
+    final_sum_ex<3>(xpart, g.nblk, tot);
     __syncthreads();
     if (threadIdx.x == 0) {
         StepState& s = *st;
@@ -644,6 +690,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
         s.step += 1;
         *ticket = 0u;
     }
+}
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
+                                                                  double* __restrict__ z, double* __restrict__ px,
+                                                                  double* __restrict__ py, double* __restrict__ pz,
+                                                                  const T* __restrict__ E4, StepState* st, double* partials,
+                                                                  unsigned* ticket) {
+    gather_body<T>(bc, x, y, z, px, py, pz, E4, st, partials, ticket, vb_grid());
 }
 
 // Fields only (PartBunch::computeSelfFields output): Ef, Bf in the beam frame,
@@ -747,7 +801,113 @@ inline int grid_for(long long work, int cap) {
     return (int)g;
 }
 
+// ------------------------------------------------------------ batched launches
+// One kernel over many bunches: block i takes work item work[i] = (bunch,
+// block, -, blocks of that bunch) and runs the same body as the single-bunch
+// kernel on the bunch's buffers (tab[bunch], a device copy of its DevBunch).
+template <bool DRIFT>
+__global__ void __launch_bounds__(kThreads, 3) k_drift_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    drift_body<DRIFT>(d.bc, d.x, d.y, d.z, d.px, d.py, d.pz, d.st, d.partials, d.ticket, VB{w.y, w.w});
+}
+
+template <bool STATS>
+__global__ void __launch_bounds__(kThreads) k_reduce_state_batch(const DevBunch* __restrict__ tab,
+                                                                 const int4* __restrict__ work, bool init_frame) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    reduce_state_body<STATS>(d.bc, d.x, d.y, d.z, d.px, d.py, d.pz, d.st, d.partials, d.ticket, init_frame,
+                             VB{w.y, w.w});
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_deposit_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    deposit_body(d.bc, d.x, d.y, d.z, d.st, d.nacc, VB{w.y, w.w});
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_assemble_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    assemble_body<T>(d.bc, d.st, d.nacc, (T*)d.rho, VB{w.y, w.w});
+}
+
+__global__ void k_advance_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    advance_reference_body(d.bc, d.st, VB{w.y, w.w});
+}
+
+__global__ void __launch_bounds__(kThreads) k_igf_tmp_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    igf_tmp_body(d.bc.n[0], d.bc.n[1], d.bc.n[2], d.st, d.gtmp, VB{w.y, w.w});
+}
+
+__global__ void __launch_bounds__(kThreads) k_igf_G_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    igf_G_body(d.bc.n[0], d.bc.n[1], d.bc.n[2], d.gtmp, d.gline, VB{w.y, w.w});
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_grad_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    grad_body<T>(d.bc, d.st, d.phi, (T*)d.E4, VB{w.y, w.w});
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 3) k_gather_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
+    const int4 w = work[blockIdx.x];
+    const DevBunch& d = tab[w.x];
+    gather_body<T>(d.bc, d.x, d.y, d.z, d.px, d.py, d.pz, (const T*)d.E4, d.st, d.partials, d.ticket, VB{w.y, w.w});
+}
+
 }  // namespace
+
+void launch_batch(int kind, int precision, int threads, const DevBunch* tab, const int4* work, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    const bool f64 = precision == 0;
+    switch (kind) {
+        case kBatchDrift: k_drift_batch<true><<<n, kThreads, 0, s>>>(tab, work); break;
+        case kBatchPsum: k_reduce_state_batch<false><<<n, kThreads, 0, s>>>(tab, work, true); break;
+        case kBatchStats: k_reduce_state_batch<true><<<n, kThreads, 0, s>>>(tab, work, false); break;
+        case kBatchDeposit:
+            if (threads == 128)
+                k_deposit_batch<128><<<n, 128, 0, s>>>(tab, work);
+            else if (threads == 512)
+                k_deposit_batch<512><<<n, 512, 0, s>>>(tab, work);
+            else
+                k_deposit_batch<256><<<n, 256, 0, s>>>(tab, work);
+            break;
+        case kBatchAssemble:
+            if (f64)
+                k_assemble_batch<double><<<n, kThreads, 0, s>>>(tab, work);
+            else
+                k_assemble_batch<float><<<n, kThreads, 0, s>>>(tab, work);
+            break;
+        case kBatchAdvance: k_advance_batch<<<n, 32, 0, s>>>(tab, work); break;
+        case kBatchIgfTmp: k_igf_tmp_batch<<<n, kThreads, 0, s>>>(tab, work); break;
+        case kBatchIgfG: k_igf_G_batch<<<n, kThreads, 0, s>>>(tab, work); break;
+        case kBatchGrad:
+            if (f64)
+                k_grad_batch<double><<<n, kThreads, 0, s>>>(tab, work);
+            else
+                k_grad_batch<float><<<n, kThreads, 0, s>>>(tab, work);
+            break;
+        case kBatchGather:
+            if (f64)
+                k_gather_batch<double><<<n, kThreads, 0, s>>>(tab, work);
+            else
+                k_gather_batch<float><<<n, kThreads, 0, s>>>(tab, work);
+            break;
+        default: break;
+    }
+}
 
 int particle_grid(const DevBunch& b) { return b.red_blocks; }
 

@@ -258,3 +258,138 @@ def beam_parameters_from_stats(record, n):
     if rc != 0:
         raise ScgpuError(rc, "beam_parameters_from_stats")
     return bp.as_dict()
+
+
+# ---------------------------------------------------------------- batches
+def _batch_lib():
+    L = lib()
+    if not getattr(L, "_batch_ready", False):
+        L.scgpu_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int]
+        L.scgpu_batch_destroy.argtypes = [C.c_void_p]
+        L.scgpu_batch_last_error.argtypes = [C.c_void_p]
+        L.scgpu_batch_last_error.restype = C.c_char_p
+        L.scgpu_batch_add.argtypes = [C.c_void_p, C.POINTER(SolverParams), C.c_longlong, _dp, _dp,
+                                      C.POINTER(BunchParams)]
+        L.scgpu_batch_remove.argtypes = [C.c_void_p, C.c_int]
+        L.scgpu_batch_member.argtypes = [C.c_void_p, C.c_int]
+        L.scgpu_batch_member.restype = C.c_void_p
+        L.scgpu_batch_size.argtypes = [C.c_void_p]
+        L.scgpu_batch_track.argtypes = [C.c_void_p, C.c_int]
+        L.scgpu_batch_last_track_ms.argtypes = [C.c_void_p]
+        L.scgpu_batch_last_track_ms.restype = C.c_double
+        L.scgpu_batch_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.scgpu_batch_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.scgpu_batch_autotune.argtypes = [C.c_void_p, C.c_int]
+        L._batch_ready = True
+    return L
+
+
+EXPORTED += [
+    "scgpu_compute_potential_noalloc",
+    "scgpu_batch_create", "scgpu_batch_destroy", "scgpu_batch_last_error", "scgpu_batch_add", "scgpu_batch_remove",
+    "scgpu_batch_member", "scgpu_batch_size", "scgpu_batch_track", "scgpu_batch_last_track_ms",
+    "scgpu_batch_set_tuning", "scgpu_batch_get_tuning", "scgpu_batch_autotune",
+]
+
+
+class _Member(Context):
+    """A bunch of a Batch: the single-bunch calls on the batch's slot context
+    (the batch owns the context; closing the view does nothing)."""
+
+    def __init__(self, handle, nr, precision, n):
+        self.h = C.c_void_p(handle)
+        self.nr = tuple(nr)
+        self.precision = precision
+        self.n = n
+
+    def close(self):
+        self.h = None
+
+
+def _bunch_params(dT, q_macro, mass, charge=-1.0, coupling=None, bz_ext=0.0, t=0.0, path_length=0.0,
+                  ref_R=(0.0, 0.0, 0.0), ref_P=(0.0, 0.0, 10.0)):
+    if coupling is None:
+        coupling = 1.0 / (4 * 3.14159265358979323846 * 8.854187817e-12)
+    return BunchParams(dT, mass, charge, q_macro, coupling, bz_ext, t, path_length, (C.c_double * 3)(*ref_R),
+                       (C.c_double * 3)(*ref_P))
+
+
+class Batch:
+    """Many bunches stepping together (scgpu_batch_*): one launch per kernel
+    of the step for all bunches, one graph launch per step."""
+
+    def __init__(self, precision=PLAIN_FP64, device=0):
+        h = C.c_void_p()
+        rc = _batch_lib().scgpu_batch_create(C.byref(h), int(device), int(precision))
+        if rc != 0:
+            raise ScgpuError(rc, "scgpu_batch_create failed")
+        self.h = h
+        self.precision = precision
+        self._meta = {}
+
+    def _check(self, rc, what):
+        if rc < 0:
+            msg = _batch_lib().scgpu_batch_last_error(self.h)
+            raise ScgpuError(rc, f"{what}: {msg.decode() if msg else ''}")
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            _batch_lib().scgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, nr, R, P, dT, q_macro, mass, bboxincr=2.0, **kw):
+        """Uploads a bunch on a mesh nr = (mx, my, mt); returns its slot."""
+        R = _f64c(R)
+        P = _f64c(P)
+        nr = tuple(int(v) for v in nr)
+        sp = SolverParams(nr[0], nr[1], nr[2], self.precision, float(bboxincr))
+        bp = _bunch_params(dT, q_macro, mass, **kw)
+        slot = self._check(_batch_lib().scgpu_batch_add(self.h, C.byref(sp), R.shape[0], _p(R), _p(P), C.byref(bp)),
+                           "batch_add")
+        self._meta[slot] = (nr, R.shape[0])
+        return slot
+
+    def remove(self, slot):
+        self._check(_batch_lib().scgpu_batch_remove(self.h, int(slot)), "batch_remove")
+        self._meta.pop(slot, None)
+
+    def member(self, slot):
+        h = _batch_lib().scgpu_batch_member(self.h, int(slot))
+        if not h:
+            raise ScgpuError(-1, f"no bunch in slot {slot}")
+        nr, n = self._meta[slot]
+        return _Member(h, nr, self.precision, n)
+
+    def size(self):
+        return _batch_lib().scgpu_batch_size(self.h)
+
+    def track(self, nsteps):
+        self._check(_batch_lib().scgpu_batch_track(self.h, int(nsteps)), "batch_track")
+        return _batch_lib().scgpu_batch_last_track_ms(self.h)
+
+    def set_tuning(self, deposit_threads=256, L=0, fft_variant=0):
+        self._check(_batch_lib().scgpu_batch_set_tuning(self.h, int(deposit_threads), int(L), int(fft_variant)),
+                    "batch_set_tuning")
+
+    def tuning(self, L):
+        t, v = C.c_int(), C.c_int()
+        self._check(_batch_lib().scgpu_batch_get_tuning(self.h, int(L), C.byref(t), C.byref(v)), "batch_get_tuning")
+        return {"deposit_threads": t.value, "fft_variant": v.value}
+
+    def autotune(self, trial_steps=3):
+        """Times the candidate launch shapes on the current bunches; returns
+        the number of steps the trials advanced every bunch."""
+        return self._check(_batch_lib().scgpu_batch_autotune(self.h, int(trial_steps)), "batch_autotune")
