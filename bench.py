@@ -222,6 +222,11 @@ def main():
     ap.add_argument("--compare-precision", action="store_true",
                     help="run the plain and the mixed form on the same bunch for --steps steps and report "
                          "the mixed form's field and emittance error against FP64 (one JSON line)")
+    ap.add_argument("--batched", action="store_true",
+                    help="batched form: 64 bunches of mixed sizes and meshes in one batch (one JSON line)")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving loop: Poisson arrivals at 50 jobs/s for --serve-seconds (one JSON line)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global N_PARTICLES, MESH, BZ, WORKLOAD
@@ -229,6 +234,12 @@ def main():
     world, rank, local = dist_setup()
     if args.compare_precision:
         compare_precision(args, local)
+        return
+    if args.batched:
+        batched(args, local)
+        return
+    if args.serve:
+        serve(args, local)
         return
 
     if args.impl == "reference":
@@ -431,6 +442,95 @@ def compare_precision(args, local):
         "speedup_mixed_over_fp64": d["ms_per_step"] / m["ms_per_step"],
         "bounds": {"field": 1e-5, "emittance_drift": 1e-6},
         "norms": "max|mixed - fp64| / max|fp64| over all mesh points (E) or particles (R, P)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def batched(args, local):
+    """64 bunches (particle counts log-uniform in [1e4, 5e5], meshes from
+    {16, 32, 48, 64}^3, sigma, charge and beta*gamma drawn per bunch) in one
+    batch: autotuned launch shapes, then --steps (200 unless given) timed
+    batched steps.  Beside it, the same bunches one after another in
+    single-bunch contexts (a probe of a few steps each, scaled), the way one
+    tracker per design point would run them."""
+    import torch
+
+    from src_b200 import scgpu
+    from src_b200.serving import MasterBunches
+    from src_b200.workloads import DT as WDT, MASS_EV, batched_jobs
+
+    torch.cuda.set_device(local)
+    prec = scgpu.PLAIN_FP64 if args.precision == "fp64" else scgpu.MIXED
+    steps = args.steps if args.steps != 1000 else 200
+    jobs = batched_jobs(steps=steps)
+    masters = MasterBunches(count=4, size=max(j.particles for j in jobs))
+    data = [masters.bunch(j) for j in jobs]
+    total_particles = sum(j.particles for j in jobs)
+    with scgpu.Batch(precision=prec, device=local) as bt:
+        for j, (R, P) in zip(jobs, data):
+            bt.add((j.mesh,) * 3, R, P, WDT, j.q_macro, MASS_EV, ref_P=j.ref_P)
+        tuned_steps = bt.autotune(3)
+        tuning = {L: bt.tuning(L) for L in (32, 64, 96, 128)}
+        bt.track(args.warmup)
+        clocks = ClockSampler(local)
+        clocks.start()
+        ms = bt.track(steps)
+        clk = clocks.stop()
+    value = total_particles * steps / (ms * 1e-3)
+    seq_ms = 0.0
+    probe = 10
+    for j, (R, P) in zip(jobs, data):
+        with scgpu.Context((j.mesh,) * 3, precision=prec, device=local) as c:
+            c.upload(R, P, WDT, j.q_macro, MASS_EV, ref_P=j.ref_P)
+            c.track(3)
+            seq_ms += c.track(probe) / probe * steps
+    line = {
+        "metric": "batched particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "precision": args.precision, "bunches": len(jobs), "particles_total": total_particles,
+        "meshes": {str(m): sum(1 for j in jobs if j.mesh == m) for m in (16, 32, 48, 64)},
+        "autotune": {"steps_taken": tuned_steps, "choices": {str(k): v for k, v in tuning.items()}},
+        "sequential_single_contexts": {"value": total_particles * steps / (seq_ms * 1e-3), "ms": seq_ms,
+                                       "note": f"each bunch alone, {probe}-step probe scaled to {steps} steps"},
+        "speedup_vs_sequential": seq_ms / ms,
+        "clocks": clk, "data": "synthetic (seeded)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def serve(args, local):
+    """Serving loop: jobs arrive by a Poisson process at 50 jobs/s for
+    --serve-seconds; each is admitted by HBM footprint into the running batch
+    and advanced with the others; reports throughput and p50/p99 latency."""
+    import torch
+
+    from src_b200 import scgpu
+    from src_b200.serving import MasterBunches, Server, latency_summary
+    from src_b200.workloads import Job, serving_jobs
+
+    torch.cuda.set_device(local)
+    prec = scgpu.PLAIN_FP64 if args.precision == "fp64" else scgpu.MIXED
+    jobs = serving_jobs(duration_s=args.serve_seconds)
+    masters = MasterBunches(count=4, size=max(j.particles for j in jobs))
+    srv = Server(precision=prec, masters=masters)
+    cal = [Job(100000 + i, 0.0, 200_000, m, (1e-3, 1e-3, 2e-3), 10.0, 1.0, 10)
+           for i, m in enumerate(sorted({j.mesh for j in jobs}))]
+    tuning = srv.calibrate(cal)
+    clocks = ClockSampler(local)
+    clocks.start()
+    try:
+        res = srv.run(jobs, realtime=True)
+    finally:
+        srv.close()
+    clk = clocks.stop()
+    lat = latency_summary(res)
+    line = {
+        "metric": "serving p50/p99 job latency and throughput", "precision": args.precision,
+        "arrival_rate_hz": 50.0, "window_s": args.serve_seconds, "jobs": len(res),
+        "throughput": {"value": srv.particle_steps / srv.makespan_s, "unit": "particle-steps/s"},
+        "particle_steps": srv.particle_steps, "latency_s": lat, "makespan_s": srv.makespan_s,
+        "rounds": srv.rounds, "hbm_budget_gb": srv.budget / 1e9, "tuning": {str(k): v for k, v in tuning.items()},
+        "clocks": clk, "data": "synthetic (seeded Poisson arrivals, log-uniform 1e4..2e6 particles, 16..128^3)",
     }
     print(json.dumps(line), flush=True)
 

@@ -91,6 +91,32 @@ def test_batch_membership_changes_and_autotune(gpu):
         np.testing.assert_array_equal(P, Pa)
 
 
+def test_serving_results_equal_alone(gpu):
+    """Continuous batching: jobs of different sizes admitted as they arrive
+    (and as memory frees) give, job by job, the result of running alone."""
+    from src_b200.serving import MasterBunches, Server, run_alone
+    from src_b200.workloads import Job
+
+    rng = np.random.default_rng(7)
+    jobs = [Job(i, 0.002 * i, int(rng.integers(10_000, 60_000)), int(rng.choice([16, 24, 32])),
+                tuple(rng.uniform(0.5e-3, 3e-3, 3)), float(rng.uniform(2, 20)), float(rng.uniform(0.1, 2)),
+                int(rng.integers(5, 40))) for i in range(10)]
+    masters = MasterBunches(count=2, size=60_000)
+    for prec in (gpu.PLAIN_FP64, gpu.MIXED):
+        # a budget of about three jobs forces queueing and slot reuse
+        budget = 3 * max(j.footprint_bytes(prec) for j in jobs)
+        srv = Server(precision=prec, hbm_budget_bytes=budget, masters=masters, keep_results=True)
+        try:
+            res = srv.run(jobs, realtime=True)
+        finally:
+            srv.close()
+        assert len(res) == len(jobs)
+        for r in res:
+            Ra, Pa = run_alone(r.job, prec, masters)
+            np.testing.assert_array_equal(r.R, Ra)
+            np.testing.assert_array_equal(r.P, Pa)
+
+
 def test_batch_errors(gpu):
     with gpu.Batch() as bt:
         with pytest.raises(gpu.ScgpuError):
