@@ -529,7 +529,8 @@ def serve(args, local):
         "arrival_rate_hz": 50.0, "window_s": args.serve_seconds, "jobs": len(res),
         "throughput": {"value": srv.particle_steps / srv.makespan_s, "unit": "particle-steps/s"},
         "particle_steps": srv.particle_steps, "latency_s": lat, "makespan_s": srv.makespan_s,
-        "rounds": srv.rounds, "hbm_budget_gb": srv.budget / 1e9, "tuning": {str(k): v for k, v in tuning.items()},
+        "rounds": srv.rounds, "host_time": srv.time, "hbm_budget_gb": srv.budget / 1e9,
+        "tuning": {str(k): v for k, v in tuning.items()},
         "clocks": clk, "data": "synthetic (seeded Poisson arrivals, log-uniform 1e4..2e6 particles, 16..128^3)",
     }
     print(json.dumps(line), flush=True)

@@ -218,6 +218,15 @@ scgpu_ctx* scgpu_batch_member(scgpu_batch* batch, int slot);
 int scgpu_batch_size(const scgpu_batch* batch);
 /* every occupied slot advances nsteps ParallelTTracker steps */
 int scgpu_batch_track(scgpu_batch* batch, int nsteps);
+/* scgpu_batch_track in two halves: launch enqueues the steps and returns, so
+ * the host can prepare and scgpu_batch_add further bunches (they join at the
+ * next launch) while the device works; wait finishes the steps and reports
+ * device errors.  Removing a slot waits for steps in flight. */
+int scgpu_batch_launch(scgpu_batch* batch, int nsteps);
+int scgpu_batch_wait(scgpu_batch* batch);
+/* Removed bunches leave their contexts (device buffers) parked for reuse by
+ * later bunches on the same mesh; trim frees the parked ones. */
+int scgpu_batch_trim(scgpu_batch* batch);
 double scgpu_batch_last_track_ms(const scgpu_batch* batch);
 /* Tuning of the batched launches: threads per block of the deposit (128,
  * 256 or 512) and, per transform length L, the FFT tile shape (0: the

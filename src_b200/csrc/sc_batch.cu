@@ -1,12 +1,12 @@
 // sc_batch.cu -- many bunches stepping together (include/scgpu.h, "batches").
 //
 // Each bunch keeps its own context (buffers, StepState, constants).  A
-// batched step launches every kernel of the step once for all bunches: the
-// blocks of a launch index a device work table of (bunch, block x, block y,
-// blocks of that bunch), and a device copy of each bunch's DevBunch gives the
-// kernel its buffers and sizes.  FFT passes are grouped by the transform
-// length of their axis, since the length is a template constant of the
-// kernels.  The step order is the single-bunch one (sc_api.cu enqueue_step):
+// batched step launches every kernel of the step once for all bunches: a
+// launch carries one item per bunch (bunch, first block, blocks in x and y),
+// each block finds its bunch by a binary search over the items, and a device
+// copy of each bunch's DevBunch gives the kernel its buffers and sizes.  FFT
+// passes are grouped by the transform length of their axis, since the length
+// is a template constant of the kernels.  The step order is the single-bunch one (sc_api.cu enqueue_step):
 //
 //   main: drift -> deposit -> assemble -> reference update [-> cell reorder]
 //   side: Green's function (antiderivative, 8-corner G, three DCT passes)
@@ -48,8 +48,9 @@ struct Launch {
     int kind;   // kBatch* for particle / grid kernels, -1 for an FFT pass
     int pass;   // kPass* when kind == -1
     int L;      // transform length of the pass's axis
-    int off;    // first work item
-    int n;      // work items (blocks)
+    int off;    // first item (one per bunch of the launch)
+    int nitems; // bunches of the launch
+    int nblocks;
 };
 
 }  // namespace
@@ -60,6 +61,10 @@ struct scgpu_batch {
     std::vector<scgpu_ctx*> slots;
     std::vector<int> members;   // occupied slots in table order
     cudaStream_t stream = nullptr, side = nullptr;
+    // Uploads and downloads of the bunches run here, at the highest stream
+    // priority, so that a bunch joining during a long batched round gets SMs
+    // as soon as blocks of the round retire instead of waiting for the round.
+    cudaStream_t xfer = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
     std::string err;
     DevBunch* d_tab = nullptr;
@@ -69,13 +74,24 @@ struct scgpu_batch {
     int* d_flags = nullptr;
     std::vector<Launch> launches;
     bool dirty = true;
-    bool eager_next = true;  // run the next step without a graph (new launch shapes)
+    // After a membership or tuning change the steps of one track call run
+    // without a graph: capturing and instantiating costs more than the few
+    // steps a serving round replays.  The next call with the same membership
+    // captures (the eager steps have also raised the kernels' shared-memory
+    // limits outside any capture).
+    bool eager_call = true;
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // [reorder]
     long long steps = 0;
     int reorder_every = 16;
     int dep_threads = 256;
     std::map<int, int> fft_variant;  // transform length -> tile-shape variant
     double last_ms = 0.0;
+    int in_flight = 0;  // steps launched and not yet waited for
+    // Contexts of removed bunches, kept with their device buffers for the
+    // next bunch on the same mesh: a serving loop then allocates and frees
+    // nothing in steady state (cudaMalloc / cudaFree synchronise the device).
+    std::vector<scgpu_ctx*> pool;
+    size_t pool_max = 4096;
 };
 
 namespace {
@@ -118,27 +134,28 @@ int rebuild(scgpu_batch* b) {
     std::vector<int4> work;
     b->launches.clear();
     auto add_per_bunch = [&](int lane, int kind, auto blocks_of) {
-        Launch l{lane, kind, 0, 0, (int)work.size(), 0};
+        Launch l{lane, kind, 0, 0, (int)work.size(), 0, 0};
         for (int i = 0; i < nm; ++i) {
             const int nb = blocks_of(tab[i]);
-            for (int k = 0; k < nb; ++k) work.push_back(make_int4(i, k, 0, nb));
+            work.push_back(make_int4(i, l.nblocks, nb, 1));
+            l.nblocks += nb;
         }
-        l.n = (int)work.size() - l.off;
+        l.nitems = (int)work.size() - l.off;
         b->launches.push_back(l);
     };
     auto add_pass = [&](int lane, int pass) {
         std::map<int, std::vector<int>> by_len;
         for (int i = 0; i < nm; ++i) by_len[fft_pass_length(pass, tab[i])].push_back(i);
         for (auto& kv : by_len) {
-            Launch l{lane, -1, pass, kv.first, (int)work.size(), 0};
+            Launch l{lane, -1, pass, kv.first, (int)work.size(), 0, 0};
             const int v = variant_of(b, kv.first);
             for (int i : kv.second) {
                 int gx = 0, gy = 0;
                 fft_pass_grid(pass, tab[i], v, &gx, &gy);
-                for (int y = 0; y < gy; ++y)
-                    for (int x = 0; x < gx; ++x) work.push_back(make_int4(i, x, y, 0));
+                work.push_back(make_int4(i, l.nblocks, gx, gy));
+                l.nblocks += gx * gy;
             }
-            l.n = (int)work.size() - l.off;
+            l.nitems = (int)work.size() - l.off;
             b->launches.push_back(l);
         }
     };
@@ -184,7 +201,7 @@ int rebuild(scgpu_batch* b) {
     if (nm) BCK(cudaMemcpy(b->d_tab, tab.data(), (size_t)nm * sizeof(DevBunch), cudaMemcpyHostToDevice));
     if (!work.empty()) BCK(cudaMemcpy(b->d_work, work.data(), work.size() * sizeof(int4), cudaMemcpyHostToDevice));
     b->dirty = false;
-    b->eager_next = true;
+    b->eager_call = true;
     return SCGPU_OK;
 }
 
@@ -193,9 +210,9 @@ void enqueue_lane(scgpu_batch* b, int lane, cudaStream_t s) {
         if (l.lane != lane) continue;
         const int4* w = b->d_work + l.off;
         if (l.kind < 0)
-            launch_fft_pass_batch(l.pass, l.L, b->precision, variant_of(b, l.L), b->d_tab, w, l.n, s);
+            launch_fft_pass_batch(l.pass, l.L, b->precision, variant_of(b, l.L), b->d_tab, w, l.nitems, l.nblocks, s);
         else
-            launch_batch(l.kind, b->precision, b->dep_threads, b->d_tab, w, l.n, s);
+            launch_batch(l.kind, b->precision, b->dep_threads, b->d_tab, w, l.nitems, l.nblocks, s);
     }
 }
 
@@ -229,23 +246,20 @@ int check_flags(scgpu_batch* b) {
     return SCGPU_OK;
 }
 
-int track(scgpu_batch* b, int nsteps) {
+// Enqueues nsteps batched steps on the batch stream and returns.
+int launch(scgpu_batch* b, int nsteps) {
     BCK(cudaSetDevice(b->device));
     if (b->dirty) {
         int rc = rebuild(b);
         if (rc) return rc;
     }
-    if (b->members.empty()) {
-        b->last_ms = 0.0;
-        return SCGPU_OK;
-    }
+    b->in_flight = nsteps;
+    if (b->members.empty()) return SCGPU_OK;
     BCK(cudaEventRecord(b->ev_t0, b->stream));
     for (int k = 0; k < nsteps; ++k) {
         const bool reorder = b->reorder_every > 0 && (b->steps % b->reorder_every) == 0;
         cudaGraphExec_t& gx = b->graphs[reorder ? 1 : 0];
-        if (!gx && !b->eager_next) {
-            // captured after an eager step with the same launch shapes (which
-            // also raises the kernels' shared-memory limits outside a capture)
+        if (!gx && !b->eager_call) {
             cudaGraph_t g = nullptr;
             BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
             enqueue_step(b, reorder);
@@ -259,17 +273,63 @@ int track(scgpu_batch* b, int nsteps) {
             BCK(cudaGraphLaunch(gx, b->stream));
         else
             enqueue_step(b, reorder);
-        b->eager_next = false;
         ++b->steps;
     }
     BCK(cudaEventRecord(b->ev_t1, b->stream));
     BCK(cudaGetLastError());
+    b->eager_call = false;
+    return SCGPU_OK;
+}
+
+// Waits for the launched steps; device error flags become the status.
+int wait(scgpu_batch* b) {
+    BCK(cudaSetDevice(b->device));
+    const int nsteps = b->in_flight;
+    b->in_flight = 0;
+    if (b->members.empty()) {
+        b->last_ms = 0.0;
+        return SCGPU_OK;
+    }
     int rc = check_flags(b);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, b->ev_t0, b->ev_t1);
+    if (nsteps > 0) cudaEventElapsedTime(&ms, b->ev_t0, b->ev_t1);
     b->last_ms = ms;
     for (int m : b->members) b->slots[m]->have_solve = (rc == SCGPU_OK && nsteps > 0);
     return rc;
+}
+
+int track(scgpu_batch* b, int nsteps) {
+    int rc = launch(b, nsteps);
+    if (rc) return rc;
+    return wait(b);
+}
+
+// A parked context for a new bunch on the same mesh, taken out of the pool:
+// the smallest one with enough particle capacity, else the largest (its
+// particle arrays then grow on upload; the grids are reused either way);
+// null if no parked context has this mesh.
+scgpu_ctx* take_pooled(scgpu_batch* b, const scgpu_solver_params& q, long long n) {
+    int best = -1;
+    for (int i = 0; i < (int)b->pool.size(); ++i) {
+        const scgpu_ctx* c = b->pool[i];
+        if (c->sp.mx != q.mx || c->sp.my != q.my || c->sp.mt != q.mt || c->sp.bboxincr != q.bboxincr) continue;
+        if (best < 0) {
+            best = i;
+            continue;
+        }
+        const long long cb = b->pool[best]->capacity, ci = c->capacity;
+        const bool fits_b = cb >= n, fits_i = ci >= n;
+        if ((fits_i && (!fits_b || ci < cb)) || (!fits_i && !fits_b && ci > cb)) best = i;
+    }
+    if (best < 0) return nullptr;
+    scgpu_ctx* c = b->pool[best];
+    b->pool.erase(b->pool.begin() + best);
+    return c;
+}
+
+void drain_pool(scgpu_batch* b) {
+    for (scgpu_ctx* c : b->pool) scgpu_destroy(c);
+    b->pool.clear();
 }
 
 }  // namespace
@@ -284,7 +344,10 @@ int scgpu_batch_create(scgpu_batch** out, int device, int precision) {
     scgpu_batch* b = new scgpu_batch();
     b->device = device;
     b->precision = precision;
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (cudaStreamCreateWithPriority(&b->xfer, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess ||
@@ -301,6 +364,7 @@ void scgpu_batch_destroy(scgpu_batch* b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
+    drain_pool(b);
     for (scgpu_ctx*& c : b->slots)
         if (c) {
             scgpu_destroy(c);
@@ -312,6 +376,7 @@ void scgpu_batch_destroy(scgpu_batch* b) {
     for (cudaEvent_t e : {b->ev_fork, b->ev_join, b->ev_t0, b->ev_t1})
         if (e) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->xfer) cudaStreamDestroy(b->xfer);
     if (b->side) cudaStreamDestroy(b->side);
     delete b;
 }
@@ -323,10 +388,23 @@ int scgpu_batch_add(scgpu_batch* b, const scgpu_solver_params* p, long long n, c
     if (!b || !p || !R || !P || !bp) return bfail(b, SCGPU_ERR_ARG, "null argument");
     scgpu_solver_params q = *p;
     q.precision = b->precision;
-    scgpu_ctx* c = nullptr;
-    int rc = scgpu_create(&c, &q, b->device);
-    if (rc) return bfail(b, rc, "scgpu_create failed for the new bunch");
+    scgpu_ctx* c = take_pooled(b, q, n);
+    int rc = SCGPU_OK;
+    if (!c) {
+        rc = scgpu_create(&c, &q, b->device);
+        if (rc == SCGPU_ERR_OOM && !b->pool.empty()) {
+            // parked contexts hold the memory: release them and try once more
+            drain_pool(b);
+            rc = scgpu_create(&c, &q, b->device);
+        }
+        if (rc) return bfail(b, rc, "scgpu_create failed for the new bunch");
+        scgpu_set_stream(c, b->xfer);
+    }
     rc = scgpu_bunch_upload(c, n, R, P, bp);
+    if (rc == SCGPU_ERR_OOM && !b->pool.empty()) {
+        drain_pool(b);
+        rc = scgpu_bunch_upload(c, n, R, P, bp);
+    }
     if (rc) {
         b->err = scgpu_last_error(c);
         scgpu_destroy(c);
@@ -350,11 +428,43 @@ int scgpu_batch_add(scgpu_batch* b, const scgpu_solver_params* p, long long n, c
 int scgpu_batch_remove(scgpu_batch* b, int slot) {
     if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot]) return bfail(b, SCGPU_ERR_ARG, "no such slot");
     cudaSetDevice(b->device);
+    // steps in flight still read this bunch (and the flag check reads its
+    // state): finish them first
+    if (b->in_flight) {
+        const int rc = wait(b);
+        if (rc) return rc;
+    }
     cudaStreamSynchronize(b->stream);
-    scgpu_destroy(b->slots[slot]);
+    cudaStreamSynchronize(b->side);
+    scgpu_ctx* c = b->slots[slot];
     b->slots[slot] = nullptr;
     b->dirty = true;
+    if (b->pool.size() < b->pool_max) {
+        c->have_bunch = false;
+        c->have_solve = false;
+        b->pool.push_back(c);
+    } else {
+        scgpu_destroy(c);
+    }
     return SCGPU_OK;
+}
+
+int scgpu_batch_trim(scgpu_batch* b) {
+    if (!b) return SCGPU_ERR_ARG;
+    cudaSetDevice(b->device);
+    drain_pool(b);
+    return SCGPU_OK;
+}
+
+int scgpu_batch_launch(scgpu_batch* b, int nsteps) {
+    if (!b || nsteps < 0) return bfail(b, SCGPU_ERR_ARG, "bad argument");
+    if (b->in_flight) return bfail(b, SCGPU_ERR_STATE, "steps are already in flight: call scgpu_batch_wait");
+    return launch(b, nsteps);
+}
+
+int scgpu_batch_wait(scgpu_batch* b) {
+    if (!b) return SCGPU_ERR_ARG;
+    return wait(b);
 }
 
 scgpu_ctx* scgpu_batch_member(scgpu_batch* b, int slot) {
@@ -371,6 +481,10 @@ int scgpu_batch_size(const scgpu_batch* b) {
 
 int scgpu_batch_track(scgpu_batch* b, int nsteps) {
     if (!b || nsteps < 0) return bfail(b, SCGPU_ERR_ARG, "bad argument");
+    if (b->in_flight) {
+        const int rc = wait(b);
+        if (rc) return rc;
+    }
     return track(b, nsteps);
 }
 

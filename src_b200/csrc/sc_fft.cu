@@ -858,8 +858,9 @@ __device__ __forceinline__ const Cx<T>* tw_dev(const DevBunch& d, int a) {
 // at block coordinates (work[i].y, work[i].z), with that bunch's sizes and
 // buffers (T: the forward-half type, as in convolution_t).
 template <typename T, int PASS, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_fft_pass_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void __launch_bounds__(NT) k_fft_pass_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work,
+                                                        int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     const int n0 = d.bc.n[0], n1 = d.bc.n[1], n2 = d.bc.n[2];
     const int L0 = 2 * n0, L1 = 2 * n1, L2 = 2 * n2;
@@ -906,7 +907,7 @@ template <typename T, int PASS, int V>
 struct LaunchPassBatch {
     const DevBunch* tab;
     const int4* work;
-    int n, L;
+    int nitems, n, L;
     cudaStream_t s;
     template <int LT>
     void run() {
@@ -918,29 +919,29 @@ struct LaunchPassBatch {
             return true;
         }();
         (void)limits;
-        k<<<n, NT, sm, s>>>(tab, work);
+        k<<<n, NT, sm, s>>>(tab, work, nitems);
     }
 };
 
 template <typename T, int PASS>
-void pass_batch_t(int L, int variant, const DevBunch* tab, const int4* work, int n, cudaStream_t s) {
+void pass_batch_t(int L, int variant, const DevBunch* tab, const int4* work, int nitems, int n, cudaStream_t s) {
     if (variant == 0)
-        with_length(L, LaunchPassBatch<T, PASS, 0>{tab, work, n, L, s});
+        with_length(L, LaunchPassBatch<T, PASS, 0>{tab, work, nitems, n, L, s});
     else
-        with_length(L, LaunchPassBatch<T, PASS, 1>{tab, work, n, L, s});
+        with_length(L, LaunchPassBatch<T, PASS, 1>{tab, work, nitems, n, L, s});
 }
 
 template <typename T>
-void pass_batch(int pass, int L, int variant, const DevBunch* tab, const int4* work, int n, cudaStream_t s) {
+void pass_batch(int pass, int L, int variant, const DevBunch* tab, const int4* work, int nitems, int n, cudaStream_t s) {
     switch (pass) {
-        case kPassZR2C: pass_batch_t<T, kPassZR2C>(L, variant, tab, work, n, s); break;
-        case kPassYFwd: pass_batch_t<T, kPassYFwd>(L, variant, tab, work, n, s); break;
-        case kPassXConv: pass_batch_t<T, kPassXConv>(L, variant, tab, work, n, s); break;
-        case kPassYInv: pass_batch_t<T, kPassYInv>(L, variant, tab, work, n, s); break;
-        case kPassZC2R: pass_batch_t<T, kPassZC2R>(L, variant, tab, work, n, s); break;
-        case kPassDctZ: pass_batch_t<T, kPassDctZ>(L, variant, tab, work, n, s); break;
-        case kPassDctY: pass_batch_t<T, kPassDctY>(L, variant, tab, work, n, s); break;
-        default: pass_batch_t<T, kPassDctX>(L, variant, tab, work, n, s); break;
+        case kPassZR2C: pass_batch_t<T, kPassZR2C>(L, variant, tab, work, nitems, n, s); break;
+        case kPassYFwd: pass_batch_t<T, kPassYFwd>(L, variant, tab, work, nitems, n, s); break;
+        case kPassXConv: pass_batch_t<T, kPassXConv>(L, variant, tab, work, nitems, n, s); break;
+        case kPassYInv: pass_batch_t<T, kPassYInv>(L, variant, tab, work, nitems, n, s); break;
+        case kPassZC2R: pass_batch_t<T, kPassZC2R>(L, variant, tab, work, nitems, n, s); break;
+        case kPassDctZ: pass_batch_t<T, kPassDctZ>(L, variant, tab, work, nitems, n, s); break;
+        case kPassDctY: pass_batch_t<T, kPassDctY>(L, variant, tab, work, nitems, n, s); break;
+        default: pass_batch_t<T, kPassDctX>(L, variant, tab, work, nitems, n, s); break;
     }
 }
 
@@ -994,13 +995,13 @@ void fft_pass_grid(int pass, const DevBunch& b, int variant, int* gx, int* gy) {
     }
 }
 
-void launch_fft_pass_batch(int pass, int L, int precision, int variant, const DevBunch* tab, const int4* work, int n,
-                           cudaStream_t s) {
-    if (n <= 0) return;
+void launch_fft_pass_batch(int pass, int L, int precision, int variant, const DevBunch* tab, const int4* work, int nitems,
+                           int n, cudaStream_t s) {
+    if (n <= 0 || nitems <= 0) return;
     if (precision == 0)
-        pass_batch<double>(pass, L, variant, tab, work, n, s);
+        pass_batch<double>(pass, L, variant, tab, work, nitems, n, s);
     else
-        pass_batch<float>(pass, L, variant, tab, work, n, s);
+        pass_batch<float>(pass, L, variant, tab, work, nitems, n, s);
 }
 
 FftPlan make_plan(int L) {

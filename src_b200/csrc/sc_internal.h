@@ -83,8 +83,26 @@ void launch_f64_to_f32(const double* in, float* out, long long n, cudaStream_t s
 void launch_f32_to_f64(const float* in, double* out, long long n, cudaStream_t s);
 
 // Batched launches (many bunches, one kernel): `tab` is a device array of
-// DevBunch, `work` a device array of n work items; item i = (bunch, block x,
-// block y, blocks of that bunch) drives block i.
+// DevBunch; `items` holds one entry per bunch of the launch, (bunch, first
+// block, blocks in x, blocks in y), sorted by first block; `nblocks` blocks
+// are launched and each finds its bunch by a binary search over the items.
+#ifdef __CUDACC__
+__device__ __forceinline__ int4 resolve_block(const int4* __restrict__ items, int nitems) {
+    const int blk = (int)blockIdx.x;
+    int lo = 0, hi = nitems - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&items[mid].y) <= blk)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int4 it = __ldg(&items[lo]);
+    const int local = blk - it.y;
+    // (bunch, block x, block y, blocks of the bunch)
+    return make_int4(it.x, local % it.z, local / it.z, it.z * it.w);
+}
+#endif
 enum : int {
     kBatchDrift = 0,
     kBatchPsum,
@@ -97,7 +115,8 @@ enum : int {
     kBatchGrad,
     kBatchGather,
 };
-void launch_batch(int kind, int precision, int threads, const DevBunch* tab, const int4* work, int n, cudaStream_t s);
+void launch_batch(int kind, int precision, int threads, const DevBunch* tab, const int4* items, int nitems, int nblocks,
+                  cudaStream_t s);
 
 // FFT passes of a batch: every bunch of one launch has the same transform
 // length L on the pass's axis; `variant` picks the tile shape (columns per
@@ -118,8 +137,8 @@ constexpr int kFftVariants = 2;
 void fft_pass_grid(int pass, const DevBunch& b, int variant, int* gx, int* gy);
 // Transform length of a pass's axis for a bunch.
 int fft_pass_length(int pass, const DevBunch& b);
-void launch_fft_pass_batch(int pass, int L, int precision, int variant, const DevBunch* tab, const int4* work, int n,
-                           cudaStream_t s);
+void launch_fft_pass_batch(int pass, int L, int precision, int variant, const DevBunch* tab, const int4* items,
+                           int nitems, int nblocks, cudaStream_t s);
 
 // sort TU (sc_sort.cu)
 long long scan_scratch_ints(long long n);

@@ -806,104 +806,105 @@ inline int grid_for(long long work, int cap) {
 // block, -, blocks of that bunch) and runs the same body as the single-bunch
 // kernel on the bunch's buffers (tab[bunch], a device copy of its DevBunch).
 template <bool DRIFT>
-__global__ void __launch_bounds__(kThreads, 3) k_drift_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void __launch_bounds__(kThreads, 3) k_drift_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     drift_body<DRIFT>(d.bc, d.x, d.y, d.z, d.px, d.py, d.pz, d.st, d.partials, d.ticket, VB{w.y, w.w});
 }
 
 template <bool STATS>
 __global__ void __launch_bounds__(kThreads) k_reduce_state_batch(const DevBunch* __restrict__ tab,
-                                                                 const int4* __restrict__ work, bool init_frame) {
-    const int4 w = work[blockIdx.x];
+                                                                 const int4* __restrict__ work, int nitems, bool init_frame) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     reduce_state_body<STATS>(d.bc, d.x, d.y, d.z, d.px, d.py, d.pz, d.st, d.partials, d.ticket, init_frame,
                              VB{w.y, w.w});
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) k_deposit_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void __launch_bounds__(NT) k_deposit_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     deposit_body(d.bc, d.x, d.y, d.z, d.st, d.nacc, VB{w.y, w.w});
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_assemble_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void __launch_bounds__(kThreads) k_assemble_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     assemble_body<T>(d.bc, d.st, d.nacc, (T*)d.rho, VB{w.y, w.w});
 }
 
-__global__ void k_advance_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void k_advance_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     advance_reference_body(d.bc, d.st, VB{w.y, w.w});
 }
 
-__global__ void __launch_bounds__(kThreads) k_igf_tmp_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void __launch_bounds__(kThreads) k_igf_tmp_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     igf_tmp_body(d.bc.n[0], d.bc.n[1], d.bc.n[2], d.st, d.gtmp, VB{w.y, w.w});
 }
 
-__global__ void __launch_bounds__(kThreads) k_igf_G_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void __launch_bounds__(kThreads) k_igf_G_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     igf_G_body(d.bc.n[0], d.bc.n[1], d.bc.n[2], d.gtmp, d.gline, VB{w.y, w.w});
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_grad_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void __launch_bounds__(kThreads) k_grad_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     grad_body<T>(d.bc, d.st, d.phi, (T*)d.E4, VB{w.y, w.w});
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 3) k_gather_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work) {
-    const int4 w = work[blockIdx.x];
+__global__ void __launch_bounds__(kThreads, 3) k_gather_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
     gather_body<T>(d.bc, d.x, d.y, d.z, d.px, d.py, d.pz, (const T*)d.E4, d.st, d.partials, d.ticket, VB{w.y, w.w});
 }
 
 }  // namespace
 
-void launch_batch(int kind, int precision, int threads, const DevBunch* tab, const int4* work, int n, cudaStream_t s) {
-    if (n <= 0) return;
+void launch_batch(int kind, int precision, int threads, const DevBunch* tab, const int4* work, int nitems, int nblocks,
+                  cudaStream_t s) {
+    if (nblocks <= 0 || nitems <= 0) return;
     const bool f64 = precision == 0;
     switch (kind) {
-        case kBatchDrift: k_drift_batch<true><<<n, kThreads, 0, s>>>(tab, work); break;
-        case kBatchPsum: k_reduce_state_batch<false><<<n, kThreads, 0, s>>>(tab, work, true); break;
-        case kBatchStats: k_reduce_state_batch<true><<<n, kThreads, 0, s>>>(tab, work, false); break;
+        case kBatchDrift: k_drift_batch<true><<<nblocks, kThreads, 0, s>>>(tab, work, nitems); break;
+        case kBatchPsum: k_reduce_state_batch<false><<<nblocks, kThreads, 0, s>>>(tab, work, nitems, true); break;
+        case kBatchStats: k_reduce_state_batch<true><<<nblocks, kThreads, 0, s>>>(tab, work, nitems, false); break;
         case kBatchDeposit:
             if (threads == 128)
-                k_deposit_batch<128><<<n, 128, 0, s>>>(tab, work);
+                k_deposit_batch<128><<<nblocks, 128, 0, s>>>(tab, work, nitems);
             else if (threads == 512)
-                k_deposit_batch<512><<<n, 512, 0, s>>>(tab, work);
+                k_deposit_batch<512><<<nblocks, 512, 0, s>>>(tab, work, nitems);
             else
-                k_deposit_batch<256><<<n, 256, 0, s>>>(tab, work);
+                k_deposit_batch<256><<<nblocks, 256, 0, s>>>(tab, work, nitems);
             break;
         case kBatchAssemble:
             if (f64)
-                k_assemble_batch<double><<<n, kThreads, 0, s>>>(tab, work);
+                k_assemble_batch<double><<<nblocks, kThreads, 0, s>>>(tab, work, nitems);
             else
-                k_assemble_batch<float><<<n, kThreads, 0, s>>>(tab, work);
+                k_assemble_batch<float><<<nblocks, kThreads, 0, s>>>(tab, work, nitems);
             break;
-        case kBatchAdvance: k_advance_batch<<<n, 32, 0, s>>>(tab, work); break;
-        case kBatchIgfTmp: k_igf_tmp_batch<<<n, kThreads, 0, s>>>(tab, work); break;
-        case kBatchIgfG: k_igf_G_batch<<<n, kThreads, 0, s>>>(tab, work); break;
+        case kBatchAdvance: k_advance_batch<<<nblocks, 32, 0, s>>>(tab, work, nitems); break;
+        case kBatchIgfTmp: k_igf_tmp_batch<<<nblocks, kThreads, 0, s>>>(tab, work, nitems); break;
+        case kBatchIgfG: k_igf_G_batch<<<nblocks, kThreads, 0, s>>>(tab, work, nitems); break;
         case kBatchGrad:
             if (f64)
-                k_grad_batch<double><<<n, kThreads, 0, s>>>(tab, work);
+                k_grad_batch<double><<<nblocks, kThreads, 0, s>>>(tab, work, nitems);
             else
-                k_grad_batch<float><<<n, kThreads, 0, s>>>(tab, work);
+                k_grad_batch<float><<<nblocks, kThreads, 0, s>>>(tab, work, nitems);
             break;
         case kBatchGather:
             if (f64)
-                k_gather_batch<double><<<n, kThreads, 0, s>>>(tab, work);
+                k_gather_batch<double><<<nblocks, kThreads, 0, s>>>(tab, work, nitems);
             else
-                k_gather_batch<float><<<n, kThreads, 0, s>>>(tab, work);
+                k_gather_batch<float><<<nblocks, kThreads, 0, s>>>(tab, work, nitems);
             break;
         default: break;
     }

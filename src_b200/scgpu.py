@@ -280,6 +280,9 @@ def _batch_lib():
         L.scgpu_batch_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.scgpu_batch_get_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.scgpu_batch_autotune.argtypes = [C.c_void_p, C.c_int]
+        L.scgpu_batch_launch.argtypes = [C.c_void_p, C.c_int]
+        L.scgpu_batch_wait.argtypes = [C.c_void_p]
+        L.scgpu_batch_trim.argtypes = [C.c_void_p]
         L._batch_ready = True
     return L
 
@@ -288,7 +291,8 @@ EXPORTED += [
     "scgpu_compute_potential_noalloc",
     "scgpu_batch_create", "scgpu_batch_destroy", "scgpu_batch_last_error", "scgpu_batch_add", "scgpu_batch_remove",
     "scgpu_batch_member", "scgpu_batch_size", "scgpu_batch_track", "scgpu_batch_last_track_ms",
-    "scgpu_batch_set_tuning", "scgpu_batch_get_tuning", "scgpu_batch_autotune",
+    "scgpu_batch_set_tuning", "scgpu_batch_get_tuning", "scgpu_batch_autotune", "scgpu_batch_launch",
+    "scgpu_batch_wait", "scgpu_batch_trim",
 ]
 
 
@@ -379,6 +383,19 @@ class Batch:
     def track(self, nsteps):
         self._check(_batch_lib().scgpu_batch_track(self.h, int(nsteps)), "batch_track")
         return _batch_lib().scgpu_batch_last_track_ms(self.h)
+
+    def launch(self, nsteps):
+        """Enqueues nsteps batched steps and returns at once; wait() ends them."""
+        self._check(_batch_lib().scgpu_batch_launch(self.h, int(nsteps)), "batch_launch")
+
+    def wait(self):
+        """Finishes launched steps; returns their device milliseconds."""
+        self._check(_batch_lib().scgpu_batch_wait(self.h), "batch_wait")
+        return _batch_lib().scgpu_batch_last_track_ms(self.h)
+
+    def trim(self):
+        """Frees the parked contexts of removed bunches."""
+        self._check(_batch_lib().scgpu_batch_trim(self.h), "batch_trim")
 
     def set_tuning(self, deposit_threads=256, L=0, fft_variant=0):
         self._check(_batch_lib().scgpu_batch_set_tuning(self.h, int(deposit_threads), int(L), int(fft_variant)),

@@ -85,6 +85,8 @@ class Server:
         self.particle_steps = 0
         self.makespan_s = 0.0
         self.tuning = {}
+        # host wall time by activity, and device time of the batched steps
+        self.time = {"admit_s": 0.0, "track_wall_s": 0.0, "track_gpu_s": 0.0, "release_s": 0.0}
 
     def calibrate(self, jobs, trial_steps=3):
         """Runs the autotuner on a separate batch of `jobs` (one per mesh size
@@ -107,45 +109,66 @@ class Server:
     def run(self, jobs, realtime=True):
         """Serves `jobs`.  With realtime the arrivals are honoured on the wall
         clock; otherwise every job is available at once.  Returns the list of
-        Results in completion order."""
+        Results in completion order.
+
+        Each round launches k steps for the current slots and, while the
+        device works, admits the jobs that have arrived (their bunches are
+        prepared and uploaded meanwhile; they join at the next round)."""
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival_s))
-        active = {}  # slot -> [job, remaining steps, admitted_s, footprint]
+        active = {}   # slot -> [job, remaining steps, admitted_s, footprint]
+        joining = {}  # admitted during the current round
         results = []
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
-        while pending or active:
+
+        def admit():
             t = now()
-            # admission: arrived jobs, in order, while their footprint fits
             while pending and (not realtime or pending[0].arrival_s <= t):
                 job = pending[0]
                 fp = job.footprint_bytes(self.precision)
-                if active and self.used + fp > self.budget:
+                if (active or joining) and self.used + fp > self.budget:
                     break
                 pending.popleft()
+                ta = time.perf_counter()
                 R, P = self.masters.bunch(job)
                 slot = self.batch.add((job.mesh,) * 3, R, P, DT, job.q_macro, MASS_EV, ref_P=job.ref_P)
-                active[slot] = [job, job.steps, now(), fp]
+                self.time["admit_s"] += time.perf_counter() - ta
+                joining[slot] = [job, job.steps, now(), fp]
                 self.used += fp
-            if not active:
-                if pending and realtime:
-                    time.sleep(max(0.0, min(pending[0].arrival_s - now(), 0.01)))
-                continue
-            # every active job takes k steps this round (k <= its remaining steps)
-            k = min(MAX_ROUND_STEPS, min(a[1] for a in active.values()))
-            self.batch.track(k)
-            self.rounds += 1
-            self.steps += k
-            for slot, a in list(active.items()):
-                self.particle_steps += a[0].particles * k
-                a[1] -= k
-                if a[1] <= 0:
-                    R = P = None
-                    if self.keep_results:
-                        R, P = self.batch.member(slot).download()
-                    self.batch.remove(slot)
-                    self.used -= a[3]
-                    results.append(Result(a[0], a[2], now(), R, P))
-                    del active[slot]
+
+        while pending or active or joining:
+            k = 0
+            if active:
+                # every active job takes k steps this round (k <= its remaining steps)
+                k = min(MAX_ROUND_STEPS, min(a[1] for a in active.values()))
+                tt = time.perf_counter()
+                self.batch.launch(k)
+                self.time["track_wall_s"] += time.perf_counter() - tt
+            admit()
+            if k:
+                tt = time.perf_counter()
+                gpu_ms = self.batch.wait()
+                self.time["track_wall_s"] += time.perf_counter() - tt
+                self.time["track_gpu_s"] += gpu_ms * 1e-3
+                self.rounds += 1
+                self.steps += k
+                for slot, a in list(active.items()):
+                    self.particle_steps += a[0].particles * k
+                    a[1] -= k
+                    if a[1] <= 0:
+                        tr = time.perf_counter()
+                        R = P = None
+                        if self.keep_results:
+                            R, P = self.batch.member(slot).download()
+                        self.batch.remove(slot)
+                        self.time["release_s"] += time.perf_counter() - tr
+                        self.used -= a[3]
+                        results.append(Result(a[0], a[2], now(), R, P))
+                        del active[slot]
+            active.update(joining)
+            joining.clear()
+            if not active and pending and realtime:
+                time.sleep(max(0.0, min(pending[0].arrival_s - now(), 0.01)))
         self.makespan_s = now()
         return results
 

@@ -23,10 +23,12 @@ class FakeBatch:
     def remove(self, slot):
         del self.slots[slot]
 
-    def track(self, k):
+    def launch(self, k):
         self.tracked.append((k, len(self.slots)))
         for s in self.slots:
             self.steps[s] += k
+
+    def wait(self):
         return 0.0
 
     def set_tuning(self, *a):
@@ -51,6 +53,8 @@ def test_every_job_takes_exactly_its_steps():
     srv = Server(hbm_budget_bytes=1 << 40, batch=fb, masters=FakeMasters())
     res = srv.run(jobs, realtime=False)
     assert sorted(r.job.job_id for r in res) == list(range(6))
+    # a slot never steps past its job's request
+    assert all(fb.steps[s] <= 40 for s in fb.steps)
     assert srv.particle_steps == sum(j.particles * j.steps for j in jobs)
     assert all(k <= 16 for k, _ in fb.tracked)
     # completion order follows the requested step counts
