@@ -106,11 +106,19 @@ void enqueue_reorder(scgpu_ctx* c, cudaStream_t s) {
 }
 
 // one ParallelTTracker step on the context's stream
+//   ref:  reference-particle update (needs only the tracker state; joins
+//         before the gather, which applies its frame change)
+//   main: drift -> deposit -> assemble [-> reorder] -> FFT A, B
+//   side: (after the drift's mesh) Green's function, its spectrum
+//   main: (join side) FFT C, D, E -> grad -> (join ref) gather/kick/push
+// The branches write disjoint StepState fields.
 void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
     DevBunch& b = c->b;
+    cudaEventRecord(c->ev_start, s);
+    cudaStreamWaitEvent(c->ref, c->ev_start, 0);
+    launch_advance_reference(b, c->ref);
+    cudaEventRecord(c->ev_ref, c->ref);
     launch_drift_to_beam(b, true, s);
-    // the Green's function depends only on the mesh: a side branch beside
-    // deposit, reference-particle update and reorder
     cudaEventRecord(c->ev_fork, s);
     cudaStreamWaitEvent(c->side, c->ev_fork, 0);
     launch_igf(b, nullptr, c->side);
@@ -118,11 +126,12 @@ void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
     cudaEventRecord(c->ev_join, c->side);
     launch_deposit(b, s);
     launch_assemble_rho(b, s);
-    launch_advance_reference(b, s);
     if (reorder) enqueue_reorder(c, s);
+    launch_convolution_part(b, kConvSelfField, kConvForwardPart, s);
     cudaStreamWaitEvent(s, c->ev_join, 0);
-    launch_convolution(b, kConvSelfField, s);
+    launch_convolution_part(b, kConvSelfField, kConvRestPart, s);
     launch_grad(b, s);
+    cudaStreamWaitEvent(s, c->ev_ref, 0);
     launch_gather_kick_push(b, stats, s);
 }
 
@@ -288,9 +297,12 @@ int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
     }
     cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
     cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&c->ref, cudaStreamNonBlocking);
     c->stream = c->own;
     cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_ref, cudaEventDisableTiming);
     cudaEventCreate(&c->ev_t0);
     cudaEventCreate(&c->ev_t1);
     cudaMemsetAsync(b.nacc, 0, M * 2 * sizeof(unsigned long long), c->own);
@@ -325,7 +337,10 @@ void scgpu_destroy(scgpu_ctx* c) {
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->ev_t0) cudaEventDestroy(c->ev_t0);
     if (c->ev_t1) cudaEventDestroy(c->ev_t1);
+    if (c->ev_start) cudaEventDestroy(c->ev_start);
+    if (c->ev_ref) cudaEventDestroy(c->ev_ref);
     if (c->side) cudaStreamDestroy(c->side);
+    if (c->ref) cudaStreamDestroy(c->ref);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
 }

@@ -8,9 +8,10 @@
 // passes are grouped by the transform length of their axis, since the length
 // is a template constant of the kernels.  The step order is the single-bunch one (sc_api.cu enqueue_step):
 //
-//   main: drift -> deposit -> assemble -> reference update [-> cell reorder]
+//   ref:  reference-particle updates (joined before the gather)
+//   main: drift -> deposit -> assemble [-> cell reorder] -> FFT A, B
 //   side: Green's function (antiderivative, 8-corner G, three DCT passes)
-//   main: (join) convolution A..E -> grad -> gather/kick/push
+//   main: (join side) FFT C, D, E -> grad -> (join ref) gather/kick/push
 //
 // With unchanged membership the step is captured once per variant (with and
 // without the periodic cell reorder) and replayed as one graph launch.
@@ -44,7 +45,8 @@ int blocks_for(long long work, int threads, int cap) {
 }
 
 struct Launch {
-    int lane;   // 0 main before the fork, 1 side branch, 2 main before the join, 3 main after the join
+    int lane;   // 0 drift, 1 Green's-function branch, 2 deposit, 6 forward FFT, 3 rest of the solve,
+                // 4 reference-particle branch, 5 gather (see enqueue_step)
     int kind;   // kBatch* for particle / grid kernels, -1 for an FFT pass
     int pass;   // kPass* when kind == -1
     int L;      // transform length of the pass's axis
@@ -60,7 +62,8 @@ struct scgpu_batch {
     int precision = SCGPU_PLAIN_FP64;
     std::vector<scgpu_ctx*> slots;
     std::vector<int> members;   // occupied slots in table order
-    cudaStream_t stream = nullptr, side = nullptr;
+    cudaStream_t stream = nullptr, side = nullptr, ref = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_ref = nullptr;
     // Uploads and downloads of the bunches run here, at the highest stream
     // priority, so that a bunch joining during a long batched round gets SMs
     // as soon as blocks of the round retire instead of waiting for the round.
@@ -124,6 +127,7 @@ int rebuild(scgpu_batch* b) {
     // the tables are rewritten below: nothing enqueued may still read them
     BCK(cudaStreamSynchronize(b->stream));
     BCK(cudaStreamSynchronize(b->side));
+    BCK(cudaStreamSynchronize(b->ref));
     drop_graphs(b);
     b->members.clear();
     for (int s = 0; s < (int)b->slots.size(); ++s)
@@ -173,14 +177,14 @@ int rebuild(scgpu_batch* b) {
     add_pass(1, kPassDctX);
     add_per_bunch(2, kBatchDeposit, [dep](const DevBunch& d) { return blocks_for(d.bc.N, dep, 148 * 8 * 256 / dep); });
     add_per_bunch(2, kBatchAssemble, [&](const DevBunch& d) { return blocks_for(cells(d), 256, kCellGridCap); });
-    add_per_bunch(2, kBatchAdvance, [](const DevBunch&) { return 1; });
-    add_pass(3, kPassZR2C);
-    add_pass(3, kPassYFwd);
+    add_per_bunch(4, kBatchAdvance, [](const DevBunch&) { return 1; });
+    add_pass(6, kPassZR2C);
+    add_pass(6, kPassYFwd);
     add_pass(3, kPassXConv);
     add_pass(3, kPassYInv);
     add_pass(3, kPassZC2R);
     add_per_bunch(3, kBatchGrad, [&](const DevBunch& d) { return blocks_for(cells(d), 256, kCellGridCap); });
-    add_per_bunch(3, kBatchGather, [](const DevBunch& d) { return d.red_blocks; });
+    add_per_bunch(5, kBatchGather, [](const DevBunch& d) { return d.red_blocks; });
     if (nm > b->tab_cap) {
         if (b->d_tab) cudaFree(b->d_tab);
         if (b->d_flags) cudaFree(b->d_flags);
@@ -218,16 +222,23 @@ void enqueue_lane(scgpu_batch* b, int lane, cudaStream_t s) {
 
 void enqueue_step(scgpu_batch* b, bool reorder) {
     cudaStream_t s = b->stream;
-    enqueue_lane(b, 0, s);
+    cudaEventRecord(b->ev_start, s);
+    cudaStreamWaitEvent(b->ref, b->ev_start, 0);
+    enqueue_lane(b, 4, b->ref);  // reference particles
+    cudaEventRecord(b->ev_ref, b->ref);
+    enqueue_lane(b, 0, s);       // drift
     cudaEventRecord(b->ev_fork, s);
     cudaStreamWaitEvent(b->side, b->ev_fork, 0);
-    enqueue_lane(b, 1, b->side);
+    enqueue_lane(b, 1, b->side);  // Green's functions
     cudaEventRecord(b->ev_join, b->side);
-    enqueue_lane(b, 2, s);
+    enqueue_lane(b, 2, s);       // deposit, assemble
     if (reorder)
         for (int m : b->members) ctx_enqueue_reorder(b->slots[m], s);
+    enqueue_lane(b, 6, s);       // FFT A, B
     cudaStreamWaitEvent(s, b->ev_join, 0);
-    enqueue_lane(b, 3, s);
+    enqueue_lane(b, 3, s);       // FFT C, D, E, grad
+    cudaStreamWaitEvent(s, b->ev_ref, 0);
+    enqueue_lane(b, 5, s);       // gather, kick, push
 }
 
 int check_flags(scgpu_batch* b) {
@@ -349,6 +360,9 @@ int scgpu_batch_create(scgpu_batch** out, int device, int precision) {
     if (cudaStreamCreateWithPriority(&b->xfer, cudaStreamNonBlocking, greatest) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->ref, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_ref, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreate(&b->ev_t0) != cudaSuccess || cudaEventCreate(&b->ev_t1) != cudaSuccess) {
@@ -373,11 +387,12 @@ void scgpu_batch_destroy(scgpu_batch* b) {
     if (b->d_tab) cudaFree(b->d_tab);
     if (b->d_work) cudaFree(b->d_work);
     if (b->d_flags) cudaFree(b->d_flags);
-    for (cudaEvent_t e : {b->ev_fork, b->ev_join, b->ev_t0, b->ev_t1})
+    for (cudaEvent_t e : {b->ev_fork, b->ev_join, b->ev_t0, b->ev_t1, b->ev_start, b->ev_ref})
         if (e) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->xfer) cudaStreamDestroy(b->xfer);
     if (b->side) cudaStreamDestroy(b->side);
+    if (b->ref) cudaStreamDestroy(b->ref);
     delete b;
 }
 
@@ -436,6 +451,7 @@ int scgpu_batch_remove(scgpu_batch* b, int slot) {
     }
     cudaStreamSynchronize(b->stream);
     cudaStreamSynchronize(b->side);
+    cudaStreamSynchronize(b->ref);
     scgpu_ctx* c = b->slots[slot];
     b->slots[slot] = nullptr;
     b->dirty = true;

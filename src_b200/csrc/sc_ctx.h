@@ -15,7 +15,9 @@ struct scgpu_ctx {
     cudaStream_t stream = nullptr;   // work stream (own or the caller's)
     cudaStream_t own = nullptr;
     cudaStream_t side = nullptr;     // Green's function branch
+    cudaStream_t ref = nullptr;      // reference-particle branch
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_ref = nullptr;
     long long capacity = 0;
     long long n = 0;
     bool have_bunch = false;

@@ -1072,8 +1072,10 @@ void launch_green_transform(const DevBunch& b, cudaStream_t s) {
 
 // T is the type of the forward half (A, B and the forward x transform of C);
 // the inverse half (C's inverse, D, E) is FP64 in both forms.
+// parts: kConvForwardPart (A, B: need only rho) and/or kConvRestPart (C, D,
+// E: need the spectrum of G as well).
 template <typename T>
-static void convolution_t(const DevBunch& b, int mode, cudaStream_t s) {
+static void convolution_t(const DevBunch& b, int mode, int parts, cudaStream_t s) {
     using C = Cx<T>;
     const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
     const int L0 = 2 * n0, L1 = 2 * n1, L2 = 2 * n2;
@@ -1090,8 +1092,11 @@ static void convolution_t(const DevBunch& b, int mode, cudaStream_t s) {
     normFact /= L0;
     normFact /= L1;
     normFact /= L2;
-    with_length(L2, LaunchA<T>{(const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz, s});
-    with_length(L1, LaunchY<T, false>{fwd, n0, L0, n1, L1, n2 + 1, py, twy, s});
+    if (parts & kConvForwardPart) {
+        with_length(L2, LaunchA<T>{(const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz, s});
+        with_length(L1, LaunchY<T, false>{fwd, n0, L0, n1, L1, n2 + 1, py, twy, s});
+    }
+    if (!(parts & kConvRestPart)) return;
     with_length(L0, LaunchC<T>{fwd, inv, (const T*)b.ghat, n0, n1, L1, (n2 + 1) * L1, px, twx, twx_d, s});
     with_length(L1, LaunchY<double, true>{inv, n0, L0, L1, n1, n2 + 1, py, twy_d, s});
     if (mode == kConvSelfField)
@@ -1101,10 +1106,14 @@ static void convolution_t(const DevBunch& b, int mode, cudaStream_t s) {
 }
 
 void launch_convolution(const DevBunch& b, int mode, cudaStream_t s) {
+    launch_convolution_part(b, mode, kConvForwardPart | kConvRestPart, s);
+}
+
+void launch_convolution_part(const DevBunch& b, int mode, int parts, cudaStream_t s) {
     if (b.precision == 0)
-        convolution_t<double>(b, mode, s);
+        convolution_t<double>(b, mode, parts, s);
     else
-        convolution_t<float>(b, mode, s);
+        convolution_t<float>(b, mode, parts, s);
 }
 
 void fft_set_smem_limits() {

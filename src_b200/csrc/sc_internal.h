@@ -148,6 +148,9 @@ void launch_sort(const DevBunch& b, cudaStream_t s);
 // FFT TU (sc_fft.cu)
 void launch_green_transform(const DevBunch& b, cudaStream_t s);
 void launch_convolution(const DevBunch& b, int mode, cudaStream_t s);
+// the forward passes (A, B) need rho only; the rest (C, D, E) also the spectrum of G
+enum : int { kConvForwardPart = 1, kConvRestPart = 2 };
+void launch_convolution_part(const DevBunch& b, int mode, int parts, cudaStream_t s);
 size_t fft_smem_bytes(const DevBunch& b);
 void upload_twiddles(DevBunch& b, cudaStream_t s);
 void fft_set_smem_limits();

@@ -197,10 +197,24 @@ __device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restr
     if (threadIdx.x == 0) r2b_s = st->r2b;
     __syncthreads();
     double v[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};  // min x,y,z, -max x,y,z
-    for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
-        double R[3] = {x[i], y[i], z[i]};
+    // The next particle's loads are issued before the current one is
+    // computed, so each thread keeps two particles' reads in flight.
+    const long long stride = (long long)g.nblk * blockDim.x;
+    long long i = g.blk * (long long)blockDim.x + threadIdx.x;
+    double Rn[3] = {0.0, 0.0, 0.0}, Pn[3] = {0.0, 0.0, 0.0};
+    if (i < bc.N) {
+        Rn[0] = x[i], Rn[1] = y[i], Rn[2] = z[i];
+        if constexpr (DRIFT) Pn[0] = px[i], Pn[1] = py[i], Pn[2] = pz[i];
+    }
+    for (; i < bc.N; i += stride) {
+        double R[3] = {Rn[0], Rn[1], Rn[2]};
+        const double P[3] = {Pn[0], Pn[1], Pn[2]};
+        const long long j = i + stride;
+        if (j < bc.N) {
+            Rn[0] = x[j], Rn[1] = y[j], Rn[2] = z[j];
+            if constexpr (DRIFT) Pn[0] = px[j], Pn[1] = py[j], Pn[2] = pz[j];
+        }
         if constexpr (DRIFT) {
-            const double P[3] = {px[i], py[i], pz[i]};
             push_r(R, P, bc.s_cdt, bc.rs_cdt);
             double b[3];
             trafo_transform_to(*fresh(&r2b_s), R, b);
