@@ -227,6 +227,9 @@ def main():
     ap.add_argument("--serve", action="store_true",
                     help="serving loop: Poisson arrivals at 50 jobs/s for --serve-seconds (one JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--binned", action="store_true",
+                    help="photoinjector mode: energy bins with image charges (one JSON line)")
+    ap.add_argument("--nbins", type=int, default=10)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global N_PARTICLES, MESH, BZ, WORKLOAD
@@ -240,6 +243,9 @@ def main():
         return
     if args.serve:
         serve(args, local)
+        return
+    if args.binned:
+        binned(args, local)
         return
 
     if args.impl == "reference":
@@ -494,6 +500,75 @@ def batched(args, local):
                                        "note": f"each bunch alone, {probe}-step probe scaled to {steps} steps"},
         "speedup_vs_sequential": seq_ms / ms,
         "clocks": clk, "data": "synthetic (seeded)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def binned(args, local):
+    """Photoinjector mode: the energy-bin loop with image charges
+    (ParallelTTracker.cpp:567-578, PartBunch::computeSelfFields(int bin)):
+    a 1e6-particle bunch near the cathode with --nbins energy bins (seeded
+    photoinjector_bunch) on a 64^3 mesh; per step and bin two Green's
+    functions and two convolutions.  --steps (100 unless given) timed steps,
+    device time, bunch resident; L2 flushed before each step.  Beside it the
+    oracle's binned step on the host (one core, 1e5 particles / 32^3, one
+    step) as the CPU reference of this mode."""
+    import torch
+
+    from src_b200 import scgpu
+    from src_b200.bunch import photoinjector_bunch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    prec = scgpu.PLAIN_FP64 if args.precision == "fp64" else scgpu.MIXED
+    steps = args.steps if args.steps != 1000 else 100
+    N, mesh, nb = N_PARTICLES, MESH, args.nbins
+    R, P, bins = photoinjector_bunch(N, nbins=nb)
+    Q = -1e-9 / N
+    mass = 0.51099892e-03 * 1.0e9
+    with scgpu.Context((mesh,) * 3, precision=prec, device=local) as c:
+        stream = torch.cuda.current_stream(dev)
+        c.set_stream(stream.cuda_stream)
+        c.upload(R, P, DT, Q, mass, ref_P=(0.0, 0.0, 1.0))
+        c.set_energy_bins(bins, nb)
+        c.track(args.warmup)
+        kernels = c.kernels_per_step()
+        flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(local)
+        clocks.start()
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            c.track(1)
+            ends[k].record(stream)
+        torch.cuda.synchronize(dev)
+        clk = clocks.stop()
+        ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+        gam, cnt = c.bin_gammas()
+        bp = c.beam_parameters()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.lib()
+        Rc, Pc, bc = photoinjector_bunch(100_000, nbins=nb, bunch_id=1)
+        tr = O.OracleTracker(O.make_params((32, 32, 32), DT, ref_pz=1.0), -1e-9 / 100_000)
+        t0 = time.perf_counter()
+        tr.track(Rc, Pc, 1, bins=bc, nbins=nb)
+        cs = time.perf_counter() - t0
+        cpu = {"value": 100_000 / cs, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+               "sample": f"oracle binned step, 1e5 particles, 32^3, {nb} bins, 1 step ({cs:.2f} s)"}
+    line = {
+        "metric": "particle-steps/s (energy bins + image charges)", "value": N * steps / (ms * 1e-3),
+        "unit": "particle-steps/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms / steps, "higher_is_better": True, "precision": args.precision,
+        "config": {"workload": f"photoinjector bunch {N} e-, {mesh}^3 mesh, {nb} energy bins, image charges",
+                   "l2": "flushed before every timed step (256 MiB write)"},
+        "ms_per_bin": ms / steps / nb, "kernels_per_step": kernels, "gpu_launches": kernels * steps,
+        "bin_gammas": [float(g) for g in gam], "eps_norm": [float(v) for v in bp["eps_norm"]],
+        "clocks": clk, "cpu_baseline": cpu, "data": "synthetic (seeded)",
     }
     print(json.dumps(line), flush=True)
 

@@ -17,10 +17,23 @@
  *   scgpu_compute_potential, scgpu_compute_potential_device
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr)
  *       (src/Solvers/PoissonSolver.h:28; FFTPoissonSolver.cpp:337-382)
+ *   scgpu_compute_potential_image, scgpu_compute_potential_image_device
+ *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr, double zshift)
+ *       (src/Solvers/PoissonSolver.h:59; FFTPoissonSolver.cpp:287-327 with
+ *       shiftedIntGreensFunction :546-639 and mirrorRhoField(Field_t&) :667-693)
  *   scgpu_compute_self_fields
  *       PartBunch::computeSelfFields()  (src/Classic/Algorithms/PartBunch.cpp:482-647,
  *       declared PartBunchBase.h:372, called ParallelTTracker.cpp:583),
  *       preceded by boundp() (PartBunchBase.hpp:802-884)
+ *   scgpu_compute_self_fields_binned
+ *       the energy-bin loop of ParallelTTracker::computeSpaceChargeFields
+ *       (ParallelTTracker.cpp:567-578): calcGammas (PartBunchBase.hpp:639-683),
+ *       setBinCharge (:722-725) and PartBunch::computeSelfFields(int bin)
+ *       (PartBunch.cpp:138-430) for every emitted bin, preceded by boundp()
+ *   scgpu_set_energy_bins, scgpu_get_bin_gammas
+ *       the Bin attribute and energy-bin state of PartBunchBase
+ *       (weHaveEnergyBins :458-464, getLastEmittedEnergyBin :409-416,
+ *       Rebin :432-446, getBinGamma :710-713) for the resident bunch of scgpu_track
  *   scgpu_bunch_upload / scgpu_bunch_download
  *       DKS writeDataAsync / readData of R, P  (ParallelTTracker.h:501-512, :514-529)
  *   scgpu_register_host / scgpu_unregister_host
@@ -145,6 +158,29 @@ int scgpu_compute_potential_device(scgpu_ctx* ctx, double* rho_inout_device, con
 int scgpu_compute_self_fields(scgpu_ctx* ctx, long long n, const double* R, const double* P, double* q_macro, double dT,
                               double* Ef, double* Bf);
 
+/* PoissonSolver::computePotential(rho, hr, zshift): rho in, the potential of
+ * its image charge out (in place, same units as scgpu_compute_potential):
+ * minus the convolution with the integrated Green's function shifted by
+ * zshift along z, read back with z flipped (index k <- nz - 1 - k). */
+int scgpu_compute_potential_image(scgpu_ctx* ctx, double* rho_inout, const double hr[3], double zshift);
+int scgpu_compute_potential_image_device(scgpu_ctx* ctx, double* rho_inout_device, const double hr[3], double zshift);
+
+/* Energy bins: bins[i] in [0, nbins) for particle i; the fields of bins
+ * [0, min(last_emitted, nbins)) and of their image charges are summed; at
+ * most 64 bins. */
+#define SCGPU_MAX_BINS 64
+
+/* The energy-bin loop of computeSpaceChargeFields on a bunch already in the
+ * beam frame: boundp, calcGammas, then per emitted bin the CIC deposit of
+ * its particles (charge q_macro each), the bin's own field and its image's
+ * (the bin's gamma for the boost, its image shifted behind the cathode
+ * plane z = 0); writes Ef, Bf (N x 3, beam frame, summed over the bins) and,
+ * if bin_gamma is not NULL, the nbins bin gammas (1 for an empty bin).
+ * q_macro is left unchanged (the reference restores Q after every bin). */
+int scgpu_compute_self_fields_binned(scgpu_ctx* ctx, long long n, const double* R, const double* P, const int* bins,
+                                     int nbins, int last_emitted, double q_macro, double dT, double* Ef, double* Bf,
+                                     double* bin_gamma);
+
 int scgpu_register_host(scgpu_ctx* ctx, void* ptr, long long bytes);
 int scgpu_unregister_host(scgpu_ctx* ctx, void* ptr);
 
@@ -158,6 +194,15 @@ int scgpu_bunch_download(scgpu_ctx* ctx, double* R, double* P);
  * moment sums of the state at the end of each step (asynchronous copies;
  * pinned memory keeps them off the critical path). */
 int scgpu_track(scgpu_ctx* ctx, int nsteps, double* stats);
+
+/* Energy bins of the resident bunch: bins[i] is the bin of particle i in the
+ * order of the last scgpu_bunch_upload (an upload clears them).  With
+ * nbins > 0 scgpu_track computes the self fields by the energy-bin loop with
+ * image charges; nbins == 0 returns to one solve (Distribution::Rebin).
+ * The bins travel with the particles through the cell reorder. */
+int scgpu_set_energy_bins(scgpu_ctx* ctx, const int* bins, int nbins, int last_emitted);
+/* gammas (and, if count is not NULL, particle counts) of the nbins bins at the last step */
+int scgpu_get_bin_gammas(scgpu_ctx* ctx, double* gamma, long long* count);
 
 int scgpu_get_tracker_state(scgpu_ctx* ctx, scgpu_tracker_state* out);
 int scgpu_beam_parameters(scgpu_ctx* ctx, scgpu_beam_params* out);

@@ -215,6 +215,58 @@ def compute_potential(rho, hr):
     return r
 
 
+def igf_shifted(nr, hr, zshift):
+    """Shifted integrated Green's function of the image charge, doubled grid
+    [2nz, 2ny, 2nx] (mirrored in x and y only)."""
+    G = np.empty((2 * nr[2], 2 * nr[1], 2 * nr[0]), dtype=np.float64)
+    lib().sco_igf_shifted((C.c_int * 3)(*nr), (C.c_double * 3)(*hr), C.c_double(zshift), _ptr(G))
+    return G
+
+
+def compute_potential_shifted(rho, hr, zshift):
+    """FFTPoissonSolver::computePotential(rho, hr, zshift): the image-charge
+    convolution of rho [nz, ny, nx], read back with z flipped."""
+    r = _f64(rho).copy()
+    nr = (C.c_int * 3)(r.shape[2], r.shape[1], r.shape[0])
+    rc = lib().sco_compute_potential_shifted(nr, _ptr(r), (C.c_double * 3)(*hr), C.c_double(zshift))
+    if rc:
+        raise RuntimeError(f"sco_compute_potential_shifted failed: {rc}")
+    return r
+
+
+def bin_gammas(P, bins, nbins):
+    """calcGammas: mean gamma per energy bin (1 for an empty bin) and counts."""
+    P = _f64(P)
+    b = np.ascontiguousarray(bins, dtype=np.int32)
+    g = np.empty(nbins, dtype=np.float64)
+    cnt = np.empty(nbins, dtype=np.int64)
+    rc = lib().sco_bin_gammas(C.c_longlong(P.shape[0]), _ptr(P), b.ctypes.data_as(C.POINTER(C.c_int)),
+                              C.c_int(nbins), _ptr(g), cnt.ctypes.data_as(C.POINTER(C.c_longlong)))
+    if rc:
+        raise RuntimeError(f"sco_bin_gammas failed: {rc}")
+    return g, cnt
+
+
+def compute_self_fields_binned(params, qi, R, P, bins, nbins, last_emitted=None):
+    """The energy-bin loop of computeSpaceChargeFields on a beam-frame bunch:
+    returns (Ef, Bf, bin gammas, debug dict with the mesh)."""
+    R = _f64(R)
+    P = _f64(P)
+    n = R.shape[0]
+    b = np.ascontiguousarray(bins, dtype=np.int32)
+    Ef = np.empty_like(R)
+    Bf = np.empty_like(R)
+    g = np.empty(nbins, dtype=np.float64)
+    dbg = Debug()
+    le = nbins if last_emitted is None else last_emitted
+    rc = lib().sco_compute_self_fields_binned(C.byref(params), C.c_double(qi), C.c_longlong(n), _ptr(R), _ptr(P),
+                                              b.ctypes.data_as(C.POINTER(C.c_int)), C.c_int(nbins), C.c_int(le),
+                                              _ptr(Ef), _ptr(Bf), _ptr(g), C.byref(dbg))
+    if rc:
+        raise RuntimeError(f"compute_self_fields_binned failed: {rc}")
+    return Ef, Bf, g, _debug_dict(dbg, {}, list(params.nr))
+
+
 def neg_grad_scaled(phi, h, gammaz):
     p = _f64(phi)
     nr = (C.c_int * 3)(p.shape[2], p.shape[1], p.shape[0])
@@ -350,9 +402,11 @@ class OracleTracker:
     def ref_P(self):
         return np.array(self.tr.ref_P)
 
-    def track(self, R, P, nsteps, want_debug=False):
+    def track(self, R, P, nsteps, want_debug=False, bins=None, nbins=0, last_emitted=None):
         """Advance R, P (N x 3, updated in place) by nsteps.  With want_debug
-        the last step's grids and fields are returned."""
+        the last step's grids and fields are returned.  With bins (one
+        energy bin per particle, nbins bins) the self fields are the
+        energy-bin loop with image charges."""
         assert R.dtype == np.float64 and R.flags.c_contiguous
         assert P.dtype == np.float64 and P.flags.c_contiguous
         n = R.shape[0]
@@ -367,7 +421,14 @@ class OracleTracker:
             dbg.rho, dbg.phi, dbg.E = _ptr(grids["rho"]), _ptr(grids["phi"]), _ptr(grids["E"])
             dbg.Ef, dbg.Bf = _ptr(grids["Ef"]), _ptr(grids["Bf"])
             dbgp = C.byref(dbg)
-        rc = lib().sco_track(C.byref(self.tr), C.c_longlong(n), _ptr(R), _ptr(P), C.c_int(nsteps), dbgp)
+        if bins is None:
+            rc = lib().sco_track(C.byref(self.tr), C.c_longlong(n), _ptr(R), _ptr(P), C.c_int(nsteps), dbgp)
+        else:
+            b = np.ascontiguousarray(bins, dtype=np.int32)
+            le = nbins if last_emitted is None else last_emitted
+            rc = lib().sco_track_binned(C.byref(self.tr), C.c_longlong(n), _ptr(R), _ptr(P),
+                                        b.ctypes.data_as(C.POINTER(C.c_int)), C.c_int(nbins), C.c_int(le),
+                                        C.c_int(nsteps), dbgp)
         if rc:
             raise RuntimeError(f"sco_track failed: {rc}")
         if not want_debug:

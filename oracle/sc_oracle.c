@@ -1057,10 +1057,242 @@ int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const
 }
 
 /* ------------------------------------------------------------------------ */
+/* shifted integrated Green's function for the image charge                  */
+/* (FFTPoissonSolver::shiftedIntGreensFunction, FFTPoissonSolver.cpp:546-639, */
+/* and mirrorRhoField(ggrn2), :667-693).  Output: doubled real grid G2,        */
+/* (2nx)(2ny)(2nz), x fastest.  Along z the grid is not mirrored: indices     */
+/* k <= nz hold the offsets k (antiderivative planes at k hz - hz/2 + zshift), */
+/* indices nz < k < 2nz the offsets k - 2nz (planes shifted by -nz hz).  No   */
+/* G[0,0,0] overwrite.  The planes at index n of x and y are, as in sco_igf,  */
+/* the closed form (the reference reads them outside tmpgreen's domain; they  */
+/* never reach the physical block of phi).                                    */
+/* ------------------------------------------------------------------------ */
+void sco_igf_shifted(const int* nr, const double* hr, double zshift, double* G2) {
+    const long long n0 = nr[0], n1 = nr[1], n2 = nr[2];
+    const long long t0 = n0 + 2, t1 = n1 + 2, t2 = n2 + 2;
+    const long long L0 = 2 * n0, L1 = 2 * n1, L2 = 2 * n2;
+    double cellVolume = hr[0] * hr[1] * hr[2];
+    double* ta = (double*)malloc(t0 * t1 * t2 * sizeof(double));
+    double* tb = (double*)malloc(t0 * t1 * t2 * sizeof(double));
+    SCO_PAR
+    for (long long k = 0; k < t2; ++k)
+        for (long long j = 0; j < t1; ++j)
+            for (long long i = 0; i < t0; ++i) {
+                double vx = i * hr[0] - hr[0] / 2;
+                double vy = j * hr[1] - hr[1] / 2;
+                double vz = k * hr[2] - hr[2] / 2 + zshift;
+                ta[i + t0 * (j + t1 * k)] = igf_antiderivative(vx, vy, vz, cellVolume);
+                vz = k * hr[2] - hr[2] / 2 + zshift - n2 * hr[2];
+                tb[i + t0 * (j + t1 * k)] = igf_antiderivative(vx, vy, vz, cellVolume);
+            }
+#define CORNERS(T, a, b, c)                                                                     \
+    (((((((T[(a + 1) + t0 * ((b + 1) + t1 * (c + 1))] + T[(a + 1) + t0 * ((b) + t1 * (c))]) + \
+          T[(a) + t0 * ((b + 1) + t1 * (c))]) +                                                 \
+         T[(a) + t0 * ((b) + t1 * (c + 1))]) -                                                  \
+        T[(a + 1) + t0 * ((b + 1) + t1 * (c))]) -                                               \
+       T[(a + 1) + t0 * ((b) + t1 * (c + 1))]) -                                                \
+      T[(a) + t0 * ((b + 1) + t1 * (c + 1))]) -                                                 \
+     T[(a) + t0 * ((b) + t1 * (c))])
+    memset(G2, 0, L0 * L1 * L2 * sizeof(double));
+    SCO_PAR
+    for (long long k = 0; k < L2; ++k)
+        for (long long j = 0; j <= n1; ++j)
+            for (long long i = 0; i <= n0; ++i) {
+                if (i >= L0 || j >= L1) continue;
+                /* rho2[I][J][K] from tmpgreen (k <= nz), rho2[I][J][KE] = ggrn2[I][J][KE - nz] */
+                const double g = k <= n2 ? CORNERS(ta, i, j, k) : CORNERS(tb, i, j, k - n2);
+                G2[i + L0 * (j + L1 * k)] = g;
+            }
+#undef CORNERS
+    free(ta);
+    free(tb);
+    /* rho2[IE][J][aK] = rho2[2nx - IE][J][aK]; rho2[aI][JE][aK] = rho2[aI][2ny - JE][aK] */
+    for (long long k = 0; k < L2; ++k)
+        for (long long j = 0; j <= n1 && j < L1; ++j)
+            for (long long i = n0 + 1; i < L0; ++i)
+                G2[i + L0 * (j + L1 * k)] = G2[(L0 - i) + L0 * (j + L1 * k)];
+    for (long long k = 0; k < L2; ++k)
+        for (long long j = n1 + 1; j < L1; ++j)
+            for (long long i = 0; i < L0; ++i)
+                G2[i + L0 * (j + L1 * k)] = G2[i + L0 * ((L1 - j) + L1 * k)];
+}
+
+/* ------------------------------------------------------------------------ */
+/* FFTPoissonSolver::computePotential(rho, hr, zshift)  (FFTPoissonSolver.cpp: */
+/* 287-327): the potential of the image charge.  imgrho2tr = -rho2tr * grntr; */
+/* the inverse transform is read back with z flipped,                         */
+/* rho[i][j][k] = rho2[i][j][nz - k - 1].                                     */
+/* ------------------------------------------------------------------------ */
+int sco_compute_potential_shifted(const int* nr, double* rho, const double* hr, double zshift) {
+    const long long n0 = nr[0], n1 = nr[1], n2 = nr[2];
+    const int L[3] = {2 * nr[0], 2 * nr[1], 2 * nr[2]};
+    const long long L0 = L[0], L1 = L[1], L2 = L[2], C0 = L0 / 2 + 1;
+    const long long D = L0 * L1 * L2, S = C0 * L1 * L2;
+    double* rho2 = (double*)calloc(D, sizeof(double));
+    double* rhot = (double*)malloc(2 * S * sizeof(double));
+    double* grnt = (double*)malloc(2 * S * sizeof(double));
+    double* G2 = (double*)malloc(D * sizeof(double));
+    if (!rho2 || !rhot || !grnt || !G2) { free(rho2); free(rhot); free(grnt); free(G2); return SCO_ERR_OOM; }
+    for (long long k = 0; k < n2; ++k)
+        for (long long j = 0; j < n1; ++j)
+            memcpy(rho2 + L0 * (j + L1 * k), rho + n0 * (j + n1 * k), n0 * sizeof(double));
+    sco_fft3d_r2c(L, rho2, rhot);
+    sco_igf_shifted(nr, hr, zshift, G2);
+    sco_fft3d_r2c(L, G2, grnt);
+    for (long long s = 0; s < S; ++s) {
+        double ar = rhot[2 * s], ai = rhot[2 * s + 1], br = grnt[2 * s], bi = grnt[2 * s + 1];
+        rhot[2 * s] = -(ar * br - ai * bi);
+        rhot[2 * s + 1] = -(ar * bi + ai * br);
+    }
+    sco_fft3d_c2r(L, rhot, rho2);
+    for (long long k = 0; k < n2; ++k)
+        for (long long j = 0; j < n1; ++j)
+            memcpy(rho + n0 * (j + n1 * k), rho2 + L0 * (j + L1 * (n2 - k - 1)), n0 * sizeof(double));
+    free(rho2); free(rhot); free(grnt); free(G2);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* energy bins: calcGammas (PartBunchBase.hpp:639-683): the mean of           */
+/* sqrt(1 + P.P) over the particles of each bin, 1 for an empty bin.          */
+/* ------------------------------------------------------------------------ */
+int sco_bin_gammas(long long n, const double* P, const int* bin, int nbins, double* gamma, long long* count) {
+    if (nbins <= 0) return SCO_ERR_ARG;
+    for (long long i = 0; i < n; ++i)
+        if (bin[i] < 0 || bin[i] >= nbins) return SCO_ERR_ARG;
+    for (int b = 0; b < nbins; ++b) count[b] = 0;
+    if (g_exact) {
+        sco_i128* a = (sco_i128*)calloc(nbins, sizeof(sco_i128));
+        if (!a) return SCO_ERR_OOM;
+        for (long long i = 0; i < n; ++i) {
+            a[bin[i]] += ex_from(sqrt(1.0 + dot3(P + 3 * i, P + 3 * i)));
+            count[bin[i]] += 1;
+        }
+        for (int b = 0; b < nbins; ++b) gamma[b] = ex_to_double(a[b]);
+        free(a);
+    } else {
+        for (int b = 0; b < nbins; ++b) gamma[b] = 0.0;
+        for (long long i = 0; i < n; ++i) {
+            gamma[bin[i]] += sqrt(1.0 + dot3(P + 3 * i, P + 3 * i));
+            count[bin[i]] += 1;
+        }
+    }
+    for (int b = 0; b < nbins; ++b) {
+        if (count[b] != 0)
+            gamma[b] /= (double)count[b];
+        else
+            gamma[b] = 1.0;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* The energy-bin loop of computeSpaceChargeFields (ParallelTTracker.cpp:567- */
+/* 578) with PartBunch::computeSelfFields(int bin) (PartBunch.cpp:138-430) on */
+/* a bunch already in the beam frame, preceded by boundp.  The charge of bin  */
+/* b's particles is qi (setBinCharge, PartBunchBase.hpp:722-725), all other   */
+/* particles carry none; Q is restored after every bin, so qi is unchanged.   */
+/* Ef, Bf are accumulated from zero: per bin the field of the bin's charge    */
+/* and of its image (a mirror charge behind the cathode plane, moving the     */
+/* other way, hence the opposite sign of its magnetic field).  bin_gamma      */
+/* (optional, nbins doubles) receives calcGammas' result.                     */
+/* ------------------------------------------------------------------------ */
+int sco_compute_self_fields_binned(const sco_params* prm, double qi, long long n, const double* R,
+                                   const double* P, const int* bin, int nbins, int last_emitted,
+                                   double* Ef, double* Bf, double* bin_gamma, sco_debug* dbg) {
+    sco_mesh mesh;
+    int rc = sco_boundp(n, R, prm->nr, prm->dh, &mesh);
+    if (rc) return rc;
+    const long long n0 = prm->nr[0], n1 = prm->nr[1], n2 = prm->nr[2];
+    const long long M = n0 * n1 * n2;
+    double* gam = (double*)malloc((nbins > 0 ? nbins : 1) * sizeof(double));
+    long long* cnt = (long long*)malloc((nbins > 0 ? nbins : 1) * sizeof(long long));
+    double* rho = (double*)malloc(M * sizeof(double));
+    double* img = (double*)malloc(M * sizeof(double));
+    double* E = (double*)malloc(3 * M * sizeof(double));
+    double* Et = (double*)malloc(3 * n * sizeof(double));
+    double* Rb = (double*)malloc(3 * n * sizeof(double));
+    if (!gam || !cnt || !rho || !img || !E || !Et || !Rb) {
+        rc = SCO_ERR_OOM;
+        goto done;
+    }
+    /* calcGammas (:568) */
+    rc = sco_bin_gammas(n, P, bin, nbins, gam, cnt);
+    if (rc) goto done;
+    if (bin_gamma) memcpy(bin_gamma, gam, nbins * sizeof(double));
+    memset(Ef, 0, 3 * n * sizeof(double));
+    memset(Bf, 0, 3 * n * sizeof(double));
+    for (int b = 0; b < last_emitted && b < nbins; ++b) {
+        /* setBinCharge(b); Q *= dt; scatter; Q /= dt; rho /= dT  (:153-170) */
+        long long nb = 0;
+        for (long long i = 0; i < n; ++i)
+            if (bin[i] == b) {
+                memcpy(Rb + 3 * nb, R + 3 * i, 3 * sizeof(double));
+                ++nb;
+            }
+        memset(rho, 0, M * sizeof(double));
+        const double qdt = qi * prm->dT;
+        rc = sco_scatter_cic(nb, Rb, qdt, &mesh, rho);
+        if (rc) goto done;
+        for (long long c = 0; c < M; ++c) rho[c] /= prm->dT;
+        /* (:173-185) */
+        const double scaleFactor = 1;
+        const double gammaz = gam[b];
+        const double tmp2 = 1 / mesh.hr[0] * 1 / mesh.hr[1] * 1 / mesh.hr[2] /
+                            (scaleFactor * scaleFactor * scaleFactor) / gammaz;
+        for (long long c = 0; c < M; ++c) rho[c] *= tmp2;
+        double hr_scaled[3] = {mesh.hr[0] * scaleFactor, mesh.hr[1] * scaleFactor, mesh.hr[2] * scaleFactor};
+        hr_scaled[2] *= gammaz;
+        memcpy(img, rho, M * sizeof(double));
+        /* the bin's own field (:190-244) */
+        rc = sco_compute_potential(prm->nr, rho, hr_scaled);
+        if (rc) goto done;
+        const double hvol = hr_scaled[0] * hr_scaled[1] * hr_scaled[2];
+        for (long long c = 0; c < M; ++c) rho[c] *= hvol;
+        for (long long c = 0; c < M; ++c) rho[c] *= prm->coupling;
+        sco_neg_grad_scaled(prm->nr, rho, mesh.hr, gammaz, E);
+        rc = sco_gather_cic(n, R, &mesh, E, Et);
+        if (rc) goto done;
+        const double betaC = sqrt(gammaz * gammaz - 1.0) / gammaz / SCO_C;
+        for (long long i = 0; i < n; ++i) {
+            Bf[3 * i + 0] = Bf[3 * i + 0] - betaC * Et[3 * i + 1];
+            Bf[3 * i + 1] = Bf[3 * i + 1] + betaC * Et[3 * i + 0];
+            Ef[3 * i + 0] += Et[3 * i + 0];
+            Ef[3 * i + 1] += Et[3 * i + 1];
+            Ef[3 * i + 2] += Et[3 * i + 2];
+        }
+        /* the image charge's field (:246-427) */
+        const double zshift = -(2 * mesh.origin[2] + (0 + (n2 - 1) + 1) * mesh.hr[2]) * gammaz * scaleFactor;
+        rc = sco_compute_potential_shifted(prm->nr, img, hr_scaled, zshift);
+        if (rc) goto done;
+        for (long long c = 0; c < M; ++c) img[c] *= hvol;
+        for (long long c = 0; c < M; ++c) img[c] *= prm->coupling;
+        sco_neg_grad_scaled(prm->nr, img, mesh.hr, gammaz, E);
+        rc = sco_gather_cic(n, R, &mesh, E, Et);
+        if (rc) goto done;
+        for (long long i = 0; i < n; ++i) {
+            Bf[3 * i + 0] = Bf[3 * i + 0] + betaC * Et[3 * i + 1];
+            Bf[3 * i + 1] = Bf[3 * i + 1] - betaC * Et[3 * i + 0];
+            Ef[3 * i + 0] += Et[3 * i + 0];
+            Ef[3 * i + 1] += Et[3 * i + 1];
+            Ef[3 * i + 2] += Et[3 * i + 2];
+        }
+    }
+    if (dbg) {
+        dbg->mesh = mesh;
+        dbg->gammaz = nbins > 0 ? gam[0] : 1.0;
+    }
+done:
+    free(gam); free(cnt); free(rho); free(img); free(E); free(Et); free(Rb);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------ */
 /* one ParallelTTracker step (ParallelTTracker.cpp:343-365)                   */
+/* bins == NULL: computeSelfFields(); else the energy-bin loop (:567-578).    */
 /* ------------------------------------------------------------------------ */
 static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, double* Ef, double* Bf,
-                        sco_debug* dbg) {
+                        const sco_bins* bins, sco_debug* dbg) {
     const sco_params* prm = &tr->prm;
     const double dT = prm->dT;
     /* timeIntegration1 -> pushParticles (:434-447, .h:448-455) */
@@ -1087,7 +1319,12 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
         trafo_transform_to(&r2b, R + 3 * i, v);
         R[3 * i] = v[0]; R[3 * i + 1] = v[1]; R[3 * i + 2] = v[2];
     }
-    int rc = sco_compute_self_fields(prm, &tr->Q, n, R, P, Ef, Bf, dbg);
+    int rc;
+    if (bins)
+        rc = sco_compute_self_fields_binned(prm, tr->Q, n, R, P, bins->bin, bins->nbins, bins->last_emitted, Ef, Bf,
+                                            NULL, dbg);
+    else
+        rc = sco_compute_self_fields(prm, &tr->Q, n, R, P, Ef, Bf, dbg);
     if (rc) return rc;
     SCO_PAR
     for (long long i = 0; i < n; ++i) {
@@ -1166,17 +1403,32 @@ int sco_tracker_init(sco_tracker* tr, const sco_params* prm, double Q) {
     return 0;
 }
 
-int sco_track(sco_tracker* tr, long long n, double* R, double* P, int nsteps, sco_debug* dbg) {
+static int track_impl(sco_tracker* tr, long long n, double* R, double* P, const sco_bins* bins, int nsteps,
+                      sco_debug* dbg) {
     if (n <= 0) return SCO_ERR_ARG;
     double* Ef = (double*)malloc(3 * n * sizeof(double));
     double* Bf = (double*)malloc(3 * n * sizeof(double));
     if (!Ef || !Bf) { free(Ef); free(Bf); return SCO_ERR_OOM; }
     int rc = 0;
     for (int s = 0; s < nsteps && rc == 0; ++s)
-        rc = tracker_step(tr, n, R, P, Ef, Bf, (s == nsteps - 1) ? dbg : NULL);
+        rc = tracker_step(tr, n, R, P, Ef, Bf, bins, (s == nsteps - 1) ? dbg : NULL);
     free(Ef);
     free(Bf);
     return rc;
+}
+
+int sco_track(sco_tracker* tr, long long n, double* R, double* P, int nsteps, sco_debug* dbg) {
+    return track_impl(tr, n, R, P, NULL, nsteps, dbg);
+}
+
+/* the step loop with energy bins: bin[i] in [0, nbins) per particle (the
+ * bins travel with the particles; the loop covers bins below
+ * min(last_emitted, nbins)) */
+int sco_track_binned(sco_tracker* tr, long long n, double* R, double* P, const int* bin, int nbins,
+                     int last_emitted, int nsteps, sco_debug* dbg) {
+    if (!bin || nbins <= 0) return SCO_ERR_ARG;
+    sco_bins b = {bin, nbins, last_emitted};
+    return track_impl(tr, n, R, P, &b, nsteps, dbg);
 }
 
 int sco_sizeof_tracker(void) { return (int)sizeof(sco_tracker); }

@@ -122,8 +122,26 @@ void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, doub
 int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const double* R, const double* P,
                             double* Ef, double* Bf, sco_debug* dbg);
 
+/* image charge (FFTPoissonSolver.cpp:287-327, :546-639) */
+void sco_igf_shifted(const int* nr, const double* hr, double zshift, double* G2);
+int sco_compute_potential_shifted(const int* nr, double* rho, const double* hr, double zshift);
+
+/* energy bins (PartBunchBase.hpp:639-683; PartBunch.cpp:138-430;
+ * ParallelTTracker.cpp:567-578) */
+typedef struct {
+    const int* bin;   /* per particle, in [0, nbins) */
+    int nbins;        /* Distribution::getNumberOfEnergyBins */
+    int last_emitted; /* Distribution::getLastEmittedEnergyBin */
+} sco_bins;
+int sco_bin_gammas(long long n, const double* P, const int* bin, int nbins, double* gamma, long long* count);
+int sco_compute_self_fields_binned(const sco_params* prm, double qi, long long n, const double* R,
+                                   const double* P, const int* bin, int nbins, int last_emitted,
+                                   double* Ef, double* Bf, double* bin_gamma, sco_debug* dbg);
+
 int sco_tracker_init(sco_tracker* tr, const sco_params* prm, double Q);
 int sco_track(sco_tracker* tr, long long n, double* R, double* P, int nsteps, sco_debug* dbg);
+int sco_track_binned(sco_tracker* tr, long long n, double* R, double* P, const int* bin, int nbins,
+                     int last_emitted, int nsteps, sco_debug* dbg);
 
 int sco_sizeof_tracker(void);
 int sco_sizeof_debug(void);

@@ -97,3 +97,38 @@ def config_bunch(name, n=None, seed=DEFAULT_SEED, bunch_id=0):
     R, P = gaussian_bunch(N, seed=seed, bunch_id=bunch_id)
     return dict(R=R, P=P, N=N, nr=(mesh, mesh, mesh), steps=steps, bz_ext=bz, dT=1e-12,
                 Q=-1e-9 / N, ref_pz=10.0, dh=0.02)
+
+
+def photoinjector_bunch(n, nbins=10, sigma_r=1e-3, z_center=4e-3, sigma_z=0.8e-3, bg_head=1.5, bg_tail=0.5,
+                        rel_spread=1e-3, bg_perp=1e-3, seed=DEFAULT_SEED, bunch_id=0):
+    """A bunch shortly after emission from a cathode at z = 0, with energy bins.
+
+    The reference's photoinjector runs emit particles from the cathode over
+    time and label each with the energy bin of its emission slice
+    (src/Distribution/Distribution.cpp, setupEnergyBins / emitParticles); the
+    first slice has been accelerated longest.  This seeded stand-in draws
+    x, y ~ N(0, sigma_r), z ~ N(z_center, sigma_z) (5 sigma clear of the
+    cathode at the defaults), splits the bunch into nbins slices of equal
+    count by z (bin 0 at the head) and gives slice b a mean beta*gamma_z
+    falling linearly from bg_head (head) to bg_tail (tail), with a
+    rel_spread relative spread; transverse beta*gamma ~ N(0, bg_perp).
+    Returns R, P (n x 3) and bins (n, int32).
+    """
+    n = int(n)
+    g0, g1 = standard_normals(n, seed, bunch_id, 0)
+    g2, g3 = standard_normals(n, seed, bunch_id, 1)
+    g4, g5 = standard_normals(n, seed, bunch_id, 2)
+    R = np.empty((n, 3), dtype=np.float64)
+    P = np.empty((n, 3), dtype=np.float64)
+    R[:, 0] = sigma_r * g0
+    R[:, 1] = sigma_r * g1
+    R[:, 2] = z_center + sigma_z * g2
+    order = np.argsort(-R[:, 2], kind="stable")
+    bins = np.empty(n, dtype=np.int32)
+    bins[order] = (np.arange(n) * nbins // n).astype(np.int32)
+    frac = bins / max(nbins - 1, 1)
+    bg = bg_head + (bg_tail - bg_head) * frac
+    P[:, 0] = bg_perp * g3
+    P[:, 1] = bg_perp * g4
+    P[:, 2] = bg * (1.0 + rel_spread * g5)
+    return R, P, bins

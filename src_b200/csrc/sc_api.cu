@@ -65,6 +65,136 @@ void drop_graphs(scgpu_ctx* c) {
             if (g) cudaGraphExecDestroy(g);
             g = nullptr;
         }
+    for (auto& row : c->graphs_bins)
+        for (auto& g : row) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+void free_bins(scgpu_ctx* c) {
+    DevBunch& b = c->b;
+    dfree(b.bin); dfree(b.bin_alt); dfree(b.bst); dfree(b.nacc_bins); dfree(b.bin_partials); dfree(b.F8);
+    dfree(c->spec_fwd_buf); dfree(c->ghat_alt); dfree(c->ghat_img_alt);
+    dfree(b.gtmp_img); dfree(b.gimg); dfree(b.ghat_img);
+    for (int k = 0; k < kMaxBins; ++k) {
+        if (c->ev_bin[k]) cudaEventDestroy(c->ev_bin[k]);
+        if (c->ev_used[k]) cudaEventDestroy(c->ev_used[k]);
+        c->ev_bin[k] = c->ev_used[k] = nullptr;
+    }
+    b.nbins = b.nactive = 0;
+    c->bin_capacity = 0;
+    c->bins_nbins_alloc = 0;
+}
+
+long long mesh_cells(const DevBunch& b) { return (long long)b.bc.n[0] * b.bc.n[1] * b.bc.n[2]; }
+
+// Buffers of the image-charge solve (FFTPoissonSolver.cpp:546-639).
+int ensure_image(scgpu_ctx* c) {
+    DevBunch& b = c->b;
+    if (b.ghat_img) return SCGPU_OK;
+    const long long n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    const long long T3 = (n0 + 2) * (n1 + 2) * (n2 + 2);
+    const long long GI = (n0 + 1) * (n1 + 1) * (2 * n2);
+    const long long G3 = (n0 + 1) * (n1 + 1) * (n2 + 1);
+    const size_t cs = b.precision == SCGPU_PLAIN_FP64 ? sizeof(double2) : sizeof(float2);
+    int rc;
+    if ((rc = dalloc(c, &b.gtmp_img, 2 * T3 * sizeof(double))) || (rc = dalloc(c, &b.gimg, 2 * GI * sizeof(double))) ||
+        (rc = dalloc(c, (char**)&b.ghat_img, G3 * cs)))
+        return rc;
+    return SCGPU_OK;
+}
+
+// Buffers of the energy-bin loop for nbins bins and the current particle capacity.
+int ensure_bins(scgpu_ctx* c, int nbins) {
+    DevBunch& b = c->b;
+    int rc = ensure_image(c);
+    if (rc) return rc;
+    const long long M = mesh_cells(b);
+    const long long n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    const long long S = (n2 + 1) * (2 * n1) * (2 * n0);
+    const long long G3 = (n0 + 1) * (n1 + 1) * (n2 + 1);
+    const size_t rs = b.precision == SCGPU_PLAIN_FP64 ? sizeof(double) : sizeof(float);
+    const size_t cs = b.precision == SCGPU_PLAIN_FP64 ? sizeof(double2) : sizeof(float2);
+    if (!b.bst) {
+        if ((rc = dalloc(c, &b.bst, kMaxBins * sizeof(StepState))) ||
+            (rc = dalloc(c, &b.bin_partials, 296 * kMaxBins * 4 * sizeof(unsigned long long))) ||
+            (rc = dalloc(c, &b.F8, M * 8 * sizeof(double))) || (rc = dalloc(c, (char**)&c->ghat_alt, G3 * rs)) ||
+            (rc = dalloc(c, (char**)&c->ghat_img_alt, G3 * cs)))
+            return rc;
+        if (b.precision == SCGPU_PLAIN_FP64 && (rc = dalloc(c, (char**)&c->spec_fwd_buf, S * sizeof(double2))))
+            return rc;
+        cudaMemsetAsync(b.bst, 0, kMaxBins * sizeof(StepState), c->stream);
+        for (int k = 0; k < kMaxBins; ++k) {
+            CK(cudaEventCreateWithFlags(&c->ev_bin[k], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->ev_used[k], cudaEventDisableTiming));
+        }
+    }
+    if (c->bin_capacity < c->capacity) {
+        dfree(b.bin);
+        dfree(b.bin_alt);
+        c->bin_capacity = 0;
+        if ((rc = dalloc(c, &b.bin, c->capacity * sizeof(int))) || (rc = dalloc(c, &b.bin_alt, c->capacity * sizeof(int))))
+            return rc;
+        c->bin_capacity = c->capacity;
+    }
+    if (c->bins_nbins_alloc < nbins) {
+        dfree(b.nacc_bins);
+        c->bins_nbins_alloc = 0;
+        if ((rc = dalloc(c, &b.nacc_bins, (size_t)nbins * M * 2 * sizeof(unsigned long long)))) return rc;
+        CK(cudaMemsetAsync(b.nacc_bins, 0, (size_t)nbins * M * 2 * sizeof(unsigned long long), c->stream));
+        c->bins_nbins_alloc = nbins;
+    }
+    return SCGPU_OK;
+}
+
+// The buffers one bin's solve works on: its StepState and accumulators, the
+// kept forward spectrum, and one of two sets of Green's-function spectra.
+DevBunch bin_view(const scgpu_ctx* c, int k) {
+    DevBunch v = c->b;
+    v.st = c->b.bst + k;
+    v.nacc = c->b.nacc_bins + (size_t)2 * mesh_cells(c->b) * k;
+    v.spec_fwd = c->spec_fwd_buf;
+    if (k & 1) {
+        v.ghat = c->ghat_alt;
+        v.ghat_img = c->ghat_img_alt;
+    }
+    return v;
+}
+
+// The energy-bin loop of computeSpaceChargeFields (ParallelTTracker.cpp:567-578)
+// once the drift kernel has set this step's mesh: calcGammas, one deposit pass
+// for all active bins, then per bin the charge density, the bin's own
+// potential and its image's (computeSelfFields(bin), PartBunch.cpp:138-430),
+// each field added into F8.  The Green's functions of a bin depend on its
+// gamma only, so they run on the side stream, at most two bins ahead of the
+// main stream's convolutions (two sets of spectra).
+void enqueue_bins_fields(scgpu_ctx* c, cudaStream_t s) {
+    DevBunch& b = c->b;
+    const long long M = mesh_cells(b);
+    launch_bin_gammas(b, s);
+    cudaMemsetAsync(b.F8, 0, (size_t)M * 8 * sizeof(double), s);
+    launch_deposit_bins(b, s);
+    if (b.nactive <= 0) return;
+    cudaEventRecord(c->ev_fork, s);
+    cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+    for (int k = 0; k < b.nactive; ++k) {
+        const DevBunch v = bin_view(c, k);
+        if (k >= 2) cudaStreamWaitEvent(c->side, c->ev_used[k - 2], 0);
+        launch_igf(v, nullptr, c->side);
+        launch_green_transform(v, c->side);
+        launch_igf_image(v, c->side);
+        launch_green_transform_image(v, c->side);
+        cudaEventRecord(c->ev_bin[k], c->side);
+        launch_assemble_rho(v, s);
+        launch_convolution_part(v, kConvSelfField, kConvForwardPart, s);
+        cudaStreamWaitEvent(s, c->ev_bin[k], 0);
+        launch_convolution_part(v, kConvSelfField, kConvRestPart, s);
+        launch_grad_acc(v, false, s);
+        launch_convolution_part(v, kConvSelfField, kConvImagePart, s);
+        launch_grad_acc(v, true, s);
+        cudaEventRecord(c->ev_used[k], s);
+    }
 }
 
 int ensure_particles(scgpu_ctx* c, long long n) {
@@ -102,6 +232,7 @@ void enqueue_reorder(scgpu_ctx* c, cudaStream_t s) {
     launch_cell_keys(b, 0, s);
     launch_sort(b, s);
     launch_reorder(b, s);
+    if (b.nbins > 0) launch_permute_bins(b, s);
     cudaMemsetAsync(b.hist, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(int), s);
 }
 
@@ -135,10 +266,32 @@ void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
     launch_gather_kick_push(b, stats, s);
 }
 
+// The step with energy bins: the same branches, the self fields from the
+// energy-bin loop, the gather reading the summed fields of all bins.
+void enqueue_step_binned(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
+    DevBunch& b = c->b;
+    cudaEventRecord(c->ev_start, s);
+    cudaStreamWaitEvent(c->ref, c->ev_start, 0);
+    launch_advance_reference(b, c->ref);
+    cudaEventRecord(c->ev_ref, c->ref);
+    launch_drift_to_beam(b, true, s);
+    enqueue_bins_fields(c, s);
+    if (reorder) enqueue_reorder(c, s);
+    cudaStreamWaitEvent(s, c->ev_ref, 0);
+    launch_gather_kick_push_bins(b, stats, s);
+}
+
+void enqueue_any_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
+    if (c->b.nbins > 0)
+        enqueue_step_binned(c, stats, reorder, s);
+    else
+        enqueue_step(c, stats, reorder, s);
+}
+
 int build_graph(scgpu_ctx* c, bool stats, bool reorder, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(c, stats, reorder, c->own);
+    enqueue_any_step(c, stats, reorder, c->own);
     cudaError_t e = cudaStreamEndCapture(c->own, &g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
     e = cudaGraphInstantiate(out, g, 0);
@@ -153,6 +306,7 @@ int status_from_flags(scgpu_ctx* c, int err) {
     if (err & kFlagFrame) return fail(c, SCGPU_ERR_FRAME, "getQuaternion: anti-parallel or null vector");
     if (err & kFlagGuard) return fail(c, SCGPU_ERR_GUARD, "a CIC stencil left the mesh");
     if (err & kFlagSort) return fail(c, SCGPU_ERR_CUDA, "cell sort: scatter position out of range");
+    if (err & kFlagBin) return fail(c, SCGPU_ERR_ARG, "an energy bin outside [0, nbins)");
     return fail(c, SCGPU_ERR_CUDA, "unknown device error flag");
 }
 
@@ -328,6 +482,7 @@ void scgpu_destroy(scgpu_ctx* c) {
     if (c->stream && c->stream != c->own) cudaStreamSynchronize(c->stream);
     drop_graphs(c);
     free_particles(c);
+    free_bins(c);
     DevBunch& b = c->b;
     dfree(b.nacc); dfree(b.rho); dfree(b.phi); dfree(b.E4); dfree(b.spec); dfree(b.spec_lo);
     dfree(b.gtmp); dfree(b.gline); dfree(b.ghat); dfree(b.st); dfree(b.partials); dfree(b.ticket);
@@ -407,6 +562,52 @@ static int compute_potential_impl(scgpu_ctx* c, double* rho, const double hr[3],
     return SCGPU_OK;
 }
 
+// computePotential(rho, hr, zshift) (FFTPoissonSolver.cpp:287-327): the
+// image charge's potential, through the shifted Green's function.
+static int compute_potential_image_impl(scgpu_ctx* c, double* rho, const double hr[3], double zshift, bool device_ptr) {
+    if (!c || !rho || !hr) return fail(c, SCGPU_ERR_ARG, "null argument");
+    for (int d = 0; d < 3; ++d)
+        if (!(hr[d] > 0.0) || !std::isfinite(hr[d])) return fail(c, SCGPU_ERR_ARG, "hr must be positive and finite");
+    if (!std::isfinite(zshift)) return fail(c, SCGPU_ERR_ARG, "zshift must be finite");
+    CK(cudaSetDevice(c->device));
+    int rc = ensure_image(c);
+    if (rc) return rc;
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    const long long M = mesh_cells(b);
+    const cudaMemcpyKind in_kind = device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out_kind = device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CK(cudaMemcpyAsync(b.st->hr_scaled, hr, 3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(&b.st->zshift, &zshift, sizeof(double), cudaMemcpyHostToDevice, s));
+    if (b.precision == SCGPU_PLAIN_FP64) {
+        CK(cudaMemcpyAsync(b.rho, rho, M * sizeof(double), in_kind, s));
+    } else {
+        double* stage = nullptr;
+        CK(cudaMalloc(&stage, M * sizeof(double)));
+        cudaError_t e = cudaMemcpyAsync(stage, rho, M * sizeof(double), in_kind, s);
+        if (e == cudaSuccess) launch_f64_to_f32(stage, (float*)b.rho, M, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFree(stage);
+        if (e != cudaSuccess) return cuda_fail(c, e, "staging rho");
+    }
+    launch_igf_image(b, s);
+    launch_green_transform_image(b, s);
+    launch_convolution_part(b, kConvPotential, kConvForwardPart | kConvImagePart, s);
+    CK(cudaMemcpyAsync(rho, b.phi, M * sizeof(double), out_kind, s));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    c->have_solve = false;
+    return SCGPU_OK;
+}
+
+int scgpu_compute_potential_image(scgpu_ctx* c, double* rho, const double hr[3], double zshift) {
+    return compute_potential_image_impl(c, rho, hr, zshift, false);
+}
+
+int scgpu_compute_potential_image_device(scgpu_ctx* c, double* rho, const double hr[3], double zshift) {
+    return compute_potential_image_impl(c, rho, hr, zshift, true);
+}
+
 int scgpu_compute_potential(scgpu_ctx* c, double* rho, const double hr[3]) { return compute_potential_impl(c, rho, hr, false); }
 
 int scgpu_compute_potential_device(scgpu_ctx* c, double* rho, const double hr[3]) {
@@ -460,6 +661,121 @@ int scgpu_compute_self_fields(scgpu_ctx* c, long long n, const double* R, const 
     return rc;
 }
 
+static int check_bins_args(scgpu_ctx* c, const int* bins, int nbins, int last_emitted) {
+    if (nbins < 0 || nbins > kMaxBins) return fail(c, SCGPU_ERR_ARG, "nbins must be in [0, 64]");
+    if (nbins > 0 && !bins) return fail(c, SCGPU_ERR_ARG, "null bins");
+    if (last_emitted < 0) return fail(c, SCGPU_ERR_ARG, "last_emitted must not be negative");
+    return SCGPU_OK;
+}
+
+// Switches the resident bunch to the energy-bin loop (nbins > 0) or back to
+// one self-field solve (nbins == 0, Distribution::Rebin).  bins[i] is the
+// bin of particle i in the order of the last upload; each step computes the
+// fields of bins [0, min(last_emitted, nbins)) and their images.
+static int set_bins_impl(scgpu_ctx* c, const int* bins, int nbins, int last_emitted, bool device_ptr) {
+    if (!c) return SCGPU_ERR_ARG;
+    int rc = check_bins_args(c, bins, nbins, last_emitted);
+    if (rc) return rc;
+    if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    CK(cudaSetDevice(c->device));
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    const int nactive = last_emitted < nbins ? last_emitted : nbins;
+    if (nbins != b.nbins || nactive != b.nactive) drop_graphs(c);
+    if (nbins == 0) {
+        b.nbins = b.nactive = 0;
+        const int zero = 0;
+        CK(cudaMemcpyAsync(&b.st->binned, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        return SCGPU_OK;
+    }
+    if ((rc = ensure_bins(c, nbins))) return rc;
+    const long long n = c->n;
+    CK(cudaMemsetAsync(b.nacc_bins, 0, (size_t)c->bins_nbins_alloc * mesh_cells(b) * 2 * sizeof(unsigned long long), s));
+    int* host_order = b.bin_alt;
+    CK(cudaMemcpyAsync(host_order, bins, (size_t)n * sizeof(int), device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       s));
+    launch_bins_by_id(host_order, b.id, b.bin, n, s);
+    b.nbins = nbins;
+    b.nactive = nactive;
+    const int one = 1;
+    CK(cudaMemcpyAsync(&b.st->binned, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return SCGPU_OK;
+}
+
+int scgpu_set_energy_bins(scgpu_ctx* c, const int* bins, int nbins, int last_emitted) {
+    return set_bins_impl(c, bins, nbins, last_emitted, false);
+}
+
+int scgpu_get_bin_gammas(scgpu_ctx* c, double* gamma, long long* count) {
+    if (!c || !gamma) return fail(c, SCGPU_ERR_ARG, "null argument");
+    DevBunch& b = c->b;
+    if (b.nbins <= 0 || !b.bst) return fail(c, SCGPU_ERR_STATE, "no energy bins");
+    CK(cudaSetDevice(c->device));
+    std::vector<StepState> h(b.nbins);
+    CK(cudaMemcpyAsync(h.data(), b.bst, b.nbins * sizeof(StepState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < b.nbins; ++k) {
+        gamma[k] = h[k].gammaz;
+        if (count) count[k] = h[k].bin_count;
+    }
+    return SCGPU_OK;
+}
+
+int scgpu_compute_self_fields_binned(scgpu_ctx* c, long long n, const double* R, const double* P, const int* bins,
+                                     int nbins, int last_emitted, double q_macro, double dT, double* Ef, double* Bf,
+                                     double* bin_gamma) {
+    if (!c || !R || !P || !Ef || !Bf) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!(dT > 0.0)) return fail(c, SCGPU_ERR_ARG, "dT must be positive");
+    int rc = check_bins_args(c, bins, nbins, last_emitted);
+    if (rc) return rc;
+    if (nbins == 0) return fail(c, SCGPU_ERR_ARG, "nbins must be positive");
+    CK(cudaSetDevice(c->device));
+    if ((rc = ensure_particles(c, n))) return rc;
+    if ((rc = ensure_bins(c, nbins))) return rc;
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    drop_graphs(c);
+    b.bc.dT = dT;
+    if (b.bc.coupling == 0.0) b.bc.coupling = 1.0 / (4 * kPi * 8.854187817e-12);
+    if (b.bc.mass == 0.0) b.bc.mass = 0.51099892e-03 * 1.0e9;
+    bunch_constants(b.bc);
+    CK(cudaMemcpyAsync(b.Ef, R, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(b.Bf, P, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_aos_to_soa(b.Ef, b.x, b.y, b.z, n, s);
+    launch_aos_to_soa(b.Bf, b.px, b.py, b.pz, n, s);
+    CK(cudaMemcpyAsync(b.bin, bins, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(b.nacc_bins, 0, (size_t)c->bins_nbins_alloc * mesh_cells(b) * 2 * sizeof(unsigned long long), s));
+    CK(cudaMemcpyAsync(&b.st->Q, &q_macro, sizeof(double), cudaMemcpyHostToDevice, s));
+    const int one = 1;
+    CK(cudaMemcpyAsync(&b.st->binned, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(&b.st->gen, 0, sizeof(unsigned), s));
+    b.nbins = nbins;
+    b.nactive = last_emitted < nbins ? last_emitted : nbins;
+    launch_reduce_state(b, false, s);
+    STAGE("reduce_state");
+    launch_drift_to_beam(b, false, s);
+    STAGE("bounds");
+    enqueue_bins_fields(c, s);
+    STAGE("bins");
+    launch_gather_fields_bins(b, s);
+    STAGE("gather");
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(Ef, b.Ef, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(Bf, b.Bf, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    rc = check_device_err(c);
+    if (rc == SCGPU_OK && bin_gamma) rc = scgpu_get_bin_gammas(c, bin_gamma, nullptr);
+    const int zero = 0;
+    cudaMemcpyAsync(&b.st->binned, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    b.nbins = b.nactive = 0;
+    c->have_bunch = false;  // the particle buffers now hold a beam-frame bunch
+    c->have_solve = false;
+    return rc;
+}
+
 int scgpu_bunch_upload(scgpu_ctx* c, long long n, const double* R, const double* P, const scgpu_bunch_params* bp) {
     if (!c || !R || !P || !bp) return fail(c, SCGPU_ERR_ARG, "null argument");
     if (!(bp->dT > 0.0) || !(bp->mass > 0.0)) return fail(c, SCGPU_ERR_ARG, "dT and mass must be positive");
@@ -489,6 +805,11 @@ int scgpu_bunch_upload(scgpu_ctx* c, long long n, const double* R, const double*
     h.Q = bp->q_macro;
     h.step = 0;
     h.gen = 0;
+    h.binned = 0;  // energy bins refer to the previous particle order: set them again after an upload
+    if (b.nbins > 0) {
+        drop_graphs(c);
+        b.nbins = b.nactive = 0;
+    }
     CK(cudaMemcpyAsync(b.st, &h, sizeof(StepState), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(b.nacc, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * 2 * sizeof(unsigned long long), s));
     CK(cudaMemsetAsync(b.hist, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(int), s));
@@ -530,14 +851,14 @@ int scgpu_track(scgpu_ctx* c, int nsteps, double* stats) {
     for (int k = 0; k < nsteps; ++k) {
         const bool reorder = c->reorder_every > 0 && (c->steps_done % c->reorder_every) == 0;
         if (c->use_graphs) {
-            cudaGraphExec_t& gx = c->graphs[want ? 1 : 0][reorder ? 1 : 0];
+            cudaGraphExec_t& gx = (c->b.nbins > 0 ? c->graphs_bins : c->graphs)[want ? 1 : 0][reorder ? 1 : 0];
             if (!gx) {
                 int rc = build_graph(c, want, reorder, &gx);
                 if (rc) return rc;
             }
             CK(cudaGraphLaunch(gx, s));
         } else {
-            enqueue_step(c, want, reorder, s);
+            enqueue_any_step(c, want, reorder, s);
         }
         ++c->steps_done;
         if (want)
@@ -646,6 +967,7 @@ double scgpu_last_track_ms(const scgpu_ctx* c) { return c ? c->last_ms : 0.0; }
 int scgpu_profile_track(scgpu_ctx* c, int nsteps, double* phase_ms) {
     if (!c || nsteps < 0 || !phase_ms) return fail(c, SCGPU_ERR_ARG, "bad argument");
     if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    if (c->b.nbins > 0) return fail(c, SCGPU_ERR_UNSUPPORTED, "phase profile of a step with energy bins");
     CK(cudaSetDevice(c->device));
     DevBunch& b = c->b;
     cudaStream_t s = c->stream;
@@ -701,7 +1023,7 @@ int scgpu_kernels_per_step(scgpu_ctx* c) {
     CK(cudaSetDevice(c->device));
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(c, false, false, c->own);
+    enqueue_any_step(c, false, false, c->own);
     CK(cudaStreamEndCapture(c->own, &g));
     size_t nn = 0;
     cudaGraphGetNodes(g, nullptr, &nn);

@@ -41,6 +41,7 @@ enum : int {
     kFlagGuard = 2,
     kFlagFrame = 4,
     kFlagSort = 8,  // a sort position fell outside [0, N): inconsistent histogram
+    kFlagBin = 16,  // an energy bin outside [0, nbins)
 };
 
 struct Trafo {
@@ -82,6 +83,11 @@ struct StepState {
     double betaC;  // sqrt(gz^2-1)/gz/c
     double qdt;    // Q * dt (the scattered charge)
     Trafo upd;     // reference-particle update of this step
+    // energy bins / image charge
+    double zshift;      // z shift of the image's Green's function (PartBunch.cpp:249)
+    long long bin_count;  // particles in the bin (per-bin copies)
+    int binned;         // the energy-bin loop is on: Q is restored after the scatter (ParallelTTracker.cpp:576)
+    int pad_;
 };
 
 struct BunchConst {

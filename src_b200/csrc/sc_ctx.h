@@ -30,6 +30,15 @@ struct scgpu_ctx {
     int reorder_every = 16;   // put the particle arrays in cell order every k steps (0: never)
     long long steps_done = 0; // steps since the last upload
     size_t smem_fft = 0;
+    // energy bins and image charges (buffers allocated on first use)
+    cudaGraphExec_t graphs_bins[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [stats][reorder]
+    long long bin_capacity = 0;
+    int bins_nbins_alloc = 0;     // bins the per-bin accumulators were sized for
+    void* spec_fwd_buf = nullptr; // plain form: forward spectrum of a bin
+    void* ghat_alt = nullptr;     // second spectrum buffers: the side stream builds bin k+1's Green's
+    void* ghat_img_alt = nullptr; // functions while the main stream convolves bin k
+    cudaEvent_t ev_bin[sc::kMaxBins] = {};
+    cudaEvent_t ev_used[sc::kMaxBins] = {};
 };
 
 namespace sc {

@@ -499,7 +499,10 @@ __global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, 
 // amplify, while rounding after the multiplication would be noise relative
 // to phi itself and is kept at FP64.  `in` and `out` alias in the plain form;
 // every block reads its rows before it writes them.
-template <typename TI, typename TO, int LT, int NC, int NT>
+//
+// CG: ghat holds complex values (the image charge's shifted G is not even in
+// z, FFTPoissonSolver.cpp:316); the product is the complex one.
+template <typename TI, typename TO, int LT, int NC, int NT, bool CG = false>
 __device__ __forceinline__ void fft_x_conv_body(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0, int n1,
                                                 int L1, int rows, const FftPlan& px, const Cx<TI>* __restrict__ twi,
                                                 const Cx<TO>* __restrict__ two, int bx) {
@@ -540,9 +543,15 @@ __device__ __forceinline__ void fft_x_conv_body(const Cx<TI>* in, Cx<TO>* out, c
         const int ky = r - kz * L1;
         const int gy = ky <= n1 ? ky : L1 - ky;
         const int gx = kx <= n0 ? kx : L0 - kx;
-        const TI gv = ghat[((size_t)kz * (n1 + 1) + gy) * (n0 + 1) + gx];
+        const size_t gi = ((size_t)kz * (n1 + 1) + gy) * (n0 + 1) + gx;
         const CI v = f[ri * CS + sk(kx)];
-        g[ri * CS + sk(kx)] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
+        if constexpr (CG) {
+            const CI gc = reinterpret_cast<const CI*>(ghat)[gi];
+            g[ri * CS + sk(kx)] = CO{(TO)(v.x * gc.x - v.y * gc.y), (TO)(v.x * gc.y + v.y * gc.x)};
+        } else {
+            const TI gv = ghat[gi];
+            g[ri * CS + sk(kx)] = CO{(TO)(v.x * gv), (TO)(v.y * gv)};
+        }
     }
     __syncthreads();
     const CO* o = block_fft<TO, true, LT, NC, NT, kPruneOut>(g, h, px, tw_o);
@@ -552,15 +561,17 @@ __device__ __forceinline__ void fft_x_conv_body(const Cx<TI>* in, Cx<TO>* out, c
         if (r < rows) out[(size_t)r * L0 + x] = o[ri * CS + sk(x)];
     }
 }
-template <typename TI, typename TO, int LT, int NC, int NT>
+template <typename TI, typename TO, int LT, int NC, int NT, bool CG = false>
 __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0, int n1,
                                                    int L1, int rows, FftPlan px, const Cx<TI>* __restrict__ twi,
                                                    const Cx<TO>* __restrict__ two) {
-    fft_x_conv_body<TI, TO, LT, NC, NT>(in, out, ghat, n0, n1, L1, rows, px, twi, two, blockIdx.x);
+    fft_x_conv_body<TI, TO, LT, NC, NT, CG>(in, out, ghat, n0, n1, L1, rows, px, twi, two, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- pass E
-template <typename T, bool SELF, int LT, int NC, int NT>
+// FLIP: the image potential is read back with z flipped,
+// rho[i][j][k] = rho2[i][j][n2 - k - 1] (FFTPoissonSolver.cpp:322-326).
+template <typename T, bool SELF, int LT, int NC, int NT, bool FLIP = false>
 __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
                                                int n2, int L0, int L1, const FftPlan& pz, const Cx<T>* __restrict__ twz,
                                                const StepState* __restrict__ st, double normFact, double coupling, int bx,
@@ -620,15 +631,15 @@ __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, d
             r = r * hvol;
             r = r * coupling;
         }
-        phi[((size_t)zz * n1 + y) * n0 + x] = r;
+        phi[((size_t)(FLIP ? n2 - 1 - zz : zz) * n1 + y) * n0 + x] = r;
     }
 }
-template <typename T, bool SELF, int LT, int NC, int NT>
+template <typename T, bool SELF, int LT, int NC, int NT, bool FLIP = false>
 __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
                                                   int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz,
                                                   const StepState* __restrict__ st, double normFact, double coupling) {
-    fft_z_c2r_body<T, SELF, LT, NC, NT>(spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling, blockIdx.x,
-                                        blockIdx.y);
+    fft_z_c2r_body<T, SELF, LT, NC, NT, FLIP>(spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling, blockIdx.x,
+                                              blockIdx.y);
 }
 
 // ---------------------------------------------------------------- G spectrum
@@ -680,6 +691,60 @@ __global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in,
                                                   long long sb, long long so, long long se, FftPlan pl,
                                                   const double2* __restrict__ twd) {
     dct_lines_body<TO, LT, NC, NT>(in, out, len, nb, sb, so, se, pl, twd, blockIdx.x, blockIdx.y);
+}
+
+// Full real transform of lines of length L along z (stride se), 2 NC lines
+// per block packed two per complex FFT and split by the Hermitian symmetry,
+// as pass A; the half spectrum k in [0, L/2] of line b goes to
+// out[k * nb + b], negated (imgrho2tr = -rho2tr * grntr, FFTPoissonSolver.cpp:316).
+template <typename TO, int LT, int NC, int NT>
+__device__ __forceinline__ void rfft_lines_neg_body(const double* __restrict__ in, Cx<TO>* __restrict__ out, int nb,
+                                                    long long se, const FftPlan& pl, const double2* __restrict__ twd,
+                                                    int bx) {
+    constexpr int RC = 2 * NC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int L = LT > 0 ? LT : pl.L;
+    const int CS = col_stride(L);
+    double2* tw = reinterpret_cast<double2*>(smem_raw);
+    double2* buf = tw + L;
+    double2* tmp = buf + NC * CS + RC;
+    stage_twiddles<double2, NT>(tw, twd, L);
+    const int b0 = bx * RC;
+    for (int e = threadIdx.x; e < RC * L; e += NT) {
+        const int li = e % RC, m = e / RC;
+        const int b = b0 + li;
+        double* slot = reinterpret_cast<double*>(&buf[(li >> 1) * CS + sk(m)]) + (li & 1);
+        if (b < nb)
+            cp_elem(slot, in + b + (long long)m * se);
+        else
+            *slot = 0.0;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const double2* o = block_fft<double, false, LT, NC, NT>(buf, tmp, pl, tw);
+    const int half = L / 2;
+    for (int e = threadIdx.x; e < RC * (half + 1); e += NT) {
+        const int li = e % RC, k = e / RC;
+        const int b = b0 + li;
+        if (b >= nb) continue;
+        const int q = li >> 1;
+        const double2 Z = o[q * CS + sk(k)];
+        const double2 Zm = o[q * CS + sk(k == 0 ? 0 : L - k)];
+        double re, im;
+        if ((li & 1) == 0) {
+            re = 0.5 * (Z.x + Zm.x);
+            im = 0.5 * (Z.y - Zm.y);
+        } else {
+            re = 0.5 * (Z.y + Zm.y);
+            im = -0.5 * (Z.x - Zm.x);
+        }
+        out[(long long)k * nb + b] = Cx<TO>{(TO)(-re), (TO)(-im)};
+    }
+}
+template <typename TO, int LT, int NC, int NT>
+__global__ void __launch_bounds__(NT) k_rfft_lines_neg(const double* __restrict__ in, Cx<TO>* __restrict__ out, int nb,
+                                                       long long se, FftPlan pl, const double2* __restrict__ twd) {
+    rfft_lines_neg_body<TO, LT, NC, NT>(in, out, nb, se, pl, twd, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- dispatch
@@ -743,7 +808,7 @@ struct LaunchY {
     }
 };
 
-template <typename TI>
+template <typename TI, bool CG = false>
 struct LaunchC {
     const Cx<TI>* in;
     double2* out;
@@ -756,12 +821,29 @@ struct LaunchC {
     template <int LT>
     void run() {
         constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
-        k_fft_x_conv<TI, double, LT, NC, NT><<<(unsigned)((rows + NC - 1) / NC), NT, smem_conv<TI>(px.L, NC), s>>>(
+        k_fft_x_conv<TI, double, LT, NC, NT, CG><<<(unsigned)((rows + NC - 1) / NC), NT, smem_conv<TI>(px.L, NC), s>>>(
             in, out, ghat, n0, n1, L1, rows, px, twi, two);
     }
 };
 
-template <bool SELF>
+template <typename TO>
+struct LaunchRfftNeg {
+    const double* in;
+    Cx<TO>* out;
+    int nb;
+    long long se;
+    FftPlan pl;
+    const double2* tw;
+    cudaStream_t s;
+    template <int LT>
+    void run() {
+        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        k_rfft_lines_neg<TO, LT, NC, NT><<<(unsigned)((nb + 2 * NC - 1) / (2 * NC)), NT, smem_of<double2>(pl.L, NC), s>>>(
+            in, out, nb, se, pl, tw);
+    }
+};
+
+template <bool SELF, bool FLIP = false>
 struct LaunchE {
     const double2* spec;
     double* phi;
@@ -775,8 +857,8 @@ struct LaunchE {
     void run() {
         constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
         dim3 g((unsigned)((n0 + 2 * NC - 1) / (2 * NC)), (unsigned)n1);
-        k_fft_z_c2r<double, SELF, LT, NC, NT><<<g, NT, smem_of<double2>(pz.L, NC), s>>>(spec, phi, n0, n1, n2, L0, L1, pz,
-                                                                                          twz, st, normFact, coupling);
+        k_fft_z_c2r<double, SELF, LT, NC, NT, FLIP><<<g, NT, smem_of<double2>(pz.L, NC), s>>>(
+            spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling);
     }
 };
 
@@ -817,6 +899,12 @@ struct SetLimits {
         allow(k_fft_z_c2r<double, false, LT, NC, NT>);
         allow(k_dct_lines<double, LT, NC, NT>);
         allow(k_dct_lines<float, LT, NC, NT>);
+        allow(k_fft_x_conv<double, double, LT, NC, NT, true>);
+        allow(k_fft_x_conv<float, double, LT, NC, NT, true>);
+        allow(k_fft_z_c2r<double, true, LT, NC, NT, true>);
+        allow(k_fft_z_c2r<double, false, LT, NC, NT, true>);
+        allow(k_rfft_lines_neg<double, LT, NC, NT>);
+        allow(k_rfft_lines_neg<float, LT, NC, NT>);
     }
 };
 
@@ -1070,8 +1158,35 @@ void launch_green_transform(const DevBunch& b, cudaStream_t s) {
         with_length(2 * n0, LaunchDct<float>{b.gline, (float*)b.ghat, (int)g0, (int)g1, (int)g2, g0, g0 * g1, 1, p0, tw0, s});
 }
 
+// Spectrum of the image's shifted G (b.gimg, (n0+1)(n1+1)(2 n2), FP64):
+// cosine transforms along y and x on every z plane (G is even in x and y),
+// then a full real transform along z (it is not even in z), negated, into
+// b.ghat_img (n2+1)(n1+1)(n0+1) complex T.
+void launch_green_transform_image(const DevBunch& b, cudaStream_t s) {
+    const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    const long long g0 = n0 + 1, g1 = n1 + 1, L2 = 2 * n2;
+    const long long GI = g0 * g1 * L2;
+    const FftPlan p0 = make_plan(2 * n0), p1 = make_plan(2 * n1), p2 = make_plan(2 * n2);
+    const double2* tw0 = reinterpret_cast<const double2*>(b.tw[0]);
+    const double2* tw1 = reinterpret_cast<const double2*>(b.tw[1]);
+    const double2* tw2 = reinterpret_cast<const double2*>(b.tw[2]);
+    double* ga = b.gimg;
+    double* gb = b.gimg + GI;
+    // y lines: batch x, outer z (2 n2 planes)
+    with_length(2 * n1, LaunchDct<double>{ga, gb, (int)g1, (int)g0, (int)L2, 1, g0 * g1, g0, p1, tw1, s});
+    // x lines: batch y (stride g0), outer z
+    with_length(2 * n0, LaunchDct<double>{gb, ga, (int)g0, (int)g1, (int)L2, g0, g0 * g1, 1, p0, tw0, s});
+    // z lines of length 2 n2: batch (x, y), element stride g0 g1
+    if (b.precision == 0)
+        with_length(2 * n2, LaunchRfftNeg<double>{ga, (double2*)b.ghat_img, (int)(g0 * g1), g0 * g1, p2, tw2, s});
+    else
+        with_length(2 * n2, LaunchRfftNeg<float>{ga, (float2*)b.ghat_img, (int)(g0 * g1), g0 * g1, p2, tw2, s});
+}
+
 // T is the type of the forward half (A, B and the forward x transform of C);
-// the inverse half (C's inverse, D, E) is FP64 in both forms.
+// the inverse half (C's inverse, D, E) is FP64 in both forms.  With energy
+// bins the plain form keeps the forward spectrum in b.spec_fwd, so the bin's
+// own and its image's convolutions (C, D, E twice) start from one A, B.
 // parts: kConvForwardPart (A, B: need only rho) and/or kConvRestPart (C, D,
 // E: need the spectrum of G as well).
 template <typename T>
@@ -1086,7 +1201,7 @@ static void convolution_t(const DevBunch& b, int mode, int parts, cudaStream_t s
     const double2* twx_d = reinterpret_cast<const double2*>(b.tw[0]);
     const double2* twy_d = reinterpret_cast<const double2*>(b.tw[1]);
     const double2* twz_d = reinterpret_cast<const double2*>(b.tw[2]);
-    C* fwd = reinterpret_cast<C*>(b.precision == 0 ? b.spec : b.spec_lo);
+    C* fwd = reinterpret_cast<C*>(b.precision == 0 ? (b.spec_fwd ? b.spec_fwd : b.spec) : b.spec_lo);
     double2* inv = reinterpret_cast<double2*>(b.spec);
     double normFact = 1.0;
     normFact /= L0;
@@ -1096,13 +1211,23 @@ static void convolution_t(const DevBunch& b, int mode, int parts, cudaStream_t s
         with_length(L2, LaunchA<T>{(const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz, s});
         with_length(L1, LaunchY<T, false>{fwd, n0, L0, n1, L1, n2 + 1, py, twy, s});
     }
-    if (!(parts & kConvRestPart)) return;
-    with_length(L0, LaunchC<T>{fwd, inv, (const T*)b.ghat, n0, n1, L1, (n2 + 1) * L1, px, twx, twx_d, s});
-    with_length(L1, LaunchY<double, true>{inv, n0, L0, L1, n1, n2 + 1, py, twy_d, s});
-    if (mode == kConvSelfField)
-        with_length(L2, LaunchE<true>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact, b.bc.coupling, s});
-    else
-        with_length(L2, LaunchE<false>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact, b.bc.coupling, s});
+    if (parts & kConvRestPart) {
+        with_length(L0, LaunchC<T>{fwd, inv, (const T*)b.ghat, n0, n1, L1, (n2 + 1) * L1, px, twx, twx_d, s});
+        with_length(L1, LaunchY<double, true>{inv, n0, L0, L1, n1, n2 + 1, py, twy_d, s});
+        if (mode == kConvSelfField)
+            with_length(L2, LaunchE<true>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact, b.bc.coupling, s});
+        else
+            with_length(L2, LaunchE<false>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact, b.bc.coupling, s});
+    }
+    if (parts & kConvImagePart) {
+        with_length(L0, LaunchC<T, true>{fwd, inv, (const T*)b.ghat_img, n0, n1, L1, (n2 + 1) * L1, px, twx, twx_d, s});
+        with_length(L1, LaunchY<double, true>{inv, n0, L0, L1, n1, n2 + 1, py, twy_d, s});
+        if (mode == kConvSelfField)
+            with_length(L2, LaunchE<true, true>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact, b.bc.coupling, s});
+        else
+            with_length(L2,
+                        LaunchE<false, true>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact, b.bc.coupling, s});
+    }
 }
 
 void launch_convolution(const DevBunch& b, int mode, cudaStream_t s) {

@@ -50,6 +50,20 @@ struct DevBunch {
     // per-launch scratch for optional outputs
     double* Ef;
     double* Bf;
+    // energy bins (PartBunchBase.hpp:639-725); null / 0 for a bunch without
+    int* bin;                        // energy bin of the particle in each slot
+    int* bin_alt;                    // reorder scratch
+    int nbins;                       // getNumberOfEnergyBins
+    int nactive;                     // bins whose fields are computed: min(last emitted, nbins)
+    StepState* bst;                  // per bin: this step's mesh scalars with the bin's gamma
+    unsigned long long* nacc_bins;   // per active bin: node accumulators (as nacc)
+    unsigned long long* bin_partials;
+    double* F8;                      // n^3 x 8: summed E (x, y, z, -) and B (x, y, -, -) of every bin and image
+    void* spec_fwd;                  // plain form with bins: forward spectrum kept for the image solve
+    // image charge (FFTPoissonSolver.cpp:287-327, :546-639); null until used
+    double* gtmp_img;                // 2 x (n0+2)(n1+2)(n2+2): antiderivative planes, z and z - n2 hz
+    double* gimg;                    // 2 x (n0+1)(n1+1)(2 n2): the shifted G and its cosine transforms
+    void* ghat_img;                  // (n2+1)(n1+1)(n0+1) complex T: minus the spectrum of the shifted G
 };
 
 struct FftPlan {
@@ -81,6 +95,24 @@ void launch_soa_to_aos_by_id(const double* a, const double* b, const double* c, 
                              long long n, cudaStream_t s);
 void launch_f64_to_f32(const double* in, float* out, long long n, cudaStream_t s);
 void launch_f32_to_f64(const float* in, double* out, long long n, cudaStream_t s);
+
+// energy bins (sc_particles.cu)
+constexpr int kMaxBins = 64;
+// calcGammas (PartBunchBase.hpp:639-683) into bst[b].gammaz, and the bin's
+// solver scalars (PartBunch.cpp:173-185, :240-246) derived from this step's mesh
+void launch_bin_gammas(const DevBunch& b, cudaStream_t s);
+// one pass over the particles: the charge of every active bin into its own accumulators
+void launch_deposit_bins(const DevBunch& b, cudaStream_t s);
+// -grad phi of one bin's potential (view.st = its StepState), added into F8:
+// E, and B = -+ betaC (E_y, -E_x) (PartBunch.cpp:238-244, image :417-427)
+void launch_grad_acc(const DevBunch& view, bool image, cudaStream_t s);
+void launch_gather_kick_push_bins(const DevBunch& b, bool stats, cudaStream_t s);
+void launch_gather_fields_bins(const DevBunch& b, cudaStream_t s);
+// bin of every slot from a host-order array (slot s holds particle id[s])
+void launch_bins_by_id(const int* host_order, const uint32_t* id, int* bin, long long n, cudaStream_t s);
+void launch_permute_bins(const DevBunch& b, cudaStream_t s);
+// shifted antiderivative planes (st->hr_scaled, st->zshift) and the shifted G on (n0+1)(n1+1)(2 n2)
+void launch_igf_image(const DevBunch& b, cudaStream_t s);
 
 // Batched launches (many bunches, one kernel): `tab` is a device array of
 // DevBunch; `items` holds one entry per bunch of the launch, (bunch, first
@@ -148,9 +180,13 @@ void launch_sort(const DevBunch& b, cudaStream_t s);
 // FFT TU (sc_fft.cu)
 void launch_green_transform(const DevBunch& b, cudaStream_t s);
 void launch_convolution(const DevBunch& b, int mode, cudaStream_t s);
-// the forward passes (A, B) need rho only; the rest (C, D, E) also the spectrum of G
-enum : int { kConvForwardPart = 1, kConvRestPart = 2 };
+// the forward passes (A, B) need rho only; the rest (C, D, E) also the spectrum of G.
+// The image part runs C, D, E with the shifted G's complex spectrum and
+// writes phi with z flipped (FFTPoissonSolver.cpp:312-326).
+enum : int { kConvForwardPart = 1, kConvRestPart = 2, kConvImagePart = 4 };
 void launch_convolution_part(const DevBunch& b, int mode, int parts, cudaStream_t s);
+// spectrum of the shifted G (b.gimg) into b.ghat_img
+void launch_green_transform_image(const DevBunch& b, cudaStream_t s);
 size_t fft_smem_bytes(const DevBunch& b);
 void upload_twiddles(DevBunch& b, cudaStream_t s);
 void fft_set_smem_limits();

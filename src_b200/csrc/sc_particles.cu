@@ -257,9 +257,10 @@ __device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restr
             s.bmax[k] = -tot[3 + k];
         }
         if (!derive_mesh(s, bc)) atomicOr(&s.err, kFlagMesh);
-        // Q *= dt; scatter; Q /= dt  (PartBunch.cpp:493-495)
+        // Q *= dt; scatter; Q /= dt  (PartBunch.cpp:493-495); the energy-bin
+        // loop restores Q from its copy after every bin (ParallelTTracker.cpp:570-576)
         s.qdt = s.Q * bc.dT;
-        s.Q = s.qdt / bc.dT;
+        if (!s.binned) s.Q = s.qdt / bc.dT;
         s.gen += 1u;
         if (s.gen == 0u) s.gen = 1u;
         *ticket = 0u;
@@ -377,8 +378,14 @@ __device__ __forceinline__ void acc_add(unsigned long long* a, long long v) {
 // particles / 64^3; warps with more than kMaxGroupPasses multi-lane groups
 // (sparse regions) add per lane.  No floating-point value is accumulated by
 // an atomic.
+//
+// With energy bins (BINNED) the key is bin * n^3 + cell: every active bin's
+// charge goes to its own accumulators in the same pass, particles of bins
+// not yet emitted deposit nothing (setBinCharge, PartBunchBase.hpp:722-725).
+template <bool BINNED>
 __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double* __restrict__ x,
-                                             const double* __restrict__ y, const double* __restrict__ z, StepState* st,
+                                             const double* __restrict__ y, const double* __restrict__ z,
+                                             const int* __restrict__ bin, int nactive, StepState* st,
                                              unsigned long long* __restrict__ acc, VB g) {
     __shared__ MeshConsts ms;
     __shared__ double qdt_s, to_int_s;
@@ -390,10 +397,13 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int nx = bc.n[0], nxy = bc.n[0] * bc.n[1];
+    const uint32_t M = (uint32_t)nxy * (uint32_t)bc.n[2];
     bool bad = false;
     for (long long i0 = (long long)g.blk * blockDim.x; i0 < bc.N; i0 += (long long)g.nblk * blockDim.x) {
         const long long i = i0 + threadIdx.x;
-        const bool valid = i < bc.N;
+        int bk = 0;
+        if constexpr (BINNED) bk = i < bc.N ? bin[i] : -1;
+        const bool valid = i < bc.N && (!BINNED || (unsigned)bk < (unsigned)nactive);
         uint32_t key = 0xffffffffu;
         double c[8];
         if (valid) {
@@ -403,7 +413,7 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
             const MeshConsts* m = fresh(&ms);
             if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
             cic_charge(d, *fresh(&qdt_s), c);
-            key = (uint32_t)(l[0] + nx * l[1] + nxy * l[2]);
+            key = (uint32_t)(l[0] + nx * l[1] + nxy * l[2]) + (uint32_t)bk * M;
         } else {
 #pragma unroll
             for (int k = 0; k < 8; ++k) c[k] = 0.0;
@@ -451,7 +461,13 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
 __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
                                                       const double* __restrict__ z, StepState* st,
                                                       unsigned long long* __restrict__ acc) {
-    deposit_body(bc, x, y, z, st, acc, vb_grid());
+    deposit_body<false>(bc, x, y, z, nullptr, 0, st, acc, vb_grid());
+}
+__global__ void __launch_bounds__(kThreads) k_deposit_bins(BunchConst bc, const double* __restrict__ x,
+                                                           const double* __restrict__ y, const double* __restrict__ z,
+                                                           const int* __restrict__ bin, int nactive, StepState* st,
+                                                           unsigned long long* __restrict__ acc) {
+    deposit_body<true>(bc, x, y, z, bin, nactive, st, acc, vb_grid());
 }
 
 // correctly rounded double of the 128-bit accumulator (lo, hi), times unit
@@ -560,6 +576,193 @@ __global__ void __launch_bounds__(kThreads) k_igf_G(int n0, int n1, int n2, cons
     igf_G_body(n0, n1, n2, tmp, G, vb_grid());
 }
 
+// ------------------------------------------------------------ image charge
+// Antiderivative planes of the image's Green's function
+// (shiftedIntGreensFunction, FFTPoissonSolver.cpp:556-596): set 0 at
+// z = k hz - hz/2 + zshift (tmpgreen), set 1 at z = k hz - hz/2 + zshift - n2 hz
+// (grn2), k in [0, n2+1]; x, y as in the unshifted function.  hz and zshift
+// are the bin's (st->hr_scaled, st->zshift).
+__global__ void __launch_bounds__(kThreads) k_igf_tmp_img(int n0, int n1, int n2, const StepState* __restrict__ st,
+                                                          double* __restrict__ tmp) {
+    const int t0 = n0 + 2, t1 = n1 + 2, t2 = n2 + 2;
+    const int T3 = t0 * t1 * t2;
+    const double h0 = st->hr_scaled[0], h1 = st->hr_scaled[1], h2 = st->hr_scaled[2];
+    const double zshift = st->zshift;
+    const double cellVolume = h0 * h1 * h2;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < 2 * T3; c += gridDim.x * blockDim.x) {
+        const int set = c >= T3 ? 1 : 0;
+        const int r = c - set * T3;
+        const int i = r % t0, j = (r / t0) % t1, k = r / (t0 * t1);
+        const double vx = i * h0 - h0 / 2;
+        const double vy = j * h1 - h1 / 2;
+        double vz = k * h2 - h2 / 2 + zshift;
+        if (set) vz = vz - n2 * h2;
+        tmp[c] = igf_antiderivative(vx, vy, vz, cellVolume);
+    }
+}
+
+// The image's G on (n0+1)(n1+1)(2 n2), x fastest: z index k <= n2 is the
+// eight-corner sum of set 0 at k (rho2[I][J][K], :598-607), k > n2 that of
+// set 1 at k - n2 (mirrorRhoField(ggrn2), :672-676).  Mirrored in x and y
+// only, so the cosine transforms cover x, y and z takes a full real
+// transform.  No G[0,0,0] overwrite.
+__global__ void __launch_bounds__(kThreads) k_igf_G_img(int n0, int n1, int n2, const double* __restrict__ tmp,
+                                                        double* __restrict__ G) {
+    const int g0 = n0 + 1, g1 = n1 + 1, L2 = 2 * n2;
+    const int t0 = n0 + 2, t1 = n1 + 2;
+    const int T3 = t0 * t1 * (n2 + 2);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g0 * g1 * L2; c += gridDim.x * blockDim.x) {
+        const int i = c % g0, j = (c / g0) % g1, kk = c / (g0 * g1);
+        const double* t = kk <= n2 ? tmp : tmp + T3;
+        const int k = kk <= n2 ? kk : kk - n2;
+#define TG(a, b, e) t[(a) + t0 * ((b) + t1 * (e))]
+        double g = TG(i + 1, j + 1, k + 1);
+        g += TG(i + 1, j, k);
+        g += TG(i, j + 1, k);
+        g += TG(i, j, k + 1);
+        g -= TG(i + 1, j + 1, k);
+        g -= TG(i + 1, j, k + 1);
+        g -= TG(i, j + 1, k + 1);
+        g -= TG(i, j, k);
+#undef TG
+        G[c] = g;
+    }
+}
+
+// ------------------------------------------------------------ energy bins
+// calcGammas (PartBunchBase.hpp:639-683): per bin the sum of sqrt(1 + P.P)
+// and the particle count.  The sum is exact (the 2^-72 fixed point of
+// sc_exact.cuh in three 32-bit limbs, each summed in a 64-bit shared counter:
+// no carry is lost for fewer than 2^32 particles), so the mean does not
+// depend on the particle order.  The last block writes each bin's StepState:
+// this step's mesh with the bin's gamma and the scalars of
+// computeSelfFields(bin) (PartBunch.cpp:173-185, :246-249).
+__global__ void __launch_bounds__(kThreads) k_bin_gammas(BunchConst bc, const double* __restrict__ px,
+                                                         const double* __restrict__ py, const double* __restrict__ pz,
+                                                         const int* __restrict__ bin, int nbins, StepState* st,
+                                                         StepState* __restrict__ bst,
+                                                         unsigned long long* __restrict__ partials, unsigned* ticket) {
+    __shared__ unsigned long long acc[kMaxBins][4];
+    for (int e = threadIdx.x; e < nbins * 4; e += blockDim.x) acc[e >> 2][e & 3] = 0ull;
+    __syncthreads();
+    bool bad = false;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)gridDim.x * blockDim.x) {
+        const int b = bin[i];
+        if ((unsigned)b >= (unsigned)nbins) {
+            bad = true;
+            continue;
+        }
+        const double P[3] = {px[i], py[i], pz[i]};
+        const u128 v = (u128)ex_from(sqrt(1.0 + dot3(P, P)));  // gamma in [1, 2^24): v < 2^96
+        atomicAdd(&acc[b][0], (unsigned long long)(v & 0xffffffffull));
+        atomicAdd(&acc[b][1], (unsigned long long)((v >> 32) & 0xffffffffull));
+        atomicAdd(&acc[b][2], (unsigned long long)(v >> 64));
+        atomicAdd(&acc[b][3], 1ull);
+    }
+    if (bad) atomicOr(&st->err, kFlagBin);
+    __syncthreads();
+    for (int e = threadIdx.x; e < nbins * 4; e += blockDim.x)
+        partials[(size_t)blockIdx.x * nbins * 4 + e] = acc[e >> 2][e & 3];
+    if (!last_block(ticket, gridDim.x)) return;
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
+        unsigned long long t[4] = {0ull, 0ull, 0ull, 0ull};
+        for (int k = 0; k < (int)gridDim.x; ++k)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) t[q] += __ldcg(partials + ((size_t)k * nbins + b) * 4 + q);
+        const u128 sum = (u128)t[0] + ((u128)t[1] << 32) + ((u128)t[2] << 64);
+        const long long cnt = (long long)t[3];
+        double gz = ex_to_double((i128)sum);
+        if (cnt != 0)
+            gz /= (double)cnt;
+        else
+            gz = 1.0;
+        // the fields the bin's kernels read (assemble, Green's functions,
+        // pass E, gradient); the rest of the StepState is not used per bin
+        StepState& o = bst[b];
+        for (int d = 0; d < 3; ++d) {
+            o.hr[d] = st->hr[d];
+            o.rhr[d] = st->rhr[d];
+            o.origin[d] = st->origin[d];
+        }
+        o.qdt = st->qdt;
+        const double scaleFactor = 1;
+        o.gammaz = gz;
+        o.bin_count = cnt;
+        o.tmp2 = 1 / st->hr[0] * 1 / st->hr[1] * 1 / st->hr[2] / (scaleFactor * scaleFactor * scaleFactor) / gz;
+        o.hr_scaled[0] = st->hr[0] * scaleFactor;
+        o.hr_scaled[1] = st->hr[1] * scaleFactor;
+        o.hr_scaled[2] = st->hr[2] * scaleFactor;
+        o.hr_scaled[2] *= gz;
+        o.hvol = o.hr_scaled[0] * o.hr_scaled[1] * o.hr_scaled[2];
+        o.betaC = sqrt(gz * gz - 1.0) / gz / kC;
+        o.zshift = -(2 * st->origin[2] + (0 + (bc.n[2] - 1) + 1) * st->hr[2]) * gz * scaleFactor;
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// -grad phi of one bin (UniformCartesian.hpp:2129-2203, scaled by the bin's
+// (g, g, 1/g), PartBunch.cpp:199-200) added into F8; B of the bin's charge
+// -betaC E_y, +betaC E_x (:238-239), of its image the opposite (:426-427).
+template <bool IMAGE>
+__global__ void __launch_bounds__(kThreads) k_grad_acc(BunchConst bc, const StepState* __restrict__ st,
+                                                       const double* __restrict__ phi, double* __restrict__ F8) {
+    const int n[3] = {bc.n[0], bc.n[1], bc.n[2]};
+    const int M = n[0] * n[1] * n[2];
+    const int stv[3] = {1, n[0], n[0] * n[1]};
+    const double h[3] = {st->hr[0], st->hr[1], st->hr[2]};
+    const double id[3] = {0.5 / h[0], 0.5 / h[1], 0.5 / h[2]};
+    const double gz = st->gammaz;
+    const double sc[3] = {gz / 1.0, gz / 1.0, 1.0 / (1.0 * gz)};
+    const double betaC = st->betaC;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x) {
+        const int idx[3] = {c % n[0], (c / n[0]) % n[1], c / (n[0] * n[1])};
+        double e[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double* f = phi + c;
+            const int s = stv[d];
+            double g;
+            if (idx[d] == 0)
+                g = id[d] * (-1.0 * f[2 * s] + 4.0 * f[s] - 3.0 * f[0]);
+            else if (idx[d] == n[d] - 1)
+                g = id[d] * (1.0 * f[-2 * s] - 4.0 * f[-s] + 3.0 * f[0]);
+            else
+                g = id[d] * (f[s] - f[-s]);
+            e[d] = (-g) * sc[d];
+        }
+        double* o = F8 + 8 * (size_t)c;
+        double2 exy = *reinterpret_cast<const double2*>(o);
+        double2 ez = *reinterpret_cast<const double2*>(o + 2);
+        double2 bxy = *reinterpret_cast<const double2*>(o + 4);
+        exy.x = exy.x + e[0];
+        exy.y = exy.y + e[1];
+        ez.x = ez.x + e[2];
+        if (IMAGE) {
+            bxy.x = bxy.x + betaC * e[1];
+            bxy.y = bxy.y - betaC * e[0];
+        } else {
+            bxy.x = bxy.x - betaC * e[1];
+            bxy.y = bxy.y + betaC * e[0];
+        }
+        *reinterpret_cast<double2*>(o) = exy;
+        *reinterpret_cast<double2*>(o + 2) = ez;
+        *reinterpret_cast<double2*>(o + 4) = bxy;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_bins_by_id(const int* __restrict__ host_order,
+                                                         const uint32_t* __restrict__ id, int* __restrict__ bin,
+                                                         long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        bin[i] = host_order[id[i]];
+}
+
+__global__ void __launch_bounds__(kThreads) k_permute_i32(const uint32_t* __restrict__ sval, const int* __restrict__ in,
+                                                          int* __restrict__ out, long long n) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        out[p] = in[sval[p]];
+}
+
 // ------------------------------------------------------------ gradient
 // phi is FP64 in both forms; T is the storage type of the field.
 template <typename T>
@@ -638,11 +841,45 @@ __device__ __forceinline__ void cic_gather(const T* __restrict__ E4, const int* 
     }
 }
 
-template <typename T>
+// The energy-bin form gathers E and B from the summed field of all bins and
+// images, F8 = (Ex, Ey, Ez, -, Bx, By, -, -) per node (64-byte aligned).
+// Ef += Eftmp and Bf +-= betaC Eftmp of every bin (PartBunch.cpp:238-244,
+// :417-427) are linear in the gathered values, so summing the nodes first
+// gives the same fields up to the order of the additions.
+__device__ __forceinline__ void cic_gather8(const double* __restrict__ F8, const int* n, const int* l, const double* d,
+                                            double* Eb, double* Bb) {
+    const int nx = n[0], nxy = n[0] * n[1];
+    const int b = l[0] + nx * l[1] + nxy * l[2];
+    const double u[3] = {1 - d[0], 1 - d[1], 1 - d[2]};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int a0 = k & 1, a1 = (k >> 1) & 1, a2 = (k >> 2) & 1;
+        const double w = (a0 ? d[0] : u[0]) * (a1 ? d[1] : u[1]) * (a2 ? d[2] : u[2]);
+        const double* p = F8 + 8 * (size_t)(b + a0 + a1 * nx + a2 * nxy);
+        const double2 exy = *reinterpret_cast<const double2*>(p);
+        const double ez = p[2];
+        const double2 bxy = *reinterpret_cast<const double2*>(p + 4);
+        if (k == 0) {
+            Eb[0] = w * exy.x;
+            Eb[1] = w * exy.y;
+            Eb[2] = w * ez;
+            Bb[0] = w * bxy.x;
+            Bb[1] = w * bxy.y;
+        } else {
+            Eb[0] = Eb[0] + w * exy.x;
+            Eb[1] = Eb[1] + w * exy.y;
+            Eb[2] = Eb[2] + w * ez;
+            Bb[0] = Bb[0] + w * bxy.x;
+            Bb[1] = Bb[1] + w * bxy.y;
+        }
+    }
+}
+
+template <typename T, bool BINNED = false>
 __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
                                             double* __restrict__ z, double* __restrict__ px, double* __restrict__ py,
                                             double* __restrict__ pz, const T* __restrict__ E4, StepState* st,
-                                            double* partials, unsigned* ticket, VB g) {
+                                            double* partials, unsigned* ticket, VB g, const double* __restrict__ F8 = nullptr) {
     __shared__ Trafo b2r_s, upd_s;
     __shared__ MeshConsts ms;
     __shared__ double betaC_s;
@@ -662,10 +899,17 @@ __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __rest
         double d[3];
         const MeshConsts* m = fresh(&ms);
         if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
-        double Eb[3];
-        cic_gather(E4, bc.n, l, d, Eb);
-        const double betaC = *fresh(&betaC_s);
-        const double Bb[3] = {0.0 - betaC * Eb[1], 0.0 + betaC * Eb[0], 0.0};
+        double Eb[3], Bb[3];
+        if constexpr (BINNED) {
+            cic_gather8(F8, bc.n, l, d, Eb, Bb);
+            Bb[2] = 0.0;
+        } else {
+            cic_gather(E4, bc.n, l, d, Eb);
+            const double betaC = *fresh(&betaC_s);
+            Bb[0] = 0.0 - betaC * Eb[1];
+            Bb[1] = 0.0 + betaC * Eb[0];
+            Bb[2] = 0.0;
+        }
         double R[3], Ef[3], Bf[3];
         const Trafo* b2r = fresh(&b2r_s);
         trafo_transform_to(*b2r, X, R);
@@ -713,6 +957,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
                                                                   unsigned* ticket) {
     gather_body<T>(bc, x, y, z, px, py, pz, E4, st, partials, ticket, vb_grid());
 }
+__global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push_bins(BunchConst bc, double* __restrict__ x,
+                                                                       double* __restrict__ y, double* __restrict__ z,
+                                                                       double* __restrict__ px, double* __restrict__ py,
+                                                                       double* __restrict__ pz,
+                                                                       const double* __restrict__ F8, StepState* st,
+                                                                       double* partials, unsigned* ticket) {
+    gather_body<double, true>(bc, x, y, z, px, py, pz, nullptr, st, partials, ticket, vb_grid(), F8);
+}
 
 // Fields only (PartBunch::computeSelfFields output): Ef, Bf in the beam frame,
 // AoS (x, y, z per particle).
@@ -742,6 +994,35 @@ __global__ void __launch_bounds__(kThreads) k_gather_fields(BunchConst bc, const
         Ef[3 * i + 2] = E[2];
         Bf[3 * i + 0] = 0.0 - betaC * E[1];
         Bf[3 * i + 1] = 0.0 + betaC * E[0];
+        Bf[3 * i + 2] = 0.0;
+    }
+    if (bad) atomicOr(&st->err, kFlagGuard);
+}
+__global__ void __launch_bounds__(kThreads) k_gather_fields_bins(BunchConst bc, const double* __restrict__ x,
+                                                                 const double* __restrict__ y,
+                                                                 const double* __restrict__ z,
+                                                                 const double* __restrict__ F8, StepState* st,
+                                                                 double* __restrict__ Ef, double* __restrict__ Bf) {
+    __shared__ double hr[3], rhr[3], org[3];
+    if (threadIdx.x < 3) {
+        hr[threadIdx.x] = st->hr[threadIdx.x];
+        rhr[threadIdx.x] = st->rhr[threadIdx.x];
+        org[threadIdx.x] = st->origin[threadIdx.x];
+    }
+    __syncthreads();
+    bool bad = false;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)gridDim.x * blockDim.x) {
+        double X[3] = {x[i], y[i], z[i]};
+        int l[3];
+        double d[3];
+        if (!cic_locate_r(hr, rhr, org, bc.n, X, l, d)) bad = true;
+        double E[3], B[2];
+        cic_gather8(F8, bc.n, l, d, E, B);
+        Ef[3 * i + 0] = E[0];
+        Ef[3 * i + 1] = E[1];
+        Ef[3 * i + 2] = E[2];
+        Bf[3 * i + 0] = B[0];
+        Bf[3 * i + 1] = B[1];
         Bf[3 * i + 2] = 0.0;
     }
     if (bad) atomicOr(&st->err, kFlagGuard);
@@ -839,7 +1120,7 @@ template <int NT>
 __global__ void __launch_bounds__(NT) k_deposit_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
     const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
-    deposit_body(d.bc, d.x, d.y, d.z, d.st, d.nacc, VB{w.y, w.w});
+    deposit_body<false>(d.bc, d.x, d.y, d.z, nullptr, 0, d.st, d.nacc, VB{w.y, w.w});
 }
 
 template <typename T>
@@ -993,6 +1274,54 @@ void launch_gather_fields(const DevBunch& b, cudaStream_t s) {
         k_gather_fields<double><<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, (const double*)b.E4, b.st, b.Ef, b.Bf);
     else
         k_gather_fields<float><<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, (const float*)b.E4, b.st, b.Ef, b.Bf);
+}
+
+constexpr int kBinGammaBlocks = 296;
+
+void launch_bin_gammas(const DevBunch& b, cudaStream_t s) {
+    const int g = b.red_blocks < kBinGammaBlocks ? b.red_blocks : kBinGammaBlocks;
+    k_bin_gammas<<<g, kThreads, 0, s>>>(b.bc, b.px, b.py, b.pz, b.bin, b.nbins, b.st, b.bst, b.bin_partials, b.ticket);
+}
+
+void launch_deposit_bins(const DevBunch& b, cudaStream_t s) {
+    k_deposit_bins<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.bin, b.nactive, b.st, b.nacc_bins);
+}
+
+void launch_grad_acc(const DevBunch& v, bool image, cudaStream_t s) {
+    const long long M = (long long)v.bc.n[0] * v.bc.n[1] * v.bc.n[2];
+    const int g = grid_for(M, 148 * 16);
+    if (image)
+        k_grad_acc<true><<<g, kThreads, 0, s>>>(v.bc, v.st, v.phi, v.F8);
+    else
+        k_grad_acc<false><<<g, kThreads, 0, s>>>(v.bc, v.st, v.phi, v.F8);
+}
+
+void launch_gather_kick_push_bins(const DevBunch& b, bool stats, cudaStream_t s) {
+    k_gather_kick_push_bins<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.F8, b.st,
+                                                              b.partials, b.ticket);
+    if (stats) launch_reduce_stats(b, s);
+}
+
+void launch_gather_fields_bins(const DevBunch& b, cudaStream_t s) {
+    k_gather_fields_bins<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.F8, b.st, b.Ef, b.Bf);
+}
+
+void launch_bins_by_id(const int* host_order, const uint32_t* id, int* bin, long long n, cudaStream_t s) {
+    k_bins_by_id<<<grid_for(n, 148 * 16), kThreads, 0, s>>>(host_order, id, bin, n);
+}
+
+void launch_permute_bins(const DevBunch& b, cudaStream_t s) {
+    const long long n = b.bc.N;
+    k_permute_i32<<<grid_for(n, 148 * 16), kThreads, 0, s>>>(b.vals, b.bin, b.bin_alt, n);
+    cudaMemcpyAsync(b.bin, b.bin_alt, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, s);
+}
+
+void launch_igf_image(const DevBunch& b, cudaStream_t s) {
+    const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    const long long T3 = (long long)(n0 + 2) * (n1 + 2) * (n2 + 2);
+    const long long GI = (long long)(n0 + 1) * (n1 + 1) * (2 * n2);
+    k_igf_tmp_img<<<grid_for(2 * T3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.st, b.gtmp_img);
+    k_igf_G_img<<<grid_for(GI, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.gtmp_img, b.gimg);
 }
 
 void launch_aos_to_soa(const double* aos, double* a, double* b, double* c, long long n, cudaStream_t s) {

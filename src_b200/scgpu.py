@@ -98,6 +98,13 @@ def lib():
         L.scgpu_get_mesh.argtypes = [C.c_void_p, C.POINTER(Mesh)]
         L.scgpu_profile_track.argtypes = [C.c_void_p, C.c_int, _dp]
         L.scgpu_kernels_per_step.argtypes = [C.c_void_p]
+        _ip = C.POINTER(C.c_int)
+        L.scgpu_compute_potential_image.argtypes = [C.c_void_p, _dp, _dp, C.c_double]
+        L.scgpu_compute_potential_image_device.argtypes = [C.c_void_p, C.c_void_p, _dp, C.c_double]
+        L.scgpu_compute_self_fields_binned.argtypes = [C.c_void_p, C.c_longlong, _dp, _dp, _ip, C.c_int, C.c_int,
+                                                       C.c_double, C.c_double, _dp, _dp, _dp]
+        L.scgpu_set_energy_bins.argtypes = [C.c_void_p, _ip, C.c_int, C.c_int]
+        L.scgpu_get_bin_gammas.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong)]
         _lib = L
     return _lib
 
@@ -108,8 +115,11 @@ EXPORTED = [
     "scgpu_compute_self_fields", "scgpu_register_host", "scgpu_unregister_host", "scgpu_bunch_upload",
     "scgpu_bunch_download", "scgpu_track", "scgpu_get_tracker_state", "scgpu_beam_parameters",
     "scgpu_beam_parameters_from_stats", "scgpu_get_field", "scgpu_get_mesh", "scgpu_last_track_ms",
-    "scgpu_profile_track", "scgpu_kernels_per_step",
+    "scgpu_profile_track", "scgpu_kernels_per_step", "scgpu_compute_potential_image",
+    "scgpu_compute_potential_image_device", "scgpu_compute_self_fields_binned", "scgpu_set_energy_bins",
+    "scgpu_get_bin_gammas",
 ]
+MAX_BINS = 64
 
 PHASES = ["drift_bounds", "deposit", "assemble_rho", "green", "convolution", "grad", "gather_kick_push", "reorder"]
 
@@ -138,6 +148,7 @@ class Context:
             raise ScgpuError(rc, f"scgpu_create(nr={self.nr}, precision={precision}) failed")
         self.h = h
         self.n = 0
+        self.nbins = 0
 
     def _check(self, rc, what):
         if rc != 0:
@@ -169,6 +180,55 @@ class Context:
         self._check(lib().scgpu_compute_potential(self.h, _p(r), (C.c_double * 3)(*hr)), "compute_potential")
         return r
 
+    # ---- PoissonSolver::computePotential(rho, hr, zshift): image charge
+    def compute_potential_image(self, rho, hr, zshift):
+        """rho: array [nz, ny, nx].  Returns the image charge's potential
+        (minus the shifted convolution, z flipped)."""
+        r = _f64c(rho).copy()
+        assert r.shape == (self.nr[2], self.nr[1], self.nr[0])
+        self._check(lib().scgpu_compute_potential_image(self.h, _p(r), (C.c_double * 3)(*hr), float(zshift)),
+                    "compute_potential_image")
+        return r
+
+    # ---- the energy-bin loop of computeSpaceChargeFields
+    def compute_self_fields_binned(self, R, P, bins, nbins, q_macro, dT, last_emitted=None):
+        """Beam-frame bunch with one energy bin per particle.  Returns Ef, Bf
+        (summed over the emitted bins and their images) and the bin gammas."""
+        R = _f64c(R)
+        P = _f64c(P)
+        n = R.shape[0]
+        b = np.ascontiguousarray(bins, dtype=np.int32)
+        assert b.shape == (n,)
+        Ef = np.empty_like(R)
+        Bf = np.empty_like(R)
+        g = np.empty(max(int(nbins), 1))
+        le = int(nbins) if last_emitted is None else int(last_emitted)
+        self._check(lib().scgpu_compute_self_fields_binned(self.h, n, _p(R), _p(P), b.ctypes.data_as(C.POINTER(C.c_int)),
+                                                           int(nbins), le, float(q_macro), float(dT), _p(Ef), _p(Bf),
+                                                           _p(g)), "compute_self_fields_binned")
+        return Ef, Bf, g[:int(nbins)]
+
+    def set_energy_bins(self, bins, nbins, last_emitted=None):
+        """Energy bins of the resident bunch (order of the last upload);
+        nbins = 0 returns to one self-field solve."""
+        le = int(nbins) if last_emitted is None else int(last_emitted)
+        if int(nbins) == 0:
+            self._check(lib().scgpu_set_energy_bins(self.h, None, 0, le), "set_energy_bins")
+            return
+        b = np.ascontiguousarray(bins, dtype=np.int32)
+        if self.n and b.shape != (self.n,):
+            raise ValueError(f"bins: expected shape ({self.n},), got {b.shape}")
+        self._check(lib().scgpu_set_energy_bins(self.h, b.ctypes.data_as(C.POINTER(C.c_int)), int(nbins), le),
+                    "set_energy_bins")
+        self.nbins = int(nbins)
+
+    def bin_gammas(self):
+        g = np.empty(self.nbins)
+        cnt = np.empty(self.nbins, dtype=np.int64)
+        self._check(lib().scgpu_get_bin_gammas(self.h, _p(g), cnt.ctypes.data_as(C.POINTER(C.c_longlong))),
+                    "get_bin_gammas")
+        return g, cnt
+
     # ---- PartBunch::computeSelfFields
     def compute_self_fields(self, R, P, q_macro, dT):
         R = _f64c(R)
@@ -192,6 +252,7 @@ class Context:
                          (C.c_double * 3)(*ref_P))
         self._check(lib().scgpu_bunch_upload(self.h, R.shape[0], _p(R), _p(P), C.byref(bp)), "bunch_upload")
         self.n = R.shape[0]
+        self.nbins = 0
 
     def download(self, R=None, P=None):
         """Returns R, P (n x 3); pass pinned arrays to receive them in place."""

@@ -13,6 +13,14 @@ convolution_n8.npz
 step_n8.npz
     A 2000-particle bunch tracked 3 steps on an 8^3 mesh by the oracle with the
     reference's FFTPACK engine: final R, P and the last step's rho, phi, E.
+image_n8.npz
+    rho, hr, zshift and the image-charge potential of
+    FFTPoissonSolver::computePotential(rho, hr, zshift) with the shifted
+    Green's function G2s, by the oracle with the reference's FFTPACK engine.
+binned_step_n8.npz
+    A 3000-particle photoinjector bunch with 4 energy bins tracked 3 steps by
+    the energy-bin loop with image charges (oracle, reference FFTPACK): final
+    R, P and the last step's Ef, Bf.
 
     python tests/golden/make_golden.py
 """
@@ -63,8 +71,27 @@ def main():
     dbg = tr.track(R, P, 3, want_debug=True)
     np.savez_compressed(os.path.join(HERE, "step_n8.npz"), R0=R0, P0=P0, R=R, P=P, rho=dbg["rho"], phi=dbg["phi"],
                         E=dbg["E"], Q=tr.Q, path_length=tr.path_length, t=tr.t)
+    image_and_bins()
     O.use_reference_fft(False)
-    print("wrote fftpack_kat.npz, convolution_n8.npz, step_n8.npz")
+    print("wrote fftpack_kat.npz, convolution_n8.npz, step_n8.npz, image_n8.npz, binned_step_n8.npz")
+
+
+def image_and_bins():
+    from src_b200.bunch import photoinjector_bunch  # noqa: E402
+    rng = np.random.default_rng(20261205)
+    nr = (8, 8, 8)
+    hr = (2.5e-4, 3.0e-4, 4.0e-3)
+    zshift = -3.3e-2
+    rho = rng.standard_normal((nr[2], nr[1], nr[0]))
+    phi = O.compute_potential_shifted(rho, hr, zshift)
+    G2s = O.igf_shifted(nr, hr, zshift)
+    np.savez_compressed(os.path.join(HERE, "image_n8.npz"), rho=rho, hr=np.array(hr), zshift=zshift, phi=phi, G2s=G2s)
+    R, P, bins = photoinjector_bunch(3000, nbins=4, bunch_id=9)
+    R0, P0 = R.copy(), P.copy()
+    tr = O.OracleTracker(O.make_params(nr, 1e-12, ref_pz=1.0), -1e-9 / 3000)
+    dbg = tr.track(R, P, 3, want_debug=True, bins=bins, nbins=4)
+    np.savez_compressed(os.path.join(HERE, "binned_step_n8.npz"), R0=R0, P0=P0, bins=bins, R=R, P=P, Ef=dbg["Ef"],
+                        Bf=dbg["Bf"], Q=tr.Q)
 
 
 if __name__ == "__main__":

@@ -201,3 +201,116 @@ def test_tracker_reference_particle(oracle):
     assert math.isclose(tr.path_length, 4 * beta * oracle.c_light() * 1e-12, rel_tol=1e-13)
     assert np.all(tr.ref_R == 0.0)
     assert math.isclose(tr.t, 4e-12, rel_tol=1e-15)
+
+
+# ---------------------------------------------------------------- image charge and energy bins
+# FFTPoissonSolver::computePotential(rho, hr, zshift) (FFTPoissonSolver.cpp:287-327),
+# shiftedIntGreensFunction (:546-639), computeSelfFields(int bin) (PartBunch.cpp:138-430),
+# calcGammas (PartBunchBase.hpp:639-683).  The reference has no test of these paths;
+# the checks are the shifted solve's own definition (a cyclic convolution with the
+# shifted G), its relation to the unshifted G at zshift = 0, the Coulomb field of a
+# point charge's mirror image, and linearity over bins.
+
+def test_image_solve_is_flipped_negative_convolution(oracle):
+    nr, hr, zs = (16, 12, 20), (1.0e-4, 1.3e-4, 0.8e-4), -3.7e-3
+    rho = np.random.default_rng(1).standard_normal((nr[2], nr[1], nr[0]))
+    G = oracle.igf_shifted(nr, hr, zs)
+    r2 = np.zeros(G.shape)
+    r2[:nr[2], :nr[1], :nr[0]] = rho
+    conv = np.real(np.fft.ifftn(np.fft.fftn(r2) * np.fft.fftn(G)))
+    ref = -conv[:nr[2], :nr[1], :nr[0]][::-1]
+    assert rel(oracle.compute_potential_shifted(rho, hr, zs), ref) < 1e-13
+
+
+def test_shifted_green_at_zero_shift_is_the_unshifted_one(oracle):
+    nr, hr = (16, 12, 20), (1.0e-4, 1.3e-4, 0.8e-4)
+    G0 = oracle.igf(nr, hr)
+    Gs = oracle.igf_shifted(nr, hr, 0.0)
+    m = np.ones(G0.shape, bool)
+    m[0, 0, 0] = False  # the unshifted function's G[0,0,0] <- G[0,0,1] (FFTPoissonSolver.cpp:657)
+    # the eight-corner cancellation turns the ulp differences of mirrored
+    # antiderivative planes into ~1e-12 of the maximum
+    assert np.max(np.abs(Gs - G0)[m]) < 1e-10 * np.max(np.abs(G0))
+    assert Gs[0, 0, 0] > G0[0, 0, 0]
+
+
+def test_image_of_point_charge_is_mirror_coulomb(oracle):
+    nr, hr = (16, 12, 20), (1.0e-4, 1.3e-4, 0.8e-4)
+    b = (3, 5, 8)  # (z, y, x)
+    rho = np.zeros((nr[2], nr[1], nr[0]))
+    rho[b] = 1.0
+    zs = -1e-2
+    phi = oracle.compute_potential_shifted(rho, hr, zs)
+    for a in ((0, 0, 0), (19, 11, 15), (10, 2, 1), (5, 9, 14)):
+        dz = (nr[2] - 1 - a[0] - b[0]) * hr[2] + zs
+        dy = (a[1] - b[1]) * hr[1]
+        dx = (a[2] - b[2]) * hr[0]
+        assert abs(phi[a] * math.sqrt(dx * dx + dy * dy + dz * dz) + 1.0) < 1e-4
+
+
+def test_bin_gammas(oracle):
+    from src_b200.bunch import photoinjector_bunch
+    R, P, bins = photoinjector_bunch(5000, nbins=6, bunch_id=3)
+    bins[bins == 4] = 5  # bin 4 empty
+    g, cnt = oracle.bin_gammas(P, bins, 6)
+    gam = np.sqrt(1.0 + (P * P).sum(1))
+    for k in range(6):
+        if k == 4:
+            assert cnt[k] == 0 and g[k] == 1.0
+        else:
+            assert cnt[k] == np.sum(bins == k)
+            assert abs(g[k] - gam[bins == k].mean()) < 1e-14 * g[k]
+
+
+def test_binned_fields_are_linear_in_bins(oracle):
+    """With equal bin gammas the fields of two bins add up to the field of one
+    bin holding both (the solve is linear in the charge)."""
+    rng = np.random.default_rng(2)
+    n = 20000
+    R = np.column_stack([rng.normal(0, 1e-3, n), rng.normal(0, 1e-3, n), rng.normal(4e-3, 1e-3, n)])
+    P = np.tile([0.0, 0.0, 5.0], (n, 1))
+    prm = oracle.make_params((16, 16, 16), 1e-12)
+    qi = -1e-9 / n
+    with oracle.exact():
+        b2 = (R[:, 2] > 4e-3).astype(np.int32)
+        E2, B2, g2, _ = oracle.compute_self_fields_binned(prm, qi, R, P, b2, 2)
+        E1, B1, g1, _ = oracle.compute_self_fields_binned(prm, qi, R, P, np.zeros(n, np.int32), 1)
+        assert g2[0] == g2[1] == g1[0]
+        assert np.linalg.norm(E2 - E1) < 1e-13 * np.linalg.norm(E1)
+        assert np.linalg.norm(B2 - B1) < 1e-13 * np.linalg.norm(B1)
+        # bins not yet emitted carry no field
+        E0, _, _, _ = oracle.compute_self_fields_binned(prm, qi, R, P, b2, 2, last_emitted=1)
+        Ea, _, _, _ = oracle.compute_self_fields_binned(prm, qi, R, P, np.where(b2 == 0, 0, 1).astype(np.int32), 3,
+                                                        last_emitted=1)
+        np.testing.assert_array_equal(E0, Ea)
+        # the image of an electron bunch behind the cathode (z < 0) is positive: it pushes E_z up
+        Eu, _, _, _ = oracle.compute_self_fields(prm, qi, R, P, want_grids=False)
+        assert np.mean((E1 - Eu)[:, 2]) > 0
+
+
+def test_binned_tracker_runs(oracle):
+    from src_b200.bunch import photoinjector_bunch
+    R, P, bins = photoinjector_bunch(3000, nbins=4, bunch_id=5)
+    tr = oracle.OracleTracker(oracle.make_params((8, 8, 8), 1e-12, ref_pz=1.0), -1e-9 / 3000)
+    Q0 = tr.Q
+    tr.track(R, P, 3, bins=bins, nbins=4)
+    assert np.all(np.isfinite(R)) and np.all(np.isfinite(P))
+    assert tr.Q == Q0  # the bin loop restores Q (ParallelTTracker.cpp:576)
+
+
+def test_image_solve_matches_reference_fftpack_golden(oracle):
+    g = np.load(os.path.join(GOLD, "image_n8.npz"))
+    phi = oracle.compute_potential_shifted(g["rho"], g["hr"], float(g["zshift"]))
+    assert rel(phi, g["phi"]) < 1e-14
+    G2s = oracle.igf_shifted((8, 8, 8), g["hr"], float(g["zshift"]))
+    assert rel(G2s, g["G2s"]) < 1e-15
+
+
+def test_binned_step_golden(oracle):
+    g = np.load(os.path.join(GOLD, "binned_step_n8.npz"))
+    R, P = g["R0"].copy(), g["P0"].copy()
+    tr = oracle.OracleTracker(oracle.make_params((8, 8, 8), 1e-12, ref_pz=1.0), -1e-9 / 3000)
+    dbg = tr.track(R, P, 3, want_debug=True, bins=g["bins"], nbins=4)
+    assert rel(R, g["R"]) < 1e-14 and rel(P, g["P"]) < 1e-14
+    assert rel(dbg["Ef"], g["Ef"]) < 1e-13 and rel(dbg["Bf"], g["Bf"]) < 1e-13
+    assert tr.Q == float(g["Q"])
