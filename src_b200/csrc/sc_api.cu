@@ -780,6 +780,11 @@ int scgpu_bunch_upload(scgpu_ctx* c, long long n, const double* R, const double*
     if (!c || !R || !P || !bp) return fail(c, SCGPU_ERR_ARG, "null argument");
     if (!(bp->dT > 0.0) || !(bp->mass > 0.0)) return fail(c, SCGPU_ERR_ARG, "dT and mass must be positive");
     CK(cudaSetDevice(c->device));
+    // A bunch of the same size keeps the device's slot order (slot s takes
+    // host particle id[s]): the cell order of the last reorder stays nearly
+    // right for the next steps, and no result depends on the order (every
+    // sum over particles is exact).
+    const bool keep_order = c->have_bunch && n == c->n;
     int rc = ensure_particles(c, n);
     if (rc) return rc;
     DevBunch& b = c->b;
@@ -815,10 +820,15 @@ int scgpu_bunch_upload(scgpu_ctx* c, long long n, const double* R, const double*
     CK(cudaMemsetAsync(b.hist, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(int), s));
     CK(cudaMemcpyAsync(b.Ef, R, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(b.Bf, P, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
-    launch_aos_to_soa(b.Ef, b.x, b.y, b.z, n, s);
-    launch_aos_to_soa(b.Bf, b.px, b.py, b.pz, n, s);
-    launch_iota(b.id, n, s);
-    c->steps_done = 0;
+    if (keep_order) {
+        launch_aos_to_soa_by_id(b.Ef, b.id, b.x, b.y, b.z, n, s);
+        launch_aos_to_soa_by_id(b.Bf, b.id, b.px, b.py, b.pz, n, s);
+    } else {
+        launch_aos_to_soa(b.Ef, b.x, b.y, b.z, n, s);
+        launch_aos_to_soa(b.Bf, b.px, b.py, b.pz, n, s);
+        launch_iota(b.id, n, s);
+        c->steps_done = 0;
+    }
     launch_reduce_state(b, true, s);
     CK(cudaGetLastError());
     rc = check_device_err(c);

@@ -88,6 +88,9 @@ void launch_gather_kick_push(const DevBunch& b, bool stats, cudaStream_t s);
 void launch_gather_fields(const DevBunch& b, cudaStream_t s);
 void launch_reduce_stats(const DevBunch& b, cudaStream_t s);
 void launch_aos_to_soa(const double* aos, double* a, double* b, double* c, long long n, cudaStream_t s);
+// host order AoS -> slot order SoA: slot i takes particle id[i]
+void launch_aos_to_soa_by_id(const double* aos, const uint32_t* id, double* a, double* b, double* c, long long n,
+                             cudaStream_t s);
 void launch_soa_to_aos(const double* a, const double* b, const double* c, double* aos, long long n, cudaStream_t s);
 void launch_reorder(const DevBunch& b, cudaStream_t s);
 void launch_iota(uint32_t* id, long long n, cudaStream_t s);

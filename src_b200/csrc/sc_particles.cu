@@ -90,9 +90,37 @@ __device__ __forceinline__ void block_sum_ex(i128 (&v)[NV], i128* __restrict__ p
 }
 
 // Exact total of column k over nb block partials, rounded once: out[k].
+// For a few columns every thread of the (last) block loads a share of the
+// rows, so all loads are in flight at once instead of one warp walking each
+// column; the integer sums are exact, so the order does not matter.
 template <int NV>
 __device__ __forceinline__ void final_sum_ex(const i128* partials, int nb, double* out) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if constexpr (NV <= 8) {
+        i128 s[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s[k] = 0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            const unsigned long long* q = reinterpret_cast<const unsigned long long*>(partials + (size_t)b * NV);
+#pragma unroll
+            for (int k = 0; k < NV; ++k) s[k] += (i128)(((u128)__ldcg(q + 2 * k + 1) << 64) | __ldcg(q + 2 * k));
+        }
+        __shared__ i128 sm[NV][kWarps];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) s[k] += ex_shfl_down(s[k], off);
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) sm[k][warp] = s[k];
+        __syncthreads();
+        if (threadIdx.x < NV) {
+            i128 t = 0;
+            for (int w = 0; w < kWarps; ++w) t += sm[threadIdx.x][w];
+            out[threadIdx.x] = ex_to_double(t);
+        }
+        return;
+    }
     for (int k = warp; k < NV; k += kWarps) {
         i128 s = 0;
         for (int b = lane; b < nb; b += 32) {
@@ -106,16 +134,29 @@ __device__ __forceinline__ void final_sum_ex(const i128* partials, int nb, doubl
     }
 }
 
-// Same pattern with min (exact, order-independent).
+// Same pattern with min (exact, order-independent), all threads loading.
 template <int NV>
 __device__ __forceinline__ void final_min(const double* partials, int nb, double* out) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = warp; k < NV; k += kWarps) {
-        double s = INFINITY;
-        for (int b = lane; b < nb; b += 32) s = fmin(s, __ldcg(partials + (size_t)b * NV + k));
+    double s[NV];
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s = fmin(s, __shfl_down_sync(kFull, s, off));
-        if (lane == 0) out[k] = s;
+    for (int k = 0; k < NV; ++k) s[k] = INFINITY;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s[k] = fmin(s[k], __ldcg(partials + (size_t)b * NV + k));
+    __shared__ double sm[NV][kWarps];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s[k] = fmin(s[k], __shfl_down_sync(kFull, s[k], off));
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sm[k][warp] = s[k];
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double t = INFINITY;
+        for (int w = 0; w < kWarps; ++w) t = fmin(t, sm[threadIdx.x][w]);
+        out[threadIdx.x] = t;
     }
 }
 
@@ -1028,6 +1069,18 @@ __global__ void __launch_bounds__(kThreads) k_gather_fields_bins(BunchConst bc, 
     if (bad) atomicOr(&st->err, kFlagGuard);
 }
 
+__global__ void __launch_bounds__(kThreads) k_aos_to_soa_by_id(const double* __restrict__ aos,
+                                                               const uint32_t* __restrict__ id, double* __restrict__ a,
+                                                               double* __restrict__ b, double* __restrict__ c,
+                                                               long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const size_t q = 3 * (size_t)id[i];
+        a[i] = aos[q + 0];
+        b[i] = aos[q + 1];
+        c[i] = aos[q + 2];
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ a,
                                                          double* __restrict__ b, double* __restrict__ c, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -1322,6 +1375,11 @@ void launch_igf_image(const DevBunch& b, cudaStream_t s) {
     const long long GI = (long long)(n0 + 1) * (n1 + 1) * (2 * n2);
     k_igf_tmp_img<<<grid_for(2 * T3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.st, b.gtmp_img);
     k_igf_G_img<<<grid_for(GI, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.gtmp_img, b.gimg);
+}
+
+void launch_aos_to_soa_by_id(const double* aos, const uint32_t* id, double* a, double* b, double* c, long long n,
+                             cudaStream_t s) {
+    k_aos_to_soa_by_id<<<grid_for(n, 148 * 16), kThreads, 0, s>>>(aos, id, a, b, c, n);
 }
 
 void launch_aos_to_soa(const double* aos, double* a, double* b, double* c, long long n, cudaStream_t s) {

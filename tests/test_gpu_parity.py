@@ -279,3 +279,27 @@ def test_mixed_form_long_run_bounds(gpu, oracle):
     Em, epsm = out[gpu.MIXED]
     assert rel(Em, Ed) < 1e-5
     assert np.max(np.abs(epsm - epsd) / np.abs(epsd)) < 1e-6
+
+
+def test_reupload_keeps_order_and_results(oracle, gpu):
+    """An upload of a bunch of the same size keeps the device's slot (cell)
+    order; the results equal those of a fresh context, bitwise, because
+    every sum over particles is exact."""
+    N, nr = 50_000, (32, 32, 32)
+    R, P = gaussian_bunch(N, bunch_id=4)
+    Q, m = -1e-9 / N, oracle.electron_mass_ev()
+    with gpu.Context(nr) as a:
+        a.upload(R, P, 1e-12, Q, m)
+        a.track(5)
+        R1, P1 = a.download()
+        st = a.tracker_state()
+        kw = dict(t=st["t"], path_length=st["path_length"], ref_R=st["ref_R"], ref_P=st["ref_P"])
+        a.upload(R1, P1, 1e-12, st["q_macro"], m, **kw)
+        a.track(7)
+        Ra, Pa = a.download()
+    with gpu.Context(nr) as b:
+        b.upload(R1, P1, 1e-12, st["q_macro"], m, **kw)
+        b.track(7)
+        Rb, Pb = b.download()
+    np.testing.assert_array_equal(Ra, Rb)
+    np.testing.assert_array_equal(Pa, Pb)
