@@ -209,6 +209,34 @@ int scgpu_beam_parameters(scgpu_ctx* ctx, scgpu_beam_params* out);
 /* beam parameters from one SCGPU_NSTATS record of scgpu_track */
 int scgpu_beam_parameters_from_stats(const double* record, long long n, scgpu_beam_params* out);
 
+/* Statistics and particle files in the reference's formats.
+ *
+ * scgpu_stat_row: one row of the SDDS .stat file for the resident bunch
+ * (DataSink::doWriteStatData, src/Structure/DataSink.cpp:281-449, after
+ * calcBeamParameters, PartBunchBase.hpp:1529-1614): SCGPU_STAT_COLUMNS
+ * values in the file's column order (t [ns], s, numParticles, charge, mean
+ * energy [MeV], rms, emittances, means, reference particle, max extent,
+ * correlations, dispersion, the external field at the reference particle,
+ * energy spread, dt [ns], particles outside n sigma, particle 0).
+ * scgpu_sdds_write_header / scgpu_sdds_append_row write the file
+ * (header DataSink.cpp:585-1032; values as the reference's stream writes
+ * them, %.15e followed by nine spaces and a tab); with_particle0 = 0 leaves
+ * out the last six columns, as a multi-rank reference run does.
+ * scgpu_read_fromfile[_count] / scgpu_write_fromfile: the ASCII distribution
+ * of DISTRIBUTION TYPE=FROMFILE (Distribution.cpp:1074-1159): comment lines
+ * ('#'), the count N, then N records "x px y py z pz"; momenta_in_ev
+ * converts eV to beta*gamma (converteVToBetaGamma, :1047-1053). */
+#define SCGPU_STAT_COLUMNS 48
+int scgpu_stat_row(scgpu_ctx* ctx, double* row);
+const char* scgpu_stat_column_name(int column);
+int scgpu_sdds_write_header(const char* path, const char* input_name, int processors, const char* revision,
+                            const char* flavor);
+int scgpu_sdds_append_row(const char* path, const double* row, int with_particle0);
+int scgpu_read_fromfile_count(const char* path, long long* n);
+int scgpu_read_fromfile(const char* path, long long capacity, double* R, double* P, int momenta_in_ev, double mass_ev,
+                        long long* n);
+int scgpu_write_fromfile(const char* path, long long n, const double* R, const double* P);
+
 /* diagnostics of the last solve: SCGPU_FIELD_* grids and the mesh */
 int scgpu_get_field(scgpu_ctx* ctx, int which, double* out);
 int scgpu_get_mesh(scgpu_ctx* ctx, scgpu_mesh* out);

@@ -915,6 +915,74 @@ int scgpu_beam_parameters(scgpu_ctx* c, scgpu_beam_params* out) {
     return scgpu_beam_parameters_from_stats(rec, c->n, out);
 }
 
+// One row of DataSink::doWriteStatData (DataSink.cpp:281-449) for the resident
+// bunch: calcBeamParameters (PartBunchBase.hpp:1529-1614) with calcEMean
+// (:2099-2114), get_bounds, the tracker state and particle 0.
+int scgpu_stat_row(scgpu_ctx* c, double* row) {
+    if (!c || !row) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    CK(cudaSetDevice(c->device));
+    DevBunch& b = c->b;
+    cudaStream_t s = c->stream;
+    launch_reduce_stats(b, s);
+    double* scratch = b.Ef;  // 3 N doubles >= 12
+    launch_bounds(b, scratch, s);
+    launch_find_id(b, 0u, scratch + 6, s);
+    double rec[SCGPU_NSTATS], ext[12];
+    StepState h;
+    CK(cudaMemcpyAsync(rec, b.st->moments, sizeof(rec), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(ext, scratch, sizeof(ext), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&h, b.st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    const long long n = c->n;
+    const double N = (double)n;
+    scgpu_beam_params bp;
+    std::memset(&bp, 0, sizeof bp);
+    beam_params_from_sums(rec, rec[27], N, &bp);
+    // calcEMean: sum of sqrt(P.P + 1) minus N, times m [MeV], over N
+    double eKin = rec[27];
+    eKin -= N;
+    eKin *= b.bc.mass * 1.0e-6;
+    eKin /= N;
+    // getCharge: sum(Q) over the particles, in storage order
+    double Q = 0.0;
+    for (long long i = 0; i < n; ++i) Q += h.Q;
+    const double m0 = b.bc.mass * 1.E-6;
+    const double tmp = 1.0 / std::pow(eKin / m0 + 1., 2.0);
+    const double dE = bp.prms[2] * m0 * std::sqrt(1.0 - tmp);
+    int k = 0;
+    row[k++] = h.t * 1e9;
+    row[k++] = h.path_length;
+    row[k++] = N;
+    row[k++] = Q;
+    row[k++] = eKin;
+    for (int d = 0; d < 3; ++d) row[k++] = bp.rrms[d];
+    for (int d = 0; d < 3; ++d) row[k++] = bp.prms[d];
+    for (int d = 0; d < 3; ++d) row[k++] = bp.eps_norm[d];
+    for (int d = 0; d < 3; ++d) row[k++] = bp.rmean[d];
+    for (int d = 0; d < 3; ++d) row[k++] = h.ref_R[d];
+    for (int d = 0; d < 3; ++d) row[k++] = h.ref_P[d];
+    for (int d = 0; d < 3; ++d) row[k++] = ext[3 + d];  // get_maxExtent = rmax
+    for (int d = 0; d < 3; ++d) row[k++] = bp.rprms[d];
+    row[k++] = rec[mom_idx(0, 5)] / N;  // Dx
+    row[k++] = rec[mom_idx(1, 5)] / N;  // DDx
+    row[k++] = rec[mom_idx(2, 5)] / N;  // Dy
+    row[k++] = rec[mom_idx(3, 5)] / N;  // DDy
+    // external B [T] and E [MV/m] at the reference particle: the uniform solenoid field
+    row[k++] = 0.0;
+    row[k++] = 0.0;
+    row[k++] = b.bc.bz_ext;
+    row[k++] = 0.0;
+    row[k++] = 0.0;
+    row[k++] = 0.0;
+    row[k++] = dE;
+    row[k++] = b.bc.dT * 1e9;
+    row[k++] = 0.0;  // outside n sigma: Options::beamHaloBoundary is 0 by default
+    for (int d = 0; d < 6; ++d) row[k++] = ext[6 + d];
+    return SCGPU_OK;
+}
+
 int scgpu_beam_parameters_from_stats(const double* rec, long long n, scgpu_beam_params* out) {
     if (!rec || !out || n <= 0) return SCGPU_ERR_ARG;
     std::memset(out, 0, sizeof(*out));

@@ -791,6 +791,62 @@ __global__ void __launch_bounds__(kThreads) k_grad_acc(BunchConst bc, const Step
     }
 }
 
+// get_bounds of the particle positions (PartBunchBase.hpp:1178-1219) for the
+// statistics: min of x, y, z and of -x, -y, -z into out[6] (exact, any order).
+__global__ void __launch_bounds__(kThreads) k_bounds(BunchConst bc, const double* __restrict__ x,
+                                                     const double* __restrict__ y, const double* __restrict__ z,
+                                                     double* partials, unsigned* ticket, double* __restrict__ out) {
+    double v[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)gridDim.x * blockDim.x) {
+        const double R[3] = {x[i], y[i], z[i]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            v[d] = fmin(v[d], R[d]);
+            v[3 + d] = fmin(v[3 + d], -R[d]);
+        }
+    }
+    __shared__ double sm[6][kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = fmin(v[k], __shfl_down_sync(kFull, v[k], off));
+    if (lane == 0)
+        for (int k = 0; k < 6; ++k) sm[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double m = INFINITY;
+        for (int w = 0; w < kWarps; ++w) m = fmin(m, sm[threadIdx.x][w]);
+        partials[(size_t)blockIdx.x * 6 + threadIdx.x] = m;
+    }
+    if (!last_block(ticket, gridDim.x)) return;
+    __shared__ double tot[6];
+    final_min<6>(partials, gridDim.x, tot);
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        out[threadIdx.x] = tot[threadIdx.x];
+        out[3 + threadIdx.x] = -tot[3 + threadIdx.x];
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// The state of the particle with original index `target` (R[0], P[0] of the statistics).
+__global__ void __launch_bounds__(kThreads) k_find_id(const uint32_t* __restrict__ id, long long n, uint32_t target,
+                                                      const double* __restrict__ x, const double* __restrict__ y,
+                                                      const double* __restrict__ z, const double* __restrict__ px,
+                                                      const double* __restrict__ py, const double* __restrict__ pz,
+                                                      double* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (id[i] == target) {
+            out[0] = x[i];
+            out[1] = y[i];
+            out[2] = z[i];
+            out[3] = px[i];
+            out[4] = py[i];
+            out[5] = pz[i];
+        }
+}
+
 __global__ void __launch_bounds__(kThreads) k_bins_by_id(const int* __restrict__ host_order,
                                                          const uint32_t* __restrict__ id, int* __restrict__ bin,
                                                          long long n) {
@@ -1357,6 +1413,14 @@ void launch_gather_kick_push_bins(const DevBunch& b, bool stats, cudaStream_t s)
 
 void launch_gather_fields_bins(const DevBunch& b, cudaStream_t s) {
     k_gather_fields_bins<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.F8, b.st, b.Ef, b.Bf);
+}
+
+void launch_bounds(const DevBunch& b, double* out6, cudaStream_t s) {
+    k_bounds<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.partials, b.ticket, out6);
+}
+
+void launch_find_id(const DevBunch& b, uint32_t target, double* out6, cudaStream_t s) {
+    k_find_id<<<grid_for(b.bc.N, 148 * 16), kThreads, 0, s>>>(b.id, b.bc.N, target, b.x, b.y, b.z, b.px, b.py, b.pz, out6);
 }
 
 void launch_bins_by_id(const int* host_order, const uint32_t* id, int* bin, long long n, cudaStream_t s) {

@@ -105,6 +105,15 @@ def lib():
                                                        C.c_double, C.c_double, _dp, _dp, _dp]
         L.scgpu_set_energy_bins.argtypes = [C.c_void_p, _ip, C.c_int, C.c_int]
         L.scgpu_get_bin_gammas.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong)]
+        L.scgpu_stat_row.argtypes = [C.c_void_p, _dp]
+        L.scgpu_stat_column_name.argtypes = [C.c_int]
+        L.scgpu_stat_column_name.restype = C.c_char_p
+        L.scgpu_sdds_write_header.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_char_p]
+        L.scgpu_sdds_append_row.argtypes = [C.c_char_p, _dp, C.c_int]
+        L.scgpu_read_fromfile_count.argtypes = [C.c_char_p, C.POINTER(C.c_longlong)]
+        L.scgpu_read_fromfile.argtypes = [C.c_char_p, C.c_longlong, _dp, _dp, C.c_int, C.c_double,
+                                          C.POINTER(C.c_longlong)]
+        L.scgpu_write_fromfile.argtypes = [C.c_char_p, C.c_longlong, _dp, _dp]
         _lib = L
     return _lib
 
@@ -117,8 +126,10 @@ EXPORTED = [
     "scgpu_beam_parameters_from_stats", "scgpu_get_field", "scgpu_get_mesh", "scgpu_last_track_ms",
     "scgpu_profile_track", "scgpu_kernels_per_step", "scgpu_compute_potential_image",
     "scgpu_compute_potential_image_device", "scgpu_compute_self_fields_binned", "scgpu_set_energy_bins",
-    "scgpu_get_bin_gammas",
+    "scgpu_get_bin_gammas", "scgpu_stat_row", "scgpu_stat_column_name", "scgpu_sdds_write_header",
+    "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
 ]
+STAT_COLUMNS = 48
 MAX_BINS = 64
 
 PHASES = ["drift_bounds", "deposit", "assemble_rho", "green", "convolution", "grad", "gather_kick_push", "reorder"]
@@ -221,6 +232,12 @@ class Context:
         self._check(lib().scgpu_set_energy_bins(self.h, b.ctypes.data_as(C.POINTER(C.c_int)), int(nbins), le),
                     "set_energy_bins")
         self.nbins = int(nbins)
+
+    def stat_row(self):
+        """One row of the reference's .stat file for the resident bunch."""
+        row = np.empty(STAT_COLUMNS)
+        self._check(lib().scgpu_stat_row(self.h, _p(row)), "stat_row")
+        return row
 
     def bin_gammas(self):
         g = np.empty(self.nbins)
@@ -471,3 +488,50 @@ class Batch:
         """Times the candidate launch shapes on the current bunches; returns
         the number of steps the trials advanced every bunch."""
         return self._check(_batch_lib().scgpu_batch_autotune(self.h, int(trial_steps)), "batch_autotune")
+
+
+# ---- the reference's file formats (host side of the C ABI; no device needed)
+def stat_column_names():
+    return [lib().scgpu_stat_column_name(i).decode() for i in range(STAT_COLUMNS)]
+
+
+class StatWriter:
+    """DataSink's SDDS statistics file: the header on creation, one row per
+    write(row) (rows from Context.stat_row)."""
+
+    def __init__(self, path, input_name="", processors=1, revision="", flavor="opal-t", with_particle0=True):
+        self.path = os.fsencode(path)
+        self.with_particle0 = with_particle0
+        rc = lib().scgpu_sdds_write_header(self.path, input_name.encode(), int(processors), revision.encode(),
+                                           flavor.encode())
+        if rc != 0:
+            raise ScgpuError(rc, f"cannot write {path}")
+
+    def write(self, row):
+        r = _f64c(row, (STAT_COLUMNS,))
+        rc = lib().scgpu_sdds_append_row(self.path, _p(r), 1 if self.with_particle0 else 0)
+        if rc != 0:
+            raise ScgpuError(rc, "cannot append a statistics row")
+
+
+def read_fromfile(path, momenta_in_ev=False, mass_ev=0.51099892e6):
+    """DISTRIBUTION TYPE=FROMFILE: returns R, P (n x 3, P as beta*gamma)."""
+    n = C.c_longlong(0)
+    rc = lib().scgpu_read_fromfile_count(os.fsencode(path), C.byref(n))
+    if rc != 0:
+        raise ScgpuError(rc, f"{path} does not hold an ASCII distribution")
+    R = np.empty((n.value, 3))
+    P = np.empty((n.value, 3))
+    rc = lib().scgpu_read_fromfile(os.fsencode(path), n.value, _p(R), _p(P), 1 if momenta_in_ev else 0,
+                                   float(mass_ev), C.byref(n))
+    if rc != 0:
+        raise ScgpuError(rc, f"cannot read {path}")
+    return R, P
+
+
+def write_fromfile(path, R, P):
+    R = _f64c(R)
+    P = _f64c(P)
+    rc = lib().scgpu_write_fromfile(os.fsencode(path), R.shape[0], _p(R), _p(P))
+    if rc != 0:
+        raise ScgpuError(rc, f"cannot write {path}")

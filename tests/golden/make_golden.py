@@ -21,6 +21,10 @@ binned_step_n8.npz
     A 3000-particle photoinjector bunch with 4 energy bins tracked 3 steps by
     the energy-bin loop with image charges (oracle, reference FFTPACK): final
     R, P and the last step's Ef, Bf.
+sdds_stat_columns.json
+    The column definitions (name, type, units, description), the &data block
+    and the parameter rows of the reference's SDDS statistics file, read from
+    src/Structure/DataSink.cpp (writeSDDSHeader).
 
     python tests/golden/make_golden.py
 """
@@ -72,6 +76,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "step_n8.npz"), R0=R0, P0=P0, R=R, P=P, rho=dbg["rho"], phi=dbg["phi"],
                         E=dbg["E"], Q=tr.Q, path_length=tr.path_length, t=tr.t)
     image_and_bins()
+    sdds_columns()
     O.use_reference_fft(False)
     print("wrote fftpack_kat.npz, convolution_n8.npz, step_n8.npz, image_n8.npz, binned_step_n8.npz")
 
@@ -96,3 +101,21 @@ def image_and_bins():
 
 if __name__ == "__main__":
     main()
+
+
+def sdds_columns():
+    import json
+    import re
+    ref = os.environ.get("REF_DIR", "/root/reference")
+    src = open(os.path.join(ref, "src", "Structure", "DataSink.cpp")).read()
+    i = src.index("void DataSink::writeSDDSHeader(std::ofstream &outputFile,\n")
+    j = src.index("void DataSink::", i + 50)
+    blk = src[i:j]
+    cols = re.findall(r'&column\\n"\s*<< indent << "name=([^,]*),\\n"\s*<< indent << "type=([^,]*),\\n"'
+                      r'\s*<< indent << "units=([^,]*),\\n"\s*<< indent << "description=\\"([^"]*)\\"', blk)
+    params = re.findall(r'&parameter\\n"\s*<< indent << "name=([^,]*),\\n"\s*<< indent << "type=([^,]*),', blk)
+    data = re.findall(r'<< indent << "(mode=ascii,|no_row_counts=1)', blk)
+    out = {"source": "src/Structure/DataSink.cpp writeSDDSHeader", "columns": cols, "parameters": params,
+           "data": data, "value_format": "scientific, precision 15 (DataSink::open_m), then setw(10) << tab"}
+    with open(os.path.join(HERE, "sdds_stat_columns.json"), "w") as f:
+        json.dump(out, f, indent=1)

@@ -20,7 +20,9 @@ Tolerances are norm-wise, max|gpu - oracle| / max|oracle|:
   cancellation of the reference's one-pass formula (PartBunchBase.hpp:1549-1557):
   the tolerance is 1e-12 times the condition number sum(p^2)/(sum(p^2) - N pmean^2).
 """
+import functools
 import math
+import operator
 
 import numpy as np
 import pytest
@@ -303,3 +305,42 @@ def test_reupload_keeps_order_and_results(oracle, gpu):
         Rb, Pb = b.download()
     np.testing.assert_array_equal(Ra, Rb)
     np.testing.assert_array_equal(Pa, Pb)
+
+
+def test_stat_row_vs_oracle(oracle, gpu, tmp_path):
+    """One .stat row (DataSink::doWriteStatData) after a few steps against the
+    oracle's calcBeamParameters of its own tracked bunch."""
+    N, nr, steps = 20_000, (16, 16, 16), 4
+    R, P = gaussian_bunch(N, bunch_id=6)
+    Q = -1e-9 / N
+    tr = oracle.OracleTracker(oracle.make_params(nr, 1e-12, bz_ext=0.2), Q)
+    Ro, Po = R.copy(), P.copy()
+    tr.track(Ro, Po, steps)
+    with gpu.Context(nr) as c:
+        c.upload(R, P, 1e-12, Q, oracle.electron_mass_ev(), bz_ext=0.2)
+        c.track(steps)
+        row = c.stat_row()
+        w = gpu.StatWriter(tmp_path / "run.stat")
+        w.write(row)
+    names = gpu.stat_column_names()
+    v = dict(zip(names, row))
+    bp = oracle.beam_parameters(Ro, Po)
+    m = oracle.electron_mass_ev()
+    assert v["t"] == tr.t * 1e9 and v["s"] == tr.path_length and v["numParticles"] == N
+    # sum(Q) in storage order (not Python's compensated sum())
+    assert v["charge"] == functools.reduce(operator.add, [tr.Q] * N, 0.0)
+    gam = np.sqrt(1.0 + (Po * Po).sum(1))
+    assert abs(v["energy"] - (gam.sum() - N) * m * 1e-6 / N) < 1e-12 * v["energy"]
+    for key, arr in (("rms_", bp["rrms"]), ("emit_", bp["eps_norm"]), ("mean_", bp["rmean"])):
+        got = np.array([v[key + a] for a in ("x", "y", "s")])
+        assert rel(got, arr) < 1e-11, key
+    got = np.array([v["rms_px"], v["rms_py"], v["rms_ps"]])
+    assert rel(got, bp["prms"]) < 1e-11
+    assert rel(np.array([v["max_x"], v["max_y"], v["max_s"]]), Ro.max(0)) < 1e-12
+    assert rel(np.array([v["R0_x"], v["R0_y"], v["R0_s"]]), Ro[0]) < 1e-12
+    assert rel(np.array([v["P0_x"], v["P0_y"], v["P0_s"]]), Po[0]) < 1e-12
+    mom = bp["moments"]
+    assert abs(v["Dx"] - mom[21] / N) <= 1e-12 * abs(mom[21] / N) + 1e-30
+    assert v["Bz_ref"] == 0.2 and v["dt"] == 1e-12 * 1e9 and v["partsOutside"] == 0
+    text = (tmp_path / "run.stat").read_text().splitlines()
+    assert float(text[-1].split("\t")[0]) == float(f"{v['t']:.15e}")
