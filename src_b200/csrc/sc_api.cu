@@ -118,7 +118,7 @@ int ensure_bins(scgpu_ctx* c, int nbins) {
     const size_t cs = b.precision == SCGPU_PLAIN_FP64 ? sizeof(double2) : sizeof(float2);
     if (!b.bst) {
         if ((rc = dalloc(c, &b.bst, kMaxBins * sizeof(StepState))) ||
-            (rc = dalloc(c, &b.bin_partials, 296 * kMaxBins * 4 * sizeof(unsigned long long))) ||
+            (rc = dalloc(c, &b.bin_partials, 296 * kMaxBins * 8 * sizeof(unsigned long long))) ||
             (rc = dalloc(c, &b.F8, M * 8 * sizeof(double))) || (rc = dalloc(c, (char**)&c->ghat_alt, G3 * rs)) ||
             (rc = dalloc(c, (char**)&c->ghat_img_alt, G3 * cs)))
             return rc;

@@ -672,46 +672,71 @@ __global__ void __launch_bounds__(kThreads) k_igf_G_img(int n0, int n1, int n2, 
 
 // ------------------------------------------------------------ energy bins
 // calcGammas (PartBunchBase.hpp:639-683): per bin the sum of sqrt(1 + P.P)
-// and the particle count.  The sum is exact (the 2^-72 fixed point of
-// sc_exact.cuh in three 32-bit limbs, each summed in a 64-bit shared counter:
-// no carry is lost for fewer than 2^32 particles), so the mean does not
-// depend on the particle order.  The last block writes each bin's StepState:
-// this step's mesh with the bin's gamma and the scalars of
-// computeSelfFields(bin) (PartBunch.cpp:173-185, :246-249).
+// and the particle count.  The sum is exact: gamma as the 2^-72 fixed point
+// of sc_exact.cuh (below 2^96 for gamma < 2^24) in six 16-bit limbs.  Lanes
+// of a warp with the same bin (match.any) sum their limbs with redux.sync
+// (at most 32 * 2^16 < 2^21 per limb) and the group's first lane adds them
+// to 64-bit shared counters, so no carry is lost for fewer than 2^48
+// particles and the mean does not depend on the particle order.  The last
+// block sums the block partials (all threads, one column per lane) and
+// writes each bin's StepState: this step's mesh with the bin's gamma and the
+// scalars of computeSelfFields(bin) (PartBunch.cpp:173-185, :246-249).
+constexpr int kGammaLimbs = 6;
+constexpr int kGammaCols = kGammaLimbs + 1;  // limbs and the count
 __global__ void __launch_bounds__(kThreads) k_bin_gammas(BunchConst bc, const double* __restrict__ px,
                                                          const double* __restrict__ py, const double* __restrict__ pz,
                                                          const int* __restrict__ bin, int nbins, StepState* st,
                                                          StepState* __restrict__ bst,
                                                          unsigned long long* __restrict__ partials, unsigned* ticket) {
-    __shared__ unsigned long long acc[kMaxBins][4];
-    for (int e = threadIdx.x; e < nbins * 4; e += blockDim.x) acc[e >> 2][e & 3] = 0ull;
+    __shared__ unsigned long long acc[kMaxBins * kGammaCols];
+    const int ncol = nbins * kGammaCols;
+    for (int e = threadIdx.x; e < ncol; e += blockDim.x) acc[e] = 0ull;
     __syncthreads();
+    const int lane = threadIdx.x & 31;
     bool bad = false;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)gridDim.x * blockDim.x) {
-        const int b = bin[i];
-        if ((unsigned)b >= (unsigned)nbins) {
-            bad = true;
-            continue;
+    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < bc.N; i0 += (long long)gridDim.x * blockDim.x) {
+        const long long i = i0 + threadIdx.x;
+        int b = -1;
+        unsigned limb[kGammaLimbs] = {0u, 0u, 0u, 0u, 0u, 0u};
+        if (i < bc.N) {
+            b = bin[i];
+            if ((unsigned)b >= (unsigned)nbins) {
+                bad = true;
+                b = -1;
+            } else {
+                const double P[3] = {px[i], py[i], pz[i]};
+                const u128 v = (u128)ex_from(sqrt(1.0 + dot3(P, P)));
+#pragma unroll
+                for (int q = 0; q < kGammaLimbs; ++q) limb[q] = (unsigned)(v >> (16 * q)) & 0xffffu;
+            }
         }
-        const double P[3] = {px[i], py[i], pz[i]};
-        const u128 v = (u128)ex_from(sqrt(1.0 + dot3(P, P)));  // gamma in [1, 2^24): v < 2^96
-        atomicAdd(&acc[b][0], (unsigned long long)(v & 0xffffffffull));
-        atomicAdd(&acc[b][1], (unsigned long long)((v >> 32) & 0xffffffffull));
-        atomicAdd(&acc[b][2], (unsigned long long)(v >> 64));
-        atomicAdd(&acc[b][3], 1ull);
+        const unsigned group = __match_any_sync(kFull, b);
+        unsigned sum[kGammaLimbs];
+#pragma unroll
+        for (int q = 0; q < kGammaLimbs; ++q) sum[q] = __reduce_add_sync(group, limb[q]);
+        if (b >= 0 && lane == __ffs(group) - 1) {
+            unsigned long long* a = acc + b * kGammaCols;
+#pragma unroll
+            for (int q = 0; q < kGammaLimbs; ++q) atomicAdd(a + q, (unsigned long long)sum[q]);
+            atomicAdd(a + kGammaLimbs, (unsigned long long)__popc(group));
+        }
     }
     if (bad) atomicOr(&st->err, kFlagBin);
     __syncthreads();
-    for (int e = threadIdx.x; e < nbins * 4; e += blockDim.x)
-        partials[(size_t)blockIdx.x * nbins * 4 + e] = acc[e >> 2][e & 3];
+    for (int e = threadIdx.x; e < ncol; e += blockDim.x) partials[(size_t)blockIdx.x * ncol + e] = acc[e];
     if (!last_block(ticket, gridDim.x)) return;
+    __shared__ unsigned long long tot[kMaxBins * kGammaCols];
+    for (int e = threadIdx.x; e < ncol; e += blockDim.x) tot[e] = 0ull;
+    __syncthreads();
+    for (long long e = threadIdx.x; e < (long long)gridDim.x * ncol; e += blockDim.x)
+        atomicAdd(&tot[e % ncol], __ldcg(partials + e));
+    __syncthreads();
     for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
-        unsigned long long t[4] = {0ull, 0ull, 0ull, 0ull};
-        for (int k = 0; k < (int)gridDim.x; ++k)
+        const unsigned long long* t = tot + b * kGammaCols;
+        u128 sum = 0;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) t[q] += __ldcg(partials + ((size_t)k * nbins + b) * 4 + q);
-        const u128 sum = (u128)t[0] + ((u128)t[1] << 32) + ((u128)t[2] << 64);
-        const long long cnt = (long long)t[3];
+        for (int q = 0; q < kGammaLimbs; ++q) sum += (u128)t[q] << (16 * q);
+        const long long cnt = (long long)t[kGammaLimbs];
         double gz = ex_to_double((i128)sum);
         if (cnt != 0)
             gz /= (double)cnt;
