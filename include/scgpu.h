@@ -17,6 +17,8 @@
  *   scgpu_compute_potential, scgpu_compute_potential_device
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr)
  *       (src/Solvers/PoissonSolver.h:28; FFTPoissonSolver.cpp:337-382)
+ *   scgpu_set_periodic_z
+ *       the bcz argument of FFTPoissonSolver (FieldSolver BCFFTZ, src/Structure/FieldSolver.cpp:431, :486)
  *   scgpu_compute_potential_image, scgpu_compute_potential_image_device
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr, double zshift)
  *       (src/Solvers/PoissonSolver.h:59; FFTPoissonSolver.cpp:287-327 with
@@ -157,6 +159,16 @@ int scgpu_compute_potential_device(scgpu_ctx* ctx, double* rho_inout_device, con
  * Q *= dt ... Q /= dt round trip. */
 int scgpu_compute_self_fields(scgpu_ctx* ctx, long long n, const double* R, const double* P, double* q_macro, double dT,
                               double* Ef, double* Bf);
+
+/* FIELDSOLVER BCFFTZ=PERIODIC (FFTPoissonSolver(..., bcz="PERIODIC"),
+ * src/Solvers/FFTPoissonSolver.cpp:60, :130-155, :189-190, :661-662): the
+ * context's Poisson solves (scgpu_compute_potential[_device],
+ * scgpu_compute_self_fields) double the grid in x and y only and convolve
+ * cyclically along z with the integrated Green's function at offsets
+ * [0, nz) (not mirrored in z).  Needs an even nz; tracking (which would need
+ * the periodic particle boundary of a DC beam), energy bins and image
+ * charges return SCGPU_ERR_UNSUPPORTED while it is on. */
+int scgpu_set_periodic_z(scgpu_ctx* ctx, int periodic);
 
 /* PoissonSolver::computePotential(rho, hr, zshift): rho in, the potential of
  * its image charge out (in place, same units as scgpu_compute_potential):

@@ -215,6 +215,23 @@ def compute_potential(rho, hr):
     return r
 
 
+def igf_periodic_z(nr, hr):
+    """Green's function of the periodic-z solver, grid [nz, 2ny, 2nx]."""
+    G = np.empty((nr[2], 2 * nr[1], 2 * nr[0]), dtype=np.float64)
+    lib().sco_igf_periodic_z((C.c_int * 3)(*nr), (C.c_double * 3)(*hr), _ptr(G))
+    return G
+
+
+def compute_potential_periodic_z(rho, hr):
+    """computePotential with BCFFTZ=PERIODIC: open in x, y, cyclic along z."""
+    r = _f64(rho).copy()
+    nr = (C.c_int * 3)(r.shape[2], r.shape[1], r.shape[0])
+    rc = lib().sco_compute_potential_periodic_z(nr, _ptr(r), (C.c_double * 3)(*hr))
+    if rc:
+        raise RuntimeError(f"sco_compute_potential_periodic_z failed: {rc}")
+    return r
+
+
 def igf_shifted(nr, hr, zshift):
     """Shifted integrated Green's function of the image charge, doubled grid
     [2nz, 2ny, 2nx] (mirrored in x and y only)."""

@@ -1057,6 +1057,86 @@ int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const
 }
 
 /* ------------------------------------------------------------------------ */
+/* periodic z (FFTPoissonSolver with bcz = "PERIODIC", FFTPoissonSolver.cpp:  */
+/* 60, :130-155, :189-190, :661-662): the grid is doubled in x and y only;     */
+/* G is the integrated Green's function at offsets k in [0, nz) along z,      */
+/* mirrored in x and y but not in z, with G[0,0,0] <- G[0,0,1]; the          */
+/* convolution is cyclic along z.  G2: (2nx)(2ny)(nz), x fastest.            */
+/* ------------------------------------------------------------------------ */
+void sco_igf_periodic_z(const int* nr, const double* hr, double* G2) {
+    const long long n0 = nr[0], n1 = nr[1], n2 = nr[2];
+    const long long t0 = n0 + 2, t1 = n1 + 2, t2 = n2 + 2;
+    const long long L0 = 2 * n0, L1 = 2 * n1, L2 = n2;
+    double cellVolume = hr[0] * hr[1] * hr[2];
+    double* tmp = (double*)malloc(t0 * t1 * t2 * sizeof(double));
+    SCO_PAR
+    for (long long k = 0; k < t2; ++k)
+        for (long long j = 0; j < t1; ++j)
+            for (long long i = 0; i < t0; ++i) {
+                double vx = i * hr[0] - hr[0] / 2;
+                double vy = j * hr[1] - hr[1] / 2;
+                double vz = k * hr[2] - hr[2] / 2;
+                tmp[i + t0 * (j + t1 * k)] = igf_antiderivative(vx, vy, vz, cellVolume);
+            }
+#define TG(a, b, c) tmp[(a) + t0 * ((b) + t1 * (c))]
+    memset(G2, 0, L0 * L1 * L2 * sizeof(double));
+    SCO_PAR
+    for (long long k = 0; k < L2; ++k)
+        for (long long j = 0; j <= n1; ++j)
+            for (long long i = 0; i <= n0; ++i) {
+                double g = TG(i + 1, j + 1, k + 1);
+                g += TG(i + 1, j, k);
+                g += TG(i, j + 1, k);
+                g += TG(i, j, k + 1);
+                g -= TG(i + 1, j + 1, k);
+                g -= TG(i + 1, j, k + 1);
+                g -= TG(i, j + 1, k + 1);
+                g -= TG(i, j, k);
+                if (i < L0 && j < L1) G2[i + L0 * (j + L1 * k)] = g;
+            }
+#undef TG
+    free(tmp);
+    if (L2 > 1) G2[0] = G2[L0 * L1 * 1];
+    for (long long k = 0; k < L2; ++k)
+        for (long long j = 0; j <= n1 && j < L1; ++j)
+            for (long long i = n0 + 1; i < L0; ++i)
+                G2[i + L0 * (j + L1 * k)] = G2[(L0 - i) + L0 * (j + L1 * k)];
+    for (long long k = 0; k < L2; ++k)
+        for (long long j = n1 + 1; j < L1; ++j)
+            for (long long i = 0; i < L0; ++i)
+                G2[i + L0 * (j + L1 * k)] = G2[i + L0 * ((L1 - j) + L1 * k)];
+}
+
+int sco_compute_potential_periodic_z(const int* nr, double* rho, const double* hr) {
+    const long long n0 = nr[0], n1 = nr[1], n2 = nr[2];
+    const int L[3] = {2 * nr[0], 2 * nr[1], nr[2]};
+    const long long L0 = L[0], L1 = L[1], L2 = L[2], C0 = L0 / 2 + 1;
+    const long long D = L0 * L1 * L2, S = C0 * L1 * L2;
+    double* rho2 = (double*)calloc(D, sizeof(double));
+    double* rhot = (double*)malloc(2 * S * sizeof(double));
+    double* grnt = (double*)malloc(2 * S * sizeof(double));
+    double* G2 = (double*)malloc(D * sizeof(double));
+    if (!rho2 || !rhot || !grnt || !G2) { free(rho2); free(rhot); free(grnt); free(G2); return SCO_ERR_OOM; }
+    for (long long k = 0; k < n2; ++k)
+        for (long long j = 0; j < n1; ++j)
+            memcpy(rho2 + L0 * (j + L1 * k), rho + n0 * (j + n1 * k), n0 * sizeof(double));
+    sco_fft3d_r2c(L, rho2, rhot);
+    sco_igf_periodic_z(nr, hr, G2);
+    sco_fft3d_r2c(L, G2, grnt);
+    for (long long s = 0; s < S; ++s) {
+        double ar = rhot[2 * s], ai = rhot[2 * s + 1], br = grnt[2 * s], bi = grnt[2 * s + 1];
+        rhot[2 * s] = ar * br - ai * bi;
+        rhot[2 * s + 1] = ar * bi + ai * br;
+    }
+    sco_fft3d_c2r(L, rhot, rho2);
+    for (long long k = 0; k < n2; ++k)
+        for (long long j = 0; j < n1; ++j)
+            memcpy(rho + n0 * (j + n1 * k), rho2 + L0 * (j + L1 * k), n0 * sizeof(double));
+    free(rho2); free(rhot); free(grnt); free(G2);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* shifted integrated Green's function for the image charge                  */
 /* (FFTPoissonSolver::shiftedIntGreensFunction, FFTPoissonSolver.cpp:546-639, */
 /* and mirrorRhoField(ggrn2), :667-693).  Output: doubled real grid G2,        */

@@ -122,6 +122,10 @@ void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, doub
 int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const double* R, const double* P,
                             double* Ef, double* Bf, sco_debug* dbg);
 
+/* periodic z, BCFFTZ=PERIODIC (FFTPoissonSolver.cpp:60, :130-155, :661-662) */
+void sco_igf_periodic_z(const int* nr, const double* hr, double* G2);
+int sco_compute_potential_periodic_z(const int* nr, double* rho, const double* hr);
+
 /* image charge (FFTPoissonSolver.cpp:287-327, :546-639) */
 void sco_igf_shifted(const int* nr, const double* hr, double zshift, double* G2);
 int sco_compute_potential_shifted(const int* nr, double* rho, const double* hr, double zshift);

@@ -383,7 +383,10 @@ int stage_check(scgpu_ctx* c, cudaStream_t s, const char* name) {
 // the solve shared by compute_potential and compute_self_fields
 void enqueue_green(scgpu_ctx* c, cudaStream_t s) {
     launch_igf(c->b, nullptr, s);
-    launch_green_transform(c->b, s);
+    if (c->b.periodic_z)
+        launch_green_transform_periodic(c->b, s);
+    else
+        launch_green_transform(c->b, s);
 }
 
 }  // namespace
@@ -569,6 +572,7 @@ static int compute_potential_image_impl(scgpu_ctx* c, double* rho, const double 
     for (int d = 0; d < 3; ++d)
         if (!(hr[d] > 0.0) || !std::isfinite(hr[d])) return fail(c, SCGPU_ERR_ARG, "hr must be positive and finite");
     if (!std::isfinite(zshift)) return fail(c, SCGPU_ERR_ARG, "zshift must be finite");
+    if (c->b.periodic_z) return fail(c, SCGPU_ERR_UNSUPPORTED, "image charges with periodic z");
     CK(cudaSetDevice(c->device));
     int rc = ensure_image(c);
     if (rc) return rc;
@@ -596,6 +600,34 @@ static int compute_potential_image_impl(scgpu_ctx* c, double* rho, const double 
     CK(cudaMemcpyAsync(rho, b.phi, M * sizeof(double), out_kind, s));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
+    c->have_solve = false;
+    return SCGPU_OK;
+}
+
+// BCFFTZ=PERIODIC (FieldSolver.cpp:431, :486; FFTPoissonSolver.cpp:60,
+// :130-155, :189-190, :661-662): the solves of this context use a grid
+// doubled in x and y only and a cyclic convolution along z.
+int scgpu_set_periodic_z(scgpu_ctx* c, int periodic) {
+    if (!c) return SCGPU_ERR_ARG;
+    DevBunch& b = c->b;
+    const int on = periodic ? 1 : 0;
+    if (on == b.periodic_z) return SCGPU_OK;
+    if (on) {
+        const int n2 = b.bc.n[2];
+        if (n2 % 2 != 0 || n2 < 4 || make_plan(n2).nst <= 0)
+            return fail(c, SCGPU_ERR_UNSUPPORTED, "periodic z needs an even mesh size along z with a supported transform");
+        if (b.nbins > 0) return fail(c, SCGPU_ERR_UNSUPPORTED, "periodic z with energy bins");
+    }
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (on) {
+        int rc = ensure_image(c);
+        if (rc) return rc;
+    }
+    drop_graphs(c);
+    b.periodic_z = on;
+    upload_twiddles(b, c->stream);
+    CK(cudaGetLastError());
     c->have_solve = false;
     return SCGPU_OK;
 }
@@ -681,6 +713,7 @@ static int set_bins_impl(scgpu_ctx* c, const int* bins, int nbins, int last_emit
     DevBunch& b = c->b;
     cudaStream_t s = c->stream;
     const int nactive = last_emitted < nbins ? last_emitted : nbins;
+    if (nbins > 0 && b.periodic_z) return fail(c, SCGPU_ERR_UNSUPPORTED, "energy bins with periodic z");
     if (nbins != b.nbins || nactive != b.nactive) drop_graphs(c);
     if (nbins == 0) {
         b.nbins = b.nactive = 0;
@@ -732,6 +765,7 @@ int scgpu_compute_self_fields_binned(scgpu_ctx* c, long long n, const double* R,
     int rc = check_bins_args(c, bins, nbins, last_emitted);
     if (rc) return rc;
     if (nbins == 0) return fail(c, SCGPU_ERR_ARG, "nbins must be positive");
+    if (c->b.periodic_z) return fail(c, SCGPU_ERR_UNSUPPORTED, "energy bins with periodic z");
     CK(cudaSetDevice(c->device));
     if ((rc = ensure_particles(c, n))) return rc;
     if ((rc = ensure_bins(c, nbins))) return rc;
@@ -854,6 +888,8 @@ int scgpu_bunch_download(scgpu_ctx* c, double* R, double* P) {
 int scgpu_track(scgpu_ctx* c, int nsteps, double* stats) {
     if (!c || nsteps < 0) return fail(c, SCGPU_ERR_ARG, "bad argument");
     if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    if (c->b.periodic_z)
+        return fail(c, SCGPU_ERR_UNSUPPORTED, "tracking a DC beam (periodic z needs the periodic particle boundary)");
     CK(cudaSetDevice(c->device));
     const bool want = stats != nullptr;
     cudaStream_t s = c->stream;

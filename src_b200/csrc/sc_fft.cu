@@ -404,7 +404,10 @@ __host__ __device__ constexpr size_t tile_elems(int L, int nc) {
 
 // ---------------------------------------------------------------- pass A
 // 2 NC real columns (x) of one y per block, packed two per complex FFT.
-template <typename T, int LT, int NC, int NT>
+// FULL: the z transform covers the data without zero padding (periodic z,
+// L2 = n2); otherwise L2 = 2 n2 and the upper half is zero.  The half
+// spectrum has L2/2 + 1 entries either way.
+template <typename T, int LT, int NC, int NT, bool FULL = false>
 __device__ __forceinline__ void fft_z_r2c_body(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1, int n2,
                                                int L0, int L1, const FftPlan& pz, const Cx<T>* __restrict__ twz, int bx,
                                                int by) {
@@ -430,8 +433,9 @@ __device__ __forceinline__ void fft_z_r2c_body(const T* __restrict__ rho, Cx<T>*
     }
     cp_async_wait_all();
     __syncthreads();
-    const C* out = block_fft<T, false, LT, NC, NT, kPruneIn>(buf, tmp, pz, tw);
-    for (int e = threadIdx.x; e < RC * (n2 + 1); e += NT) {
+    const C* out = block_fft<T, false, LT, NC, NT, FULL ? kPruneNone : kPruneIn>(buf, tmp, pz, tw);
+    const int K = L2 / 2;
+    for (int e = threadIdx.x; e < RC * (K + 1); e += NT) {
         const int xi = e % RC, k = e / RC;
         const int x = x0 + xi;
         if (x >= n0) continue;
@@ -446,10 +450,10 @@ __device__ __forceinline__ void fft_z_r2c_body(const T* __restrict__ rho, Cx<T>*
         spec[((size_t)k * L1 + y) * L0 + x] = r;
     }
 }
-template <typename T, int LT, int NC, int NT>
+template <typename T, int LT, int NC, int NT, bool FULL = false>
 __global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1, int n2,
                                                   int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz) {
-    fft_z_r2c_body<T, LT, NC, NT>(rho, spec, n0, n1, n2, L0, L1, pz, twz, blockIdx.x, blockIdx.y);
+    fft_z_r2c_body<T, LT, NC, NT, FULL>(rho, spec, n0, n1, n2, L0, L1, pz, twz, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------- pass B / D
@@ -571,7 +575,8 @@ __global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out
 // ---------------------------------------------------------------- pass E
 // FLIP: the image potential is read back with z flipped,
 // rho[i][j][k] = rho2[i][j][n2 - k - 1] (FFTPoissonSolver.cpp:322-326).
-template <typename T, bool SELF, int LT, int NC, int NT, bool FLIP = false>
+// FULL: all L2 = n2 outputs of an unpadded (periodic) z transform.
+template <typename T, bool SELF, int LT, int NC, int NT, bool FLIP = false, bool FULL = false>
 __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
                                                int n2, int L0, int L1, const FftPlan& pz, const Cx<T>* __restrict__ twz,
                                                const StepState* __restrict__ st, double normFact, double coupling, int bx,
@@ -587,11 +592,12 @@ __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, d
     stage_twiddles<C, NT>(tw, twz, L2);
     const int y = by;
     const int x0 = bx * RC;
-    // the half spectra of the 2 NC columns in tmp: [xi][k], k <= n2
-    for (int e = threadIdx.x; e < RC * (n2 + 1); e += NT) {
+    // the half spectra of the 2 NC columns in tmp: [xi][k], k <= K = L2 / 2
+    const int K = L2 / 2;
+    for (int e = threadIdx.x; e < RC * (K + 1); e += NT) {
         const int xi = e % RC, k = e / RC;
         const int x = x0 + xi;
-        C* slot = &tmp[xi * (n2 + 1) + k];
+        C* slot = &tmp[xi * (K + 1) + k];
         if (x < n0)
             cp_elem(slot, &spec[((size_t)k * L1 + y) * L0 + x]);
         else
@@ -601,12 +607,12 @@ __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, d
     __syncthreads();
     for (int e = threadIdx.x; e < NC * L2; e += NT) {
         const int q = e / L2, k = e - q * L2;
-        const C* A = tmp + (2 * q) * (n2 + 1);
-        const C* B = tmp + (2 * q + 1) * (n2 + 1);
+        const C* A = tmp + (2 * q) * (K + 1);
+        const C* B = tmp + (2 * q + 1) * (K + 1);
         C z;
-        if (k <= n2) {
+        if (k <= K) {
             C a = A[k], b = B[k];
-            if (k == 0 || k == n2) {  // the half-complex format holds no imaginary part there
+            if (k == 0 || k == K) {  // the half-complex format holds no imaginary part there
                 a.y = (T)0;
                 b.y = (T)0;
             }
@@ -618,7 +624,7 @@ __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, d
         buf[q * CS + sk(k)] = z;
     }
     __syncthreads();
-    const C* out = block_fft<T, true, LT, NC, NT, kPruneOut>(buf, tmp, pz, tw);
+    const C* out = block_fft<T, true, LT, NC, NT, FULL ? kPruneNone : kPruneOut>(buf, tmp, pz, tw);
     const double hvol = SELF ? st->hvol : 1.0;
     for (int e = threadIdx.x; e < RC * n2; e += NT) {
         const int xi = e % RC, zz = e / RC;
@@ -634,12 +640,12 @@ __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, d
         phi[((size_t)(FLIP ? n2 - 1 - zz : zz) * n1 + y) * n0 + x] = r;
     }
 }
-template <typename T, bool SELF, int LT, int NC, int NT, bool FLIP = false>
+template <typename T, bool SELF, int LT, int NC, int NT, bool FLIP = false, bool FULL = false>
 __global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
                                                   int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz,
                                                   const StepState* __restrict__ st, double normFact, double coupling) {
-    fft_z_c2r_body<T, SELF, LT, NC, NT, FLIP>(spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling, blockIdx.x,
-                                              blockIdx.y);
+    fft_z_c2r_body<T, SELF, LT, NC, NT, FLIP, FULL>(spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling,
+                                                    blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------- G spectrum
@@ -696,8 +702,9 @@ __global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in,
 // Full real transform of lines of length L along z (stride se), 2 NC lines
 // per block packed two per complex FFT and split by the Hermitian symmetry,
 // as pass A; the half spectrum k in [0, L/2] of line b goes to
-// out[k * nb + b], negated (imgrho2tr = -rho2tr * grntr, FFTPoissonSolver.cpp:316).
-template <typename TO, int LT, int NC, int NT>
+// out[k * nb + b], negated with NEG (imgrho2tr = -rho2tr * grntr,
+// FFTPoissonSolver.cpp:316).
+template <typename TO, int LT, int NC, int NT, bool NEG = true>
 __device__ __forceinline__ void rfft_lines_neg_body(const double* __restrict__ in, Cx<TO>* __restrict__ out, int nb,
                                                     long long se, const FftPlan& pl, const double2* __restrict__ twd,
                                                     int bx) {
@@ -738,13 +745,13 @@ __device__ __forceinline__ void rfft_lines_neg_body(const double* __restrict__ i
             re = 0.5 * (Z.y + Zm.y);
             im = -0.5 * (Z.x - Zm.x);
         }
-        out[(long long)k * nb + b] = Cx<TO>{(TO)(-re), (TO)(-im)};
+        out[(long long)k * nb + b] = NEG ? Cx<TO>{(TO)(-re), (TO)(-im)} : Cx<TO>{(TO)re, (TO)im};
     }
 }
-template <typename TO, int LT, int NC, int NT>
+template <typename TO, int LT, int NC, int NT, bool NEG = true>
 __global__ void __launch_bounds__(NT) k_rfft_lines_neg(const double* __restrict__ in, Cx<TO>* __restrict__ out, int nb,
                                                        long long se, FftPlan pl, const double2* __restrict__ twd) {
-    rfft_lines_neg_body<TO, LT, NC, NT>(in, out, nb, se, pl, twd, blockIdx.x);
+    rfft_lines_neg_body<TO, LT, NC, NT, NEG>(in, out, nb, se, pl, twd, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- dispatch
@@ -777,7 +784,7 @@ void with_length(int L, F&& f) {
     }
 }
 
-template <typename T>
+template <typename T, bool FULL = false>
 struct LaunchA {
     const T* rho;
     Cx<T>* spec;
@@ -789,7 +796,7 @@ struct LaunchA {
     void run() {
         constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
         dim3 g((unsigned)((n0 + 2 * NC - 1) / (2 * NC)), (unsigned)n1);
-        k_fft_z_r2c<T, LT, NC, NT><<<g, NT, smem_of<Cx<T>>(pz.L, NC), s>>>(rho, spec, n0, n1, n2, L0, L1, pz, twz);
+        k_fft_z_r2c<T, LT, NC, NT, FULL><<<g, NT, smem_of<Cx<T>>(pz.L, NC), s>>>(rho, spec, n0, n1, n2, L0, L1, pz, twz);
     }
 };
 
@@ -826,7 +833,7 @@ struct LaunchC {
     }
 };
 
-template <typename TO>
+template <typename TO, bool NEG = true>
 struct LaunchRfftNeg {
     const double* in;
     Cx<TO>* out;
@@ -838,12 +845,12 @@ struct LaunchRfftNeg {
     template <int LT>
     void run() {
         constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
-        k_rfft_lines_neg<TO, LT, NC, NT><<<(unsigned)((nb + 2 * NC - 1) / (2 * NC)), NT, smem_of<double2>(pl.L, NC), s>>>(
-            in, out, nb, se, pl, tw);
+        k_rfft_lines_neg<TO, LT, NC, NT, NEG>
+            <<<(unsigned)((nb + 2 * NC - 1) / (2 * NC)), NT, smem_of<double2>(pl.L, NC), s>>>(in, out, nb, se, pl, tw);
     }
 };
 
-template <bool SELF, bool FLIP = false>
+template <bool SELF, bool FLIP = false, bool FULL = false>
 struct LaunchE {
     const double2* spec;
     double* phi;
@@ -857,7 +864,7 @@ struct LaunchE {
     void run() {
         constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
         dim3 g((unsigned)((n0 + 2 * NC - 1) / (2 * NC)), (unsigned)n1);
-        k_fft_z_c2r<double, SELF, LT, NC, NT, FLIP><<<g, NT, smem_of<double2>(pz.L, NC), s>>>(
+        k_fft_z_c2r<double, SELF, LT, NC, NT, FLIP, FULL><<<g, NT, smem_of<double2>(pz.L, NC), s>>>(
             spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling);
     }
 };
@@ -905,6 +912,12 @@ struct SetLimits {
         allow(k_fft_z_c2r<double, false, LT, NC, NT, true>);
         allow(k_rfft_lines_neg<double, LT, NC, NT>);
         allow(k_rfft_lines_neg<float, LT, NC, NT>);
+        allow(k_rfft_lines_neg<double, LT, NC, NT, false>);
+        allow(k_rfft_lines_neg<float, LT, NC, NT, false>);
+        allow(k_fft_z_r2c<double, LT, NC, NT, true>);
+        allow(k_fft_z_r2c<float, LT, NC, NT, true>);
+        allow(k_fft_z_c2r<double, true, LT, NC, NT, false, true>);
+        allow(k_fft_z_c2r<double, false, LT, NC, NT, false, true>);
     }
 };
 
@@ -1112,9 +1125,14 @@ size_t fft_smem_bytes(const DevBunch& b) {
 }
 
 // twiddles exp(-2 pi i e / L) from long double arithmetic, rounded once
+// Axis d's transform length: the doubled grid, except z with periodic z.
+static inline int axis_length(const DevBunch& b, int d) {
+    return (d == 2 && b.periodic_z) ? b.bc.n[2] : 2 * b.bc.n[d];
+}
+
 void upload_twiddles(DevBunch& b, cudaStream_t s) {
     for (int d = 0; d < 3; ++d) {
-        const int L = 2 * b.bc.n[d];
+        const int L = axis_length(b, d);
         std::vector<double2> td(L);
         std::vector<float2> tf(L);
         for (int e = 0; e < L; ++e) {
@@ -1134,7 +1152,7 @@ void upload_twiddles(DevBunch& b, cudaStream_t s) {
 }
 
 static inline const void* tw_for(const DevBunch& b, int d) {
-    const int L = 2 * b.bc.n[d];
+    const int L = axis_length(b, d);
     const double2* dptr = reinterpret_cast<const double2*>(b.tw[d]);
     return b.precision == 0 ? (const void*)dptr : (const void*)(dptr + L);
 }
@@ -1183,6 +1201,25 @@ void launch_green_transform_image(const DevBunch& b, cudaStream_t s) {
         with_length(2 * n2, LaunchRfftNeg<float>{ga, (float2*)b.ghat_img, (int)(g0 * g1), g0 * g1, p2, tw2, s});
 }
 
+// Periodic z (FFTPoissonSolver with bcz, :130-155, :661-662): G on its first
+// n2 z planes (the unshifted G of b.gline, not mirrored in z), cosine
+// transforms along y and x, then a full real transform of length n2 along z
+// into b.ghat_img (complex T).
+void launch_green_transform_periodic(const DevBunch& b, cudaStream_t s) {
+    const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    const long long g0 = n0 + 1, g1 = n1 + 1;
+    const FftPlan p0 = make_plan(2 * n0), p1 = make_plan(2 * n1), pz = make_plan(n2);
+    const double2* tw0 = reinterpret_cast<const double2*>(b.tw[0]);
+    const double2* tw1 = reinterpret_cast<const double2*>(b.tw[1]);
+    const double2* tw2 = reinterpret_cast<const double2*>(b.tw[2]);
+    with_length(2 * n1, LaunchDct<double>{b.gline, b.gtmp, (int)g1, (int)g0, n2, 1, g0 * g1, g0, p1, tw1, s});
+    with_length(2 * n0, LaunchDct<double>{b.gtmp, b.gline, (int)g0, (int)g1, n2, g0, g0 * g1, 1, p0, tw0, s});
+    if (b.precision == 0)
+        with_length(n2, LaunchRfftNeg<double, false>{b.gline, (double2*)b.ghat_img, (int)(g0 * g1), g0 * g1, pz, tw2, s});
+    else
+        with_length(n2, LaunchRfftNeg<float, false>{b.gline, (float2*)b.ghat_img, (int)(g0 * g1), g0 * g1, pz, tw2, s});
+}
+
 // T is the type of the forward half (A, B and the forward x transform of C);
 // the inverse half (C's inverse, D, E) is FP64 in both forms.  With energy
 // bins the plain form keeps the forward spectrum in b.spec_fwd, so the bin's
@@ -1193,7 +1230,8 @@ template <typename T>
 static void convolution_t(const DevBunch& b, int mode, int parts, cudaStream_t s) {
     using C = Cx<T>;
     const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
-    const int L0 = 2 * n0, L1 = 2 * n1, L2 = 2 * n2;
+    const int L0 = 2 * n0, L1 = 2 * n1, L2 = axis_length(b, 2);
+    const int K = L2 / 2;  // half-spectrum planes 0..K along z
     const FftPlan px = make_plan(L0), py = make_plan(L1), pz = make_plan(L2);
     const C* twx = reinterpret_cast<const C*>(tw_for(b, 0));
     const C* twy = reinterpret_cast<const C*>(tw_for(b, 1));
@@ -1208,8 +1246,22 @@ static void convolution_t(const DevBunch& b, int mode, int parts, cudaStream_t s
     normFact /= L1;
     normFact /= L2;
     if (parts & kConvForwardPart) {
-        with_length(L2, LaunchA<T>{(const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz, s});
-        with_length(L1, LaunchY<T, false>{fwd, n0, L0, n1, L1, n2 + 1, py, twy, s});
+        if (b.periodic_z)
+            with_length(L2, LaunchA<T, true>{(const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz, s});
+        else
+            with_length(L2, LaunchA<T>{(const T*)b.rho, fwd, n0, n1, n2, L0, L1, pz, twz, s});
+        with_length(L1, LaunchY<T, false>{fwd, n0, L0, n1, L1, K + 1, py, twy, s});
+    }
+    if ((parts & kConvRestPart) && b.periodic_z) {
+        with_length(L0, LaunchC<T, true>{fwd, inv, (const T*)b.ghat_img, n0, n1, L1, (K + 1) * L1, px, twx, twx_d, s});
+        with_length(L1, LaunchY<double, true>{inv, n0, L0, L1, n1, K + 1, py, twy_d, s});
+        if (mode == kConvSelfField)
+            with_length(L2, LaunchE<true, false, true>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact,
+                                                       b.bc.coupling, s});
+        else
+            with_length(L2, LaunchE<false, false, true>{inv, b.phi, n0, n1, n2, L0, L1, pz, twz_d, b.st, normFact,
+                                                        b.bc.coupling, s});
+        return;
     }
     if (parts & kConvRestPart) {
         with_length(L0, LaunchC<T>{fwd, inv, (const T*)b.ghat, n0, n1, L1, (n2 + 1) * L1, px, twx, twx_d, s});

@@ -64,6 +64,8 @@ struct DevBunch {
     double* gtmp_img;                // 2 x (n0+2)(n1+2)(n2+2): antiderivative planes, z and z - n2 hz
     double* gimg;                    // 2 x (n0+1)(n1+1)(2 n2): the shifted G and its cosine transforms
     void* ghat_img;                  // (n2+1)(n1+1)(n0+1) complex T: minus the spectrum of the shifted G
+                                     // (periodic z: the spectrum of the periodic G)
+    int periodic_z;                  // BCFFTZ=PERIODIC: z not doubled, cyclic convolution along z
 };
 
 struct FftPlan {
@@ -193,6 +195,8 @@ enum : int { kConvForwardPart = 1, kConvRestPart = 2, kConvImagePart = 4 };
 void launch_convolution_part(const DevBunch& b, int mode, int parts, cudaStream_t s);
 // spectrum of the shifted G (b.gimg) into b.ghat_img
 void launch_green_transform_image(const DevBunch& b, cudaStream_t s);
+// periodic z: spectrum of G on its first n2 z planes (b.gline) into b.ghat_img
+void launch_green_transform_periodic(const DevBunch& b, cudaStream_t s);
 size_t fft_smem_bytes(const DevBunch& b);
 void upload_twiddles(DevBunch& b, cudaStream_t s);
 void fft_set_smem_limits();

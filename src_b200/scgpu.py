@@ -105,6 +105,7 @@ def lib():
                                                        C.c_double, C.c_double, _dp, _dp, _dp]
         L.scgpu_set_energy_bins.argtypes = [C.c_void_p, _ip, C.c_int, C.c_int]
         L.scgpu_get_bin_gammas.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong)]
+        L.scgpu_set_periodic_z.argtypes = [C.c_void_p, C.c_int]
         L.scgpu_stat_row.argtypes = [C.c_void_p, _dp]
         L.scgpu_stat_column_name.argtypes = [C.c_int]
         L.scgpu_stat_column_name.restype = C.c_char_p
@@ -128,6 +129,7 @@ EXPORTED = [
     "scgpu_compute_potential_image_device", "scgpu_compute_self_fields_binned", "scgpu_set_energy_bins",
     "scgpu_get_bin_gammas", "scgpu_stat_row", "scgpu_stat_column_name", "scgpu_sdds_write_header",
     "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
+    "scgpu_set_periodic_z",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
@@ -190,6 +192,10 @@ class Context:
         assert r.shape == (self.nr[2], self.nr[1], self.nr[0])
         self._check(lib().scgpu_compute_potential(self.h, _p(r), (C.c_double * 3)(*hr)), "compute_potential")
         return r
+
+    # ---- FIELDSOLVER BCFFTZ=PERIODIC
+    def set_periodic_z(self, periodic=True):
+        self._check(lib().scgpu_set_periodic_z(self.h, 1 if periodic else 0), "set_periodic_z")
 
     # ---- PoissonSolver::computePotential(rho, hr, zshift): image charge
     def compute_potential_image(self, rho, hr, zshift):

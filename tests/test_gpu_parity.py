@@ -344,3 +344,36 @@ def test_stat_row_vs_oracle(oracle, gpu, tmp_path):
     assert v["Bz_ref"] == 0.2 and v["dt"] == 1e-12 * 1e9 and v["partsOutside"] == 0
     text = (tmp_path / "run.stat").read_text().splitlines()
     assert float(text[-1].split("\t")[0]) == float(f"{v['t']:.15e}")
+
+
+@pytest.mark.parametrize("nr", [(16, 16, 16), (16, 24, 32), (40, 20, 60), (64, 64, 64), (32, 32, 128)])
+def test_compute_potential_periodic_z_vs_oracle(oracle, gpu, nr):
+    rng = np.random.default_rng(sum(nr) + 1)
+    rho = np.abs(rng.standard_normal((nr[2], nr[1], nr[0])))
+    hr = (2.7e-4, 2.9e-4, 5.1e-4)
+    with gpu.Context(nr) as c:
+        c.set_periodic_z(True)
+        phi = c.compute_potential(rho, hr)
+        c.set_periodic_z(False)
+        phi_open = c.compute_potential(rho, hr)
+    assert rel(phi, oracle.compute_potential_periodic_z(rho, hr)) < FIELD_TOL
+    assert rel(phi_open, oracle.compute_potential(rho, hr)) < FIELD_TOL
+
+
+def test_periodic_z_mixed_and_limits(oracle, gpu):
+    nr = (32, 32, 32)
+    rho = np.abs(np.random.default_rng(5).standard_normal((32, 32, 32)))
+    hr = (2.7e-4, 2.9e-4, 5.1e-4)
+    with gpu.Context(nr, precision=gpu.MIXED) as c:
+        c.set_periodic_z(True)
+        phi = c.compute_potential(rho, hr)
+        R, P = gaussian_bunch(1000)
+        c.upload(R, P, 1e-12, -1e-12, oracle.electron_mass_ev())
+        with pytest.raises(gpu.ScgpuError) as e:
+            c.track(1)
+        assert e.value.code == -8
+    assert rel(phi, oracle.compute_potential_periodic_z(rho, hr)) < 1e-5
+    with gpu.Context((16, 16, 15)) as c:
+        with pytest.raises(gpu.ScgpuError) as e:
+            c.set_periodic_z(True)
+        assert e.value.code == -8

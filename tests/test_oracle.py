@@ -314,3 +314,17 @@ def test_binned_step_golden(oracle):
     assert rel(R, g["R"]) < 1e-14 and rel(P, g["P"]) < 1e-14
     assert rel(dbg["Ef"], g["Ef"]) < 1e-13 and rel(dbg["Bf"], g["Bf"]) < 1e-13
     assert tr.Q == float(g["Q"])
+
+
+def test_periodic_z_solve_is_cyclic_along_z(oracle):
+    """FFTPoissonSolver with bcz = PERIODIC (FFTPoissonSolver.cpp:130-155, :661-662):
+    doubled in x, y only; G = the unshifted G on z offsets [0, nz), not mirrored
+    in z (including the G[0,0,0] <- G[0,0,1] rule); cyclic convolution along z."""
+    nr, hr = (16, 12, 20), (1.0e-4, 1.3e-4, 0.8e-4)
+    rho = np.random.default_rng(1).standard_normal((nr[2], nr[1], nr[0]))
+    G = oracle.igf_periodic_z(nr, hr)
+    np.testing.assert_array_equal(G, oracle.igf(nr, hr)[:nr[2]])
+    r2 = np.zeros(G.shape)
+    r2[:, :nr[1], :nr[0]] = rho
+    conv = np.real(np.fft.ifftn(np.fft.fftn(r2) * np.fft.fftn(G)))[:, :nr[1], :nr[0]]
+    assert rel(oracle.compute_potential_periodic_z(rho, hr), conv) < 1e-13
