@@ -17,6 +17,9 @@
  *   scgpu_compute_potential, scgpu_compute_potential_device
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr)
  *       (src/Solvers/PoissonSolver.h:28; FFTPoissonSolver.cpp:337-382)
+ *   scgpu_set_exchange
+ *       the MPI reductions of a distributed bunch (get_bounds, calcMoments,
+ *       the scatter into the distributed rho field) as an exchange callback
  *   scgpu_set_periodic_z
  *       the bcz argument of FFTPoissonSolver (FieldSolver BCFFTZ, src/Structure/FieldSolver.cpp:431, :486)
  *   scgpu_compute_potential_image, scgpu_compute_potential_image_device
@@ -75,6 +78,7 @@ extern "C" {
 #define SCGPU_ERR_CUDA (-6)         /* CUDA runtime error */
 #define SCGPU_ERR_STATE (-7)        /* call order (e.g. tracking without a bunch) */
 #define SCGPU_ERR_UNSUPPORTED (-8)  /* mesh size or option this build does not support */
+#define SCGPU_ERR_EXCHANGE (-9)     /* the exchange callback of a sharded bunch failed */
 
 #define SCGPU_PLAIN_FP64 0  /* FP64 throughout */
 #define SCGPU_MIXED 1       /* FP32 grid work, FP64 particles / Green's function / boost */
@@ -159,6 +163,30 @@ int scgpu_compute_potential_device(scgpu_ctx* ctx, double* rho_inout_device, con
  * Q *= dt ... Q /= dt round trip. */
 int scgpu_compute_self_fields(scgpu_ctx* ctx, long long n, const double* R, const double* P, double* q_macro, double dT,
                               double* Ef, double* Bf);
+
+/* Particle sharding over ranks (one context per GPU, each holding a shard of
+ * one bunch; the reference distributes particles over MPI ranks and reduces
+ * bounds, moments and the charge density across them: PartBunchBase.hpp:
+ * 1178-1219 get_bounds, :2185-2259 calcMoments, IPPL's scatter into a
+ * distributed field).  At fixed points of a step the library hands a
+ * device buffer of this rank's partial results to `fn`, which combines it
+ * over the ranks in place, on `cuda_stream` (e.g. ncclAllReduce), and
+ * returns 0:
+ *   SCGPU_EXCHANGE_MIN_F64  count doubles, elementwise minimum (bounds);
+ *   SCGPU_EXCHANGE_SUM_U64  count 64-bit unsigned integers, sum modulo 2^64
+ *                           (the deposit's fixed-point node sums and the
+ *                           momentum / moment sums as 32-bit chunks).
+ * Every combined value is exact, so the union of the shards evolves
+ * bitwise as the whole bunch on one GPU.  total_particles is the bunch's
+ * particle count over all ranks.  Call before scgpu_bunch_upload (the upload
+ * combines the momentum sums); fn = NULL returns to a single-GPU bunch.
+ * capturable = 1 when fn only enqueues stream work, so the step can be a
+ * CUDA graph; otherwise steps are enqueued directly.  Energy bins, the
+ * phase profile and scgpu_compute_self_fields are single-GPU only. */
+#define SCGPU_EXCHANGE_SUM_U64 0
+#define SCGPU_EXCHANGE_MIN_F64 1
+typedef int (*scgpu_exchange_fn)(void* device_buffer, long long count, int op, void* cuda_stream, void* user);
+int scgpu_set_exchange(scgpu_ctx* ctx, scgpu_exchange_fn fn, void* user, long long total_particles, int capturable);
 
 /* FIELDSOLVER BCFFTZ=PERIODIC (FFTPoissonSolver(..., bcz="PERIODIC"),
  * src/Solvers/FFTPoissonSolver.cpp:60, :130-155, :189-190, :661-662): the

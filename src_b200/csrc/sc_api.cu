@@ -218,11 +218,43 @@ int ensure_particles(scgpu_ctx* c, long long n) {
     if (n != c->n) drop_graphs(c);
     c->n = n;
     b.bc.N = n;
+    b.bc.sharded = c->xfn ? 1 : 0;
+    b.bc.Ntot = c->xfn ? c->ntot : n;
     long long g = (n + 255) / 256;
     if (g < 1) g = 1;
     if (g > 148 * 8) g = 148 * 8;
     b.red_blocks = (int)g;
     return SCGPU_OK;
+}
+
+// One exchange of a sharded bunch; the first failure is kept for the caller.
+void exchange(scgpu_ctx* c, void* buf, long long count, int op, cudaStream_t s) {
+    const int rc = c->xfn(buf, count, op, (void*)s, c->xuser);
+    if (rc != 0 && c->xerr == 0) c->xerr = rc;
+}
+
+int exchange_status(scgpu_ctx* c) {
+    if (!c->xerr) return SCGPU_OK;
+    const int rc = c->xerr;
+    c->xerr = 0;
+    return fail(c, SCGPU_ERR_EXCHANGE, "exchange callback returned " + std::to_string(rc));
+}
+
+// The momentum sums (and, with init_frame, the beam frame) of the whole
+// bunch: reduce_state, then for a shard the exchange of the limbs.
+void enqueue_psum(scgpu_ctx* c, bool init_frame, cudaStream_t s) {
+    launch_reduce_state(c->b, init_frame, s);
+    if (!c->xfn) return;
+    exchange(c, c->b.st->xlimbs, 3 * 4, SCGPU_EXCHANGE_SUM_U64, s);
+    launch_finish_psum(c->b, init_frame, false, s);
+}
+
+// The 27 moment sums and the sum of gamma of the whole bunch.
+void enqueue_stats(scgpu_ctx* c, cudaStream_t s) {
+    launch_reduce_stats(c->b, s);
+    if (!c->xfn) return;
+    exchange(c, c->b.st->xlimbs, 28 * 4, SCGPU_EXCHANGE_SUM_U64, s);
+    launch_finish_stats(c->b, s);
 }
 
 // Puts the particle arrays in cell order: counting sort (keys, ranks, cell
@@ -245,17 +277,24 @@ void enqueue_reorder(scgpu_ctx* c, cudaStream_t s) {
 // The branches write disjoint StepState fields.
 void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
     DevBunch& b = c->b;
+    const bool shard = c->xfn != nullptr;
     cudaEventRecord(c->ev_start, s);
     cudaStreamWaitEvent(c->ref, c->ev_start, 0);
     launch_advance_reference(b, c->ref);
     cudaEventRecord(c->ev_ref, c->ref);
     launch_drift_to_beam(b, true, s);
+    if (shard) {  // the bounds of all shards, then the mesh
+        exchange(c, b.st->bnd6, 6, SCGPU_EXCHANGE_MIN_F64, s);
+        launch_finish_mesh(b, s);
+    }
     cudaEventRecord(c->ev_fork, s);
     cudaStreamWaitEvent(c->side, c->ev_fork, 0);
     launch_igf(b, nullptr, c->side);
     launch_green_transform(b, c->side);
     cudaEventRecord(c->ev_join, c->side);
     launch_deposit(b, s);
+    if (shard)  // the charge of all shards: exact integer node sums
+        exchange(c, b.nacc, 2 * mesh_cells(b), SCGPU_EXCHANGE_SUM_U64, s);
     launch_assemble_rho(b, s);
     if (reorder) enqueue_reorder(c, s);
     launch_convolution_part(b, kConvSelfField, kConvForwardPart, s);
@@ -263,7 +302,14 @@ void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
     launch_convolution_part(b, kConvSelfField, kConvRestPart, s);
     launch_grad(b, s);
     cudaStreamWaitEvent(s, c->ev_ref, 0);
-    launch_gather_kick_push(b, stats, s);
+    if (!shard) {
+        launch_gather_kick_push(b, stats, s);
+        return;
+    }
+    launch_gather_kick_push(b, false, s);
+    exchange(c, b.st->xlimbs, 3 * 4, SCGPU_EXCHANGE_SUM_U64, s);
+    launch_finish_psum(b, true, true, s);
+    if (stats) enqueue_stats(c, s);
 }
 
 // The step with energy bins: the same branches, the self fields from the
@@ -604,6 +650,24 @@ static int compute_potential_image_impl(scgpu_ctx* c, double* rho, const double 
     return SCGPU_OK;
 }
 
+int scgpu_set_exchange(scgpu_ctx* c, scgpu_exchange_fn fn, void* user, long long total_particles, int capturable) {
+    if (!c) return SCGPU_ERR_ARG;
+    if (fn && total_particles <= 0) return fail(c, SCGPU_ERR_ARG, "total_particles must be positive");
+    if (fn && c->b.nbins > 0) return fail(c, SCGPU_ERR_UNSUPPORTED, "energy bins of a sharded bunch");
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->xfn = fn;
+    c->xuser = fn ? user : nullptr;
+    c->ntot = fn ? total_particles : 0;
+    c->xcapturable = fn && capturable;
+    c->xerr = 0;
+    c->b.bc.sharded = fn ? 1 : 0;
+    c->b.bc.Ntot = fn ? total_particles : c->n;
+    c->have_bunch = false;  // the bunch is uploaded again as a shard (or whole)
+    return SCGPU_OK;
+}
+
 // BCFFTZ=PERIODIC (FieldSolver.cpp:431, :486; FFTPoissonSolver.cpp:60,
 // :130-155, :189-190, :661-662): the solves of this context use a grid
 // doubled in x and y only and a cyclic convolution along z.
@@ -649,6 +713,7 @@ int scgpu_compute_potential_device(scgpu_ctx* c, double* rho, const double hr[3]
 int scgpu_compute_self_fields(scgpu_ctx* c, long long n, const double* R, const double* P, double* q_macro, double dT,
                               double* Ef, double* Bf) {
     if (!c || !R || !P || !q_macro || !Ef || !Bf) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (c->xfn) return fail(c, SCGPU_ERR_UNSUPPORTED, "self fields of a sharded bunch (use scgpu_track)");
     if (!(dT > 0.0)) return fail(c, SCGPU_ERR_ARG, "dT must be positive");
     CK(cudaSetDevice(c->device));
     int rc = ensure_particles(c, n);
@@ -714,6 +779,7 @@ static int set_bins_impl(scgpu_ctx* c, const int* bins, int nbins, int last_emit
     cudaStream_t s = c->stream;
     const int nactive = last_emitted < nbins ? last_emitted : nbins;
     if (nbins > 0 && b.periodic_z) return fail(c, SCGPU_ERR_UNSUPPORTED, "energy bins with periodic z");
+    if (nbins > 0 && c->xfn) return fail(c, SCGPU_ERR_UNSUPPORTED, "energy bins of a sharded bunch");
     if (nbins != b.nbins || nactive != b.nactive) drop_graphs(c);
     if (nbins == 0) {
         b.nbins = b.nactive = 0;
@@ -766,6 +832,7 @@ int scgpu_compute_self_fields_binned(scgpu_ctx* c, long long n, const double* R,
     if (rc) return rc;
     if (nbins == 0) return fail(c, SCGPU_ERR_ARG, "nbins must be positive");
     if (c->b.periodic_z) return fail(c, SCGPU_ERR_UNSUPPORTED, "energy bins with periodic z");
+    if (c->xfn) return fail(c, SCGPU_ERR_UNSUPPORTED, "energy bins of a sharded bunch");
     CK(cudaSetDevice(c->device));
     if ((rc = ensure_particles(c, n))) return rc;
     if ((rc = ensure_bins(c, nbins))) return rc;
@@ -863,9 +930,10 @@ int scgpu_bunch_upload(scgpu_ctx* c, long long n, const double* R, const double*
         launch_iota(b.id, n, s);
         c->steps_done = 0;
     }
-    launch_reduce_state(b, true, s);
+    enqueue_psum(c, true, s);
     CK(cudaGetLastError());
-    rc = check_device_err(c);
+    rc = exchange_status(c);
+    if (rc == SCGPU_OK) rc = check_device_err(c);
     c->have_bunch = (rc == SCGPU_OK);
     return rc;
 }
@@ -896,7 +964,7 @@ int scgpu_track(scgpu_ctx* c, int nsteps, double* stats) {
     CK(cudaEventRecord(c->ev_t0, s));
     for (int k = 0; k < nsteps; ++k) {
         const bool reorder = c->reorder_every > 0 && (c->steps_done % c->reorder_every) == 0;
-        if (c->use_graphs) {
+        if (c->use_graphs && (!c->xfn || c->xcapturable)) {
             cudaGraphExec_t& gx = (c->b.nbins > 0 ? c->graphs_bins : c->graphs)[want ? 1 : 0][reorder ? 1 : 0];
             if (!gx) {
                 int rc = build_graph(c, want, reorder, &gx);
@@ -913,7 +981,8 @@ int scgpu_track(scgpu_ctx* c, int nsteps, double* stats) {
     }
     CK(cudaEventRecord(c->ev_t1, s));
     CK(cudaGetLastError());
-    int rc = check_device_err(c);
+    int rc = exchange_status(c);
+    if (rc == SCGPU_OK) rc = check_device_err(c);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev_t0, c->ev_t1);
     c->last_ms = ms;
@@ -944,11 +1013,13 @@ int scgpu_beam_parameters(scgpu_ctx* c, scgpu_beam_params* out) {
     if (!c || !out) return fail(c, SCGPU_ERR_ARG, "null argument");
     if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
     CK(cudaSetDevice(c->device));
-    launch_reduce_stats(c->b, c->stream);
+    enqueue_stats(c, c->stream);
     double rec[SCGPU_NSTATS];
     CK(cudaMemcpyAsync(rec, c->b.st->moments, sizeof(rec), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    return scgpu_beam_parameters_from_stats(rec, c->n, out);
+    int rc = exchange_status(c);
+    if (rc) return rc;
+    return scgpu_beam_parameters_from_stats(rec, c->b.bc.Ntot, out);
 }
 
 // One row of DataSink::doWriteStatData (DataSink.cpp:281-449) for the resident
@@ -960,9 +1031,10 @@ int scgpu_stat_row(scgpu_ctx* c, double* row) {
     CK(cudaSetDevice(c->device));
     DevBunch& b = c->b;
     cudaStream_t s = c->stream;
-    launch_reduce_stats(b, s);
+    enqueue_stats(c, s);
     double* scratch = b.Ef;  // 3 N doubles >= 12
     launch_bounds(b, scratch, s);
+    if (c->xfn) exchange(c, scratch, 6, SCGPU_EXCHANGE_MIN_F64, s);
     launch_find_id(b, 0u, scratch + 6, s);
     double rec[SCGPU_NSTATS], ext[12];
     StepState h;
@@ -971,7 +1043,9 @@ int scgpu_stat_row(scgpu_ctx* c, double* row) {
     CK(cudaMemcpyAsync(&h, b.st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
-    const long long n = c->n;
+    int rc = exchange_status(c);
+    if (rc) return rc;
+    const long long n = b.bc.Ntot;
     const double N = (double)n;
     scgpu_beam_params bp;
     std::memset(&bp, 0, sizeof bp);
@@ -999,7 +1073,7 @@ int scgpu_stat_row(scgpu_ctx* c, double* row) {
     for (int d = 0; d < 3; ++d) row[k++] = bp.rmean[d];
     for (int d = 0; d < 3; ++d) row[k++] = h.ref_R[d];
     for (int d = 0; d < 3; ++d) row[k++] = h.ref_P[d];
-    for (int d = 0; d < 3; ++d) row[k++] = ext[3 + d];  // get_maxExtent = rmax
+    for (int d = 0; d < 3; ++d) row[k++] = -ext[3 + d];  // get_maxExtent = rmax
     for (int d = 0; d < 3; ++d) row[k++] = bp.rprms[d];
     row[k++] = rec[mom_idx(0, 5)] / N;  // Dx
     row[k++] = rec[mom_idx(1, 5)] / N;  // DDx
@@ -1082,6 +1156,7 @@ int scgpu_profile_track(scgpu_ctx* c, int nsteps, double* phase_ms) {
     if (!c || nsteps < 0 || !phase_ms) return fail(c, SCGPU_ERR_ARG, "bad argument");
     if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
     if (c->b.nbins > 0) return fail(c, SCGPU_ERR_UNSUPPORTED, "phase profile of a step with energy bins");
+    if (c->xfn) return fail(c, SCGPU_ERR_UNSUPPORTED, "phase profile of a sharded bunch");
     CK(cudaSetDevice(c->device));
     DevBunch& b = c->b;
     cudaStream_t s = c->stream;
@@ -1134,6 +1209,7 @@ int scgpu_profile_track(scgpu_ctx* c, int nsteps, double* phase_ms) {
 int scgpu_kernels_per_step(scgpu_ctx* c) {
     if (!c) return SCGPU_ERR_ARG;
     if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
+    if (c->xfn && !c->xcapturable) return fail(c, SCGPU_ERR_UNSUPPORTED, "step of a shard with a host exchange");
     CK(cudaSetDevice(c->device));
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));

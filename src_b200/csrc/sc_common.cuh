@@ -88,12 +88,20 @@ struct StepState {
     long long bin_count;  // particles in the bin (per-bin copies)
     int binned;         // the energy-bin loop is on: Q is restored after the scatter (ParallelTTracker.cpp:576)
     int pad_;
+    // sharded bunch: this rank's partial results, combined over the ranks
+    // between kernels (bounds by min; exact sums as 32-bit chunks of the
+    // 128-bit fixed point, summed as 64-bit integers)
+    double bnd6[6];                 // min x, y, z and -max x, y, z
+    unsigned long long xlimbs[28 * 4];
 };
 
 struct BunchConst {
     int n[3];       // mesh cells per axis (MX, MY, MT)
     int key_bits;
-    long long N;    // particles
+    long long N;    // particles (of this rank when the bunch is sharded)
+    long long Ntot; // particles of the whole bunch (the N of the means)
+    int sharded;    // 1: bounds and particle sums are combined over ranks between kernels
+    int pad_;
     double dT;
     double mass;    // eV
     double charge;  // e
@@ -447,7 +455,7 @@ SC_HD_COLD bool derive_mesh(StepState& s, const BunchConst& bc) {
     bool ok = s.hr[0] * s.hr[1] * s.hr[2] > 0;
     for (int i = 0; i < 3; ++i) s.origin[i] = rmin[i] - s.hr[i] / 2.0;
     for (int i = 0; i < 3; ++i) s.rhr[i] = 1.0 / s.hr[i];
-    double gz = s.psum[2] / (double)bc.N;
+    double gz = s.psum[2] / (double)bc.Ntot;
     gz *= gz;
     gz = sqrt(gz + 1.0);
     s.gammaz = gz;
@@ -465,7 +473,7 @@ SC_HD_COLD bool derive_mesh(StepState& s, const BunchConst& bc) {
 // from the momentum sum and the path length.  Returns false for an
 // anti-parallel mean momentum.
 SC_HD_COLD bool derive_beam_frame(StepState& s, const BunchConst& bc) {
-    const double N = (double)bc.N;
+    const double N = (double)bc.Ntot;
     double pmean[3] = {s.psum[0] / N, s.psum[1] / N, s.psum[2] / N};
     double zhat[3] = {0.0, 0.0, 1.0}, q[4];
     bool ok = get_quaternion(pmean, zhat, q);

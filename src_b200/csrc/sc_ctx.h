@@ -39,6 +39,12 @@ struct scgpu_ctx {
     void* ghat_img_alt = nullptr; // functions while the main stream convolves bin k
     cudaEvent_t ev_bin[sc::kMaxBins] = {};
     cudaEvent_t ev_used[sc::kMaxBins] = {};
+    // sharded bunch (scgpu_set_exchange): this context holds one rank's shard
+    scgpu_exchange_fn xfn = nullptr;
+    void* xuser = nullptr;
+    long long ntot = 0;        // particles over all ranks
+    bool xcapturable = false;
+    int xerr = 0;              // first failing exchange of the last enqueue
 };
 
 namespace sc {

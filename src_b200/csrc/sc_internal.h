@@ -100,7 +100,11 @@ void launch_soa_to_aos_by_id(const double* a, const double* b, const double* c, 
                              long long n, cudaStream_t s);
 void launch_f64_to_f32(const double* in, float* out, long long n, cudaStream_t s);
 void launch_f32_to_f64(const float* in, double* out, long long n, cudaStream_t s);
-// statistics: bounds of the positions (out6 = min x, y, z, max x, y, z) and one particle's state
+// sharded bunch: the reduction tails after the ranks' partials were combined
+void launch_finish_mesh(const DevBunch& b, cudaStream_t s);
+void launch_finish_psum(const DevBunch& b, bool frame, bool advance, cudaStream_t s);
+void launch_finish_stats(const DevBunch& b, cudaStream_t s);
+// statistics: bounds of the positions (out6 = min x, y, z, -max x, y, z) and one particle's state
 void launch_bounds(const DevBunch& b, double* out6, cudaStream_t s);
 void launch_find_id(const DevBunch& b, uint32_t target, double* out6, cudaStream_t s);
 

@@ -94,7 +94,7 @@ __device__ __forceinline__ void block_sum_ex(i128 (&v)[NV], i128* __restrict__ p
 // rows, so all loads are in flight at once instead of one warp walking each
 // column; the integer sums are exact, so the order does not matter.
 template <int NV>
-__device__ __forceinline__ void final_sum_ex(const i128* partials, int nb, double* out) {
+__device__ __forceinline__ void final_sum_ex(const i128* partials, int nb, double* out, i128* exact = nullptr) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if constexpr (NV <= 8) {
         i128 s[NV];
@@ -118,6 +118,7 @@ __device__ __forceinline__ void final_sum_ex(const i128* partials, int nb, doubl
             i128 t = 0;
             for (int w = 0; w < kWarps; ++w) t += sm[threadIdx.x][w];
             out[threadIdx.x] = ex_to_double(t);
+            if (exact) exact[threadIdx.x] = t;
         }
         return;
     }
@@ -130,7 +131,10 @@ __device__ __forceinline__ void final_sum_ex(const i128* partials, int nb, doubl
         }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) s += ex_shfl_down(s, off);
-        if (lane == 0) out[k] = ex_to_double(s);
+        if (lane == 0) {
+            out[k] = ex_to_double(s);
+            if (exact) exact[k] = s;
+        }
     }
 }
 
@@ -158,6 +162,20 @@ __device__ __forceinline__ void final_min(const double* partials, int nb, double
         for (int w = 0; w < kWarps; ++w) t = fmin(t, sm[threadIdx.x][w]);
         out[threadIdx.x] = t;
     }
+}
+
+// A 128-bit exact sum as four 32-bit chunks of its two's complement, each
+// in a 64-bit word: summing the words of several ranks as integers and
+// recombining gives the exact total (mod 2^128, which holds it).
+__device__ __forceinline__ void put_limbs(unsigned long long* dst, i128 v) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dst[j] = (unsigned long long)(unsigned)((u128)v >> (32 * j));
+}
+__device__ __forceinline__ i128 get_limbs(const unsigned long long* src) {
+    u128 t = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) t += (u128)src[j] << (32 * j);
+    return (i128)t;
 }
 
 // moments in OPAL's order (x, px, y, py, z, pz), PartBunchBase.hpp:2185-2259,
@@ -204,8 +222,14 @@ __device__ __forceinline__ void reduce_state_body(const BunchConst& bc, const do
     block_sum_ex<NV>(v, xpart, g.blk);
     if (!last_block(ticket, g.nblk)) return;
     __shared__ double tot[NV];
-    final_sum_ex<NV>(xpart, g.nblk, tot);
+    __shared__ i128 ex[NV];
+    final_sum_ex<NV>(xpart, g.nblk, tot, ex);
     __syncthreads();
+    if (bc.sharded) {  // this rank's exact sums; k_finish_* completes after the exchange
+        for (int k = threadIdx.x; k < NV; k += blockDim.x) put_limbs(st->xlimbs + 4 * k, ex[k]);
+        if (threadIdx.x == 0) *ticket = 0u;
+        return;
+    }
     if (threadIdx.x == 0) {
         if constexpr (STATS) {
             for (int k = 0; k < 27; ++k) st->moments[k] = tot[k];
@@ -229,6 +253,18 @@ __global__ void __launch_bounds__(kThreads) k_reduce_state(BunchConst bc, const 
 }
 
 // ------------------------------------------------------------ drift + frame
+// The mesh of this step from the bounds in s.bmin / s.bmax, and the charge
+// of the scatter: Q *= dt; scatter; Q /= dt  (PartBunch.cpp:493-495); the
+// energy-bin loop restores Q from its copy after every bin
+// (ParallelTTracker.cpp:570-576).
+__device__ __forceinline__ void finish_mesh(StepState& s, const BunchConst& bc) {
+    if (!derive_mesh(s, bc)) atomicOr(&s.err, kFlagMesh);
+    s.qdt = s.Q * bc.dT;
+    if (!s.binned) s.Q = s.qdt / bc.dT;
+    s.gen += 1u;
+    if (s.gen == 0u) s.gen = 1u;
+}
+
 template <bool DRIFT>
 __device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
                                            double* __restrict__ z, const double* __restrict__ px,
@@ -293,17 +329,15 @@ __device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restr
     __syncthreads();
     if (threadIdx.x == 0) {
         StepState& s = *st;
-        for (int k = 0; k < 3; ++k) {
-            s.bmin[k] = tot[k];
-            s.bmax[k] = -tot[3 + k];
+        if (bc.sharded) {  // this rank's bounds; k_finish_mesh completes after the exchange
+            for (int k = 0; k < 6; ++k) s.bnd6[k] = tot[k];
+        } else {
+            for (int k = 0; k < 3; ++k) {
+                s.bmin[k] = tot[k];
+                s.bmax[k] = -tot[3 + k];
+            }
+            finish_mesh(s, bc);
         }
-        if (!derive_mesh(s, bc)) atomicOr(&s.err, kFlagMesh);
-        // Q *= dt; scatter; Q /= dt  (PartBunch.cpp:493-495); the energy-bin
-        // loop restores Q from its copy after every bin (ParallelTTracker.cpp:570-576)
-        s.qdt = s.Q * bc.dT;
-        if (!s.binned) s.Q = s.qdt / bc.dT;
-        s.gen += 1u;
-        if (s.gen == 0u) s.gen = 1u;
         *ticket = 0u;
     }
 }
@@ -617,6 +651,38 @@ __global__ void __launch_bounds__(kThreads) k_igf_G(int n0, int n1, int n2, cons
     igf_G_body(n0, n1, n2, tmp, G, vb_grid());
 }
 
+// ------------------------------------------------------------ sharded bunch
+// Tails of the reductions once the ranks' partial results have been combined
+// (bounds by min, exact sums as integer limbs), on one thread.
+__global__ void k_finish_mesh(BunchConst bc, StepState* st) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    StepState& s = *st;
+    for (int k = 0; k < 3; ++k) {
+        s.bmin[k] = s.bnd6[k];
+        s.bmax[k] = -s.bnd6[3 + k];
+    }
+    finish_mesh(s, bc);
+}
+
+// psum from the combined limbs; frame: the beam frame of the next step
+// (derive_beam_frame); advance: the step counter of the gather.
+__global__ void k_finish_psum(BunchConst bc, StepState* st, int frame, int advance) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    StepState& s = *st;
+    for (int k = 0; k < 3; ++k) s.psum[k] = ex_to_double(get_limbs(s.xlimbs + 4 * k));
+    if (frame && !derive_beam_frame(s, bc)) atomicOr(&s.err, kFlagFrame);
+    if (advance) s.step += 1;
+}
+
+__global__ void k_finish_stats(StepState* st) {
+    if (blockIdx.x != 0 || threadIdx.x >= 28) return;
+    const double v = ex_to_double(get_limbs(st->xlimbs + 4 * threadIdx.x));
+    if (threadIdx.x < 27)
+        st->moments[threadIdx.x] = v;
+    else
+        st->gsum = v;
+}
+
 // ------------------------------------------------------------ image charge
 // Antiderivative planes of the image's Green's function
 // (shiftedIntGreensFunction, FFTPoissonSolver.cpp:556-596): set 0 at
@@ -817,7 +883,8 @@ __global__ void __launch_bounds__(kThreads) k_grad_acc(BunchConst bc, const Step
 }
 
 // get_bounds of the particle positions (PartBunchBase.hpp:1178-1219) for the
-// statistics: min of x, y, z and of -x, -y, -z into out[6] (exact, any order).
+// statistics: min of x, y, z and of -x, -y, -z into out[6] (exact, any order;
+// the shards of a bunch combine by min).
 __global__ void __launch_bounds__(kThreads) k_bounds(BunchConst bc, const double* __restrict__ x,
                                                      const double* __restrict__ y, const double* __restrict__ z,
                                                      double* partials, unsigned* ticket, double* __restrict__ out) {
@@ -848,10 +915,7 @@ __global__ void __launch_bounds__(kThreads) k_bounds(BunchConst bc, const double
     __shared__ double tot[6];
     final_min<6>(partials, gridDim.x, tot);
     __syncthreads();
-    if (threadIdx.x < 3) {
-        out[threadIdx.x] = tot[threadIdx.x];
-        out[3 + threadIdx.x] = -tot[3 + threadIdx.x];
-    }
+    if (threadIdx.x < 6) out[threadIdx.x] = tot[threadIdx.x];
     if (threadIdx.x == 0) *ticket = 0u;
 }
 
@@ -1059,15 +1123,20 @@ __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __rest
     block_sum_ex<3>(acc, xpart, g.blk);
     if (!last_block(ticket, g.nblk)) return;
     __shared__ double tot[3];
-    final_sum_ex<3>(xpart, g.nblk, tot);
+    __shared__ i128 ex[3];
+    final_sum_ex<3>(xpart, g.nblk, tot, ex);
     __syncthreads();
     if (threadIdx.x == 0) {
         StepState& s = *st;
-        s.psum[0] = tot[0];
-        s.psum[1] = tot[1];
-        s.psum[2] = tot[2];
-        if (!derive_beam_frame(s, bc)) atomicOr(&s.err, kFlagFrame);
-        s.step += 1;
+        if (bc.sharded) {  // this rank's momentum sums; k_finish_psum completes after the exchange
+            for (int k = 0; k < 3; ++k) put_limbs(s.xlimbs + 4 * k, ex[k]);
+        } else {
+            s.psum[0] = tot[0];
+            s.psum[1] = tot[1];
+            s.psum[2] = tot[2];
+            if (!derive_beam_frame(s, bc)) atomicOr(&s.err, kFlagFrame);
+            s.step += 1;
+        }
         *ticket = 0u;
     }
 }
@@ -1409,6 +1478,12 @@ void launch_gather_fields(const DevBunch& b, cudaStream_t s) {
     else
         k_gather_fields<float><<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, (const float*)b.E4, b.st, b.Ef, b.Bf);
 }
+
+void launch_finish_mesh(const DevBunch& b, cudaStream_t s) { k_finish_mesh<<<1, 32, 0, s>>>(b.bc, b.st); }
+void launch_finish_psum(const DevBunch& b, bool frame, bool advance, cudaStream_t s) {
+    k_finish_psum<<<1, 32, 0, s>>>(b.bc, b.st, frame ? 1 : 0, advance ? 1 : 0);
+}
+void launch_finish_stats(const DevBunch& b, cudaStream_t s) { k_finish_stats<<<1, 32, 0, s>>>(b.st); }
 
 constexpr int kBinGammaBlocks = 296;
 

@@ -24,9 +24,12 @@ FIELD_RHO, FIELD_PHI, FIELD_E = 0, 1, 2
 ERRORS = {
     -1: "SCGPU_ERR_ARG", -2: "SCGPU_ERR_OOM", -3: "SCGPU_ERR_MESH", -4: "SCGPU_ERR_GUARD",
     -5: "SCGPU_ERR_FRAME", -6: "SCGPU_ERR_CUDA", -7: "SCGPU_ERR_STATE", -8: "SCGPU_ERR_UNSUPPORTED",
+    -9: "SCGPU_ERR_EXCHANGE",
 }
 
 _dp = C.POINTER(C.c_double)
+# scgpu_exchange_fn(device_buffer, count, op, cuda_stream, user) -> status
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p)
 
 
 class SolverParams(C.Structure):
@@ -106,6 +109,7 @@ def lib():
         L.scgpu_set_energy_bins.argtypes = [C.c_void_p, _ip, C.c_int, C.c_int]
         L.scgpu_get_bin_gammas.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong)]
         L.scgpu_set_periodic_z.argtypes = [C.c_void_p, C.c_int]
+        L.scgpu_set_exchange.argtypes = [C.c_void_p, EXCHANGE_FN, C.c_void_p, C.c_longlong, C.c_int]
         L.scgpu_stat_row.argtypes = [C.c_void_p, _dp]
         L.scgpu_stat_column_name.argtypes = [C.c_int]
         L.scgpu_stat_column_name.restype = C.c_char_p
@@ -129,7 +133,7 @@ EXPORTED = [
     "scgpu_compute_potential_image_device", "scgpu_compute_self_fields_binned", "scgpu_set_energy_bins",
     "scgpu_get_bin_gammas", "scgpu_stat_row", "scgpu_stat_column_name", "scgpu_sdds_write_header",
     "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
-    "scgpu_set_periodic_z",
+    "scgpu_set_periodic_z", "scgpu_set_exchange",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
