@@ -59,4 +59,45 @@ __device__ __forceinline__ i128 ex_shfl_down(i128 v, int off) {
     return (i128)(((u128)hi << 64) | lo);
 }
 
+// ---------------------------------------------------------------- deposit
+// Exact sums of the scattered charges: each charge v (|v| <= |q dt|) becomes
+// the integer t = rint(v * 2^(52 - E)) with 2^E > 2 |q dt|, so |t| < 2^51;
+// the sums are integer additions, exact, so any order gives the same total,
+// which is rounded to a double once.  The rounding of t is at most 2^-52 of
+// one particle's charge.
+constexpr int kFxFrac = 52;
+
+__device__ __forceinline__ int fx_exponent(double qdt) { return qdt != 0.0 ? ilogb(qdt) + 2 : 0; }
+
+// correctly rounded double of the 128-bit accumulator (lo, hi), times unit
+__device__ __forceinline__ double acc_to_double(unsigned long long lo, unsigned long long hi, double unit) {
+    const long long shi = (long long)hi;
+    if (shi == ((long long)lo < 0 ? -1 : 0)) return __ll2double_rn((long long)lo) * unit;  // fits in 64 bits
+    const bool neg = shi < 0;
+    unsigned long long mlo = lo, mhi = hi;
+    if (neg) {
+        mlo = ~mlo + 1ull;
+        mhi = ~mhi + (mlo == 0 ? 1ull : 0ull);
+    }
+    const int lz = __clzll(mhi);
+    const unsigned long long top = lz ? ((mhi << lz) | (mlo >> (64 - lz))) : mhi;
+    const unsigned long long rest = mlo << lz;
+    unsigned long long mant = top >> 11;
+    const unsigned long long rem = top & 0x7ffull;
+    if (rem > 0x400ull || (rem == 0x400ull && (rest != 0 || (mant & 1ull)))) mant += 1;
+    const double r = ldexp((double)mant, 75 - lz);
+    return (neg ? -r : r) * unit;
+}
+
+// The charge density of one node from its accumulator (L, H) = H 2^32 + L:
+// (exact node sum) / dT * tmp2 (PartBunch.cpp:496, :510-511).  Only a
+// product and a quotient: no contraction can change its rounding.
+__device__ __forceinline__ double node_density(ulonglong2 a, double unit, double dT, double tmp2) {
+    const i128 w = (i128)(long long)a.y * (i128)4294967296 + (i128)a.x;
+    double s = acc_to_double((unsigned long long)w, (unsigned long long)(w >> 64), unit);
+    s /= dT;
+    s *= tmp2;
+    return s;
+}
+
 }  // namespace sc

@@ -407,14 +407,8 @@ __device__ __forceinline__ void cic_charge(const double* d, double q, double* v)
     v[7] = d[0] * d[1] * d[2] * q;
 }
 
-// Exact sums of the scattered charges: each charge v (|v| <= |q dt|) becomes
-// the integer t = rint(v * 2^(52 - E)) with 2^E > 2 |q dt|, so |t| < 2^51;
-// the sums are integer additions, exact, so any order gives the same total,
-// which is rounded to a double once.  The rounding of t is at most 2^-52 of
-// one particle's charge.
-constexpr int kFxFrac = 52;
-
-__device__ __forceinline__ int fx_exponent(double qdt) { return qdt != 0.0 ? ilogb(qdt) + 2 : 0; }
+// Exact sums of the scattered charges (kFxFrac, fx_exponent, node_density in
+// sc_exact.cuh).
 
 // A fixed-point charge t (an integer-valued double, |t| < 2^51) as two exact
 // 32-bit limbs: hi = floor(t / 2^26) in [-2^25, 2^25), lo = t - hi 2^26 in
@@ -545,26 +539,6 @@ __global__ void __launch_bounds__(kThreads) k_deposit_bins(BunchConst bc, const 
     deposit_body<true>(bc, x, y, z, bin, nactive, st, acc, vb_grid());
 }
 
-// correctly rounded double of the 128-bit accumulator (lo, hi), times unit
-__device__ __forceinline__ double acc_to_double(unsigned long long lo, unsigned long long hi, double unit) {
-    const long long shi = (long long)hi;
-    if (shi == ((long long)lo < 0 ? -1 : 0)) return __ll2double_rn((long long)lo) * unit;  // fits in 64 bits
-    const bool neg = shi < 0;
-    unsigned long long mlo = lo, mhi = hi;
-    if (neg) {
-        mlo = ~mlo + 1ull;
-        mhi = ~mhi + (mlo == 0 ? 1ull : 0ull);
-    }
-    const int lz = __clzll(mhi);
-    const unsigned long long top = lz ? ((mhi << lz) | (mlo >> (64 - lz))) : mhi;
-    const unsigned long long rest = mlo << lz;
-    unsigned long long mant = top >> 11;
-    const unsigned long long rem = top & 0x7ffull;
-    if (rem > 0x400ull || (rem == 0x400ull && (rest != 0 || (mant & 1ull)))) mant += 1;
-    const double r = ldexp((double)mant, 75 - lz);
-    return (neg ? -r : r) * unit;
-}
-
 // rho = (exact node sum) / dT * tmp2   (PartBunch.cpp:496, :510-511); the
 // accumulators are cleared for the next deposit.
 template <typename T>
@@ -574,11 +548,7 @@ __device__ __forceinline__ void assemble_body(const BunchConst& bc, const StepSt
     const double dT = bc.dT, tmp2 = st->tmp2;
     const double unit = ldexp(1.0, fx_exponent(st->qdt) - kFxFrac);
     for (int c = g.blk * blockDim.x + threadIdx.x; c < M; c += g.nblk * blockDim.x) {
-        const ulonglong2 a = reinterpret_cast<const ulonglong2*>(acc)[c];
-        const i128 w = (i128)(long long)a.y * (i128)4294967296 + (i128)a.x;  // H 2^32 + L
-        double s = acc_to_double((unsigned long long)w, (unsigned long long)(w >> 64), unit);
-        s /= dT;
-        s *= tmp2;
+        const double s = node_density(reinterpret_cast<const ulonglong2*>(acc)[c], unit, dT, tmp2);
         rho[c] = (T)s;
         reinterpret_cast<ulonglong2*>(acc)[c] = make_ulonglong2(0ull, 0ull);
     }
