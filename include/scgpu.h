@@ -17,6 +17,9 @@
  *   scgpu_compute_potential, scgpu_compute_potential_device
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr)
  *       (src/Solvers/PoissonSolver.h:28; FFTPoissonSolver.cpp:337-382)
+ *   scgpu_add_solenoid, scgpu_clear_elements, scgpu_fieldmap_astra1d
+ *       ParallelTTracker::computeExternalFields (ParallelTTracker.cpp:595-643)
+ *       with Solenoid::apply and Astra1DMagnetoStatic (see below)
  *   scgpu_set_exchange
  *       the MPI reductions of a distributed bunch (get_bounds, calcMoments,
  *       the scatter into the distributed rho field) as an exchange callback
@@ -187,6 +190,20 @@ int scgpu_compute_self_fields(scgpu_ctx* ctx, long long n, const double* R, cons
 #define SCGPU_EXCHANGE_MIN_F64 1
 typedef int (*scgpu_exchange_fn)(void* device_buffer, long long count, int op, void* cuda_stream, void* user);
 int scgpu_set_exchange(scgpu_ctx* ctx, scgpu_exchange_fn fn, void* user, long long total_particles, int capturable);
+
+/* Beamline elements with external fields, the step's computeExternalFields
+ * (src/Algorithms/ParallelTTracker.cpp:595-643) and the reference
+ * particle's (:1134-1155): SOLENOID elements (src/Classic/AbsBeamline/
+ * Solenoid.cpp:163-215) with a 1D magnetostatic field map in ASTRA format
+ * (src/Classic/Fields/Astra1DMagnetoStatic.cpp), at ELEMEDGE on a straight
+ * beamline along z, scaled by KS [T].  Up to 8 elements; they add to the
+ * uniform bz_ext of the bunch parameters.  scgpu_fieldmap_astra1d returns the
+ * map's Fourier coefficients (2 accuracy - 1 of them), its first and last z
+ * and the Fourier period, as Astra1DMagnetoStatic::readMap computes them. */
+int scgpu_add_solenoid(scgpu_ctx* ctx, const char* fieldmap_path, double elemedge, double ks);
+int scgpu_clear_elements(scgpu_ctx* ctx);
+int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin, double* zend,
+                           double* period);
 
 /* FIELDSOLVER BCFFTZ=PERIODIC (FFTPoissonSolver(..., bcz="PERIODIC"),
  * src/Solvers/FFTPoissonSolver.cpp:60, :130-155, :189-190, :661-662): the

@@ -52,6 +52,11 @@ class Debug(C.Structure):
                 ("rot_beam_to_ref", C.c_double * 9), ("update_origin", C.c_double * 3)]
 
 
+class Solenoid(C.Structure):
+    _fields_ = [("edge", C.c_double), ("scale", C.c_double), ("zbegin", C.c_double), ("range", C.c_double),
+                ("period", C.c_double), ("accuracy", C.c_int), ("pad_", C.c_int), ("coefs", C.c_double * 255)]
+
+
 class BeamParams(C.Structure):
     _fields_ = [(name, C.c_double * 3) for name in
                 ("rmin", "rmax", "rmean", "pmean", "rrms", "prms", "eps_norm", "eps", "rprms")] + \
@@ -213,6 +218,34 @@ def compute_potential(rho, hr):
     if rc:
         raise RuntimeError(f"sco_compute_potential failed: {rc}")
     return r
+
+
+def make_solenoid(coefs, zbegin, zend, period, edge, ks):
+    e = Solenoid()
+    c = np.asarray(coefs, dtype=np.float64)
+    e.edge, e.scale, e.zbegin, e.range, e.period = edge, ks, zbegin, zend - zbegin, period
+    e.accuracy = (c.size + 1) // 2
+    e.coefs[:c.size] = list(c)
+    return e
+
+
+def set_solenoids(elements):
+    """SOLENOID elements applied by the tracker (computeExternalFields)."""
+    arr = (Solenoid * max(len(elements), 1))(*elements)
+    rc = lib().sco_set_solenoids(arr, C.c_int(len(elements)))
+    if rc:
+        raise RuntimeError(f"sco_set_solenoids failed: {rc}")
+
+
+def solenoid_field(element, R):
+    """B [T] of one element at points R (n x 3, element frame)."""
+    R = _f64(R)
+    out = np.empty_like(R)
+    for i in range(R.shape[0]):
+        b = (C.c_double * 3)()
+        lib().sco_solenoid_field(C.byref(element), R[i].ctypes.data_as(_dp), b)
+        out[i] = list(b)
+    return out
 
 
 def igf_periodic_z(nr, hr):

@@ -1368,6 +1368,101 @@ done:
 }
 
 /* ------------------------------------------------------------------------ */
+/* external fields of SOLENOID elements with ASTRA 1D magnetostatic maps      */
+/* (Solenoid.cpp:163-193, Astra1DMagnetoStatic.cpp:162-196) on a straight     */
+/* beamline along z (element frame = lab frame shifted by ELEMEDGE), as       */
+/* computeExternalFields (ParallelTTracker.cpp:614-643) and                   */
+/* updateReferenceParticle (:1134-1155) apply them.                           */
+/* ------------------------------------------------------------------------ */
+static sco_solenoid g_sol[SCO_MAX_ELEMENTS];
+static int g_nsol = 0;
+
+int sco_set_solenoids(const sco_solenoid* s, int n) {
+    if (n < 0 || n > SCO_MAX_ELEMENTS) return SCO_ERR_ARG;
+    for (int k = 0; k < n; ++k) g_sol[k] = s[k];
+    g_nsol = n;
+    return 0;
+}
+
+/* Solenoid::apply with Astra1DMagnetoStatic::getFieldstrength: B of one
+ * element at R (element frame), 0 outside [zbegin, zbegin + range). */
+void sco_solenoid_field(const sco_solenoid* e, const double* R, double* B) {
+    B[0] = B[1] = B[2] = 0.0;
+    const double tmpR[3] = {R[0], R[1], R[2] - e->zbegin};
+    if (!(tmpR[2] >= 0.0 && tmpR[2] < e->range)) return;
+    const double two_pi = 2 * SCO_PI;
+    const double RR2 = tmpR[0] * tmpR[0] + tmpR[1] * tmpR[1];
+    const double kz = two_pi * tmpR[2] / e->period + SCO_PI;
+    double ez = e->coefs[0], ezp = 0.0, ezpp = 0.0, ezppp = 0.0;
+    int n = 1;
+    for (int l = 1; l < e->accuracy; l++, n += 2) {
+        double somefactor_base = two_pi / e->period * l;
+        double somefactor = 1.0;
+        double coskzl = cos(kz * l);
+        double sinkzl = sin(kz * l);
+        ez += (e->coefs[n] * coskzl - e->coefs[n + 1] * sinkzl);
+        somefactor *= somefactor_base;
+        ezp += somefactor * (-e->coefs[n] * sinkzl - e->coefs[n + 1] * coskzl);
+        somefactor *= somefactor_base;
+        ezpp += somefactor * (-e->coefs[n] * coskzl + e->coefs[n + 1] * sinkzl);
+        somefactor *= somefactor_base;
+        ezppp += somefactor * (e->coefs[n] * sinkzl + e->coefs[n + 1] * coskzl);
+    }
+    const double BfieldR = -ezp / 2. + ezppp / 16. * RR2;
+    const double tB[3] = {BfieldR * tmpR[0], BfieldR * tmpR[1], ez - ezpp * RR2 / 4.};
+    B[0] = e->scale * tB[0];
+    B[1] = e->scale * tB[1];
+    B[2] = e->scale * tB[2];
+}
+
+static void element_lab2local(const sco_solenoid* e, sco_trafo* t) {
+    const double o[3] = {0.0, 0.0, e->edge}, q[4] = {1.0, 0.0, 0.0, 0.0};
+    sco_trafo_make(t, o, q);
+}
+
+/* the particles: refToLocal = misalignment * (lab2local * referenceToLab) */
+static void add_element_fields(const sco_trafo* ref_to_lab, long long n, const double* R, double* Bf) {
+    for (int k = 0; k < g_nsol; ++k) {
+        sco_trafo l2l, r2loc, mis;
+        element_lab2local(&g_sol[k], &l2l);
+        r2loc = l2l;
+        sco_trafo_compose(&r2loc, ref_to_lab);
+        const double o[3] = {0.0, 0.0, 0.0}, q[4] = {1.0, 0.0, 0.0, 0.0};
+        sco_trafo_make(&mis, o, q);
+        sco_trafo_compose(&mis, &r2loc);
+        r2loc = mis;
+        sco_trafo loc2r = r2loc;
+        sco_trafo_invert(&loc2r);
+        SCO_PAR
+        for (long long i = 0; i < n; ++i) {
+            double loc[3], Bl[3], Br[3];
+            trafo_transform_to(&r2loc, R + 3 * i, loc);
+            sco_solenoid_field(&g_sol[k], loc, Bl);
+            trafo_rotate_to(&loc2r, Bl, Br);
+            Bf[3 * i + 0] += Br[0];
+            Bf[3 * i + 1] += Br[1];
+            Bf[3 * i + 2] += Br[2];
+        }
+    }
+}
+
+/* the reference particle: refToLocal = lab2local * referenceToLab, B rotated from */
+static void add_element_fields_ref(const sco_trafo* ref_to_lab, const double* R, double* Bf) {
+    for (int k = 0; k < g_nsol; ++k) {
+        sco_trafo r2loc;
+        element_lab2local(&g_sol[k], &r2loc);
+        sco_trafo_compose(&r2loc, ref_to_lab);
+        double loc[3], Bl[3];
+        trafo_transform_to(&r2loc, R, loc);
+        sco_solenoid_field(&g_sol[k], loc, Bl);
+        const double* M = r2loc.M;
+        Bf[0] += M[0] * Bl[0] + M[3] * Bl[1] + M[6] * Bl[2];
+        Bf[1] += M[1] * Bl[0] + M[4] * Bl[1] + M[7] * Bl[2];
+        Bf[2] += M[2] * Bl[0] + M[5] * Bl[1] + M[8] * Bl[2];
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* one ParallelTTracker step (ParallelTTracker.cpp:343-365)                   */
 /* bins == NULL: computeSelfFields(); else the energy-bin loop (:567-578).    */
 /* ------------------------------------------------------------------------ */
@@ -1425,6 +1520,7 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
         SCO_PAR
         for (long long i = 0; i < n; ++i) Bf[3 * i + 2] += prm->bz_ext;
     }
+    add_element_fields(&tr->ref_to_lab, n, R, Bf);
     if (dbg && dbg->Ef) memcpy(dbg->Ef, Ef, 3 * n * sizeof(double));
     if (dbg && dbg->Bf) memcpy(dbg->Bf, Bf, 3 * n * sizeof(double));
     /* timeIntegration2: kick + push (:450-491) */
@@ -1441,6 +1537,7 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
         rr[0] /= scaleFactor; rr[1] /= scaleFactor; rr[2] /= scaleFactor;
         { double g = sqrt(1.0 + dot3(rp, rp)); rr[0] += 0.5 * rp[0] / g; rr[1] += 0.5 * rp[1] / g; rr[2] += 0.5 * rp[2] / g; }
         rr[0] *= scaleFactor; rr[1] *= scaleFactor; rr[2] *= scaleFactor;
+        add_element_fields_ref(&tr->ref_to_lab, rr, bref);
         if (prm->bz_ext != 0.0) bref[2] += prm->bz_ext;
         kick_one(rp, zero, bref, dt, prm->mass, prm->charge);
         rr[0] /= scaleFactor; rr[1] /= scaleFactor; rr[2] /= scaleFactor;

@@ -132,3 +132,23 @@ def photoinjector_bunch(n, nbins=10, sigma_r=1e-3, z_center=4e-3, sigma_z=0.8e-3
     P[:, 1] = bg_perp * g4
     P[:, 2] = bg * (1.0 + rel_spread * g5)
     return R, P, bins
+
+
+def write_solenoid_map(path, accuracy=30, length=0.3, npts=241, b0=1.0, edge=0.03, width=0.01, jitter=0.0, seed=3):
+    """A seeded synthetic on-axis solenoid profile in ASTRA 1D format
+    ("AstraMagnetostatic <accuracy>", then "z Bz" lines): a flat top of
+    b0 between edge and length - edge with tanh fringes of the given width.
+    jitter > 0 moves the sample points off the equidistant grid (the reader
+    resamples them by a cubic spline).  Stands in for the field maps of the
+    reference's examples, which are not shipped here."""
+    z = np.linspace(0.0, length, npts)
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        dz = length / (npts - 1)
+        z[1:-1] += rng.uniform(-jitter, jitter, npts - 2) * dz
+    bz = 0.5 * b0 * (np.tanh((z - edge) / width) - np.tanh((z - (length - edge)) / width))
+    with open(path, "w") as f:
+        f.write(f"AstraMagnetostatic {accuracy}\n")
+        for zi, bi in zip(z, bz):
+            f.write(f"{zi:.17g} {bi:.17g}\n")
+    return z, bz

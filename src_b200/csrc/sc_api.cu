@@ -532,6 +532,7 @@ void scgpu_destroy(scgpu_ctx* c) {
     drop_graphs(c);
     free_particles(c);
     free_bins(c);
+    dfree(c->d_elements);
     DevBunch& b = c->b;
     dfree(b.nacc); dfree(b.rho); dfree(b.phi); dfree(b.E4); dfree(b.spec); dfree(b.spec_lo);
     dfree(b.gtmp); dfree(b.gline); dfree(b.ghat); dfree(b.st); dfree(b.partials); dfree(b.ticket);
@@ -648,6 +649,54 @@ static int compute_potential_image_impl(scgpu_ctx* c, double* rho, const double 
     CK(cudaStreamSynchronize(s));
     c->have_solve = false;
     return SCGPU_OK;
+}
+
+// SOLENOID elements with ASTRA 1D magnetostatic maps on a straight beamline
+// (Solenoid.cpp, Astra1DMagnetoStatic.cpp; ParallelTTracker::computeExternalFields).
+static int upload_elements(scgpu_ctx* c) {
+    DevBunch& b = c->b;
+    drop_graphs(c);
+    if (c->elements.empty()) {
+        b.bc.sol = nullptr;
+        b.bc.nsol = 0;
+        return SCGPU_OK;
+    }
+    if (!c->d_elements) {
+        int rc = dalloc(c, &c->d_elements, kMaxElements * sizeof(SolElem));
+        if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(c->d_elements, c->elements.data(), c->elements.size() * sizeof(SolElem), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    b.bc.sol = c->d_elements;
+    b.bc.nsol = (int)c->elements.size();
+    return SCGPU_OK;
+}
+
+int scgpu_add_solenoid(scgpu_ctx* c, const char* fieldmap, double elemedge, double ks) {
+    if (!c || !fieldmap) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!std::isfinite(elemedge) || !std::isfinite(ks)) return fail(c, SCGPU_ERR_ARG, "ELEMEDGE and KS must be finite");
+    if ((int)c->elements.size() >= kMaxElements) return fail(c, SCGPU_ERR_UNSUPPORTED, "at most 8 elements");
+    SolElem e{};
+    int ncoef = 0;
+    int rc = scgpu_fieldmap_astra1d(fieldmap, e.coefs, kMaxSolCoefs, &ncoef, &e.zbegin, &e.range, &e.period);
+    if (rc) return fail(c, rc, std::string("cannot read the field map ") + fieldmap);
+    e.range = e.range - e.zbegin;  // zend - zbegin
+    e.accuracy = (ncoef + 1) / 2;
+    e.edge = elemedge;
+    e.scale = ks;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    c->elements.push_back(e);
+    return upload_elements(c);
+}
+
+int scgpu_clear_elements(scgpu_ctx* c) {
+    if (!c) return SCGPU_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    c->elements.clear();
+    return upload_elements(c);
 }
 
 int scgpu_set_exchange(scgpu_ctx* c, scgpu_exchange_fn fn, void* user, long long total_particles, int capturable) {

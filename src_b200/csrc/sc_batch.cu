@@ -134,7 +134,12 @@ int rebuild(scgpu_batch* b) {
         if (b->slots[s]) b->members.push_back(s);
     const int nm = (int)b->members.size();
     std::vector<DevBunch> tab(nm);
-    for (int i = 0; i < nm; ++i) tab[i] = b->slots[b->members[i]]->b;
+    for (int i = 0; i < nm; ++i) {
+        tab[i] = b->slots[b->members[i]]->b;
+        // the batched gather has no external-field variant; a sharded bunch needs its exchanges
+        if (tab[i].bc.nsol > 0 || tab[i].bc.sharded)
+            return bfail(b, SCGPU_ERR_UNSUPPORTED, "beamline elements or a sharded bunch in a batch");
+    }
     std::vector<int4> work;
     b->launches.clear();
     auto add_per_bunch = [&](int lane, int kind, auto blocks_of) {

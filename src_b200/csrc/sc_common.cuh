@@ -83,6 +83,7 @@ struct StepState {
     double betaC;  // sqrt(gz^2-1)/gz/c
     double qdt;    // Q * dt (the scattered charge)
     Trafo upd;     // reference-particle update of this step
+    Trafo ref_to_lab_step;  // ref -> lab at the start of the step (the external fields' frame)
     // energy bins / image charge
     double zshift;      // z shift of the image's Green's function (PartBunch.cpp:249)
     long long bin_count;  // particles in the bin (per-bin copies)
@@ -93,6 +94,22 @@ struct StepState {
     // 128-bit fixed point, summed as 64-bit integers)
     double bnd6[6];                 // min x, y, z and -max x, y, z
     unsigned long long xlimbs[28 * 4];
+};
+
+// A SOLENOID element with a 1D magnetostatic field map in ASTRA format
+// (Solenoid.cpp:163-215; Astra1DMagnetoStatic.cpp:162-196) on a straight
+// beamline along z: element frame = lab frame shifted by ELEMEDGE.
+constexpr int kMaxSolCoefs = 255;  // 2 accuracy - 1, accuracy <= 128
+constexpr int kMaxElements = 8;
+struct SolElem {
+    double edge;    // ELEMEDGE: the element origin on the lab z axis [m]
+    double scale;   // KS [T] (the map is normalised to 1)
+    double zbegin;  // startField: the map's first z (element frame)
+    double range;   // zend - zbegin: the field region (Solenoid::length_m)
+    double period;  // 2 N (zend - zbegin) / (N - 1): the Fourier period
+    int accuracy;   // harmonics 0 .. accuracy - 1
+    int pad_;
+    double coefs[kMaxSolCoefs];
 };
 
 struct BunchConst {
@@ -113,6 +130,10 @@ struct BunchConst {
     double rs_cdt;  // RN(1 / (c * dT))
     double ke;      // 0.5 * dT * charge * c / mass (BorisPusher.h:88)
     double ktn;     // 0.5 * dT * charge * c * c    (BorisPusher.h:99, numerator)
+    // beamline elements with external fields (device table), none when nsol == 0
+    const SolElem* sol;
+    int nsol;
+    int pad2_;
 };
 
 // fill the derived pusher constants of bc (host side)
@@ -259,6 +280,63 @@ SC_HD void trafo_transform_to(const Trafo& t, const double* r, double* out) {
     matvec(t.M, d, out);
 }
 SC_HD void trafo_rotate_to(const Trafo& t, const double* r, double* out) { matvec(t.M, r, out); }
+// the inverse rotation (the rotation matrix of the inverted trafo is M^T exactly)
+SC_HD void trafo_rotate_from(const Trafo& t, const double* r, double* out) {
+    const double* M = t.M;
+    out[0] = M[0] * r[0] + M[3] * r[1] + M[6] * r[2];
+    out[1] = M[1] * r[0] + M[4] * r[1] + M[7] * r[2];
+    out[2] = M[2] * r[0] + M[5] * r[1] + M[8] * r[2];
+}
+
+// ---------------------------------------------------------------- external fields
+// Astra1DMagnetoStatic::getFieldstrength (Astra1DMagnetoStatic.cpp:162-196):
+// the Fourier series of the on-axis field and its first three derivatives,
+// expanded off axis, for R in the element frame; Solenoid::apply
+// (Solenoid.cpp:167-179): only inside [zbegin, zbegin + range), scaled by KS.
+SC_HD void solenoid_field(const SolElem& e, const double* R, double* B) {
+    const double tz = R[2] - e.zbegin;
+    if (!(tz >= 0.0 && tz < e.range)) return;
+    const double RR2 = R[0] * R[0] + R[1] * R[1];
+    const double two_pi = 2 * kPi;
+    const double kz = two_pi * tz / e.period + kPi;
+    double ez = e.coefs[0], ezp = 0.0, ezpp = 0.0, ezppp = 0.0;
+    int n = 1;
+    for (int l = 1; l < e.accuracy; l++, n += 2) {
+        const double base = two_pi / e.period * l;
+        double f = 1.0;
+        const double c = cos(kz * l), s = sin(kz * l);
+        ez += (e.coefs[n] * c - e.coefs[n + 1] * s);
+        f *= base;
+        ezp += f * (-e.coefs[n] * s - e.coefs[n + 1] * c);
+        f *= base;
+        ezpp += f * (-e.coefs[n] * c + e.coefs[n + 1] * s);
+        f *= base;
+        ezppp += f * (e.coefs[n] * s + e.coefs[n + 1] * c);
+    }
+    const double BfieldR = -ezp / 2. + ezppp / 16. * RR2;
+    const double tB[3] = {BfieldR * R[0], BfieldR * R[1], ez - ezpp * RR2 / 4.};
+    B[0] = e.scale * tB[0];
+    B[1] = e.scale * tB[1];
+    B[2] = e.scale * tB[2];
+}
+
+// computeExternalFields (ParallelTTracker.cpp:614-643) for the elements of
+// the table: R in the reference frame -> lab (ref_to_lab) -> element frame
+// (minus ELEMEDGE along z); each element's B rotated back and added to Bf.
+SC_HD void add_external_B(const SolElem* el, int n, const Trafo& ref_to_lab, const double* R, double* Bf) {
+    for (int k = 0; k < n; ++k) {
+        double lab[3], loc[3], Bl[3] = {0.0, 0.0, 0.0}, Br[3];
+        trafo_transform_to(ref_to_lab, R, lab);
+        loc[0] = lab[0] - 0.0;
+        loc[1] = lab[1] - 0.0;
+        loc[2] = lab[2] - el[k].edge;
+        solenoid_field(el[k], loc, Bl);
+        trafo_rotate_from(ref_to_lab, Bl, Br);
+        Bf[0] += Br[0];
+        Bf[1] += Br[1];
+        Bf[2] += Br[2];
+    }
+}
 
 // ---------------------------------------------------------------- pusher
 // BorisPusher::push between switchToUnitlessPositions / switchOff...
@@ -492,6 +570,7 @@ SC_HD_COLD bool derive_beam_frame(StepState& s, const BunchConst& bc) {
 // updateReferenceParticle + updateRefToLabCSTrafo (ParallelTTracker.cpp:1123-1212)
 // for a beamline with no elements except an optional uniform B_z.
 SC_HD bool advance_reference(StepState& s, const BunchConst& bc) {
+    s.ref_to_lab_step = s.ref_to_lab;  // the particles' external fields use the frame of the step's start
     s.t += bc.dT;
     const double dt = s.t < bc.dT ? s.t : bc.dT;
     const double scaleFactor = kC * dt;
@@ -510,6 +589,9 @@ SC_HD bool advance_reference(StepState& s, const BunchConst& bc) {
         rr[1] *= scaleFactor;
         rr[2] *= scaleFactor;
         if (pass == 0) {
+            // updateReferenceParticle (ParallelTTracker.cpp:1134-1155): the
+            // elements' fields at the reference particle, then the kick
+            add_external_B(bc.sol, bc.nsol, s.ref_to_lab, rr, bref);
             if (bc.bz_ext != 0.0) bref[2] += bc.bz_ext;
             kick_one(rp, zero, bref, dt, bc.mass, bc.charge);
         }

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <string>
+#include <vector>
 
 #include "scgpu.h"
 #include "sc_internal.h"
@@ -39,6 +40,9 @@ struct scgpu_ctx {
     void* ghat_img_alt = nullptr; // functions while the main stream convolves bin k
     cudaEvent_t ev_bin[sc::kMaxBins] = {};
     cudaEvent_t ev_used[sc::kMaxBins] = {};
+    // beamline elements (scgpu_add_solenoid): host copy and device table
+    std::vector<sc::SolElem> elements;
+    sc::SolElem* d_elements = nullptr;
     // sharded bunch (scgpu_set_exchange): this context holds one rank's shard
     scgpu_exchange_fn xfn = nullptr;
     void* xuser = nullptr;

@@ -1,0 +1,166 @@
+// sc_fieldmap.cpp -- 1D magnetostatic field maps in ASTRA format, as OPAL's
+// Astra1DMagnetoStatic reads them (src/Classic/Fields/Astra1DMagnetoStatic.cpp:
+// constructor :15-77, readMap :83-160): a header "AstraMagnetostatic
+// <accuracy> [TRUE|FALSE]" and lines "z Bz(z)" ('#' comments and blank lines
+// skipped, points whose z does not increase by more than 1e-10 dropped).  The
+// on-axis field is resampled on an equidistant grid by a natural cubic spline,
+// mirrored to an even periodic sequence of 2N points and expanded in a
+// Fourier series; the first 2 accuracy - 1 coefficients, normalised to the
+// largest |Bz| unless the header says FALSE, are what the device evaluates.
+//
+// Host C++ only (no CUDA); the evaluation is in sc_common.cuh.
+#include <cctype>
+#include <cmath>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "scgpu.h"
+
+namespace {
+
+// One content line: '#' starts a comment; lines without an alphanumeric
+// character are skipped; surrounding blanks removed (Fieldmap::getLine,
+// Fieldmap.cpp:519-541).
+bool content_line(std::ifstream& in, std::string& out) {
+    std::string line;
+    while (std::getline(in, line)) {
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.erase(hash);
+        size_t first = std::string::npos, last = std::string::npos;
+        for (size_t i = 0; i < line.size(); ++i)
+            if (std::isalnum((unsigned char)line[i])) {
+                if (first == std::string::npos) first = i;
+                last = i;
+            }
+        if (first == std::string::npos) continue;
+        out = line.substr(first, last - first + 1);
+        return true;
+    }
+    return false;
+}
+
+// A data line holds exactly two numbers (Fieldmap::interpreteLine<double, double>).
+bool two_numbers(const std::string& s, double& a, double& b) {
+    std::istringstream is(s);
+    if (!(is >> a >> b)) return false;
+    std::string rest;
+    return !(is >> rest);
+}
+
+// Natural cubic spline through (x, y) evaluated at t (the second derivatives
+// from the tridiagonal system with zero end curvature, then the cubic of the
+// interval holding t).
+struct NaturalSpline {
+    std::vector<double> x, y, m;
+    NaturalSpline(const std::vector<double>& xs, const std::vector<double>& ys) : x(xs), y(ys), m(xs.size(), 0.0) {
+        const size_t n = x.size();
+        if (n < 3) return;
+        std::vector<double> c(n, 0.0), d(n, 0.0);
+        for (size_t i = 1; i + 1 < n; ++i) {
+            const double h0 = x[i] - x[i - 1], h1 = x[i + 1] - x[i];
+            const double a = h0, bdiag = 2.0 * (h0 + h1), cc = h1;
+            const double r = 6.0 * ((y[i + 1] - y[i]) / h1 - (y[i] - y[i - 1]) / h0);
+            const double denom = bdiag - a * c[i - 1];
+            c[i] = cc / denom;
+            d[i] = (r - a * d[i - 1]) / denom;
+        }
+        for (size_t i = n - 2; i >= 1; --i) {
+            m[i] = d[i] - c[i] * m[i + 1];
+            if (i == 1) break;
+        }
+    }
+    double operator()(double t) const {
+        const size_t n = x.size();
+        size_t i = 0;
+        if (t >= x[n - 1]) {
+            i = n - 2;
+        } else {
+            size_t lo = 0, hi = n - 1;
+            while (hi - lo > 1) {
+                const size_t mid = (lo + hi) / 2;
+                if (x[mid] > t)
+                    hi = mid;
+                else
+                    lo = mid;
+            }
+            i = lo;
+        }
+        const double h = x[i + 1] - x[i];
+        const double A = (x[i + 1] - t) / h, B = (t - x[i]) / h;
+        return A * y[i] + B * y[i + 1] + ((A * A * A - A) * m[i] + (B * B * B - B) * m[i + 1]) * h * h / 6.0;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin, double* zend,
+                           double* period) {
+    if (!path || !coefs || !ncoefs || !zbegin || !zend || !period) return SCGPU_ERR_ARG;
+    std::ifstream in(path);
+    if (!in) return SCGPU_ERR_ARG;
+    std::string line;
+    if (!content_line(in, line)) return SCGPU_ERR_ARG;
+    std::istringstream hs(line);
+    std::string name, flag;
+    int accuracy = 0;
+    if (!(hs >> name >> accuracy) || name.compare(0, 6, "AstraM") != 0 || accuracy < 1) return SCGPU_ERR_ARG;
+    bool normalize = true;
+    if (hs >> flag) {
+        for (char& ch : flag) ch = (char)std::toupper((unsigned char)ch);
+        if (flag != "TRUE" && flag != "FALSE") return SCGPU_ERR_ARG;
+        normalize = flag == "TRUE";
+    }
+    std::vector<double> zs, bz;
+    double z = 0.0, b = 0.0, last = 0.0, zlast = 0.0;
+    while (content_line(in, line)) {
+        if (!two_numbers(line, z, b)) return SCGPU_ERR_ARG;
+        zlast = z;  // the last line read sets zend, accepted or not (:45-52)
+        if (zs.empty() || z - last > 1e-10) {
+            zs.push_back(z);
+            bz.push_back(b);
+            last = z;
+        }
+    }
+    const int N = (int)zs.size();
+    if (N < 3 || 2 * accuracy - 1 > max_coefs || accuracy > N) return SCGPU_ERR_ARG;
+    const double zb = zs[0], ze = zlast;
+    const double dz = (ze - zb) / (N - 1);
+    double bmax = 0.0;
+    for (double v : bz) bmax = std::fmax(bmax, std::fabs(v));
+    if (!normalize) bmax = 1.0;
+    if (!(bmax > 0.0)) return SCGPU_ERR_ARG;
+    // equidistant resampling, then the mirror image in front: 2N samples
+    const NaturalSpline spline(zs, bz);
+    std::vector<double> seq(2 * (size_t)N);
+    for (int i = 0; i < N - 1; ++i) seq[N + i] = spline(zb + dz * i);
+    seq[2 * (size_t)N - 1] = bz[N - 1];
+    for (int i = 0; i < N; ++i) seq[i] = seq[2 * (size_t)N - 1 - i];
+    // forward DFT X_k = sum_j x_j exp(-2 pi i j k / 2N) for k < accuracy, in long double
+    const long n = 2L * N;
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int k = 0; k < accuracy; ++k) {
+        long double re = 0.0L, im = 0.0L;
+        for (long j = 0; j < n; ++j) {
+            const long double a = two_pi * (long double)((j * (long)k) % n) / (long double)n;
+            re += (long double)seq[j] * cosl(a);
+            im -= (long double)seq[j] * sinl(a);
+        }
+        if (k == 0) {
+            coefs[0] = (double)re / (bmax * 2. * N);
+        } else {
+            coefs[2 * k - 1] = (double)re / (bmax * N);
+            coefs[2 * k] = (double)im / (bmax * N);
+        }
+    }
+    *ncoefs = 2 * accuracy - 1;
+    *zbegin = zb;
+    *zend = ze;
+    *period = 2.0 * N * (ze - zb) / (N - 1);
+    return SCGPU_OK;
+}
+
+}  // extern "C"

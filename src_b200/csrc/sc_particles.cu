@@ -1031,7 +1031,7 @@ __device__ __forceinline__ void cic_gather8(const double* __restrict__ F8, const
     }
 }
 
-template <typename T, bool BINNED = false>
+template <typename T, bool BINNED = false, bool EXT = false>
 __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
                                             double* __restrict__ z, double* __restrict__ px, double* __restrict__ py,
                                             double* __restrict__ pz, const T* __restrict__ E4, StepState* st,
@@ -1072,6 +1072,8 @@ __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __rest
         trafo_rotate_to(*b2r, Eb, Ef);
         trafo_rotate_to(*b2r, Bb, Bf);
         if (bc.bz_ext != 0.0) Bf[2] += bc.bz_ext;
+        // the beamline elements' fields at R, in the frame of the step's start
+        if constexpr (EXT) add_external_B(bc.sol, bc.nsol, st->ref_to_lab_step, R, Bf);
         kick_r(P, Ef, Bf, bc.ke, bc.ktn, bc.mass);
         push_r(R, P, bc.s_cdt, bc.rs_cdt);
         double Ru[3], Pu[3];
@@ -1110,21 +1112,22 @@ __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __rest
         *ticket = 0u;
     }
 }
-template <typename T>
+template <typename T, bool EXT = false>
 __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
                                                                   double* __restrict__ z, double* __restrict__ px,
                                                                   double* __restrict__ py, double* __restrict__ pz,
                                                                   const T* __restrict__ E4, StepState* st, double* partials,
                                                                   unsigned* ticket) {
-    gather_body<T>(bc, x, y, z, px, py, pz, E4, st, partials, ticket, vb_grid());
+    gather_body<T, false, EXT>(bc, x, y, z, px, py, pz, E4, st, partials, ticket, vb_grid());
 }
+template <bool EXT = false>
 __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push_bins(BunchConst bc, double* __restrict__ x,
                                                                        double* __restrict__ y, double* __restrict__ z,
                                                                        double* __restrict__ px, double* __restrict__ py,
                                                                        double* __restrict__ pz,
                                                                        const double* __restrict__ F8, StepState* st,
                                                                        double* partials, unsigned* ticket) {
-    gather_body<double, true>(bc, x, y, z, px, py, pz, nullptr, st, partials, ticket, vb_grid(), F8);
+    gather_body<double, true, EXT>(bc, x, y, z, px, py, pz, nullptr, st, partials, ticket, vb_grid(), F8);
 }
 
 // Fields only (PartBunch::computeSelfFields output): Ef, Bf in the beam frame,
@@ -1433,12 +1436,16 @@ void launch_grad(const DevBunch& b, cudaStream_t s) {
 }
 
 void launch_gather_kick_push(const DevBunch& b, bool stats, cudaStream_t s) {
-    if (b.precision == 0)
-        k_gather_kick_push<double><<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz,
-                                                                     (const double*)b.E4, b.st, b.partials, b.ticket);
-    else
-        k_gather_kick_push<float><<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz,
-                                                                    (const float*)b.E4, b.st, b.partials, b.ticket);
+    const bool ext = b.bc.nsol > 0;
+    if (b.precision == 0) {
+        auto k = ext ? k_gather_kick_push<double, true> : k_gather_kick_push<double, false>;
+        k<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, (const double*)b.E4, b.st, b.partials,
+                                            b.ticket);
+    } else {
+        auto k = ext ? k_gather_kick_push<float, true> : k_gather_kick_push<float, false>;
+        k<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, (const float*)b.E4, b.st, b.partials,
+                                            b.ticket);
+    }
     if (stats) launch_reduce_stats(b, s);
 }
 
@@ -1476,8 +1483,8 @@ void launch_grad_acc(const DevBunch& v, bool image, cudaStream_t s) {
 }
 
 void launch_gather_kick_push_bins(const DevBunch& b, bool stats, cudaStream_t s) {
-    k_gather_kick_push_bins<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.F8, b.st,
-                                                              b.partials, b.ticket);
+    auto k = b.bc.nsol > 0 ? k_gather_kick_push_bins<true> : k_gather_kick_push_bins<false>;
+    k<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.F8, b.st, b.partials, b.ticket);
     if (stats) launch_reduce_stats(b, s);
 }
 

@@ -110,6 +110,9 @@ def lib():
         L.scgpu_get_bin_gammas.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong)]
         L.scgpu_set_periodic_z.argtypes = [C.c_void_p, C.c_int]
         L.scgpu_set_exchange.argtypes = [C.c_void_p, EXCHANGE_FN, C.c_void_p, C.c_longlong, C.c_int]
+        L.scgpu_add_solenoid.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double]
+        L.scgpu_clear_elements.argtypes = [C.c_void_p]
+        L.scgpu_fieldmap_astra1d.argtypes = [C.c_char_p, _dp, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp]
         L.scgpu_stat_row.argtypes = [C.c_void_p, _dp]
         L.scgpu_stat_column_name.argtypes = [C.c_int]
         L.scgpu_stat_column_name.restype = C.c_char_p
@@ -133,7 +136,8 @@ EXPORTED = [
     "scgpu_compute_potential_image_device", "scgpu_compute_self_fields_binned", "scgpu_set_energy_bins",
     "scgpu_get_bin_gammas", "scgpu_stat_row", "scgpu_stat_column_name", "scgpu_sdds_write_header",
     "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
-    "scgpu_set_periodic_z", "scgpu_set_exchange",
+    "scgpu_set_periodic_z", "scgpu_set_exchange", "scgpu_add_solenoid", "scgpu_clear_elements",
+    "scgpu_fieldmap_astra1d",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
@@ -196,6 +200,14 @@ class Context:
         assert r.shape == (self.nr[2], self.nr[1], self.nr[0])
         self._check(lib().scgpu_compute_potential(self.h, _p(r), (C.c_double * 3)(*hr)), "compute_potential")
         return r
+
+    # ---- beamline elements (computeExternalFields)
+    def add_solenoid(self, fieldmap, elemedge, ks):
+        """SOLENOID with an ASTRA 1D magnetostatic map at ELEMEDGE [m], KS [T]."""
+        self._check(lib().scgpu_add_solenoid(self.h, os.fsencode(fieldmap), float(elemedge), float(ks)), "add_solenoid")
+
+    def clear_elements(self):
+        self._check(lib().scgpu_clear_elements(self.h), "clear_elements")
 
     # ---- FIELDSOLVER BCFFTZ=PERIODIC
     def set_periodic_z(self, periodic=True):
@@ -545,3 +557,15 @@ def write_fromfile(path, R, P):
     rc = lib().scgpu_write_fromfile(os.fsencode(path), R.shape[0], _p(R), _p(P))
     if rc != 0:
         raise ScgpuError(rc, f"cannot write {path}")
+
+
+def fieldmap_astra1d(path):
+    """Astra1DMagnetoStatic::readMap: (Fourier coefficients, zbegin, zend, period)."""
+    coefs = np.empty(255)
+    n = C.c_int(0)
+    zb, ze, per = C.c_double(), C.c_double(), C.c_double()
+    rc = lib().scgpu_fieldmap_astra1d(os.fsencode(path), _p(coefs), 255, C.byref(n), C.byref(zb), C.byref(ze),
+                                      C.byref(per))
+    if rc != 0:
+        raise ScgpuError(rc, f"cannot read the field map {path}")
+    return coefs[:n.value].copy(), zb.value, ze.value, per.value

@@ -377,3 +377,39 @@ def test_periodic_z_mixed_and_limits(oracle, gpu):
         with pytest.raises(gpu.ScgpuError) as e:
             c.set_periodic_z(True)
         assert e.value.code == -8
+
+
+def test_tracking_with_solenoid_map_vs_oracle(oracle, gpu, tmp_path):
+    """SOLENOID elements with ASTRA 1D maps (computeExternalFields): the bunch
+    sits in the fringe of one element (radial field from dBz/dz) and inside
+    a second, overlapping one; 20 steps against the oracle."""
+    from src_b200.bunch import write_solenoid_map
+    N, nr, steps = 50_000, (32, 32, 32), 20
+    path = tmp_path / "sol.txt"
+    write_solenoid_map(path, accuracy=40)
+    c, zb, ze, per = gpu.fieldmap_astra1d(path)
+    R, P = gaussian_bunch(N, bunch_id=12)
+    Q = -1e-9 / N
+    elems = [(-0.03, 0.5), (-0.15, -0.2)]
+    oracle.set_solenoids([oracle.make_solenoid(c, zb, ze, per, e, ks) for e, ks in elems])
+    try:
+        tr = oracle.OracleTracker(oracle.make_params(nr, 1e-12), Q)
+        Ro, Po = R.copy(), P.copy()
+        tr.track(Ro, Po, steps)
+    finally:
+        oracle.set_solenoids([])
+    with gpu.Context(nr) as ctx:
+        for e, ks in elems:
+            ctx.add_solenoid(path, e, ks)
+        ctx.upload(R, P, 1e-12, Q, oracle.electron_mass_ev())
+        ctx.track(steps)
+        Rg, Pg = ctx.download()
+        st = ctx.tracker_state()
+        ctx.clear_elements()
+        ctx.upload(R, P, 1e-12, Q, oracle.electron_mass_ev())
+        ctx.track(steps)
+        Rn, Pn = ctx.download()
+    assert rel(Rg, Ro) < STATE_TOL and rel(Pg, Po) < STATE_TOL
+    assert st["path_length"] == tr.path_length
+    # the elements act: transverse momenta change well beyond the tolerance
+    assert rel(Pg[:, :2], Pn[:, :2]) > 1e-3
