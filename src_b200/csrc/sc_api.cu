@@ -513,6 +513,7 @@ int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
     cudaMemsetAsync(b.ticket, 0, 64, c->own);
     cudaMemsetAsync(b.st, 0, sizeof(StepState), c->own);
     fft_set_smem_limits();
+    prime_particle_grids();
     upload_twiddles(b, c->own);
     e = cudaStreamSynchronize(c->own);
     if (e == cudaSuccess) e = cudaGetLastError();

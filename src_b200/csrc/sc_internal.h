@@ -76,6 +76,7 @@ struct FftPlan {
 
 FftPlan make_plan(int L);
 int particle_grid(const DevBunch& b);
+void prime_particle_grids();  // occupancy of the particle kernels, before any capture
 
 // particle TU (sc_particles.cu)
 void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s);

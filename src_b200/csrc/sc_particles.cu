@@ -16,6 +16,8 @@
 //   k_gather_kick_push   CIC gather, B from E, back to the reference frame, Boris
 //                        kick, half drift, reference-frame update, momentum sums
 #include <cstdio>
+#include <mutex>
+#include <unordered_map>
 
 #include "sc_ddmath.cuh"
 #include "sc_exact.cuh"
@@ -1383,18 +1385,60 @@ void launch_batch(int kind, int precision, int threads, const DevBunch* tab, con
 
 int particle_grid(const DevBunch& b) { return b.red_blocks; }
 
+#ifndef SC_PARTICLE_WAVES
+#define SC_PARTICLE_WAVES 1
+#endif
+
+// Resident blocks of kThreads on the whole device for one kernel (the
+// occupancy query runs once per kernel, outside stream capture: contexts
+// call prime_particle_grids when they are created).
+int resident_blocks(const void* kernel) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(kernel);
+    if (it != cache.end()) return it->second;
+    int dev = 0, nsm = 0, k = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, kernel, kThreads, 0) != cudaSuccess || k < 1) k = 1;
+    cudaGetLastError();
+    return cache.emplace(kernel, k * nsm).first->second;
+}
+
+// Blocks for a particle loop (grid-stride, one reduction per block): the
+// blocks the SMs hold at once, SC_PARTICLE_WAVES times, so each block loops
+// over several particles and its set-up and reduction are paid once per
+// resident block; never more than b.red_blocks (the partials' size).
+template <typename K>
+int wave_grid(K kernel, const DevBunch& b) {
+    if (SC_PARTICLE_WAVES <= 0) return b.red_blocks;
+    const int blocks = resident_blocks((const void*)kernel) * SC_PARTICLE_WAVES;
+    return blocks < b.red_blocks ? blocks : b.red_blocks;
+}
+
+void prime_particle_grids() {
+    const void* kernels[] = {(const void*)k_drift_to_beam<true>,
+                             (const void*)k_drift_to_beam<false>,
+                             (const void*)k_deposit,
+                             (const void*)k_deposit_bins,
+                             (const void*)k_gather_kick_push<double, false>,
+                             (const void*)k_gather_kick_push<double, true>,
+                             (const void*)k_gather_kick_push<float, false>,
+                             (const void*)k_gather_kick_push<float, true>,
+                             (const void*)k_gather_kick_push_bins<false>,
+                             (const void*)k_gather_kick_push_bins<true>};
+    for (const void* k : kernels) resident_blocks(k);
+}
+
 void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s) {
     k_reduce_state<false><<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials,
                                                            b.ticket, init_frame);
 }
 
 void launch_drift_to_beam(const DevBunch& b, bool drift, cudaStream_t s) {
-    if (drift)
-        k_drift_to_beam<true><<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials,
-                                                                b.ticket);
-    else
-        k_drift_to_beam<false><<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials,
-                                                                 b.ticket);
+    auto k = drift ? k_drift_to_beam<true> : k_drift_to_beam<false>;
+    k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials, b.ticket);
 }
 
 void launch_advance_reference(const DevBunch& b, cudaStream_t s) { k_advance_reference<<<1, 32, 0, s>>>(b.bc, b.st); }
@@ -1405,7 +1449,7 @@ void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s) {
 }
 
 void launch_deposit(const DevBunch& b, cudaStream_t s) {
-    k_deposit<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
+    k_deposit<<<wave_grid(k_deposit, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
 }
 
 void launch_assemble_rho(const DevBunch& b, cudaStream_t s) {
@@ -1439,12 +1483,12 @@ void launch_gather_kick_push(const DevBunch& b, bool stats, cudaStream_t s) {
     const bool ext = b.bc.nsol > 0;
     if (b.precision == 0) {
         auto k = ext ? k_gather_kick_push<double, true> : k_gather_kick_push<double, false>;
-        k<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, (const double*)b.E4, b.st, b.partials,
-                                            b.ticket);
+        k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, (const double*)b.E4, b.st,
+                                               b.partials, b.ticket);
     } else {
         auto k = ext ? k_gather_kick_push<float, true> : k_gather_kick_push<float, false>;
-        k<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, (const float*)b.E4, b.st, b.partials,
-                                            b.ticket);
+        k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, (const float*)b.E4, b.st,
+                                               b.partials, b.ticket);
     }
     if (stats) launch_reduce_stats(b, s);
 }
@@ -1470,7 +1514,8 @@ void launch_bin_gammas(const DevBunch& b, cudaStream_t s) {
 }
 
 void launch_deposit_bins(const DevBunch& b, cudaStream_t s) {
-    k_deposit_bins<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.bin, b.nactive, b.st, b.nacc_bins);
+    k_deposit_bins<<<wave_grid(k_deposit_bins, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.bin, b.nactive, b.st,
+                                                                      b.nacc_bins);
 }
 
 void launch_grad_acc(const DevBunch& v, bool image, cudaStream_t s) {
@@ -1484,7 +1529,7 @@ void launch_grad_acc(const DevBunch& v, bool image, cudaStream_t s) {
 
 void launch_gather_kick_push_bins(const DevBunch& b, bool stats, cudaStream_t s) {
     auto k = b.bc.nsol > 0 ? k_gather_kick_push_bins<true> : k_gather_kick_push_bins<false>;
-    k<<<b.red_blocks, kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.F8, b.st, b.partials, b.ticket);
+    k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.F8, b.st, b.partials, b.ticket);
     if (stats) launch_reduce_stats(b, s);
 }
 

@@ -1,6 +1,7 @@
 // Host build of the device double-double log / atan (sc_ddmath.cuh) checked
 // against quad precision rounded once (libquadmath).  Prints one line:
 //   <n> <log mismatches> <atan mismatches> <libm log mismatches> <libm atan mismatches>
+//   <log quick != full> <atan quick != full> <log quick accepted> <atan quick accepted>
 // Arguments are log-uniform over the ranges the Green's function produces.
 #include <quadmath.h>
 
@@ -14,22 +15,30 @@ int main(int argc, char** argv) {
     const long n = argc > 1 ? std::atol(argv[1]) : 1000000;
     std::mt19937_64 g(12345);
     std::uniform_real_distribution<double> el(-30.0, 30.0), ea(-22.0, 22.0), sg(-1.0, 1.0);
-    long bl = 0, ba = 0, ll = 0, la = 0;
+    long bl = 0, ba = 0, ll = 0, la = 0, dl = 0, da = 0, ql = 0, qa = 0;
     for (long i = 0; i < n; ++i) {
         const double x = std::exp(el(g));
         const double lq = (double)logq((__float128)x);
-        bl += sc::ddm::log_dd(x) != lq;
+        const double l = sc::ddm::log_dd(x);
+        bl += l != lq;
         ll += std::log(x) != lq;
+        dl += l != sc::ddm::log_dd_full(x);
+        double r;
+        ql += sc::ddm::log_quick(x, r);
         const double y = (sg(g) < 0 ? -1.0 : 1.0) * std::exp(ea(g));
         const double aq = (double)atanq((__float128)y);
-        ba += sc::ddm::atan_dd(y) != aq;
+        const double t = sc::ddm::atan_dd(y);
+        ba += t != aq;
         la += std::atan(y) != aq;
+        da += t != sc::ddm::atan_dd_full(y);
+        // outside [2^-30, 2^30] the quick phase is not tried: count as decided
+        qa += !(std::fabs(y) >= 9.3132257461547852e-10 && std::fabs(y) <= 1073741824.0) || sc::ddm::atan_quick(y, r);
     }
     // a few exact cases
     bl += sc::ddm::log_dd(1.0) != 0.0;
     ba += sc::ddm::atan_dd(0.0) != 0.0;
     ba += sc::ddm::atan_dd(1.0) != (double)atanq((__float128)1.0);
     ba += sc::ddm::atan_dd(-1.0) != (double)atanq((__float128)-1.0);
-    std::printf("%ld %ld %ld %ld %ld\n", n, bl, ba, ll, la);
+    std::printf("%ld %ld %ld %ld %ld %ld %ld %ld %ld\n", n, bl, ba, ll, la, dl, da, ql, qa);
     return 0;
 }
