@@ -412,17 +412,18 @@ __device__ __forceinline__ void cic_charge(const double* d, double q, double* v)
 // Exact sums of the scattered charges (kFxFrac, fx_exponent, node_density in
 // sc_exact.cuh).
 
-// A fixed-point charge t (an integer-valued double, |t| < 2^51) as two exact
-// 32-bit limbs: hi = floor(t / 2^26) in [-2^25, 2^25), lo = t - hi 2^26 in
-// [0, 2^26).  Sums of up to 32 limbs fit 32 bits (|sum hi| < 2^30,
-// sum lo < 2^31) and recombine exactly in 64 bits.
+// A fixed-point charge t = rint(v) (|t| < 2^51; the conversion rounds half
+// to even, as rint) as two exact 32-bit limbs: hi = floor(t / 2^26) in
+// [-2^25, 2^25) (arithmetic shift), lo = t - hi 2^26 in [0, 2^26).  Sums of
+// up to 32 limbs fit 32 bits (|sum hi| < 2^30, sum lo < 2^31) and recombine
+// exactly in 64 bits.
 struct Limbs {
     int hi;
     unsigned lo;
 };
-__device__ __forceinline__ Limbs limbs_of(double t) {
-    const double h = floor(t * 0x1p-26);
-    return Limbs{__double2int_rz(h), __double2uint_rz(fma(-h, 0x1p26, t))};
+__device__ __forceinline__ Limbs limbs_of(double v) {
+    const long long t = __double2ll_rn(v);
+    return Limbs{(int)(t >> 26), (unsigned)(t & 0x3ffffffll)};
 }
 __device__ __forceinline__ long long join(long long hi, long long lo) { return hi * (1ll << 26) + lo; }
 
@@ -492,7 +493,7 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
         const double to_int = *fresh(&to_int_s);
         Limbs t[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) t[k] = limbs_of(rint(c[k] * to_int));
+        for (int k = 0; k < 8; ++k) t[k] = limbs_of(c[k] * to_int);
         const unsigned group = __match_any_sync(kFull, key);
         const int gsize = __popc(group);
         const bool leader = lane == __ffs(group) - 1;
@@ -714,9 +715,9 @@ __global__ void __launch_bounds__(kThreads) k_igf_G_img(int n0, int n1, int n2, 
 // of sc_exact.cuh (below 2^96 for gamma < 2^24) in six 16-bit limbs.  Lanes
 // of a warp with the same bin (match.any) sum their limbs with redux.sync
 // (at most 32 * 2^16 < 2^21 per limb) and the group's first lane adds them
-// to 64-bit shared counters, so no carry is lost for fewer than 2^48
-// particles and the mean does not depend on the particle order.  The last
-// block sums the block partials (all threads, one column per lane) and
+// to its warp's 64-bit shared counters, so no carry is lost for fewer than
+// 2^48 particles and the mean does not depend on the particle order.  The
+// last block sums the block partials (one column per thread) and
 // writes each bin's StepState: this step's mesh with the bin's gamma and the
 // scalars of computeSelfFields(bin) (PartBunch.cpp:173-185, :246-249).
 constexpr int kGammaLimbs = 6;
@@ -726,11 +727,13 @@ __global__ void __launch_bounds__(kThreads) k_bin_gammas(BunchConst bc, const do
                                                          const int* __restrict__ bin, int nbins, StepState* st,
                                                          StepState* __restrict__ bst,
                                                          unsigned long long* __restrict__ partials, unsigned* ticket) {
-    __shared__ unsigned long long acc[kMaxBins * kGammaCols];
+    // one set of counters per warp: a warp's group leaders hold distinct
+    // bins, so they add without atomics
+    __shared__ unsigned long long acc[kWarps][kMaxBins * kGammaCols];
     const int ncol = nbins * kGammaCols;
-    for (int e = threadIdx.x; e < ncol; e += blockDim.x) acc[e] = 0ull;
+    for (int e = threadIdx.x; e < kWarps * kMaxBins * kGammaCols; e += blockDim.x) (&acc[0][0])[e] = 0ull;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     bool bad = false;
     for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < bc.N; i0 += (long long)gridDim.x * blockDim.x) {
         const long long i = i0 + threadIdx.x;
@@ -753,21 +756,27 @@ __global__ void __launch_bounds__(kThreads) k_bin_gammas(BunchConst bc, const do
 #pragma unroll
         for (int q = 0; q < kGammaLimbs; ++q) sum[q] = __reduce_add_sync(group, limb[q]);
         if (b >= 0 && lane == __ffs(group) - 1) {
-            unsigned long long* a = acc + b * kGammaCols;
+            unsigned long long* a = acc[warp] + b * kGammaCols;
 #pragma unroll
-            for (int q = 0; q < kGammaLimbs; ++q) atomicAdd(a + q, (unsigned long long)sum[q]);
-            atomicAdd(a + kGammaLimbs, (unsigned long long)__popc(group));
+            for (int q = 0; q < kGammaLimbs; ++q) a[q] += (unsigned long long)sum[q];
+            a[kGammaLimbs] += (unsigned long long)__popc(group);
         }
     }
     if (bad) atomicOr(&st->err, kFlagBin);
     __syncthreads();
-    for (int e = threadIdx.x; e < ncol; e += blockDim.x) partials[(size_t)blockIdx.x * ncol + e] = acc[e];
+    for (int e = threadIdx.x; e < ncol; e += blockDim.x) {
+        unsigned long long t = 0ull;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) t += acc[w][e];
+        partials[(size_t)blockIdx.x * ncol + e] = t;
+    }
     if (!last_block(ticket, gridDim.x)) return;
     __shared__ unsigned long long tot[kMaxBins * kGammaCols];
-    for (int e = threadIdx.x; e < ncol; e += blockDim.x) tot[e] = 0ull;
-    __syncthreads();
-    for (long long e = threadIdx.x; e < (long long)gridDim.x * ncol; e += blockDim.x)
-        atomicAdd(&tot[e % ncol], __ldcg(partials + e));
+    for (int e = threadIdx.x; e < ncol; e += blockDim.x) {
+        unsigned long long t = 0ull;
+        for (int k = 0; k < (int)gridDim.x; ++k) t += __ldcg(partials + (size_t)k * ncol + e);
+        tot[e] = t;
+    }
     __syncthreads();
     for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
         const unsigned long long* t = tot + b * kGammaCols;
