@@ -34,6 +34,25 @@ int main(int argc, char** argv) {
         // outside [2^-30, 2^30] the quick phase is not tried: count as decided
         qa += !(std::fabs(y) >= 9.3132257461547852e-10 && std::fabs(y) <= 1073741824.0) || sc::ddm::atan_quick(y, r);
     }
+    // every table interval of both reductions, edges included, where the
+    // quick phases' error is largest (log near 1 +- 1/128, atan near j/64)
+    std::uniform_real_distribution<double> w(-1.0 / 128, 1.0 / 128);
+    for (long i = 0; i < n / 4; ++i) {
+        const double x = (45 + (int)(i % 47)) / 64.0 + w(g);
+        if (x > 0.0) {
+            const double lq = (double)logq((__float128)x);
+            const double l = sc::ddm::log_dd(x);
+            bl += l != lq;
+            dl += l != sc::ddm::log_dd_full(x);
+        }
+        double y = (i % 65) / 64.0 + w(g);
+        if (i & 1) y = 1.0 / y;
+        if (y != 0.0 && std::fabs(y) < 1e300) {
+            const double t = sc::ddm::atan_dd(y);
+            ba += t != (double)atanq((__float128)y);
+            da += t != sc::ddm::atan_dd_full(y);
+        }
+    }
     // a few exact cases
     bl += sc::ddm::log_dd(1.0) != 0.0;
     ba += sc::ddm::atan_dd(0.0) != 0.0;
