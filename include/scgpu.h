@@ -23,6 +23,8 @@
  *   scgpu_set_exchange
  *       the MPI reductions of a distributed bunch (get_bounds, calcMoments,
  *       the scatter into the distributed rho field) as an exchange callback
+ *   scgpu_set_reorder_interval
+ *       no counterpart (a tuning setting of this implementation's cell order)
  *   scgpu_set_periodic_z
  *       the bcz argument of FFTPoissonSolver (FieldSolver BCFFTZ, src/Structure/FieldSolver.cpp:431, :486)
  *   scgpu_compute_potential_image, scgpu_compute_potential_image_device
@@ -214,6 +216,15 @@ int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* 
  * the periodic particle boundary of a DC beam), energy bins and image
  * charges return SCGPU_ERR_UNSUPPORTED while it is on. */
 int scgpu_set_periodic_z(scgpu_ctx* ctx, int periodic);
+
+/* How often the tracker puts the particle arrays in cell order (a counting
+ * sort by the CIC cell, so that the deposit's warps share few cells): every
+ * `steps` steps of scgpu_track, counted from the upload; 0 never (the
+ * deposit then slows as the order decays; results do not change, the sums
+ * are exact).  Default 32, or the environment variable SCGPU_REORDER_EVERY
+ * at scgpu_create.  No counterpart in the reference, whose scatter runs in
+ * storage order. */
+int scgpu_set_reorder_interval(scgpu_ctx* ctx, int steps);
 
 /* PoissonSolver::computePotential(rho, hr, zshift): rho in, the potential of
  * its image charge out (in place, same units as scgpu_compute_potential):

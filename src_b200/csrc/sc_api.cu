@@ -718,6 +718,14 @@ int scgpu_set_exchange(scgpu_ctx* c, scgpu_exchange_fn fn, void* user, long long
     return SCGPU_OK;
 }
 
+// Interval of the cell reorder in scgpu_track (0: never); the step graphs
+// are keyed by whether a step reorders, so no graph is rebuilt.
+int scgpu_set_reorder_interval(scgpu_ctx* c, int steps) {
+    if (!c || steps < 0) return fail(c, SCGPU_ERR_ARG, "the reorder interval must be >= 0");
+    c->reorder_every = steps;
+    return SCGPU_OK;
+}
+
 // BCFFTZ=PERIODIC (FieldSolver.cpp:431, :486; FFTPoissonSolver.cpp:60,
 // :130-155, :189-190, :661-662): the solves of this context use a grid
 // doubled in x and y only and a cyclic convolution along z.

@@ -28,7 +28,7 @@ struct scgpu_ctx {
     double last_ms = 0.0;
     cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [stats][reorder]
     bool use_graphs = true;
-    int reorder_every = 16;   // put the particle arrays in cell order every k steps (0: never)
+    int reorder_every = 32;   // put the particle arrays in cell order every k steps (0: never)
     long long steps_done = 0; // steps since the last upload
     size_t smem_fft = 0;
     // energy bins and image charges (buffers allocated on first use)

@@ -107,8 +107,8 @@ def test_self_fields_binned_linearity_full_size(gpu):
 
 @pytest.mark.parametrize("N,nr,nbins,steps", [(20_000, (16, 16, 16), 4, 5), (50_000, (32, 32, 32), 6, 20)])
 def test_tracking_binned_vs_oracle(oracle, gpu, N, nr, nbins, steps):
-    """The step loop with energy bins (20 steps cross the every-16-steps cell
-    reorder, so the bins must travel with their particles)."""
+    """The step loop with energy bins (a reorder every 7 steps: the bins must
+    travel with their particles)."""
     R, P, bins = photoinjector_bunch(N, nbins=nbins, bunch_id=nbins)
     Q = -1e-9 / N
     tr = oracle.OracleTracker(oracle.make_params(nr, 1e-12, ref_pz=1.0), Q)
@@ -117,6 +117,7 @@ def test_tracking_binned_vs_oracle(oracle, gpu, N, nr, nbins, steps):
     with gpu.Context(nr) as c:
         c.upload(R, P, 1e-12, Q, oracle.electron_mass_ev(), ref_P=(0.0, 0.0, 1.0))
         c.set_energy_bins(bins, nbins)
+        c.set_reorder_interval(7)
         c.track(steps)
         Rg, Pg = c.download()
         st = c.tracker_state()
