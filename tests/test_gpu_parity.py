@@ -166,6 +166,28 @@ def test_deterministic_bitwise(gpu, oracle):
         np.testing.assert_array_equal(a, b)
 
 
+def test_reorder_interval_does_not_change_results(gpu, oracle):
+    """The deposit's node sums and the momentum / moment sums are exact
+    integers, so the particle order cannot show in any result: a cell
+    reorder every step, every 7 steps or never gives the same bits."""
+    N = 60_000
+    R, P = gaussian_bunch(N, bunch_id=11)
+    outs = []
+    for k in (1, 7, 0):
+        with gpu.Context((24, 24, 24)) as c:
+            c.set_reorder_interval(k)
+            c.upload(R, P, 1e-12, -1e-9 / N, oracle.electron_mass_ev())
+            stats = np.zeros((12, gpu.NSTATS))
+            c.track(12, stats)
+            outs.append((*c.download(), c.field(gpu.FIELD_RHO), c.field(gpu.FIELD_E), stats))
+            with pytest.raises(gpu.ScgpuError) as e:
+                c.set_reorder_interval(-1)
+            assert e.value.code == -1
+    for o in outs[1:]:
+        for a, b in zip(outs[0], o):
+            np.testing.assert_array_equal(a, b)
+
+
 def test_stats_records_match_beam_parameters(gpu, oracle):
     R, P = gaussian_bunch(50_000, bunch_id=6)
     with gpu.Context((16, 16, 16)) as c:

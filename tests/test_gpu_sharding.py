@@ -23,6 +23,7 @@ MASS = 0.51099892e6
 
 def _single(gpu, R, P, nr, steps, Q):
     with gpu.Context(nr) as c:
+        c.set_reorder_interval(7)
         c.upload(R, P, 1e-12, Q, MASS)
         stats = np.zeros((steps, gpu.NSTATS))
         c.track(steps, stats)
@@ -43,6 +44,7 @@ def _sharded(gpu, R, P, nr, steps, Q, bounds):
             lo, hi = bounds[r], bounds[r + 1]
             with gpu.Context(nr) as c:
                 attach(c, ex.callback(r), R.shape[0])
+                c.set_reorder_interval(5)  # the shards reorder at other steps than the whole bunch
                 c.upload(R[lo:hi], P[lo:hi], 1e-12, Q, MASS)
                 stats = np.zeros((steps, gpu.NSTATS))
                 c.track(steps, stats)
