@@ -75,7 +75,7 @@ void drop_graphs(scgpu_ctx* c) {
 void free_bins(scgpu_ctx* c) {
     DevBunch& b = c->b;
     dfree(b.bin); dfree(b.bin_alt); dfree(b.bst); dfree(b.nacc_bins); dfree(b.bin_partials); dfree(b.F8);
-    dfree(c->spec_fwd_buf); dfree(c->ghat_alt); dfree(c->ghat_img_alt);
+    dfree(c->spec_fwd_buf); dfree(c->ghat_alt); dfree(c->ghat_img_alt); dfree(c->phi_img_buf);
     dfree(b.gtmp_img); dfree(b.gimg); dfree(b.ghat_img);
     for (int k = 0; k < kMaxBins; ++k) {
         if (c->ev_bin[k]) cudaEventDestroy(c->ev_bin[k]);
@@ -119,7 +119,8 @@ int ensure_bins(scgpu_ctx* c, int nbins) {
     if (!b.bst) {
         if ((rc = dalloc(c, &b.bst, kMaxBins * sizeof(StepState))) ||
             (rc = dalloc(c, &b.bin_partials, 296 * kMaxBins * 8 * sizeof(unsigned long long))) ||
-            (rc = dalloc(c, &b.F8, M * 8 * sizeof(double))) || (rc = dalloc(c, (char**)&c->ghat_alt, G3 * rs)) ||
+            (rc = dalloc(c, &b.F8, M * 8 * sizeof(double))) || (rc = dalloc(c, &c->phi_img_buf, M * sizeof(double))) ||
+            (rc = dalloc(c, (char**)&c->ghat_alt, G3 * rs)) ||
             (rc = dalloc(c, (char**)&c->ghat_img_alt, G3 * cs)))
             return rc;
         if (b.precision == SCGPU_PLAIN_FP64 && (rc = dalloc(c, (char**)&c->spec_fwd_buf, S * sizeof(double2))))
@@ -190,9 +191,10 @@ void enqueue_bins_fields(scgpu_ctx* c, cudaStream_t s) {
         launch_convolution_part(v, kConvSelfField, kConvForwardPart, s);
         cudaStreamWaitEvent(s, c->ev_bin[k], 0);
         launch_convolution_part(v, kConvSelfField, kConvRestPart, s);
-        launch_grad_acc(v, false, s);
-        launch_convolution_part(v, kConvSelfField, kConvImagePart, s);
-        launch_grad_acc(v, true, s);
+        DevBunch vi = v;  // the image's potential into its own buffer
+        vi.phi = c->phi_img_buf;
+        launch_convolution_part(vi, kConvSelfField, kConvImagePart, s);
+        launch_grad_acc(v, c->phi_img_buf, s);
         cudaEventRecord(c->ev_used[k], s);
     }
 }

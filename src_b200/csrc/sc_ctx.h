@@ -38,6 +38,7 @@ struct scgpu_ctx {
     void* spec_fwd_buf = nullptr; // plain form: forward spectrum of a bin
     void* ghat_alt = nullptr;     // second spectrum buffers: the side stream builds bin k+1's Green's
     void* ghat_img_alt = nullptr; // functions while the main stream convolves bin k
+    double* phi_img_buf = nullptr; // the image's potential of the bin being convolved
     cudaEvent_t ev_bin[sc::kMaxBins] = {};
     cudaEvent_t ev_used[sc::kMaxBins] = {};
     // beamline elements (scgpu_add_solenoid): host copy and device table

@@ -116,9 +116,10 @@ constexpr int kMaxBins = 64;
 void launch_bin_gammas(const DevBunch& b, cudaStream_t s);
 // one pass over the particles: the charge of every active bin into its own accumulators
 void launch_deposit_bins(const DevBunch& b, cudaStream_t s);
-// -grad phi of one bin's potential (view.st = its StepState), added into F8:
-// E, and B = -+ betaC (E_y, -E_x) (PartBunch.cpp:238-244, image :417-427)
-void launch_grad_acc(const DevBunch& view, bool image, cudaStream_t s);
+// -grad phi of one bin's potential (view.phi) and of its image's (phi_img)
+// (view.st = the bin's StepState), added into F8 in that order: E, and
+// B = -+ betaC (E_y, -E_x) (PartBunch.cpp:238-244, image :417-427)
+void launch_grad_acc(const DevBunch& view, const double* phi_img, cudaStream_t s);
 void launch_gather_kick_push_bins(const DevBunch& b, bool stats, cudaStream_t s);
 void launch_gather_fields_bins(const DevBunch& b, cudaStream_t s);
 // bin of every slot from a host-order array (slot s holds particle id[s])

@@ -813,12 +813,33 @@ __global__ void __launch_bounds__(kThreads) k_bin_gammas(BunchConst bc, const do
     if (threadIdx.x == 0) *ticket = 0u;
 }
 
-// -grad phi of one bin (UniformCartesian.hpp:2129-2203, scaled by the bin's
-// (g, g, 1/g), PartBunch.cpp:199-200) added into F8; B of the bin's charge
-// -betaC E_y, +betaC E_x (:238-239), of its image the opposite (:426-427).
-template <bool IMAGE>
-__global__ void __launch_bounds__(kThreads) k_grad_acc(BunchConst bc, const StepState* __restrict__ st,
-                                                       const double* __restrict__ phi, double* __restrict__ F8) {
+// -grad phi (UniformCartesian.hpp:2129-2203, scaled by the bin's (g, g, 1/g),
+// PartBunch.cpp:199-200) of one node of a potential.
+__device__ __forceinline__ void neg_grad_scaled(const double* __restrict__ phi, int c, const int (&idx)[3],
+                                                const int (&n)[3], const int (&stv)[3], const double (&id)[3],
+                                                const double (&sc)[3], double (&e)[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double* f = phi + c;
+        const int s = stv[d];
+        double g;
+        if (idx[d] == 0)
+            g = id[d] * (-1.0 * f[2 * s] + 4.0 * f[s] - 3.0 * f[0]);
+        else if (idx[d] == n[d] - 1)
+            g = id[d] * (1.0 * f[-2 * s] - 4.0 * f[-s] + 3.0 * f[0]);
+        else
+            g = id[d] * (f[s] - f[-s]);
+        e[d] = (-g) * sc[d];
+    }
+}
+
+// One bin's fields added into F8: first its own charge's E and B =
+// (-betaC E_y, +betaC E_x) (:238-239), then its image's E and B = (+betaC
+// E_y, -betaC E_x) (:426-427) -- the additions in the order of two separate
+// passes, in one read and write of F8.
+__global__ void __launch_bounds__(kThreads, 4) k_grad_acc(BunchConst bc, const StepState* __restrict__ st,
+                                                       const double* __restrict__ phi,
+                                                       const double* __restrict__ phi_img, double* __restrict__ F8) {
     const int n[3] = {bc.n[0], bc.n[1], bc.n[2]};
     const int M = n[0] * n[1] * n[2];
     const int stv[3] = {1, n[0], n[0] * n[1]};
@@ -829,20 +850,9 @@ __global__ void __launch_bounds__(kThreads) k_grad_acc(BunchConst bc, const Step
     const double betaC = st->betaC;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < M; c += gridDim.x * blockDim.x) {
         const int idx[3] = {c % n[0], (c / n[0]) % n[1], c / (n[0] * n[1])};
-        double e[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double* f = phi + c;
-            const int s = stv[d];
-            double g;
-            if (idx[d] == 0)
-                g = id[d] * (-1.0 * f[2 * s] + 4.0 * f[s] - 3.0 * f[0]);
-            else if (idx[d] == n[d] - 1)
-                g = id[d] * (1.0 * f[-2 * s] - 4.0 * f[-s] + 3.0 * f[0]);
-            else
-                g = id[d] * (f[s] - f[-s]);
-            e[d] = (-g) * sc[d];
-        }
+        double e[3], ei[3];
+        neg_grad_scaled(phi, c, idx, n, stv, id, sc, e);
+        neg_grad_scaled(phi_img, c, idx, n, stv, id, sc, ei);
         double* o = F8 + 8 * (size_t)c;
         double2 exy = *reinterpret_cast<const double2*>(o);
         double2 ez = *reinterpret_cast<const double2*>(o + 2);
@@ -850,13 +860,13 @@ __global__ void __launch_bounds__(kThreads) k_grad_acc(BunchConst bc, const Step
         exy.x = exy.x + e[0];
         exy.y = exy.y + e[1];
         ez.x = ez.x + e[2];
-        if (IMAGE) {
-            bxy.x = bxy.x + betaC * e[1];
-            bxy.y = bxy.y - betaC * e[0];
-        } else {
-            bxy.x = bxy.x - betaC * e[1];
-            bxy.y = bxy.y + betaC * e[0];
-        }
+        bxy.x = bxy.x - betaC * e[1];
+        bxy.y = bxy.y + betaC * e[0];
+        exy.x = exy.x + ei[0];
+        exy.y = exy.y + ei[1];
+        ez.x = ez.x + ei[2];
+        bxy.x = bxy.x + betaC * ei[1];
+        bxy.y = bxy.y - betaC * ei[0];
         *reinterpret_cast<double2*>(o) = exy;
         *reinterpret_cast<double2*>(o + 2) = ez;
         *reinterpret_cast<double2*>(o + 4) = bxy;
@@ -1527,13 +1537,10 @@ void launch_deposit_bins(const DevBunch& b, cudaStream_t s) {
                                                                       b.nacc_bins);
 }
 
-void launch_grad_acc(const DevBunch& v, bool image, cudaStream_t s) {
+void launch_grad_acc(const DevBunch& v, const double* phi_img, cudaStream_t s) {
     const long long M = (long long)v.bc.n[0] * v.bc.n[1] * v.bc.n[2];
     const int g = grid_for(M, 148 * 16);
-    if (image)
-        k_grad_acc<true><<<g, kThreads, 0, s>>>(v.bc, v.st, v.phi, v.F8);
-    else
-        k_grad_acc<false><<<g, kThreads, 0, s>>>(v.bc, v.st, v.phi, v.F8);
+    k_grad_acc<<<g, kThreads, 0, s>>>(v.bc, v.st, v.phi, phi_img, v.F8);
 }
 
 void launch_gather_kick_push_bins(const DevBunch& b, bool stats, cudaStream_t s) {
