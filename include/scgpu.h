@@ -25,6 +25,8 @@
  *       the scatter into the distributed rho field) as an exchange callback
  *   scgpu_set_reorder_interval
  *       no counterpart (a tuning setting of this implementation's cell order)
+ *   scgpu_kernels_per_step, scgpu_launch_count, scgpu_profile_track
+ *       no counterpart (measurement of this implementation)
  *   scgpu_set_periodic_z
  *       the bcz argument of FFTPoissonSolver (FieldSolver BCFFTZ, src/Structure/FieldSolver.cpp:431, :486)
  *   scgpu_compute_potential_image, scgpu_compute_potential_image_device
@@ -330,6 +332,12 @@ double scgpu_last_track_ms(const scgpu_ctx* ctx);
 int scgpu_profile_track(scgpu_ctx* ctx, int nsteps, double* phase_ms);
 /* number of kernels one tracking step launches (from the step's CUDA graph) */
 int scgpu_kernels_per_step(scgpu_ctx* ctx);
+/* kernels scgpu_track has launched on this context so far, reorder and
+ * statistics steps included (the kernel nodes of the step graphs it ran);
+ * SCGPU_ERR_UNSUPPORTED once a step ran outside a graph (a sharded bunch
+ * with a host-side exchange).  No counterpart in the reference: the
+ * benchmark's count of device launches. */
+int scgpu_launch_count(scgpu_ctx* ctx, long long* kernels);
 
 /* ------------------------------------------------------------------ batches
  * Many independent bunches that step together: every batched step launches

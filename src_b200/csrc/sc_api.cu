@@ -336,12 +336,28 @@ void enqueue_any_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
         enqueue_step(c, stats, reorder, s);
 }
 
+// Kernel nodes of a captured graph.
+int graph_kernel_nodes(cudaGraph_t g) {
+    size_t nn = 0;
+    cudaGraphGetNodes(g, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    cudaGraphGetNodes(g, nodes.data(), &nn);
+    int kernels = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nd, &t);
+        if (t == cudaGraphNodeTypeKernel) ++kernels;
+    }
+    return kernels;
+}
+
 int build_graph(scgpu_ctx* c, bool stats, bool reorder, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
     enqueue_any_step(c, stats, reorder, c->own);
     cudaError_t e = cudaStreamEndCapture(c->own, &g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+    (c->b.nbins > 0 ? c->graph_kernels_bins : c->graph_kernels)[stats ? 1 : 0][reorder ? 1 : 0] = graph_kernel_nodes(g);
     e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
@@ -1031,8 +1047,10 @@ int scgpu_track(scgpu_ctx* c, int nsteps, double* stats) {
                 if (rc) return rc;
             }
             CK(cudaGraphLaunch(gx, s));
+            c->kernels_launched += (c->b.nbins > 0 ? c->graph_kernels_bins : c->graph_kernels)[want ? 1 : 0][reorder ? 1 : 0];
         } else {
             enqueue_any_step(c, want, reorder, s);
+            c->kernels_uncounted = true;
         }
         ++c->steps_done;
         if (want)
@@ -1275,18 +1293,18 @@ int scgpu_kernels_per_step(scgpu_ctx* c) {
     CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
     enqueue_any_step(c, false, false, c->own);
     CK(cudaStreamEndCapture(c->own, &g));
-    size_t nn = 0;
-    cudaGraphGetNodes(g, nullptr, &nn);
-    std::vector<cudaGraphNode_t> nodes(nn);
-    cudaGraphGetNodes(g, nodes.data(), &nn);
-    int kernels = 0;
-    for (auto nd : nodes) {
-        cudaGraphNodeType t;
-        cudaGraphNodeGetType(nd, &t);
-        if (t == cudaGraphNodeTypeKernel) ++kernels;
-    }
+    const int kernels = graph_kernel_nodes(g);
     cudaGraphDestroy(g);
     return kernels;
+}
+
+// Kernels launched by scgpu_track on this context so far (reorder and
+// statistics steps included), counted from the nodes of the step graphs.
+int scgpu_launch_count(scgpu_ctx* c, long long* kernels) {
+    if (!c || !kernels) return fail(c, SCGPU_ERR_ARG, "bad argument");
+    if (c->kernels_uncounted) return fail(c, SCGPU_ERR_UNSUPPORTED, "steps ran outside step graphs");
+    *kernels = c->kernels_launched;
+    return SCGPU_OK;
 }
 
 }  // extern "C"

@@ -27,6 +27,10 @@ struct scgpu_ctx {
     std::string err;
     double last_ms = 0.0;
     cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [stats][reorder]
+    int graph_kernels[2][2] = {{0, 0}, {0, 0}};       // kernel nodes of each step graph
+    int graph_kernels_bins[2][2] = {{0, 0}, {0, 0}};
+    long long kernels_launched = 0;   // kernels of the steps scgpu_track launched as graphs
+    bool kernels_uncounted = false;   // a step ran outside a graph (host exchange)
     bool use_graphs = true;
     int reorder_every = 32;   // put the particle arrays in cell order every k steps (0: never)
     long long steps_done = 0; // steps since the last upload

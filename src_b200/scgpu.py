@@ -110,6 +110,7 @@ def lib():
         L.scgpu_get_bin_gammas.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong)]
         L.scgpu_set_periodic_z.argtypes = [C.c_void_p, C.c_int]
         L.scgpu_set_reorder_interval.argtypes = [C.c_void_p, C.c_int]
+        L.scgpu_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
         L.scgpu_set_exchange.argtypes = [C.c_void_p, EXCHANGE_FN, C.c_void_p, C.c_longlong, C.c_int]
         L.scgpu_add_solenoid.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double]
         L.scgpu_clear_elements.argtypes = [C.c_void_p]
@@ -138,7 +139,7 @@ EXPORTED = [
     "scgpu_get_bin_gammas", "scgpu_stat_row", "scgpu_stat_column_name", "scgpu_sdds_write_header",
     "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
     "scgpu_set_periodic_z", "scgpu_set_exchange", "scgpu_add_solenoid", "scgpu_clear_elements",
-    "scgpu_fieldmap_astra1d", "scgpu_set_reorder_interval",
+    "scgpu_fieldmap_astra1d", "scgpu_set_reorder_interval", "scgpu_launch_count",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
@@ -209,6 +210,12 @@ class Context:
 
     def clear_elements(self):
         self._check(lib().scgpu_clear_elements(self.h), "clear_elements")
+
+    def launch_count(self):
+        """Kernels scgpu_track has launched on this context so far."""
+        n = C.c_longlong(0)
+        self._check(lib().scgpu_launch_count(self.h, C.byref(n)), "launch_count")
+        return int(n.value)
 
     def set_reorder_interval(self, steps):
         """Cell reorder every `steps` tracked steps (0: never); results do not change."""

@@ -58,6 +58,7 @@ def test_null_arguments_are_rejected():
     assert L.scgpu_set_stream(None, None) == -1
     assert L.scgpu_track(None, 1, None) == -1
     assert L.scgpu_set_reorder_interval(None, 8) == -1
+    assert L.scgpu_launch_count(None, None) == -1
     out = scgpu.BeamParams()
     assert L.scgpu_beam_parameters_from_stats(None, 10, C.byref(out)) == -1
 
