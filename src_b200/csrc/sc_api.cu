@@ -358,7 +358,7 @@ int build_graph(scgpu_ctx* c, bool stats, bool reorder, cudaGraphExec_t* out) {
     cudaError_t e = cudaStreamEndCapture(c->own, &g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
     (c->b.nbins > 0 ? c->graph_kernels_bins : c->graph_kernels)[stats ? 1 : 0][reorder ? 1 : 0] = graph_kernel_nodes(g);
-    e = cudaGraphInstantiate(out, g, 0);
+    e = cudaGraphInstantiate(out, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
     return SCGPU_OK;
@@ -516,9 +516,15 @@ int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
             return rc;
         }
     }
-    cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
-    cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
-    cudaStreamCreateWithFlags(&c->ref, cudaStreamNonBlocking);
+    // the step's main chain (captured on `own`) and the reference particle
+    // at the highest priority, the Green's-function branch at the lowest, so
+    // the branch fills the SMs the main chain leaves free (the step graphs
+    // keep the priorities: cudaGraphInstantiateFlagUseNodePriority)
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    cudaStreamCreateWithPriority(&c->own, cudaStreamNonBlocking, prio_high);
+    cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_low);
+    cudaStreamCreateWithPriority(&c->ref, cudaStreamNonBlocking, prio_high);
     c->stream = c->own;
     cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
