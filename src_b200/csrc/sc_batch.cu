@@ -281,7 +281,7 @@ int launch(scgpu_batch* b, int nsteps) {
             enqueue_step(b, reorder);
             cudaError_t e = cudaStreamEndCapture(b->stream, &g);
             if (e != cudaSuccess) return bfail(b, SCGPU_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&gx, g, 0);
+            e = cudaGraphInstantiate(&gx, g, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return bfail(b, SCGPU_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
         }
@@ -363,9 +363,11 @@ int scgpu_batch_create(scgpu_batch** out, int device, int precision) {
     int least = 0, greatest = 0;
     cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if (cudaStreamCreateWithPriority(&b->xfer, cudaStreamNonBlocking, greatest) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->ref, cudaStreamNonBlocking) != cudaSuccess ||
+        // the main chain at the highest priority, the Green's functions at the
+        // lowest (kept in the step graphs: cudaGraphInstantiateFlagUseNodePriority)
+        cudaStreamCreateWithPriority(&b->stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, least) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&b->ref, cudaStreamNonBlocking, greatest) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_ref, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
