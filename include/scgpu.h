@@ -153,7 +153,11 @@ int scgpu_abi_version(void);
 int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* params, int device);
 void scgpu_destroy(scgpu_ctx* ctx);
 const char* scgpu_last_error(const scgpu_ctx* ctx);
-/* run on a caller-owned cudaStream_t (passed as void*); NULL = the context's own stream */
+/* run on a caller-owned cudaStream_t (passed as void*); NULL = the context's own stream.
+ * scgpu_track launches its step graphs on that stream; the kernels inside keep
+ * the graph's own priorities (the main chain at the device's highest stream
+ * priority, the Green's-function branch at the lowest), whatever the
+ * priority of the caller's stream. */
 int scgpu_set_stream(scgpu_ctx* ctx, void* cuda_stream);
 int scgpu_synchronize(scgpu_ctx* ctx);
 
