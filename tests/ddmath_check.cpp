@@ -2,6 +2,7 @@
 // against quad precision rounded once (libquadmath).  Prints one line:
 //   <n> <log mismatches> <atan mismatches> <libm log mismatches> <libm atan mismatches>
 //   <log quick != full> <atan quick != full> <log quick accepted> <atan quick accepted>
+//   <Green's-function arguments> <of them decided by the quick phases>
 // Arguments are log-uniform over the ranges the Green's function produces.
 #include <quadmath.h>
 
@@ -58,6 +59,25 @@ int main(int argc, char** argv) {
     ba += sc::ddm::atan_dd(0.0) != 0.0;
     ba += sc::ddm::atan_dd(1.0) != (double)atanq((__float128)1.0);
     ba += sc::ddm::atan_dd(-1.0) != (double)atanq((__float128)-1.0);
-    std::printf("%ld %ld %ld %ld %ld %ld %ld %ld %ld\n", n, bl, ba, ll, la, dl, da, ql, qa);
+    // the arguments the integrated Green's function evaluates: ln(x + r) and
+    // atan(x y / (z r)) at the cell-corner offsets of a 40^3 grid with
+    // unequal spacings (FFTPoissonSolver.cpp:472-493)
+    long garg = 0, gquick = 0;
+    const double h[3] = {1.1e-4, 0.9e-4, 3.7e-4};
+    for (int i = 0; i < 40; ++i)
+        for (int j = 0; j < 40; ++j)
+            for (int k = 0; k < 40; ++k) {
+                const double x = i * h[0] - h[0] / 2, y = j * h[1] - h[1] / 2, z = k * h[2] - h[2] / 2;
+                const double r = std::sqrt(x * x + y * y + z * z);
+                double o;
+                const double log_args[3] = {x + r, y + r, z + r};
+                const double atan_args[3] = {x * y / (z * r), x * z / (y * r), y * z / (x * r)};
+                for (int m = 0; m < 3; ++m) {
+                    garg += 2;
+                    gquick += sc::ddm::log_quick(log_args[m], o);
+                    gquick += sc::ddm::atan_quick(atan_args[m], o);
+                }
+            }
+    std::printf("%ld %ld %ld %ld %ld %ld %ld %ld %ld %ld %ld\n", n, bl, ba, ll, la, dl, da, ql, qa, garg, gquick);
     return 0;
 }
