@@ -42,6 +42,7 @@ WORKLOADS = {
                                  "uniform solenoid B_z = 0.2 T"),
 }
 N_PARTICLES, MESH, BZ, WORKLOAD = WORKLOADS["c2"]
+REORDER_EVERY = 32  # the library's default cell-reorder interval
 
 
 def algorithmic_bytes(N, n, precision):
@@ -78,15 +79,43 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic(kernel):
-    """DRAM bytes per launch of a kernel from the committed ncu summary."""
+def committed_traffic(kernel, workload, precision):
+    """DRAM bytes per launch of a kernel from the committed ncu summary of
+    the same workload and precision (None when that capture does not exist)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         t = json.load(f)
-    v = t.get(kernel)
+    v = t.get(f"{workload}/{precision}", {}).get(kernel)
     return None if v is None else float(v)
+
+
+def reorder_cost_ms(ctx, stream, flush, every, steps_done, rounds=2, plain=3):
+    """Extra device time of a step that also puts the particles in cell
+    order: a reorder step against the plain steps that follow it, L2 flushed
+    before each, averaged over `rounds` reorder intervals.  Returns (ms,
+    steps advanced)."""
+    import torch
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    extra, advanced = [], 0
+    for _ in range(rounds):
+        k = (-(steps_done + advanced)) % every
+        if k:
+            ctx.track(k)
+            advanced += k
+        t = []
+        for _ in range(1 + plain):
+            flush.zero_()
+            ev[0].record(stream)
+            ctx.track(1)
+            ev[1].record(stream)
+            ev[1].synchronize()
+            t.append(ev[0].elapsed_time(ev[1]))
+            advanced += 1
+        extra.append(t[0] - sum(t[1:]) / plain)
+    return max(0.0, sum(extra) / rounds), advanced
 
 
 class ClockSampler:
@@ -212,6 +241,35 @@ def cpu_baseline_single(target_s=12.0):
                       f"({'reference FFTPACK' if not O.fft_engine_is_own() else 'oracle FFT'} engine)"}
 
 
+def cpu_baseline_c1(target_s=6.0):
+    """The CPU figures of the 1e5-particle / 32^3 workload (c1): the oracle
+    port with the reference's FFTPACK on 1 core and on all host threads,
+    bounded samples of the 100-step run."""
+    from oracle import oracle as O
+    from src_b200.bunch import config_bunch
+
+    if O.reference_fft_available():
+        O.use_reference_fft(True)
+    b = config_bunch("c1")
+    out = {}
+    for label, threads in (("1_core", 1), ("all_cores", O.lib().sco_max_threads())):
+        O.lib().sco_set_threads(threads)
+        tr = O.OracleTracker(O.make_params(b["nr"], b["dT"]), b["Q"])
+        R, P = b["R"].copy(), b["P"].copy()
+        t0 = time.perf_counter()
+        tr.track(R, P, 1)
+        one = time.perf_counter() - t0
+        steps = max(1, min(b["steps"] - 1, int(target_s / max(one, 1e-3))))
+        t0 = time.perf_counter()
+        tr.track(R, P, steps)
+        el = time.perf_counter() - t0
+        out[label] = {"value": b["N"] * steps / el, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                      "sample": f"steps 2-{steps + 1} of the 100-step 1e5-particle / 32^3 run "
+                                f"({'reference FFTPACK' if not O.fft_engine_is_own() else 'oracle FFT'} engine)"}
+    O.lib().sco_set_threads(1)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -273,6 +331,7 @@ def main():
     ctx = scgpu.Context((MESH, MESH, MESH), precision=prec, device=local)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
+    ctx.set_reorder_interval(REORDER_EVERY)
     ctx.upload(R, P, DT, Q, mass, bz_ext=BZ)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
@@ -302,7 +361,15 @@ def main():
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
-    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    ms_measured = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    # The cell reorder runs every REORDER_EVERY steps counted from the
+    # upload; a window of K steps holds K / REORDER_EVERY of them on average
+    # but may hold none or one.  The whole job's rate counts the average:
+    # the window's own reorders are exchanged for K / REORDER_EVERY times
+    # the measured cost of one.
+    in_window = sum(1 for k in range(args.warmup, args.warmup + args.steps) if k % REORDER_EVERY == 0)
+    reorder_ms, _ = reorder_cost_ms(ctx, stream, flush, REORDER_EVERY, args.warmup + args.steps)
+    ms = ms_measured + (args.steps / REORDER_EVERY - in_window) * reorder_ms
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -319,7 +386,7 @@ def main():
     dom = max((k for k in phases if k in SINGLE_KERNEL_PHASES), key=phases.get)
     dom_ms = phases[dom] / nprof
     achieved = phase_bytes[dom] / (dom_ms * 1e-3) / 1e9
-    traffic = committed_traffic(dom)
+    traffic = committed_traffic(dom, args.workload, args.precision)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes": phase_bytes[dom], "avg_launch_ms": dom_ms}
@@ -368,9 +435,10 @@ def main():
     job_value = N_PARTICLES * job_steps / (e0.elapsed_time(e1) * 1e-3)
 
     ctx.close()
-    cpu = None
+    cpu = cpu_c1 = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "c2":
         cpu = cpu_baseline_single()
+        cpu_c1 = cpu_baseline_c1()
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -396,7 +464,11 @@ def main():
         "kernels_per_step": kernels,
         "clocks": clk,
         "wall_s_timed_region": wall,
+        "reorder": {"interval": REORDER_EVERY, "in_window": in_window, "cost_ms": reorder_ms,
+                    "ms_per_step_measured": ms_measured / args.steps,
+                    "note": "value counts K / interval reorders at the measured cost in place of the window's own"},
         "cpu_baseline": cpu,
+        "cpu_baseline_c1": cpu_c1,
     }
     print(json.dumps(line), flush=True)
 

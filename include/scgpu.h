@@ -166,6 +166,9 @@ int scgpu_synchronize(scgpu_ctx* ctx);
  * i.e. phi * 4 pi eps0 / (hx hy hz) in the reference's units.  hr is the
  * rest-frame mesh spacing. */
 int scgpu_compute_potential(scgpu_ctx* ctx, double* rho_inout, const double hr[3]);
+/* the same on a device buffer of the context's GPU (device or managed memory
+ * holding nx*ny*nz doubles); anything else returns SCGPU_ERR_ARG before any
+ * work is enqueued */
 int scgpu_compute_potential_device(scgpu_ctx* ctx, double* rho_inout_device, const double hr[3]);
 
 /* PartBunch::computeSelfFields on a bunch already in the beam frame: boundp,
@@ -398,16 +401,23 @@ int scgpu_batch_autotune(scgpu_batch* batch, int trial_steps);
  * synchronisation of cudaMalloc / cudaFree.  It has no counterpart in the
  * reference.  No context is needed and nothing is allocated: rho_dev
  * (nx*ny*nz doubles, x fastest) and phi_dev (same size; may equal rho_dev)
- * are the caller's device buffers on the current device, and the scratch is
- * a 4 MiB array inside the library that every GPU loading the library keeps
- * until the process exits.  Limits: at most 32 cells per axis (and 2n
- * factoring into 2, 3, 5); larger meshes return SCGPU_ERR_UNSUPPORTED.  The
- * first call on a device looks up that array's device address
- * (cudaGetSymbolAddress) with the device current; make that first call before
- * any stream capture.  Every call shares the one array, so calls that overlap
- * on the GPU (different streams, or several host threads) race; serialise
- * them on one stream.  The work is enqueued on cuda_stream (a cudaStream_t,
- * NULL for the default stream) and returns without synchronising. */
+ * are the caller's device buffers on the current device (a host pointer, a
+ * buffer of another GPU or one smaller than the mesh returns SCGPU_ERR_ARG
+ * before anything is enqueued), and the scratch is a 4 MiB array inside the
+ * library that every GPU loading the library keeps until the process exits.
+ * Limits: at most 32 cells per axis (and 2n factoring into 2, 3, 5); larger
+ * meshes return SCGPU_ERR_UNSUPPORTED.  The first call on a device sets it
+ * up with the device current: it looks up the arrays' device addresses
+ * (cudaGetSymbolAddress) and writes the library's twiddle table with one
+ * synchronous copy; make that first call before any stream capture.  The
+ * results are bitwise those of scgpu_compute_potential_device in the plain
+ * form.  Every call shares the one scratch array, so calls that overlap on
+ * the GPU (different streams, or several host threads) race; serialise them
+ * on one stream.  The work is enqueued on cuda_stream (a cudaStream_t, NULL
+ * for the default stream) and returns without synchronising.  A CUDA error
+ * already pending in the calling thread is left in place and the call
+ * returns SCGPU_ERR_CUDA without enqueuing anything; SCGPU_ERR_CUDA from a
+ * failed launch of this call means its work may be partly enqueued. */
 int scgpu_compute_potential_noalloc(const double* rho_dev, double* phi_dev, int nx, int ny, int nz,
                                     const double hr[3], void* cuda_stream);
 

@@ -21,6 +21,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscoracle.so")
 REF_FFT_PATH = os.path.join(HERE, "_ref", "libfftpack_ref.so")
+# BorisPusher, Quaternion and CoordinateSystemTrafo of the reference, compiled
+# from its sources by oracle/Makefile (refpin/refpin.cpp gives them a C ABI)
+REF_PIN_PATH = os.path.join(HERE, "_ref", "librefpin.so")
 
 _dp = C.POINTER(C.c_double)
 
@@ -489,3 +492,127 @@ class OracleTracker:
         out["Ef"], out["Bf"] = ef, bf
         out["update_origin"] = np.array(dbg.update_origin)
         return out
+
+
+# ---------------------------------------------------------------- pinning
+# The oracle's frame and pusher functions beside the reference's own
+# (oracle/_ref/librefpin.so), on the same inputs, one case per row.
+
+_ref_pin = None
+
+
+def reference_pin_available():
+    return os.path.exists(REF_PIN_PATH)
+
+
+def reference_pin():
+    """The reference's BorisPusher / Quaternion / CoordinateSystemTrafo
+    behind a C ABI (None when oracle/_ref was not built)."""
+    global _ref_pin
+    if _ref_pin is None and reference_pin_available():
+        _ref_pin = C.CDLL(REF_PIN_PATH)
+    return _ref_pin
+
+
+def _rows(fn, *arrays, out_shapes):
+    """Calls fn(row pointers..., out pointers...) for every row."""
+    n = len(arrays[0])
+    ins = [_f64(a) for a in arrays]
+    outs = [np.zeros((n,) + sh) for sh in out_shapes]
+    for i in range(n):
+        fn(*[_ptr(a[i]) for a in ins], *[_ptr(o[i]) for o in outs])
+    return outs
+
+
+def pin_cases_oracle(cases):
+    """The oracle's answers for the pinning cases (see tests/golden/make_golden.py)."""
+    L = lib()
+    c = cases
+    out = {}
+    P = _f64(c["kick_P"]).copy()
+    L.sco_kick(C.c_longlong(len(P)), _ptr(P), _ptr(_f64(c["kick_Ef"])), _ptr(_f64(c["kick_Bf"])),
+               C.c_double(float(c["dt"])), C.c_double(float(c["mass"])), C.c_double(float(c["charge"])))
+    out["kick"] = P
+    R = _f64(c["push_R"]).copy()
+    L.sco_push(C.c_longlong(len(R)), _ptr(R), _ptr(_f64(c["push_P"])), C.c_double(float(c["dt"])))
+    out["push"] = R
+
+    def quat(u, ref, q):
+        L.sco_get_quaternion(u, ref, q)
+    out["quaternion"], = _rows(quat, c["quat_u"], c["quat_ref"], out_shapes=[(4,)])
+
+    def rotmat(q, M):
+        t = Trafo()
+        L.sco_trafo_make(C.byref(t), _ptr(np.zeros(3)), q)
+        C.memmove(M, t.M, 9 * 8)
+    out["rotation_matrix"], = _rows(rotmat, c["rotmat_quat"], out_shapes=[(9,)])
+    out["quaternion_rotate"], = _rows(L.sco_quat_rotate, c["trafo_quat"], c["trafo_r"], out_shapes=[(3,)])
+
+    def make(o, q):
+        t = Trafo()
+        L.sco_trafo_make(C.byref(t), o, q)
+        return t
+
+    def transform(o, q, r, res):
+        t = make(o, q)
+        L.sco_trafo_transform_to(C.byref(t), r, res)
+
+    def rotate(o, q, r, res):
+        t = make(o, q)
+        L.sco_trafo_rotate_to(C.byref(t), r, res)
+
+    def inverted(o, q, oo, qo):
+        t = make(o, q)
+        L.sco_trafo_invert(C.byref(t))
+        C.memmove(oo, t.origin, 24)
+        C.memmove(qo, t.quat, 32)
+
+    def compose(lo, lq, ro, rq, oo, qo):
+        t, r = make(lo, lq), make(ro, rq)
+        L.sco_trafo_compose(C.byref(t), C.byref(r))
+        C.memmove(oo, t.origin, 24)
+        C.memmove(qo, t.quat, 32)
+    out["transform_to"], = _rows(transform, c["trafo_origin"], c["trafo_quat"], c["trafo_r"], out_shapes=[(3,)])
+    out["rotate_to"], = _rows(rotate, c["trafo_origin"], c["trafo_quat"], c["trafo_r"], out_shapes=[(3,)])
+    out["inverted_origin"], out["inverted_quat"] = _rows(inverted, c["trafo_origin"], c["trafo_quat"],
+                                                         out_shapes=[(3,), (4,)])
+    out["compose_origin"], out["compose_quat"] = _rows(compose, c["trafo_origin"], c["trafo_quat"], c["right_origin"],
+                                                       c["right_quat"], out_shapes=[(3,), (4,)])
+    return out
+
+
+def pin_cases_reference(cases):
+    """The reference's answers for the same cases, from oracle/_ref/librefpin.so.
+    The push is BorisPusher::push between the unit switches of
+    PartBunchBase.hpp:468-513 (R / (c dt) per component, then R * (c dt))."""
+    L = reference_pin()
+    if L is None:
+        raise RuntimeError("oracle/_ref/librefpin.so is missing: the reference tree is needed")
+    c = cases
+    dt, mass, charge = (C.c_double(float(c[k])) for k in ("dt", "mass", "charge"))
+    out = {}
+    P = _f64(c["kick_P"]).copy()
+    R0 = np.zeros(3)
+    for i in range(len(P)):
+        L.ref_boris_kick(_ptr(R0), _ptr(P[i]), _ptr(_f64(c["kick_Ef"][i])), _ptr(_f64(c["kick_Bf"][i])), dt, mass,
+                         charge)
+    out["kick"] = P
+    R = _f64(c["push_R"]).copy()
+    s = c_light() * float(c["dt"])
+    for i in range(len(R)):
+        r = np.array([R[i, 0] / s, R[i, 1] / s, R[i, 2] / s])
+        L.ref_boris_push_unitless(_ptr(r), _ptr(_f64(c["push_P"][i])), dt)
+        R[i] = [r[0] * s, r[1] * s, r[2] * s]
+    out["push"] = R
+    out["quaternion"], = _rows(L.ref_get_quaternion, c["quat_u"], c["quat_ref"], out_shapes=[(4,)])
+    out["rotation_matrix"], = _rows(L.ref_rotation_matrix, c["rotmat_quat"], out_shapes=[(9,)])
+    out["quaternion_rotate"], = _rows(L.ref_quaternion_rotate, c["trafo_quat"], c["trafo_r"], out_shapes=[(3,)])
+    out["transform_to"], = _rows(L.ref_trafo_transform_to, c["trafo_origin"], c["trafo_quat"], c["trafo_r"],
+                                 out_shapes=[(3,)])
+    out["rotate_to"], = _rows(L.ref_trafo_rotate_to, c["trafo_origin"], c["trafo_quat"], c["trafo_r"],
+                              out_shapes=[(3,)])
+    out["inverted_origin"], out["inverted_quat"] = _rows(L.ref_trafo_inverted, c["trafo_origin"], c["trafo_quat"],
+                                                         out_shapes=[(3,), (4,)])
+    out["compose_origin"], out["compose_quat"] = _rows(L.ref_trafo_compose, c["trafo_origin"], c["trafo_quat"],
+                                                       c["right_origin"], c["right_quat"], out_shapes=[(3,), (4,)])
+    return out

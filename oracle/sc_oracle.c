@@ -244,6 +244,12 @@ static inline void trafo_rotate_to(const sco_trafo* t, const double* r, double* 
     matvec(t->M, r, out);
 }
 
+/* exported for the pinning tests against the reference's own
+   CoordinateSystemTrafo::transformTo / rotateTo and Quaternion::rotate */
+void sco_trafo_transform_to(const sco_trafo* t, const double* r, double* out) { trafo_transform_to(t, r, out); }
+void sco_trafo_rotate_to(const sco_trafo* t, const double* r, double* out) { trafo_rotate_to(t, r, out); }
+void sco_quat_rotate(const double* q, const double* v, double* out) { quat_rotate(q, v, out); }
+
 /* ------------------------------------------------------------------------ */
 /* pusher: BorisPusher.h:56-124 and the unit switches PartBunchBase.hpp:468-513 */
 /* ------------------------------------------------------------------------ */

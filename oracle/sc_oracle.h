@@ -90,6 +90,9 @@ int sco_get_quaternion(const double* u, const double* ref, double* q);
 void sco_trafo_make(sco_trafo* t, const double* origin, const double* quat);
 void sco_trafo_invert(sco_trafo* t);
 void sco_trafo_compose(sco_trafo* t, const sco_trafo* right);
+void sco_trafo_transform_to(const sco_trafo* t, const double* r, double* out);
+void sco_trafo_rotate_to(const sco_trafo* t, const double* r, double* out);
+void sco_quat_rotate(const double* q, const double* v, double* out);
 
 void sco_push(long long n, double* R, const double* P, double dt);
 void sco_kick(long long n, double* P, const double* Ef, const double* Bf, double dt, double mass, double charge);

@@ -11,6 +11,55 @@
 
 using namespace sc;
 
+namespace sc {
+
+// cuMemGetAddressRange from the driver, looked up once through the runtime
+// (the library does not link the driver library itself).
+using GetAddressRangeFn = int (*)(unsigned long long* base, size_t* size, unsigned long long ptr);
+static GetAddressRangeFn address_range_fn() {
+    static GetAddressRangeFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        cudaGetLastError();
+        return reinterpret_cast<GetAddressRangeFn>(f);
+    }();
+    return fn;
+}
+
+bool device_buffer_ok(const void* p, size_t bytes, int device, std::string* why) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        *why = "not a pointer the CUDA runtime knows";
+        return false;
+    }
+    if (a.type == cudaMemoryTypeDevice) {
+        if (a.device != device) {
+            *why = "device memory of another GPU";
+            return false;
+        }
+    } else if (a.type != cudaMemoryTypeManaged) {
+        *why = "host memory, not device memory";
+        return false;
+    }
+    if (GetAddressRangeFn fn = address_range_fn()) {
+        unsigned long long base = 0;
+        size_t size = 0;
+        const unsigned long long at = (unsigned long long)(uintptr_t)p;
+        if (fn(&base, &size, at) == 0 && (at < base || at - base + bytes > size)) {
+            *why = "allocation smaller than the mesh (" + std::to_string(size - (at - base)) + " bytes from the pointer, " +
+                   std::to_string(bytes) + " needed)";
+            return false;
+        }
+    }
+    return true;
+}
+
+}  // namespace sc
+
 namespace {
 
 int fail(scgpu_ctx* c, int code, const std::string& what) {
@@ -609,6 +658,11 @@ static int compute_potential_impl(scgpu_ctx* c, double* rho, const double hr[3],
     DevBunch& b = c->b;
     cudaStream_t s = c->stream;
     const long long M = (long long)b.bc.n[0] * b.bc.n[1] * b.bc.n[2];
+    if (device_ptr) {
+        std::string why;
+        if (!device_buffer_ok(rho, (size_t)M * sizeof(double), c->device, &why))
+            return fail(c, SCGPU_ERR_ARG, "rho_inout_device: " + why);
+    }
     const cudaMemcpyKind in_kind = device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     const cudaMemcpyKind out_kind = device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     CK(cudaMemcpyAsync(b.st->hr_scaled, hr, 3 * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -646,6 +700,11 @@ static int compute_potential_image_impl(scgpu_ctx* c, double* rho, const double 
     if (!std::isfinite(zshift)) return fail(c, SCGPU_ERR_ARG, "zshift must be finite");
     if (c->b.periodic_z) return fail(c, SCGPU_ERR_UNSUPPORTED, "image charges with periodic z");
     CK(cudaSetDevice(c->device));
+    if (device_ptr) {
+        std::string why;
+        if (!device_buffer_ok(rho, (size_t)mesh_cells(c->b) * sizeof(double), c->device, &why))
+            return fail(c, SCGPU_ERR_ARG, "rho_inout_device: " + why);
+    }
     int rc = ensure_image(c);
     if (rc) return rc;
     DevBunch& b = c->b;

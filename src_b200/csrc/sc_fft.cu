@@ -1124,10 +1124,19 @@ size_t fft_smem_bytes(const DevBunch& b) {
     return m;
 }
 
-// twiddles exp(-2 pi i e / L) from long double arithmetic, rounded once
 // Axis d's transform length: the doubled grid, except z with periodic z.
 static inline int axis_length(const DevBunch& b, int d) {
     return (d == 2 && b.periodic_z) ? b.bc.n[2] : 2 * b.bc.n[d];
+}
+
+// twiddles exp(-2 pi i e / L), e in [0, L), from long double arithmetic
+// rounded once to the table's type (tf may be null)
+void twiddle_values(int L, double2* td, float2* tf) {
+    for (int e = 0; e < L; ++e) {
+        const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)e / (long double)L;
+        td[e] = double2{(double)cosl(a), (double)sinl(a)};
+        if (tf) tf[e] = float2{(float)cosl(a), (float)sinl(a)};
+    }
 }
 
 void upload_twiddles(DevBunch& b, cudaStream_t s) {
@@ -1135,11 +1144,7 @@ void upload_twiddles(DevBunch& b, cudaStream_t s) {
         const int L = axis_length(b, d);
         std::vector<double2> td(L);
         std::vector<float2> tf(L);
-        for (int e = 0; e < L; ++e) {
-            const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)e / (long double)L;
-            td[e] = double2{(double)cosl(a), (double)sinl(a)};
-            tf[e] = float2{(float)cosl(a), (float)sinl(a)};
-        }
+        twiddle_values(L, td.data(), tf.data());
         // the double table always (the G spectrum is built in FP64); the float one in the mixed form
         double2* dptr = reinterpret_cast<double2*>(b.tw[d]);
         cudaMemcpyAsync(dptr, td.data(), L * sizeof(double2), cudaMemcpyHostToDevice, s);

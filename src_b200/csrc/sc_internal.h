@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "sc_common.cuh"
@@ -75,6 +76,13 @@ struct FftPlan {
 };
 
 FftPlan make_plan(int L);
+
+// A buffer a caller hands to a *_device entry point: device memory of
+// `device` (or managed memory) holding at least `bytes` from p.  Checked
+// before anything is enqueued, so a host or foreign pointer becomes
+// SCGPU_ERR_ARG instead of an illegal-address fault on the GPU.  *why says
+// what is wrong.
+bool device_buffer_ok(const void* p, size_t bytes, int device, std::string* why);
 int particle_grid(const DevBunch& b);
 void prime_particle_grids();  // occupancy of the particle kernels, before any capture
 
@@ -205,6 +213,8 @@ void launch_green_transform_image(const DevBunch& b, cudaStream_t s);
 void launch_green_transform_periodic(const DevBunch& b, cudaStream_t s);
 size_t fft_smem_bytes(const DevBunch& b);
 void upload_twiddles(DevBunch& b, cudaStream_t s);
+// the values upload_twiddles stores for transform length L (host)
+void twiddle_values(int L, double2* td, float2* tf);
 void fft_set_smem_limits();
 
 // convolution modes

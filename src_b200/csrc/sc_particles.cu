@@ -1408,21 +1408,28 @@ int particle_grid(const DevBunch& b) { return b.red_blocks; }
 #define SC_PARTICLE_WAVES 1
 #endif
 
-// Resident blocks of kThreads on the whole device for one kernel (the
-// occupancy query runs once per kernel, outside stream capture: contexts
-// call prime_particle_grids when they are created).
+constexpr int kMaxCachedDevices = 64;
+
+// Resident blocks of kThreads on the whole current device for one kernel
+// (the occupancy query runs once per device and kernel, outside stream
+// capture: contexts call prime_particle_grids when they are created).  The
+// cache is keyed by the device too, since devices may differ in SM count.
 int resident_blocks(const void* kernel) {
     static std::mutex mu;
-    static std::unordered_map<const void*, int> cache;
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = cache.find(kernel);
-    if (it != cache.end()) return it->second;
+    static std::unordered_map<const void*, int> cache[kMaxCachedDevices];
     int dev = 0, nsm = 0, k = 0;
     cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    std::unordered_map<const void*, int>* c = (dev >= 0 && dev < kMaxCachedDevices) ? &cache[dev] : nullptr;
+    if (c) {
+        auto it = c->find(kernel);
+        if (it != c->end()) return it->second;
+    }
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, kernel, kThreads, 0) != cudaSuccess || k < 1) k = 1;
     cudaGetLastError();
-    return cache.emplace(kernel, k * nsm).first->second;
+    if (!c) return k * nsm;
+    return c->emplace(kernel, k * nsm).first->second;
 }
 
 // Blocks for a particle loop (grid-stride, one reduction per block): the

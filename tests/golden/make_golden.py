@@ -21,6 +21,12 @@ binned_step_n8.npz
     A 3000-particle photoinjector bunch with 4 energy bins tracked 3 steps by
     the energy-bin loop with image charges (oracle, reference FFTPACK): final
     R, P and the last step's Ef, Bf.
+refpin_kat.npz
+    Random inputs and the answers of the reference's own BorisPusher::kick /
+    push, getQuaternion, Quaternion::getRotationMatrix / rotate and
+    CoordinateSystemTrafo::transformTo / rotateTo / inverted / operator*,
+    compiled from src/ into oracle/_ref/librefpin.so (``python
+    tests/golden/make_golden.py refpin`` writes only this file).
 sdds_stat_columns.json
     The column definitions (name, type, units, description), the &data block
     and the parameter rows of the reference's SDDS statistics file, read from
@@ -99,10 +105,6 @@ def image_and_bins():
                         Bf=dbg["Bf"], Q=tr.Q)
 
 
-if __name__ == "__main__":
-    main()
-
-
 def sdds_columns():
     import json
     import re
@@ -119,3 +121,65 @@ def sdds_columns():
            "data": data, "value_format": "scientific, precision 15 (DataSink::open_m), then setw(10) << tab"}
     with open(os.path.join(HERE, "sdds_stat_columns.json"), "w") as f:
         json.dump(out, f, indent=1)
+
+
+def pin_cases(seed=20261204):
+    """Random inputs of the pinning cases: Boris kicks and pushes of beam-like
+    and arbitrary momenta, getQuaternion of mean momenta near the z axis and
+    of arbitrary directions, trafos with random origins and
+    orientations, rotation matrices of not quite normalised quaternions."""
+    rng = np.random.default_rng(seed)
+    n = 1000
+    c = {"dt": 1e-12, "mass": O.electron_mass_ev(), "charge": -1.0}
+    beam = np.column_stack([1e-3 * rng.standard_normal(n), 1e-3 * rng.standard_normal(n),
+                            10.0 * (1 + 1e-3 * rng.standard_normal(n))])
+    anyp = rng.standard_normal((n, 3)) * np.exp(rng.uniform(np.log(0.05), np.log(50.0), (n, 1)))
+    c["kick_P"] = np.concatenate([beam, anyp])
+    c["kick_Ef"] = rng.standard_normal((2 * n, 3)) * np.exp(rng.uniform(np.log(1e3), np.log(1e8), (2 * n, 1)))
+    Bf = 0.3 * rng.standard_normal((2 * n, 3))
+    Bf[: n // 4] = 0.0
+    c["kick_Bf"] = Bf
+    c["push_R"] = 1e-3 * rng.standard_normal((2 * n, 3))
+    c["push_P"] = c["kick_P"].copy()
+    near = np.column_stack([1e-6 * rng.standard_normal(n), 1e-6 * rng.standard_normal(n),
+                            10.0 * (1 + 1e-3 * rng.standard_normal(n))])
+    near[: n // 8, :2] *= 1e-8   # within getQuaternion's parallel tolerance
+    u_any = rng.standard_normal((n, 3))
+    ref_any = rng.standard_normal((n, 3))
+    flip = np.sum(u_any * ref_any, axis=1) < 0
+    u_any[flip] *= -1.0          # no anti-parallel pairs (the reference draws a random axis there)
+    zhat = np.tile([0.0, 0.0, 1.0], (n, 1))
+    c["quat_u"] = np.concatenate([near, u_any])
+    c["quat_ref"] = np.concatenate([zhat, ref_any])
+    q = rng.standard_normal((n, 4))
+    c["trafo_quat"] = q / np.linalg.norm(q, axis=1, keepdims=True)
+    # getRotationMatrix normalises its own copy; Quaternion::rotate (and so
+    # every trafo operation that rotates a vector) requires a unit quaternion
+    c["rotmat_quat"] = c["trafo_quat"] * (1 + 1e-3 * rng.standard_normal((n, 1)))
+    c["trafo_origin"] = rng.standard_normal((n, 3))
+    c["trafo_r"] = 1e-3 * rng.standard_normal((n, 3))
+    rq = rng.standard_normal((n, 4))
+    c["right_quat"] = rq / np.linalg.norm(rq, axis=1, keepdims=True)
+    c["right_origin"] = rng.standard_normal((n, 3))
+    return c
+
+
+def refpin():
+    """refpin_kat.npz: the pinning cases and the answers of the reference's
+    own BorisPusher, Quaternion and CoordinateSystemTrafo (compiled from
+    source into oracle/_ref/librefpin.so)."""
+    if not O.reference_pin_available():
+        raise SystemExit("oracle/_ref/librefpin.so is missing: the reference tree is needed")
+    c = pin_cases()
+    ref = O.pin_cases_reference(c)
+    np.savez_compressed(os.path.join(HERE, "refpin_kat.npz"), **{f"in_{k}": np.asarray(v) for k, v in c.items()},
+                        **{f"ref_{k}": v for k, v in ref.items()})
+
+
+if __name__ == "__main__":
+    if sys.argv[1:] == ["refpin"]:
+        O.build()
+        refpin()
+    else:
+        main()
+        refpin()
