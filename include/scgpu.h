@@ -386,7 +386,8 @@ int scgpu_batch_trim(scgpu_batch* batch);
 double scgpu_batch_last_track_ms(const scgpu_batch* batch);
 /* Tuning of the batched launches: threads per block of the deposit (128,
  * 256 or 512) and, per transform length L, the FFT tile shape (0: the
- * single-bunch shape, 1: half as many columns per block). */
+ * widest, up to 256 threads per block; 1, 2, 3: a half, a quarter, an eighth
+ * as many columns per block, down to one warp). */
 int scgpu_batch_set_tuning(scgpu_batch* batch, int deposit_threads, int L, int fft_variant);
 int scgpu_batch_get_tuning(const scgpu_batch* batch, int L, int* deposit_threads, int* fft_variant);
 /* The autotuner: times trial_steps batched steps per candidate (deposit block

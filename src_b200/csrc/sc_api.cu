@@ -420,6 +420,7 @@ int status_from_flags(scgpu_ctx* c, int err) {
     if (err & kFlagGuard) return fail(c, SCGPU_ERR_GUARD, "a CIC stencil left the mesh");
     if (err & kFlagSort) return fail(c, SCGPU_ERR_CUDA, "cell sort: scatter position out of range");
     if (err & kFlagBin) return fail(c, SCGPU_ERR_ARG, "an energy bin outside [0, nbins)");
+    if (err & kFlagCopy) return fail(c, SCGPU_ERR_CUDA, "a bulk copy into shared memory did not complete");
     return fail(c, SCGPU_ERR_CUDA, "unknown device error flag");
 }
 

@@ -569,16 +569,20 @@ int scgpu_batch_autotune(scgpu_batch* b, int trial_steps) {
     std::sort(lengths.begin(), lengths.end());
     lengths.erase(std::unique(lengths.begin(), lengths.end()), lengths.end());
     for (int L : lengths) {
-        double ms0 = 0.0, ms1 = 0.0;
-        b->fft_variant[L] = 0;
-        b->dirty = true;
-        int rc = time_it(&ms0);
-        if (rc) return rc;
-        b->fft_variant[L] = 1;
-        b->dirty = true;
-        rc = time_it(&ms1);
-        if (rc) return rc;
-        b->fft_variant[L] = ms1 < ms0 ? 1 : 0;
+        double best_ms = 0.0;
+        int best_v = 0;
+        for (int v = 0; v < kFftVariants; ++v) {
+            double ms = 0.0;
+            b->fft_variant[L] = v;
+            b->dirty = true;
+            int rc = time_it(&ms);
+            if (rc) return rc;
+            if (v == 0 || ms < best_ms) {
+                best_ms = ms;
+                best_v = v;
+            }
+        }
+        b->fft_variant[L] = best_v;
         b->dirty = true;
     }
     return taken;

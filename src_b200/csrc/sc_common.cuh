@@ -42,6 +42,7 @@ enum : int {
     kFlagFrame = 4,
     kFlagSort = 8,  // a sort position fell outside [0, N): inconsistent histogram
     kFlagBin = 16,  // an energy bin outside [0, nbins)
+    kFlagCopy = 32, // a bulk copy into shared memory did not complete in time
 };
 
 struct Trafo {

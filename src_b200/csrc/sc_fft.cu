@@ -28,6 +28,7 @@
 // constants, so the stage loops unroll and the index arithmetic folds; other
 // lengths take the same kernels with the length read at run time.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <vector>
 
@@ -754,12 +755,52 @@ __global__ void __launch_bounds__(NT) k_rfft_lines_neg(const double* __restrict_
     rfft_lines_neg_body<TO, LT, NC, NT, NEG>(in, out, nb, se, pl, twd, blockIdx.x);
 }
 
+// Tile-shape variants of a length: V = 0 is the widest shape (cols_for
+// columns, up to 256 threads), each further variant halves the columns per
+// block (more, smaller blocks, down to a single warp for the long
+// transforms), which shortens each block's chain of barriers.  The batched
+// autotuner picks per length; single-bunch launches use single_variant().
+__host__ __device__ constexpr int cols_v(int LT, int V) {
+    const int c = cols_for(LT) >> V;
+    return c > 1 ? c : 1;
+}
+__host__ __device__ constexpr int threads_v(int LT, int V) {
+    if (LT == 0) return 256;
+    const int t = cols_v(LT, V) * (LT / min_radix(LT));
+    return t < 32 ? 32 : t;
+}
+
 // ---------------------------------------------------------------- dispatch
-template <int LT>
+template <int LT, int V = 0>
 struct Geo {
-    static constexpr int NC = cols_for(LT);
-    static constexpr int NT = threads_for(LT);
+    static constexpr int NC = cols_v(LT, V);
+    static constexpr int NT = threads_v(LT, V);
 };
+
+// Tile-shape variant of single-bunch launches for a transform length (0 for
+// lengths without a template instance): SCGPU_FFT_VARIANT=v forces one for
+// every length, otherwise the measured default of the length.
+int single_variant(int LT) {
+    static const int forced = [] {
+        const char* e = std::getenv("SCGPU_FFT_VARIANT");
+        const int v = e ? std::atoi(e) : -1;
+        return (v >= 0 && v < kFftVariants) ? v : -1;
+    }();
+    if (LT == 0) return 0;
+    if (forced >= 0) return forced;
+    return LT >= 64 ? 1 : 0;  // half-width tiles measured faster from 64 points up (the cosine transforms most)
+}
+
+// Calls f.template go<LT, V>() with V = single_variant(LT).
+template <int LT, typename F>
+void with_variant(F& f) {
+    switch (single_variant(LT)) {
+        case 1: f.template go<LT, 1>(); break;
+        case 2: f.template go<LT, 2>(); break;
+        case 3: f.template go<LT, 3>(); break;
+        default: f.template go<LT, 0>(); break;
+    }
+}
 
 template <typename C>
 size_t smem_of(int L, int nc) {
@@ -794,7 +835,11 @@ struct LaunchA {
     cudaStream_t s;
     template <int LT>
     void run() {
-        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        with_variant<LT>(*this);
+    }
+    template <int LT, int V>
+    void go() {
+        constexpr int NC = Geo<LT, V>::NC, NT = Geo<LT, V>::NT;
         dim3 g((unsigned)((n0 + 2 * NC - 1) / (2 * NC)), (unsigned)n1);
         k_fft_z_r2c<T, LT, NC, NT, FULL><<<g, NT, smem_of<Cx<T>>(pz.L, NC), s>>>(rho, spec, n0, n1, n2, L0, L1, pz, twz);
     }
@@ -809,7 +854,11 @@ struct LaunchY {
     cudaStream_t s;
     template <int LT>
     void run() {
-        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        with_variant<LT>(*this);
+    }
+    template <int LT, int V>
+    void go() {
+        constexpr int NC = Geo<LT, V>::NC, NT = Geo<LT, V>::NT;
         dim3 g((unsigned)((n0 + NC - 1) / NC), (unsigned)planes);
         k_fft_y<T, INV, LT, NC, NT><<<g, NT, smem_of<Cx<T>>(py.L, NC), s>>>(spec, n0, L0, n_in, n_out, py, twy);
     }
@@ -827,7 +876,11 @@ struct LaunchC {
     cudaStream_t s;
     template <int LT>
     void run() {
-        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        with_variant<LT>(*this);
+    }
+    template <int LT, int V>
+    void go() {
+        constexpr int NC = Geo<LT, V>::NC, NT = Geo<LT, V>::NT;
         k_fft_x_conv<TI, double, LT, NC, NT, CG><<<(unsigned)((rows + NC - 1) / NC), NT, smem_conv<TI>(px.L, NC), s>>>(
             in, out, ghat, n0, n1, L1, rows, px, twi, two);
     }
@@ -844,7 +897,11 @@ struct LaunchRfftNeg {
     cudaStream_t s;
     template <int LT>
     void run() {
-        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        with_variant<LT>(*this);
+    }
+    template <int LT, int V>
+    void go() {
+        constexpr int NC = Geo<LT, V>::NC, NT = Geo<LT, V>::NT;
         k_rfft_lines_neg<TO, LT, NC, NT, NEG>
             <<<(unsigned)((nb + 2 * NC - 1) / (2 * NC)), NT, smem_of<double2>(pl.L, NC), s>>>(in, out, nb, se, pl, tw);
     }
@@ -862,7 +919,11 @@ struct LaunchE {
     cudaStream_t s;
     template <int LT>
     void run() {
-        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        with_variant<LT>(*this);
+    }
+    template <int LT, int V>
+    void go() {
+        constexpr int NC = Geo<LT, V>::NC, NT = Geo<LT, V>::NT;
         dim3 g((unsigned)((n0 + 2 * NC - 1) / (2 * NC)), (unsigned)n1);
         k_fft_z_c2r<double, SELF, LT, NC, NT, FLIP, FULL><<<g, NT, smem_of<double2>(pz.L, NC), s>>>(
             spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling);
@@ -880,7 +941,11 @@ struct LaunchDct {
     cudaStream_t s;
     template <int LT>
     void run() {
-        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        with_variant<LT>(*this);
+    }
+    template <int LT, int V>
+    void go() {
+        constexpr int NC = Geo<LT, V>::NC, NT = Geo<LT, V>::NT;
         dim3 g((unsigned)((nb + 2 * NC - 1) / (2 * NC)), (unsigned)outer);
         k_dct_lines<TO, LT, NC, NT><<<g, NT, smem_of<double2>(pl.L, NC), s>>>(in, out, len, nb, sb, so, se, pl, tw);
     }
@@ -894,7 +959,16 @@ struct SetLimits {
     }
     template <int LT>
     void run() {
-        constexpr int NC = Geo<LT>::NC, NT = Geo<LT>::NT;
+        go<LT, 0>();
+        if constexpr (LT > 0) {
+            go<LT, 1>();
+            go<LT, 2>();
+            go<LT, 3>();
+        }
+    }
+    template <int LT, int V>
+    void go() {
+        constexpr int NC = Geo<LT, V>::NC, NT = Geo<LT, V>::NT;
         allow(k_fft_z_r2c<double, LT, NC, NT>);
         allow(k_fft_z_r2c<float, LT, NC, NT>);
         allow(k_fft_y<double, false, LT, NC, NT>);
@@ -922,19 +996,6 @@ struct SetLimits {
 };
 
 // ---------------------------------------------------------------- batches
-// Tile-shape variants of a length for batched launches: V = 0 is the
-// single-bunch shape (cols_for), V = 1 half as many columns per block (more,
-// smaller blocks; the autotuner picks per length).
-__host__ __device__ constexpr int cols_v(int LT, int V) {
-    const int c = cols_for(LT);
-    return V == 0 ? c : (c > 1 ? c / 2 : 1);
-}
-__host__ __device__ constexpr int threads_v(int LT, int V) {
-    if (LT == 0) return 256;
-    const int t = cols_v(LT, V) * (LT / min_radix(LT));
-    return t < 32 ? 32 : t;
-}
-
 __device__ __forceinline__ FftPlan plan_dev(int L) {
     const RadixPlan r = radix_plan(L);
     FftPlan p;
@@ -1026,10 +1087,12 @@ struct LaunchPassBatch {
 
 template <typename T, int PASS>
 void pass_batch_t(int L, int variant, const DevBunch* tab, const int4* work, int nitems, int n, cudaStream_t s) {
-    if (variant == 0)
-        with_length(L, LaunchPassBatch<T, PASS, 0>{tab, work, nitems, n, L, s});
-    else
-        with_length(L, LaunchPassBatch<T, PASS, 1>{tab, work, nitems, n, L, s});
+    switch (variant) {
+        case 1: with_length(L, LaunchPassBatch<T, PASS, 1>{tab, work, nitems, n, L, s}); break;
+        case 2: with_length(L, LaunchPassBatch<T, PASS, 2>{tab, work, nitems, n, L, s}); break;
+        case 3: with_length(L, LaunchPassBatch<T, PASS, 3>{tab, work, nitems, n, L, s}); break;
+        default: with_length(L, LaunchPassBatch<T, PASS, 0>{tab, work, nitems, n, L, s}); break;
+    }
 }
 
 template <typename T>

@@ -186,7 +186,7 @@ enum : int {
     kPassDctX,
     kNumPasses
 };
-constexpr int kFftVariants = 2;
+constexpr int kFftVariants = 4;
 // Blocks of one pass for one bunch (grid x, y) with a tile-shape variant.
 void fft_pass_grid(int pass, const DevBunch& b, int variant, int* gx, int* gy);
 // Transform length of a pass's axis for a bunch.

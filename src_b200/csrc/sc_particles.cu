@@ -16,9 +16,12 @@
 //   k_gather_kick_push   CIC gather, B from E, back to the reference frame, Boris
 //                        kick, half drift, reference-frame update, momentum sums
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
+#include <string>
 #include <unordered_map>
 
+#include "sc_bulk.cuh"
 #include "sc_ddmath.cuh"
 #include "sc_exact.cuh"
 #include "sc_internal.h"
@@ -267,6 +270,9 @@ __device__ __forceinline__ void finish_mesh(StepState& s, const BunchConst& bc) 
     if (s.gen == 0u) s.gen = 1u;
 }
 
+__device__ __forceinline__ void bounds_tail(const BunchConst& bc, double (&v)[6], StepState* st, double* partials,
+                                            unsigned* ticket, VB g);
+
 template <bool DRIFT>
 __device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
                                            double* __restrict__ z, const double* __restrict__ px,
@@ -311,6 +317,14 @@ __device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restr
         v[4] = fmin(v[4], -R[1]);
         v[5] = fmin(v[5], -R[2]);
     }
+    bounds_tail(bc, v, st, partials, ticket, g);
+}
+
+// Block minimum of the per-thread bounds v (min x, y, z, -max x, y, z) into
+// partials[blk], then in the last block the bunch's bounds and its mesh
+// (sharded: this rank's bounds for the exchange).
+__device__ __forceinline__ void bounds_tail(const BunchConst& bc, double (&v)[6], StepState* st, double* partials,
+                                            unsigned* ticket, VB g) {
     __shared__ double sm[6][kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -349,6 +363,111 @@ __global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, do
                                                             const double* __restrict__ py, const double* __restrict__ pz,
                                                             StepState* st, double* partials, unsigned* ticket) {
     drift_body<DRIFT>(bc, x, y, z, px, py, pz, st, partials, ticket, vb_grid());
+}
+
+// drift_body with the particle state streamed through shared memory: each
+// block walks chunks of kDriftChunk particles, double-buffered; the bulk
+// copies of the next chunk's six arrays are in flight while the threads work
+// on the current one (lane-contiguous reads of the staged doubles).  Same
+// arithmetic and exact min / max as drift_body, so the same bits.
+constexpr int kDriftChunk = 512;
+constexpr size_t kDriftSmem = 2 * 6 * kDriftChunk * sizeof(double);
+
+template <bool DRIFT>
+__device__ __forceinline__ void drift_staged_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
+                                                  double* __restrict__ z, const double* __restrict__ px,
+                                                  const double* __restrict__ py, const double* __restrict__ pz,
+                                                  StepState* st, double* partials, unsigned* ticket, VB g,
+                                                  double* sm) {
+    __shared__ Trafo r2b_s;
+    __shared__ __align__(8) uint64_t bar[2];
+    if (threadIdx.x == 0) {
+        r2b_s = st->r2b;
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const double* const src[6] = {x, y, z, px, py, pz};
+    const long long nchunks = (bc.N + kDriftChunk - 1) / kDriftChunk;
+    auto buffers = [&](int b) {
+        double* base = sm + (size_t)b * 6 * kDriftChunk;
+        return base;
+    };
+    auto issue = [&](long long c, int b) {
+        const long long first = c * kDriftChunk;
+        const long long count = bc.N - first < kDriftChunk ? bc.N - first : kDriftChunk;
+        double* base = buffers(b);
+        if constexpr (DRIFT) {
+            double* const dst[6] = {base,
+                                    base + kDriftChunk,
+                                    base + 2 * kDriftChunk,
+                                    base + 3 * kDriftChunk,
+                                    base + 4 * kDriftChunk,
+                                    base + 5 * kDriftChunk};
+            stage_doubles<6>(dst, src, first, count, &bar[b]);
+        } else {
+            double* const dst[3] = {base, base + kDriftChunk, base + 2 * kDriftChunk};
+            const double* const s3[3] = {src[0], src[1], src[2]};
+            stage_doubles<3>(dst, s3, first, count, &bar[b]);
+        }
+    };
+    double v[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};  // min x,y,z, -max x,y,z
+    if (g.blk < nchunks) issue(g.blk, 0);
+    int k = 0;
+    for (long long c = g.blk; c < nchunks; c += g.nblk, ++k) {
+        const int b = k & 1;
+        if (c + g.nblk < nchunks) issue(c + g.nblk, b ^ 1);
+        if (__syncthreads_or(!mbar_wait(&bar[b], (unsigned)(k >> 1) & 1u))) {
+            if (threadIdx.x == 0) atomicOr(&st->err, kFlagCopy);
+            if (c + g.nblk < nchunks) mbar_wait(&bar[b ^ 1], (unsigned)((k + 1) >> 1) & 1u);
+            return;
+        }
+        const long long first = c * kDriftChunk;
+        const int count = (int)(bc.N - first < kDriftChunk ? bc.N - first : kDriftChunk);
+        const int body = count & ~1;
+        const double* base = buffers(b);
+        for (int j = threadIdx.x; j < count; j += blockDim.x) {
+            const long long i = first + j;
+            double R[3], P[3];
+            if (j < body) {
+                R[0] = base[j], R[1] = base[kDriftChunk + j], R[2] = base[2 * kDriftChunk + j];
+                if constexpr (DRIFT)
+                    P[0] = base[3 * kDriftChunk + j], P[1] = base[4 * kDriftChunk + j], P[2] = base[5 * kDriftChunk + j];
+            } else {
+                R[0] = x[i], R[1] = y[i], R[2] = z[i];
+                if constexpr (DRIFT) P[0] = px[i], P[1] = py[i], P[2] = pz[i];
+            }
+            if constexpr (DRIFT) {
+                push_r(R, P, bc.s_cdt, bc.rs_cdt);
+                double bb[3];
+                trafo_transform_to(*fresh(&r2b_s), R, bb);
+                R[0] = bb[0];
+                R[1] = bb[1];
+                R[2] = bb[2];
+                x[i] = R[0];
+                y[i] = R[1];
+                z[i] = R[2];
+            }
+            v[0] = fmin(v[0], R[0]);
+            v[1] = fmin(v[1], R[1]);
+            v[2] = fmin(v[2], R[2]);
+            v[3] = fmin(v[3], -R[0]);
+            v[4] = fmin(v[4], -R[1]);
+            v[5] = fmin(v[5], -R[2]);
+        }
+        __syncthreads();  // buffer b is read before the copies two chunks on land in it
+    }
+    bounds_tail(bc, v, st, partials, ticket, g);
+}
+
+template <bool DRIFT>
+__global__ void __launch_bounds__(kThreads, 3) k_drift_staged(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
+                                                           double* __restrict__ z, const double* __restrict__ px,
+                                                           const double* __restrict__ py, const double* __restrict__ pz,
+                                                           StepState* st, double* partials, unsigned* ticket) {
+    extern __shared__ __align__(16) double drift_sm[];
+    drift_staged_body<DRIFT>(bc, x, y, z, px, py, pz, st, partials, ticket, vb_grid(), drift_sm);
 }
 
 // The reference particle needs no particle data: it runs beside the deposit.
@@ -530,6 +649,141 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
     }
     if (bad) atomicOr(&st->err, kFlagGuard);
 }
+// Charge deposit by runs.  The arrays are in cell order, so consecutive
+// particles mostly share a cell: each block takes chunks of kDepChunk
+// consecutive particles, stages their positions into shared memory with bulk
+// asynchronous copies, and each thread walks kRunK consecutive particles of a
+// chunk, adding their eight fixed-point corner charges into 64-bit registers
+// while the cell stays the same; when the cell changes the thread adds the
+// eight sums to the node accumulators, and the last runs of the warp's lanes
+// are summed per cell across the warp before one lane adds them.  kRunK is odd
+// so that the threads' strided reads of the staged doubles fall into
+// distinct shared-memory banks.  The fixed-point charges and their integer
+// sums are those of deposit_body, so rho is bitwise the same.
+constexpr int kRunK = 9;
+constexpr int kDepThreads = 256;
+constexpr int kDepChunk = kDepThreads * kRunK;  // even: chunk starts stay 16-byte aligned
+constexpr size_t kDepSmem = 3 * kDepChunk * sizeof(double) + 16;
+
+__device__ __forceinline__ void flush_run(unsigned long long* __restrict__ acc, uint32_t key, const long long (&a)[8],
+                                          int nx, int nxy) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int node = (int)key + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
+        if (a[k] != 0) acc_add(acc + 2 * (size_t)node, a[k]);
+    }
+}
+
+template <bool BINNED>
+__device__ __forceinline__ void deposit_runs_body(const BunchConst& bc, const double* __restrict__ x,
+                                                  const double* __restrict__ y, const double* __restrict__ z,
+                                                  const int* __restrict__ bin, int nactive, StepState* st,
+                                                  unsigned long long* __restrict__ acc, VB g, double* sm) {
+    __shared__ MeshConsts ms;
+    __shared__ double qdt_s, to_int_s;
+    __shared__ __align__(8) uint64_t bar;
+    load_mesh_consts(ms, st);
+    if (threadIdx.x == 0) {
+        qdt_s = st->qdt;
+        to_int_s = ldexp(1.0, kFxFrac - fx_exponent(st->qdt));
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    double* const buf[3] = {sm, sm + kDepChunk, sm + 2 * kDepChunk};
+    const double* const src[3] = {x, y, z};
+    const int nx = bc.n[0], nxy = bc.n[0] * bc.n[1];
+    const uint32_t M = (uint32_t)nxy * (uint32_t)bc.n[2];
+    const long long nchunks = (bc.N + kDepChunk - 1) / kDepChunk;
+    bool bad = false;
+    unsigned parity = 0;
+    for (long long c = g.blk; c < nchunks; c += g.nblk, parity ^= 1u) {
+        const long long first = c * kDepChunk;
+        const long long count = bc.N - first < kDepChunk ? bc.N - first : kDepChunk;
+        const long long body = stage_doubles<3>(buf, src, first, count, &bar);
+        // a lost copy: flag it and leave the loop on every thread together
+        if (__syncthreads_or(!mbar_wait(&bar, parity))) {
+            if (threadIdx.x == 0) atomicOr(&st->err, kFlagCopy);
+            return;
+        }
+        const double to_int = to_int_s, qdt = qdt_s;
+        uint32_t run = 0xffffffffu;
+        long long a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const int i0 = threadIdx.x * kRunK;
+        for (int j = 0; j < kRunK; ++j) {
+            const int i = i0 + j;
+            if (i >= count) break;
+            int bk = 0;
+            if constexpr (BINNED) {
+                bk = bin[first + i];
+                if ((unsigned)bk >= (unsigned)nactive) continue;
+            }
+            double X[3];
+            if (i < body) {
+                X[0] = buf[0][i], X[1] = buf[1][i], X[2] = buf[2][i];
+            } else {
+                X[0] = x[first + i], X[1] = y[first + i], X[2] = z[first + i];
+            }
+            int l[3];
+            double d[3];
+            const MeshConsts* m = fresh(&ms);
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
+            double v[8];
+            cic_charge(d, qdt, v);
+            const uint32_t key = (uint32_t)(l[0] + nx * l[1] + nxy * l[2]) + (uint32_t)bk * M;
+            if (key != run) {
+                if (run != 0xffffffffu) flush_run(acc, run, a, nx, nxy);
+                run = key;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) a[k] = 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) a[k] += __double2ll_rn(v[k] * to_int);
+        }
+        // The lanes' last runs: consecutive lanes in one cell are summed
+        // together first (one pass of full-warp redux.sync per group, each sum
+        // as three limbs of at most 21 bits so that 32 of them fit 32 bits),
+        // and the group's first lane adds the sums to the node accumulators.
+        const int lane = threadIdx.x & 31;
+        const unsigned grp = __match_any_sync(kFull, run);
+        const bool multi = __popc(grp) > 1 && run != 0xffffffffu;
+        if (run != 0xffffffffu && !multi) flush_run(acc, run, a, nx, nxy);
+        unsigned leaders = __ballot_sync(kFull, multi && lane == __ffs(grp) - 1);
+        while (leaders) {
+            const int ld = __ffs(leaders) - 1;
+            leaders &= leaders - 1;
+            const bool in = (__shfl_sync(kFull, grp, ld) >> lane) & 1u;
+            long long sum[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const long long v = in ? a[k] : 0;
+                const unsigned lo = (unsigned)(v & 0x1fffff), mid = (unsigned)((v >> 21) & 0x1fffff);
+                const int hi = (int)(v >> 42);
+                sum[k] = (long long)__reduce_add_sync(kFull, hi) * (1ll << 42) +
+                         (long long)__reduce_add_sync(kFull, mid) * (1ll << 21) + (long long)__reduce_add_sync(kFull, lo);
+            }
+            if (lane == ld) flush_run(acc, run, sum, nx, nxy);
+        }
+        __syncthreads();  // the buffer is read before the next chunk's copies land in it
+    }
+    if (bad) atomicOr(&st->err, kFlagGuard);
+}
+__global__ void __launch_bounds__(kDepThreads) k_deposit_runs(BunchConst bc, const double* __restrict__ x,
+                                                              const double* __restrict__ y,
+                                                              const double* __restrict__ z, StepState* st,
+                                                              unsigned long long* __restrict__ acc) {
+    extern __shared__ __align__(16) double dep_sm[];
+    deposit_runs_body<false>(bc, x, y, z, nullptr, 0, st, acc, vb_grid(), dep_sm);
+}
+__global__ void __launch_bounds__(kDepThreads) k_deposit_runs_bins(BunchConst bc, const double* __restrict__ x,
+                                                                   const double* __restrict__ y,
+                                                                   const double* __restrict__ z,
+                                                                   const int* __restrict__ bin, int nactive,
+                                                                   StepState* st, unsigned long long* __restrict__ acc) {
+    extern __shared__ __align__(16) double dep_sm[];
+    deposit_runs_body<true>(bc, x, y, z, bin, nactive, st, acc, vb_grid(), dep_sm);
+}
+
 __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
                                                       const double* __restrict__ z, StepState* st,
                                                       unsigned long long* __restrict__ acc) {
@@ -568,17 +822,32 @@ __global__ void __launch_bounds__(kThreads) k_assemble_rho(BunchConst bc, const 
 // once (sc_ddmath.cuh): correctly rounded except in rare near-tie cases, so
 // G does not carry the device library's last-bit differences into the
 // eight-corner cancellation.
+// CR: the correctly rounded double-double atan / log of the plain form;
+// otherwise CUDA's own FP64 atan / log (a few ulp), the mixed form's
+// Green's function, still FP64 throughout.
+template <bool CR = true>
 __device__ __forceinline__ double igf_antiderivative(double x, double y, double z, double cellVolume) {
     double r = sqrt(x * x + y * y + z * z);
-    double tmpgrn = -z * z * ddm::atan_dd(x * y / (z * r)) / 2;
-    tmpgrn += -y * y * ddm::atan_dd(x * z / (y * r)) / 2;
-    tmpgrn += -x * x * ddm::atan_dd(y * z / (x * r)) / 2;
-    tmpgrn += y * z * ddm::log_dd(x + r);
-    tmpgrn += x * z * ddm::log_dd(y + r);
-    tmpgrn += x * y * ddm::log_dd(z + r);
-    return tmpgrn / cellVolume;
+    if constexpr (CR) {
+        double tmpgrn = -z * z * ddm::atan_dd(x * y / (z * r)) / 2;
+        tmpgrn += -y * y * ddm::atan_dd(x * z / (y * r)) / 2;
+        tmpgrn += -x * x * ddm::atan_dd(y * z / (x * r)) / 2;
+        tmpgrn += y * z * ddm::log_dd(x + r);
+        tmpgrn += x * z * ddm::log_dd(y + r);
+        tmpgrn += x * y * ddm::log_dd(z + r);
+        return tmpgrn / cellVolume;
+    } else {
+        double tmpgrn = -z * z * atan(x * y / (z * r)) / 2;
+        tmpgrn += -y * y * atan(x * z / (y * r)) / 2;
+        tmpgrn += -x * x * atan(y * z / (x * r)) / 2;
+        tmpgrn += y * z * log(x + r);
+        tmpgrn += x * z * log(y + r);
+        tmpgrn += x * y * log(z + r);
+        return tmpgrn / cellVolume;
+    }
 }
 
+template <bool CR = true>
 __device__ __forceinline__ void igf_tmp_body(int n0, int n1, int n2, const StepState* __restrict__ st,
                                              double* __restrict__ tmp, VB g) {
     const int t0 = n0 + 2, t1 = n1 + 2, t2 = n2 + 2;
@@ -589,12 +858,13 @@ __device__ __forceinline__ void igf_tmp_body(int n0, int n1, int n2, const StepS
         const double vx = i * h0 - h0 / 2;
         const double vy = j * h1 - h1 / 2;
         const double vz = k * h2 - h2 / 2;
-        tmp[c] = igf_antiderivative(vx, vy, vz, cellVolume);
+        tmp[c] = igf_antiderivative<CR>(vx, vy, vz, cellVolume);
     }
 }
+template <bool CR = true>
 __global__ void __launch_bounds__(kThreads) k_igf_tmp(int n0, int n1, int n2, const StepState* __restrict__ st,
                                                       double* __restrict__ tmp) {
-    igf_tmp_body(n0, n1, n2, st, tmp, vb_grid());
+    igf_tmp_body<CR>(n0, n1, n2, st, tmp, vb_grid());
 }
 
 // G on (n0+1)(n1+1)(n2+1) points, 8-corner difference (:508-516), then
@@ -1052,6 +1322,125 @@ __device__ __forceinline__ void cic_gather8(const double* __restrict__ F8, const
     }
 }
 
+// ------------------------------------------------------------ mixed form
+// The mixed form's particle update: the CIC cell from the FP64 position, the
+// eight weights and the gathered field in FP32 (fused multiply-adds), the
+// magnetic field B = beta c (-E_y, E_x, 0) in FP32; then, in FP64 with fused
+// multiply-adds, the beam -> reference frame rotation of R, E and B, the
+// Boris kick, the half drift R += (c dt / 2) P / gamma (no unitless round
+// trip) and the reference-frame update.  Results differ from the plain
+// form's by rounding only (relative 1e-7 in E, 1e-16 in the FP64 steps).
+__device__ __forceinline__ void matvec_fma(const double* M, const double* v, double* r) {
+    const double r0 = fma(M[0], v[0], fma(M[1], v[1], M[2] * v[2]));
+    const double r1 = fma(M[3], v[0], fma(M[4], v[1], M[5] * v[2]));
+    const double r2 = fma(M[6], v[0], fma(M[7], v[1], M[8] * v[2]));
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+}
+__device__ __forceinline__ void cross_fma(const double* a, const double* b, double* r) {
+    const double r0 = fma(a[1], b[2], -a[2] * b[1]);
+    const double r1 = fma(a[2], b[0], -a[0] * b[2]);
+    const double r2 = fma(a[0], b[1], -a[1] * b[0]);
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+}
+// CIC cell and offset in units of the spacing: u = (x - origin) / h, cell
+// centres at u = l + 1/2; false when the stencil would leave the mesh.
+__device__ __forceinline__ bool cic_locate_fast(const double* rhr, const double* org, const int* n, const double* x,
+                                                int* l, float* d) {
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double u = fma(x[a] - org[a], rhr[a], -0.5);
+        const double f = floor(u);
+        int li = (int)f;
+        float di = (float)(u - f);
+        if (li < 0) {
+            ok = false;
+            li = 0;
+        }
+        if (li > n[a] - 2) {
+            ok = false;
+            li = n[a] - 2;
+        }
+        l[a] = li;
+        d[a] = di;
+    }
+    return ok;
+}
+__device__ __forceinline__ void cic_gather_f32(const float* __restrict__ E4, const int* n, const int* l, const float* d,
+                                               float* Ef) {
+    const int nx = n[0], nxy = n[0] * n[1];
+    const int b = l[0] + nx * l[1] + nxy * l[2];
+    const float u[3] = {1.0f - d[0], 1.0f - d[1], 1.0f - d[2]};
+    float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int a0 = k & 1, a1 = (k >> 1) & 1, a2 = (k >> 2) & 1;
+        const float w = (a0 ? d[0] : u[0]) * (a1 ? d[1] : u[1]) * (a2 ? d[2] : u[2]);
+        const float4 a = __ldg(reinterpret_cast<const float4*>(E4) + (b + a0 + a1 * nx + a2 * nxy));
+        e0 = fmaf(w, a.x, e0);
+        e1 = fmaf(w, a.y, e1);
+        e2 = fmaf(w, a.z, e2);
+    }
+    Ef[0] = e0;
+    Ef[1] = e1;
+    Ef[2] = e2;
+}
+// returns false when the CIC stencil left the mesh
+template <bool EXT>
+__device__ __forceinline__ bool mixed_particle(const BunchConst& bc, const MeshConsts& m, const float* __restrict__ E4,
+                                               const Trafo& b2r, const Trafo& upd, double betaC, const StepState* st,
+                                               double* R, double* P) {
+    int l[3];
+    float d[3], e[3];
+    const bool ok = cic_locate_fast(m.rhr, m.org, bc.n, R, l, d);
+    cic_gather_f32(E4, bc.n, l, d, e);
+    const float bc32 = (float)betaC;
+    const double Eb[3] = {(double)e[0], (double)e[1], (double)e[2]};
+    const double Bb[3] = {(double)(-bc32 * e[1]), (double)(bc32 * e[0]), 0.0};
+    double X[3] = {R[0] - b2r.origin[0], R[1] - b2r.origin[1], R[2] - b2r.origin[2]};
+    double Rr[3], Ef[3], Bf[3];
+    matvec_fma(b2r.M, X, Rr);
+    matvec_fma(b2r.M, Eb, Ef);
+    matvec_fma(b2r.M, Bb, Bf);
+    if (bc.bz_ext != 0.0) Bf[2] += bc.bz_ext;
+    if constexpr (EXT) add_external_B(bc.sol, bc.nsol, st->ref_to_lab_step, Rr, Bf);
+    // Boris kick (BorisPusher.h:56-113)
+    const double ke = bc.ke;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) P[a] = fma(ke, Ef[a], P[a]);
+    const double gamma = sqrt(fma(P[0], P[0], fma(P[1], P[1], fma(P[2], P[2], 1.0))));
+    const double kt = bc.ktn / (gamma * bc.mass);
+    const double t[3] = {kt * Bf[0], kt * Bf[1], kt * Bf[2]};
+    double c[3], w[3];
+    cross_fma(P, t, c);
+    w[0] = P[0] + c[0];
+    w[1] = P[1] + c[1];
+    w[2] = P[2] + c[2];
+    const double ks = 2.0 / fma(t[0], t[0], fma(t[1], t[1], fma(t[2], t[2], 1.0)));
+    const double sv[3] = {ks * t[0], ks * t[1], ks * t[2]};
+    cross_fma(w, sv, c);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) P[a] = fma(ke, Ef[a], P[a] + c[a]);
+    // half drift
+    const double g = sqrt(fma(P[0], P[0], fma(P[1], P[1], fma(P[2], P[2], 1.0))));
+    const double hv = (0.5 * bc.s_cdt) / g;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) Rr[a] = fma(hv, P[a], Rr[a]);
+    // reference-frame update
+    double Y[3] = {Rr[0] - upd.origin[0], Rr[1] - upd.origin[1], Rr[2] - upd.origin[2]};
+    matvec_fma(upd.M, Y, R);
+    double Pu[3];
+    matvec_fma(upd.M, P, Pu);
+    P[0] = Pu[0];
+    P[1] = Pu[1];
+    P[2] = Pu[2];
+    return ok;
+}
+
 template <typename T, bool BINNED = false, bool EXT = false>
 __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
                                             double* __restrict__ z, double* __restrict__ px, double* __restrict__ py,
@@ -1069,6 +1458,24 @@ __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __rest
     __syncthreads();
     i128 acc[3] = {0, 0, 0};
     bool bad = false;
+    if constexpr (sizeof(T) == sizeof(float) && !BINNED) {
+        for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
+            double R[3] = {x[i], y[i], z[i]};
+            double P[3] = {px[i], py[i], pz[i]};
+            if (!mixed_particle<EXT>(bc, *fresh(&ms), reinterpret_cast<const float*>(E4), *fresh(&b2r_s),
+                                     *fresh(&upd_s), *fresh(&betaC_s), st, R, P))
+                bad = true;
+            x[i] = R[0];
+            y[i] = R[1];
+            z[i] = R[2];
+            px[i] = P[0];
+            py[i] = P[1];
+            pz[i] = P[2];
+            acc[0] += ex_from(P[0]);
+            acc[1] += ex_from(P[1]);
+            acc[2] += ex_from(P[2]);
+        }
+    } else
     for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
         const double X[3] = {x[i], y[i], z[i]};
         double P[3] = {px[i], py[i], pz[i]};
@@ -1336,7 +1743,10 @@ __global__ void k_advance_batch(const DevBunch* __restrict__ tab, const int4* __
 __global__ void __launch_bounds__(kThreads) k_igf_tmp_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
     const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
-    igf_tmp_body(d.bc.n[0], d.bc.n[1], d.bc.n[2], d.st, d.gtmp, VB{w.y, w.w});
+    if (d.precision == 0)
+        igf_tmp_body<true>(d.bc.n[0], d.bc.n[1], d.bc.n[2], d.st, d.gtmp, VB{w.y, w.w});
+    else
+        igf_tmp_body<false>(d.bc.n[0], d.bc.n[1], d.bc.n[2], d.st, d.gtmp, VB{w.y, w.w});
 }
 
 __global__ void __launch_bounds__(kThreads) k_igf_G_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
@@ -1414,7 +1824,7 @@ constexpr int kMaxCachedDevices = 64;
 // (the occupancy query runs once per device and kernel, outside stream
 // capture: contexts call prime_particle_grids when they are created).  The
 // cache is keyed by the device too, since devices may differ in SM count.
-int resident_blocks(const void* kernel) {
+int resident_blocks(const void* kernel, size_t smem = 0) {
     static std::mutex mu;
     static std::unordered_map<const void*, int> cache[kMaxCachedDevices];
     int dev = 0, nsm = 0, k = 0;
@@ -1426,7 +1836,7 @@ int resident_blocks(const void* kernel) {
         if (it != c->end()) return it->second;
     }
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, kernel, kThreads, 0) != cudaSuccess || k < 1) k = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, kernel, kThreads, smem) != cudaSuccess || k < 1) k = 1;
     cudaGetLastError();
     if (!c) return k * nsm;
     return c->emplace(kernel, k * nsm).first->second;
@@ -1437,14 +1847,40 @@ int resident_blocks(const void* kernel) {
 // over several particles and its set-up and reduction are paid once per
 // resident block; never more than b.red_blocks (the partials' size).
 template <typename K>
-int wave_grid(K kernel, const DevBunch& b) {
+int wave_grid(K kernel, const DevBunch& b, size_t smem = 0) {
     if (SC_PARTICLE_WAVES <= 0) return b.red_blocks;
-    const int blocks = resident_blocks((const void*)kernel) * SC_PARTICLE_WAVES;
+    const int blocks = resident_blocks((const void*)kernel, smem) * SC_PARTICLE_WAVES;
     return blocks < b.red_blocks ? blocks : b.red_blocks;
 }
 
+// The run deposit is the default; SCGPU_DEPOSIT=warp selects the warp-group
+// deposit (same bits) for comparisons.
+// Particle kernels stream the particle state through shared memory with bulk
+// copies (default); SCGPU_STREAM=0 selects the direct-load kernels (same bits).
+bool stream_particles() {
+    static const bool on = [] {
+        const char* e = std::getenv("SCGPU_STREAM");
+        return !(e && std::string(e) == "0");
+    }();
+    return on;
+}
+
+bool deposit_by_runs() {
+    static const bool runs = [] {
+        const char* e = std::getenv("SCGPU_DEPOSIT");
+        return !(e && std::string(e) == "warp");
+    }();
+    return runs;
+}
+
 void prime_particle_grids() {
-    const void* kernels[] = {(const void*)k_drift_to_beam<true>,
+    cudaFuncSetAttribute(k_drift_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDriftSmem);
+    cudaFuncSetAttribute(k_drift_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDriftSmem);
+    cudaFuncSetAttribute(k_deposit_runs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
+    cudaFuncSetAttribute(k_deposit_runs_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
+    const void* kernels[] = {(const void*)k_drift_staged<true>,
+                             (const void*)k_drift_staged<false>,
+                             (const void*)k_drift_to_beam<true>,
                              (const void*)k_drift_to_beam<false>,
                              (const void*)k_deposit,
                              (const void*)k_deposit_bins,
@@ -1454,7 +1890,8 @@ void prime_particle_grids() {
                              (const void*)k_gather_kick_push<float, true>,
                              (const void*)k_gather_kick_push_bins<false>,
                              (const void*)k_gather_kick_push_bins<true>};
-    for (const void* k : kernels) resident_blocks(k);
+    for (const void* k : kernels) resident_blocks(k, (k == (const void*)k_drift_staged<true> ||
+                                                      k == (const void*)k_drift_staged<false>) ? kDriftSmem : 0);
 }
 
 void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s) {
@@ -1463,6 +1900,12 @@ void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s) {
 }
 
 void launch_drift_to_beam(const DevBunch& b, bool drift, cudaStream_t s) {
+    if (stream_particles()) {
+        auto k = drift ? k_drift_staged<true> : k_drift_staged<false>;
+        k<<<wave_grid(k, b, kDriftSmem), kThreads, kDriftSmem, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials,
+                                                         b.ticket);
+        return;
+    }
     auto k = drift ? k_drift_to_beam<true> : k_drift_to_beam<false>;
     k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials, b.ticket);
 }
@@ -1475,6 +1918,12 @@ void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s) {
 }
 
 void launch_deposit(const DevBunch& b, cudaStream_t s) {
+    if (deposit_by_runs()) {
+        const long long nchunks = (b.bc.N + kDepChunk - 1) / kDepChunk;
+        const int g = (int)(nchunks < 1 ? 1 : nchunks);
+        k_deposit_runs<<<g, kDepThreads, kDepSmem, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
+        return;
+    }
     k_deposit<<<wave_grid(k_deposit, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
 }
 
@@ -1492,7 +1941,10 @@ void launch_igf(const DevBunch& b, const double* hr_host, cudaStream_t s) {
     const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
     const long long T3 = (long long)(n0 + 2) * (n1 + 2) * (n2 + 2);
     const long long G3 = (long long)(n0 + 1) * (n1 + 1) * (n2 + 1);
-    k_igf_tmp<<<grid_for(T3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.st, b.gtmp);
+    if (b.precision == 0)
+        k_igf_tmp<true><<<grid_for(T3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.st, b.gtmp);
+    else
+        k_igf_tmp<false><<<grid_for(T3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.st, b.gtmp);
     k_igf_G<<<grid_for(G3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.gtmp, b.gline);
 }
 
@@ -1540,6 +1992,13 @@ void launch_bin_gammas(const DevBunch& b, cudaStream_t s) {
 }
 
 void launch_deposit_bins(const DevBunch& b, cudaStream_t s) {
+    if (deposit_by_runs()) {
+        const long long nchunks = (b.bc.N + kDepChunk - 1) / kDepChunk;
+        const int g = (int)(nchunks < 1 ? 1 : nchunks);
+        k_deposit_runs_bins<<<g, kDepThreads, kDepSmem, s>>>(b.bc, b.x, b.y, b.z, b.bin, b.nactive, b.st,
+                                                             b.nacc_bins);
+        return;
+    }
     k_deposit_bins<<<wave_grid(k_deposit_bins, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.bin, b.nactive, b.st,
                                                                       b.nacc_bins);
 }

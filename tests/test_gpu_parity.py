@@ -322,6 +322,48 @@ def test_step100_parity_vs_oracle(oracle, gpu, cfg):
     print(f"{cfg} step 100 vs reference-arithmetic oracle: {ref}")
 
 
+_DEPOSIT_RUN = r"""
+import sys
+import numpy as np
+sys.path.insert(0, {root!r})
+from src_b200 import scgpu
+from src_b200.bunch import gaussian_bunch
+out = {{}}
+for name, N, every in (("sorted", 200_000, 32), ("unsorted", 50_001, 0)):
+    R, P = gaussian_bunch(N, bunch_id=17)
+    with scgpu.Context((32, 32, 32)) as c:
+        c.set_reorder_interval(every)
+        c.upload(R, P, 1e-12, -1e-9 / N, 510998.92)
+        c.track(3)
+        out[name] = c.field(scgpu.FIELD_RHO)
+np.savez({path!r}, **out)
+"""
+
+
+def test_run_deposit_equals_warp_deposit(gpu, tmp_path):
+    """The run deposit (chunks staged by bulk copies, per-thread runs of
+    consecutive particles) and the warp-group deposit (SCGPU_DEPOSIT=warp)
+    add the same fixed-point charges: rho is bitwise equal, in cell order and
+    out of it."""
+    import os
+    import subprocess
+    import sys
+
+    res = {}
+    for mode in ("runs", "warp"):
+        path = str(tmp_path / f"{mode}.npz")
+        env = dict(os.environ)
+        env.pop("SCGPU_DEPOSIT", None)
+        if mode == "warp":
+            env["SCGPU_DEPOSIT"] = "warp"
+        code = _DEPOSIT_RUN.format(root=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), path=path)
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-3000:]
+        res[mode] = np.load(path)
+    for name in ("sorted", "unsorted"):
+        np.testing.assert_array_equal(res["runs"][name], res["warp"][name])
+
+
 def test_device_entry_points_check_pointers(gpu):
     """The *_device solves take the caller's device buffer; a host pointer or
     an allocation smaller than the mesh is refused with SCGPU_ERR_ARG before
