@@ -288,6 +288,7 @@ def main():
     ap.add_argument("--serve", action="store_true",
                     help="serving loop: Poisson arrivals at 50 jobs/s for --serve-seconds (one JSON line)")
     ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-rate", type=float, default=50.0, help="Poisson arrival rate of the serving loop [jobs/s]")
     ap.add_argument("--binned", action="store_true",
                     help="photoinjector mode: energy bins with image charges (one JSON line)")
     ap.add_argument("--nbins", type=int, default=10)
@@ -666,7 +667,7 @@ def serve(args, local):
 
     torch.cuda.set_device(local)
     prec = scgpu.PLAIN_FP64 if args.precision == "fp64" else scgpu.MIXED
-    jobs = serving_jobs(duration_s=args.serve_seconds)
+    jobs = serving_jobs(rate_hz=args.serve_rate, duration_s=args.serve_seconds)
     masters = MasterBunches(count=4, size=max(j.particles for j in jobs))
     srv = Server(precision=prec, masters=masters)
     cal = [Job(100000 + i, 0.0, 200_000, m, (1e-3, 1e-3, 2e-3), 10.0, 1.0, 10)
@@ -682,7 +683,8 @@ def serve(args, local):
     lat = latency_summary(res)
     line = {
         "metric": "serving p50/p99 job latency and throughput", "precision": args.precision,
-        "arrival_rate_hz": 50.0, "window_s": args.serve_seconds, "jobs": len(res),
+        "arrival_rate_hz": args.serve_rate, "window_s": args.serve_seconds, "jobs": len(res),
+        "device_busy_frac": srv.time["track_gpu_s"] / srv.makespan_s,
         "throughput": {"value": srv.particle_steps / srv.makespan_s, "unit": "particle-steps/s"},
         "particle_steps": srv.particle_steps, "latency_s": lat, "makespan_s": srv.makespan_s,
         "rounds": srv.rounds, "host_time": srv.time, "hbm_budget_gb": srv.budget / 1e9,

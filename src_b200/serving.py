@@ -65,6 +65,88 @@ class MasterBunches:
         return R, P
 
 
+class Preparer:
+    """Prepares the bunches of arriving jobs on a worker thread, ahead of
+    admission: each job's scaled copy of its master bunch is written into one
+    of a few page-locked host buffers (sized for the largest job), so the
+    serving thread only uploads (from pinned memory, at full link speed) while
+    the device runs a round.  Jobs are prepared in arrival order, at most
+    `depth` ahead; a buffer returns to the pool once its job is uploaded."""
+
+    def __init__(self, masters, max_particles, depth=4, realtime=True):
+        import queue
+        import threading
+
+        import torch
+
+        self.masters = masters
+        self.realtime = realtime
+        self.free = queue.Queue()
+        pin = torch.cuda.is_available()
+        for _ in range(depth):
+            self.free.put(tuple(torch.empty((max_particles, 3), dtype=torch.float64, pin_memory=pin).numpy()
+                                for _ in range(2)))
+        self.ready = collections.deque()
+        self.cv = threading.Condition()
+        self.jobs = None
+        self.t0 = None
+        self.prep_s = 0.0
+        self.stop = False
+        self.thread = None
+
+    def start(self, jobs, t0):
+        import threading
+
+        self.jobs = list(jobs)
+        self.t0 = t0
+        self.thread = threading.Thread(target=self._work, daemon=True)
+        self.thread.start()
+
+    def _work(self):
+        for job in self.jobs:
+            # a job is prepared once it has arrived, never before
+            while self.realtime and not self.stop and time.perf_counter() - self.t0 < job.arrival_s:
+                time.sleep(min(0.002, max(0.0, job.arrival_s - (time.perf_counter() - self.t0))))
+            if self.stop:
+                return
+            bufs = self.free.get()
+            if self.stop or bufs is None:
+                return
+            ta = time.perf_counter()
+            n = job.particles
+            R, P = bufs[0][:n], bufs[1][:n]
+            if hasattr(self.masters, "masters"):
+                R0, P0 = self.masters.masters[job.job_id % len(self.masters.masters)]
+                np.multiply(R0[:n], np.asarray(job.sigma), out=R)
+                P[:] = P0[:n]
+                P[:, 2] *= job.bg_z
+            else:
+                R[:], P[:] = self.masters.bunch(job)
+            self.prep_s += time.perf_counter() - ta
+            with self.cv:
+                self.ready.append((job, R, P, bufs))
+                self.cv.notify_all()
+
+    def take(self, job, timeout=60.0):
+        """The prepared (R, P, buffers) of `job` (the next one in arrival order)."""
+        with self.cv:
+            ok = self.cv.wait_for(lambda: self.ready and self.ready[0][0] is job, timeout=timeout)
+            if not ok:
+                raise RuntimeError(f"job {job.job_id} was not prepared in time")
+            _, R, P, bufs = self.ready.popleft()
+        return R, P, bufs
+
+    def give_back(self, bufs):
+        self.free.put(bufs)
+
+    def close(self):
+        self.stop = True
+        for _ in range(2):
+            self.free.put(None)
+        if self.thread is not None:
+            self.thread.join(timeout=10)
+
+
 class Server:
     def __init__(self, precision=scgpu.PLAIN_FP64, hbm_budget_bytes=None, device=0, masters=None, batch=None,
                  keep_results=False):
@@ -106,20 +188,26 @@ class Server:
     def close(self):
         self.batch.close()
 
-    def run(self, jobs, realtime=True):
+    def run(self, jobs, realtime=True, prepare_ahead=4):
         """Serves `jobs`.  With realtime the arrivals are honoured on the wall
         clock; otherwise every job is available at once.  Returns the list of
         Results in completion order.
 
         Each round launches k steps for the current slots and, while the
-        device works, admits the jobs that have arrived (their bunches are
-        prepared and uploaded meanwhile; they join at the next round)."""
+        device works, admits the jobs that have arrived (their bunches were
+        prepared in pinned memory by the Preparer thread and are uploaded
+        meanwhile; they join at the next round).  prepare_ahead = 0 prepares
+        each bunch on the serving thread at admission instead."""
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival_s))
         active = {}   # slot -> [job, remaining steps, admitted_s, footprint]
         joining = {}  # admitted during the current round
         results = []
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
+        prep = None
+        if prepare_ahead > 0 and pending:
+            prep = Preparer(self.masters, max(j.particles for j in pending), depth=prepare_ahead, realtime=realtime)
+            prep.start(pending, t0)
 
         def admit():
             t = now()
@@ -130,8 +218,13 @@ class Server:
                     break
                 pending.popleft()
                 ta = time.perf_counter()
-                R, P = self.masters.bunch(job)
+                if prep is not None:
+                    R, P, bufs = prep.take(job)
+                else:
+                    R, P = self.masters.bunch(job)
                 slot = self.batch.add((job.mesh,) * 3, R, P, DT, job.q_macro, MASS_EV, ref_P=job.ref_P)
+                if prep is not None:
+                    prep.give_back(bufs)
                 self.time["admit_s"] += time.perf_counter() - ta
                 joining[slot] = [job, job.steps, now(), fp]
                 self.used += fp
@@ -170,6 +263,9 @@ class Server:
             if not active and pending and realtime:
                 time.sleep(max(0.0, min(pending[0].arrival_s - now(), 0.01)))
         self.makespan_s = now()
+        if prep is not None:
+            self.time["prepare_s"] = prep.prep_s
+            prep.close()
         return results
 
 

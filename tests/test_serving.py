@@ -104,3 +104,17 @@ def test_latency_summary():
             self.latency_s = lat
     s = latency_summary([R(v) for v in range(1, 101)])
     assert s["jobs"] == 100 and abs(s["p50_s"] - 50.5) < 1e-9 and s["p99_s"] > 98
+
+
+def test_preparer_thread_matches_inline_preparation():
+    """Bunches prepared ahead on the worker thread (into reusable host
+    buffers) give the same admissions and rounds as bunches prepared on the
+    serving thread at admission."""
+    jobs = [job(i, n=500 + 37 * i, steps=10 + 3 * i) for i in range(12)]
+    out = []
+    for ahead in (0, 3):
+        fb = FakeBatch()
+        srv = Server(hbm_budget_bytes=1 << 40, batch=fb, masters=FakeMasters())
+        res = srv.run(jobs, realtime=False, prepare_ahead=ahead)
+        out.append(([r.job.job_id for r in res], fb.tracked))
+    assert out[0] == out[1]
