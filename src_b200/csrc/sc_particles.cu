@@ -365,13 +365,65 @@ __global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, do
     drift_body<DRIFT>(bc, x, y, z, px, py, pz, st, partials, ticket, vb_grid());
 }
 
-// drift_body with the particle state streamed through shared memory: each
-// block walks chunks of kDriftChunk particles, double-buffered; the bulk
-// copies of the next chunk's six arrays are in flight while the threads work
-// on the current one (lane-contiguous reads of the staged doubles).  Same
-// arithmetic and exact min / max as drift_body, so the same bits.
-constexpr int kDriftChunk = 512;
-constexpr size_t kDriftSmem = 2 * 6 * kDriftChunk * sizeof(double);
+// Streams this block's chunks (chunks blk, blk + nblk, ... of kStreamChunk
+// elements) of NA double arrays through shared memory, double-buffered: the
+// bulk copies of the next chunk are in flight while f(i, v) runs on every
+// element i of the current one (v[a] = src[a][i], lane-contiguous reads).
+// bar[0], bar[1] must be initialised barriers.  Returns false, with the
+// copy-timeout flag raised, when a copy did not complete (every thread of the
+// block returns false together, after waiting for its other copy).
+constexpr int kStreamChunk = 512;
+
+template <int NA>
+__device__ __forceinline__ void stream_issue(const double* const (&src)[NA], long long N, long long c, double* buf,
+                                             uint64_t* bar) {
+    const long long first = c * kStreamChunk;
+    const long long count = N - first < kStreamChunk ? N - first : kStreamChunk;
+    double* dst[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) dst[a] = buf + a * kStreamChunk;
+    stage_doubles<NA>(dst, src, first, count, bar);
+}
+
+template <int NA, typename F>
+__device__ __forceinline__ bool stream_chunks(const double* const (&src)[NA], long long N, VB g, double* sm,
+                                              uint64_t* bar, int* err, F&& f) {
+    const long long nchunks = (N + kStreamChunk - 1) / kStreamChunk;
+    if (g.blk < nchunks) stream_issue<NA>(src, N, g.blk, sm, &bar[0]);
+    int k = 0;
+    for (long long c = g.blk; c < nchunks; c += g.nblk, ++k) {
+        const int b = k & 1;
+        double* buf = sm + (size_t)b * NA * kStreamChunk;
+        if (c + g.nblk < nchunks) stream_issue<NA>(src, N, c + g.nblk, sm + (size_t)(b ^ 1) * NA * kStreamChunk,
+                                                   &bar[b ^ 1]);
+        if (__syncthreads_or(!mbar_wait(&bar[b], (unsigned)(k >> 1) & 1u))) {
+            if (threadIdx.x == 0) atomicOr(err, kFlagCopy);
+            if (c + g.nblk < nchunks) mbar_wait(&bar[b ^ 1], (unsigned)((k + 1) >> 1) & 1u);
+            return false;
+        }
+        const long long first = c * kStreamChunk;
+        const int count = (int)(N - first < kStreamChunk ? N - first : kStreamChunk);
+        const int body = count & ~1;
+        for (int j = threadIdx.x; j < count; j += blockDim.x) {
+            double v[NA];
+            if (j < body) {
+#pragma unroll
+                for (int a = 0; a < NA; ++a) v[a] = buf[a * kStreamChunk + j];
+            } else {
+#pragma unroll
+                for (int a = 0; a < NA; ++a) v[a] = src[a][first + j];
+            }
+            f(first + j, v);
+        }
+        __syncthreads();  // buffer b is read before the copies two chunks on land in it
+    }
+    return true;
+}
+
+// drift_body with the particle state streamed through shared memory
+// (stream_chunks).  Same arithmetic and exact min / max as drift_body, so the
+// same bits.
+constexpr size_t kDriftSmem = 2 * 6 * kStreamChunk * sizeof(double);
 
 template <bool DRIFT>
 __device__ __forceinline__ void drift_staged_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
@@ -388,76 +440,34 @@ __device__ __forceinline__ void drift_staged_body(const BunchConst& bc, double* 
         mbar_fence_init();
     }
     __syncthreads();
-    const double* const src[6] = {x, y, z, px, py, pz};
-    const long long nchunks = (bc.N + kDriftChunk - 1) / kDriftChunk;
-    auto buffers = [&](int b) {
-        double* base = sm + (size_t)b * 6 * kDriftChunk;
-        return base;
-    };
-    auto issue = [&](long long c, int b) {
-        const long long first = c * kDriftChunk;
-        const long long count = bc.N - first < kDriftChunk ? bc.N - first : kDriftChunk;
-        double* base = buffers(b);
-        if constexpr (DRIFT) {
-            double* const dst[6] = {base,
-                                    base + kDriftChunk,
-                                    base + 2 * kDriftChunk,
-                                    base + 3 * kDriftChunk,
-                                    base + 4 * kDriftChunk,
-                                    base + 5 * kDriftChunk};
-            stage_doubles<6>(dst, src, first, count, &bar[b]);
-        } else {
-            double* const dst[3] = {base, base + kDriftChunk, base + 2 * kDriftChunk};
-            const double* const s3[3] = {src[0], src[1], src[2]};
-            stage_doubles<3>(dst, s3, first, count, &bar[b]);
-        }
-    };
     double v[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};  // min x,y,z, -max x,y,z
-    if (g.blk < nchunks) issue(g.blk, 0);
-    int k = 0;
-    for (long long c = g.blk; c < nchunks; c += g.nblk, ++k) {
-        const int b = k & 1;
-        if (c + g.nblk < nchunks) issue(c + g.nblk, b ^ 1);
-        if (__syncthreads_or(!mbar_wait(&bar[b], (unsigned)(k >> 1) & 1u))) {
-            if (threadIdx.x == 0) atomicOr(&st->err, kFlagCopy);
-            if (c + g.nblk < nchunks) mbar_wait(&bar[b ^ 1], (unsigned)((k + 1) >> 1) & 1u);
-            return;
-        }
-        const long long first = c * kDriftChunk;
-        const int count = (int)(bc.N - first < kDriftChunk ? bc.N - first : kDriftChunk);
-        const int body = count & ~1;
-        const double* base = buffers(b);
-        for (int j = threadIdx.x; j < count; j += blockDim.x) {
-            const long long i = first + j;
-            double R[3], P[3];
-            if (j < body) {
-                R[0] = base[j], R[1] = base[kDriftChunk + j], R[2] = base[2 * kDriftChunk + j];
-                if constexpr (DRIFT)
-                    P[0] = base[3 * kDriftChunk + j], P[1] = base[4 * kDriftChunk + j], P[2] = base[5 * kDriftChunk + j];
-            } else {
-                R[0] = x[i], R[1] = y[i], R[2] = z[i];
-                if constexpr (DRIFT) P[0] = px[i], P[1] = py[i], P[2] = pz[i];
-            }
-            if constexpr (DRIFT) {
-                push_r(R, P, bc.s_cdt, bc.rs_cdt);
-                double bb[3];
-                trafo_transform_to(*fresh(&r2b_s), R, bb);
-                R[0] = bb[0];
-                R[1] = bb[1];
-                R[2] = bb[2];
-                x[i] = R[0];
-                y[i] = R[1];
-                z[i] = R[2];
-            }
-            v[0] = fmin(v[0], R[0]);
-            v[1] = fmin(v[1], R[1]);
-            v[2] = fmin(v[2], R[2]);
-            v[3] = fmin(v[3], -R[0]);
-            v[4] = fmin(v[4], -R[1]);
-            v[5] = fmin(v[5], -R[2]);
-        }
-        __syncthreads();  // buffer b is read before the copies two chunks on land in it
+    auto bound = [&](const double* R) {
+        v[0] = fmin(v[0], R[0]);
+        v[1] = fmin(v[1], R[1]);
+        v[2] = fmin(v[2], R[2]);
+        v[3] = fmin(v[3], -R[0]);
+        v[4] = fmin(v[4], -R[1]);
+        v[5] = fmin(v[5], -R[2]);
+    };
+    bool ok;
+    if constexpr (DRIFT) {
+        const double* const src[6] = {x, y, z, px, py, pz};
+        ok = stream_chunks<6>(src, bc.N, g, sm, bar, &st->err, [&](long long i, const double* q) {
+            double R[3] = {q[0], q[1], q[2]};
+            const double P[3] = {q[3], q[4], q[5]};
+            push_r(R, P, bc.s_cdt, bc.rs_cdt);
+            double bb[3];
+            trafo_transform_to(*fresh(&r2b_s), R, bb);
+            x[i] = bb[0];
+            y[i] = bb[1];
+            z[i] = bb[2];
+            bound(bb);
+        });
+    } else {
+        const double* const src[3] = {x, y, z};
+        ok = stream_chunks<3>(src, bc.N, g, sm, bar, &st->err, [&](long long, const double* q) { bound(q); });
     }
+    if (!ok) return;
     bounds_tail(bc, v, st, partials, ticket, g);
 }
 
@@ -1441,73 +1451,73 @@ __device__ __forceinline__ bool mixed_particle(const BunchConst& bc, const MeshC
     return ok;
 }
 
-template <typename T, bool BINNED = false, bool EXT = false>
+// STAGED: the particle state streamed through shared memory (stream_chunks,
+// dynamic shared memory sm); the arithmetic is the same either way.
+template <typename T, bool BINNED = false, bool EXT = false, bool STAGED = false>
 __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
                                             double* __restrict__ z, double* __restrict__ px, double* __restrict__ py,
                                             double* __restrict__ pz, const T* __restrict__ E4, StepState* st,
-                                            double* partials, unsigned* ticket, VB g, const double* __restrict__ F8 = nullptr) {
+                                            double* partials, unsigned* ticket, VB g, const double* __restrict__ F8 = nullptr,
+                                            double* sm = nullptr) {
     __shared__ Trafo b2r_s, upd_s;
     __shared__ MeshConsts ms;
     __shared__ double betaC_s;
+    __shared__ __align__(8) uint64_t bar[2];
     load_mesh_consts(ms, st);
     if (threadIdx.x == 0) {
         b2r_s = st->b2r;
         upd_s = st->upd;
         betaC_s = st->betaC;
+        if constexpr (STAGED) {
+            mbar_init(&bar[0], 1);
+            mbar_init(&bar[1], 1);
+            mbar_fence_init();
+        }
     }
     __syncthreads();
     i128 acc[3] = {0, 0, 0};
     bool bad = false;
-    if constexpr (sizeof(T) == sizeof(float) && !BINNED) {
-        for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
-            double R[3] = {x[i], y[i], z[i]};
-            double P[3] = {px[i], py[i], pz[i]};
+    // one particle: state X, P in, new state out to slot i
+    auto one = [&](long long i, const double* X, const double* Pin) {
+        double P[3] = {Pin[0], Pin[1], Pin[2]};
+        double Ru[3], Pu[3];
+        if constexpr (sizeof(T) == sizeof(float) && !BINNED) {
+            double R[3] = {X[0], X[1], X[2]};
             if (!mixed_particle<EXT>(bc, *fresh(&ms), reinterpret_cast<const float*>(E4), *fresh(&b2r_s),
                                      *fresh(&upd_s), *fresh(&betaC_s), st, R, P))
                 bad = true;
-            x[i] = R[0];
-            y[i] = R[1];
-            z[i] = R[2];
-            px[i] = P[0];
-            py[i] = P[1];
-            pz[i] = P[2];
-            acc[0] += ex_from(P[0]);
-            acc[1] += ex_from(P[1]);
-            acc[2] += ex_from(P[2]);
-        }
-    } else
-    for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
-        const double X[3] = {x[i], y[i], z[i]};
-        double P[3] = {px[i], py[i], pz[i]};
-        int l[3];
-        double d[3];
-        const MeshConsts* m = fresh(&ms);
-        if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
-        double Eb[3], Bb[3];
-        if constexpr (BINNED) {
-            cic_gather8(F8, bc.n, l, d, Eb, Bb);
-            Bb[2] = 0.0;
+            Ru[0] = R[0], Ru[1] = R[1], Ru[2] = R[2];
+            Pu[0] = P[0], Pu[1] = P[1], Pu[2] = P[2];
         } else {
-            cic_gather(E4, bc.n, l, d, Eb);
-            const double betaC = *fresh(&betaC_s);
-            Bb[0] = 0.0 - betaC * Eb[1];
-            Bb[1] = 0.0 + betaC * Eb[0];
-            Bb[2] = 0.0;
+            int l[3];
+            double d[3];
+            const MeshConsts* m = fresh(&ms);
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
+            double Eb[3], Bb[3];
+            if constexpr (BINNED) {
+                cic_gather8(F8, bc.n, l, d, Eb, Bb);
+                Bb[2] = 0.0;
+            } else {
+                cic_gather(E4, bc.n, l, d, Eb);
+                const double betaC = *fresh(&betaC_s);
+                Bb[0] = 0.0 - betaC * Eb[1];
+                Bb[1] = 0.0 + betaC * Eb[0];
+                Bb[2] = 0.0;
+            }
+            double R[3], Ef[3], Bf[3];
+            const Trafo* b2r = fresh(&b2r_s);
+            trafo_transform_to(*b2r, X, R);
+            trafo_rotate_to(*b2r, Eb, Ef);
+            trafo_rotate_to(*b2r, Bb, Bf);
+            if (bc.bz_ext != 0.0) Bf[2] += bc.bz_ext;
+            // the beamline elements' fields at R, in the frame of the step's start
+            if constexpr (EXT) add_external_B(bc.sol, bc.nsol, st->ref_to_lab_step, R, Bf);
+            kick_r(P, Ef, Bf, bc.ke, bc.ktn, bc.mass);
+            push_r(R, P, bc.s_cdt, bc.rs_cdt);
+            const Trafo* upd = fresh(&upd_s);
+            trafo_transform_to(*upd, R, Ru);
+            trafo_rotate_to(*upd, P, Pu);
         }
-        double R[3], Ef[3], Bf[3];
-        const Trafo* b2r = fresh(&b2r_s);
-        trafo_transform_to(*b2r, X, R);
-        trafo_rotate_to(*b2r, Eb, Ef);
-        trafo_rotate_to(*b2r, Bb, Bf);
-        if (bc.bz_ext != 0.0) Bf[2] += bc.bz_ext;
-        // the beamline elements' fields at R, in the frame of the step's start
-        if constexpr (EXT) add_external_B(bc.sol, bc.nsol, st->ref_to_lab_step, R, Bf);
-        kick_r(P, Ef, Bf, bc.ke, bc.ktn, bc.mass);
-        push_r(R, P, bc.s_cdt, bc.rs_cdt);
-        double Ru[3], Pu[3];
-        const Trafo* upd = fresh(&upd_s);
-        trafo_transform_to(*upd, R, Ru);
-        trafo_rotate_to(*upd, P, Pu);
         x[i] = Ru[0];
         y[i] = Ru[1];
         z[i] = Ru[2];
@@ -1517,6 +1527,17 @@ __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __rest
         acc[0] += ex_from(Pu[0]);
         acc[1] += ex_from(Pu[1]);
         acc[2] += ex_from(Pu[2]);
+    };
+    if constexpr (STAGED) {
+        const double* const src[6] = {x, y, z, px, py, pz};
+        if (!stream_chunks<6>(src, bc.N, g, sm, bar, &st->err, [&](long long i, const double* q) { one(i, q, q + 3); }))
+            return;
+    } else {
+        for (long long i = g.blk * (long long)blockDim.x + threadIdx.x; i < bc.N; i += (long long)g.nblk * blockDim.x) {
+            const double X[3] = {x[i], y[i], z[i]};
+            const double P[3] = {px[i], py[i], pz[i]};
+            one(i, X, P);
+        }
     }
     if (bad) atomicOr(&st->err, kFlagGuard);
     i128* xpart = reinterpret_cast<i128*>(partials);
@@ -1547,6 +1568,16 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
                                                                   const T* __restrict__ E4, StepState* st, double* partials,
                                                                   unsigned* ticket) {
     gather_body<T, false, EXT>(bc, x, y, z, px, py, pz, E4, st, partials, ticket, vb_grid());
+}
+constexpr size_t kGatherSmem = 2 * 6 * kStreamChunk * sizeof(double);
+template <typename T, bool EXT = false>
+__global__ void __launch_bounds__(kThreads, 3) k_gather_staged(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
+                                                               double* __restrict__ z, double* __restrict__ px,
+                                                               double* __restrict__ py, double* __restrict__ pz,
+                                                               const T* __restrict__ E4, StepState* st, double* partials,
+                                                               unsigned* ticket) {
+    extern __shared__ __align__(16) double gather_sm[];
+    gather_body<T, false, EXT, true>(bc, x, y, z, px, py, pz, E4, st, partials, ticket, vb_grid(), nullptr, gather_sm);
 }
 template <bool EXT = false>
 __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push_bins(BunchConst bc, double* __restrict__ x,
@@ -1877,6 +1908,10 @@ void prime_particle_grids() {
     cudaFuncSetAttribute(k_drift_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDriftSmem);
     cudaFuncSetAttribute(k_drift_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDriftSmem);
     cudaFuncSetAttribute(k_deposit_runs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
+    cudaFuncSetAttribute(k_gather_staged<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
+    cudaFuncSetAttribute(k_gather_staged<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
+    cudaFuncSetAttribute(k_gather_staged<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
+    cudaFuncSetAttribute(k_gather_staged<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
     cudaFuncSetAttribute(k_deposit_runs_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
     const void* kernels[] = {(const void*)k_drift_staged<true>,
                              (const void*)k_drift_staged<false>,
@@ -1892,6 +1927,9 @@ void prime_particle_grids() {
                              (const void*)k_gather_kick_push_bins<true>};
     for (const void* k : kernels) resident_blocks(k, (k == (const void*)k_drift_staged<true> ||
                                                       k == (const void*)k_drift_staged<false>) ? kDriftSmem : 0);
+    const void* staged[] = {(const void*)k_gather_staged<double, false>, (const void*)k_gather_staged<double, true>,
+                            (const void*)k_gather_staged<float, false>, (const void*)k_gather_staged<float, true>};
+    for (const void* k : staged) resident_blocks(k, kGatherSmem);
 }
 
 void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s) {
@@ -1959,6 +1997,21 @@ void launch_grad(const DevBunch& b, cudaStream_t s) {
 
 void launch_gather_kick_push(const DevBunch& b, bool stats, cudaStream_t s) {
     const bool ext = b.bc.nsol > 0;
+    if (stream_particles()) {
+        if (b.precision == 0) {
+            auto k = ext ? k_gather_staged<double, true> : k_gather_staged<double, false>;
+            k<<<wave_grid(k, b, kGatherSmem), kThreads, kGatherSmem, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz,
+                                                                           (const double*)b.E4, b.st, b.partials,
+                                                                           b.ticket);
+        } else {
+            auto k = ext ? k_gather_staged<float, true> : k_gather_staged<float, false>;
+            k<<<wave_grid(k, b, kGatherSmem), kThreads, kGatherSmem, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz,
+                                                                           (const float*)b.E4, b.st, b.partials,
+                                                                           b.ticket);
+        }
+        if (stats) launch_reduce_stats(b, s);
+        return;
+    }
     if (b.precision == 0) {
         auto k = ext ? k_gather_kick_push<double, true> : k_gather_kick_push<double, false>;
         k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, (const double*)b.E4, b.st,
