@@ -420,66 +420,6 @@ __device__ __forceinline__ bool stream_chunks(const double* const (&src)[NA], lo
     return true;
 }
 
-// drift_body with the particle state streamed through shared memory
-// (stream_chunks).  Same arithmetic and exact min / max as drift_body, so the
-// same bits.
-constexpr size_t kDriftSmem = 2 * 6 * kStreamChunk * sizeof(double);
-
-template <bool DRIFT>
-__device__ __forceinline__ void drift_staged_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
-                                                  double* __restrict__ z, const double* __restrict__ px,
-                                                  const double* __restrict__ py, const double* __restrict__ pz,
-                                                  StepState* st, double* partials, unsigned* ticket, VB g,
-                                                  double* sm) {
-    __shared__ Trafo r2b_s;
-    __shared__ __align__(8) uint64_t bar[2];
-    if (threadIdx.x == 0) {
-        r2b_s = st->r2b;
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    double v[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};  // min x,y,z, -max x,y,z
-    auto bound = [&](const double* R) {
-        v[0] = fmin(v[0], R[0]);
-        v[1] = fmin(v[1], R[1]);
-        v[2] = fmin(v[2], R[2]);
-        v[3] = fmin(v[3], -R[0]);
-        v[4] = fmin(v[4], -R[1]);
-        v[5] = fmin(v[5], -R[2]);
-    };
-    bool ok;
-    if constexpr (DRIFT) {
-        const double* const src[6] = {x, y, z, px, py, pz};
-        ok = stream_chunks<6>(src, bc.N, g, sm, bar, &st->err, [&](long long i, const double* q) {
-            double R[3] = {q[0], q[1], q[2]};
-            const double P[3] = {q[3], q[4], q[5]};
-            push_r(R, P, bc.s_cdt, bc.rs_cdt);
-            double bb[3];
-            trafo_transform_to(*fresh(&r2b_s), R, bb);
-            x[i] = bb[0];
-            y[i] = bb[1];
-            z[i] = bb[2];
-            bound(bb);
-        });
-    } else {
-        const double* const src[3] = {x, y, z};
-        ok = stream_chunks<3>(src, bc.N, g, sm, bar, &st->err, [&](long long, const double* q) { bound(q); });
-    }
-    if (!ok) return;
-    bounds_tail(bc, v, st, partials, ticket, g);
-}
-
-template <bool DRIFT>
-__global__ void __launch_bounds__(kThreads, 3) k_drift_staged(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
-                                                           double* __restrict__ z, const double* __restrict__ px,
-                                                           const double* __restrict__ py, const double* __restrict__ pz,
-                                                           StepState* st, double* partials, unsigned* ticket) {
-    extern __shared__ __align__(16) double drift_sm[];
-    drift_staged_body<DRIFT>(bc, x, y, z, px, py, pz, st, partials, ticket, vb_grid(), drift_sm);
-}
-
 // The reference particle needs no particle data: it runs beside the deposit.
 __device__ __forceinline__ void advance_reference_body(const BunchConst& bc, StepState* st, VB g) {
     if (threadIdx.x == 0 && g.blk == 0)
@@ -659,141 +599,6 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
     }
     if (bad) atomicOr(&st->err, kFlagGuard);
 }
-// Charge deposit by runs.  The arrays are in cell order, so consecutive
-// particles mostly share a cell: each block takes chunks of kDepChunk
-// consecutive particles, stages their positions into shared memory with bulk
-// asynchronous copies, and each thread walks kRunK consecutive particles of a
-// chunk, adding their eight fixed-point corner charges into 64-bit registers
-// while the cell stays the same; when the cell changes the thread adds the
-// eight sums to the node accumulators, and the last runs of the warp's lanes
-// are summed per cell across the warp before one lane adds them.  kRunK is odd
-// so that the threads' strided reads of the staged doubles fall into
-// distinct shared-memory banks.  The fixed-point charges and their integer
-// sums are those of deposit_body, so rho is bitwise the same.
-constexpr int kRunK = 9;
-constexpr int kDepThreads = 256;
-constexpr int kDepChunk = kDepThreads * kRunK;  // even: chunk starts stay 16-byte aligned
-constexpr size_t kDepSmem = 3 * kDepChunk * sizeof(double) + 16;
-
-__device__ __forceinline__ void flush_run(unsigned long long* __restrict__ acc, uint32_t key, const long long (&a)[8],
-                                          int nx, int nxy) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int node = (int)key + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
-        if (a[k] != 0) acc_add(acc + 2 * (size_t)node, a[k]);
-    }
-}
-
-template <bool BINNED>
-__device__ __forceinline__ void deposit_runs_body(const BunchConst& bc, const double* __restrict__ x,
-                                                  const double* __restrict__ y, const double* __restrict__ z,
-                                                  const int* __restrict__ bin, int nactive, StepState* st,
-                                                  unsigned long long* __restrict__ acc, VB g, double* sm) {
-    __shared__ MeshConsts ms;
-    __shared__ double qdt_s, to_int_s;
-    __shared__ __align__(8) uint64_t bar;
-    load_mesh_consts(ms, st);
-    if (threadIdx.x == 0) {
-        qdt_s = st->qdt;
-        to_int_s = ldexp(1.0, kFxFrac - fx_exponent(st->qdt));
-        mbar_init(&bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    double* const buf[3] = {sm, sm + kDepChunk, sm + 2 * kDepChunk};
-    const double* const src[3] = {x, y, z};
-    const int nx = bc.n[0], nxy = bc.n[0] * bc.n[1];
-    const uint32_t M = (uint32_t)nxy * (uint32_t)bc.n[2];
-    const long long nchunks = (bc.N + kDepChunk - 1) / kDepChunk;
-    bool bad = false;
-    unsigned parity = 0;
-    for (long long c = g.blk; c < nchunks; c += g.nblk, parity ^= 1u) {
-        const long long first = c * kDepChunk;
-        const long long count = bc.N - first < kDepChunk ? bc.N - first : kDepChunk;
-        const long long body = stage_doubles<3>(buf, src, first, count, &bar);
-        // a lost copy: flag it and leave the loop on every thread together
-        if (__syncthreads_or(!mbar_wait(&bar, parity))) {
-            if (threadIdx.x == 0) atomicOr(&st->err, kFlagCopy);
-            return;
-        }
-        const double to_int = to_int_s, qdt = qdt_s;
-        uint32_t run = 0xffffffffu;
-        long long a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        const int i0 = threadIdx.x * kRunK;
-        for (int j = 0; j < kRunK; ++j) {
-            const int i = i0 + j;
-            if (i >= count) break;
-            int bk = 0;
-            if constexpr (BINNED) {
-                bk = bin[first + i];
-                if ((unsigned)bk >= (unsigned)nactive) continue;
-            }
-            double X[3];
-            if (i < body) {
-                X[0] = buf[0][i], X[1] = buf[1][i], X[2] = buf[2][i];
-            } else {
-                X[0] = x[first + i], X[1] = y[first + i], X[2] = z[first + i];
-            }
-            int l[3];
-            double d[3];
-            const MeshConsts* m = fresh(&ms);
-            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
-            double v[8];
-            cic_charge(d, qdt, v);
-            const uint32_t key = (uint32_t)(l[0] + nx * l[1] + nxy * l[2]) + (uint32_t)bk * M;
-            if (key != run) {
-                if (run != 0xffffffffu) flush_run(acc, run, a, nx, nxy);
-                run = key;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) a[k] = 0;
-            }
-#pragma unroll
-            for (int k = 0; k < 8; ++k) a[k] += __double2ll_rn(v[k] * to_int);
-        }
-        // The lanes' last runs: consecutive lanes in one cell are summed
-        // together first (one pass of full-warp redux.sync per group, each sum
-        // as three limbs of at most 21 bits so that 32 of them fit 32 bits),
-        // and the group's first lane adds the sums to the node accumulators.
-        const int lane = threadIdx.x & 31;
-        const unsigned grp = __match_any_sync(kFull, run);
-        const bool multi = __popc(grp) > 1 && run != 0xffffffffu;
-        if (run != 0xffffffffu && !multi) flush_run(acc, run, a, nx, nxy);
-        unsigned leaders = __ballot_sync(kFull, multi && lane == __ffs(grp) - 1);
-        while (leaders) {
-            const int ld = __ffs(leaders) - 1;
-            leaders &= leaders - 1;
-            const bool in = (__shfl_sync(kFull, grp, ld) >> lane) & 1u;
-            long long sum[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const long long v = in ? a[k] : 0;
-                const unsigned lo = (unsigned)(v & 0x1fffff), mid = (unsigned)((v >> 21) & 0x1fffff);
-                const int hi = (int)(v >> 42);
-                sum[k] = (long long)__reduce_add_sync(kFull, hi) * (1ll << 42) +
-                         (long long)__reduce_add_sync(kFull, mid) * (1ll << 21) + (long long)__reduce_add_sync(kFull, lo);
-            }
-            if (lane == ld) flush_run(acc, run, sum, nx, nxy);
-        }
-        __syncthreads();  // the buffer is read before the next chunk's copies land in it
-    }
-    if (bad) atomicOr(&st->err, kFlagGuard);
-}
-__global__ void __launch_bounds__(kDepThreads) k_deposit_runs(BunchConst bc, const double* __restrict__ x,
-                                                              const double* __restrict__ y,
-                                                              const double* __restrict__ z, StepState* st,
-                                                              unsigned long long* __restrict__ acc) {
-    extern __shared__ __align__(16) double dep_sm[];
-    deposit_runs_body<false>(bc, x, y, z, nullptr, 0, st, acc, vb_grid(), dep_sm);
-}
-__global__ void __launch_bounds__(kDepThreads) k_deposit_runs_bins(BunchConst bc, const double* __restrict__ x,
-                                                                   const double* __restrict__ y,
-                                                                   const double* __restrict__ z,
-                                                                   const int* __restrict__ bin, int nactive,
-                                                                   StepState* st, unsigned long long* __restrict__ acc) {
-    extern __shared__ __align__(16) double dep_sm[];
-    deposit_runs_body<true>(bc, x, y, z, bin, nactive, st, acc, vb_grid(), dep_sm);
-}
-
 __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
                                                       const double* __restrict__ z, StepState* st,
                                                       unsigned long long* __restrict__ acc) {
@@ -1884,10 +1689,8 @@ int wave_grid(K kernel, const DevBunch& b, size_t smem = 0) {
     return blocks < b.red_blocks ? blocks : b.red_blocks;
 }
 
-// The run deposit is the default; SCGPU_DEPOSIT=warp selects the warp-group
-// deposit (same bits) for comparisons.
-// Particle kernels stream the particle state through shared memory with bulk
-// copies (default); SCGPU_STREAM=0 selects the direct-load kernels (same bits).
+// The gather streams the particle state through shared memory with bulk
+// copies (default); SCGPU_STREAM=0 selects the direct-load kernel (same bits).
 bool stream_particles() {
     static const bool on = [] {
         const char* e = std::getenv("SCGPU_STREAM");
@@ -1896,26 +1699,13 @@ bool stream_particles() {
     return on;
 }
 
-bool deposit_by_runs() {
-    static const bool runs = [] {
-        const char* e = std::getenv("SCGPU_DEPOSIT");
-        return !(e && std::string(e) == "warp");
-    }();
-    return runs;
-}
 
 void prime_particle_grids() {
-    cudaFuncSetAttribute(k_drift_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDriftSmem);
-    cudaFuncSetAttribute(k_drift_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDriftSmem);
-    cudaFuncSetAttribute(k_deposit_runs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
     cudaFuncSetAttribute(k_gather_staged<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
     cudaFuncSetAttribute(k_gather_staged<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
     cudaFuncSetAttribute(k_gather_staged<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
     cudaFuncSetAttribute(k_gather_staged<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
-    cudaFuncSetAttribute(k_deposit_runs_bins, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
-    const void* kernels[] = {(const void*)k_drift_staged<true>,
-                             (const void*)k_drift_staged<false>,
-                             (const void*)k_drift_to_beam<true>,
+    const void* kernels[] = {(const void*)k_drift_to_beam<true>,
                              (const void*)k_drift_to_beam<false>,
                              (const void*)k_deposit,
                              (const void*)k_deposit_bins,
@@ -1925,8 +1715,7 @@ void prime_particle_grids() {
                              (const void*)k_gather_kick_push<float, true>,
                              (const void*)k_gather_kick_push_bins<false>,
                              (const void*)k_gather_kick_push_bins<true>};
-    for (const void* k : kernels) resident_blocks(k, (k == (const void*)k_drift_staged<true> ||
-                                                      k == (const void*)k_drift_staged<false>) ? kDriftSmem : 0);
+    for (const void* k : kernels) resident_blocks(k);
     const void* staged[] = {(const void*)k_gather_staged<double, false>, (const void*)k_gather_staged<double, true>,
                             (const void*)k_gather_staged<float, false>, (const void*)k_gather_staged<float, true>};
     for (const void* k : staged) resident_blocks(k, kGatherSmem);
@@ -1938,12 +1727,6 @@ void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s) {
 }
 
 void launch_drift_to_beam(const DevBunch& b, bool drift, cudaStream_t s) {
-    if (stream_particles()) {
-        auto k = drift ? k_drift_staged<true> : k_drift_staged<false>;
-        k<<<wave_grid(k, b, kDriftSmem), kThreads, kDriftSmem, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials,
-                                                         b.ticket);
-        return;
-    }
     auto k = drift ? k_drift_to_beam<true> : k_drift_to_beam<false>;
     k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials, b.ticket);
 }
@@ -1956,12 +1739,6 @@ void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s) {
 }
 
 void launch_deposit(const DevBunch& b, cudaStream_t s) {
-    if (deposit_by_runs()) {
-        const long long nchunks = (b.bc.N + kDepChunk - 1) / kDepChunk;
-        const int g = (int)(nchunks < 1 ? 1 : nchunks);
-        k_deposit_runs<<<g, kDepThreads, kDepSmem, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
-        return;
-    }
     k_deposit<<<wave_grid(k_deposit, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
 }
 
@@ -2045,13 +1822,6 @@ void launch_bin_gammas(const DevBunch& b, cudaStream_t s) {
 }
 
 void launch_deposit_bins(const DevBunch& b, cudaStream_t s) {
-    if (deposit_by_runs()) {
-        const long long nchunks = (b.bc.N + kDepChunk - 1) / kDepChunk;
-        const int g = (int)(nchunks < 1 ? 1 : nchunks);
-        k_deposit_runs_bins<<<g, kDepThreads, kDepSmem, s>>>(b.bc, b.x, b.y, b.z, b.bin, b.nactive, b.st,
-                                                             b.nacc_bins);
-        return;
-    }
     k_deposit_bins<<<wave_grid(k_deposit_bins, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.bin, b.nactive, b.st,
                                                                       b.nacc_bins);
 }
