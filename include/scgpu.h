@@ -17,9 +17,11 @@
  *   scgpu_compute_potential, scgpu_compute_potential_device
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr)
  *       (src/Solvers/PoissonSolver.h:28; FFTPoissonSolver.cpp:337-382)
- *   scgpu_add_solenoid, scgpu_clear_elements, scgpu_fieldmap_astra1d
+ *   scgpu_add_solenoid, scgpu_add_rfcavity, scgpu_clear_elements,
+ *   scgpu_fieldmap_astra1d, scgpu_fieldmap_astra1d_dynamic
  *       ParallelTTracker::computeExternalFields (ParallelTTracker.cpp:595-643)
- *       with Solenoid::apply and Astra1DMagnetoStatic (see below)
+ *       with Solenoid::apply / Astra1DMagnetoStatic and RFCavity::apply /
+ *       Astra1DDynamic (see below)
  *   scgpu_set_exchange
  *       the MPI reductions of a distributed bunch (get_bounds, calcMoments,
  *       the scatter into the distributed rho field) as an exchange callback
@@ -215,6 +217,23 @@ int scgpu_add_solenoid(scgpu_ctx* ctx, const char* fieldmap_path, double elemedg
 int scgpu_clear_elements(scgpu_ctx* ctx);
 int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin, double* zend,
                            double* period);
+
+/* RFCAVITY elements (src/Classic/AbsBeamline/RFCavity.cpp:232-310, built by
+ * src/Elements/OpalCavity.cpp:150-195) with a 1D dynamic field map in ASTRA
+ * format (src/Classic/Fields/Astra1DDynamic.cpp: header "AstraDynamic
+ * <accuracy> [TRUE|FALSE]", the frequency in MHz, then "z Ez" lines), at
+ * ELEMEDGE on a straight beamline along z, with VOLT [MV/m], FREQ [MHz] and
+ * LAG [rad]: inside the map's z range the particles see
+ * E += VOLT cos(omega t + LAG) E_map and B -= VOLT sin(omega t + LAG) B_map
+ * at t = the step's start + dT / 2, the reference particle at the end of
+ * the step - dT / 2 (ParallelTTracker.cpp:628, :1149).  They share the
+ * table of 8 elements with the solenoids.  scgpu_fieldmap_astra1d_dynamic
+ * returns the map's coefficients (scaled to V/m per MV/m), first and last z,
+ * Fourier period and frequency [MHz]. */
+int scgpu_add_rfcavity(scgpu_ctx* ctx, const char* fieldmap_path, double elemedge, double volt_mv_per_m,
+                       double freq_mhz, double lag_rad);
+int scgpu_fieldmap_astra1d_dynamic(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin,
+                                   double* zend, double* period, double* frequency_mhz);
 
 /* FIELDSOLVER BCFFTZ=PERIODIC (FFTPoissonSolver(..., bcz="PERIODIC"),
  * src/Solvers/FFTPoissonSolver.cpp:60, :130-155, :189-190, :661-662): the

@@ -56,8 +56,10 @@ class Debug(C.Structure):
 
 
 class Solenoid(C.Structure):
+    """A beamline element with a 1D map: kind 0 SOLENOID, kind 1 RFCAVITY."""
     _fields_ = [("edge", C.c_double), ("scale", C.c_double), ("zbegin", C.c_double), ("range", C.c_double),
-                ("period", C.c_double), ("accuracy", C.c_int), ("pad_", C.c_int), ("coefs", C.c_double * 255)]
+                ("period", C.c_double), ("accuracy", C.c_int), ("kind", C.c_int), ("omega", C.c_double),
+                ("phase", C.c_double), ("xlrep", C.c_double), ("coefs", C.c_double * 255)]
 
 
 class BeamParams(C.Structure):
@@ -232,8 +234,33 @@ def make_solenoid(coefs, zbegin, zend, period, edge, ks):
     return e
 
 
+def make_rfcavity(coefs, zbegin, zend, period, freq_map_mhz, edge, volt, freq_mhz, lag):
+    """RFCAVITY (OpalCavity.cpp:150-195, RFCavity::initialise :286-310): the
+    element's omega = 1e6 * two_pi * FREQ unless it differs from the map's by
+    more than 1 %; the off-axis wave number from the map's frequency."""
+    e = make_solenoid(coefs, zbegin, zend, period, edge, volt)
+    two_pi = 2 * 3.14159265358979323846
+    omega_map = freq_map_mhz * (two_pi * 1e6)
+    omega = 1e6 * two_pi * freq_mhz
+    if abs((omega - omega_map) / omega) > 0.01:
+        omega = omega_map
+    e.kind, e.omega, e.phase, e.xlrep = 1, omega, lag, omega_map / c_light()
+    return e
+
+
+def rfcavity_field(element, R, t):
+    """E [V/m] and B [T] of one RF cavity at points R (element frame), time t."""
+    R = _f64(R)
+    E, B = np.zeros_like(R), np.zeros_like(R)
+    for i in range(R.shape[0]):
+        e, b = (C.c_double * 3)(), (C.c_double * 3)()
+        lib().sco_rfcavity_field(C.byref(element), R[i].ctypes.data_as(_dp), C.c_double(t), e, b)
+        E[i], B[i] = list(e), list(b)
+    return E, B
+
+
 def set_solenoids(elements):
-    """SOLENOID elements applied by the tracker (computeExternalFields)."""
+    """SOLENOID / RFCAVITY elements applied by the tracker (computeExternalFields)."""
     arr = (Solenoid * max(len(elements), 1))(*elements)
     rc = lib().sco_set_solenoids(arr, C.c_int(len(elements)))
     if rc:

@@ -1421,13 +1421,68 @@ void sco_solenoid_field(const sco_solenoid* e, const double* R, double* B) {
     B[2] = e->scale * tB[2];
 }
 
+/* RFCavity::apply (RFCavity.cpp:232-249) with Astra1DDynamic::getFieldstrength
+ * (Astra1DDynamic.cpp:192-229): E and B of one element at R (element frame)
+ * and time t added to E, B; nothing outside [zbegin, zbegin + range). */
+void sco_rfcavity_field(const sco_solenoid* e, const double* R, double t, double* E, double* B) {
+    const double tmpR[3] = {R[0], R[1], R[2] - e->zbegin};
+    if (!(tmpR[2] >= 0.0 && tmpR[2] < e->range)) return;
+    const double two_pi = 2 * SCO_PI;
+    const double RR2 = tmpR[0] * tmpR[0] + tmpR[1] * tmpR[1];
+    const double kz = two_pi * tmpR[2] / e->period + SCO_PI;
+    double ez = e->coefs[0], ezp = 0.0, ezpp = 0.0, ezppp = 0.0;
+    int n = 1;
+    for (int l = 1; l < e->accuracy; ++l, n += 2) {
+        double somefactor_base = two_pi / e->period * l;
+        double somefactor = 1.0;
+        double coskzl = cos(kz * l);
+        double sinkzl = sin(kz * l);
+        ez += (e->coefs[n] * coskzl - e->coefs[n + 1] * sinkzl);
+        somefactor *= somefactor_base;
+        ezp += somefactor * (-e->coefs[n] * sinkzl - e->coefs[n + 1] * coskzl);
+        somefactor *= somefactor_base;
+        ezpp += somefactor * (-e->coefs[n] * coskzl + e->coefs[n + 1] * sinkzl);
+        somefactor *= somefactor_base;
+        ezppp += somefactor * (e->coefs[n] * sinkzl + e->coefs[n + 1] * coskzl);
+    }
+    const double f = -(ezpp + ez * e->xlrep * e->xlrep) / 16.;
+    const double fp = -(ezppp + ezp * e->xlrep * e->xlrep) / 16.;
+    const double EfieldR = -(ezp / 2. + fp * RR2);
+    const double BfieldT = (ez / 2. + f * RR2) * e->xlrep / SCO_C;
+    double tE[3] = {0.0, 0.0, 0.0}, tB[3] = {0.0, 0.0, 0.0};
+    tE[0] += EfieldR * tmpR[0];
+    tE[1] += EfieldR * tmpR[1];
+    tE[2] += ez + 4. * f * RR2;
+    tB[0] += -BfieldT * tmpR[1];
+    tB[1] += BfieldT * tmpR[0];
+    const double c = e->scale * cos(e->omega * t + e->phase);
+    const double s = e->scale * sin(e->omega * t + e->phase);
+    for (int d = 0; d < 3; ++d) {
+        E[d] += c * tE[d];
+        B[d] -= s * tB[d];
+    }
+}
+
+/* one element's E (RF cavities) and B at R (element frame), time t */
+static void element_field(const sco_solenoid* e, const double* R, double t, double* E, double* B) {
+    E[0] = E[1] = E[2] = 0.0;
+    if (e->kind == 1) {
+        B[0] = B[1] = B[2] = 0.0;
+        sco_rfcavity_field(e, R, t, E, B);
+    } else {
+        sco_solenoid_field(e, R, B);
+    }
+}
+
 static void element_lab2local(const sco_solenoid* e, sco_trafo* t) {
     const double o[3] = {0.0, 0.0, e->edge}, q[4] = {1.0, 0.0, 0.0, 0.0};
     sco_trafo_make(t, o, q);
 }
 
-/* the particles: refToLocal = misalignment * (lab2local * referenceToLab) */
-static void add_element_fields(const sco_trafo* ref_to_lab, long long n, const double* R, double* Bf) {
+/* the particles at time t: refToLocal = misalignment * (lab2local *
+   referenceToLab); E and B rotated back (localToRef.rotateTo) */
+static void add_element_fields(const sco_trafo* ref_to_lab, long long n, const double* R, double t, double* Ef,
+                               double* Bf) {
     for (int k = 0; k < g_nsol; ++k) {
         sco_trafo l2l, r2loc, mis;
         element_lab2local(&g_sol[k], &l2l);
@@ -1441,30 +1496,42 @@ static void add_element_fields(const sco_trafo* ref_to_lab, long long n, const d
         sco_trafo_invert(&loc2r);
         SCO_PAR
         for (long long i = 0; i < n; ++i) {
-            double loc[3], Bl[3], Br[3];
+            double loc[3], El[3], Bl[3], Er[3], Br[3];
             trafo_transform_to(&r2loc, R + 3 * i, loc);
-            sco_solenoid_field(&g_sol[k], loc, Bl);
+            element_field(&g_sol[k], loc, t, El, Bl);
             trafo_rotate_to(&loc2r, Bl, Br);
             Bf[3 * i + 0] += Br[0];
             Bf[3 * i + 1] += Br[1];
             Bf[3 * i + 2] += Br[2];
+            if (g_sol[k].kind == 1) {
+                trafo_rotate_to(&loc2r, El, Er);
+                Ef[3 * i + 0] += Er[0];
+                Ef[3 * i + 1] += Er[1];
+                Ef[3 * i + 2] += Er[2];
+            }
         }
     }
 }
 
-/* the reference particle: refToLocal = lab2local * referenceToLab, B rotated from */
-static void add_element_fields_ref(const sco_trafo* ref_to_lab, const double* R, double* Bf) {
+/* the reference particle at time t: refToLocal = lab2local * referenceToLab,
+   E and B rotated from */
+static void add_element_fields_ref(const sco_trafo* ref_to_lab, const double* R, double t, double* Ef, double* Bf) {
     for (int k = 0; k < g_nsol; ++k) {
         sco_trafo r2loc;
         element_lab2local(&g_sol[k], &r2loc);
         sco_trafo_compose(&r2loc, ref_to_lab);
-        double loc[3], Bl[3];
+        double loc[3], El[3], Bl[3];
         trafo_transform_to(&r2loc, R, loc);
-        sco_solenoid_field(&g_sol[k], loc, Bl);
+        element_field(&g_sol[k], loc, t, El, Bl);
         const double* M = r2loc.M;
         Bf[0] += M[0] * Bl[0] + M[3] * Bl[1] + M[6] * Bl[2];
         Bf[1] += M[1] * Bl[0] + M[4] * Bl[1] + M[7] * Bl[2];
         Bf[2] += M[2] * Bl[0] + M[5] * Bl[1] + M[8] * Bl[2];
+        if (g_sol[k].kind == 1) {
+            Ef[0] += M[0] * El[0] + M[3] * El[1] + M[6] * El[2];
+            Ef[1] += M[1] * El[0] + M[4] * El[1] + M[7] * El[2];
+            Ef[2] += M[2] * El[0] + M[5] * El[1] + M[8] * El[2];
+        }
     }
 }
 
@@ -1526,7 +1593,8 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
         SCO_PAR
         for (long long i = 0; i < n; ++i) Bf[3 * i + 2] += prm->bz_ext;
     }
-    add_element_fields(&tr->ref_to_lab, n, R, Bf);
+    /* the particles' field time: getT() + 0.5 dt (:628) */
+    add_element_fields(&tr->ref_to_lab, n, R, tr->t + 0.5 * dT, Ef, Bf);
     if (dbg && dbg->Ef) memcpy(dbg->Ef, Ef, 3 * n * sizeof(double));
     if (dbg && dbg->Bf) memcpy(dbg->Bf, Bf, 3 * n * sizeof(double));
     /* timeIntegration2: kick + push (:450-491) */
@@ -1539,13 +1607,14 @@ static int tracker_step(sco_tracker* tr, long long n, double* R, double* P, doub
         const double scaleFactor = SCO_C * dt;
         double* rr = tr->ref_R;
         double* rp = tr->ref_P;
-        double zero[3] = {0.0, 0.0, 0.0}, bref[3] = {0.0, 0.0, 0.0};
+        double eref[3] = {0.0, 0.0, 0.0}, bref[3] = {0.0, 0.0, 0.0};
         rr[0] /= scaleFactor; rr[1] /= scaleFactor; rr[2] /= scaleFactor;
         { double g = sqrt(1.0 + dot3(rp, rp)); rr[0] += 0.5 * rp[0] / g; rr[1] += 0.5 * rp[1] / g; rr[2] += 0.5 * rp[2] / g; }
         rr[0] *= scaleFactor; rr[1] *= scaleFactor; rr[2] *= scaleFactor;
-        add_element_fields_ref(&tr->ref_to_lab, rr, bref);
+        /* the reference particle's field time: getT() - 0.5 dt (:1149) */
+        add_element_fields_ref(&tr->ref_to_lab, rr, tr->t - 0.5 * dt, eref, bref);
         if (prm->bz_ext != 0.0) bref[2] += prm->bz_ext;
-        kick_one(rp, zero, bref, dt, prm->mass, prm->charge);
+        kick_one(rp, eref, bref, dt, prm->mass, prm->charge);
         rr[0] /= scaleFactor; rr[1] /= scaleFactor; rr[2] /= scaleFactor;
         { double g = sqrt(1.0 + dot3(rp, rp)); rr[0] += 0.5 * rp[0] / g; rr[1] += 0.5 * rp[1] / g; rr[2] += 0.5 * rp[2] / g; }
         rr[0] *= scaleFactor; rr[1] *= scaleFactor; rr[2] *= scaleFactor;

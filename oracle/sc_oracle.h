@@ -125,18 +125,21 @@ void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, doub
 int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const double* R, const double* P,
                             double* Ef, double* Bf, sco_debug* dbg);
 
-/* SOLENOID elements with ASTRA 1D magnetostatic maps (Solenoid.cpp:163-193,
- * Astra1DMagnetoStatic.cpp:162-196): the tracker adds their fields
+/* Elements with ASTRA 1D field maps: SOLENOID (kind 0; Solenoid.cpp:163-193,
+ * Astra1DMagnetoStatic.cpp:162-196) and RFCAVITY (kind 1; RFCavity.cpp:
+ * 232-270, Astra1DDynamic.cpp:192-229): the tracker adds their fields
  * (computeExternalFields, ParallelTTracker.cpp:614-643) */
 #define SCO_MAX_ELEMENTS 8
 typedef struct {
     double edge, scale, zbegin, range, period;
     int accuracy;
-    int pad_;
+    int kind;
+    double omega, phase, xlrep; /* RF: angular frequency, LAG, map's omega / c */
     double coefs[255];
 } sco_solenoid;
 int sco_set_solenoids(const sco_solenoid* s, int n);
 void sco_solenoid_field(const sco_solenoid* e, const double* R, double* B);
+void sco_rfcavity_field(const sco_solenoid* e, const double* R, double t, double* E, double* B);
 
 /* periodic z, BCFFTZ=PERIODIC (FFTPoissonSolver.cpp:60, :130-155, :661-662) */
 void sco_igf_periodic_z(const int* nr, const double* hr, double* G2);

@@ -152,3 +152,26 @@ def write_solenoid_map(path, accuracy=30, length=0.3, npts=241, b0=1.0, edge=0.0
         for zi, bi in zip(z, bz):
             f.write(f"{zi:.17g} {bi:.17g}\n")
     return z, bz
+
+
+def write_rfcavity_map(path, accuracy=40, freq_mhz=1300.0, cells=2, npts=301, width=0.01, jitter=0.0, seed=5):
+    """A seeded synthetic on-axis E_z profile of a standing-wave cavity in
+    ASTRA 1D dynamic format ("AstraDynamic <accuracy>", the frequency in MHz,
+    then "z Ez" lines): `cells` pi-mode cells of length c / (2 f),
+    E_z = sin(pi z / cell) inside, with tanh fringes of the given width at
+    both ends.  Stands in for the reference examples' cavity maps, which are
+    not shipped here.  Returns z, Ez."""
+    cell = 299792458.0 / (2.0 * freq_mhz * 1e6)
+    length = cells * cell
+    z = np.linspace(0.0, length, npts)
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        dz = length / (npts - 1)
+        z[1:-1] += rng.uniform(-jitter, jitter, npts - 2) * dz
+    env = 0.5 * (np.tanh(z / width) - np.tanh((z - length) / width))
+    ez = np.sin(np.pi * z / cell) * env
+    with open(path, "w") as f:
+        f.write(f"AstraDynamic {accuracy}\n{freq_mhz:.17g}\n")
+        for zi, ei in zip(z, ez):
+            f.write(f"{zi:.17g} {ei:.17g}\n")
+    return z, ez

@@ -747,10 +747,10 @@ static int upload_elements(scgpu_ctx* c) {
         return SCGPU_OK;
     }
     if (!c->d_elements) {
-        int rc = dalloc(c, &c->d_elements, kMaxElements * sizeof(SolElem));
+        int rc = dalloc(c, &c->d_elements, kMaxElements * sizeof(MapElem));
         if (rc) return rc;
     }
-    CK(cudaMemcpyAsync(c->d_elements, c->elements.data(), c->elements.size() * sizeof(SolElem), cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(c->d_elements, c->elements.data(), c->elements.size() * sizeof(MapElem), cudaMemcpyHostToDevice,
                        c->stream));
     CK(cudaStreamSynchronize(c->stream));
     b.bc.sol = c->d_elements;
@@ -762,7 +762,7 @@ int scgpu_add_solenoid(scgpu_ctx* c, const char* fieldmap, double elemedge, doub
     if (!c || !fieldmap) return fail(c, SCGPU_ERR_ARG, "null argument");
     if (!std::isfinite(elemedge) || !std::isfinite(ks)) return fail(c, SCGPU_ERR_ARG, "ELEMEDGE and KS must be finite");
     if ((int)c->elements.size() >= kMaxElements) return fail(c, SCGPU_ERR_UNSUPPORTED, "at most 8 elements");
-    SolElem e{};
+    MapElem e{};
     int ncoef = 0;
     int rc = scgpu_fieldmap_astra1d(fieldmap, e.coefs, kMaxSolCoefs, &ncoef, &e.zbegin, &e.range, &e.period);
     if (rc) return fail(c, rc, std::string("cannot read the field map ") + fieldmap);
@@ -770,6 +770,43 @@ int scgpu_add_solenoid(scgpu_ctx* c, const char* fieldmap, double elemedge, doub
     e.accuracy = (ncoef + 1) / 2;
     e.edge = elemedge;
     e.scale = ks;
+    e.kind = kElemSolenoid;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    c->elements.push_back(e);
+    return upload_elements(c);
+}
+
+// RFCAVITY with an ASTRA dynamic map (OpalCavity.cpp:150-195, RFCavity.cpp:
+// 232-310).  The element's angular frequency is 1e6 * two_pi * FREQ
+// (OpalCavity.cpp:159); when it differs from the map's by more than 1 % the
+// map's is taken, as RFCavity::initialise does (:294-305).  The off-axis
+// expansion uses the map's frequency (Astra1DDynamic.cpp:80-82).
+int scgpu_add_rfcavity(scgpu_ctx* c, const char* fieldmap, double elemedge, double volt_mv_per_m, double freq_mhz,
+                       double lag_rad) {
+    if (!c || !fieldmap) return fail(c, SCGPU_ERR_ARG, "null argument");
+    if (!std::isfinite(elemedge) || !std::isfinite(volt_mv_per_m) || !std::isfinite(lag_rad) || !(freq_mhz > 0.0) ||
+        !std::isfinite(freq_mhz))
+        return fail(c, SCGPU_ERR_ARG, "ELEMEDGE, VOLT and LAG must be finite and FREQ positive");
+    if ((int)c->elements.size() >= kMaxElements) return fail(c, SCGPU_ERR_UNSUPPORTED, "at most 8 elements");
+    MapElem e{};
+    int ncoef = 0;
+    double fmap = 0.0;
+    int rc = scgpu_fieldmap_astra1d_dynamic(fieldmap, e.coefs, kMaxSolCoefs, &ncoef, &e.zbegin, &e.range, &e.period,
+                                            &fmap);
+    if (rc) return fail(c, rc, std::string("cannot read the field map ") + fieldmap);
+    e.range = e.range - e.zbegin;  // zend - zbegin
+    e.accuracy = (ncoef + 1) / 2;
+    e.edge = elemedge;
+    e.scale = volt_mv_per_m;
+    e.kind = kElemRfCavity;
+    const double two_pi = 2 * kPi;
+    const double omega_map = fmap * (two_pi * 1e6);
+    double omega = 1e6 * two_pi * freq_mhz;
+    if (std::fabs((omega - omega_map) / omega) > 0.01) omega = omega_map;
+    e.omega = omega;
+    e.phase = lag_rad;
+    e.xlrep = omega_map / kC;
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     c->elements.push_back(e);

@@ -85,6 +85,7 @@ struct StepState {
     double qdt;    // Q * dt (the scattered charge)
     Trafo upd;     // reference-particle update of this step
     Trafo ref_to_lab_step;  // ref -> lab at the start of the step (the external fields' frame)
+    double t_step;          // t at the start of the step (the particles' field time is t_step + dT / 2)
     // energy bins / image charge
     double zshift;      // z shift of the image's Green's function (PartBunch.cpp:249)
     long long bin_count;  // particles in the bin (per-bin copies)
@@ -97,19 +98,27 @@ struct StepState {
     unsigned long long xlimbs[28 * 4];
 };
 
-// A SOLENOID element with a 1D magnetostatic field map in ASTRA format
-// (Solenoid.cpp:163-215; Astra1DMagnetoStatic.cpp:162-196) on a straight
-// beamline along z: element frame = lab frame shifted by ELEMEDGE.
+// A beamline element with a 1D field map in ASTRA format on a straight
+// beamline along z (element frame = lab frame shifted by ELEMEDGE):
+//  * SOLENOID with a magnetostatic map (Solenoid.cpp:163-215;
+//    Astra1DMagnetoStatic.cpp:162-196), scaled by KS [T];
+//  * RFCAVITY with a dynamic (standing-wave) map (RFCavity.cpp:232-270;
+//    Astra1DDynamic.cpp:162-229), scaled by VOLT [MV/m], oscillating as
+//    cos(omega t + LAG) (E) and sin(omega t + LAG) (B).
 constexpr int kMaxSolCoefs = 255;  // 2 accuracy - 1, accuracy <= 128
 constexpr int kMaxElements = 8;
-struct SolElem {
+enum : int { kElemSolenoid = 0, kElemRfCavity = 1 };
+struct MapElem {
     double edge;    // ELEMEDGE: the element origin on the lab z axis [m]
-    double scale;   // KS [T] (the map is normalised to 1)
+    double scale;   // KS [T] or VOLT [MV/m] (the map is normalised to 1 T, or to 1 MV/m in V/m)
     double zbegin;  // startField: the map's first z (element frame)
-    double range;   // zend - zbegin: the field region (Solenoid::length_m)
+    double range;   // zend - zbegin: the field region (the element's length)
     double period;  // 2 N (zend - zbegin) / (N - 1): the Fourier period
     int accuracy;   // harmonics 0 .. accuracy - 1
-    int pad_;
+    int kind;       // kElemSolenoid or kElemRfCavity
+    double omega;   // RF: angular frequency [rad/s]
+    double phase;   // RF: LAG [rad]
+    double xlrep;   // RF: the map's angular frequency / c [1/m]
     double coefs[kMaxSolCoefs];
 };
 
@@ -132,7 +141,7 @@ struct BunchConst {
     double ke;      // 0.5 * dT * charge * c / mass (BorisPusher.h:88)
     double ktn;     // 0.5 * dT * charge * c * c    (BorisPusher.h:99, numerator)
     // beamline elements with external fields (device table), none when nsol == 0
-    const SolElem* sol;
+    const MapElem* sol;
     int nsol;
     int pad2_;
 };
@@ -290,17 +299,13 @@ SC_HD void trafo_rotate_from(const Trafo& t, const double* r, double* out) {
 }
 
 // ---------------------------------------------------------------- external fields
-// Astra1DMagnetoStatic::getFieldstrength (Astra1DMagnetoStatic.cpp:162-196):
-// the Fourier series of the on-axis field and its first three derivatives,
-// expanded off axis, for R in the element frame; Solenoid::apply
-// (Solenoid.cpp:167-179): only inside [zbegin, zbegin + range), scaled by KS.
-SC_HD void solenoid_field(const SolElem& e, const double* R, double* B) {
-    const double tz = R[2] - e.zbegin;
-    if (!(tz >= 0.0 && tz < e.range)) return;
-    const double RR2 = R[0] * R[0] + R[1] * R[1];
+// The Fourier series of a map's on-axis field and its first three z
+// derivatives at tz = z - zbegin (the loops of Astra1DMagnetoStatic.cpp:
+// 170-189 and Astra1DDynamic.cpp:199-216, one expression order).
+SC_HD void map_series(const MapElem& e, double tz, double& ez, double& ezp, double& ezpp, double& ezppp) {
     const double two_pi = 2 * kPi;
     const double kz = two_pi * tz / e.period + kPi;
-    double ez = e.coefs[0], ezp = 0.0, ezpp = 0.0, ezppp = 0.0;
+    ez = e.coefs[0], ezp = 0.0, ezpp = 0.0, ezppp = 0.0;
     int n = 1;
     for (int l = 1; l < e.accuracy; l++, n += 2) {
         const double base = two_pi / e.period * l;
@@ -314,6 +319,17 @@ SC_HD void solenoid_field(const SolElem& e, const double* R, double* B) {
         f *= base;
         ezppp += f * (e.coefs[n] * s + e.coefs[n + 1] * c);
     }
+}
+
+// Astra1DMagnetoStatic::getFieldstrength expanded off axis, for R in the
+// element frame; Solenoid::apply (Solenoid.cpp:167-179): only inside
+// [zbegin, zbegin + range), scaled by KS.
+SC_HD void solenoid_field(const MapElem& e, const double* R, double* B) {
+    const double tz = R[2] - e.zbegin;
+    if (!(tz >= 0.0 && tz < e.range)) return;
+    const double RR2 = R[0] * R[0] + R[1] * R[1];
+    double ez, ezp, ezpp, ezppp;
+    map_series(e, tz, ez, ezp, ezpp, ezppp);
     const double BfieldR = -ezp / 2. + ezppp / 16. * RR2;
     const double tB[3] = {BfieldR * R[0], BfieldR * R[1], ez - ezpp * RR2 / 4.};
     B[0] = e.scale * tB[0];
@@ -321,17 +337,53 @@ SC_HD void solenoid_field(const SolElem& e, const double* R, double* B) {
     B[2] = e.scale * tB[2];
 }
 
+// Astra1DDynamic::getFieldstrength (:192-229): the standing-wave field of the
+// on-axis E_z expanded off axis with the wave number xlrep, and
+// RFCavity::apply (:232-249): inside [zbegin, zbegin + range) at time t,
+// E += VOLT cos(omega t + LAG) E_map, B -= VOLT sin(omega t + LAG) B_map.
+SC_HD void rfcavity_field(const MapElem& e, const double* R, double t, double* E, double* B) {
+    const double tz = R[2] - e.zbegin;
+    if (!(tz >= 0.0 && tz < e.range)) return;
+    const double RR2 = R[0] * R[0] + R[1] * R[1];
+    double ez, ezp, ezpp, ezppp;
+    map_series(e, tz, ez, ezp, ezpp, ezppp);
+    const double f = -(ezpp + ez * e.xlrep * e.xlrep) / 16.;
+    const double fp = -(ezppp + ezp * e.xlrep * e.xlrep) / 16.;
+    const double EfieldR = -(ezp / 2. + fp * RR2);
+    const double BfieldT = (ez / 2. + f * RR2) * e.xlrep / kC;
+    const double tE[3] = {EfieldR * R[0], EfieldR * R[1], ez + 4. * f * RR2};
+    const double tB[3] = {-BfieldT * R[1], BfieldT * R[0], 0.0};
+    const double arg = e.omega * t + e.phase;
+    const double ce = e.scale * cos(arg), sb = e.scale * sin(arg);
+    E[0] += ce * tE[0];
+    E[1] += ce * tE[1];
+    E[2] += ce * tE[2];
+    B[0] -= sb * tB[0];
+    B[1] -= sb * tB[1];
+    B[2] -= sb * tB[2];
+}
+
 // computeExternalFields (ParallelTTracker.cpp:614-643) for the elements of
-// the table: R in the reference frame -> lab (ref_to_lab) -> element frame
-// (minus ELEMEDGE along z); each element's B rotated back and added to Bf.
-SC_HD void add_external_B(const SolElem* el, int n, const Trafo& ref_to_lab, const double* R, double* Bf) {
+// the table at time t: R in the reference frame -> lab (ref_to_lab) ->
+// element frame (minus ELEMEDGE along z); each element's E and B rotated
+// back and added to Ef, Bf.
+SC_HD void add_external_fields(const MapElem* el, int n, const Trafo& ref_to_lab, const double* R, double t, double* Ef,
+                               double* Bf) {
     for (int k = 0; k < n; ++k) {
-        double lab[3], loc[3], Bl[3] = {0.0, 0.0, 0.0}, Br[3];
+        double lab[3], loc[3], El[3] = {0.0, 0.0, 0.0}, Bl[3] = {0.0, 0.0, 0.0}, Er[3], Br[3];
         trafo_transform_to(ref_to_lab, R, lab);
         loc[0] = lab[0] - 0.0;
         loc[1] = lab[1] - 0.0;
         loc[2] = lab[2] - el[k].edge;
-        solenoid_field(el[k], loc, Bl);
+        if (el[k].kind == kElemRfCavity) {
+            rfcavity_field(el[k], loc, t, El, Bl);
+            trafo_rotate_from(ref_to_lab, El, Er);
+            Ef[0] += Er[0];
+            Ef[1] += Er[1];
+            Ef[2] += Er[2];
+        } else {
+            solenoid_field(el[k], loc, Bl);
+        }
         trafo_rotate_from(ref_to_lab, Bl, Br);
         Bf[0] += Br[0];
         Bf[1] += Br[1];
@@ -569,15 +621,16 @@ SC_HD_COLD bool derive_beam_frame(StepState& s, const BunchConst& bc) {
 }
 
 // updateReferenceParticle + updateRefToLabCSTrafo (ParallelTTracker.cpp:1123-1212)
-// for a beamline with no elements except an optional uniform B_z.
+// with the elements of the table and an optional uniform B_z.
 SC_HD bool advance_reference(StepState& s, const BunchConst& bc) {
     s.ref_to_lab_step = s.ref_to_lab;  // the particles' external fields use the frame of the step's start
+    s.t_step = s.t;
     s.t += bc.dT;
     const double dt = s.t < bc.dT ? s.t : bc.dT;
     const double scaleFactor = kC * dt;
     double* rr = s.ref_R;
     double* rp = s.ref_P;
-    double zero[3] = {0.0, 0.0, 0.0}, bref[3] = {0.0, 0.0, 0.0};
+    double eref[3] = {0.0, 0.0, 0.0}, bref[3] = {0.0, 0.0, 0.0};
     for (int pass = 0; pass < 2; ++pass) {
         rr[0] /= scaleFactor;
         rr[1] /= scaleFactor;
@@ -591,10 +644,11 @@ SC_HD bool advance_reference(StepState& s, const BunchConst& bc) {
         rr[2] *= scaleFactor;
         if (pass == 0) {
             // updateReferenceParticle (ParallelTTracker.cpp:1134-1155): the
-            // elements' fields at the reference particle, then the kick
-            add_external_B(bc.sol, bc.nsol, s.ref_to_lab, rr, bref);
+            // elements' fields at the reference particle at t - dt / 2, then
+            // the kick
+            add_external_fields(bc.sol, bc.nsol, s.ref_to_lab, rr, s.t - 0.5 * dt, eref, bref);
             if (bc.bz_ext != 0.0) bref[2] += bc.bz_ext;
-            kick_one(rp, zero, bref, dt, bc.mass, bc.charge);
+            kick_one(rp, eref, bref, dt, bc.mass, bc.charge);
         }
     }
     s.path_length += sqrt(dot3(rr, rr));

@@ -46,8 +46,8 @@ struct scgpu_ctx {
     cudaEvent_t ev_bin[sc::kMaxBins] = {};
     cudaEvent_t ev_used[sc::kMaxBins] = {};
     // beamline elements (scgpu_add_solenoid): host copy and device table
-    std::vector<sc::SolElem> elements;
-    sc::SolElem* d_elements = nullptr;
+    std::vector<sc::MapElem> elements;
+    sc::MapElem* d_elements = nullptr;
     // sharded bunch (scgpu_set_exchange): this context holds one rank's shard
     scgpu_exchange_fn xfn = nullptr;
     void* xuser = nullptr;

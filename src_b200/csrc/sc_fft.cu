@@ -82,9 +82,12 @@ __device__ __forceinline__ void cp_elem(V* smem, const V* gmem) {
 }
 
 // ---------------------------------------------------------------- plans
-// Radix sequence of a length L = 2^p 3^a 5^b: radix-8 stages for the power of
-// two (a remainder of 2 with an 8 becomes 4 x 4, so no radix-2 stage runs
-// beside radix 8), then 3s and 5s.  nst = -1 when L has another factor.
+// Radix sequence of a length L = 2^p 3^a 5^b: radix-16 stages for the power
+// of two, the remainder p mod 4 as one radix-8 (3), radix-4 (2) or radix-8
+// and radix-4 stage in place of one 16 (1; radix 2 alone for L = 2), then 3s
+// and 5s.  Fewer stages are fewer passes through shared memory: 128 = 16 x 8,
+// 256 = 16 x 16, 64 = 16 x 4, 32 = 8 x 4.  nst = -1 when L has another
+// factor.
 struct RadixPlan {
     int nst;
     int r[12];
@@ -100,18 +103,23 @@ __host__ __device__ constexpr RadixPlan radix_plan(int L) {
         m /= 2;
         ++twos;
     }
-    int e8 = twos / 3;
-    const int rem = twos % 3;
-    if (rem == 1 && e8 > 0) {
-        e8 -= 1;
-        p.r[p.nst++] = 4;
+    int e16 = twos / 4;
+    const int rem = twos % 4;
+    if (rem == 1 && e16 > 0) {
+        e16 -= 1;
+        p.r[p.nst++] = 8;
         p.r[p.nst++] = 4;
     } else if (rem == 1) {
         p.r[p.nst++] = 2;
     } else if (rem == 2) {
         p.r[p.nst++] = 4;
+    } else if (rem == 3) {
+        p.r[p.nst++] = 8;
     }
-    for (int i = 0; i < e8; ++i) p.r[p.nst++] = 8;
+    // the 16s first: the first stage carries no twiddles and, pruned, reads half
+    for (int i = p.nst - 1; i >= 0; --i) p.r[i + e16] = p.r[i];
+    for (int i = 0; i < e16; ++i) p.r[i] = 16;
+    p.nst += e16;
     while (m % 3 == 0 && p.nst < 12) {
         p.r[p.nst++] = 3;
         m /= 3;
@@ -147,6 +155,25 @@ __host__ __device__ constexpr int threads_for(int LT) {
 }
 
 // ---------------------------------------------------------------- butterflies
+// z times W16^m = exp(-+2 pi i m / 16) (minus sign forward), m in {0, 1, 2,
+// 3, 4, 6, 9} (the products n2 k1 of the radix-16 stage; m is a constant
+// after unrolling).
+template <typename T, bool INV>
+__device__ __forceinline__ Cx<T> w16(Cx<T> z, int m) {
+    using C = Cx<T>;
+    const T c = (T)0.92387953251128675613, s = (T)0.38268343236508977173, h = (T)0.70710678118654752440;
+    const T sg = INV ? (T)1 : (T)-1;  // sign of the imaginary part of W16^1
+    switch (m) {
+        case 0: return z;
+        case 1: return C{c * z.x - sg * s * z.y, c * z.y + sg * s * z.x};
+        case 2: return C{h * (z.x - sg * z.y), h * (z.y + sg * z.x)};
+        case 3: return C{s * z.x - sg * c * z.y, s * z.y + sg * c * z.x};
+        case 4: return C{-sg * z.y, sg * z.x};
+        case 6: return C{-h * (z.x + sg * z.y), -h * (z.y - sg * z.x)};
+        default: return C{-c * z.x + sg * s * z.y, -c * z.y - sg * s * z.x};  // 9
+    }
+}
+
 // R-point DFT in registers; forward uses exp(-2 pi i / R).
 template <typename T, int R, bool INV>
 __device__ __forceinline__ void dft(Cx<T>* v) {
@@ -201,6 +228,24 @@ __device__ __forceinline__ void dft(Cx<T>* v) {
             v[2 * m] = a[m];
             v[2 * m + 1] = b[m];
         }
+    } else if constexpr (R == 16) {
+        // 4 x 4: a[n2][k1] = DFT4 over n1 of x[n2 + 4 n1], times W16^(n2 k1);
+        // X[k1 + 4 k2] = DFT4 over n2
+        C a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+            C t[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
+            dft<T, 4, INV>(t);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = w16<T, INV>(t[k1], n2 * k1);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+            dft<T, 4, INV>(t);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
+        }
     } else if constexpr (R == 5) {
         const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
         const T s1 = INV ? (T)0.95105651629515357212 : (T)-0.95105651629515357212;
@@ -244,8 +289,12 @@ __device__ __forceinline__ void dft_half(Cx<T>* v) {
             v[1] = C{a.x - b.y, a.y + b.x};
             v[3] = C{a.x + b.y, a.y - b.x};
         }
+    } else if constexpr (R == 16) {
+#pragma unroll
+        for (int k = 8; k < 16; ++k) v[k] = C{(T)0, (T)0};
+        dft<T, 16, INV>(v);
     } else {
-        static_assert(R == 8, "half-input DFT for radix 2, 4, 8");
+        static_assert(R == 8, "half-input DFT for radix 2, 4, 8, 16");
         const T h = (T)0.70710678118654752440;
         C a[4], b[4];
 #pragma unroll
@@ -274,7 +323,10 @@ __device__ __forceinline__ void dft_half(Cx<T>* v) {
 // and writes element (j / Ns) Ns R + k + r Ns (positions through sk()).
 // NZ < R: inputs r >= NZ are known zeros (NZ = R/2 only); NO < R: only
 // outputs r < NO are needed; FIRST: Ns = 1, all twiddles are 1.
-template <typename T, int R, bool INV, int NZ = R, int NO = R, bool FIRST = false>
+// STW: tw is the stage's own table, W^(r k step) at (r - 1) Ns + k, so that
+// the lanes of a warp (consecutive k) read consecutive entries; otherwise tw
+// is the whole table W^e, e in [0, L).
+template <typename T, int R, bool INV, int NZ = R, int NO = R, bool FIRST = false, bool STW = false>
 __device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst, int j, int nb, int Ns,
                                           int step, const Cx<T>* __restrict__ tw) {
     using C = Cx<T>;
@@ -286,7 +338,7 @@ __device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* 
     if constexpr (!FIRST) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-            C t = tw[r * k * step];
+            C t = STW ? tw[(r - 1) * Ns + k] : tw[r * k * step];
             if (INV) t.y = -t.y;
             v[r] = cmul(v[r], t);
         }
@@ -313,7 +365,8 @@ __host__ __device__ constexpr int col_stride(int L) { return L + (L >> 3) + 1; }
 //               writes half.
 constexpr int kPruneNone = 0, kPruneIn = 1, kPruneOut = 2;
 
-// compile-time stage: length L, Ns, NC columns, NT threads
+// compile-time stage: length L, Ns, NC columns, NT threads; tw is the
+// stage's own twiddle table (stage_twiddles)
 template <typename T, int R, bool INV, int L, int NS, int NC, int NT, int NZ, int NO>
 __device__ __forceinline__ void stage_c(const Cx<T>* in, Cx<T>* out, const Cx<T>* tw) {
     constexpr int NB = L / R;
@@ -325,11 +378,13 @@ __device__ __forceinline__ void stage_c(const Cx<T>* in, Cx<T>* out, const Cx<T>
         if ((NC * NB) % NT != 0 && w >= NC * NB) break;
         const int col = w / NB;
         const int j = w - col * NB;
-        butterfly<T, R, INV, NZ, NO, NS == 1>(in + col * CS, out + col * CS, j, NB, NS, STEP, tw);
+        butterfly<T, R, INV, NZ, NO, NS == 1, true>(in + col * CS, out + col * CS, j, NB, NS, STEP, tw);
     }
 }
 
-template <typename T, bool INV, int L, int S, int NS, int NC, int NT, int PR>
+// OFF: offset of stage S's table in the per-stage twiddle layout (the first
+// stage has none; stage s > 0 holds (R_s - 1) Ns_s entries).
+template <typename T, bool INV, int L, int S, int NS, int NC, int NT, int PR, int OFF = 0>
 __device__ __forceinline__ Cx<T>* stages_c(Cx<T>* a, Cx<T>* b, const Cx<T>* tw) {
     constexpr RadixPlan P = radix_plan(L);
     if constexpr (S == P.nst) {
@@ -337,11 +392,11 @@ __device__ __forceinline__ Cx<T>* stages_c(Cx<T>* a, Cx<T>* b, const Cx<T>* tw) 
     } else {
         constexpr int R = P.r[S];
         constexpr bool even = R % 2 == 0;
-        constexpr int NZ = (PR == kPruneIn && S == 0 && even && R <= 8) ? R / 2 : R;
+        constexpr int NZ = (PR == kPruneIn && S == 0 && even && R <= 16) ? R / 2 : R;
         constexpr int NO = (PR == kPruneOut && S == P.nst - 1 && even) ? R / 2 : R;
-        stage_c<T, R, INV, L, NS, NC, NT, NZ, NO>(a, b, tw);
+        stage_c<T, R, INV, L, NS, NC, NT, NZ, NO>(a, b, tw + OFF);
         __syncthreads();
-        return stages_c<T, INV, L, S + 1, NS * R, NC, NT, PR>(b, a, tw);
+        return stages_c<T, INV, L, S + 1, NS * R, NC, NT, PR, OFF + (S > 0 ? (R - 1) * NS : 0)>(b, a, tw);
     }
 }
 
@@ -373,7 +428,9 @@ __device__ __forceinline__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, const FftPla
         Cx<T>* b = tmp;
         for (int s = 0; s < pl.nst; ++s) {
             const int R = pl.r[s];
-            if (R == 8)
+            if (R == 16)
+                stage_r<T, 16, INV>(a, b, pl.L, Ns, NC, tw);
+            else if (R == 8)
                 stage_r<T, 8, INV>(a, b, pl.L, Ns, NC, tw);
             else if (R == 4)
                 stage_r<T, 4, INV>(a, b, pl.L, Ns, NC, tw);
@@ -393,9 +450,34 @@ __device__ __forceinline__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, const FftPla
     }
 }
 
-template <typename V, int NT>
+// The twiddles of a block's transforms into shared memory.  A template
+// length stages the per-stage layout the compile-time stages read (stage s >
+// 0: W^(r k step_s) at offset_s + (r - 1) Ns_s + k, L - R_0 entries in all,
+// taken from the full table src[e] = W^e); a run-time length stages the full
+// table.
+template <typename V, int LT, int NT>
 __device__ __forceinline__ void stage_twiddles(V* dst, const V* __restrict__ src, int L) {
-    for (int e = threadIdx.x; e < L; e += NT) cp_elem(dst + e, src + e);
+    if constexpr (LT > 0) {
+        constexpr RadixPlan P = radix_plan(LT);
+        for (int e = threadIdx.x; e < LT - P.r[0]; e += NT) {
+            int off = 0, ns = P.r[0], q = e;
+#pragma unroll
+            for (int st = 1; st < P.nst; ++st) {
+                const int size = (P.r[st] - 1) * ns;
+                if (q < size) {
+                    const int r = q / ns + 1, k = q - (r - 1) * ns;
+                    const int step = LT / (ns * P.r[st]);
+                    cp_elem(dst + off + q, src + r * k * step);
+                    break;
+                }
+                q -= size;
+                off += size;
+                ns *= P.r[st];
+            }
+        }
+    } else {
+        for (int e = threadIdx.x; e < L; e += NT) cp_elem(dst + e, src + e);
+    }
 }
 
 // elements of one tile: twiddles (L), buf and tmp (NC col_stride(L) + 2 NC each)
@@ -420,7 +502,7 @@ __device__ __forceinline__ void fft_z_r2c_body(const T* __restrict__ rho, Cx<T>*
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L2;
     C* tmp = buf + NC * CS + RC;
-    stage_twiddles<C, NT>(tw, twz, L2);
+    stage_twiddles<C, LT, NT>(tw, twz, L2);
     const int y = by;
     const int x0 = bx * RC;
     for (int e = threadIdx.x; e < RC * (LT > 0 ? n2 : L2); e += NT) {  // the zero half is not staged when pruned
@@ -469,7 +551,7 @@ __device__ __forceinline__ void fft_y_body(Cx<T>* __restrict__ spec, int n0, int
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L1;
     C* tmp = buf + NC * CS + 2 * NC;
-    stage_twiddles<C, NT>(tw, twy, L1);
+    stage_twiddles<C, LT, NT>(tw, twy, L1);
     const int kz = by;
     const int x0 = bx * NC;
     C* plane = spec + (size_t)kz * L1 * L0;
@@ -520,8 +602,8 @@ __device__ __forceinline__ void fft_x_conv_body(const Cx<TI>* in, Cx<TO>* out, c
     CI* tw_i = reinterpret_cast<CI*>(tw_o + L0);
     CO* bufo = reinterpret_cast<CO*>(tw_i + L0);
     CO* tmpo = bufo + NC * CS;
-    stage_twiddles<CO, NT>(tw_o, two, L0);
-    stage_twiddles<CI, NT>(tw_i, twi, L0);
+    stage_twiddles<CO, LT, NT>(tw_o, two, L0);
+    stage_twiddles<CI, LT, NT>(tw_i, twi, L0);
     CI* bufi = reinterpret_cast<CI*>(bufo);
     CI* tmpi = reinterpret_cast<CI*>(tmpo);
     const int r0 = bx * NC;
@@ -590,7 +672,7 @@ __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, d
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L2;
     C* tmp = buf + NC * CS + RC;
-    stage_twiddles<C, NT>(tw, twz, L2);
+    stage_twiddles<C, LT, NT>(tw, twz, L2);
     const int y = by;
     const int x0 = bx * RC;
     // the half spectra of the 2 NC columns in tmp: [xi][k], k <= K = L2 / 2
@@ -664,7 +746,7 @@ __device__ __forceinline__ void dct_lines_body(const double* __restrict__ in, TO
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double2* buf = tw + L;
     double2* tmp = buf + NC * CS + RC;
-    stage_twiddles<double2, NT>(tw, twd, L);
+    stage_twiddles<double2, LT, NT>(tw, twd, L);
     const int b0 = bx * RC;
     const long long obase = (long long)by * so;
     for (int e = threadIdx.x; e < RC * len; e += NT) {
@@ -716,7 +798,7 @@ __device__ __forceinline__ void rfft_lines_neg_body(const double* __restrict__ i
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double2* buf = tw + L;
     double2* tmp = buf + NC * CS + RC;
-    stage_twiddles<double2, NT>(tw, twd, L);
+    stage_twiddles<double2, LT, NT>(tw, twd, L);
     const int b0 = bx * RC;
     for (int e = threadIdx.x; e < RC * L; e += NT) {
         const int li = e % RC, m = e / RC;

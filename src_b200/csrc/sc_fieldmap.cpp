@@ -1,4 +1,4 @@
-// sc_fieldmap.cpp -- 1D magnetostatic field maps in ASTRA format, as OPAL's
+// sc_fieldmap.cpp -- 1D field maps in ASTRA format.  Magnetostatic maps as OPAL's
 // Astra1DMagnetoStatic reads them (src/Classic/Fields/Astra1DMagnetoStatic.cpp:
 // constructor :15-77, readMap :83-160): a header "AstraMagnetostatic
 // <accuracy> [TRUE|FALSE]" and lines "z Bz(z)" ('#' comments and blank lines
@@ -7,6 +7,12 @@
 // mirrored to an even periodic sequence of 2N points and expanded in a
 // Fourier series; the first 2 accuracy - 1 coefficients, normalised to the
 // largest |Bz| unless the header says FALSE, are what the device evaluates.
+//
+// Dynamic (RF standing-wave) maps, as Astra1DDynamic reads them
+// (src/Classic/Fields/Astra1DDynamic.cpp: constructor :19-90, readMap
+// :96-185): a header "AstraDynamic <accuracy> [TRUE|FALSE]", a line with the
+// frequency in MHz, then lines "z Ez(z)"; the same resampling, mirroring and
+// series, normalised to the largest |Ez| and scaled by 1e6 (MV/m to V/m).
 //
 // Host C++ only (no CUDA); the evaluation is in sc_common.cuh.
 #include <cctype>
@@ -93,12 +99,12 @@ struct NaturalSpline {
     }
 };
 
-}  // namespace
-
-extern "C" {
-
-int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin, double* zend,
-                           double* period) {
+// Reads a magnetostatic ("AstraM...") or, with dynamic, a dynamic
+// ("AstraD...") map; the dynamic header line is followed by the frequency in
+// MHz (Astra1DDynamic.cpp:19-90) and its coefficients carry the factor 1e6
+// of the MV/m -> V/m conversion (:150-153).
+int read_astra1d(const char* path, bool dynamic, double* coefs, int max_coefs, int* ncoefs, double* zbegin,
+                 double* zend, double* period, double* freq_mhz) {
     if (!path || !coefs || !ncoefs || !zbegin || !zend || !period) return SCGPU_ERR_ARG;
     std::ifstream in(path);
     if (!in) return SCGPU_ERR_ARG;
@@ -107,12 +113,21 @@ int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* 
     std::istringstream hs(line);
     std::string name, flag;
     int accuracy = 0;
-    if (!(hs >> name >> accuracy) || name.compare(0, 6, "AstraM") != 0 || accuracy < 1) return SCGPU_ERR_ARG;
+    if (!(hs >> name >> accuracy) || name.compare(0, 6, dynamic ? "AstraD" : "AstraM") != 0 || accuracy < 1)
+        return SCGPU_ERR_ARG;
     bool normalize = true;
     if (hs >> flag) {
         for (char& ch : flag) ch = (char)std::toupper((unsigned char)ch);
         if (flag != "TRUE" && flag != "FALSE") return SCGPU_ERR_ARG;
         normalize = flag == "TRUE";
+    }
+    if (dynamic) {
+        if (!content_line(in, line)) return SCGPU_ERR_ARG;
+        std::istringstream fs(line);
+        double f = 0.0;
+        std::string rest;
+        if (!(fs >> f) || (fs >> rest) || !(f > 0.0)) return SCGPU_ERR_ARG;
+        if (freq_mhz) *freq_mhz = f;
     }
     std::vector<double> zs, bz;
     double z = 0.0, b = 0.0, last = 0.0, zlast = 0.0;
@@ -149,11 +164,12 @@ int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* 
             re += (long double)seq[j] * cosl(a);
             im -= (long double)seq[j] * sinl(a);
         }
+        const double u = dynamic ? 1.0e6 : 1.0;
         if (k == 0) {
-            coefs[0] = (double)re / (bmax * 2. * N);
+            coefs[0] = u * (double)re / (bmax * 2. * N);
         } else {
-            coefs[2 * k - 1] = (double)re / (bmax * N);
-            coefs[2 * k] = (double)im / (bmax * N);
+            coefs[2 * k - 1] = u * (double)re / (bmax * N);
+            coefs[2 * k] = u * (double)im / (bmax * N);
         }
     }
     *ncoefs = 2 * accuracy - 1;
@@ -161,6 +177,21 @@ int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* 
     *zend = ze;
     *period = 2.0 * N * (ze - zb) / (N - 1);
     return SCGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin, double* zend,
+                           double* period) {
+    return read_astra1d(path, false, coefs, max_coefs, ncoefs, zbegin, zend, period, nullptr);
+}
+
+int scgpu_fieldmap_astra1d_dynamic(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin,
+                                   double* zend, double* period, double* frequency_mhz) {
+    if (!frequency_mhz) return SCGPU_ERR_ARG;
+    return read_astra1d(path, true, coefs, max_coefs, ncoefs, zbegin, zend, period, frequency_mhz);
 }
 
 }  // extern "C"

@@ -1222,7 +1222,7 @@ __device__ __forceinline__ bool mixed_particle(const BunchConst& bc, const MeshC
     matvec_fma(b2r.M, Eb, Ef);
     matvec_fma(b2r.M, Bb, Bf);
     if (bc.bz_ext != 0.0) Bf[2] += bc.bz_ext;
-    if constexpr (EXT) add_external_B(bc.sol, bc.nsol, st->ref_to_lab_step, Rr, Bf);
+    if constexpr (EXT) add_external_fields(bc.sol, bc.nsol, st->ref_to_lab_step, Rr, st->t_step + 0.5 * bc.dT, Ef, Bf);
     // Boris kick (BorisPusher.h:56-113)
     const double ke = bc.ke;
 #pragma unroll
@@ -1316,7 +1316,8 @@ __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __rest
             trafo_rotate_to(*b2r, Bb, Bf);
             if (bc.bz_ext != 0.0) Bf[2] += bc.bz_ext;
             // the beamline elements' fields at R, in the frame of the step's start
-            if constexpr (EXT) add_external_B(bc.sol, bc.nsol, st->ref_to_lab_step, R, Bf);
+            if constexpr (EXT)
+                add_external_fields(bc.sol, bc.nsol, st->ref_to_lab_step, R, st->t_step + 0.5 * bc.dT, Ef, Bf);
             kick_r(P, Ef, Bf, bc.ke, bc.ktn, bc.mass);
             push_r(R, P, bc.s_cdt, bc.rs_cdt);
             const Trafo* upd = fresh(&upd_s);

@@ -115,6 +115,8 @@ def lib():
         L.scgpu_add_solenoid.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double]
         L.scgpu_clear_elements.argtypes = [C.c_void_p]
         L.scgpu_fieldmap_astra1d.argtypes = [C.c_char_p, _dp, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp]
+        L.scgpu_add_rfcavity.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.scgpu_fieldmap_astra1d_dynamic.argtypes = [C.c_char_p, _dp, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
         L.scgpu_stat_row.argtypes = [C.c_void_p, _dp]
         L.scgpu_stat_column_name.argtypes = [C.c_int]
         L.scgpu_stat_column_name.restype = C.c_char_p
@@ -139,7 +141,8 @@ EXPORTED = [
     "scgpu_get_bin_gammas", "scgpu_stat_row", "scgpu_stat_column_name", "scgpu_sdds_write_header",
     "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
     "scgpu_set_periodic_z", "scgpu_set_exchange", "scgpu_add_solenoid", "scgpu_clear_elements",
-    "scgpu_fieldmap_astra1d", "scgpu_set_reorder_interval", "scgpu_launch_count",
+    "scgpu_fieldmap_astra1d", "scgpu_add_rfcavity", "scgpu_fieldmap_astra1d_dynamic", "scgpu_set_reorder_interval",
+    "scgpu_launch_count",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
@@ -207,6 +210,11 @@ class Context:
     def add_solenoid(self, fieldmap, elemedge, ks):
         """SOLENOID with an ASTRA 1D magnetostatic map at ELEMEDGE [m], KS [T]."""
         self._check(lib().scgpu_add_solenoid(self.h, os.fsencode(fieldmap), float(elemedge), float(ks)), "add_solenoid")
+
+    def add_rfcavity(self, fieldmap, elemedge, volt, freq_mhz, lag):
+        """RFCAVITY with an ASTRA dynamic map at ELEMEDGE [m]: VOLT [MV/m], FREQ [MHz], LAG [rad]."""
+        self._check(lib().scgpu_add_rfcavity(self.h, os.fsencode(fieldmap), float(elemedge), float(volt),
+                                             float(freq_mhz), float(lag)), "add_rfcavity")
 
     def clear_elements(self):
         self._check(lib().scgpu_clear_elements(self.h), "clear_elements")
@@ -581,3 +589,15 @@ def fieldmap_astra1d(path):
     if rc != 0:
         raise ScgpuError(rc, f"cannot read the field map {path}")
     return coefs[:n.value].copy(), zb.value, ze.value, per.value
+
+
+def fieldmap_astra1d_dynamic(path):
+    """Astra1DDynamic::readMap: (coefficients in V/m per MV/m, zbegin, zend, period, frequency [MHz])."""
+    coefs = np.empty(255)
+    n = C.c_int(0)
+    zb, ze, per, f = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+    rc = lib().scgpu_fieldmap_astra1d_dynamic(os.fsencode(path), _p(coefs), 255, C.byref(n), C.byref(zb), C.byref(ze),
+                                              C.byref(per), C.byref(f))
+    if rc != 0:
+        raise ScgpuError(rc, f"cannot read the field map {path}")
+    return coefs[:n.value].copy(), zb.value, ze.value, per.value, f.value
