@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -100,11 +101,63 @@ bool length_ok(int n) {
     return make_plan(2 * n).nst > 0;
 }
 
+// Particle arrays (the buffers that change size with the bunch) come from a
+// per-device stream-ordered memory pool that keeps freed memory: resizing a
+// context -- a serving loop reusing a parked context for a larger bunch --
+// then costs no device-wide synchronisation, as cudaFree would, and steps in
+// flight on other contexts keep running.
+cudaMemPool_t particle_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
+template <typename P>
+int palloc(scgpu_ctx* c, P** p, size_t bytes) {
+    cudaMemPool_t pool = particle_pool(c->device);
+    if (!pool) return dalloc(c, p, bytes);
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMallocFromPoolAsync((void**)p, bytes, pool, c->stream);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(c, SCGPU_ERR_OOM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
+    }
+    return SCGPU_OK;
+}
+
+template <typename P>
+void pfree(scgpu_ctx* c, P*& p) {
+    if (p) {
+        if (particle_pool(c->device))
+            cudaFreeAsync((void*)p, c->stream);
+        else
+            cudaFree((void*)p);
+    }
+    p = nullptr;
+}
+
 void free_particles(scgpu_ctx* c) {
     DevBunch& b = c->b;
-    dfree(b.x); dfree(b.y); dfree(b.z); dfree(b.px); dfree(b.py); dfree(b.pz); dfree(b.id);
-    dfree(b.keys); dfree(b.keys_alt); dfree(b.vals); dfree(b.vals_alt);
-    dfree(b.Ef); dfree(b.Bf);
+    pfree(c, b.x); pfree(c, b.y); pfree(c, b.z); pfree(c, b.px); pfree(c, b.py); pfree(c, b.pz); pfree(c, b.id);
+    pfree(c, b.keys); pfree(c, b.keys_alt); pfree(c, b.vals); pfree(c, b.vals_alt);
+    pfree(c, b.Ef); pfree(c, b.Bf);
     c->capacity = 0;
 }
 
@@ -257,13 +310,13 @@ int ensure_particles(scgpu_ctx* c, long long n) {
         int rc;
         const size_t d = (size_t)n * sizeof(double);
         const size_t u = (size_t)n * sizeof(uint32_t);
-        if ((rc = dalloc(c, &b.x, d)) || (rc = dalloc(c, &b.y, d)) || (rc = dalloc(c, &b.z, d)) ||
-            (rc = dalloc(c, &b.px, d)) || (rc = dalloc(c, &b.py, d)) || (rc = dalloc(c, &b.pz, d)))
+        if ((rc = palloc(c, &b.x, d)) || (rc = palloc(c, &b.y, d)) || (rc = palloc(c, &b.z, d)) ||
+            (rc = palloc(c, &b.px, d)) || (rc = palloc(c, &b.py, d)) || (rc = palloc(c, &b.pz, d)))
             return rc;
-        if ((rc = dalloc(c, &b.keys, u)) || (rc = dalloc(c, &b.keys_alt, u)) || (rc = dalloc(c, &b.vals, u)) ||
-            (rc = dalloc(c, &b.vals_alt, u)) || (rc = dalloc(c, &b.id, u)))
+        if ((rc = palloc(c, &b.keys, u)) || (rc = palloc(c, &b.keys_alt, u)) || (rc = palloc(c, &b.vals, u)) ||
+            (rc = palloc(c, &b.vals_alt, u)) || (rc = palloc(c, &b.id, u)))
             return rc;
-        if ((rc = dalloc(c, &b.Ef, 3 * d)) || (rc = dalloc(c, &b.Bf, 3 * d))) return rc;
+        if ((rc = palloc(c, &b.Ef, 3 * d)) || (rc = palloc(c, &b.Bf, 3 * d))) return rc;
         c->capacity = n;
     }
     if (n != c->n) drop_graphs(c);
