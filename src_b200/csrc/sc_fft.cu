@@ -82,12 +82,12 @@ __device__ __forceinline__ void cp_elem(V* smem, const V* gmem) {
 }
 
 // ---------------------------------------------------------------- plans
-// Radix sequence of a length L = 2^p 3^a 5^b: radix-16 stages for the power
-// of two, the remainder p mod 4 as one radix-8 (3), radix-4 (2) or radix-8
-// and radix-4 stage in place of one 16 (1; radix 2 alone for L = 2), then 3s
-// and 5s.  Fewer stages are fewer passes through shared memory: 128 = 16 x 8,
-// 256 = 16 x 16, 64 = 16 x 4, 32 = 8 x 4.  nst = -1 when L has another
-// factor.
+// Radix sequence of a length L = 2^p 3^a 5^b: radix-8 stages for the power of
+// two (a remainder of 2 with an 8 becomes 4 x 4, so no radix-2 stage runs
+// beside radix 8), then 3s and 5s.  nst = -1 when L has another factor.
+// (Radix-16 stages -- 128 = 16 x 8 -- were measured slower at 128 points:
+// their registers halve the resident blocks and half the threads idle in
+// the 16-point stage.)
 struct RadixPlan {
     int nst;
     int r[12];
@@ -103,23 +103,18 @@ __host__ __device__ constexpr RadixPlan radix_plan(int L) {
         m /= 2;
         ++twos;
     }
-    int e16 = twos / 4;
-    const int rem = twos % 4;
-    if (rem == 1 && e16 > 0) {
-        e16 -= 1;
-        p.r[p.nst++] = 8;
+    int e8 = twos / 3;
+    const int rem = twos % 3;
+    if (rem == 1 && e8 > 0) {
+        e8 -= 1;
+        p.r[p.nst++] = 4;
         p.r[p.nst++] = 4;
     } else if (rem == 1) {
         p.r[p.nst++] = 2;
     } else if (rem == 2) {
         p.r[p.nst++] = 4;
-    } else if (rem == 3) {
-        p.r[p.nst++] = 8;
     }
-    // the 16s first: the first stage carries no twiddles and, pruned, reads half
-    for (int i = p.nst - 1; i >= 0; --i) p.r[i + e16] = p.r[i];
-    for (int i = 0; i < e16; ++i) p.r[i] = 16;
-    p.nst += e16;
+    for (int i = 0; i < e8; ++i) p.r[p.nst++] = 8;
     while (m % 3 == 0 && p.nst < 12) {
         p.r[p.nst++] = 3;
         m /= 3;
@@ -155,25 +150,6 @@ __host__ __device__ constexpr int threads_for(int LT) {
 }
 
 // ---------------------------------------------------------------- butterflies
-// z times W16^m = exp(-+2 pi i m / 16) (minus sign forward), m in {0, 1, 2,
-// 3, 4, 6, 9} (the products n2 k1 of the radix-16 stage; m is a constant
-// after unrolling).
-template <typename T, bool INV>
-__device__ __forceinline__ Cx<T> w16(Cx<T> z, int m) {
-    using C = Cx<T>;
-    const T c = (T)0.92387953251128675613, s = (T)0.38268343236508977173, h = (T)0.70710678118654752440;
-    const T sg = INV ? (T)1 : (T)-1;  // sign of the imaginary part of W16^1
-    switch (m) {
-        case 0: return z;
-        case 1: return C{c * z.x - sg * s * z.y, c * z.y + sg * s * z.x};
-        case 2: return C{h * (z.x - sg * z.y), h * (z.y + sg * z.x)};
-        case 3: return C{s * z.x - sg * c * z.y, s * z.y + sg * c * z.x};
-        case 4: return C{-sg * z.y, sg * z.x};
-        case 6: return C{-h * (z.x + sg * z.y), -h * (z.y - sg * z.x)};
-        default: return C{-c * z.x + sg * s * z.y, -c * z.y - sg * s * z.x};  // 9
-    }
-}
-
 // R-point DFT in registers; forward uses exp(-2 pi i / R).
 template <typename T, int R, bool INV>
 __device__ __forceinline__ void dft(Cx<T>* v) {
@@ -228,24 +204,6 @@ __device__ __forceinline__ void dft(Cx<T>* v) {
             v[2 * m] = a[m];
             v[2 * m + 1] = b[m];
         }
-    } else if constexpr (R == 16) {
-        // 4 x 4: a[n2][k1] = DFT4 over n1 of x[n2 + 4 n1], times W16^(n2 k1);
-        // X[k1 + 4 k2] = DFT4 over n2
-        C a[4][4];
-#pragma unroll
-        for (int n2 = 0; n2 < 4; ++n2) {
-            C t[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
-            dft<T, 4, INV>(t);
-#pragma unroll
-            for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = w16<T, INV>(t[k1], n2 * k1);
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1) {
-            C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
-            dft<T, 4, INV>(t);
-#pragma unroll
-            for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
-        }
     } else if constexpr (R == 5) {
         const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
         const T s1 = INV ? (T)0.95105651629515357212 : (T)-0.95105651629515357212;
@@ -289,12 +247,8 @@ __device__ __forceinline__ void dft_half(Cx<T>* v) {
             v[1] = C{a.x - b.y, a.y + b.x};
             v[3] = C{a.x + b.y, a.y - b.x};
         }
-    } else if constexpr (R == 16) {
-#pragma unroll
-        for (int k = 8; k < 16; ++k) v[k] = C{(T)0, (T)0};
-        dft<T, 16, INV>(v);
     } else {
-        static_assert(R == 8, "half-input DFT for radix 2, 4, 8, 16");
+        static_assert(R == 8, "half-input DFT for radix 2, 4, 8");
         const T h = (T)0.70710678118654752440;
         C a[4], b[4];
 #pragma unroll
@@ -392,7 +346,7 @@ __device__ __forceinline__ Cx<T>* stages_c(Cx<T>* a, Cx<T>* b, const Cx<T>* tw) 
     } else {
         constexpr int R = P.r[S];
         constexpr bool even = R % 2 == 0;
-        constexpr int NZ = (PR == kPruneIn && S == 0 && even && R <= 16) ? R / 2 : R;
+        constexpr int NZ = (PR == kPruneIn && S == 0 && even && R <= 8) ? R / 2 : R;
         constexpr int NO = (PR == kPruneOut && S == P.nst - 1 && even) ? R / 2 : R;
         stage_c<T, R, INV, L, NS, NC, NT, NZ, NO>(a, b, tw + OFF);
         __syncthreads();
@@ -428,9 +382,7 @@ __device__ __forceinline__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, const FftPla
         Cx<T>* b = tmp;
         for (int s = 0; s < pl.nst; ++s) {
             const int R = pl.r[s];
-            if (R == 16)
-                stage_r<T, 16, INV>(a, b, pl.L, Ns, NC, tw);
-            else if (R == 8)
+            if (R == 8)
                 stage_r<T, 8, INV>(a, b, pl.L, Ns, NC, tw);
             else if (R == 4)
                 stage_r<T, 4, INV>(a, b, pl.L, Ns, NC, tw);

@@ -1377,7 +1377,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
 }
 constexpr size_t kGatherSmem = 2 * 6 * kStreamChunk * sizeof(double);
 template <typename T, bool EXT = false>
-__global__ void __launch_bounds__(kThreads, 3) k_gather_staged(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == sizeof(float) ? 4 : 3) k_gather_staged(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
                                                                double* __restrict__ z, double* __restrict__ px,
                                                                double* __restrict__ py, double* __restrict__ pz,
                                                                const T* __restrict__ E4, StepState* st, double* partials,
