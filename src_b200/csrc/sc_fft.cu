@@ -85,9 +85,6 @@ __device__ __forceinline__ void cp_elem(V* smem, const V* gmem) {
 // Radix sequence of a length L = 2^p 3^a 5^b: radix-8 stages for the power of
 // two (a remainder of 2 with an 8 becomes 4 x 4, so no radix-2 stage runs
 // beside radix 8), then 3s and 5s.  nst = -1 when L has another factor.
-// (Radix-16 stages -- 128 = 16 x 8 -- were measured slower at 128 points:
-// their registers halve the resident blocks and half the threads idle in
-// the 16-point stage.)
 struct RadixPlan {
     int nst;
     int r[12];
@@ -277,10 +274,7 @@ __device__ __forceinline__ void dft_half(Cx<T>* v) {
 // and writes element (j / Ns) Ns R + k + r Ns (positions through sk()).
 // NZ < R: inputs r >= NZ are known zeros (NZ = R/2 only); NO < R: only
 // outputs r < NO are needed; FIRST: Ns = 1, all twiddles are 1.
-// STW: tw is the stage's own table, W^(r k step) at (r - 1) Ns + k, so that
-// the lanes of a warp (consecutive k) read consecutive entries; otherwise tw
-// is the whole table W^e, e in [0, L).
-template <typename T, int R, bool INV, int NZ = R, int NO = R, bool FIRST = false, bool STW = false>
+template <typename T, int R, bool INV, int NZ = R, int NO = R, bool FIRST = false>
 __device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst, int j, int nb, int Ns,
                                           int step, const Cx<T>* __restrict__ tw) {
     using C = Cx<T>;
@@ -292,7 +286,7 @@ __device__ __forceinline__ void butterfly(const Cx<T>* __restrict__ src, Cx<T>* 
     if constexpr (!FIRST) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-            C t = STW ? tw[(r - 1) * Ns + k] : tw[r * k * step];
+            C t = tw[r * k * step];
             if (INV) t.y = -t.y;
             v[r] = cmul(v[r], t);
         }
@@ -319,8 +313,7 @@ __host__ __device__ constexpr int col_stride(int L) { return L + (L >> 3) + 1; }
 //               writes half.
 constexpr int kPruneNone = 0, kPruneIn = 1, kPruneOut = 2;
 
-// compile-time stage: length L, Ns, NC columns, NT threads; tw is the
-// stage's own twiddle table (stage_twiddles)
+// compile-time stage: length L, Ns, NC columns, NT threads
 template <typename T, int R, bool INV, int L, int NS, int NC, int NT, int NZ, int NO>
 __device__ __forceinline__ void stage_c(const Cx<T>* in, Cx<T>* out, const Cx<T>* tw) {
     constexpr int NB = L / R;
@@ -332,13 +325,11 @@ __device__ __forceinline__ void stage_c(const Cx<T>* in, Cx<T>* out, const Cx<T>
         if ((NC * NB) % NT != 0 && w >= NC * NB) break;
         const int col = w / NB;
         const int j = w - col * NB;
-        butterfly<T, R, INV, NZ, NO, NS == 1, true>(in + col * CS, out + col * CS, j, NB, NS, STEP, tw);
+        butterfly<T, R, INV, NZ, NO, NS == 1>(in + col * CS, out + col * CS, j, NB, NS, STEP, tw);
     }
 }
 
-// OFF: offset of stage S's table in the per-stage twiddle layout (the first
-// stage has none; stage s > 0 holds (R_s - 1) Ns_s entries).
-template <typename T, bool INV, int L, int S, int NS, int NC, int NT, int PR, int OFF = 0>
+template <typename T, bool INV, int L, int S, int NS, int NC, int NT, int PR>
 __device__ __forceinline__ Cx<T>* stages_c(Cx<T>* a, Cx<T>* b, const Cx<T>* tw) {
     constexpr RadixPlan P = radix_plan(L);
     if constexpr (S == P.nst) {
@@ -348,9 +339,9 @@ __device__ __forceinline__ Cx<T>* stages_c(Cx<T>* a, Cx<T>* b, const Cx<T>* tw) 
         constexpr bool even = R % 2 == 0;
         constexpr int NZ = (PR == kPruneIn && S == 0 && even && R <= 8) ? R / 2 : R;
         constexpr int NO = (PR == kPruneOut && S == P.nst - 1 && even) ? R / 2 : R;
-        stage_c<T, R, INV, L, NS, NC, NT, NZ, NO>(a, b, tw + OFF);
+        stage_c<T, R, INV, L, NS, NC, NT, NZ, NO>(a, b, tw);
         __syncthreads();
-        return stages_c<T, INV, L, S + 1, NS * R, NC, NT, PR, OFF + (S > 0 ? (R - 1) * NS : 0)>(b, a, tw);
+        return stages_c<T, INV, L, S + 1, NS * R, NC, NT, PR>(b, a, tw);
     }
 }
 
@@ -402,34 +393,9 @@ __device__ __forceinline__ Cx<T>* block_fft(Cx<T>* buf, Cx<T>* tmp, const FftPla
     }
 }
 
-// The twiddles of a block's transforms into shared memory.  A template
-// length stages the per-stage layout the compile-time stages read (stage s >
-// 0: W^(r k step_s) at offset_s + (r - 1) Ns_s + k, L - R_0 entries in all,
-// taken from the full table src[e] = W^e); a run-time length stages the full
-// table.
-template <typename V, int LT, int NT>
+template <typename V, int NT>
 __device__ __forceinline__ void stage_twiddles(V* dst, const V* __restrict__ src, int L) {
-    if constexpr (LT > 0) {
-        constexpr RadixPlan P = radix_plan(LT);
-        for (int e = threadIdx.x; e < LT - P.r[0]; e += NT) {
-            int off = 0, ns = P.r[0], q = e;
-#pragma unroll
-            for (int st = 1; st < P.nst; ++st) {
-                const int size = (P.r[st] - 1) * ns;
-                if (q < size) {
-                    const int r = q / ns + 1, k = q - (r - 1) * ns;
-                    const int step = LT / (ns * P.r[st]);
-                    cp_elem(dst + off + q, src + r * k * step);
-                    break;
-                }
-                q -= size;
-                off += size;
-                ns *= P.r[st];
-            }
-        }
-    } else {
-        for (int e = threadIdx.x; e < L; e += NT) cp_elem(dst + e, src + e);
-    }
+    for (int e = threadIdx.x; e < L; e += NT) cp_elem(dst + e, src + e);
 }
 
 // elements of one tile: twiddles (L), buf and tmp (NC col_stride(L) + 2 NC each)
@@ -454,7 +420,7 @@ __device__ __forceinline__ void fft_z_r2c_body(const T* __restrict__ rho, Cx<T>*
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L2;
     C* tmp = buf + NC * CS + RC;
-    stage_twiddles<C, LT, NT>(tw, twz, L2);
+    stage_twiddles<C, NT>(tw, twz, L2);
     const int y = by;
     const int x0 = bx * RC;
     for (int e = threadIdx.x; e < RC * (LT > 0 ? n2 : L2); e += NT) {  // the zero half is not staged when pruned
@@ -503,7 +469,7 @@ __device__ __forceinline__ void fft_y_body(Cx<T>* __restrict__ spec, int n0, int
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L1;
     C* tmp = buf + NC * CS + 2 * NC;
-    stage_twiddles<C, LT, NT>(tw, twy, L1);
+    stage_twiddles<C, NT>(tw, twy, L1);
     const int kz = by;
     const int x0 = bx * NC;
     C* plane = spec + (size_t)kz * L1 * L0;
@@ -554,8 +520,8 @@ __device__ __forceinline__ void fft_x_conv_body(const Cx<TI>* in, Cx<TO>* out, c
     CI* tw_i = reinterpret_cast<CI*>(tw_o + L0);
     CO* bufo = reinterpret_cast<CO*>(tw_i + L0);
     CO* tmpo = bufo + NC * CS;
-    stage_twiddles<CO, LT, NT>(tw_o, two, L0);
-    stage_twiddles<CI, LT, NT>(tw_i, twi, L0);
+    stage_twiddles<CO, NT>(tw_o, two, L0);
+    stage_twiddles<CI, NT>(tw_i, twi, L0);
     CI* bufi = reinterpret_cast<CI*>(bufo);
     CI* tmpi = reinterpret_cast<CI*>(tmpo);
     const int r0 = bx * NC;
@@ -624,7 +590,7 @@ __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, d
     C* tw = reinterpret_cast<C*>(smem_raw);
     C* buf = tw + L2;
     C* tmp = buf + NC * CS + RC;
-    stage_twiddles<C, LT, NT>(tw, twz, L2);
+    stage_twiddles<C, NT>(tw, twz, L2);
     const int y = by;
     const int x0 = bx * RC;
     // the half spectra of the 2 NC columns in tmp: [xi][k], k <= K = L2 / 2
@@ -698,7 +664,7 @@ __device__ __forceinline__ void dct_lines_body(const double* __restrict__ in, TO
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double2* buf = tw + L;
     double2* tmp = buf + NC * CS + RC;
-    stage_twiddles<double2, LT, NT>(tw, twd, L);
+    stage_twiddles<double2, NT>(tw, twd, L);
     const int b0 = bx * RC;
     const long long obase = (long long)by * so;
     for (int e = threadIdx.x; e < RC * len; e += NT) {
@@ -750,7 +716,7 @@ __device__ __forceinline__ void rfft_lines_neg_body(const double* __restrict__ i
     double2* tw = reinterpret_cast<double2*>(smem_raw);
     double2* buf = tw + L;
     double2* tmp = buf + NC * CS + RC;
-    stage_twiddles<double2, LT, NT>(tw, twd, L);
+    stage_twiddles<double2, NT>(tw, twd, L);
     const int b0 = bx * RC;
     for (int e = threadIdx.x; e < RC * L; e += NT) {
         const int li = e % RC, m = e / RC;

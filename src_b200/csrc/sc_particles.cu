@@ -1,9 +1,11 @@
 // sc_particles.cu -- particle-side kernels of the space-charge step.
 //
-// Compiled with -fmad=false: every per-particle expression rounds like the
-// reference's CPU code (push, kick, frame transforms, CIC weights).  Divisions
-// by a per-bunch or per-step constant use div_rcp (a correctly rounded
-// quotient from the correctly rounded reciprocal), so they stay bit-exact.
+// Compiled with -fmad=false: every per-particle expression of the plain form
+// rounds like the reference's CPU code (push, kick, frame transforms, CIC
+// weights).  Divisions by a per-bunch or per-step constant use div_rcp (a
+// correctly rounded quotient from the correctly rounded reciprocal), so they
+// stay bit-exact.  The mixed form's particle update (mixed_particle) writes
+// its fused multiply-adds explicitly.
 //
 //   k_reduce_state       momentum sums (+ beam statistics) and the beam frame
 //   k_drift_to_beam      half drift, reference -> beam frame, bounds, mesh
@@ -15,6 +17,8 @@
 //   k_grad               -Grad phi (UniformCartesian.hpp:2129-2203), boost scaling
 //   k_gather_kick_push   CIC gather, B from E, back to the reference frame, Boris
 //                        kick, half drift, reference-frame update, momentum sums
+//   k_gather_staged      the same with the particle state streamed through shared
+//                        memory by bulk copies (cp.async.bulk, mbarrier), the default
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -1377,7 +1381,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_gather_kick_push(BunchConst bc,
 }
 constexpr size_t kGatherSmem = 2 * 6 * kStreamChunk * sizeof(double);
 template <typename T, bool EXT = false>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == sizeof(float) ? 4 : 3) k_gather_staged(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
+__global__ void __launch_bounds__(kThreads, 3) k_gather_staged(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
                                                                double* __restrict__ z, double* __restrict__ px,
                                                                double* __restrict__ py, double* __restrict__ pz,
                                                                const T* __restrict__ E4, StepState* st, double* partials,
