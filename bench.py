@@ -145,6 +145,14 @@ class ClockSampler:
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        if not self.lines:
+            # a timed region shorter than the sampling period: one sample as it ends
+            try:
+                out = subprocess.run(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=10).stdout
+                self.lines.extend(l.strip() for l in out.splitlines() if l.strip())
+            except (OSError, subprocess.TimeoutExpired):
+                pass
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
