@@ -452,7 +452,7 @@ __device__ __forceinline__ void fft_z_r2c_body(const T* __restrict__ rho, Cx<T>*
     }
 }
 template <typename T, int LT, int NC, int NT, bool FULL = false>
-__global__ void __launch_bounds__(NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1, int n2,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_fft_z_r2c(const T* __restrict__ rho, Cx<T>* __restrict__ spec, int n0, int n1, int n2,
                                                   int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz) {
     fft_z_r2c_body<T, LT, NC, NT, FULL>(rho, spec, n0, n1, n2, L0, L1, pz, twz, blockIdx.x, blockIdx.y);
 }
@@ -492,7 +492,7 @@ __device__ __forceinline__ void fft_y_body(Cx<T>* __restrict__ spec, int n0, int
     }
 }
 template <typename T, bool INV, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, int L0, int n_in, int n_out, FftPlan py,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_fft_y(Cx<T>* __restrict__ spec, int n0, int L0, int n_in, int n_out, FftPlan py,
                                               const Cx<T>* __restrict__ twy) {
     fft_y_body<T, INV, LT, NC, NT>(spec, n0, L0, n_in, n_out, py, twy, blockIdx.x, blockIdx.y);
 }
@@ -567,7 +567,7 @@ __device__ __forceinline__ void fft_x_conv_body(const Cx<TI>* in, Cx<TO>* out, c
     }
 }
 template <typename TI, typename TO, int LT, int NC, int NT, bool CG = false>
-__global__ void __launch_bounds__(NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0, int n1,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_fft_x_conv(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0, int n1,
                                                    int L1, int rows, FftPlan px, const Cx<TI>* __restrict__ twi,
                                                    const Cx<TO>* __restrict__ two) {
     fft_x_conv_body<TI, TO, LT, NC, NT, CG>(in, out, ghat, n0, n1, L1, rows, px, twi, two, blockIdx.x);
@@ -642,7 +642,7 @@ __device__ __forceinline__ void fft_z_c2r_body(const Cx<T>* __restrict__ spec, d
     }
 }
 template <typename T, bool SELF, int LT, int NC, int NT, bool FLIP = false, bool FULL = false>
-__global__ void __launch_bounds__(NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_fft_z_c2r(const Cx<T>* __restrict__ spec, double* __restrict__ phi, int n0, int n1,
                                                   int n2, int L0, int L1, FftPlan pz, const Cx<T>* __restrict__ twz,
                                                   const StepState* __restrict__ st, double normFact, double coupling) {
     fft_z_c2r_body<T, SELF, LT, NC, NT, FLIP, FULL>(spec, phi, n0, n1, n2, L0, L1, pz, twz, st, normFact, coupling,
@@ -694,7 +694,7 @@ __device__ __forceinline__ void dct_lines_body(const double* __restrict__ in, TO
     }
 }
 template <typename TO, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_dct_lines(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_dct_lines(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
                                                   long long sb, long long so, long long se, FftPlan pl,
                                                   const double2* __restrict__ twd) {
     dct_lines_body<TO, LT, NC, NT>(in, out, len, nb, sb, so, se, pl, twd, blockIdx.x, blockIdx.y);
@@ -750,7 +750,7 @@ __device__ __forceinline__ void rfft_lines_neg_body(const double* __restrict__ i
     }
 }
 template <typename TO, int LT, int NC, int NT, bool NEG = true>
-__global__ void __launch_bounds__(NT) k_rfft_lines_neg(const double* __restrict__ in, Cx<TO>* __restrict__ out, int nb,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_rfft_lines_neg(const double* __restrict__ in, Cx<TO>* __restrict__ out, int nb,
                                                        long long se, FftPlan pl, const double2* __restrict__ twd) {
     rfft_lines_neg_body<TO, LT, NC, NT, NEG>(in, out, nb, se, pl, twd, blockIdx.x);
 }
@@ -1020,7 +1020,7 @@ __device__ __forceinline__ const Cx<T>* tw_dev(const DevBunch& d, int a) {
 // at block coordinates (work[i].y, work[i].z), with that bunch's sizes and
 // buffers (T: the forward-half type, as in convolution_t).
 template <typename T, int PASS, int LT, int NC, int NT>
-__global__ void __launch_bounds__(NT) k_fft_pass_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_fft_pass_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work,
                                                         int nitems) {
     const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
