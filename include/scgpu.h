@@ -31,6 +31,9 @@
  *       no counterpart (measurement of this implementation)
  *   scgpu_set_periodic_z
  *       the bcz argument of FFTPoissonSolver (FieldSolver BCFFTZ, src/Structure/FieldSolver.cpp:431, :486)
+ *       with PartBunch::setBCForDCBeam (src/Classic/Algorithms/PartBunch.cpp:1079-1098)
+ *   scgpu_set_beam_frequency
+ *       PartBunchBase::setBeamFrequency (src/Classic/Algorithms/PartBunchBase.hpp:2535-2537)
  *   scgpu_compute_potential_image, scgpu_compute_potential_image_device
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr, double zshift)
  *       (src/Solvers/PoissonSolver.h:59; FFTPoissonSolver.cpp:287-327 with
@@ -238,12 +241,33 @@ int scgpu_fieldmap_astra1d_dynamic(const char* path, double* coefs, int max_coef
 /* FIELDSOLVER BCFFTZ=PERIODIC (FFTPoissonSolver(..., bcz="PERIODIC"),
  * src/Solvers/FFTPoissonSolver.cpp:60, :130-155, :189-190, :661-662): the
  * context's Poisson solves (scgpu_compute_potential[_device],
- * scgpu_compute_self_fields) double the grid in x and y only and convolve
- * cyclically along z with the integrated Green's function at offsets
- * [0, nz) (not mirrored in z).  Needs an even nz; tracking (which would need
- * the periodic particle boundary of a DC beam), energy bins and image
- * charges return SCGPU_ERR_UNSUPPORTED while it is on. */
+ * scgpu_compute_self_fields, scgpu_track) double the grid in x and y only
+ * and convolve cyclically along z with the integrated Green's function at
+ * offsets [0, nz) (not mirrored in z).  Needs an even nz.
+ *
+ * The bunch becomes a DC beam, as TrackRun pairs a periodic-z solver with
+ * PartBunch::setBCForDCBeam (src/Track/TrackRun.cpp:899-902,
+ * src/Classic/Algorithms/PartBunch.cpp:1079-1098):
+ *   - boundp's mesh (PartBunchBase.hpp:813-843): x and y as for an open
+ *     bunch; z starts at the lowest particle, not enlarged, and spans the
+ *     period length L: hz = L / (nz - 1), origin_z = zmin - hz / 2;
+ *   - the periodic particle boundary along z (ParticlePeriodicBCond,
+ *     ippl/src/Particle/ParticleBConds.h:37-45) over the mesh's domain
+ *     [origin_z, origin_z + nz hz), applied once per step before the
+ *     scatter; a wrapped position stays wrapped (the tracked bunch carries
+ *     it, as the reference's does);
+ *   - the scatter drops the charge that lands in the z guard planes -1 and
+ *     nz (the reference's single-rank scatter does not carry guard cells
+ *     into the field); the gather reads there the field's periodic images
+ *     (PeriodicFace: plane nz is plane 0, plane -1 is plane nz-1).
+ * Energy bins and image charges return SCGPU_ERR_UNSUPPORTED while it is on. */
 int scgpu_set_periodic_z(scgpu_ctx* ctx, int periodic);
+
+/* PartBunchBase::setBeamFrequency (src/Classic/Algorithms/PartBunchBase.hpp:
+ * 2535-2537; TrackRun.cpp:496 passes the BEAM's FREQUENCY in Hz): the DC
+ * beam's period length L = c / f.  Default L = c / 1 GHz (PartBunchBase.hpp:
+ * 132).  f must be positive and finite. */
+int scgpu_set_beam_frequency(scgpu_ctx* ctx, double f_hz);
 
 /* How often the tracker puts the particle arrays in cell order (a counting
  * sort by the CIC cell, so that the deposit's warps share few cells): every

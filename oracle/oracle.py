@@ -40,7 +40,7 @@ class Trafo(C.Structure):
 class Params(C.Structure):
     _fields_ = [("nr", C.c_int * 3), ("pad_", C.c_int), ("dh", C.c_double), ("dT", C.c_double),
                 ("mass", C.c_double), ("charge", C.c_double), ("coupling", C.c_double),
-                ("bz_ext", C.c_double), ("ref_pz", C.c_double)]
+                ("bz_ext", C.c_double), ("ref_pz", C.c_double), ("period", C.c_double)]
 
 
 class Tracker(C.Structure):
@@ -364,21 +364,41 @@ def boundp(R, nr, dh):
     return m
 
 
-def scatter_cic(R, q, mesh):
+def boundp_dc(R, nr, dh, period):
+    """boundp of a DC beam: z spans one period from the lowest particle."""
+    R = _f64(R)
+    m = Mesh()
+    rc = lib().sco_boundp_dc(C.c_longlong(R.shape[0]), _ptr(R), (C.c_int * 3)(*nr), C.c_double(dh),
+                             C.c_double(period), C.byref(m))
+    if rc:
+        raise RuntimeError(f"boundp_dc failed: {rc}")
+    return m
+
+
+def wrap_z(R, mesh):
+    """The periodic particle boundary along z over the mesh's domain."""
+    R = _f64(R).copy()
+    lib().sco_wrap_z(C.c_longlong(R.shape[0]), _ptr(R), C.byref(mesh))
+    return R
+
+
+def scatter_cic(R, q, mesh, dc=False):
     R = _f64(R)
     nr = list(mesh.nr)
     rho = np.zeros((nr[2], nr[1], nr[0]), dtype=np.float64)
-    rc = lib().sco_scatter_cic(C.c_longlong(R.shape[0]), _ptr(R), C.c_double(q), C.byref(mesh), _ptr(rho))
+    fn = lib().sco_scatter_cic_dc if dc else lib().sco_scatter_cic
+    rc = fn(C.c_longlong(R.shape[0]), _ptr(R), C.c_double(q), C.byref(mesh), _ptr(rho))
     if rc:
         raise RuntimeError(f"scatter failed: {rc}")
     return rho
 
 
-def gather_cic(R, mesh, E):
+def gather_cic(R, mesh, E, dc=False):
     R = _f64(R)
     E = _f64(E)
     Ef = np.empty_like(R)
-    rc = lib().sco_gather_cic(C.c_longlong(R.shape[0]), _ptr(R), C.byref(mesh), _ptr(E), _ptr(Ef))
+    fn = lib().sco_gather_cic_dc if dc else lib().sco_gather_cic
+    rc = fn(C.c_longlong(R.shape[0]), _ptr(R), C.byref(mesh), _ptr(E), _ptr(Ef))
     if rc:
         raise RuntimeError(f"gather failed: {rc}")
     return Ef
@@ -406,7 +426,9 @@ def beam_parameters(R, P):
     return bp.as_dict()
 
 
-def make_params(nr, dT, dh=0.02, bz_ext=0.0, ref_pz=10.0, mass=None, charge=-1.0):
+def make_params(nr, dT, dh=0.02, bz_ext=0.0, ref_pz=10.0, mass=None, charge=-1.0, period=0.0):
+    """Solver and tracker parameters; period > 0 makes the bunch a DC beam
+    (periodic z) with that period length [m]."""
     p = Params()
     p.nr = (C.c_int * 3)(*nr)
     p.dh = dh
@@ -416,13 +438,16 @@ def make_params(nr, dT, dh=0.02, bz_ext=0.0, ref_pz=10.0, mass=None, charge=-1.0
     p.coupling = coupling()
     p.bz_ext = bz_ext
     p.ref_pz = ref_pz
+    p.period = period
     return p
 
 
 def compute_self_fields(params, Q, R, P, want_grids=True):
     """PartBunch::computeSelfFields on a bunch in the beam frame.
-    Returns (Ef, Bf, Q_after, debug dict)."""
-    R = _f64(R)
+    Returns (Ef, Bf, Q_after, debug dict); for a DC beam the debug dict's
+    "R" holds the positions after the periodic boundary (the caller's R is
+    not changed)."""
+    R = _f64(R).copy()
     P = _f64(P)
     n = R.shape[0]
     nr = list(params.nr)
@@ -439,7 +464,9 @@ def compute_self_fields(params, Q, R, P, want_grids=True):
                                        _ptr(Ef), _ptr(Bf), C.byref(dbg))
     if rc:
         raise RuntimeError(f"compute_self_fields failed: {rc}")
-    return Ef, Bf, q.value, _debug_dict(dbg, grids, nr)
+    out = _debug_dict(dbg, grids, nr)
+    out["R"] = R
+    return Ef, Bf, q.value, out
 
 
 def _debug_dict(dbg, grids, nr):

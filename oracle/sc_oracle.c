@@ -490,12 +490,64 @@ int sco_boundp(long long n, const double* R, const int* nr, double dh, sco_mesh*
     return 0;
 }
 
+/* boundp of a DC beam (PartBunchBase.hpp:813-843 with dcBeam_m): x and y as
+ * above, z not enlarged: rmax_z = rmin_z + periodLength, hr_z = periodLength
+ * / (MT - 1). */
+int sco_boundp_dc(long long n, const double* R, const int* nr, double dh, double period, sco_mesh* mesh) {
+    double rmin[3], rmax[3];
+    sco_bounds(n, R, rmin, rmax);
+    for (int i = 0; i < 2; ++i) {
+        double length = fabs(rmax[i] - rmin[i]);
+        if (length < 1e-10) {
+            rmax[i] += 1e-10;
+            rmin[i] -= 1e-10;
+        } else {
+            rmax[i] += dh * length;
+            rmin[i] -= dh * length;
+        }
+        mesh->hr[i] = (rmax[i] - rmin[i]) / (nr[i] - 1);
+    }
+    rmax[2] = rmin[2] + period;
+    mesh->hr[2] = period / (nr[2] - 1);
+    for (int i = 0; i < 3; ++i) {
+        mesh->rmin[i] = rmin[i];
+        mesh->rmax[i] = rmax[i];
+        mesh->nr[i] = nr[i];
+    }
+    if (mesh->hr[0] * mesh->hr[1] * mesh->hr[2] <= 0) return SCO_ERR_MESH;
+    mesh->origin[0] = rmin[0] - mesh->hr[0] / 2.0;
+    mesh->origin[1] = rmin[1] - mesh->hr[1] / 2.0;
+    mesh->origin[2] = rmin[2] - mesh->hr[2] / 2.0;
+    return 0;
+}
+
+/* boundp's update() for a DC beam: the particle layout's domain follows the
+ * mesh (RegionLayout::Repartition on the mesh's change notification,
+ * RegionLayout.hpp:871-896; getMeshDomain :773-789: [origin, origin + h *
+ * cells)), and ParticleSpatialLayout::update (ParticleSpatialLayout.hpp:
+ * 296-297) applies ParticlePeriodicBCond (ParticleBConds.h:37-45) along z,
+ * once per particle. */
+void sco_wrap_z(long long n, double* R, const sco_mesh* m) {
+    const double lo = m->origin[2];
+    const double hi = m->origin[2] + m->hr[2] * (double)m->nr[2];
+    SCO_PAR
+    for (long long i = 0; i < n; ++i) {
+        const double t = R[3 * i + 2];
+        if (t < lo)
+            R[3 * i + 2] = hi - (lo - t);
+        else if (t >= hi)
+            R[3 * i + 2] = lo + (t - hi);
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* CIC (IntCIC.h:818-858 scatter, :935-975 gather)                           */
 /* ------------------------------------------------------------------------ */
 /* lower grid point and normalised offset; returns 0 when all 8 targets lie
- * inside the n^3 cell field, -1 otherwise (a guard-cell access). */
-static inline int cic_locate(const sco_mesh* m, const double* x, int* lgp, double* dpos) {
+ * inside the n^3 cell field, -1 otherwise (a guard-cell access).  With pz
+ * (a DC beam) the z targets may also lie in the guard layer, planes -1 and
+ * n: lower points -1 .. n-1 along z. */
+static inline int cic_locate_bc(const sco_mesh* m, const double* x, int* lgp, double* dpos, int pz) {
     for (int d = 0; d < 3; ++d) {
         /* getVertexBelow (UniformCartesian.hpp:1025-1039) */
         int i = (int)((x[d] - m->origin[d]) / m->hr[d]);
@@ -511,14 +563,19 @@ static inline int cic_locate(const sco_mesh* m, const double* x, int* lgp, doubl
         }
         dpos[d] = x[d] - gpos;
         dpos[d] /= delta;
-        if (lgp[d] < 0 || lgp[d] + 1 > m->nr[d] - 1) return -1;
+        const int guard = (pz && d == 2) ? 1 : 0;
+        if (lgp[d] < -guard || lgp[d] + 1 > m->nr[d] - 1 + guard) return -1;
     }
     return 0;
 }
+static inline int cic_locate(const sco_mesh* m, const double* x, int* lgp, double* dpos) {
+    return cic_locate_bc(m, x, lgp, dpos, 0);
+}
 
-static int scatter_range(long long p0, long long p1, const double* R, double q, const sco_mesh* m, double* rho);
+static int scatter_range(long long p0, long long p1, const double* R, double q, const sco_mesh* m, double* rho,
+                         int pz);
 
-int sco_scatter_cic(long long n, const double* R, double q, const sco_mesh* m, double* rho) {
+static int scatter_bc(long long n, const double* R, double q, const sco_mesh* m, double* rho, int pz) {
     if (g_threads > 1) {
         const int T = g_threads;
         const long long M = (long long)m->nr[0] * m->nr[1] * m->nr[2];
@@ -531,7 +588,7 @@ int sco_scatter_cic(long long n, const double* R, double q, const sco_mesh* m, d
 #else
             const int t = 0;
 #endif
-            bad |= scatter_range(n * t / T, n * (t + 1) / T, R, q, m, grids + (size_t)t * M) != 0;
+            bad |= scatter_range(n * t / T, n * (t + 1) / T, R, q, m, grids + (size_t)t * M, pz) != 0;
         }
 #pragma omp parallel for num_threads(T) schedule(static)
         for (long long c = 0; c < M; ++c)
@@ -539,40 +596,64 @@ int sco_scatter_cic(long long n, const double* R, double q, const sco_mesh* m, d
         free(grids);
         return bad ? SCO_ERR_GUARD : 0;
     }
-    return scatter_range(0, n, R, q, m, rho);
+    return scatter_range(0, n, R, q, m, rho, pz);
 }
 
-static int scatter_range(long long p0, long long p1, const double* R, double q, const sco_mesh* m, double* rho) {
+int sco_scatter_cic(long long n, const double* R, double q, const sco_mesh* m, double* rho) {
+    return scatter_bc(n, R, q, m, rho, 0);
+}
+
+/* The single-rank scatter of a DC beam: the charge IntCIC writes into the z
+ * guard layer is not carried into the field (ParticleAttrib::scatter zeroes
+ * the guard cells, ParticleAttrib.h:207-221, and accumGuardCells,
+ * BareField.hpp:1013-1079, adds guard cells only into neighbouring local
+ * fields, of which one vnode has none). */
+int sco_scatter_cic_dc(long long n, const double* R, double q, const sco_mesh* m, double* rho) {
+    return scatter_bc(n, R, q, m, rho, 1);
+}
+
+static int scatter_range(long long p0, long long p1, const double* R, double q, const sco_mesh* m, double* rho,
+                         int pz) {
     const long long nx = m->nr[0], nxy = (long long)m->nr[0] * m->nr[1];
     const long long n = p1;
     int bad = 0;
     for (long long p = p0; p < n; ++p) {
         int l[3];
         double d[3];
-        if (cic_locate(m, R + 3 * p, l, d)) { bad = 1; continue; }
-        double* f = rho + l[0] + nx * l[1] + nxy * l[2];
-        f[0] += (1 - d[0]) * (1 - d[1]) * (1 - d[2]) * q;
-        f[1] += d[0] * (1 - d[1]) * (1 - d[2]) * q;
-        f[nx] += (1 - d[0]) * d[1] * (1 - d[2]) * q;
-        f[nx + 1] += d[0] * d[1] * (1 - d[2]) * q;
-        f[nxy] += (1 - d[0]) * (1 - d[1]) * d[2] * q;
-        f[nxy + 1] += d[0] * (1 - d[1]) * d[2] * q;
-        f[nxy + nx] += (1 - d[0]) * d[1] * d[2] * q;
-        f[nxy + nx + 1] += d[0] * d[1] * d[2] * q;
+        if (cic_locate_bc(m, R + 3 * p, l, d, pz)) { bad = 1; continue; }
+        const long long b = l[0] + nx * l[1] + nxy * l[2];
+        if (l[2] >= 0) { /* plane l: inside unless a DC beam's guard plane -1 */
+            rho[b] += (1 - d[0]) * (1 - d[1]) * (1 - d[2]) * q;
+            rho[b + 1] += d[0] * (1 - d[1]) * (1 - d[2]) * q;
+            rho[b + nx] += (1 - d[0]) * d[1] * (1 - d[2]) * q;
+            rho[b + nx + 1] += d[0] * d[1] * (1 - d[2]) * q;
+        }
+        if (l[2] + 1 < m->nr[2]) { /* plane l + 1: inside unless the guard plane n */
+            rho[b + nxy] += (1 - d[0]) * (1 - d[1]) * d[2] * q;
+            rho[b + nxy + 1] += d[0] * (1 - d[1]) * d[2] * q;
+            rho[b + nxy + nx] += (1 - d[0]) * d[1] * d[2] * q;
+            rho[b + nxy + nx + 1] += d[0] * d[1] * d[2] * q;
+        }
     }
     return bad ? SCO_ERR_GUARD : 0;
 }
 
-/* E: 3 components per cell (interleaved).  Ef: 3 per particle. */
-int sco_gather_cic(long long n, const double* R, const sco_mesh* m, const double* E, double* Ef) {
+/* E: 3 components per cell (interleaved).  Ef: 3 per particle.  With pz the
+ * z guard planes hold the periodic images of the field (PeriodicFace, filled
+ * before the gather, ParticleAttrib.h:297-299): plane n is plane 0 and plane
+ * -1 is plane n-1. */
+static int gather_bc(long long n, const double* R, const sco_mesh* m, const double* E, double* Ef, int pz) {
     const long long nx = m->nr[0], nxy = (long long)m->nr[0] * m->nr[1];
+    const int n2 = m->nr[2];
     int bad = 0;
 #pragma omp parallel for num_threads(g_threads) if(g_threads > 1) schedule(static) reduction(| : bad)
     for (long long p = 0; p < n; ++p) {
         int l[3];
         double d[3];
-        if (cic_locate(m, R + 3 * p, l, d)) { bad = 1; Ef[3 * p] = Ef[3 * p + 1] = Ef[3 * p + 2] = 0.0; continue; }
-        const double* f = E + 3 * (l[0] + nx * l[1] + nxy * l[2]);
+        if (cic_locate_bc(m, R + 3 * p, l, d, pz)) { bad = 1; Ef[3 * p] = Ef[3 * p + 1] = Ef[3 * p + 2] = 0.0; continue; }
+        const int z0 = l[2] < 0 ? n2 - 1 : l[2];
+        const int z1 = l[2] + 1 >= n2 ? 0 : l[2] + 1;
+        const double* f = E + 3 * (l[0] + nx * l[1] + nxy * z0);
         const double w0 = (1 - d[0]) * (1 - d[1]) * (1 - d[2]);
         const double w1 = d[0] * (1 - d[1]) * (1 - d[2]);
         const double w2 = (1 - d[0]) * d[1] * (1 - d[2]);
@@ -581,14 +662,23 @@ int sco_gather_cic(long long n, const double* R, const sco_mesh* m, const double
         const double w5 = d[0] * (1 - d[1]) * d[2];
         const double w6 = (1 - d[0]) * d[1] * d[2];
         const double w7 = d[0] * d[1] * d[2];
-        const long long o1 = 3, o2 = 3 * nx, o3 = 3 * (nx + 1), o4 = 3 * nxy, o5 = 3 * (nxy + 1),
-                        o6 = 3 * (nxy + nx), o7 = 3 * (nxy + nx + 1);
+        const long long dz = 3 * nxy * (long long)(z1 - z0);
+        const long long o1 = 3, o2 = 3 * nx, o3 = 3 * (nx + 1), o4 = dz, o5 = dz + 3,
+                        o6 = dz + 3 * nx, o7 = dz + 3 * (nx + 1);
         for (int c = 0; c < 3; ++c) {
             Ef[3 * p + c] = w0 * f[c] + w1 * f[o1 + c] + w2 * f[o2 + c] + w3 * f[o3 + c] +
                             w4 * f[o4 + c] + w5 * f[o5 + c] + w6 * f[o6 + c] + w7 * f[o7 + c];
         }
     }
     return bad ? SCO_ERR_GUARD : 0;
+}
+
+int sco_gather_cic(long long n, const double* R, const sco_mesh* m, const double* E, double* Ef) {
+    return gather_bc(n, R, m, E, Ef, 0);
+}
+
+int sco_gather_cic_dc(long long n, const double* R, const sco_mesh* m, const double* E, double* Ef) {
+    return gather_bc(n, R, m, E, Ef, 1);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -996,11 +1086,13 @@ void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, doub
 /* PartBunch::computeSelfFields()  (PartBunch.cpp:482-647) on a bunch that is */
 /* already in the beam frame, preceded by boundp (PartBunchBase.hpp:802-884). */
 /* ------------------------------------------------------------------------ */
-int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const double* R,
+int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, double* R,
                             const double* P, double* Ef, double* Bf, sco_debug* dbg) {
     sco_mesh mesh;
-    int rc = sco_boundp(n, R, prm->nr, prm->dh, &mesh);
+    const int dc = prm->period > 0.0;
+    int rc = dc ? sco_boundp_dc(n, R, prm->nr, prm->dh, prm->period, &mesh) : sco_boundp(n, R, prm->nr, prm->dh, &mesh);
     if (rc) return rc;
+    if (dc) sco_wrap_z(n, R, &mesh);
     const long long n0 = prm->nr[0], n1 = prm->nr[1], n2 = prm->nr[2];
     const long long M = n0 * n1 * n2;
     double* rho = (double*)calloc(M, sizeof(double));
@@ -1009,7 +1101,7 @@ int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const
     const double dt = prm->dT;
     /* Q *= dt; Q.scatter(rho, R, CIC); Q /= dt; rho /= dT   (:493-496) */
     double qdt = *Q * dt;
-    rc = sco_scatter_cic(n, R, qdt, &mesh, rho);
+    rc = dc ? sco_scatter_cic_dc(n, R, qdt, &mesh, rho) : sco_scatter_cic(n, R, qdt, &mesh, rho);
     *Q = qdt / dt;
     if (rc) { free(rho); free(E); return rc; }
     SCO_PAR
@@ -1032,7 +1124,7 @@ int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const
     SCO_PAR
     for (long long c = 0; c < M; ++c) rho[c] *= tmp2;
     if (dbg && dbg->rho) memcpy(dbg->rho, rho, M * sizeof(double));
-    rc = sco_compute_potential(prm->nr, rho, hr_scaled);
+    rc = dc ? sco_compute_potential_periodic_z(prm->nr, rho, hr_scaled) : sco_compute_potential(prm->nr, rho, hr_scaled);
     if (rc) { free(rho); free(E); return rc; }
     const double hvol = hr_scaled[0] * hr_scaled[1] * hr_scaled[2];
     SCO_PAR
@@ -1042,7 +1134,7 @@ int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const
     if (dbg && dbg->phi) memcpy(dbg->phi, rho, M * sizeof(double));
     sco_neg_grad_scaled(prm->nr, rho, mesh.hr, gammaz, E);
     if (dbg && dbg->E) memcpy(dbg->E, E, 3 * M * sizeof(double));
-    rc = sco_gather_cic(n, R, &mesh, E, Ef);
+    rc = dc ? sco_gather_cic_dc(n, R, &mesh, E, Ef) : sco_gather_cic(n, R, &mesh, E, Ef);
     const double betaC = sqrt(gammaz * gammaz - 1.0) / gammaz / SCO_C;
     SCO_PAR
     for (long long i = 0; i < n; ++i) {
@@ -1287,6 +1379,7 @@ int sco_compute_self_fields_binned(const sco_params* prm, double qi, long long n
                                    const double* P, const int* bin, int nbins, int last_emitted,
                                    double* Ef, double* Bf, double* bin_gamma, sco_debug* dbg) {
     sco_mesh mesh;
+    if (prm->period > 0.0) return SCO_ERR_ARG; /* energy bins with a DC beam: not a reference configuration */
     int rc = sco_boundp(n, R, prm->nr, prm->dh, &mesh);
     if (rc) return rc;
     const long long n0 = prm->nr[0], n1 = prm->nr[1], n2 = prm->nr[2];

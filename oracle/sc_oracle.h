@@ -39,6 +39,8 @@ typedef struct {
     double coupling; /* 1 / (4 pi eps0) */
     double bz_ext;   /* uniform external B_z [T] (0: drift) */
     double ref_pz;   /* reference particle beta*gamma along z at start */
+    double period;   /* 0: open boundaries; > 0: DC beam (periodic z) with
+                        this period length [m] (periodLength_m) */
 } sco_params;
 
 typedef struct {
@@ -107,6 +109,18 @@ int sco_boundp(long long n, const double* R, const int* nr, double dh, sco_mesh*
 int sco_scatter_cic(long long n, const double* R, double q, const sco_mesh* m, double* rho);
 int sco_gather_cic(long long n, const double* R, const sco_mesh* m, const double* E, double* Ef);
 
+/* DC beam (PartBunch::setBCForDCBeam, PartBunch.cpp:1079-1098; chosen for a
+ * field solver with periodic z, TrackRun.cpp:899-902): boundp's mesh with z
+ * not enlarged and spanning one period (PartBunchBase.hpp:813-843); the
+ * periodic particle boundary along z (ParticlePeriodicBCond,
+ * ParticleBConds.h:37-45) over the mesh's domain [origin, origin + n h);
+ * CIC scatter dropping the charge that lands in the z guard layer and
+ * gather reading the periodically filled guard layer. */
+int sco_boundp_dc(long long n, const double* R, const int* nr, double dh, double period, sco_mesh* mesh);
+void sco_wrap_z(long long n, double* R, const sco_mesh* mesh);
+int sco_scatter_cic_dc(long long n, const double* R, double q, const sco_mesh* m, double* rho);
+int sco_gather_cic_dc(long long n, const double* R, const sco_mesh* m, const double* E, double* Ef);
+
 void sco_set_fft_engine(void* cffti, void* cfftf, void* cfftb, void* rffti, void* rfftf, void* rfftb);
 int sco_fft_engine_is_own(void);
 void sco_fft1d(int kind, long long n, double* data);
@@ -122,7 +136,9 @@ int sco_get_exact(void);
 void sco_igf(const int* nr, const double* hr, double* G2);
 int sco_compute_potential(const int* nr, double* rho, const double* hr);
 void sco_neg_grad_scaled(const int* nr, const double* phi, const double* h, double gammaz, double* E);
-int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, const double* R, const double* P,
+/* R: beam-frame positions; a DC beam's (prm->period > 0) are wrapped along
+ * z in place, as boundp's update() does */
+int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, double* R, const double* P,
                             double* Ef, double* Bf, sco_debug* dbg);
 
 /* Elements with ASTRA 1D field maps: SOLENOID (kind 0; Solenoid.cpp:163-193,

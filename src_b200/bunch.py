@@ -99,6 +99,35 @@ def config_bunch(name, n=None, seed=DEFAULT_SEED, bunch_id=0):
                 Q=-1e-9 / N, ref_pz=10.0, dh=0.02)
 
 
+def dc_bunch(n, length, sigma_r=1e-3, bg_z=10.0, rel_spread=1e-3, bg_perp=1e-3, seed=DEFAULT_SEED, bunch_id=0):
+    """A DC (coasting) beam segment: x, y ~ N(0, sigma_r), z uniform on
+    [-length/2, length/2) (53-bit uniforms from the same Philox stream),
+    momenta as gaussian_bunch.  The reference's DC-beam runs take their
+    distributions from the input deck (Distribution.cpp); this seeded
+    stand-in is the shape such a run tracks: a beam whose longitudinal
+    extent is about one period of the periodic-z solver.
+    Returns R, P (n x 3)."""
+    n = int(n)
+    g0, g1 = standard_normals(n, seed, bunch_id, 0)
+    g3, g4 = standard_normals(n, seed, bunch_id, 1)
+    g5, _ = standard_normals(n, seed, bunch_id, 2)
+    i = np.arange(n, dtype=np.uint64)
+    key = (np.uint32(seed & 0xFFFFFFFF), np.uint32((seed >> 32) & 0xFFFFFFFF))
+    ctr = ((i & _MASK).astype(np.uint32), np.full(n, bunch_id & 0xFFFFFFFF, dtype=np.uint32),
+           np.full(n, 3, dtype=np.uint32), (i >> np.uint64(32)).astype(np.uint32))
+    r0, r1, _, _ = philox4x32(ctr, key)
+    u = _uniform53(r0, r1)
+    R = np.empty((n, 3), dtype=np.float64)
+    P = np.empty((n, 3), dtype=np.float64)
+    R[:, 0] = sigma_r * g0
+    R[:, 1] = sigma_r * g1
+    R[:, 2] = length * (u - 0.5)
+    P[:, 0] = bg_perp * g3
+    P[:, 1] = bg_perp * g4
+    P[:, 2] = bg_z * (1.0 + rel_spread * g5)
+    return R, P
+
+
 def photoinjector_bunch(n, nbins=10, sigma_r=1e-3, z_center=4e-3, sigma_z=0.8e-3, bg_head=1.5, bg_tail=0.5,
                         rel_spread=1e-3, bg_perp=1e-3, seed=DEFAULT_SEED, bunch_id=0):
     """A bunch shortly after emission from a cathode at z = 0, with energy bins.

@@ -372,6 +372,16 @@ void enqueue_reorder(scgpu_ctx* c, cudaStream_t s) {
     cudaMemsetAsync(b.hist, 0, (size_t)b.bc.n[0] * b.bc.n[1] * b.bc.n[2] * sizeof(int), s);
 }
 
+// The Green's function and its spectrum (open or periodic z), shared by the
+// step and the solver entry points.
+void enqueue_green(scgpu_ctx* c, cudaStream_t s) {
+    launch_igf(c->b, nullptr, s);
+    if (c->b.periodic_z)
+        launch_green_transform_periodic(c->b, s);
+    else
+        launch_green_transform(c->b, s);
+}
+
 // one ParallelTTracker step on the context's stream
 //   ref:  reference-particle update (needs only the tracker state; joins
 //         before the gather, which applies its frame change)
@@ -393,8 +403,7 @@ void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
     }
     cudaEventRecord(c->ev_fork, s);
     cudaStreamWaitEvent(c->side, c->ev_fork, 0);
-    launch_igf(b, nullptr, c->side);
-    launch_green_transform(b, c->side);
+    enqueue_green(c, c->side);
     cudaEventRecord(c->ev_join, c->side);
     launch_deposit(b, s);
     if (shard)  // the charge of all shards: exact integer node sums
@@ -547,14 +556,6 @@ int stage_check(scgpu_ctx* c, cudaStream_t s, const char* name) {
         if (rc_) return rc_;                         \
     } while (0)
 
-// the solve shared by compute_potential and compute_self_fields
-void enqueue_green(scgpu_ctx* c, cudaStream_t s) {
-    launch_igf(c->b, nullptr, s);
-    if (c->b.periodic_z)
-        launch_green_transform_periodic(c->b, s);
-    else
-        launch_green_transform(c->b, s);
-}
 
 }  // namespace
 
@@ -590,6 +591,8 @@ int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
     b.bc.n[1] = p->my;
     b.bc.n[2] = p->mt;
     b.bc.dh = p->bboxincr / 100.0;
+    b.bc.pz = 0;
+    b.bc.period = kC / 1e9;  // periodLength_m's default (PartBunchBase.hpp:132)
     const long long n0 = p->mx, n1 = p->my, n2 = p->mt;
     const long long M = n0 * n1 * n2;
     int bits = 0;
@@ -892,6 +895,21 @@ int scgpu_set_exchange(scgpu_ctx* c, scgpu_exchange_fn fn, void* user, long long
     return SCGPU_OK;
 }
 
+// setBeamFrequency (PartBunchBase.hpp:2535-2537, from the BEAM's FREQUENCY,
+// TrackRun.cpp:496): the period length c / f of a DC beam.
+int scgpu_set_beam_frequency(scgpu_ctx* c, double f_hz) {
+    if (!c) return SCGPU_ERR_ARG;
+    if (!(f_hz > 0.0) || !std::isfinite(f_hz)) return fail(c, SCGPU_ERR_ARG, "the beam frequency must be positive and finite");
+    const double period = kC / f_hz;
+    if (!std::isfinite(period) || !(period > 0.0)) return fail(c, SCGPU_ERR_ARG, "period length out of range");
+    if (period == c->b.bc.period) return SCGPU_OK;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);  // the step graphs hold the bunch constants
+    c->b.bc.period = period;
+    return SCGPU_OK;
+}
+
 // Interval of the cell reorder in scgpu_track (0: never); the step graphs
 // are keyed by whether a step reorders, so no graph is rebuilt.
 int scgpu_set_reorder_interval(scgpu_ctx* c, int steps) {
@@ -902,7 +920,10 @@ int scgpu_set_reorder_interval(scgpu_ctx* c, int steps) {
 
 // BCFFTZ=PERIODIC (FieldSolver.cpp:431, :486; FFTPoissonSolver.cpp:60,
 // :130-155, :189-190, :661-662): the solves of this context use a grid
-// doubled in x and y only and a cyclic convolution along z.
+// doubled in x and y only and a cyclic convolution along z.  The resident
+// bunch becomes a DC beam, as TrackRun selects setBCForDCBeam for a solver
+// with periodic z (TrackRun.cpp:899-902; PartBunch.cpp:1079-1098): boundp's
+// mesh spans one period along z and the particles wrap at the mesh's ends.
 int scgpu_set_periodic_z(scgpu_ctx* c, int periodic) {
     if (!c) return SCGPU_ERR_ARG;
     DevBunch& b = c->b;
@@ -922,6 +943,7 @@ int scgpu_set_periodic_z(scgpu_ctx* c, int periodic) {
     }
     drop_graphs(c);
     b.periodic_z = on;
+    b.bc.pz = on;
     upload_twiddles(b, c->stream);
     CK(cudaGetLastError());
     c->have_solve = false;
@@ -1188,8 +1210,6 @@ int scgpu_bunch_download(scgpu_ctx* c, double* R, double* P) {
 int scgpu_track(scgpu_ctx* c, int nsteps, double* stats) {
     if (!c || nsteps < 0) return fail(c, SCGPU_ERR_ARG, "bad argument");
     if (!c->have_bunch) return fail(c, SCGPU_ERR_STATE, "no bunch on the device");
-    if (c->b.periodic_z)
-        return fail(c, SCGPU_ERR_UNSUPPORTED, "tracking a DC beam (periodic z needs the periodic particle boundary)");
     CK(cudaSetDevice(c->device));
     const bool want = stats != nullptr;
     cudaStream_t s = c->stream;

@@ -128,13 +128,14 @@ struct BunchConst {
     long long N;    // particles (of this rank when the bunch is sharded)
     long long Ntot; // particles of the whole bunch (the N of the means)
     int sharded;    // 1: bounds and particle sums are combined over ranks between kernels
-    int pad_;
+    int pz;         // 1: DC beam (periodic z: the period's mesh, the periodic particle boundary)
     double dT;
     double mass;    // eV
     double charge;  // e
     double coupling;
     double bz_ext;
     double dh;
+    double period;  // DC beam: period length along z [m] (periodLength_m, c / beam frequency)
     // per-bunch constants of the pusher, evaluated in the reference's order
     double s_cdt;   // c * dT                      (PartBunchBase.hpp:481)
     double rs_cdt;  // RN(1 / (c * dT))
@@ -458,9 +459,11 @@ SC_HD double div_rcp_nc(double a, double b, double rb, bool& fast) {
 // ---------------------------------------------------------------- CIC
 // Lower grid point and normalised offset of a particle (IntCIC.h:818-858 with
 // getVertexBelow, UniformCartesian.hpp:1025-1039, and getCellPosition,
-// :1084-1097).  Returns false when a stencil point would leave the n^3 field.
+// :1084-1097).  Returns false when a stencil point would leave the n^3 field;
+// with pz (a DC beam) the z stencil may also reach the guard planes -1 and n
+// (lower points -1 .. n-1).
 SC_HD bool cic_locate(const double* hr, const double* origin, const int* n, const double* x, int* lgp,
-                      double* dpos) {
+                      double* dpos, int pz = 0) {
     bool ok = true;
     for (int d = 0; d < 3; ++d) {
         int i = (int)((x[d] - origin[d]) / hr[d]);
@@ -474,13 +477,14 @@ SC_HD bool cic_locate(const double* hr, const double* origin, const int* n, cons
         }
         double dp = x[d] - gpos;
         dp /= delta;
-        if (l < 0) {
+        const int g = d == 2 ? pz : 0;
+        if (l < -g) {
             ok = false;
-            l = 0;
+            l = -g;
         }
-        if (l > n[d] - 2) {
+        if (l > n[d] - 2 + g) {
             ok = false;
-            l = n[d] - 2;
+            l = n[d] - 2 + g;
         }
         lgp[d] = l;
         dpos[d] = dp;
@@ -490,7 +494,7 @@ SC_HD bool cic_locate(const double* hr, const double* origin, const int* n, cons
 
 // cic_locate with the reciprocals rhr[d] = RN(1 / hr[d]): same results.
 SC_HD bool cic_locate_r(const double* hr, const double* rhr, const double* origin, const int* n, const double* x,
-                        int* lgp, double* dpos) {
+                        int* lgp, double* dpos, int pz = 0) {
     bool ok = true, fast = true;
     for (int d = 0; d < 3; ++d) {
         int i = (int)div_rcp_nc(x[d] - origin[d], hr[d], rhr[d], fast);
@@ -504,19 +508,31 @@ SC_HD bool cic_locate_r(const double* hr, const double* rhr, const double* origi
         }
         double dp = x[d] - gpos;
         dp = div_rcp_nc(dp, delta, rhr[d], fast);
-        if (l < 0) {
+        const int g = d == 2 ? pz : 0;
+        if (l < -g) {
             ok = false;
-            l = 0;
+            l = -g;
         }
-        if (l > n[d] - 2) {
+        if (l > n[d] - 2 + g) {
             ok = false;
-            l = n[d] - 2;
+            l = n[d] - 2 + g;
         }
         lgp[d] = l;
         dpos[d] = dp;
     }
-    if (!fast) return cic_locate(hr, origin, n, x, lgp, dpos);
+    if (!fast) return cic_locate(hr, origin, n, x, lgp, dpos, pz);
     return ok;
+}
+
+// The periodic particle boundary of a DC beam along z (ParticlePeriodicBCond,
+// ParticleBConds.h:37-45), applied once by boundp's update() over the
+// particle layout's domain, which follows the mesh: [origin, origin + h n)
+// (RegionLayout::Repartition and getMeshDomain, RegionLayout.hpp:773-789,
+// :871-896; ParticleSpatialLayout.hpp:296-297).
+SC_HD double wrap_z(double t, double lo, double hi) {
+    if (t < lo) return hi - (lo - t);
+    if (t >= hi) return lo + (t - hi);
+    return t;
 }
 
 // push_one with s = c dt and rs = RN(1/s) precomputed: same results.
@@ -569,7 +585,16 @@ SC_HD void kick_r(double* P, const double* Ef, const double* Bf, double ke, doub
 SC_HD_COLD bool derive_mesh(StepState& s, const BunchConst& bc) {
     double rmin[3] = {s.bmin[0], s.bmin[1], s.bmin[2]};
     double rmax[3] = {s.bmax[0], s.bmax[1], s.bmax[2]};
-    for (int i = 0; i < 3; ++i) {
+    // a DC beam's z spans one period from the lowest particle, not enlarged
+    // (PartBunchBase.hpp:813-814, :840-843)
+    const int dims = bc.pz ? 2 : 3;
+    if (bc.pz) {
+        rmax[2] = rmin[2] + bc.period;
+        s.hr[2] = bc.period / (bc.n[2] - 1);
+        s.mesh_rmin[2] = rmin[2];
+        s.mesh_rmax[2] = rmax[2];
+    }
+    for (int i = 0; i < dims; ++i) {
         double length = rmax[i] - rmin[i];
         if (length < 0) length = -length;
         if (length < 1e-10) {

@@ -453,8 +453,9 @@ __global__ void __launch_bounds__(kThreads) k_cell_keys(BunchConst bc, const dou
             int l[3];
             double d[3];
             const MeshConsts* m = fresh(&ms);
-            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
-            key = (uint32_t)l[0] + (uint32_t)bc.n[0] * ((uint32_t)l[1] + (uint32_t)bc.n[1] * (uint32_t)l[2]);
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d, bc.pz)) bad = true;
+            const int lz = l[2] < 0 ? 0 : l[2];  // a DC beam's guard plane -1 sorts with plane 0
+            key = (uint32_t)l[0] + (uint32_t)bc.n[0] * ((uint32_t)l[1] + (uint32_t)bc.n[1] * (uint32_t)lz);
             keys[i] = key;
         }
         // one atomic per distinct key in the warp; lanes take consecutive ranks
@@ -527,9 +528,17 @@ __device__ __forceinline__ void acc_add(unsigned long long* a, long long v) {
 // With energy bins (BINNED) the key is bin * n^3 + cell: every active bin's
 // charge goes to its own accumulators in the same pass, particles of bins
 // not yet emitted deposit nothing (setBinCharge, PartBunchBase.hpp:722-725).
-template <bool BINNED>
+//
+// A DC beam (PZ) first takes each particle through the periodic boundary
+// along z (boundp's update(), the first use of the step's mesh; a wrapped
+// position is written back) and drops the corner charges that land in the z
+// guard planes -1 and n: the reference's single-rank scatter writes them
+// into the guard layer, which ParticleAttrib::scatter zeroed and
+// accumGuardCells (BareField.hpp:1013-1079) carries only into neighbouring
+// local fields, of which one vnode has none (ParticleAttrib.h:207-221).
+template <bool BINNED, bool PZ = false>
 __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double* __restrict__ x,
-                                             const double* __restrict__ y, const double* __restrict__ z,
+                                             const double* __restrict__ y, double* __restrict__ z,
                                              const int* __restrict__ bin, int nactive, StepState* st,
                                              unsigned long long* __restrict__ acc, VB g) {
     __shared__ MeshConsts ms;
@@ -550,15 +559,24 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
         if constexpr (BINNED) bk = i < bc.N ? bin[i] : -1;
         const bool valid = i < bc.N && (!BINNED || (unsigned)bk < (unsigned)nactive);
         uint32_t key = 0xffffffffu;
+        int lz = 0;  // z of the lower corner plane (DC beam: -1 .. n-1)
         double c[8];
         if (valid) {
             double X[3] = {x[i], y[i], z[i]};
             int l[3];
             double d[3];
             const MeshConsts* m = fresh(&ms);
-            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
+            if constexpr (PZ) {
+                const double w = wrap_z(X[2], m->org[2], m->org[2] + m->hr[2] * (double)bc.n[2]);
+                if (w != X[2]) {
+                    z[i] = w;
+                    X[2] = w;
+                }
+            }
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d, PZ ? 1 : 0)) bad = true;
             cic_charge(d, *fresh(&qdt_s), c);
             key = (uint32_t)(l[0] + nx * l[1] + nxy * l[2]) + (uint32_t)bk * M;
+            lz = l[2];
         } else {
 #pragma unroll
             for (int k = 0; k < 8; ++k) c[k] = 0.0;
@@ -581,7 +599,8 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const int node = (int)key + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
-                acc_add(acc + 2 * (size_t)node, join(t[k].hi, t[k].lo));
+                if (!PZ || (unsigned)(lz + (k >> 2)) < (unsigned)bc.n[2])
+                    acc_add(acc + 2 * (long long)node, join(t[k].hi, t[k].lo));
             }
         }
         while (passes && multi) {
@@ -596,20 +615,21 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const int node = (int)key + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
-                    acc_add(acc + 2 * (size_t)node, s[k]);
+                    if (!PZ || (unsigned)(lz + (k >> 2)) < (unsigned)bc.n[2]) acc_add(acc + 2 * (long long)node, s[k]);
                 }
             }
         }
     }
     if (bad) atomicOr(&st->err, kFlagGuard);
 }
+template <bool PZ>
 __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
-                                                      const double* __restrict__ z, StepState* st,
+                                                      double* __restrict__ z, StepState* st,
                                                       unsigned long long* __restrict__ acc) {
-    deposit_body<false>(bc, x, y, z, nullptr, 0, st, acc, vb_grid());
+    deposit_body<false, PZ>(bc, x, y, z, nullptr, 0, st, acc, vb_grid());
 }
 __global__ void __launch_bounds__(kThreads) k_deposit_bins(BunchConst bc, const double* __restrict__ x,
-                                                           const double* __restrict__ y, const double* __restrict__ z,
+                                                           const double* __restrict__ y, double* __restrict__ z,
                                                            const int* __restrict__ bin, int nactive, StepState* st,
                                                            unsigned long long* __restrict__ acc) {
     deposit_body<true>(bc, x, y, z, bin, nactive, st, acc, vb_grid());
@@ -1072,17 +1092,27 @@ __global__ void __launch_bounds__(kThreads) k_grad(BunchConst bc, const StepStat
 // ------------------------------------------------------------ gather, kick, push
 // CIC gather (IntCIC.h:935-975): the eight weighted corner values added in
 // the reference's order, accumulated as the corners are loaded.
+// The corner planes along z: l and l + 1, or for a DC beam's guard planes
+// their periodic images (PeriodicFace fills the guard layer before the
+// gather, ParticleAttrib.h:297-299): plane -1 is plane n-1, plane n is 0.
+__device__ __forceinline__ void corner_planes(const int* n, int lz, int (&zp)[2]) {
+    zp[0] = lz < 0 ? n[2] - 1 : lz;
+    zp[1] = lz + 1 >= n[2] ? 0 : lz + 1;
+}
+
 template <typename T>
 __device__ __forceinline__ void cic_gather(const T* __restrict__ E4, const int* n, const int* l, const double* d,
                                            double* Ef) {
     const int nx = n[0], nxy = n[0] * n[1];
-    const int b = l[0] + nx * l[1] + nxy * l[2];
+    int zp[2];
+    corner_planes(n, l[2], zp);
+    const int b = l[0] + nx * l[1];
     const double u[3] = {1 - d[0], 1 - d[1], 1 - d[2]};
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int a0 = k & 1, a1 = (k >> 1) & 1, a2 = (k >> 2) & 1;
         const double w = (a0 ? d[0] : u[0]) * (a1 ? d[1] : u[1]) * (a2 ? d[2] : u[2]);
-        const T* p = E4 + 4 * (size_t)(b + a0 + a1 * nx + a2 * nxy);
+        const T* p = E4 + 4 * (size_t)(b + a0 + a1 * nx + zp[a2] * nxy);
         double e0, e1, e2;
         if constexpr (sizeof(T) == sizeof(double)) {
             const double2 a = *reinterpret_cast<const double2*>(p);  // nodes are 32-byte aligned
@@ -1168,7 +1198,7 @@ __device__ __forceinline__ void cross_fma(const double* a, const double* b, doub
 // CIC cell and offset in units of the spacing: u = (x - origin) / h, cell
 // centres at u = l + 1/2; false when the stencil would leave the mesh.
 __device__ __forceinline__ bool cic_locate_fast(const double* rhr, const double* org, const int* n, const double* x,
-                                                int* l, float* d) {
+                                                int* l, float* d, int pz) {
     bool ok = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -1176,13 +1206,14 @@ __device__ __forceinline__ bool cic_locate_fast(const double* rhr, const double*
         const double f = floor(u);
         int li = (int)f;
         float di = (float)(u - f);
-        if (li < 0) {
+        const int g = a == 2 ? pz : 0;  // a DC beam's z guard planes
+        if (li < -g) {
             ok = false;
-            li = 0;
+            li = -g;
         }
-        if (li > n[a] - 2) {
+        if (li > n[a] - 2 + g) {
             ok = false;
-            li = n[a] - 2;
+            li = n[a] - 2 + g;
         }
         l[a] = li;
         d[a] = di;
@@ -1192,14 +1223,16 @@ __device__ __forceinline__ bool cic_locate_fast(const double* rhr, const double*
 __device__ __forceinline__ void cic_gather_f32(const float* __restrict__ E4, const int* n, const int* l, const float* d,
                                                float* Ef) {
     const int nx = n[0], nxy = n[0] * n[1];
-    const int b = l[0] + nx * l[1] + nxy * l[2];
+    int zp[2];
+    corner_planes(n, l[2], zp);
+    const int b = l[0] + nx * l[1];
     const float u[3] = {1.0f - d[0], 1.0f - d[1], 1.0f - d[2]};
     float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int a0 = k & 1, a1 = (k >> 1) & 1, a2 = (k >> 2) & 1;
         const float w = (a0 ? d[0] : u[0]) * (a1 ? d[1] : u[1]) * (a2 ? d[2] : u[2]);
-        const float4 a = __ldg(reinterpret_cast<const float4*>(E4) + (b + a0 + a1 * nx + a2 * nxy));
+        const float4 a = __ldg(reinterpret_cast<const float4*>(E4) + (b + a0 + a1 * nx + zp[a2] * nxy));
         e0 = fmaf(w, a.x, e0);
         e1 = fmaf(w, a.y, e1);
         e2 = fmaf(w, a.z, e2);
@@ -1215,7 +1248,7 @@ __device__ __forceinline__ bool mixed_particle(const BunchConst& bc, const MeshC
                                                double* R, double* P) {
     int l[3];
     float d[3], e[3];
-    const bool ok = cic_locate_fast(m.rhr, m.org, bc.n, R, l, d);
+    const bool ok = cic_locate_fast(m.rhr, m.org, bc.n, R, l, d, bc.pz);
     cic_gather_f32(E4, bc.n, l, d, e);
     const float bc32 = (float)betaC;
     const double Eb[3] = {(double)e[0], (double)e[1], (double)e[2]};
@@ -1301,7 +1334,7 @@ __device__ __forceinline__ void gather_body(const BunchConst& bc, double* __rest
             int l[3];
             double d[3];
             const MeshConsts* m = fresh(&ms);
-            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d)) bad = true;
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, X, l, d, bc.pz)) bad = true;
             double Eb[3], Bb[3];
             if constexpr (BINNED) {
                 cic_gather8(F8, bc.n, l, d, Eb, Bb);
@@ -1712,7 +1745,8 @@ void prime_particle_grids() {
     cudaFuncSetAttribute(k_gather_staged<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
     const void* kernels[] = {(const void*)k_drift_to_beam<true>,
                              (const void*)k_drift_to_beam<false>,
-                             (const void*)k_deposit,
+                             (const void*)k_deposit<false>,
+                             (const void*)k_deposit<true>,
                              (const void*)k_deposit_bins,
                              (const void*)k_gather_kick_push<double, false>,
                              (const void*)k_gather_kick_push<double, true>,
@@ -1744,7 +1778,10 @@ void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s) {
 }
 
 void launch_deposit(const DevBunch& b, cudaStream_t s) {
-    k_deposit<<<wave_grid(k_deposit, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
+    if (b.bc.pz)
+        k_deposit<true><<<wave_grid(k_deposit<true>, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
+    else
+        k_deposit<false><<<wave_grid(k_deposit<false>, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
 }
 
 void launch_assemble_rho(const DevBunch& b, cudaStream_t s) {

@@ -109,6 +109,7 @@ def lib():
         L.scgpu_set_energy_bins.argtypes = [C.c_void_p, _ip, C.c_int, C.c_int]
         L.scgpu_get_bin_gammas.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong)]
         L.scgpu_set_periodic_z.argtypes = [C.c_void_p, C.c_int]
+        L.scgpu_set_beam_frequency.argtypes = [C.c_void_p, C.c_double]
         L.scgpu_set_reorder_interval.argtypes = [C.c_void_p, C.c_int]
         L.scgpu_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
         L.scgpu_set_exchange.argtypes = [C.c_void_p, EXCHANGE_FN, C.c_void_p, C.c_longlong, C.c_int]
@@ -142,7 +143,7 @@ EXPORTED = [
     "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
     "scgpu_set_periodic_z", "scgpu_set_exchange", "scgpu_add_solenoid", "scgpu_clear_elements",
     "scgpu_fieldmap_astra1d", "scgpu_add_rfcavity", "scgpu_fieldmap_astra1d_dynamic", "scgpu_set_reorder_interval",
-    "scgpu_launch_count",
+    "scgpu_launch_count", "scgpu_set_beam_frequency",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
@@ -229,9 +230,15 @@ class Context:
         """Cell reorder every `steps` tracked steps (0: never); results do not change."""
         self._check(lib().scgpu_set_reorder_interval(self.h, int(steps)), "set_reorder_interval")
 
-    # ---- FIELDSOLVER BCFFTZ=PERIODIC
+    # ---- FIELDSOLVER BCFFTZ=PERIODIC: periodic-z solves and a DC beam
     def set_periodic_z(self, periodic=True):
+        """Cyclic convolution along z; the tracked bunch becomes a DC beam
+        (the period's mesh along z, the periodic particle boundary)."""
         self._check(lib().scgpu_set_periodic_z(self.h, 1 if periodic else 0), "set_periodic_z")
+
+    def set_beam_frequency(self, f_hz):
+        """setBeamFrequency: the DC beam's period length c / f."""
+        self._check(lib().scgpu_set_beam_frequency(self.h, float(f_hz)), "set_beam_frequency")
 
     # ---- PoissonSolver::computePotential(rho, hr, zshift): image charge
     def compute_potential_image(self, rho, hr, zshift):
