@@ -1452,7 +1452,7 @@ __global__ void __launch_bounds__(kThreads) k_gather_fields(BunchConst bc, const
         double X[3] = {x[i], y[i], z[i]};
         int l[3];
         double d[3];
-        if (!cic_locate_r(hr, rhr, org, bc.n, X, l, d)) bad = true;
+        if (!cic_locate_r(hr, rhr, org, bc.n, X, l, d, bc.pz)) bad = true;
         double E[3];
         cic_gather(E4, bc.n, l, d, E);
         Ef[3 * i + 0] = E[0];
