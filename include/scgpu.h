@@ -32,6 +32,9 @@
  *   scgpu_set_periodic_z
  *       the bcz argument of FFTPoissonSolver (FieldSolver BCFFTZ, src/Structure/FieldSolver.cpp:431, :486)
  *       with PartBunch::setBCForDCBeam (src/Classic/Algorithms/PartBunch.cpp:1079-1098)
+ *   scgpu_add_multipole
+ *       OpalMultipole::update (src/Elements/OpalMultipole.cpp:127-166) with Multipole::apply
+ *       (src/Classic/AbsBeamline/Multipole.cpp:352-397) in computeExternalFields
  *   scgpu_set_beam_frequency
  *       PartBunchBase::setBeamFrequency (src/Classic/Algorithms/PartBunchBase.hpp:2535-2537)
  *   scgpu_compute_potential_image, scgpu_compute_potential_image_device
@@ -237,6 +240,23 @@ int scgpu_add_rfcavity(scgpu_ctx* ctx, const char* fieldmap_path, double elemedg
                        double freq_mhz, double lag_rad);
 int scgpu_fieldmap_astra1d_dynamic(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin,
                                    double* zend, double* period, double* frequency_mhz);
+
+/* MULTIPOLE (src/Elements/OpalMultipole.cpp:127-166 attributes L, KN, DKN,
+ * KS, DKS and ELEMEDGE; src/Classic/AbsBeamline/Multipole.cpp): a straight
+ * multipole at ELEMEDGE on the lab z axis with field for 0 <= z - ELEMEDGE
+ * <= L.  kn[0..nkn) and ks[0..nks) are the normal and skew strengths of
+ * orders 1 (dipole) .. 20 [T m^(1-n)], dkn / dks their errors (NULL: none);
+ * each is stored as Multipole::setNormalComponent / setSkewComponent do
+ * (:106-163, the dipole and sextupole halved, octupole and decapole
+ * divided) and the field is Multipole::computeField (:229-349) in its
+ * expression order.  The particles see components plus errors, the
+ * reference particle components alone (applyToReferenceParticle,
+ * :377-397).  OPAL's default aperture, an ellipse of 0.5 m semi-axes,
+ * applies: outside it no field is added (the reference also marks such a
+ * particle lost; particle removal is not part of this library).  At most 8
+ * elements of all kinds. */
+int scgpu_add_multipole(scgpu_ctx* ctx, double elemedge, double length, const double* kn, int nkn, const double* dkn,
+                        const double* ks, int nks, const double* dks);
 
 /* FIELDSOLVER BCFFTZ=PERIODIC (FFTPoissonSolver(..., bcz="PERIODIC"),
  * src/Solvers/FFTPoissonSolver.cpp:60, :130-155, :189-190, :661-662): the

@@ -56,10 +56,11 @@ class Debug(C.Structure):
 
 
 class Solenoid(C.Structure):
-    """A beamline element with a 1D map: kind 0 SOLENOID, kind 1 RFCAVITY."""
+    """A beamline element: kind 0 SOLENOID, kind 1 RFCAVITY (1D maps), kind 2 MULTIPOLE."""
     _fields_ = [("edge", C.c_double), ("scale", C.c_double), ("zbegin", C.c_double), ("range", C.c_double),
                 ("period", C.c_double), ("accuracy", C.c_int), ("kind", C.c_int), ("omega", C.c_double),
-                ("phase", C.c_double), ("xlrep", C.c_double), ("coefs", C.c_double * 255)]
+                ("phase", C.c_double), ("xlrep", C.c_double), ("nskew", C.c_int), ("pad_", C.c_int),
+                ("aperture", C.c_double * 2), ("coefs", C.c_double * 255)]
 
 
 class BeamParams(C.Structure):
@@ -246,6 +247,39 @@ def make_rfcavity(coefs, zbegin, zend, period, freq_map_mhz, edge, volt, freq_mh
         omega = omega_map
     e.kind, e.omega, e.phase, e.xlrep = 1, omega, lag, omega_map / c_light()
     return e
+
+
+def make_multipole(elemedge, length, kn=(), dkn=None, ks=(), dks=None, aperture=(0.5, 0.5)):
+    """MULTIPOLE (OpalMultipole::update, OpalMultipole.cpp:127-166): the
+    components stored as Multipole::setNormalComponent / setSkewComponent do."""
+    e = Solenoid()
+    e.kind, e.edge, e.range = 2, elemedge, length
+    nn, ns = len(kn), len(ks)
+    e.accuracy, e.nskew = nn, ns
+    e.aperture[0], e.aperture[1] = aperture
+    L = lib()
+    L.sco_multipole_component.restype = C.c_double
+    err = C.c_double()
+    for i in range(nn):
+        v = L.sco_multipole_component(C.c_int(i + 1), C.c_int(0), C.c_double(kn[i]),
+                                      C.c_double(0.0 if dkn is None else dkn[i]), C.byref(err))
+        e.coefs[i], e.coefs[nn + i] = v, err.value
+    for i in range(ns):
+        v = L.sco_multipole_component(C.c_int(i + 1), C.c_int(1), C.c_double(ks[i]),
+                                      C.c_double(0.0 if dks is None else dks[i]), C.byref(err))
+        e.coefs[2 * nn + i], e.coefs[2 * nn + ns + i] = v, err.value
+    return e
+
+
+def multipole_field(element, R, ref_particle=False):
+    """B [T] of one MULTIPOLE at points R (n x 3, element frame)."""
+    R = _f64(R)
+    out = np.zeros_like(R)
+    for i in range(R.shape[0]):
+        b = (C.c_double * 3)()
+        lib().sco_multipole_field(C.byref(element), R[i].ctypes.data_as(_dp), C.c_int(1 if ref_particle else 0), b)
+        out[i] = list(b)
+    return out
 
 
 def rfcavity_field(element, R, t):

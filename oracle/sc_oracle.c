@@ -1556,12 +1556,122 @@ void sco_rfcavity_field(const sco_solenoid* e, const double* R, double t, double
     }
 }
 
+/* Multipole::setNormalComponent / setSkewComponent (Multipole.cpp:106-163):
+ * order n (1 = dipole): dipole and sextupole halved, the normal octupole and
+ * decapole over 24, the skew octupole over 6 and decapole over 24, the
+ * others as given; the dipole's stored error is its whole value. */
+double sco_multipole_component(int n, int skew, double v, double verr, double* err) {
+    double c, e;
+    switch (n - 1) {
+    case 0: c = (v + verr) / 2; e = c; break;
+    case 2: c = (v + verr) / 2; e = verr / 2; break;
+    case 3:
+        if (skew) { c = (v + verr) / 6; e = verr / 6; }
+        else { c = (v + verr) / 24; e = verr / 24; }
+        break;
+    case 4: c = (v + verr) / 24; e = verr / 24; break;
+    default: c = (v + verr); e = verr;
+    }
+    if (err) *err = e;
+    return c;
+}
+
+/* Multipole::computeField for one kind of components k[0..m), added to B
+ * (Multipole.cpp:229-290 normal, :292-349 skew) */
+static void multipole_terms(const double* k, int m, int skew, const double* R, double* B) {
+    double Rn[SCO_MAX_MULTIPOLE + 1][2], fact[SCO_MAX_MULTIPOLE + 1];
+    Rn[0][0] = 1.0;
+    Rn[0][1] = 1.0;
+    fact[0] = 1;
+    for (int i = 0; i < m; ++i) {
+        if (!skew) {
+            if (i == 0) {
+                B[1] += k[i];
+            } else if (i == 1) {
+                B[0] += k[i] * R[1];
+                B[1] += k[i] * R[0];
+            } else if (i == 2) {
+                B[0] += 2 * k[i] * R[0] * R[1];
+                B[1] += k[i] * (Rn[2][0] - Rn[2][1]);
+            } else if (i == 3) {
+                B[0] += k[i] * (3 * Rn[2][0] * Rn[1][1] - Rn[3][1]);
+                B[1] += k[i] * (Rn[3][0] - 3 * Rn[1][0] * Rn[2][1]);
+            } else if (i == 4) {
+                B[0] += 4 * k[i] * (Rn[3][0] * Rn[1][1] - Rn[1][0] * Rn[3][1]);
+                B[1] += k[i] * (Rn[4][0] - 6 * Rn[2][0] * Rn[2][1] + Rn[4][1]);
+            } else {
+                double sgn = 1, Bx = 0.0, By = 0.0;
+                for (int j = 1; j <= (i + 1) / 2; ++j) {
+                    Bx += sgn * k[i] * (Rn[i - 2 * j + 1][0] * fact[i - 2 * j + 1] * Rn[2 * j - 1][1] * fact[2 * j - 1]);
+                    By += sgn * k[i] * (Rn[i - 2 * j + 2][0] * fact[i - 2 * j + 2] * Rn[2 * j - 2][1] * fact[2 * j - 2]);
+                    sgn *= -1;
+                }
+                if ((i + 1) / 2 == i / 2) {
+                    const int j = (i + 2) / 2;
+                    By += sgn * k[i] * (Rn[i - 2 * j + 2][0] * fact[i - 2 * j + 2] * Rn[2 * j - 2][1] * fact[2 * j - 2]);
+                }
+                B[0] += Bx;
+                B[1] += By;
+            }
+        } else {
+            if (i == 0) {
+                B[0] -= k[i];
+            } else if (i == 1) {
+                B[0] -= k[i] * R[0];
+                B[1] += k[i] * R[1];
+            } else if (i == 2) {
+                B[0] -= k[i] * (Rn[2][0] - Rn[2][1]);
+                B[1] += 2 * k[i] * R[0] * R[1];
+            } else if (i == 3) {
+                B[0] -= k[i] * (Rn[3][0] - 3 * Rn[1][0] * Rn[2][1]);
+                B[1] += k[i] * (3 * Rn[2][0] * Rn[1][1] - Rn[3][1]);
+            } else if (i == 4) {
+                B[0] -= k[i] * (Rn[4][0] - 6 * Rn[2][0] * Rn[2][1] + Rn[4][1]);
+                B[1] += 4 * k[i] * (Rn[3][0] * Rn[1][1] - Rn[1][0] * Rn[3][1]);
+            } else {
+                double sgn = 1, Bx = 0, By = 0;
+                for (int j = 1; j <= (i + 1) / 2; ++j) {
+                    Bx -= sgn * k[i] * (Rn[i - 2 * j + 2][0] * fact[i - 2 * j + 2] * Rn[2 * j - 2][1] * fact[2 * j - 2]);
+                    By += sgn * k[i] * (Rn[i - 2 * j + 1][0] * fact[i - 2 * j + 1] * Rn[2 * j - 1][1] * fact[2 * j - 1]);
+                    sgn *= -1;
+                }
+                if ((i + 1) / 2 == i / 2) {
+                    const int j = (i + 2) / 2;
+                    Bx -= sgn * k[i] * (Rn[i - 2 * j + 2][0] * fact[i - 2 * j + 2] * Rn[2 * j - 2][1] * fact[2 * j - 2]);
+                }
+                B[0] += Bx;
+                B[1] += By;
+            }
+        }
+        Rn[i + 1][0] = Rn[i][0] * R[0];
+        Rn[i + 1][1] = Rn[i][1] * R[1];
+        fact[i + 1] = fact[i] / (i + 1);
+    }
+}
+
+/* Multipole::apply (:352-366): nothing outside 0 <= z <= L; nothing outside
+ * the aperture (ElementBase::isInsideTransverse, ELLIPTICAL; the reference
+ * also marks such a particle lost) */
+void sco_multipole_field(const sco_solenoid* e, const double* R, int ref_particle, double* B) {
+    if (R[2] < 0.0 || R[2] > e->range) return;
+    if (!(pow(R[0] / e->aperture[0], 2) + pow(R[1] / e->aperture[1], 2) < 1.0)) return;
+    const int nn = e->accuracy, ns = e->nskew;
+    double k[SCO_MAX_MULTIPOLE];
+    for (int i = 0; i < nn; ++i) k[i] = ref_particle ? e->coefs[i] - e->coefs[nn + i] : e->coefs[i];
+    multipole_terms(k, nn, 0, R, B);
+    for (int i = 0; i < ns; ++i) k[i] = ref_particle ? e->coefs[2 * nn + i] - e->coefs[2 * nn + ns + i] : e->coefs[2 * nn + i];
+    multipole_terms(k, ns, 1, R, B);
+}
+
 /* one element's E (RF cavities) and B at R (element frame), time t */
-static void element_field(const sco_solenoid* e, const double* R, double t, double* E, double* B) {
+static void element_field(const sco_solenoid* e, const double* R, double t, int ref_particle, double* E, double* B) {
     E[0] = E[1] = E[2] = 0.0;
     if (e->kind == 1) {
         B[0] = B[1] = B[2] = 0.0;
         sco_rfcavity_field(e, R, t, E, B);
+    } else if (e->kind == 2) {
+        B[0] = B[1] = B[2] = 0.0;
+        sco_multipole_field(e, R, ref_particle, B);
     } else {
         sco_solenoid_field(e, R, B);
     }
@@ -1591,7 +1701,7 @@ static void add_element_fields(const sco_trafo* ref_to_lab, long long n, const d
         for (long long i = 0; i < n; ++i) {
             double loc[3], El[3], Bl[3], Er[3], Br[3];
             trafo_transform_to(&r2loc, R + 3 * i, loc);
-            element_field(&g_sol[k], loc, t, El, Bl);
+            element_field(&g_sol[k], loc, t, 0, El, Bl);
             trafo_rotate_to(&loc2r, Bl, Br);
             Bf[3 * i + 0] += Br[0];
             Bf[3 * i + 1] += Br[1];
@@ -1615,7 +1725,7 @@ static void add_element_fields_ref(const sco_trafo* ref_to_lab, const double* R,
         sco_trafo_compose(&r2loc, ref_to_lab);
         double loc[3], El[3], Bl[3];
         trafo_transform_to(&r2loc, R, loc);
-        element_field(&g_sol[k], loc, t, El, Bl);
+        element_field(&g_sol[k], loc, t, 1, El, Bl);
         const double* M = r2loc.M;
         Bf[0] += M[0] * Bl[0] + M[3] * Bl[1] + M[6] * Bl[2];
         Bf[1] += M[1] * Bl[0] + M[4] * Bl[1] + M[7] * Bl[2];

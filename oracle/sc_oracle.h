@@ -146,16 +146,28 @@ int sco_compute_self_fields(const sco_params* prm, double* Q, long long n, doubl
  * 232-270, Astra1DDynamic.cpp:192-229): the tracker adds their fields
  * (computeExternalFields, ParallelTTracker.cpp:614-643) */
 #define SCO_MAX_ELEMENTS 8
+#define SCO_MAX_MULTIPOLE 20
 typedef struct {
     double edge, scale, zbegin, range, period;
-    int accuracy;
+    int accuracy;   /* map harmonics; MULTIPOLE (kind 2): normal components */
     int kind;
     double omega, phase, xlrep; /* RF: angular frequency, LAG, map's omega / c */
-    double coefs[255];
+    int nskew;      /* MULTIPOLE: skew components */
+    int pad_;
+    double aperture[2]; /* MULTIPOLE: elliptical aperture semi-axes [m] */
+    double coefs[255];  /* map coefficients; MULTIPOLE: normal, normal errors, skew, skew errors */
 } sco_solenoid;
 int sco_set_solenoids(const sco_solenoid* s, int n);
 void sco_solenoid_field(const sco_solenoid* e, const double* R, double* B);
 void sco_rfcavity_field(const sco_solenoid* e, const double* R, double t, double* E, double* B);
+/* MULTIPOLE (kind 2; Multipole.cpp:106-163 component scaling, :229-349
+ * computeField, :352-397 apply / applyToReferenceParticle): B at R (element
+ * frame) added to B; ref_particle: components less their errors. */
+void sco_multipole_field(const sco_solenoid* e, const double* R, int ref_particle, double* B);
+/* Multipole::setNormalComponent / setSkewComponent (Multipole.cpp:106-163):
+ * the stored component of order n (1 = dipole) from KN (or KS) and its error;
+ * *err receives the stored error. */
+double sco_multipole_component(int n, int skew, double v, double verr, double* err);
 
 /* periodic z, BCFFTZ=PERIODIC (FFTPoissonSolver.cpp:60, :130-155, :661-662) */
 void sco_igf_periodic_z(const int* nr, const double* hr, double* G2);

@@ -869,6 +869,69 @@ int scgpu_add_rfcavity(scgpu_ctx* c, const char* fieldmap, double elemedge, doub
     return upload_elements(c);
 }
 
+// Multipole::setNormalComponent / setSkewComponent (Multipole.cpp:106-163):
+// the stored component of order n (1 = dipole) from KN or KS and its error,
+// and the stored error.
+static double multipole_component(int n, bool skew, double v, double verr, double* err) {
+    double c, e;
+    switch (n - 1) {
+        case 0:  // dipole
+            c = (v + verr) / 2;
+            e = c;
+            break;
+        case 2:  // sextupole
+            c = (v + verr) / 2;
+            e = verr / 2;
+            break;
+        case 3:  // octupole
+            c = skew ? (v + verr) / 6 : (v + verr) / 24;
+            e = skew ? verr / 6 : verr / 24;
+            break;
+        case 4:  // decapole
+            c = (v + verr) / 24;
+            e = verr / 24;
+            break;
+        default:
+            c = v + verr;
+            e = verr;
+    }
+    *err = e;
+    return c;
+}
+
+// MULTIPOLE (OpalMultipole::update, OpalMultipole.cpp:127-166: L, KN, DKN,
+// KS, DKS; the errors padded with zeros to the components' count).
+int scgpu_add_multipole(scgpu_ctx* c, double elemedge, double length, const double* kn, int nkn, const double* dkn,
+                        const double* ks, int nks, const double* dks) {
+    if (!c) return SCGPU_ERR_ARG;
+    if (nkn < 0 || nks < 0 || nkn > kMaxMultipoleOrder || nks > kMaxMultipoleOrder || (nkn > 0 && !kn) ||
+        (nks > 0 && !ks))
+        return fail(c, SCGPU_ERR_ARG, "KN and KS hold 0 .. 20 components");
+    if (!std::isfinite(elemedge) || !(length >= 0.0) || !std::isfinite(length))
+        return fail(c, SCGPU_ERR_ARG, "ELEMEDGE must be finite and L finite and not negative");
+    for (int i = 0; i < nkn; ++i)
+        if (!std::isfinite(kn[i]) || (dkn && !std::isfinite(dkn[i]))) return fail(c, SCGPU_ERR_ARG, "KN, DKN must be finite");
+    for (int i = 0; i < nks; ++i)
+        if (!std::isfinite(ks[i]) || (dks && !std::isfinite(dks[i]))) return fail(c, SCGPU_ERR_ARG, "KS, DKS must be finite");
+    if ((int)c->elements.size() >= kMaxElements) return fail(c, SCGPU_ERR_UNSUPPORTED, "at most 8 elements");
+    MapElem e{};
+    e.kind = kElemMultipole;
+    e.edge = elemedge;
+    e.range = length;
+    e.accuracy = nkn;
+    e.nskew = nks;
+    e.aperture[0] = 0.5;  // OpalElement::getApert's default: ELLIPTICAL(0.5, 0.5)
+    e.aperture[1] = 0.5;
+    for (int i = 0; i < nkn; ++i)
+        e.coefs[i] = multipole_component(i + 1, false, kn[i], dkn ? dkn[i] : 0.0, &e.coefs[nkn + i]);
+    for (int i = 0; i < nks; ++i)
+        e.coefs[2 * nkn + i] = multipole_component(i + 1, true, ks[i], dks ? dks[i] : 0.0, &e.coefs[2 * nkn + nks + i]);
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    c->elements.push_back(e);
+    return upload_elements(c);
+}
+
 int scgpu_clear_elements(scgpu_ctx* c) {
     if (!c) return SCGPU_ERR_ARG;
     CK(cudaSetDevice(c->device));

@@ -107,18 +107,24 @@ struct StepState {
 //    cos(omega t + LAG) (E) and sin(omega t + LAG) (B).
 constexpr int kMaxSolCoefs = 255;  // 2 accuracy - 1, accuracy <= 128
 constexpr int kMaxElements = 8;
-enum : int { kElemSolenoid = 0, kElemRfCavity = 1 };
+constexpr int kMaxMultipoleOrder = 20;  // components per kind (normal, skew) of a MULTIPOLE
+enum : int { kElemSolenoid = 0, kElemRfCavity = 1, kElemMultipole = 2 };
 struct MapElem {
     double edge;    // ELEMEDGE: the element origin on the lab z axis [m]
     double scale;   // KS [T] or VOLT [MV/m] (the map is normalised to 1 T, or to 1 MV/m in V/m)
     double zbegin;  // startField: the map's first z (element frame)
     double range;   // zend - zbegin: the field region (the element's length)
     double period;  // 2 N (zend - zbegin) / (N - 1): the Fourier period
-    int accuracy;   // harmonics 0 .. accuracy - 1
-    int kind;       // kElemSolenoid or kElemRfCavity
+    int accuracy;   // harmonics 0 .. accuracy - 1; MULTIPOLE: normal components
+    int kind;       // kElemSolenoid, kElemRfCavity or kElemMultipole
     double omega;   // RF: angular frequency [rad/s]
     double phase;   // RF: LAG [rad]
     double xlrep;   // RF: the map's angular frequency / c [1/m]
+    int nskew;      // MULTIPOLE: skew components
+    int pad_;
+    double aperture[2];  // MULTIPOLE: semi-axes of the elliptical aperture [m]
+    // map: Fourier coefficients; MULTIPOLE: normal components, their errors,
+    // skew components, their errors (accuracy, accuracy, nskew, nskew values)
     double coefs[kMaxSolCoefs];
 };
 
@@ -364,12 +370,121 @@ SC_HD void rfcavity_field(const MapElem& e, const double* R, double t, double* E
     B[2] -= sb * tB[2];
 }
 
+// Multipole::computeField (Multipole.cpp:229-349): the normal components
+// c[0..nn), then the skew components s[0..ns), each order's term added to
+// B_x, B_y in the reference's expression order (special forms for the
+// dipole .. decapole, the general series with the inverse factorials beyond).
+SC_HD void multipole_terms(const double* c, int nn, bool skew, const double* R, double* B) {
+    double Rn0[kMaxMultipoleOrder + 1], Rn1[kMaxMultipoleOrder + 1], fact[kMaxMultipoleOrder + 1];
+    Rn0[0] = 1.0;
+    Rn1[0] = 1.0;
+    fact[0] = 1;
+    for (int i = 0; i < nn; ++i) {
+        const double k = c[i];
+        if (!skew) {
+            switch (i) {
+                case 0:
+                    B[1] += k;
+                    break;
+                case 1:
+                    B[0] += k * R[1];
+                    B[1] += k * R[0];
+                    break;
+                case 2:
+                    B[0] += 2 * k * R[0] * R[1];
+                    B[1] += k * (Rn0[2] - Rn1[2]);
+                    break;
+                case 3:
+                    B[0] += k * (3 * Rn0[2] * Rn1[1] - Rn1[3]);
+                    B[1] += k * (Rn0[3] - 3 * Rn0[1] * Rn1[2]);
+                    break;
+                case 4:
+                    B[0] += 4 * k * (Rn0[3] * Rn1[1] - Rn0[1] * Rn1[3]);
+                    B[1] += k * (Rn0[4] - 6 * Rn0[2] * Rn1[2] + Rn1[4]);
+                    break;
+                default: {
+                    double pm = 1, Bx = 0.0, By = 0.0;
+                    for (int j = 1; j <= (i + 1) / 2; ++j) {
+                        Bx += pm * k * (Rn0[i - 2 * j + 1] * fact[i - 2 * j + 1] * Rn1[2 * j - 1] * fact[2 * j - 1]);
+                        By += pm * k * (Rn0[i - 2 * j + 2] * fact[i - 2 * j + 2] * Rn1[2 * j - 2] * fact[2 * j - 2]);
+                        pm *= -1;
+                    }
+                    if ((i + 1) / 2 == i / 2) {
+                        const int j = (i + 2) / 2;
+                        By += pm * k * (Rn0[i - 2 * j + 2] * fact[i - 2 * j + 2] * Rn1[2 * j - 2] * fact[2 * j - 2]);
+                    }
+                    B[0] += Bx;
+                    B[1] += By;
+                }
+            }
+        } else {
+            switch (i) {
+                case 0:
+                    B[0] -= k;
+                    break;
+                case 1:
+                    B[0] -= k * R[0];
+                    B[1] += k * R[1];
+                    break;
+                case 2:
+                    B[0] -= k * (Rn0[2] - Rn1[2]);
+                    B[1] += 2 * k * R[0] * R[1];
+                    break;
+                case 3:
+                    B[0] -= k * (Rn0[3] - 3 * Rn0[1] * Rn1[2]);
+                    B[1] += k * (3 * Rn0[2] * Rn1[1] - Rn1[3]);
+                    break;
+                case 4:
+                    B[0] -= k * (Rn0[4] - 6 * Rn0[2] * Rn1[2] + Rn1[4]);
+                    B[1] += 4 * k * (Rn0[3] * Rn1[1] - Rn0[1] * Rn1[3]);
+                    break;
+                default: {
+                    double pm = 1, Bx = 0, By = 0;
+                    for (int j = 1; j <= (i + 1) / 2; ++j) {
+                        Bx -= pm * k * (Rn0[i - 2 * j + 2] * fact[i - 2 * j + 2] * Rn1[2 * j - 2] * fact[2 * j - 2]);
+                        By += pm * k * (Rn0[i - 2 * j + 1] * fact[i - 2 * j + 1] * Rn1[2 * j - 1] * fact[2 * j - 1]);
+                        pm *= -1;
+                    }
+                    if ((i + 1) / 2 == i / 2) {
+                        const int j = (i + 2) / 2;
+                        Bx -= pm * k * (Rn0[i - 2 * j + 2] * fact[i - 2 * j + 2] * Rn1[2 * j - 2] * fact[2 * j - 2]);
+                    }
+                    B[0] += Bx;
+                    B[1] += By;
+                }
+            }
+        }
+        Rn0[i + 1] = Rn0[i] * R[0];
+        Rn1[i + 1] = Rn1[i] * R[1];
+        fact[i + 1] = fact[i] / (i + 1);
+    }
+}
+
+// Multipole::apply (Multipole.cpp:352-366) for R in the element frame: a
+// field only for 0 <= z <= L and inside the elliptical aperture
+// (ElementBase::isInsideTransverse, ElementBase.h:627-640; OPAL's default
+// 0.5 m x 0.5 m, OpalElement.cpp:225-226); the reference particle's field
+// (applyToReferenceParticle :377-397) with every component less its error.
+SC_HD void multipole_field(const MapElem& e, const double* R, bool ref_particle, double* B) {
+    if (R[2] < 0.0 || R[2] > e.range) return;
+    const double ax = R[0] / e.aperture[0], ay = R[1] / e.aperture[1];
+    if (!(ax * ax + ay * ay < 1.0)) return;
+    const int nn = e.accuracy, ns = e.nskew;
+    double c[kMaxMultipoleOrder];
+    for (int i = 0; i < nn; ++i) c[i] = ref_particle ? e.coefs[i] - e.coefs[nn + i] : e.coefs[i];
+    multipole_terms(c, nn, false, R, B);
+    for (int i = 0; i < ns; ++i)
+        c[i] = ref_particle ? e.coefs[2 * nn + i] - e.coefs[2 * nn + ns + i] : e.coefs[2 * nn + i];
+    multipole_terms(c, ns, true, R, B);
+}
+
 // computeExternalFields (ParallelTTracker.cpp:614-643) for the elements of
 // the table at time t: R in the reference frame -> lab (ref_to_lab) ->
 // element frame (minus ELEMEDGE along z); each element's E and B rotated
-// back and added to Ef, Bf.
+// back and added to Ef, Bf.  ref_particle: the reference particle's fields
+// (updateReferenceParticle, :1134-1155).
 SC_HD void add_external_fields(const MapElem* el, int n, const Trafo& ref_to_lab, const double* R, double t, double* Ef,
-                               double* Bf) {
+                               double* Bf, bool ref_particle = false) {
     for (int k = 0; k < n; ++k) {
         double lab[3], loc[3], El[3] = {0.0, 0.0, 0.0}, Bl[3] = {0.0, 0.0, 0.0}, Er[3], Br[3];
         trafo_transform_to(ref_to_lab, R, lab);
@@ -382,6 +497,8 @@ SC_HD void add_external_fields(const MapElem* el, int n, const Trafo& ref_to_lab
             Ef[0] += Er[0];
             Ef[1] += Er[1];
             Ef[2] += Er[2];
+        } else if (el[k].kind == kElemMultipole) {
+            multipole_field(el[k], loc, ref_particle, Bl);
         } else {
             solenoid_field(el[k], loc, Bl);
         }
@@ -671,7 +788,7 @@ SC_HD bool advance_reference(StepState& s, const BunchConst& bc) {
             // updateReferenceParticle (ParallelTTracker.cpp:1134-1155): the
             // elements' fields at the reference particle at t - dt / 2, then
             // the kick
-            add_external_fields(bc.sol, bc.nsol, s.ref_to_lab, rr, s.t - 0.5 * dt, eref, bref);
+            add_external_fields(bc.sol, bc.nsol, s.ref_to_lab, rr, s.t - 0.5 * dt, eref, bref, true);
             if (bc.bz_ext != 0.0) bref[2] += bc.bz_ext;
             kick_one(rp, eref, bref, dt, bc.mass, bc.charge);
         }

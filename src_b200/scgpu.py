@@ -117,6 +117,7 @@ def lib():
         L.scgpu_clear_elements.argtypes = [C.c_void_p]
         L.scgpu_fieldmap_astra1d.argtypes = [C.c_char_p, _dp, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp]
         L.scgpu_add_rfcavity.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.scgpu_add_multipole.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp, C.c_int, _dp, _dp, C.c_int, _dp]
         L.scgpu_fieldmap_astra1d_dynamic.argtypes = [C.c_char_p, _dp, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
         L.scgpu_stat_row.argtypes = [C.c_void_p, _dp]
         L.scgpu_stat_column_name.argtypes = [C.c_int]
@@ -143,7 +144,7 @@ EXPORTED = [
     "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
     "scgpu_set_periodic_z", "scgpu_set_exchange", "scgpu_add_solenoid", "scgpu_clear_elements",
     "scgpu_fieldmap_astra1d", "scgpu_add_rfcavity", "scgpu_fieldmap_astra1d_dynamic", "scgpu_set_reorder_interval",
-    "scgpu_launch_count", "scgpu_set_beam_frequency",
+    "scgpu_launch_count", "scgpu_set_beam_frequency", "scgpu_add_multipole",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
@@ -216,6 +217,20 @@ class Context:
         """RFCAVITY with an ASTRA dynamic map at ELEMEDGE [m]: VOLT [MV/m], FREQ [MHz], LAG [rad]."""
         self._check(lib().scgpu_add_rfcavity(self.h, os.fsencode(fieldmap), float(elemedge), float(volt),
                                              float(freq_mhz), float(lag)), "add_rfcavity")
+
+    def add_multipole(self, elemedge, length, kn=(), dkn=None, ks=(), dks=None):
+        """MULTIPOLE at ELEMEDGE [m] of length L [m]: normal / skew strengths
+        KN, KS (order 1 = dipole first) with optional errors DKN, DKS."""
+        def arr(v, n):
+            if v is None:
+                return None
+            a = np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.float64), (n,)))
+            return a
+        kn_a, ks_a = arr(kn, len(kn)), arr(ks, len(ks))
+        dkn_a, dks_a = arr(dkn, len(kn)), arr(dks, len(ks))
+        p = lambda a: _p(a) if a is not None and a.size else None
+        self._check(lib().scgpu_add_multipole(self.h, float(elemedge), float(length), p(kn_a), len(kn), p(dkn_a),
+                                              p(ks_a), len(ks), p(dks_a)), "add_multipole")
 
     def clear_elements(self):
         self._check(lib().scgpu_clear_elements(self.h), "clear_elements")

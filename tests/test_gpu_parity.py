@@ -634,3 +634,57 @@ def test_tracking_with_rfcavity_map_vs_oracle(oracle, gpu, tmp_path):
     np.testing.assert_allclose(st["ref_P"], tr.ref_P, rtol=1e-13, atol=1e-18)
     # the cavity acts: the longitudinal momenta change well beyond the tolerance
     assert rel(Pg[:, 2], Pn[:, 2]) > 1e-4
+
+
+def test_tracking_with_multipole_vs_oracle(oracle, gpu):
+    """MULTIPOLE elements (Multipole::computeField, the component scaling of
+    setNormalComponent / setSkewComponent): a quadrupole with dipole,
+    sextupole, decapole and order-7 terms and errors (the reference particle
+    sees the components less their errors), and a skew element; the bunch
+    starts inside both and crosses the first one's exit.  20 steps against
+    the oracle."""
+    N, nr, steps = 50_000, (32, 32, 32), 20
+    R, P = gaussian_bunch(N, bunch_id=14)
+    Q = -1e-9 / N
+    specs = [dict(elemedge=-0.01, length=0.013, kn=[2e-3, 4.0, 300.0, 0.0, 5e4, 0.0, 2e8], dkn=[1e-4, 0.05, 3.0]),
+             dict(elemedge=-0.02, length=0.05, kn=[], ks=[0.0, 1.5, 0.0, 2e3], dks=[0.0, 0.01])]
+    els = []
+    for sp in specs:
+        dkn = list(sp.get("dkn", [])) + [0.0] * (len(sp.get("kn", [])) - len(sp.get("dkn", [])))
+        dks = list(sp.get("dks", [])) + [0.0] * (len(sp.get("ks", [])) - len(sp.get("dks", [])))
+        els.append((sp, dkn, dks))
+    oracle.set_solenoids([oracle.make_multipole(sp["elemedge"], sp["length"], sp.get("kn", []), dkn,
+                                                sp.get("ks", []), dks) for sp, dkn, dks in els])
+    try:
+        tr = oracle.OracleTracker(oracle.make_params(nr, 1e-12), Q)
+        Ro, Po = R.copy(), P.copy()
+        tr.track(Ro, Po, steps)
+    finally:
+        oracle.set_solenoids([])
+    with gpu.Context(nr) as ctx:
+        for sp, dkn, dks in els:
+            ctx.add_multipole(sp["elemedge"], sp["length"], sp.get("kn", []), dkn or None, sp.get("ks", []),
+                              dks or None)
+        ctx.upload(R, P, 1e-12, Q, oracle.electron_mass_ev())
+        ctx.track(steps)
+        Rg, Pg = ctx.download()
+        st = ctx.tracker_state()
+        ctx.clear_elements()
+        ctx.upload(R, P, 1e-12, Q, oracle.electron_mass_ev())
+        ctx.track(steps)
+        Rn, Pn = ctx.download()
+    assert rel(Rg, Ro) < STATE_TOL and rel(Pg, Po) < STATE_TOL
+    assert st["path_length"] == tr.path_length
+    assert np.array_equal(st["ref_P"], tr.ref_P) and np.array_equal(st["ref_R"], tr.ref_R)
+    assert rel(Pg[:, :2], Pn[:, :2]) > 1e-3  # the elements act
+
+
+def test_multipole_arguments(gpu):
+    with gpu.Context((16, 16, 16)) as ctx:
+        for bad in (dict(kn=[1.0] * 21), dict(kn=[float("nan")]), dict(length=-1.0), dict(elemedge=float("inf"))):
+            args = dict(elemedge=0.0, length=0.1, kn=[1.0])
+            args.update(bad)
+            with pytest.raises(gpu.ScgpuError) as e:
+                ctx.add_multipole(**args)
+            assert e.value.code == -1
+        ctx.add_multipole(0.0, 0.1, kn=[0.0, 1.0], ks=[0.0, 0.5])
