@@ -59,9 +59,15 @@ template <typename C>
 __device__ __forceinline__ C csub(C a, C b) {
     return {a.x - b.x, a.y - b.y};
 }
+// Complex product with its two fused multiply-adds written out.  The file is
+// compiled without FMA contraction (-fmad=false), so every kernel that shares
+// these butterflies rounds identically, whatever the surrounding code: the
+// staged, register-resident and batched transforms give the same bits.
+__device__ __forceinline__ float fmx(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmx(double a, double b, double c) { return fma(a, b, c); }
 template <typename C>
 __device__ __forceinline__ C cmul(C a, C b) {
-    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+    return {fmx(a.x, b.x, -(a.y * b.y)), fmx(a.x, b.y, a.y * b.x)};
 }
 
 // ---------------------------------------------------------------- cp.async
