@@ -580,70 +580,97 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_fft_x_conv(const Cx<TI>* in, 
     fft_x_conv_body<TI, TO, LT, NC, NT, CG>(in, out, ghat, n0, n1, L1, rows, px, twi, two, blockIdx.x);
 }
 
-// ---------------------------------------------------------------- 128-point lines in registers
-// The same Stockham transform of a 128-point line (plan 4, 4, 8: the same
-// butterflies, twiddles and operation order as block_fft, so the same bits),
-// computed by 8 threads of one warp with the data in registers: thread a
-// holds elements a + 8m (m = 0..15).  Those are exactly the inputs of the
-// first stage's butterflies a + 8q (q = 0..3), whose outputs are the inputs
-// of the second stage's butterflies 4a + k (k = 0..3); the second stage
-// leaves elements 16a .. 16a + 15 in the thread.  One exchange through the
-// line's shared buffer (element p at p + p/16: a warp's accesses fall in
-// distinct banks) gives thread a the inputs of third-stage butterflies a and
-// a + 8, whose outputs are elements a + 8m again (m = 2r for butterfly a,
-// 2r + 1 for a + 8).  No block barrier: the 8 threads of a line are one
+// ---------------------------------------------------------------- lines in registers
+// The same Stockham transform of a 64-, 128- or 256-point line (plans 8 8;
+// 4 4 8; 4 8 8: the same butterflies, twiddles and operation order as
+// block_fft, so the same bits), computed by 8 threads of one warp with the
+// data in registers: thread a holds elements a + 8m (m < L/8).  Those are
+// exactly the inputs of the first stage's butterflies a + 8q; for 128 and 256
+// points their outputs are in turn the inputs of the second stage's
+// butterflies 4a + k, which leave elements (L/8)a .. (L/8)a + L/8 - 1 in the
+// thread.  One exchange through the line's shared buffer (element p at
+// p + p/(L/8): the 8 threads' accesses fall in distinct banks) gives thread a
+// the inputs of the last stage's butterflies a + 8s, whose outputs are the
+// elements a + 8m again.  No block barrier: the 8 threads of a line are a
 // quarter of a warp.
-__device__ __forceinline__ int xidx(int p) { return p + (p >> 4); }
-constexpr int kLine128 = 136;  // exchange buffer elements of one line
+template <int L>
+struct LineGeo {
+    static constexpr int M = L / 8;           // elements per thread
+    static constexpr int BUF = L + 8;         // exchange buffer elements of a line
+    static constexpr int LINES = L >= 256 ? 8 : 16;  // lines per block
+    static constexpr int NT = 8 * LINES;
+};
+template <int L>
+__device__ __forceinline__ int xidx(int p) {
+    return p + p / (L / 8);
+}
 
-template <typename T, bool INV, bool HALF_IN>
-__device__ __forceinline__ void line128(Cx<T> (&v)[16], int a, Cx<T>* xs, const Cx<T>* __restrict__ tw) {
+template <typename T, bool INV, bool HALF_IN, int L>
+__device__ __forceinline__ void line_fft(Cx<T> (&v)[L / 8], int a, Cx<T>* xs, const Cx<T>* __restrict__ tw) {
     using C = Cx<T>;
-    C w[4][4];
-    // stage 1: radix 4, Ns = 1 (no twiddles); butterfly a + 8q reads elements a + 8q + 32r
+    constexpr int M = L / 8;
+    C o[M];  // elements M a + i after the stages before the exchange
+    if constexpr (L == 64) {
+        // stage 1: radix 8, Ns = 1; butterfly a reads elements a + 8r
+        C u[8];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        C u[4];
-        u[0] = v[q];
-        u[1] = v[q + 4];
-        if constexpr (HALF_IN) {
-            dft_half<T, 4, INV>(u);
-        } else {
-            u[2] = v[q + 8];
-            u[3] = v[q + 12];
-            dft<T, 4, INV>(u);
+        for (int r = 0; r < 8; ++r) u[r] = v[r];
+        if constexpr (HALF_IN)
+            dft_half<T, 8, INV>(u);
+        else
+            dft<T, 8, INV>(u);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) o[r] = u[r];
+    } else {
+        constexpr int R2 = L == 128 ? 4 : 8;   // second-stage radix
+        constexpr int Q = M / 4;                // first-stage butterflies per thread
+        C w[Q][4];
+        // stage 1: radix 4, Ns = 1; butterfly a + 8q reads elements a + 8q + (L/4) r
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            C u[4];
+            u[0] = v[q];
+            u[1] = v[q + Q];
+            if constexpr (HALF_IN) {
+                dft_half<T, 4, INV>(u);
+            } else {
+                u[2] = v[q + 2 * Q];
+                u[3] = v[q + 3 * Q];
+                dft<T, 4, INV>(u);
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) w[q][r] = u[r];
         }
+        // stage 2: radix R2, Ns = 4, step L / (4 R2) = 8; butterfly 4a + k
+        // reads the first stage's outputs 4a + k + (L/R2) r = output k of
+        // butterfly a + 8r, and writes elements M a + k + 4r
 #pragma unroll
-        for (int r = 0; r < 4; ++r) w[q][r] = u[r];
-    }
-    // stage 2: radix 4, Ns = 4, step 8; butterfly 4a + k reads the first
-    // stage's outputs 4a + k + 32r = output k of butterfly a + 8r
-    C o[16];
+        for (int k = 0; k < 4; ++k) {
+            C u[R2];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        C u[4];
+            for (int r = 0; r < R2; ++r) u[r] = w[r][k];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) u[r] = w[r][k];
+            for (int r = 1; r < R2; ++r) {
+                C t = __ldg(&tw[r * k * 8]);
+                if (INV) t.y = -t.y;
+                u[r] = cmul(u[r], t);
+            }
+            dft<T, R2, INV>(u);
 #pragma unroll
-        for (int r = 1; r < 4; ++r) {
-            C t = __ldg(&tw[r * k * 8]);
-            if (INV) t.y = -t.y;
-            u[r] = cmul(u[r], t);
+            for (int r = 0; r < R2; ++r) o[k + 4 * r] = u[r];
         }
-        dft<T, 4, INV>(u);
-#pragma unroll
-        for (int r = 0; r < 4; ++r) o[k + 4 * r] = u[r];  // element 16a + k + 4r
     }
 #pragma unroll
-    for (int i = 0; i < 16; ++i) xs[xidx(16 * a + i)] = o[i];
+    for (int i = 0; i < M; ++i) xs[xidx<L>(M * a + i)] = o[i];
     __syncwarp();
-    // stage 3: radix 8, Ns = 16, step 1; butterfly j reads elements j + 16r
+    // last stage: radix 8, Ns = M, step 1; butterfly j = a + 8s reads
+    // elements j + M r and writes them back in place
 #pragma unroll
-    for (int s2 = 0; s2 < 2; ++s2) {
+    for (int s2 = 0; s2 < M / 8; ++s2) {
         const int j = a + 8 * s2;
         C u[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) u[r] = xs[xidx(j + 16 * r)];
+        for (int r = 0; r < 8; ++r) u[r] = xs[xidx<L>(j + M * r)];
 #pragma unroll
         for (int r = 1; r < 8; ++r) {
             C t = __ldg(&tw[r * j]);
@@ -652,38 +679,39 @@ __device__ __forceinline__ void line128(Cx<T> (&v)[16], int a, Cx<T>* xs, const 
         }
         dft<T, 8, INV>(u);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[2 * r + s2] = u[r];  // element j + 16r = a + 8 (2r + s2)
+        for (int r = 0; r < 8; ++r) v[s2 + (M / 8) * r] = u[r];  // element j + M r = a + 8 (s2 + (M/8) r)
     }
     __syncwarp();  // the buffer is free again
 }
 
-// Pass C on 128-point rows (n0 = 64): 8 threads per row, 16 rows per block.
-// The forward transform leaves each thread the spectrum at a + 8m, exactly
-// the inputs the inverse transform's first two stages need from it.
-template <typename TI, typename TO, bool CG>
-__global__ void __launch_bounds__(128, 4) k_fft_x_conv_r128(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat,
-                                                         int n0, int n1, int L1, int rows, const Cx<TI>* __restrict__ twi,
-                                                         const Cx<TO>* __restrict__ two) {
+// Pass C on rows of L = 2 n0 points: 8 threads per row.  The forward
+// transform leaves each thread the spectrum at a + 8m, exactly the inputs
+// the inverse transform's first stages need from it.
+template <typename TI, typename TO, bool CG, int L>
+__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_x_conv_lines(const Cx<TI>* in, Cx<TO>* out,
+                                                                   const TI* __restrict__ ghat, int n0, int n1, int L1,
+                                                                   int rows, const Cx<TI>* __restrict__ twi,
+                                                                   const Cx<TO>* __restrict__ two) {
     using CI = Cx<TI>;
     using CO = Cx<TO>;
-    constexpr int L = 128;
-    __shared__ __align__(16) CO xbuf[16][kLine128];
+    using G = LineGeo<L>;
+    constexpr int M = G::M;
+    __shared__ __align__(16) CO xbuf[G::LINES][G::BUF];
     const int li = threadIdx.x >> 3, a = threadIdx.x & 7;
-    const int r = blockIdx.x * 16 + li;
+    const int r = blockIdx.x * G::LINES + li;
     const bool live = r < rows;
-    CI v[16];
+    CI v[M];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = live ? in[(size_t)r * L + a + 8 * m] : CI{(TI)0, (TI)0};
-#pragma unroll
-    for (int m = 8; m < 16; ++m) v[m] = CI{(TI)0, (TI)0};
-    line128<TI, false, true>(v, a, reinterpret_cast<CI*>(xbuf[li]), twi);
+    for (int m = 0; m < M; ++m)
+        v[m] = (live && m < M / 2) ? in[(size_t)r * L + a + 8 * m] : CI{(TI)0, (TI)0};
+    line_fft<TI, false, true, L>(v, a, reinterpret_cast<CI*>(xbuf[li]), twi);
     const int kz = live ? r / L1 : 0;
     const int ky = live ? r - kz * L1 : 0;
     const int gy = ky <= n1 ? ky : L1 - ky;
     const size_t grow = ((size_t)kz * (n1 + 1) + gy) * (n0 + 1);
-    CO w[16];
+    CO w[M];
 #pragma unroll
-    for (int m = 0; m < 16; ++m) {
+    for (int m = 0; m < M; ++m) {
         const int kx = a + 8 * m;
         const int gx = kx <= n0 ? kx : L - kx;
         const CI f = v[m];
@@ -695,34 +723,35 @@ __global__ void __launch_bounds__(128, 4) k_fft_x_conv_r128(const Cx<TI>* in, Cx
             w[m] = CO{(TO)(f.x * gv), (TO)(f.y * gv)};
         }
     }
-    line128<TO, true, false>(w, a, xbuf[li], two);
+    line_fft<TO, true, false, L>(w, a, xbuf[li], two);
+    if (!live) return;
 #pragma unroll
-    for (int m = 0; m < 8; ++m)  // outputs x < 64: element a + 8m
-        if (live) out[(size_t)r * L + a + 8 * m] = w[m];
+    for (int m = 0; m < M / 2; ++m) out[(size_t)r * L + a + 8 * m] = w[m];  // x < n0
 }
 
-// Passes B (forward, inputs y < n_in = 64) and D (inverse, outputs y <
-// n_out = 64) on 128-point columns along y: 8 threads per column, 16
-// columns (consecutive x of one plane) per block.
-template <typename T, bool INV>
-__global__ void __launch_bounds__(128, 4) k_fft_y_r128(Cx<T>* __restrict__ spec, int n0, int L0, int planes,
-                                                    const Cx<T>* __restrict__ twy) {
+// Passes B (forward, inputs y < L/2) and D (inverse, outputs y < L/2) on
+// columns of L points along y: 8 threads per column, consecutive x of one
+// plane per block.
+template <typename T, bool INV, int L>
+__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_y_lines(Cx<T>* __restrict__ spec, int n0, int L0, int planes,
+                                                              const Cx<T>* __restrict__ twy) {
     using C = Cx<T>;
-    constexpr int L = 128;
-    __shared__ __align__(16) C xbuf[16][kLine128];
+    using G = LineGeo<L>;
+    constexpr int M = G::M;
+    __shared__ __align__(16) C xbuf[G::LINES][G::BUF];
     const int li = threadIdx.x >> 3, a = threadIdx.x & 7;
-    const int xb = (n0 + 15) / 16;
+    const int xb = (n0 + G::LINES - 1) / G::LINES;
     const int kz = blockIdx.x / xb;
-    const int x = (blockIdx.x - kz * xb) * 16 + li;
+    const int x = (blockIdx.x - kz * xb) * G::LINES + li;
     const bool live = kz < planes && x < n0;
     C* col = spec + (size_t)kz * L * L0 + (live ? x : 0);
-    C v[16];
+    C v[M];
 #pragma unroll
-    for (int m = 0; m < 16; ++m)
-        v[m] = (live && (INV || m < 8)) ? col[(size_t)(a + 8 * m) * L0] : C{(T)0, (T)0};
-    line128<T, INV, !INV>(v, a, xbuf[li], twy);
+    for (int m = 0; m < M; ++m)
+        v[m] = (live && (INV || m < M / 2)) ? col[(size_t)(a + 8 * m) * L0] : C{(T)0, (T)0};
+    line_fft<T, INV, !INV, L>(v, a, xbuf[li], twy);
     if (!live) return;
-    constexpr int MO = INV ? 8 : 16;  // D keeps y < 64
+    constexpr int MO = INV ? M / 2 : M;  // D keeps y < L/2
 #pragma unroll
     for (int m = 0; m < MO; ++m) col[(size_t)(a + 8 * m) * L0] = v[m];
 }
@@ -945,9 +974,9 @@ int single_variant(int LT) {
     return LT >= 64 ? 1 : 0;  // half-width tiles measured faster from 64 points up (the cosine transforms most)
 }
 
-// Passes B, C and D of 128-point lines take the register-resident kernels
-// (k_*_r128, the same bits as the staged ones); SCGPU_FFT_LINES=0 selects the
-// staged kernels.
+// Passes B, C and D of 64-, 128- and 256-point lines take the
+// register-resident kernels (k_*_lines, the same bits as the staged ones);
+// SCGPU_FFT_LINES=0 selects the staged kernels.
 bool register_lines() {
     static const bool on = [] {
         const char* e = std::getenv("SCGPU_FFT_LINES");
@@ -1019,10 +1048,11 @@ struct LaunchY {
     cudaStream_t s;
     template <int LT>
     void run() {
-        if constexpr (LT == 128) {
-            if (register_lines() && (INV ? n_out : n_in) == 64) {
-                const unsigned blocks = (unsigned)(planes * ((n0 + 15) / 16));
-                k_fft_y_r128<T, INV><<<blocks, 128, 0, s>>>(spec, n0, L0, planes, twy);
+        if constexpr (LT == 64 || LT == 128 || LT == 256) {
+            if (register_lines() && 2 * (INV ? n_out : n_in) == LT) {
+                using G = LineGeo<LT>;
+                const unsigned blocks = (unsigned)(planes * ((n0 + G::LINES - 1) / G::LINES));
+                k_fft_y_lines<T, INV, LT><<<blocks, G::NT, 0, s>>>(spec, n0, L0, planes, twy);
                 return;
             }
         }
@@ -1048,10 +1078,11 @@ struct LaunchC {
     cudaStream_t s;
     template <int LT>
     void run() {
-        if constexpr (LT == 128) {
-            if (register_lines() && n0 == 64) {
-                k_fft_x_conv_r128<TI, double, CG><<<(unsigned)((rows + 15) / 16), 128, 0, s>>>(in, out, ghat, n0, n1, L1,
-                                                                                           rows, twi, two);
+        if constexpr (LT == 64 || LT == 128 || LT == 256) {
+            if (register_lines() && 2 * n0 == LT) {
+                using G = LineGeo<LT>;
+                k_fft_x_conv_lines<TI, double, CG, LT><<<(unsigned)((rows + G::LINES - 1) / G::LINES), G::NT, 0, s>>>(
+                    in, out, ghat, n0, n1, L1, rows, twi, two);
                 return;
             }
         }
