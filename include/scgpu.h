@@ -450,7 +450,10 @@ double scgpu_batch_last_track_ms(const scgpu_batch* batch);
 /* Tuning of the batched launches: threads per block of the deposit (128,
  * 256 or 512) and, per transform length L, the FFT tile shape (0: the
  * widest, up to 256 threads per block; 1, 2, 3: a half, a quarter, an eighth
- * as many columns per block, down to one warp). */
+ * as many columns per block, down to one warp; 4: the y and x passes of 64-,
+ * 128- and 256-point lines as register-resident line transforms, 8 threads
+ * a line, the others as 0).  Untuned lengths take 4 where it applies, else
+ * 0.  Every variant gives the same bits. */
 int scgpu_batch_set_tuning(scgpu_batch* batch, int deposit_threads, int L, int fft_variant);
 int scgpu_batch_get_tuning(const scgpu_batch* batch, int L, int* deposit_threads, int* fft_variant);
 /* The autotuner: times trial_steps batched steps per candidate (deposit block

@@ -117,9 +117,11 @@ void drop_graphs(scgpu_batch* b) {
     }
 }
 
+// the tuned variant of a length, else the line transforms where they exist
 int variant_of(const scgpu_batch* b, int L) {
     auto it = b->fft_variant.find(L);
-    return it == b->fft_variant.end() ? 0 : it->second;
+    if (it != b->fft_variant.end()) return it->second;
+    return (fft_register_lines() && (L == 64 || L == 128 || L == 256)) ? kFftLinesVariant : 0;
 }
 
 // Work tables and launch list of the current membership, uploaded to the device.

@@ -688,17 +688,16 @@ __device__ __forceinline__ void line_fft(Cx<T> (&v)[L / 8], int a, Cx<T>* xs, co
 // transform leaves each thread the spectrum at a + 8m, exactly the inputs
 // the inverse transform's first stages need from it.
 template <typename TI, typename TO, bool CG, int L>
-__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_x_conv_lines(const Cx<TI>* in, Cx<TO>* out,
-                                                                   const TI* __restrict__ ghat, int n0, int n1, int L1,
-                                                                   int rows, const Cx<TI>* __restrict__ twi,
-                                                                   const Cx<TO>* __restrict__ two) {
+__device__ __forceinline__ void fft_x_conv_lines_body(const Cx<TI>* in, Cx<TO>* out, const TI* __restrict__ ghat, int n0,
+                                                      int n1, int L1, int rows, const Cx<TI>* __restrict__ twi,
+                                                      const Cx<TO>* __restrict__ two, int blk) {
     using CI = Cx<TI>;
     using CO = Cx<TO>;
     using G = LineGeo<L>;
     constexpr int M = G::M;
     __shared__ __align__(16) CO xbuf[G::LINES][G::BUF];
     const int li = threadIdx.x >> 3, a = threadIdx.x & 7;
-    const int r = blockIdx.x * G::LINES + li;
+    const int r = blk * G::LINES + li;
     const bool live = r < rows;
     CI v[M];
 #pragma unroll
@@ -729,20 +728,26 @@ __global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_x_conv_lines(const Cx<TI
     for (int m = 0; m < M / 2; ++m) out[(size_t)r * L + a + 8 * m] = w[m];  // x < n0
 }
 
+template <typename TI, typename TO, bool CG, int L>
+__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_x_conv_lines(const Cx<TI>* in, Cx<TO>* out,
+                                                                   const TI* __restrict__ ghat, int n0, int n1, int L1,
+                                                                   int rows, const Cx<TI>* __restrict__ twi,
+                                                                   const Cx<TO>* __restrict__ two) {
+    fft_x_conv_lines_body<TI, TO, CG, L>(in, out, ghat, n0, n1, L1, rows, twi, two, blockIdx.x);
+}
+
 // Passes B (forward, inputs y < L/2) and D (inverse, outputs y < L/2) on
 // columns of L points along y: 8 threads per column, consecutive x of one
 // plane per block.
 template <typename T, bool INV, int L>
-__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_y_lines(Cx<T>* __restrict__ spec, int n0, int L0, int planes,
-                                                              const Cx<T>* __restrict__ twy) {
+__device__ __forceinline__ void fft_y_lines_body(Cx<T>* __restrict__ spec, int n0, int L0, int planes,
+                                                 const Cx<T>* __restrict__ twy, int bx, int kz) {
     using C = Cx<T>;
     using G = LineGeo<L>;
     constexpr int M = G::M;
     __shared__ __align__(16) C xbuf[G::LINES][G::BUF];
     const int li = threadIdx.x >> 3, a = threadIdx.x & 7;
-    const int xb = (n0 + G::LINES - 1) / G::LINES;
-    const int kz = blockIdx.x / xb;
-    const int x = (blockIdx.x - kz * xb) * G::LINES + li;
+    const int x = bx * G::LINES + li;
     const bool live = kz < planes && x < n0;
     C* col = spec + (size_t)kz * L * L0 + (live ? x : 0);
     C v[M];
@@ -754,6 +759,12 @@ __global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_y_lines(Cx<T>* __restric
     constexpr int MO = INV ? M / 2 : M;  // D keeps y < L/2
 #pragma unroll
     for (int m = 0; m < MO; ++m) col[(size_t)(a + 8 * m) * L0] = v[m];
+}
+
+template <typename T, bool INV, int L>
+__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_y_lines(Cx<T>* __restrict__ spec, int n0, int L0, int planes,
+                                                              const Cx<T>* __restrict__ twy) {
+    fft_y_lines_body<T, INV, L>(spec, n0, L0, planes, twy, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------- pass E
@@ -967,7 +978,7 @@ int single_variant(int LT) {
     static const int forced = [] {
         const char* e = std::getenv("SCGPU_FFT_VARIANT");
         const int v = e ? std::atoi(e) : -1;
-        return (v >= 0 && v < kFftVariants) ? v : -1;
+        return (v >= 0 && v < kFftLinesVariant) ? v : -1;
     }();
     if (LT == 0) return 0;
     if (forced >= 0) return forced;
@@ -1051,8 +1062,8 @@ struct LaunchY {
         if constexpr (LT == 64 || LT == 128 || LT == 256) {
             if (register_lines() && 2 * (INV ? n_out : n_in) == LT) {
                 using G = LineGeo<LT>;
-                const unsigned blocks = (unsigned)(planes * ((n0 + G::LINES - 1) / G::LINES));
-                k_fft_y_lines<T, INV, LT><<<blocks, G::NT, 0, s>>>(spec, n0, L0, planes, twy);
+                const dim3 g((unsigned)((n0 + G::LINES - 1) / G::LINES), (unsigned)planes);
+                k_fft_y_lines<T, INV, LT><<<g, G::NT, 0, s>>>(spec, n0, L0, planes, twy);
                 return;
             }
         }
@@ -1268,6 +1279,42 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_fft_pass_batch(const DevBunch
     }
 }
 
+inline bool line_length(int L) { return L == 64 || L == 128 || L == 256; }
+
+// Variant kFftLinesVariant: passes B, C and D of 64-, 128- and 256-point
+// lines run the register-resident line transforms (the same bits), block
+// (x, y) of a bunch as in the single-bunch launch.
+template <typename T, int PASS, int L>
+__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_lines_batch(const DevBunch* __restrict__ tab,
+                                                                  const int4* __restrict__ work, int nitems) {
+    const int4 w = resolve_block(work, nitems);
+    const DevBunch& d = tab[w.x];
+    const int n0 = d.bc.n[0], n1 = d.bc.n[1], n2 = d.bc.n[2];
+    const int L0 = 2 * n0, L1 = 2 * n1;
+    Cx<T>* fwd = reinterpret_cast<Cx<T>*>(d.precision == 0 ? d.spec : d.spec_lo);
+    double2* inv = reinterpret_cast<double2*>(d.spec);
+    if constexpr (PASS == kPassYFwd)
+        fft_y_lines_body<T, false, L>(fwd, n0, L0, n2 + 1, tw_dev<T>(d, 1), w.y, w.z);
+    else if constexpr (PASS == kPassXConv)
+        fft_x_conv_lines_body<T, double, false, L>(fwd, inv, (const T*)d.ghat, n0, n1, L1, (n2 + 1) * L1, tw_dev<T>(d, 0),
+                                                   tw_dev<double>(d, 0), w.y);
+    else
+        fft_y_lines_body<double, true, L>(inv, n0, L0, n2 + 1, tw_dev<double>(d, 1), w.y, w.z);
+}
+
+template <typename T, int PASS>
+struct LaunchLinesBatch {
+    const DevBunch* tab;
+    const int4* work;
+    int nitems, n;
+    cudaStream_t s;
+    template <int LT>
+    void run() {
+        if constexpr (LT == 64 || LT == 128 || LT == 256)
+            k_fft_lines_batch<T, PASS, LT><<<n, LineGeo<LT>::NT, 0, s>>>(tab, work, nitems);
+    }
+};
+
 template <typename T, int PASS>
 size_t pass_smem(int L, int nc) {
     if constexpr (PASS == kPassXConv) return smem_conv<T>(L, nc);
@@ -1297,6 +1344,15 @@ struct LaunchPassBatch {
 
 template <typename T, int PASS>
 void pass_batch_t(int L, int variant, const DevBunch* tab, const int4* work, int nitems, int n, cudaStream_t s) {
+    if (variant == kFftLinesVariant) {
+        if constexpr (PASS == kPassYFwd || PASS == kPassXConv || PASS == kPassYInv) {
+            if (line_length(L)) {
+                with_length(L, LaunchLinesBatch<T, PASS>{tab, work, nitems, n, s});
+                return;
+            }
+        }
+        variant = 0;  // the other passes with the widest tiles
+    }
     switch (variant) {
         case 1: with_length(L, LaunchPassBatch<T, PASS, 1>{tab, work, nitems, n, L, s}); break;
         case 2: with_length(L, LaunchPassBatch<T, PASS, 2>{tab, work, nitems, n, L, s}); break;
@@ -1323,6 +1379,8 @@ inline bool special_length(int L) { return L == 32 || L == 64 || L == 96 || L ==
 
 }  // namespace
 
+bool fft_register_lines() { return register_lines(); }
+
 int fft_pass_length(int pass, const DevBunch& b) {
     switch (pass) {
         case kPassZR2C:
@@ -1337,8 +1395,22 @@ int fft_pass_length(int pass, const DevBunch& b) {
 
 void fft_pass_grid(int pass, const DevBunch& b, int variant, int* gx, int* gy) {
     const int L = fft_pass_length(pass, b);
-    const int nc = cols_v(special_length(L) ? L : 0, variant);
     const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    if (variant == kFftLinesVariant) {
+        const int lines = L >= 256 ? LineGeo<256>::LINES : LineGeo<128>::LINES;
+        if (line_length(L) && (pass == kPassYFwd || pass == kPassYInv)) {
+            *gx = (n0 + lines - 1) / lines;
+            *gy = n2 + 1;
+            return;
+        }
+        if (line_length(L) && pass == kPassXConv) {
+            *gx = ((n2 + 1) * 2 * n1 + lines - 1) / lines;
+            *gy = 1;
+            return;
+        }
+        variant = 0;
+    }
+    const int nc = cols_v(special_length(L) ? L : 0, variant);
     switch (pass) {
         case kPassZR2C:
         case kPassZC2R:

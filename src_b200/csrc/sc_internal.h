@@ -186,7 +186,9 @@ enum : int {
     kPassDctX,
     kNumPasses
 };
-constexpr int kFftVariants = 4;
+constexpr int kFftVariants = 5;
+constexpr int kFftLinesVariant = 4;  // register-resident line transforms for passes B, C, D (64/128/256 points)
+bool fft_register_lines();           // line transforms enabled (SCGPU_FFT_LINES is not 0)
 // Blocks of one pass for one bunch (grid x, y) with a tile-shape variant.
 void fft_pass_grid(int pass, const DevBunch& b, int variant, int* gx, int* gy);
 // Transform length of a pass's axis for a bunch.
