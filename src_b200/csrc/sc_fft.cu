@@ -605,7 +605,18 @@ __device__ __forceinline__ int xidx(int p) {
     return p + p / (L / 8);
 }
 
-template <typename T, bool INV, bool HALF_IN, int L>
+// BLOCK: the 8 threads of a line sit in different warps (the y passes, whose
+// lanes run along x for coalesced columns); the exchange then waits for the
+// whole block.
+template <bool BLOCK>
+__device__ __forceinline__ void line_sync() {
+    if constexpr (BLOCK)
+        __syncthreads();
+    else
+        __syncwarp();
+}
+
+template <typename T, bool INV, bool HALF_IN, int L, bool BLOCK = false>
 __device__ __forceinline__ void line_fft(Cx<T> (&v)[L / 8], int a, Cx<T>* xs, const Cx<T>* __restrict__ tw) {
     using C = Cx<T>;
     constexpr int M = L / 8;
@@ -662,7 +673,7 @@ __device__ __forceinline__ void line_fft(Cx<T> (&v)[L / 8], int a, Cx<T>* xs, co
     }
 #pragma unroll
     for (int i = 0; i < M; ++i) xs[xidx<L>(M * a + i)] = o[i];
-    __syncwarp();
+    line_sync<BLOCK>();
     // last stage: radix 8, Ns = M, step 1; butterfly j = a + 8s reads
     // elements j + M r and writes them back in place
 #pragma unroll
@@ -681,7 +692,7 @@ __device__ __forceinline__ void line_fft(Cx<T> (&v)[L / 8], int a, Cx<T>* xs, co
 #pragma unroll
         for (int r = 0; r < 8; ++r) v[s2 + (M / 8) * r] = u[r];  // element j + M r = a + 8 (s2 + (M/8) r)
     }
-    __syncwarp();  // the buffer is free again
+    line_sync<BLOCK>();  // the buffer is free again
 }
 
 // Pass C on rows of L = 2 n0 points: 8 threads per row.  The forward
@@ -737,16 +748,19 @@ __global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_x_conv_lines(const Cx<TI
 }
 
 // Passes B (forward, inputs y < L/2) and D (inverse, outputs y < L/2) on
-// columns of L points along y: 8 threads per column, consecutive x of one
-// plane per block.
+// columns of L points along y: 8 threads per column (in different warps),
+// consecutive x of one plane per block.
 template <typename T, bool INV, int L>
 __device__ __forceinline__ void fft_y_lines_body(Cx<T>* __restrict__ spec, int n0, int L0, int planes,
                                                  const Cx<T>* __restrict__ twy, int bx, int kz) {
     using C = Cx<T>;
     using G = LineGeo<L>;
     constexpr int M = G::M;
-    __shared__ __align__(16) C xbuf[G::LINES][G::BUF];
-    const int li = threadIdx.x >> 3, a = threadIdx.x & 7;
+    // lanes run along x (thread li + LINES a: column li, part a), so a warp
+    // reads and writes whole rows of consecutive columns; the line buffers
+    // are G::BUF + 1 apart, so the lines of one access fall in distinct banks
+    __shared__ __align__(16) C xbuf[G::LINES][G::BUF + 1];
+    const int li = threadIdx.x % G::LINES, a = threadIdx.x / G::LINES;
     const int x = bx * G::LINES + li;
     const bool live = kz < planes && x < n0;
     C* col = spec + (size_t)kz * L * L0 + (live ? x : 0);
@@ -754,7 +768,7 @@ __device__ __forceinline__ void fft_y_lines_body(Cx<T>* __restrict__ spec, int n
 #pragma unroll
     for (int m = 0; m < M; ++m)
         v[m] = (live && (INV || m < M / 2)) ? col[(size_t)(a + 8 * m) * L0] : C{(T)0, (T)0};
-    line_fft<T, INV, !INV, L>(v, a, xbuf[li], twy);
+    line_fft<T, INV, !INV, L, true>(v, a, xbuf[li], twy);
     if (!live) return;
     constexpr int MO = INV ? M / 2 : M;  // D keeps y < L/2
 #pragma unroll
