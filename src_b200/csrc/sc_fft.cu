@@ -31,6 +31,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "sc_internal.h"
@@ -714,22 +715,30 @@ __device__ __forceinline__ void fft_x_conv_lines_body(const Cx<TI>* in, Cx<TO>* 
 #pragma unroll
     for (int m = 0; m < M; ++m)
         v[m] = (live && m < M / 2) ? in[(size_t)r * L + a + 8 * m] : CI{(TI)0, (TI)0};
-    line_fft<TI, false, true, L>(v, a, reinterpret_cast<CI*>(xbuf[li]), twi);
     const int kz = live ? r / L1 : 0;
     const int ky = live ? r - kz * L1 : 0;
     const int gy = ky <= n1 ? ky : L1 - ky;
     const size_t grow = ((size_t)kz * (n1 + 1) + gy) * (n0 + 1);
-    CO w[M];
+    // the row of G's spectrum is fetched before the forward transform, so its
+    // latency hides behind the transform
+    using GV = typename std::conditional<CG, CI, TI>::type;
+    GV g[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         const int kx = a + 8 * m;
         const int gx = kx <= n0 ? kx : L - kx;
+        g[m] = live ? reinterpret_cast<const GV*>(ghat)[grow + gx] : GV{};
+    }
+    line_fft<TI, false, true, L>(v, a, reinterpret_cast<CI*>(xbuf[li]), twi);
+    CO w[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
         const CI f = v[m];
         if constexpr (CG) {
-            const CI gc = live ? reinterpret_cast<const CI*>(ghat)[grow + gx] : CI{(TI)0, (TI)0};
+            const CI gc = g[m];
             w[m] = CO{(TO)(f.x * gc.x - f.y * gc.y), (TO)(f.x * gc.y + f.y * gc.x)};
         } else {
-            const TI gv = live ? ghat[grow + gx] : (TI)0;
+            const TI gv = g[m];
             w[m] = CO{(TO)(f.x * gv), (TO)(f.y * gv)};
         }
     }
@@ -779,6 +788,123 @@ template <typename T, bool INV, int L>
 __global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_y_lines(Cx<T>* __restrict__ spec, int n0, int L0, int planes,
                                                               const Cx<T>* __restrict__ twy) {
     fft_y_lines_body<T, INV, L>(spec, n0, L0, planes, twy, blockIdx.x, blockIdx.y);
+}
+
+// Pass A on z lines of L = 2 n2 points: two real columns (x, x + 1) of one y
+// per complex line, 8 threads per line with the lanes along x (consecutive
+// column pairs, so a warp reads and writes whole rows) and block-level
+// exchanges.  The two half spectra need Z[k] and Z[L - k], which sit in
+// different threads: the transformed line goes through its buffer once more.
+template <typename T, int L>
+__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_z_r2c_lines(const T* __restrict__ rho, Cx<T>* __restrict__ spec,
+                                                                  int n0, int n1, int L0, int L1,
+                                                                  const Cx<T>* __restrict__ twz) {
+    using C = Cx<T>;
+    using G = LineGeo<L>;
+    constexpr int M = G::M, K = L / 2;
+    __shared__ __align__(16) C xbuf[G::LINES][G::BUF + 1];
+    const int li = threadIdx.x % G::LINES, a = threadIdx.x / G::LINES;
+    const int np = (n0 + 1) / 2;
+    const int line = blockIdx.x * G::LINES + li;
+    const int y = line / np, x = 2 * (line - y * np);
+    const bool live = y < n1;
+    const bool odd = live && x + 1 < n0;
+    C v[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        v[m] = C{(T)0, (T)0};
+        if (live && m < M / 2) {
+            const T* p = rho + ((size_t)(a + 8 * m) * n1 + y) * n0 + x;
+            v[m].x = p[0];
+            if (odd) v[m].y = p[1];
+        }
+    }
+    C* xs = xbuf[li];
+    line_fft<T, false, true, L, true>(v, a, xs, twz);
+#pragma unroll
+    for (int m = 0; m < M; ++m) xs[xidx<L>(a + 8 * m)] = v[m];
+    __syncthreads();
+    if (!live) return;
+#pragma unroll
+    for (int m = 0; m <= M / 2; ++m) {
+        const int k = a + 8 * m;
+        if (k > K) break;
+        const C Z = xs[xidx<L>(k)];
+        const C Zm = xs[xidx<L>(k == 0 ? 0 : L - k)];
+        C* dst = spec + ((size_t)k * L1 + y) * L0 + x;
+        dst[0] = C{(T)0.5 * (Z.x + Zm.x), (T)0.5 * (Z.y - Zm.y)};
+        if (odd) dst[1] = C{(T)0.5 * (Z.y + Zm.y), (T)-0.5 * (Z.x - Zm.x)};
+    }
+}
+
+// Pass E on z lines of L = 2 n2 points, laid out as pass A: the half spectra
+// of two columns (x, x + 1) become one complex line (Z[k] and Z[L - k] from
+// the same two values, written through the line's buffer), then the inverse
+// transform; outputs z < n2.
+template <bool SELF, bool FLIP, int L>
+__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_z_c2r_lines(const double2* __restrict__ spec,
+                                                                  double* __restrict__ phi, int n0, int n1, int L0,
+                                                                  int L1, const double2* __restrict__ twz,
+                                                                  const StepState* __restrict__ st, double normFact,
+                                                                  double coupling) {
+    using C = double2;
+    using G = LineGeo<L>;
+    constexpr int M = G::M, K = L / 2, n2 = L / 2;
+    __shared__ __align__(16) C xbuf[G::LINES][G::BUF + 1];
+    const int li = threadIdx.x % G::LINES, a = threadIdx.x / G::LINES;
+    const int np = (n0 + 1) / 2;
+    const int line = blockIdx.x * G::LINES + li;
+    const int y = line / np, x = 2 * (line - y * np);
+    const bool live = y < n1;
+    const bool odd = live && x + 1 < n0;
+    C* xs = xbuf[li];
+#pragma unroll
+    for (int m = 0; m <= M / 2; ++m) {
+        const int k = a + 8 * m;
+        if (k > K) break;
+        C A = C{0.0, 0.0}, B = C{0.0, 0.0};
+        if (live) {
+            const C* src = spec + ((size_t)k * L1 + y) * L0 + x;
+            A = src[0];
+            if (odd) B = src[1];
+        }
+        C p = A, q = B;
+        if (k == 0 || k == K) {  // the half-complex format holds no imaginary part there
+            p.y = 0.0;
+            q.y = 0.0;
+        }
+        xs[xidx<L>(k)] = C{p.x - q.y, p.y + q.x};
+        if (k != 0 && k != K) xs[xidx<L>(L - k)] = C{A.x + B.y, B.x - A.y};
+    }
+    __syncthreads();
+    C v[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) v[m] = xs[xidx<L>(a + 8 * m)];
+    __syncthreads();
+    line_fft<double, true, false, L, true>(v, a, xs, twz);
+    if (!live) return;
+    const double hvol = SELF ? st->hvol : 1.0;
+#pragma unroll
+    for (int m = 0; m < M / 2; ++m) {
+        const int zz = a + 8 * m;
+        double* dst = phi + ((size_t)(FLIP ? n2 - 1 - zz : zz) * n1 + y) * n0 + x;
+        double r0 = v[m].x;
+        r0 = r0 * normFact;
+        if (SELF) {
+            r0 = r0 * hvol;
+            r0 = r0 * coupling;
+        }
+        dst[0] = r0;
+        if (odd) {
+            double r1 = v[m].y;
+            r1 = r1 * normFact;
+            if (SELF) {
+                r1 = r1 * hvol;
+                r1 = r1 * coupling;
+            }
+            dst[1] = r1;
+        }
+    }
 }
 
 // ---------------------------------------------------------------- pass E
@@ -999,7 +1125,7 @@ int single_variant(int LT) {
     return LT >= 64 ? 1 : 0;  // half-width tiles measured faster from 64 points up (the cosine transforms most)
 }
 
-// Passes B, C and D of 64-, 128- and 256-point lines take the
+// Passes A to E of 64-, 128- and 256-point lines (open z) take the
 // register-resident kernels (k_*_lines, the same bits as the staged ones);
 // SCGPU_FFT_LINES=0 selects the staged kernels.
 bool register_lines() {
@@ -1054,6 +1180,15 @@ struct LaunchA {
     cudaStream_t s;
     template <int LT>
     void run() {
+        if constexpr (!FULL && (LT == 64 || LT == 128 || LT == 256)) {
+            if (register_lines() && 2 * n2 == LT) {
+                using G = LineGeo<LT>;
+                const long long lines = (long long)n1 * ((n0 + 1) / 2);
+                k_fft_z_r2c_lines<T, LT><<<(unsigned)((lines + G::LINES - 1) / G::LINES), G::NT, 0, s>>>(
+                    rho, spec, n0, n1, L0, L1, twz);
+                return;
+            }
+        }
         with_variant<LT>(*this);
     }
     template <int LT, int V>
@@ -1154,6 +1289,15 @@ struct LaunchE {
     cudaStream_t s;
     template <int LT>
     void run() {
+        if constexpr (!FULL && (LT == 64 || LT == 128 || LT == 256)) {
+            if (register_lines() && 2 * n2 == LT) {
+                using G = LineGeo<LT>;
+                const long long lines = (long long)n1 * ((n0 + 1) / 2);
+                k_fft_z_c2r_lines<SELF, FLIP, LT><<<(unsigned)((lines + G::LINES - 1) / G::LINES), G::NT, 0, s>>>(
+                    spec, phi, n0, n1, L0, L1, twz, st, normFact, coupling);
+                return;
+            }
+        }
         with_variant<LT>(*this);
     }
     template <int LT, int V>
