@@ -837,76 +837,6 @@ __global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_z_r2c_lines(const T* __r
     }
 }
 
-// Pass E on z lines of L = 2 n2 points, laid out as pass A: the half spectra
-// of two columns (x, x + 1) become one complex line (Z[k] and Z[L - k] from
-// the same two values, written through the line's buffer), then the inverse
-// transform; outputs z < n2.
-template <bool SELF, bool FLIP, int L>
-__global__ void __launch_bounds__(LineGeo<L>::NT) k_fft_z_c2r_lines(const double2* __restrict__ spec,
-                                                                  double* __restrict__ phi, int n0, int n1, int L0,
-                                                                  int L1, const double2* __restrict__ twz,
-                                                                  const StepState* __restrict__ st, double normFact,
-                                                                  double coupling) {
-    using C = double2;
-    using G = LineGeo<L>;
-    constexpr int M = G::M, K = L / 2, n2 = L / 2;
-    __shared__ __align__(16) C xbuf[G::LINES][G::BUF + 1];
-    const int li = threadIdx.x % G::LINES, a = threadIdx.x / G::LINES;
-    const int np = (n0 + 1) / 2;
-    const int line = blockIdx.x * G::LINES + li;
-    const int y = line / np, x = 2 * (line - y * np);
-    const bool live = y < n1;
-    const bool odd = live && x + 1 < n0;
-    C* xs = xbuf[li];
-#pragma unroll
-    for (int m = 0; m <= M / 2; ++m) {
-        const int k = a + 8 * m;
-        if (k > K) break;
-        C A = C{0.0, 0.0}, B = C{0.0, 0.0};
-        if (live) {
-            const C* src = spec + ((size_t)k * L1 + y) * L0 + x;
-            A = src[0];
-            if (odd) B = src[1];
-        }
-        C p = A, q = B;
-        if (k == 0 || k == K) {  // the half-complex format holds no imaginary part there
-            p.y = 0.0;
-            q.y = 0.0;
-        }
-        xs[xidx<L>(k)] = C{p.x - q.y, p.y + q.x};
-        if (k != 0 && k != K) xs[xidx<L>(L - k)] = C{A.x + B.y, B.x - A.y};
-    }
-    __syncthreads();
-    C v[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) v[m] = xs[xidx<L>(a + 8 * m)];
-    __syncthreads();
-    line_fft<double, true, false, L, true>(v, a, xs, twz);
-    if (!live) return;
-    const double hvol = SELF ? st->hvol : 1.0;
-#pragma unroll
-    for (int m = 0; m < M / 2; ++m) {
-        const int zz = a + 8 * m;
-        double* dst = phi + ((size_t)(FLIP ? n2 - 1 - zz : zz) * n1 + y) * n0 + x;
-        double r0 = v[m].x;
-        r0 = r0 * normFact;
-        if (SELF) {
-            r0 = r0 * hvol;
-            r0 = r0 * coupling;
-        }
-        dst[0] = r0;
-        if (odd) {
-            double r1 = v[m].y;
-            r1 = r1 * normFact;
-            if (SELF) {
-                r1 = r1 * hvol;
-                r1 = r1 * coupling;
-            }
-            dst[1] = r1;
-        }
-    }
-}
-
 // ---------------------------------------------------------------- pass E
 // FLIP: the image potential is read back with z flipped,
 // rho[i][j][k] = rho2[i][j][n2 - k - 1] (FFTPoissonSolver.cpp:322-326).
@@ -1125,9 +1055,11 @@ int single_variant(int LT) {
     return LT >= 64 ? 1 : 0;  // half-width tiles measured faster from 64 points up (the cosine transforms most)
 }
 
-// Passes A to E of 64-, 128- and 256-point lines (open z) take the
+// Passes A (open z), B, C and D of 64-, 128- and 256-point lines take the
 // register-resident kernels (k_*_lines, the same bits as the staged ones);
-// SCGPU_FFT_LINES=0 selects the staged kernels.
+// pass E stays staged (its line form measured slower: 10.1 against 7.0 us
+// at 128 points, 32.6 against 26.2 us at 256).  SCGPU_FFT_LINES=0 selects
+// the staged kernels everywhere.
 bool register_lines() {
     static const bool on = [] {
         const char* e = std::getenv("SCGPU_FFT_LINES");
@@ -1289,17 +1221,6 @@ struct LaunchE {
     cudaStream_t s;
     template <int LT>
     void run() {
-        // the line form measured slower than the staged one for 128 points
-        // (10.1 against 7.0 us at 64^3), faster at 256
-        if constexpr (!FULL && LT == 256) {
-            if (register_lines() && 2 * n2 == LT) {
-                using G = LineGeo<LT>;
-                const long long lines = (long long)n1 * ((n0 + 1) / 2);
-                k_fft_z_c2r_lines<SELF, FLIP, LT><<<(unsigned)((lines + G::LINES - 1) / G::LINES), G::NT, 0, s>>>(
-                    spec, phi, n0, n1, L0, L1, twz, st, normFact, coupling);
-                return;
-            }
-        }
         with_variant<LT>(*this);
     }
     template <int LT, int V>
