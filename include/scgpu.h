@@ -18,7 +18,7 @@
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr)
  *       (src/Solvers/PoissonSolver.h:28; FFTPoissonSolver.cpp:337-382)
  *   scgpu_add_solenoid, scgpu_add_rfcavity, scgpu_clear_elements,
- *   scgpu_fieldmap_astra1d, scgpu_fieldmap_astra1d_dynamic
+ *   scgpu_fieldmap_astra1d, scgpu_fieldmap_astra1d_dynamic, scgpu_fieldmap_2d
  *       ParallelTTracker::computeExternalFields (ParallelTTracker.cpp:595-643)
  *       with Solenoid::apply / Astra1DMagnetoStatic and RFCavity::apply /
  *       Astra1DDynamic (see below)
@@ -240,6 +240,27 @@ int scgpu_add_rfcavity(scgpu_ctx* ctx, const char* fieldmap_path, double elemedg
                        double freq_mhz, double lag_rad);
 int scgpu_fieldmap_astra1d_dynamic(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin,
                                    double* zend, double* period, double* frequency_mhz);
+
+/* 2D field maps on an (r, z) grid in OPAL's own format: scgpu_add_solenoid
+ * takes a 2DMagnetoStatic map (src/Classic/Fields/FM2DMagnetoStatic.cpp)
+ * and scgpu_add_rfcavity a 2DDynamic map (FM2DDynamic.cpp) in place of the
+ * ASTRA 1D ones, chosen by the file's first word as Fieldmap::getFieldmap
+ * does.  Header "2DMagnetoStatic XZ|ZX [TRUE|FALSE]" or "2DDynamic XZ|ZX
+ * [TRUE|FALSE]"; XZ: "zbegin zend nz" [cm, intervals], (dynamic) the
+ * frequency [MHz], "rbegin rend nr", then (nz+1)(nr+1) lines r-major of
+ * "Bz Br" or "Ez Er E Ht" [MV/m, A/m]; ZX: the r line first, z-major lines
+ * "Br Bz" or "Er Ez Ht E".  The field is the reference's bilinear
+ * interpolation at the particle's distance from the axis, B = KS (Br x/r,
+ * Br y/r, Bz); E = VOLT cos(omega t + LAG) (Er x/r, Er y/r, Ez) and
+ * B -= VOLT sin(omega t + LAG) (-Bt y/r, Bt x/r, 0); none outside the grid
+ * (the reference also loses a particle beyond the map radially).
+ * scgpu_fieldmap_2d reads a map as those elements do: *dynamic, the grid
+ * points nz and nr, ranges = {zbegin, zend, rbegin, rend} [m], the
+ * frequency [MHz] (dynamic), and, when values is not NULL, the normalised
+ * values component-major (Bz, Br or Ez [V/m], Er [V/m], Bt [T]), value
+ * (c, z i, r j) at values[(c nr + j) nz + i]; capacity counts doubles. */
+int scgpu_fieldmap_2d(const char* path, int* dynamic, int* nz, int* nr, double* ranges, double* frequency_mhz,
+                      double* values, long long capacity);
 
 /* MULTIPOLE (src/Elements/OpalMultipole.cpp:127-166 attributes L, KN, DKN,
  * KS, DKS and ELEMEDGE; src/Classic/AbsBeamline/Multipole.cpp): a straight

@@ -59,8 +59,9 @@ class Solenoid(C.Structure):
     """A beamline element: kind 0 SOLENOID, kind 1 RFCAVITY (1D maps), kind 2 MULTIPOLE."""
     _fields_ = [("edge", C.c_double), ("scale", C.c_double), ("zbegin", C.c_double), ("range", C.c_double),
                 ("period", C.c_double), ("accuracy", C.c_int), ("kind", C.c_int), ("omega", C.c_double),
-                ("phase", C.c_double), ("xlrep", C.c_double), ("nskew", C.c_int), ("pad_", C.c_int),
-                ("aperture", C.c_double * 2), ("coefs", C.c_double * 255)]
+                ("phase", C.c_double), ("xlrep", C.c_double), ("nskew", C.c_int), ("map2d", C.c_int),
+                ("aperture", C.c_double * 2), ("nz", C.c_int), ("nr", C.c_int), ("hz", C.c_double),
+                ("hr", C.c_double), ("grid", _dp), ("coefs", C.c_double * 255)]
 
 
 class BeamParams(C.Structure):
@@ -271,6 +272,124 @@ def make_multipole(elemedge, length, kn=(), dkn=None, ks=(), dks=None, aperture=
     return e
 
 
+def read_map2d(path):
+    """A 2D (r, z) map as FM2DMagnetoStatic / FM2DDynamic read it
+    (FM2DMagnetoStatic.cpp:14-155, FM2DDynamic.cpp:15-170), restated: dict
+    with dynamic, nz, nr (grid points), zbegin, zend, rbegin, rend [m],
+    freq_mhz and values [component, r, z] (Bz, Br or Ez, Er [V/m], Bt [T])."""
+    keep = set(".-+\x89")
+
+    def content(f):  # Fieldmap::getLine: cut to the first and last letter, digit, . - +
+        for raw in f:
+            line = raw.split("#", 1)[0]
+            idx = [i for i, ch in enumerate(line) if ch.isalnum() or ch in keep]
+            if idx:
+                yield line[idx[0]:idx[-1] + 1]
+    with open(path) as f:
+        lines = list(content(f))
+    head = lines[0].split()
+    dynamic = head[0].startswith("2DDy")
+    if not dynamic and not head[0].startswith("2DMa"):
+        raise ValueError("not a 2D map")
+    normalize = True
+    if len(head) > 2:
+        normalize = head[2].upper() == "TRUE"
+    swap = head[1] == "ZX"
+    pos = 1
+
+    def rng():
+        nonlocal pos
+        a, b, n = lines[pos].split()
+        pos += 1
+        return float(a), float(b), int(n)
+    freq = 0.0
+    if swap:
+        rb, re_, nri = rng()
+        if dynamic:
+            freq = float(lines[pos]); pos += 1
+        zb, ze, nzi = rng()
+    else:
+        zb, ze, nzi = rng()
+        if dynamic:
+            freq = float(lines[pos]); pos += 1
+        rb, re_, nri = rng()
+    nz, nr = nzi + 1, nri + 1
+    nc = 3 if dynamic else 2
+    v = np.zeros((nc, nr, nz))
+    rows = [[float(x) for x in l.split()] for l in lines[pos:pos + nz * nr]]
+    k = 0
+    if swap:
+        for i in range(nz):
+            for j in range(nr):
+                r = rows[k]; k += 1
+                v[1, j, i], v[0, j, i] = r[0], r[1]
+                if dynamic:
+                    v[2, j, i] = r[2]
+    else:
+        for j in range(nr):
+            for i in range(nz):
+                r = rows[k]; k += 1
+                v[0, j, i], v[1, j, i] = r[0], r[1]
+                if dynamic:
+                    v[2, j, i] = r[3]
+    amax = float(np.max(np.abs(v[0, 0, :]))) if normalize else 1.0
+    if dynamic:
+        mu_0 = 1.256637061e-06
+        v[0] *= 1.e6 / amax
+        v[1] *= 1.e6 / amax
+        v[2] *= mu_0 / amax
+    elif normalize:
+        v[0] /= amax
+        v[1] /= amax
+    return dict(dynamic=dynamic, nz=nz, nr=nr, zbegin=zb / 100.0, zend=ze / 100.0, rbegin=rb / 100.0,
+                rend=re_ / 100.0, freq_mhz=freq, values=v)
+
+
+def _attach_map2d(e, m):
+    grid = np.ascontiguousarray(m["values"], dtype=np.float64)
+    e.map2d, e.nz, e.nr = 1, m["nz"], m["nr"]
+    e.hz = (m["zend"] - m["zbegin"]) / (m["nz"] - 1)
+    e.hr = (m["rend"] - m["rbegin"]) / (m["nr"] - 1)
+    e.grid = _ptr(grid)
+    e.zbegin, e.range = m["zbegin"], m["zend"] - m["zbegin"]
+    e._keep = grid  # the grid must outlive the element
+    return e
+
+
+def make_solenoid2d(m, edge, ks):
+    """SOLENOID with a 2D magnetostatic map (read_map2d) at ELEMEDGE, KS [T]."""
+    e = Solenoid()
+    e.kind, e.edge, e.scale = 0, edge, ks
+    return _attach_map2d(e, m)
+
+
+def make_rfcavity2d(m, edge, volt, freq_mhz, lag):
+    """RFCAVITY with a 2D dynamic map (read_map2d): VOLT [MV/m], FREQ [MHz],
+    LAG [rad]; the map's frequency replaces FREQ beyond 1 % (RFCavity.cpp:294-305)."""
+    e = Solenoid()
+    two_pi = 2 * 3.14159265358979323846
+    omega_map = m["freq_mhz"] * (two_pi * 1e6)
+    omega = 1e6 * two_pi * freq_mhz
+    if abs((omega - omega_map) / omega) > 0.01:
+        omega = omega_map
+    e.kind, e.edge, e.scale, e.omega, e.phase = 1, edge, volt, omega, lag
+    return _attach_map2d(e, m)
+
+
+def element_fields(element, R, t=0.0):
+    """E, B of one SOLENOID / RFCAVITY element with a 2D map at points R (element frame)."""
+    R = _f64(R)
+    E, B = np.zeros_like(R), np.zeros_like(R)
+    for i in range(R.shape[0]):
+        e, b = (C.c_double * 3)(), (C.c_double * 3)()
+        if element.kind == 1:
+            lib().sco_rfcavity2d_field(C.byref(element), R[i].ctypes.data_as(_dp), C.c_double(t), e, b)
+        else:
+            lib().sco_solenoid2d_field(C.byref(element), R[i].ctypes.data_as(_dp), b)
+        E[i], B[i] = list(e), list(b)
+    return E, B
+
+
 def multipole_field(element, R, ref_particle=False):
     """B [T] of one MULTIPOLE at points R (n x 3, element frame)."""
     R = _f64(R)
@@ -293,8 +412,14 @@ def rfcavity_field(element, R, t):
     return E, B
 
 
+_elements_keep = []
+
+
 def set_solenoids(elements):
-    """SOLENOID / RFCAVITY elements applied by the tracker (computeExternalFields)."""
+    """SOLENOID / RFCAVITY / MULTIPOLE elements applied by the tracker
+    (computeExternalFields)."""
+    global _elements_keep
+    _elements_keep = list(elements)  # their 2D grids stay alive while the tracker uses them
     arr = (Solenoid * max(len(elements), 1))(*elements)
     rc = lib().sco_set_solenoids(arr, C.c_int(len(elements)))
     if rc:

@@ -1663,12 +1663,89 @@ void sco_multipole_field(const sco_solenoid* e, const double* R, int ref_particl
     multipole_terms(k, ns, 1, R, B);
 }
 
+/* bilinear interpolation of component F on a 2D map (FM2DMagnetoStatic.cpp:
+ * 166-182, FM2DDynamic.cpp:195-210); absi: the magnetostatic map's abs() of
+ * the floored indices; returns 0 outside the grid */
+static int grid2d(const sco_solenoid* e, double RR, double z, int absi, int* i1, double* lr, double* lz) {
+    int indexr = (int)floor(RR / e->hr);
+    int indexz = (int)floor(z / e->hz);
+    if (absi) {
+        indexr = abs(indexr);
+        indexz = abs(indexz);
+    }
+    *lr = (RR / e->hr) - indexr;
+    *lz = (z / e->hz) - indexz;
+    if ((indexz < 0) || (indexz + 2 > e->nz)) return 0;
+    if (indexr + 2 > e->nr) return 0;
+    *i1 = indexz + indexr * e->nz;
+    return 1;
+}
+static double grid2d_at(const double* F, int index1, int nz, double leverr, double leverz) {
+    const int index2 = index1 + nz;
+    return (1.0 - leverz) * (1.0 - leverr) * F[index1]
+         + leverz         * (1.0 - leverr) * F[index1 + 1]
+         + (1.0 - leverz) * leverr         * F[index2]
+         + leverz         * leverr         * F[index2 + 1];
+}
+
+void sco_solenoid2d_field(const sco_solenoid* e, const double* R, double* B) {
+    B[0] = B[1] = B[2] = 0.0;
+    const double tmpR[3] = {R[0], R[1], R[2] - e->zbegin};
+    if (!(tmpR[2] >= 0.0 && tmpR[2] < e->range)) return;
+    const double RR = sqrt(tmpR[0] * tmpR[0] + tmpR[1] * tmpR[1]);
+    int i1;
+    double lr, lz;
+    if (!grid2d(e, RR, tmpR[2], 1, &i1, &lr, &lz)) return;
+    const size_t np = (size_t)e->nz * e->nr;
+    const double BfieldR = grid2d_at(e->grid + np, i1, e->nz, lr, lz);
+    const double BfieldZ = grid2d_at(e->grid, i1, e->nz, lr, lz);
+    double tmpB[3] = {0.0, 0.0, 0.0};
+    if (RR != 0) {
+        tmpB[0] += BfieldR * tmpR[0] / RR;
+        tmpB[1] += BfieldR * tmpR[1] / RR;
+    }
+    tmpB[2] += BfieldZ;
+    for (int d = 0; d < 3; ++d) B[d] += e->scale * tmpB[d];
+}
+
+void sco_rfcavity2d_field(const sco_solenoid* e, const double* R, double t, double* E, double* B) {
+    const double tmpR[3] = {R[0], R[1], R[2] - e->zbegin};
+    if (!(tmpR[2] >= 0.0 && tmpR[2] < e->range)) return;
+    const double RR = sqrt(tmpR[0] * tmpR[0] + tmpR[1] * tmpR[1]);
+    int i1;
+    double lr, lz;
+    if (!grid2d(e, RR, tmpR[2], 0, &i1, &lr, &lz)) return;
+    const size_t np = (size_t)e->nz * e->nr;
+    const double EfieldR = grid2d_at(e->grid + np, i1, e->nz, lr, lz);
+    const double EfieldZ = grid2d_at(e->grid, i1, e->nz, lr, lz);
+    const double BfieldT = grid2d_at(e->grid + 2 * np, i1, e->nz, lr, lz);
+    double tE[3] = {0.0, 0.0, 0.0}, tB[3] = {0.0, 0.0, 0.0};
+    if (RR > 1e-10) {
+        tE[0] += EfieldR * tmpR[0] / RR;
+        tE[1] += EfieldR * tmpR[1] / RR;
+        tB[0] -= BfieldT * tmpR[1] / RR;
+        tB[1] += BfieldT * tmpR[0] / RR;
+    }
+    tE[2] += EfieldZ;
+    const double c = e->scale * cos(e->omega * t + e->phase);
+    const double s = e->scale * sin(e->omega * t + e->phase);
+    for (int d = 0; d < 3; ++d) {
+        E[d] += c * tE[d];
+        B[d] -= s * tB[d];
+    }
+}
+
 /* one element's E (RF cavities) and B at R (element frame), time t */
 static void element_field(const sco_solenoid* e, const double* R, double t, int ref_particle, double* E, double* B) {
     E[0] = E[1] = E[2] = 0.0;
     if (e->kind == 1) {
         B[0] = B[1] = B[2] = 0.0;
-        sco_rfcavity_field(e, R, t, E, B);
+        if (e->map2d)
+            sco_rfcavity2d_field(e, R, t, E, B);
+        else
+            sco_rfcavity_field(e, R, t, E, B);
+    } else if (e->kind == 0 && e->map2d) {
+        sco_solenoid2d_field(e, R, B);
     } else if (e->kind == 2) {
         B[0] = B[1] = B[2] = 0.0;
         sco_multipole_field(e, R, ref_particle, B);

@@ -153,8 +153,11 @@ typedef struct {
     int kind;
     double omega, phase, xlrep; /* RF: angular frequency, LAG, map's omega / c */
     int nskew;      /* MULTIPOLE: skew components */
-    int pad_;
+    int map2d;      /* SOLENOID / RFCAVITY: 1 = a 2D (r, z) grid map */
     double aperture[2]; /* MULTIPOLE: elliptical aperture semi-axes [m] */
+    int nz, nr;         /* 2D map: grid points along z and r */
+    double hz, hr;      /* 2D map: spacings [m] */
+    const double* grid; /* 2D map: Bz, Br or Ez, Er, Bt, each nz nr values, z fastest */
     double coefs[255];  /* map coefficients; MULTIPOLE: normal, normal errors, skew, skew errors */
 } sco_solenoid;
 int sco_set_solenoids(const sco_solenoid* s, int n);
@@ -164,6 +167,11 @@ void sco_rfcavity_field(const sco_solenoid* e, const double* R, double t, double
  * computeField, :352-397 apply / applyToReferenceParticle): B at R (element
  * frame) added to B; ref_particle: components less their errors. */
 void sco_multipole_field(const sco_solenoid* e, const double* R, int ref_particle, double* B);
+/* SOLENOID with a 2D magnetostatic map (FM2DMagnetoStatic.cpp:158-189 with
+ * Solenoid::apply) and RFCAVITY with a 2D dynamic map (FM2DDynamic.cpp:
+ * 185-221 with RFCavity::apply): B (set) and E, B (added) at R, element frame */
+void sco_solenoid2d_field(const sco_solenoid* e, const double* R, double* B);
+void sco_rfcavity2d_field(const sco_solenoid* e, const double* R, double t, double* E, double* B);
 /* Multipole::setNormalComponent / setSkewComponent (Multipole.cpp:106-163):
  * the stored component of order n (1 = dipole) from KN (or KS) and its error;
  * *err receives the stored error. */

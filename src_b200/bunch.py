@@ -204,3 +204,79 @@ def write_rfcavity_map(path, accuracy=40, freq_mhz=1300.0, cells=2, npts=301, wi
         for zi, ei in zip(z, ez):
             f.write(f"{zi:.17g} {ei:.17g}\n")
     return z, ez
+
+
+def write_2d_solenoid_map(path, orientation="XZ", normalize=None, length=0.3, radius=0.04, nz=120, nr=20, b0=1.0,
+                          edge=0.04, width=0.012, comment=True):
+    """A seeded synthetic solenoid in OPAL's 2DMagnetoStatic format on an
+    (r, z) grid (cm): the on-axis field of a tanh-edged coil, Bz(z), with its
+    paraxial off-axis expansion Bz = Bz0 - r^2/4 Bz0'', Br = -r/2 Bz0'.
+    Stands in for the reference examples' 2D maps, which are not shipped
+    here.  orientation "XZ" (r-major "Bz Br" lines) or "ZX" (z-major
+    "Br Bz"); normalize None writes no flag, else TRUE / FALSE.  Returns z, r
+    [m] and the arrays [r, z]."""
+    z = np.linspace(0.0, length, nz + 1)
+    r = np.linspace(0.0, radius, nr + 1)
+    t1, t2 = np.tanh((z - edge) / width), np.tanh((z - (length - edge)) / width)
+    bz0 = 0.5 * b0 * (t1 - t2)
+    s1, s2 = 1 - t1 ** 2, 1 - t2 ** 2
+    d1 = 0.5 * b0 * (s1 - s2) / width
+    d2 = 0.5 * b0 * (-2 * t1 * s1 + 2 * t2 * s2) / width ** 2
+    R, _ = np.meshgrid(r, z, indexing="ij")
+    BZ = bz0[None, :] - R ** 2 / 4 * d2[None, :]
+    BR = -R / 2 * d1[None, :]
+    flag = "" if normalize is None else (" TRUE" if normalize else " FALSE")
+    with open(path, "w") as f:
+        f.write(f"2DMagnetoStatic {orientation}{flag}\n")
+        if comment:
+            f.write("# synthetic coil: z and r in cm, B in T\n")
+        if orientation == "XZ":
+            f.write(f"{0.0:.17g} {100 * length:.17g} {nz}\n{0.0:.17g} {100 * radius:.17g} {nr}\n")
+            for j in range(nr + 1):
+                for i in range(nz + 1):
+                    f.write(f"{BZ[j, i]:.17g} {BR[j, i]:.17g}\n")
+        else:
+            f.write(f"{0.0:.17g} {100 * radius:.17g} {nr}\n{0.0:.17g} {100 * length:.17g} {nz}\n")
+            for i in range(nz + 1):
+                for j in range(nr + 1):
+                    f.write(f"{BR[j, i]:.17g} {BZ[j, i]:.17g}\n")
+    return z, r, BZ, BR
+
+
+def write_2d_rfcavity_map(path, orientation="XZ", normalize=None, freq_mhz=1300.0, cells=2, radius=0.03, nz=160,
+                          nr=24, comment=True):
+    """A seeded synthetic standing-wave cavity in OPAL's 2DDynamic format on
+    an (r, z) grid (cm; E in MV/m, H in A/m): `cells` pi-mode cells of length
+    c / (2 f), Ez = sin(pi z / cell) J0-like in r (1 - (k r)^2 / 4),
+    Er = -r/2 dEz/dz, H_theta = (omega eps0 r / 2) Ez.  orientation "XZ"
+    (r-major "Ez Er |E| Ht") or "ZX" (z-major "Er Ez Ht |E|").  Returns z, r
+    [m] and the arrays [r, z]."""
+    c = 299792458.0
+    cell = c / (2.0 * freq_mhz * 1e6)
+    length = cells * cell
+    k = 2 * np.pi * freq_mhz * 1e6 / c
+    z = np.linspace(0.0, length, nz + 1)
+    r = np.linspace(0.0, radius, nr + 1)
+    R, Z = np.meshgrid(r, z, indexing="ij")
+    ez0 = np.sin(np.pi * Z / cell)
+    dez0 = np.pi / cell * np.cos(np.pi * Z / cell)
+    EZ = ez0 * (1 - (k * R) ** 2 / 4)
+    ER = -R / 2 * dez0
+    HT = 2 * np.pi * freq_mhz * 1e6 * 8.854187817e-12 * R / 2 * ez0 * 1e6  # A/m of the MV/m field
+    EA = np.sqrt(EZ ** 2 + ER ** 2)
+    flag = "" if normalize is None else (" TRUE" if normalize else " FALSE")
+    with open(path, "w") as f:
+        f.write(f"2DDynamic {orientation}{flag}\n")
+        if comment:
+            f.write("# synthetic cavity: z and r in cm, E in MV/m, H in A/m\n")
+        if orientation == "XZ":
+            f.write(f"{0.0:.17g} {100 * length:.17g} {nz}\n{freq_mhz:.17g}\n{0.0:.17g} {100 * radius:.17g} {nr}\n")
+            for j in range(nr + 1):
+                for i in range(nz + 1):
+                    f.write(f"{EZ[j, i]:.17g} {ER[j, i]:.17g} {EA[j, i]:.17g} {HT[j, i]:.17g}\n")
+        else:
+            f.write(f"{0.0:.17g} {100 * radius:.17g} {nr}\n{freq_mhz:.17g}\n{0.0:.17g} {100 * length:.17g} {nz}\n")
+            for i in range(nz + 1):
+                for j in range(nr + 1):
+                    f.write(f"{ER[j, i]:.17g} {EZ[j, i]:.17g} {HT[j, i]:.17g} {EA[j, i]:.17g}\n")
+    return z, r, EZ, ER, HT

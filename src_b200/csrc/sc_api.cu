@@ -664,6 +664,7 @@ void scgpu_destroy(scgpu_ctx* c) {
     free_particles(c);
     free_bins(c);
     dfree(c->d_elements);
+    for (double*& g : c->map_grids) dfree(g);
     DevBunch& b = c->b;
     dfree(b.nacc); dfree(b.rho); dfree(b.phi); dfree(b.E4); dfree(b.spec); dfree(b.spec_lo);
     dfree(b.gtmp); dfree(b.gline); dfree(b.ghat); dfree(b.st); dfree(b.partials); dfree(b.ticket);
@@ -814,11 +815,52 @@ static int upload_elements(scgpu_ctx* c) {
     return SCGPU_OK;
 }
 
+// A 2D map's grid on the device, referenced by the element (freed with the
+// context's elements).  want_dynamic: the element needs a dynamic (RF) map.
+static int attach_map2d(scgpu_ctx* c, const char* path, bool want_dynamic, MapElem& e, double* freq_mhz) {
+    bool dynamic = false;
+    int nz = 0, nr = 0;
+    double zb = 0, ze = 0, rb = 0, re = 0, f = 0;
+    std::vector<double> v;
+    int rc = fieldmap_2d(path, &dynamic, &nz, &nr, &zb, &ze, &rb, &re, &f, &v);
+    if (rc) return fail(c, rc, std::string("cannot read the field map ") + path);
+    if (dynamic != want_dynamic)
+        return fail(c, SCGPU_ERR_ARG, std::string("the field map ") + path +
+                                          (want_dynamic ? " is not a dynamic map" : " is not a magnetostatic map"));
+    if (nz < 2 || nr < 2 || !(ze > zb) || !(re > rb)) return fail(c, SCGPU_ERR_ARG, "a 2D map needs two points per axis");
+    CK(cudaSetDevice(c->device));
+    double* d = nullptr;
+    rc = dalloc(c, &d, v.size() * sizeof(double));
+    if (rc) return rc;
+    CK(cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->map_grids.push_back(d);
+    e.map2d = 1;
+    e.nz = nz;
+    e.nr = nr;
+    e.hz = (ze - zb) / (nz - 1);  // FM2D*: (zend - zbegin) / intervals
+    e.hr = (re - rb) / (nr - 1);
+    e.grid = d;
+    e.zbegin = zb;  // Solenoid / RFCavity::initialise: startField = zBegin, length = zEnd - zBegin
+    e.range = ze - zb;
+    if (freq_mhz) *freq_mhz = f;
+    return SCGPU_OK;
+}
+
 int scgpu_add_solenoid(scgpu_ctx* c, const char* fieldmap, double elemedge, double ks) {
     if (!c || !fieldmap) return fail(c, SCGPU_ERR_ARG, "null argument");
     if (!std::isfinite(elemedge) || !std::isfinite(ks)) return fail(c, SCGPU_ERR_ARG, "ELEMEDGE and KS must be finite");
     if ((int)c->elements.size() >= kMaxElements) return fail(c, SCGPU_ERR_UNSUPPORTED, "at most 8 elements");
     MapElem e{};
+    if (fieldmap_is_2d(fieldmap)) {
+        int rc = attach_map2d(c, fieldmap, false, e, nullptr);
+        if (rc) return rc;
+        e.edge = elemedge;
+        e.scale = ks;
+        e.kind = kElemSolenoid;
+        CK(cudaStreamSynchronize(c->stream));
+        c->elements.push_back(e);
+        return upload_elements(c);
+    }
     int ncoef = 0;
     int rc = scgpu_fieldmap_astra1d(fieldmap, e.coefs, kMaxSolCoefs, &ncoef, &e.zbegin, &e.range, &e.period);
     if (rc) return fail(c, rc, std::string("cannot read the field map ") + fieldmap);
@@ -846,13 +888,19 @@ int scgpu_add_rfcavity(scgpu_ctx* c, const char* fieldmap, double elemedge, doub
         return fail(c, SCGPU_ERR_ARG, "ELEMEDGE, VOLT and LAG must be finite and FREQ positive");
     if ((int)c->elements.size() >= kMaxElements) return fail(c, SCGPU_ERR_UNSUPPORTED, "at most 8 elements");
     MapElem e{};
-    int ncoef = 0;
     double fmap = 0.0;
-    int rc = scgpu_fieldmap_astra1d_dynamic(fieldmap, e.coefs, kMaxSolCoefs, &ncoef, &e.zbegin, &e.range, &e.period,
-                                            &fmap);
-    if (rc) return fail(c, rc, std::string("cannot read the field map ") + fieldmap);
-    e.range = e.range - e.zbegin;  // zend - zbegin
-    e.accuracy = (ncoef + 1) / 2;
+    if (fieldmap_is_2d(fieldmap)) {
+        int rc = attach_map2d(c, fieldmap, true, e, &fmap);
+        if (rc) return rc;
+        if (!(fmap > 0.0)) return fail(c, SCGPU_ERR_ARG, "the 2D map's frequency must be positive");
+    } else {
+        int ncoef = 0;
+        int rc = scgpu_fieldmap_astra1d_dynamic(fieldmap, e.coefs, kMaxSolCoefs, &ncoef, &e.zbegin, &e.range, &e.period,
+                                                &fmap);
+        if (rc) return fail(c, rc, std::string("cannot read the field map ") + fieldmap);
+        e.range = e.range - e.zbegin;  // zend - zbegin
+        e.accuracy = (ncoef + 1) / 2;
+    }
     e.edge = elemedge;
     e.scale = volt_mv_per_m;
     e.kind = kElemRfCavity;
@@ -937,6 +985,8 @@ int scgpu_clear_elements(scgpu_ctx* c) {
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     c->elements.clear();
+    for (double*& g : c->map_grids) dfree(g);
+    c->map_grids.clear();
     return upload_elements(c);
 }
 

@@ -121,8 +121,13 @@ struct MapElem {
     double phase;   // RF: LAG [rad]
     double xlrep;   // RF: the map's angular frequency / c [1/m]
     int nskew;      // MULTIPOLE: skew components
-    int pad_;
+    int map2d;      // SOLENOID / RFCAVITY: 1 for a 2D (r, z) grid map in place of the 1D series
     double aperture[2];  // MULTIPOLE: semi-axes of the elliptical aperture [m]
+    // 2D map: grid points along z and r, spacings, and the device grid
+    // (Bz, Br or Ez, Er, Bt, each nz nr values, z fastest)
+    int nz, nr;
+    double hz, hr;
+    const double* grid;
     // map: Fourier coefficients; MULTIPOLE: normal components, their errors,
     // skew components, their errors (accuracy, accuracy, nskew, nskew values)
     double coefs[kMaxSolCoefs];
@@ -370,6 +375,84 @@ SC_HD void rfcavity_field(const MapElem& e, const double* R, double t, double* E
     B[2] -= sb * tB[2];
 }
 
+// Bilinear interpolation on a 2D (r, z) map at distance RR from the axis and
+// height z above the map's start (FM2DMagnetoStatic.cpp:170-186,
+// FM2DDynamic.cpp:192-212): false outside the grid.  ABSI: the magnetostatic
+// map takes the absolute value of the floored indices.
+template <bool ABSI>
+SC_HD bool grid2d_cell(const MapElem& e, double RR, double z, int& i1, double& lr, double& lz) {
+    int ir = (int)floor(RR / e.hr);
+    int iz = (int)floor(z / e.hz);
+    if (ABSI) {
+        ir = ir < 0 ? -ir : ir;
+        iz = iz < 0 ? -iz : iz;
+    }
+    lr = ABSI ? (RR / e.hr) - ir : RR / e.hr - ir;
+    lz = ABSI ? (z / e.hz) - iz : z / e.hz - iz;
+    if (iz < 0 || iz + 2 > e.nz) return false;
+    if (ir + 2 > e.nr) return false;  // out of the map radially: the reference loses the particle
+    i1 = iz + ir * e.nz;
+    return true;
+}
+SC_HD double grid2d_value(const double* F, int i1, int nz, double lr, double lz) {
+    const int i2 = i1 + nz;
+    return (1.0 - lz) * (1.0 - lr) * F[i1] + lz * (1.0 - lr) * F[i1 + 1] + (1.0 - lz) * lr * F[i2] + lz * lr * F[i2 + 1];
+}
+
+// FM2DMagnetoStatic::getFieldstrength and Solenoid::apply: B = KS (Br x/r,
+// Br y/r, Bz) inside [zbegin, zbegin + range).
+SC_HD void solenoid2d_field(const MapElem& e, const double* R, double* B) {
+    const double tz = R[2] - e.zbegin;
+    if (!(tz >= 0.0 && tz < e.range)) return;
+    const double RR = sqrt(R[0] * R[0] + R[1] * R[1]);
+    int i1;
+    double lr, lz;
+    if (!grid2d_cell<true>(e, RR, tz, i1, lr, lz)) return;
+    const size_t np = (size_t)e.nz * e.nr;
+    const double BfieldR = grid2d_value(e.grid + np, i1, e.nz, lr, lz);
+    const double BfieldZ = grid2d_value(e.grid, i1, e.nz, lr, lz);
+    double tB[3] = {0.0, 0.0, 0.0};
+    if (RR != 0) {
+        tB[0] += BfieldR * R[0] / RR;
+        tB[1] += BfieldR * R[1] / RR;
+    }
+    tB[2] += BfieldZ;
+    B[0] += e.scale * tB[0];
+    B[1] += e.scale * tB[1];
+    B[2] += e.scale * tB[2];
+}
+
+// FM2DDynamic::getFieldstrength and RFCavity::apply: E += VOLT cos(omega t +
+// LAG) (Er x/r, Er y/r, Ez), B -= VOLT sin(omega t + LAG) (-Bt y/r, Bt x/r, 0).
+SC_HD void rfcavity2d_field(const MapElem& e, const double* R, double t, double* E, double* B) {
+    const double tz = R[2] - e.zbegin;
+    if (!(tz >= 0.0 && tz < e.range)) return;
+    const double RR = sqrt(R[0] * R[0] + R[1] * R[1]);
+    int i1;
+    double lr, lz;
+    if (!grid2d_cell<false>(e, RR, tz, i1, lr, lz)) return;
+    const size_t np = (size_t)e.nz * e.nr;
+    const double EfieldR = grid2d_value(e.grid + np, i1, e.nz, lr, lz);
+    const double EfieldZ = grid2d_value(e.grid, i1, e.nz, lr, lz);
+    const double BfieldT = grid2d_value(e.grid + 2 * np, i1, e.nz, lr, lz);
+    double tE[3] = {0.0, 0.0, 0.0}, tB[3] = {0.0, 0.0, 0.0};
+    if (RR > 1e-10) {
+        tE[0] += EfieldR * R[0] / RR;
+        tE[1] += EfieldR * R[1] / RR;
+        tB[0] -= BfieldT * R[1] / RR;
+        tB[1] += BfieldT * R[0] / RR;
+    }
+    tE[2] += EfieldZ;
+    const double arg = e.omega * t + e.phase;
+    const double ce = e.scale * cos(arg), sb = e.scale * sin(arg);
+    E[0] += ce * tE[0];
+    E[1] += ce * tE[1];
+    E[2] += ce * tE[2];
+    B[0] -= sb * tB[0];
+    B[1] -= sb * tB[1];
+    B[2] -= sb * tB[2];
+}
+
 // Multipole::computeField (Multipole.cpp:229-349): the normal components
 // c[0..nn), then the skew components s[0..ns), each order's term added to
 // B_x, B_y in the reference's expression order (special forms for the
@@ -492,13 +575,18 @@ SC_HD void add_external_fields(const MapElem* el, int n, const Trafo& ref_to_lab
         loc[1] = lab[1] - 0.0;
         loc[2] = lab[2] - el[k].edge;
         if (el[k].kind == kElemRfCavity) {
-            rfcavity_field(el[k], loc, t, El, Bl);
+            if (el[k].map2d)
+                rfcavity2d_field(el[k], loc, t, El, Bl);
+            else
+                rfcavity_field(el[k], loc, t, El, Bl);
             trafo_rotate_from(ref_to_lab, El, Er);
             Ef[0] += Er[0];
             Ef[1] += Er[1];
             Ef[2] += Er[2];
         } else if (el[k].kind == kElemMultipole) {
             multipole_field(el[k], loc, ref_particle, Bl);
+        } else if (el[k].map2d) {
+            solenoid2d_field(el[k], loc, Bl);
         } else {
             solenoid_field(el[k], loc, Bl);
         }

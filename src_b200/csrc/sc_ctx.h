@@ -48,6 +48,7 @@ struct scgpu_ctx {
     // beamline elements (scgpu_add_solenoid): host copy and device table
     std::vector<sc::MapElem> elements;
     sc::MapElem* d_elements = nullptr;
+    std::vector<double*> map_grids;  // device grids of the elements' 2D maps
     // sharded bunch (scgpu_set_exchange): this context holds one rank's shard
     scgpu_exchange_fn xfn = nullptr;
     void* xuser = nullptr;

@@ -14,6 +14,8 @@
 // frequency in MHz, then lines "z Ez(z)"; the same resampling, mirroring and
 // series, normalised to the largest |Ez| and scaled by 1e6 (MV/m to V/m).
 //
+// 2D maps on an (r, z) grid: see read_map2d.
+//
 // Host C++ only (no CUDA); the evaluation is in sc_common.cuh.
 #include <cctype>
 #include <cmath>
@@ -26,9 +28,12 @@
 
 namespace {
 
-// One content line: '#' starts a comment; lines without an alphanumeric
-// character are skipped; surrounding blanks removed (Fieldmap::getLine,
-// Fieldmap.cpp:519-541).
+// One content line: '#' starts a comment; lines without a character of the
+// reference's set (letters, digits, ". - +" and the byte 0x89) are skipped;
+// the line is cut to its first and last such character (Fieldmap::getLine,
+// Fieldmap.cpp:519-541, alpha_numeric :802), so a leading sign stays.
+bool map_char(unsigned char ch) { return std::isalnum(ch) || ch == '.' || ch == '-' || ch == '+' || ch == 0x89; }
+
 bool content_line(std::ifstream& in, std::string& out) {
     std::string line;
     while (std::getline(in, line)) {
@@ -36,7 +41,7 @@ bool content_line(std::ifstream& in, std::string& out) {
         if (hash != std::string::npos) line.erase(hash);
         size_t first = std::string::npos, last = std::string::npos;
         for (size_t i = 0; i < line.size(); ++i)
-            if (std::isalnum((unsigned char)line[i])) {
+            if (map_char((unsigned char)line[i])) {
                 if (first == std::string::npos) first = i;
                 last = i;
             }
@@ -179,9 +184,195 @@ int read_astra1d(const char* path, bool dynamic, double* coefs, int max_coefs, i
     return SCGPU_OK;
 }
 
+// 2D maps on an (r, z) grid, as FM2DMagnetoStatic and FM2DDynamic read them
+// (src/Classic/Fields/FM2DMagnetoStatic.cpp: constructor :14-95, readMap
+// :101-155; FM2DDynamic.cpp: constructor :15-104, readMap :110-170): a header
+// "2DMagnetoStatic XZ|ZX [TRUE|FALSE]" or "2DDynamic XZ|ZX [TRUE|FALSE]";
+// for XZ the lines "zbegin zend nz", (dynamic: the frequency in MHz),
+// "rbegin rend nr" in cm and intervals, then (nz+1)(nr+1) value lines, r
+// outer and z inner: "Bz Br" or "Ez Er - Ht"; for ZX the r line first and
+// z outer, "Br Bz" or "Er Ez Ht -".  Lengths become m, counts become grid
+// points; unless FALSE the values are divided by the largest |Bz| (|Ez|) on
+// the axis; a dynamic map's E goes from MV/m to V/m (x 1e6 / Ezmax) and its
+// H to B (x mu_0 / Ezmax, mu_0 = 1.256637061e-06 as Physics.h:55).
+// values: component c at grid point (z i, r j) at values[(c nr + j) nz + i],
+// components Bz, Br or Ez, Er, Bt.
+struct Map2D {
+    bool dynamic = false;
+    int nz = 0, nr = 0;  // grid points
+    double zbegin = 0, zend = 0, rbegin = 0, rend = 0, freq_mhz = 0;
+    std::vector<double> v;
+};
+
+bool numbers(const std::string& s, double* out, int n) {
+    std::istringstream is(s);
+    for (int k = 0; k < n; ++k)
+        if (!(is >> out[k])) return false;
+    std::string rest;
+    return !(is >> rest);
+}
+
+bool range_line(std::ifstream& in, double& a, double& b, int& n) {
+    std::string line;
+    if (!content_line(in, line)) return false;
+    std::istringstream is(line);
+    std::string rest;
+    if (!(is >> a >> b >> n) || (is >> rest)) return false;
+    return n >= 1;
+}
+
+int read_map2d(const char* path, Map2D& m) {
+    if (!path) return SCGPU_ERR_ARG;
+    std::ifstream in(path);
+    if (!in) return SCGPU_ERR_ARG;
+    std::string line;
+    if (!content_line(in, line)) return SCGPU_ERR_ARG;
+    std::istringstream hs(line);
+    std::string name, orient, flag;
+    if (!(hs >> name >> orient)) return SCGPU_ERR_ARG;
+    if (name.compare(0, 4, "2DMa") == 0)
+        m.dynamic = false;
+    else if (name.compare(0, 4, "2DDy") == 0)
+        m.dynamic = true;
+    else
+        return SCGPU_ERR_ARG;
+    bool normalize = true;
+    if (hs >> flag) {
+        for (char& ch : flag) ch = (char)std::toupper((unsigned char)ch);
+        if (flag != "TRUE" && flag != "FALSE") return SCGPU_ERR_ARG;
+        normalize = flag == "TRUE";
+    }
+    const bool swap = orient == "ZX";
+    if (!swap && orient != "XZ") return SCGPU_ERR_ARG;
+    int nzi = 0, nri = 0;
+    auto freq = [&]() {
+        if (!m.dynamic) return true;
+        if (!content_line(in, line)) return false;
+        double f = 0.0;
+        return numbers(line, &f, 1) && (m.freq_mhz = f, true);
+    };
+    if (swap) {
+        if (!range_line(in, m.rbegin, m.rend, nri) || !freq() || !range_line(in, m.zbegin, m.zend, nzi))
+            return SCGPU_ERR_ARG;
+    } else {
+        if (!range_line(in, m.zbegin, m.zend, nzi) || !freq() || !range_line(in, m.rbegin, m.rend, nri))
+            return SCGPU_ERR_ARG;
+    }
+    m.nz = nzi + 1;
+    m.nr = nri + 1;
+    const int nc = m.dynamic ? 3 : 2;
+    const size_t np = (size_t)m.nz * m.nr;
+    if (np > ((size_t)1 << 26)) return SCGPU_ERR_ARG;
+    m.v.assign(nc * np, 0.0);
+    double* A = m.v.data();  // Bz or Ez
+    double* B = A + np;      // Br or Er
+    double* T = A + 2 * np;  // Bt (dynamic)
+    double x[4];
+    const int per = m.dynamic ? 4 : 2;
+    for (size_t k = 0; k < np; ++k) {
+        if (!content_line(in, line) || !numbers(line, x, per)) return SCGPU_ERR_ARG;
+        size_t i, j;  // z, r
+        if (swap) {
+            i = k / m.nr;
+            j = k % m.nr;
+        } else {
+            j = k / m.nz;
+            i = k % m.nz;
+        }
+        const size_t at = i + j * m.nz;
+        if (swap) {
+            B[at] = x[0];
+            A[at] = x[1];
+            if (m.dynamic) T[at] = x[2];
+        } else {
+            A[at] = x[0];
+            B[at] = x[1];
+            if (m.dynamic) T[at] = x[3];
+        }
+    }
+    if (content_line(in, line)) return SCGPU_ERR_ARG;  // interpreteEOF: nothing after the values
+    m.rbegin /= 100.0;
+    m.rend /= 100.0;
+    m.zbegin /= 100.0;
+    m.zend /= 100.0;
+    double amax = 0.0;
+    if (normalize) {
+        for (int i = 0; i < m.nz; ++i)
+            if (std::abs(A[i]) > amax) amax = std::abs(A[i]);
+        if (!(amax > 0.0)) return SCGPU_ERR_ARG;
+    } else {
+        amax = 1.0;
+    }
+    if (m.dynamic) {
+        const double mu_0 = 1.256637061e-06;
+        for (size_t k = 0; k < np; ++k) {
+            A[k] *= 1.e6 / amax;
+            B[k] *= 1.e6 / amax;
+            T[k] *= mu_0 / amax;
+        }
+    } else if (normalize) {
+        for (size_t k = 0; k < np; ++k) {
+            A[k] /= amax;
+            B[k] /= amax;
+        }
+    }
+    return SCGPU_OK;
+}
+
 }  // namespace
 
+namespace sc {
+// the map's type from its first word, as Fieldmap::readHeader does
+// (Fieldmap.cpp:296-335, the first four characters)
+bool fieldmap_is_2d(const char* path) {
+    if (!path) return false;
+    std::ifstream in(path);
+    std::string line;
+    if (!in || !content_line(in, line)) return false;
+    return line.compare(0, 4, "2DMa") == 0 || line.compare(0, 4, "2DDy") == 0;
+}
+
+// the map for the element table (sc_api.cu)
+int fieldmap_2d(const char* path, bool* dynamic, int* nz, int* nr, double* zbegin, double* zend, double* rbegin,
+                double* rend, double* freq_mhz, std::vector<double>* values) {
+    Map2D m;
+    const int rc = read_map2d(path, m);
+    if (rc) return rc;
+    *dynamic = m.dynamic;
+    *nz = m.nz;
+    *nr = m.nr;
+    *zbegin = m.zbegin;
+    *zend = m.zend;
+    *rbegin = m.rbegin;
+    *rend = m.rend;
+    *freq_mhz = m.freq_mhz;
+    values->swap(m.v);
+    return SCGPU_OK;
+}
+}  // namespace sc
+
 extern "C" {
+
+int scgpu_fieldmap_2d(const char* path, int* dynamic, int* nz, int* nr, double* ranges, double* frequency_mhz,
+                      double* values, long long capacity) {
+    if (!path || !dynamic || !nz || !nr || !ranges || !frequency_mhz) return SCGPU_ERR_ARG;
+    Map2D m;
+    const int rc = read_map2d(path, m);
+    if (rc) return rc;
+    *dynamic = m.dynamic ? 1 : 0;
+    *nz = m.nz;
+    *nr = m.nr;
+    ranges[0] = m.zbegin;
+    ranges[1] = m.zend;
+    ranges[2] = m.rbegin;
+    ranges[3] = m.rend;
+    *frequency_mhz = m.freq_mhz;
+    if (values) {
+        if (capacity < (long long)m.v.size()) return SCGPU_ERR_ARG;
+        for (size_t k = 0; k < m.v.size(); ++k) values[k] = m.v[k];
+    }
+    return SCGPU_OK;
+}
 
 int scgpu_fieldmap_astra1d(const char* path, double* coefs, int max_coefs, int* ncoefs, double* zbegin, double* zend,
                            double* period) {

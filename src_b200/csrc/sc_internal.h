@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "sc_common.cuh"
@@ -83,6 +84,12 @@ FftPlan make_plan(int L);
 // SCGPU_ERR_ARG instead of an illegal-address fault on the GPU.  *why says
 // what is wrong.
 bool device_buffer_ok(const void* p, size_t bytes, int device, std::string* why);
+// a 2D (r, z) field map (sc_fieldmap.cpp): grid points, ranges [m], the
+// frequency [MHz] of a dynamic map, and the values (Bz, Br or Ez, Er, Bt)
+int fieldmap_2d(const char* path, bool* dynamic, int* nz, int* nr, double* zbegin, double* zend, double* rbegin,
+                double* rend, double* freq_mhz, std::vector<double>* values);
+// true when the map file's first word names a 2D map (2DMagnetoStatic / 2DDynamic)
+bool fieldmap_is_2d(const char* path);
 int particle_grid(const DevBunch& b);
 void prime_particle_grids();  // occupancy of the particle kernels, before any capture
 

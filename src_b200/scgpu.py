@@ -117,6 +117,8 @@ def lib():
         L.scgpu_clear_elements.argtypes = [C.c_void_p]
         L.scgpu_fieldmap_astra1d.argtypes = [C.c_char_p, _dp, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp]
         L.scgpu_add_rfcavity.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.scgpu_fieldmap_2d.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), _dp,
+                                        _dp, _dp, C.c_longlong]
         L.scgpu_add_multipole.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp, C.c_int, _dp, _dp, C.c_int, _dp]
         L.scgpu_fieldmap_astra1d_dynamic.argtypes = [C.c_char_p, _dp, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
         L.scgpu_stat_row.argtypes = [C.c_void_p, _dp]
@@ -144,7 +146,7 @@ EXPORTED = [
     "scgpu_sdds_append_row", "scgpu_read_fromfile_count", "scgpu_read_fromfile", "scgpu_write_fromfile",
     "scgpu_set_periodic_z", "scgpu_set_exchange", "scgpu_add_solenoid", "scgpu_clear_elements",
     "scgpu_fieldmap_astra1d", "scgpu_add_rfcavity", "scgpu_fieldmap_astra1d_dynamic", "scgpu_set_reorder_interval",
-    "scgpu_launch_count", "scgpu_set_beam_frequency", "scgpu_add_multipole",
+    "scgpu_launch_count", "scgpu_set_beam_frequency", "scgpu_add_multipole", "scgpu_fieldmap_2d",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
@@ -611,6 +613,25 @@ def fieldmap_astra1d(path):
     if rc != 0:
         raise ScgpuError(rc, f"cannot read the field map {path}")
     return coefs[:n.value].copy(), zb.value, ze.value, per.value
+
+
+def fieldmap_2d(path):
+    """A 2D (r, z) map as the library reads it: dict with dynamic, nz, nr,
+    zbegin, zend, rbegin, rend [m], freq_mhz and values [component, r, z]."""
+    dyn, nz, nr = C.c_int(), C.c_int(), C.c_int()
+    ranges = (C.c_double * 4)()
+    f = C.c_double()
+    rc = lib().scgpu_fieldmap_2d(os.fsencode(path), C.byref(dyn), C.byref(nz), C.byref(nr), ranges, C.byref(f), None, 0)
+    if rc:
+        raise ScgpuError(rc, f"fieldmap_2d: cannot read {path}")
+    nc = 3 if dyn.value else 2
+    v = np.empty((nc, nr.value, nz.value))
+    rc = lib().scgpu_fieldmap_2d(os.fsencode(path), C.byref(dyn), C.byref(nz), C.byref(nr), ranges, C.byref(f),
+                                 _p(v), v.size)
+    if rc:
+        raise ScgpuError(rc, f"fieldmap_2d: cannot read {path}")
+    return dict(dynamic=bool(dyn.value), nz=nz.value, nr=nr.value, zbegin=ranges[0], zend=ranges[1], rbegin=ranges[2],
+                rend=ranges[3], freq_mhz=f.value, values=v)
 
 
 def fieldmap_astra1d_dynamic(path):

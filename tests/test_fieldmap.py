@@ -157,3 +157,90 @@ def test_rfcavity_expansion_is_divergence_free(sg, oracle, tmp_path):
         dez = (g(r, zq + h)[2] - g(r, zq - h)[2]) / (2 * h)
         drer = ((r + h) * g(r + h, zq)[0] - (r - h) * g(r - h, zq)[0]) / (2 * h)
         assert abs(dez + drer / r) < 1e-4 * max(abs(dez), 1e6)
+
+
+def test_reader_keeps_leading_signs(sg, tmp_path):
+    """Fieldmap::getLine cuts a line to its first and last letter, digit or
+    '. - +' (Fieldmap.cpp:519-541, :802): a map starting at negative z."""
+    path = tmp_path / "sol.txt"
+    path.write_text("AstraMagnetostatic 3 FALSE\n-0.1 0.5\n  -0.05 1.0\n+0.0 0.5\n.05 -0.25\n")
+    c, zb, ze, per = sg.fieldmap_astra1d(path)
+    assert zb == -0.1 and ze == 0.05
+    ref, _ = _recipe(np.array([-0.1, -0.05, 0.0, 0.05]), np.array([0.5, 1.0, 0.5, -0.25]), 3)
+    np.testing.assert_allclose(c, ref * 1.0, rtol=0, atol=1e-15)
+
+
+# ---------------------------------------------------------------- 2D maps
+# FM2DMagnetoStatic / FM2DDynamic (src/Classic/Fields/FM2D*.cpp): the
+# library's reader against the oracle's restatement, both orientations and
+# normalisation flags; the oracle's bilinear field against numpy.
+
+@pytest.mark.parametrize("orient", ["XZ", "ZX"])
+@pytest.mark.parametrize("normalize", [None, True, False])
+def test_2d_readers_agree(sg, oracle, tmp_path, orient, normalize):
+    from src_b200.bunch import write_2d_rfcavity_map, write_2d_solenoid_map
+    for kind, writer in (("s", write_2d_solenoid_map), ("c", write_2d_rfcavity_map)):
+        path = tmp_path / f"{kind}.txt"
+        writer(path, orient, normalize)
+        a, b = sg.fieldmap_2d(path), oracle.read_map2d(path)
+        for key in ("dynamic", "nz", "nr", "zbegin", "zend", "rbegin", "rend", "freq_mhz"):
+            assert a[key] == b[key], key
+        np.testing.assert_array_equal(a["values"], b["values"])
+        assert a["dynamic"] == (kind == "c")
+        if normalize is not False:  # normalised to the largest |Bz| (|Ez| in V/m) on the axis
+            top = np.abs(a["values"][0, 0]).max()
+            assert top == (1e6 if kind == "c" else 1.0)
+
+
+def test_2d_reader_errors(sg, tmp_path):
+    path = tmp_path / "bad.txt"
+    for text in ("2DMagnetoStatic YZ\n0 1 1\n0 1 1\n1 0\n1 0\n1 0\n1 0\n",  # orientation
+                 "2DMagnetoStatic XZ\n0 1 1\n0 1 1\n1 0\n1 0\n1 0\n",      # a value line short
+                 "2DMagnetoStatic XZ\n0 1 1\n0 1 1\n1 0\n1 0\n1 0\n1 0\n1 0\n",  # one too many
+                 "2DMagnetoStatic XZ MAYBE\n0 1 1\n0 1 1\n1 0\n1 0\n1 0\n1 0\n"):
+        path.write_text(text)
+        with pytest.raises(sg.ScgpuError):
+            sg.fieldmap_2d(path)
+
+
+def _bilinear(F, hz, hr, z, rr):
+    iz, ir = np.floor(z / hz).astype(int), np.floor(rr / hr).astype(int)
+    lz, lr = z / hz - iz, rr / hr - ir
+    return ((1 - lz) * (1 - lr) * F[ir, iz] + lz * (1 - lr) * F[ir, iz + 1] + (1 - lz) * lr * F[ir + 1, iz]
+            + lz * lr * F[ir + 1, iz + 1])
+
+
+def test_2d_fields_against_bilinear(oracle, tmp_path):
+    from src_b200.bunch import write_2d_rfcavity_map, write_2d_solenoid_map
+    rng = np.random.default_rng(2)
+    ps, pc = tmp_path / "s.txt", tmp_path / "c.txt"
+    write_2d_solenoid_map(ps)
+    write_2d_rfcavity_map(pc)
+    ms, mc = oracle.read_map2d(ps), oracle.read_map2d(pc)
+    es = oracle.make_solenoid2d(ms, 0.0, 0.7)
+    ec = oracle.make_rfcavity2d(mc, 0.0, 20.0, 1300.0, 0.3)
+    for e, m in ((es, ms), (ec, mc)):
+        zmax = m["zend"] - m["zbegin"]
+        R = np.column_stack([rng.uniform(-0.02, 0.02, 300), rng.uniform(-0.02, 0.02, 300),
+                             m["zbegin"] + rng.uniform(0, zmax * 0.999, 300)])
+        t = 1.1e-10
+        E, B = oracle.element_fields(e, R, t)
+        rr = np.hypot(R[:, 0], R[:, 1])
+        z = R[:, 2] - m["zbegin"]
+        hz, hr = zmax / (m["nz"] - 1), (m["rend"] - m["rbegin"]) / (m["nr"] - 1)
+        v = m["values"]
+        if m["dynamic"]:
+            ez, er, bt = (_bilinear(v[c], hz, hr, z, rr) for c in range(3))
+            ce, sb = 20.0 * np.cos(e.omega * t + 0.3), 20.0 * np.sin(e.omega * t + 0.3)
+            np.testing.assert_allclose(E[:, 0], ce * er * R[:, 0] / rr, rtol=1e-12, atol=1e-9)
+            np.testing.assert_allclose(E[:, 2], ce * ez, rtol=1e-12, atol=1e-9)
+            np.testing.assert_allclose(B[:, 0], sb * bt * R[:, 1] / rr, rtol=1e-12, atol=1e-18)
+            np.testing.assert_allclose(B[:, 1], -sb * bt * R[:, 0] / rr, rtol=1e-12, atol=1e-18)
+        else:
+            bz, br = _bilinear(v[0], hz, hr, z, rr), _bilinear(v[1], hz, hr, z, rr)
+            np.testing.assert_allclose(B[:, 2], 0.7 * bz, rtol=1e-12, atol=1e-15)
+            np.testing.assert_allclose(B[:, 1], 0.7 * br * R[:, 1] / rr, rtol=1e-12, atol=1e-15)
+            assert np.all(E == 0)
+    # outside the z range and beyond the last radial cell: no field
+    out = np.array([[0.0, 0.0, ms["zend"] + 1e-6], [0.05, 0.0, 0.1]])
+    assert np.all(oracle.element_fields(es, out)[1] == 0)

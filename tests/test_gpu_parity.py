@@ -636,6 +636,47 @@ def test_tracking_with_rfcavity_map_vs_oracle(oracle, gpu, tmp_path):
     assert rel(Pg[:, 2], Pn[:, 2]) > 1e-4
 
 
+def test_tracking_with_2d_field_maps_vs_oracle(oracle, gpu, tmp_path):
+    """SOLENOID with a 2DMagnetoStatic map and RFCAVITY with a 2DDynamic map
+    (FM2DMagnetoStatic / FM2DDynamic::getFieldstrength, the bilinear (r, z)
+    interpolation), ZX and XZ orientations: the bunch inside both, 20 steps
+    against the oracle."""
+    from src_b200.bunch import write_2d_rfcavity_map, write_2d_solenoid_map
+    N, nr, steps = 50_000, (32, 32, 32), 20
+    cav, sol = tmp_path / "cav2d.txt", tmp_path / "sol2d.txt"
+    write_2d_rfcavity_map(cav, "ZX")
+    write_2d_solenoid_map(sol, "XZ", normalize=True)
+    R, P = gaussian_bunch(N, bunch_id=15)
+    Q = -1e-9 / N
+    edge, volt, freq, lag = -0.03, 20.0, 1300.0, 0.4
+    mc, ms = oracle.read_map2d(cav), oracle.read_map2d(sol)
+    oracle.set_solenoids([oracle.make_rfcavity2d(mc, edge, volt, freq, lag), oracle.make_solenoid2d(ms, -0.1, 0.3)])
+    try:
+        tr = oracle.OracleTracker(oracle.make_params(nr, 1e-12), Q)
+        Ro, Po = R.copy(), P.copy()
+        tr.track(Ro, Po, steps)
+    finally:
+        oracle.set_solenoids([])
+    with gpu.Context(nr) as ctx:
+        ctx.add_rfcavity(cav, edge, volt, freq, lag)
+        ctx.add_solenoid(sol, -0.1, 0.3)
+        with pytest.raises(gpu.ScgpuError):  # a magnetostatic map is no cavity
+            ctx.add_rfcavity(sol, edge, volt, freq, lag)
+        ctx.upload(R, P, 1e-12, Q, oracle.electron_mass_ev())
+        ctx.track(steps)
+        Rg, Pg = ctx.download()
+        st = ctx.tracker_state()
+        ctx.clear_elements()
+        ctx.upload(R, P, 1e-12, Q, oracle.electron_mass_ev())
+        ctx.track(steps)
+        Rn, Pn = ctx.download()
+    assert rel(Rg, Ro) < STATE_TOL and rel(Pg, Po) < STATE_TOL
+    assert abs(st["path_length"] - tr.path_length) <= 1e-14 * abs(tr.path_length)
+    np.testing.assert_allclose(st["ref_P"], tr.ref_P, rtol=1e-13, atol=1e-18)
+    assert rel(Pg[:, 2], Pn[:, 2]) > 1e-4  # the cavity acts
+    assert rel(Pg[:, :2], Pn[:, :2]) > 1e-3  # the solenoid acts
+
+
 def test_tracking_with_multipole_vs_oracle(oracle, gpu):
     """MULTIPOLE elements (Multipole::computeField, the component scaling of
     setNormalComponent / setSkewComponent): a quadrupole with dipole,
