@@ -257,6 +257,7 @@ DevBunch bin_view(const scgpu_ctx* c, int k) {
     DevBunch v = c->b;
     v.st = c->b.bst + k;
     v.nacc = c->b.nacc_bins + (size_t)2 * mesh_cells(c->b) * k;
+    v.dep_weights = 0;  // the energy-bin deposit accumulates fixed-point charges
     v.spec_fwd = c->spec_fwd_buf;
     if (k & 1) {
         v.ghat = c->ghat_alt;
@@ -396,7 +397,7 @@ void enqueue_step(scgpu_ctx* c, bool stats, bool reorder, cudaStream_t s) {
     cudaStreamWaitEvent(c->ref, c->ev_start, 0);
     launch_advance_reference(b, c->ref);
     cudaEventRecord(c->ev_ref, c->ref);
-    launch_drift_to_beam(b, true, s);
+    launch_drift_to_beam(b, true, s, b.precision != SCGPU_PLAIN_FP64);
     if (shard) {  // the bounds of all shards, then the mesh
         exchange(c, b.st->bnd6, 6, SCGPU_EXCHANGE_MIN_F64, s);
         launch_finish_mesh(b, s);
@@ -587,6 +588,7 @@ int scgpu_create(scgpu_ctx** out, const scgpu_solver_params* p, int device) {
     }
     DevBunch& b = c->b;
     b.precision = p->precision;
+    b.dep_weights = p->precision == SCGPU_MIXED ? 1 : 0;
     b.bc.n[0] = p->mx;
     b.bc.n[1] = p->my;
     b.bc.n[2] = p->mt;
@@ -1533,7 +1535,7 @@ int scgpu_profile_track(scgpu_ctx* c, int nsteps, double* phase_ms) {
     int rc = SCGPU_OK;
     for (int k = 0; k < nsteps && rc == SCGPU_OK; ++k) {
         cudaEventRecord(ev[0], s);
-        launch_drift_to_beam(b, true, s);
+        launch_drift_to_beam(b, true, s, b.precision != SCGPU_PLAIN_FP64);
         launch_advance_reference(b, s);
         cudaEventRecord(ev[1], s);
         launch_deposit(b, s);

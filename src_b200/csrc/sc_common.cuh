@@ -642,10 +642,22 @@ SC_HD void kick_one(double* P, const double* Ef, const double* Bf, double dt, do
 // quotient; operands near the ends of the exponent range take the division.
 // Callers pass divisors in the normal range (mesh spacings, c dt, gamma), so
 // only the quotient is checked: a tiny, zero or huge q0 takes the division.
+// The range test reads the biased exponent of q0 from its high word on the
+// integer units: |q0| in [2^-899, 2^900) (exponent field 124 .. 1922; zero,
+// subnormals, infinities and NaN fall outside).
+SC_HD bool quot_in_range(double q) {
+#ifdef __CUDA_ARCH__
+    const unsigned hi = (unsigned)__double2hiint(q);
+#else
+    unsigned long long bits = 0;
+    __builtin_memcpy(&bits, &q, sizeof bits);
+    const unsigned hi = (unsigned)(bits >> 32);
+#endif
+    return ((hi >> 20) & 0x7ffu) - 124u < 1799u;
+}
 SC_HD double div_rcp(double a, double b, double rb) {
     const double q0 = a * rb;
-    const double aq = q0 < 0 ? -q0 : q0;
-    if (!(aq > 0x1p-900 && aq < 0x1p900)) return a / b;
+    if (!quot_in_range(q0)) return a / b;
     const double r = fma(-q0, b, a);
     return fma(r, rb, q0);
 }
@@ -655,8 +667,7 @@ SC_HD double div_rcp(double a, double b, double rb) {
 // a group of quotients and redo the group with divisions if it was cleared.
 SC_HD double div_rcp_nc(double a, double b, double rb, bool& fast) {
     const double q0 = a * rb;
-    const double aq = q0 < 0 ? -q0 : q0;
-    fast = fast && (aq > 0x1p-900 && aq < 0x1p900);
+    fast = fast && quot_in_range(q0);
     const double r = fma(-q0, b, a);
     return fma(r, rb, q0);
 }

@@ -33,6 +33,9 @@ struct DevBunch {
     int* scan_blocks; // chunk sums of the scan
     // deposit: fixed-point charge per node as (L, H), value H 2^32 + L; zero between steps
     unsigned long long* nacc;
+    // 1: nacc holds sums of 26-bit fixed-point CIC weights (the mixed form's
+    // deposit, in units of Q dt 2^-26); 0: fixed-point charges
+    int dep_weights;
     // grids
     // T is double in the plain form and float in the mixed form.
     void* rho;        // n^3 real (T)
@@ -95,7 +98,8 @@ void prime_particle_grids();  // occupancy of the particle kernels, before any c
 
 // particle TU (sc_particles.cu)
 void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s);
-void launch_drift_to_beam(const DevBunch& b, bool drift, cudaStream_t s);
+// mixed: the mixed form's half drift and frame change (fused multiply-adds)
+void launch_drift_to_beam(const DevBunch& b, bool drift, cudaStream_t s, bool mixed = false);
 void launch_advance_reference(const DevBunch& b, cudaStream_t s);
 void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s);
 void launch_deposit(const DevBunch& b, cudaStream_t s);

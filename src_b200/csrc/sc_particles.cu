@@ -277,7 +277,29 @@ __device__ __forceinline__ void finish_mesh(StepState& s, const BunchConst& bc) 
 __device__ __forceinline__ void bounds_tail(const BunchConst& bc, double (&v)[6], StepState* st, double* partials,
                                             unsigned* ticket, VB g);
 
-template <bool DRIFT>
+// Products and sums of the mixed form's FP64 steps, written as fused
+// multiply-adds (this file is compiled without contraction).
+__device__ __forceinline__ void matvec_fma(const double* M, const double* v, double* r) {
+    const double r0 = fma(M[0], v[0], fma(M[1], v[1], M[2] * v[2]));
+    const double r1 = fma(M[3], v[0], fma(M[4], v[1], M[5] * v[2]));
+    const double r2 = fma(M[6], v[0], fma(M[7], v[1], M[8] * v[2]));
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+}
+__device__ __forceinline__ void cross_fma(const double* a, const double* b, double* r) {
+    const double r0 = fma(a[1], b[2], -a[2] * b[1]);
+    const double r1 = fma(a[2], b[0], -a[0] * b[2]);
+    const double r2 = fma(a[0], b[1], -a[1] * b[0]);
+    r[0] = r0;
+    r[1] = r1;
+    r[2] = r2;
+}
+
+// MIXED: the mixed form's half drift R += (c dt / 2) P / gamma and beam-frame
+// translation and rotation in fused multiply-adds (the half drift of its
+// gather), in place of the reference's unitless round trip.
+template <bool DRIFT, bool MIXED = false>
 __device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restrict__ x, double* __restrict__ y,
                                            double* __restrict__ z, const double* __restrict__ px,
                                            const double* __restrict__ py, const double* __restrict__ pz, StepState* st,
@@ -304,9 +326,18 @@ __device__ __forceinline__ void drift_body(const BunchConst& bc, double* __restr
             if constexpr (DRIFT) Pn[0] = px[j], Pn[1] = py[j], Pn[2] = pz[j];
         }
         if constexpr (DRIFT) {
-            push_r(R, P, bc.s_cdt, bc.rs_cdt);
             double b[3];
-            trafo_transform_to(*fresh(&r2b_s), R, b);
+            if constexpr (MIXED) {
+                const double gm = sqrt(fma(P[0], P[0], fma(P[1], P[1], fma(P[2], P[2], 1.0))));
+                const double hv = (0.5 * bc.s_cdt) / gm;
+                const Trafo* t = fresh(&r2b_s);
+                const double X[3] = {fma(hv, P[0], R[0]) - t->origin[0], fma(hv, P[1], R[1]) - t->origin[1],
+                                     fma(hv, P[2], R[2]) - t->origin[2]};
+                matvec_fma(t->M, X, b);
+            } else {
+                push_r(R, P, bc.s_cdt, bc.rs_cdt);
+                trafo_transform_to(*fresh(&r2b_s), R, b);
+            }
             R[0] = b[0];
             R[1] = b[1];
             R[2] = b[2];
@@ -361,12 +392,12 @@ __device__ __forceinline__ void bounds_tail(const BunchConst& bc, double (&v)[6]
         *ticket = 0u;
     }
 }
-template <bool DRIFT>
+template <bool DRIFT, bool MIXED = false>
 __global__ void __launch_bounds__(kThreads, 3) k_drift_to_beam(BunchConst bc, double* __restrict__ x, double* __restrict__ y,
                                                             double* __restrict__ z, const double* __restrict__ px,
                                                             const double* __restrict__ py, const double* __restrict__ pz,
                                                             StepState* st, double* partials, unsigned* ticket) {
-    drift_body<DRIFT>(bc, x, y, z, px, py, pz, st, partials, ticket, vb_grid());
+    drift_body<DRIFT, MIXED>(bc, x, y, z, px, py, pz, st, partials, ticket, vb_grid());
 }
 
 // Streams this block's chunks (chunks blk, blk + nblk, ... of kStreamChunk
@@ -470,6 +501,31 @@ __global__ void __launch_bounds__(kThreads) k_cell_keys(BunchConst bc, const dou
 }
 
 // ------------------------------------------------------------ deposit
+// CIC cell and offset in units of the spacing: u = (x - origin) / h, cell
+// centres at u = l + 1/2; false when the stencil would leave the mesh.
+__device__ __forceinline__ bool cic_locate_fast(const double* rhr, const double* org, const int* n, const double* x,
+                                                int* l, float* d, int pz) {
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double u = fma(x[a] - org[a], rhr[a], -0.5);
+        const double f = floor(u);
+        int li = (int)f;
+        float di = (float)(u - f);
+        const int g = a == 2 ? pz : 0;  // a DC beam's z guard planes
+        if (li < -g) {
+            ok = false;
+            li = -g;
+        }
+        if (li > n[a] - 2 + g) {
+            ok = false;
+            li = n[a] - 2 + g;
+        }
+        l[a] = li;
+        d[a] = di;
+    }
+    return ok;
+}
 // CIC weights of one particle for the 8 corners, in IntCIC.h:850-857 order:
 // (0,0,0) (1,0,0) (0,1,0) (1,1,0) (0,0,1) (1,0,1) (0,1,1) (1,1,1).
 __device__ __forceinline__ void cic_charge(const double* d, double q, double* v) {
@@ -635,14 +691,109 @@ __global__ void __launch_bounds__(kThreads) k_deposit_bins(BunchConst bc, const 
     deposit_body<true>(bc, x, y, z, bin, nactive, st, acc, vb_grid());
 }
 
+// The mixed form's deposit.  The cell and offset come from the FP64 position
+// (cic_locate_fast, as in the mixed gather), the eight CIC weights are FP32
+// products, and each weight w <= 1 becomes the integer rint(w 2^26): the sum
+// over a lane group of up to 32 fits one 32-bit word, so a group pass is one
+// full-warp redux.sync per corner (half the passes of the two charge limbs)
+// and the group's first lane adds one 64-bit atomic per corner to the low
+// word of the node accumulator (the high word stays zero).  A node then holds
+// the exact, order-independent sum of its quantised weights; the assembly
+// multiplies it by Q dt 2^-26.  The DC beam's z boundary and guard planes as
+// in deposit_body.
+constexpr int kWeightFrac = 26;
+
+template <bool PZ>
+__device__ __forceinline__ void deposit_mixed_body(const BunchConst& bc, const double* __restrict__ x,
+                                                   const double* __restrict__ y, double* __restrict__ z, StepState* st,
+                                                   unsigned long long* __restrict__ acc, VB g) {
+    __shared__ MeshConsts ms;
+    load_mesh_consts(ms, st);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int nx = bc.n[0], nxy = bc.n[0] * bc.n[1];
+    const float scale = 0x1p26f;
+    bool bad = false;
+    for (long long i0 = (long long)g.blk * blockDim.x; i0 < bc.N; i0 += (long long)g.nblk * blockDim.x) {
+        const long long i = i0 + threadIdx.x;
+        const bool valid = i < bc.N;
+        uint32_t key = 0xffffffffu;
+        int lz = 0;
+        unsigned t[8];
+        if (valid) {
+            double X[3] = {x[i], y[i], z[i]};
+            const MeshConsts* m = fresh(&ms);
+            if constexpr (PZ) {
+                const double w = wrap_z(X[2], m->org[2], m->org[2] + m->hr[2] * (double)bc.n[2]);
+                if (w != X[2]) {
+                    z[i] = w;
+                    X[2] = w;
+                }
+            }
+            int l[3];
+            float d[3];
+            if (!cic_locate_fast(m->rhr, m->org, bc.n, X, l, d, PZ ? 1 : 0)) bad = true;
+            const float u[3] = {1.0f - d[0], 1.0f - d[1], 1.0f - d[2]};
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float w = (k & 1 ? d[0] : u[0]) * (k & 2 ? d[1] : u[1]) * (k & 4 ? d[2] : u[2]);
+                t[k] = __float2uint_rn(w * scale);
+            }
+            key = (uint32_t)(l[0] + nx * l[1] + nxy * l[2]);
+            lz = l[2];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) t[k] = 0u;
+        }
+        const unsigned group = __match_any_sync(kFull, key);
+        const int gsize = __popc(group);
+        const bool leader = lane == __ffs(group) - 1;
+        unsigned multi = __ballot_sync(kFull, leader && gsize > 1);
+        const bool passes = __popc(multi) <= kMaxGroupPasses;
+        if (valid && (gsize == 1 || !passes)) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int node = (int)key + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
+                if ((!PZ || (unsigned)(lz + (k >> 2)) < (unsigned)bc.n[2]) && t[k])
+                    atomicAdd(acc + 2 * (long long)node, (unsigned long long)t[k]);
+            }
+        }
+        while (passes && multi) {
+            const int ld = __ffs(multi) - 1;
+            multi &= multi - 1;
+            const bool in = (__shfl_sync(kFull, group, ld) >> lane) & 1u;
+            unsigned sum[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) sum[k] = __reduce_add_sync(kFull, in ? t[k] : 0u);
+            if (valid && lane == ld) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int node = (int)key + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
+                    if ((!PZ || (unsigned)(lz + (k >> 2)) < (unsigned)bc.n[2]) && sum[k])
+                        atomicAdd(acc + 2 * (long long)node, (unsigned long long)sum[k]);
+                }
+            }
+        }
+    }
+    if (bad) atomicOr(&st->err, kFlagGuard);
+}
+template <bool PZ>
+__global__ void __launch_bounds__(kThreads) k_deposit_mixed(BunchConst bc, const double* __restrict__ x,
+                                                            const double* __restrict__ y, double* __restrict__ z,
+                                                            StepState* st, unsigned long long* __restrict__ acc) {
+    deposit_mixed_body<PZ>(bc, x, y, z, st, acc, vb_grid());
+}
+
 // rho = (exact node sum) / dT * tmp2   (PartBunch.cpp:496, :510-511); the
-// accumulators are cleared for the next deposit.
+// accumulators are cleared for the next deposit.  `weights`: the node values
+// are sums of 26-bit CIC weights (the mixed deposit), in units of Q dt 2^-26.
 template <typename T>
 __device__ __forceinline__ void assemble_body(const BunchConst& bc, const StepState* __restrict__ st,
-                                              unsigned long long* __restrict__ acc, T* __restrict__ rho, VB g) {
+                                              unsigned long long* __restrict__ acc, T* __restrict__ rho, VB g,
+                                              bool weights) {
     const int M = bc.n[0] * bc.n[1] * bc.n[2];
     const double dT = bc.dT, tmp2 = st->tmp2;
-    const double unit = ldexp(1.0, fx_exponent(st->qdt) - kFxFrac);
+    const double unit = weights ? ldexp(st->qdt, -kWeightFrac) : ldexp(1.0, fx_exponent(st->qdt) - kFxFrac);
     for (int c = g.blk * blockDim.x + threadIdx.x; c < M; c += g.nblk * blockDim.x) {
         const double s = node_density(reinterpret_cast<const ulonglong2*>(acc)[c], unit, dT, tmp2);
         rho[c] = (T)s;
@@ -651,8 +802,9 @@ __device__ __forceinline__ void assemble_body(const BunchConst& bc, const StepSt
 }
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_assemble_rho(BunchConst bc, const StepState* __restrict__ st,
-                                                           unsigned long long* __restrict__ acc, T* __restrict__ rho) {
-    assemble_body<T>(bc, st, acc, rho, vb_grid());
+                                                           unsigned long long* __restrict__ acc, T* __restrict__ rho,
+                                                           int weights) {
+    assemble_body<T>(bc, st, acc, rho, vb_grid(), weights != 0);
 }
 
 // ------------------------------------------------------------ Green's function
@@ -1179,47 +1331,6 @@ __device__ __forceinline__ void cic_gather8(const double* __restrict__ F8, const
 // Boris kick, the half drift R += (c dt / 2) P / gamma (no unitless round
 // trip) and the reference-frame update.  Results differ from the plain
 // form's by rounding only (relative 1e-7 in E, 1e-16 in the FP64 steps).
-__device__ __forceinline__ void matvec_fma(const double* M, const double* v, double* r) {
-    const double r0 = fma(M[0], v[0], fma(M[1], v[1], M[2] * v[2]));
-    const double r1 = fma(M[3], v[0], fma(M[4], v[1], M[5] * v[2]));
-    const double r2 = fma(M[6], v[0], fma(M[7], v[1], M[8] * v[2]));
-    r[0] = r0;
-    r[1] = r1;
-    r[2] = r2;
-}
-__device__ __forceinline__ void cross_fma(const double* a, const double* b, double* r) {
-    const double r0 = fma(a[1], b[2], -a[2] * b[1]);
-    const double r1 = fma(a[2], b[0], -a[0] * b[2]);
-    const double r2 = fma(a[0], b[1], -a[1] * b[0]);
-    r[0] = r0;
-    r[1] = r1;
-    r[2] = r2;
-}
-// CIC cell and offset in units of the spacing: u = (x - origin) / h, cell
-// centres at u = l + 1/2; false when the stencil would leave the mesh.
-__device__ __forceinline__ bool cic_locate_fast(const double* rhr, const double* org, const int* n, const double* x,
-                                                int* l, float* d, int pz) {
-    bool ok = true;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const double u = fma(x[a] - org[a], rhr[a], -0.5);
-        const double f = floor(u);
-        int li = (int)f;
-        float di = (float)(u - f);
-        const int g = a == 2 ? pz : 0;  // a DC beam's z guard planes
-        if (li < -g) {
-            ok = false;
-            li = -g;
-        }
-        if (li > n[a] - 2 + g) {
-            ok = false;
-            li = n[a] - 2 + g;
-        }
-        l[a] = li;
-        d[a] = di;
-    }
-    return ok;
-}
 __device__ __forceinline__ void cic_gather_f32(const float* __restrict__ E4, const int* n, const int* l, const float* d,
                                                float* Ef) {
     const int nx = n[0], nxy = n[0] * n[1];
@@ -1578,11 +1689,11 @@ inline int grid_for(long long work, int cap) {
 // One kernel over many bunches: block i takes work item work[i] = (bunch,
 // block, -, blocks of that bunch) and runs the same body as the single-bunch
 // kernel on the bunch's buffers (tab[bunch], a device copy of its DevBunch).
-template <bool DRIFT>
+template <bool DRIFT, bool MIXED = false>
 __global__ void __launch_bounds__(kThreads, 3) k_drift_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
     const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
-    drift_body<DRIFT>(d.bc, d.x, d.y, d.z, d.px, d.py, d.pz, d.st, d.partials, d.ticket, VB{w.y, w.w});
+    drift_body<DRIFT, MIXED>(d.bc, d.x, d.y, d.z, d.px, d.py, d.pz, d.st, d.partials, d.ticket, VB{w.y, w.w});
 }
 
 template <bool STATS>
@@ -1594,18 +1705,21 @@ __global__ void __launch_bounds__(kThreads) k_reduce_state_batch(const DevBunch*
                              VB{w.y, w.w});
 }
 
-template <int NT>
+template <int NT, bool MIXED = false>
 __global__ void __launch_bounds__(NT) k_deposit_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
     const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
-    deposit_body<false>(d.bc, d.x, d.y, d.z, nullptr, 0, d.st, d.nacc, VB{w.y, w.w});
+    if constexpr (MIXED)
+        deposit_mixed_body<false>(d.bc, d.x, d.y, d.z, d.st, d.nacc, VB{w.y, w.w});
+    else
+        deposit_body<false>(d.bc, d.x, d.y, d.z, nullptr, 0, d.st, d.nacc, VB{w.y, w.w});
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_assemble_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
     const int4 w = resolve_block(work, nitems);
     const DevBunch& d = tab[w.x];
-    assemble_body<T>(d.bc, d.st, d.nacc, (T*)d.rho, VB{w.y, w.w});
+    assemble_body<T>(d.bc, d.st, d.nacc, (T*)d.rho, VB{w.y, w.w}, d.dep_weights != 0);
 }
 
 __global__ void k_advance_batch(const DevBunch* __restrict__ tab, const int4* __restrict__ work, int nitems) {
@@ -1650,16 +1764,21 @@ void launch_batch(int kind, int precision, int threads, const DevBunch* tab, con
     if (nblocks <= 0 || nitems <= 0) return;
     const bool f64 = precision == 0;
     switch (kind) {
-        case kBatchDrift: k_drift_batch<true><<<nblocks, kThreads, 0, s>>>(tab, work, nitems); break;
+        case kBatchDrift:
+            if (f64)
+                k_drift_batch<true><<<nblocks, kThreads, 0, s>>>(tab, work, nitems);
+            else
+                k_drift_batch<true, true><<<nblocks, kThreads, 0, s>>>(tab, work, nitems);
+            break;
         case kBatchPsum: k_reduce_state_batch<false><<<nblocks, kThreads, 0, s>>>(tab, work, nitems, true); break;
         case kBatchStats: k_reduce_state_batch<true><<<nblocks, kThreads, 0, s>>>(tab, work, nitems, false); break;
         case kBatchDeposit:
             if (threads == 128)
-                k_deposit_batch<128><<<nblocks, 128, 0, s>>>(tab, work, nitems);
+                (f64 ? k_deposit_batch<128> : k_deposit_batch<128, true>)<<<nblocks, 128, 0, s>>>(tab, work, nitems);
             else if (threads == 512)
-                k_deposit_batch<512><<<nblocks, 512, 0, s>>>(tab, work, nitems);
+                (f64 ? k_deposit_batch<512> : k_deposit_batch<512, true>)<<<nblocks, 512, 0, s>>>(tab, work, nitems);
             else
-                k_deposit_batch<256><<<nblocks, 256, 0, s>>>(tab, work, nitems);
+                (f64 ? k_deposit_batch<256> : k_deposit_batch<256, true>)<<<nblocks, 256, 0, s>>>(tab, work, nitems);
             break;
         case kBatchAssemble:
             if (f64)
@@ -1744,9 +1863,12 @@ void prime_particle_grids() {
     cudaFuncSetAttribute(k_gather_staged<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
     cudaFuncSetAttribute(k_gather_staged<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem);
     const void* kernels[] = {(const void*)k_drift_to_beam<true>,
+                             (const void*)k_drift_to_beam<true, true>,
                              (const void*)k_drift_to_beam<false>,
                              (const void*)k_deposit<false>,
                              (const void*)k_deposit<true>,
+                             (const void*)k_deposit_mixed<false>,
+                             (const void*)k_deposit_mixed<true>,
                              (const void*)k_deposit_bins,
                              (const void*)k_gather_kick_push<double, false>,
                              (const void*)k_gather_kick_push<double, true>,
@@ -1765,8 +1887,8 @@ void launch_reduce_state(const DevBunch& b, bool init_frame, cudaStream_t s) {
                                                            b.ticket, init_frame);
 }
 
-void launch_drift_to_beam(const DevBunch& b, bool drift, cudaStream_t s) {
-    auto k = drift ? k_drift_to_beam<true> : k_drift_to_beam<false>;
+void launch_drift_to_beam(const DevBunch& b, bool drift, cudaStream_t s, bool mixed) {
+    auto k = !drift ? k_drift_to_beam<false> : mixed ? k_drift_to_beam<true, true> : k_drift_to_beam<true>;
     k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.px, b.py, b.pz, b.st, b.partials, b.ticket);
 }
 
@@ -1778,7 +1900,10 @@ void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s) {
 }
 
 void launch_deposit(const DevBunch& b, cudaStream_t s) {
-    if (b.bc.pz)
+    if (b.dep_weights) {
+        auto k = b.bc.pz ? k_deposit_mixed<true> : k_deposit_mixed<false>;
+        k<<<wave_grid(k, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
+    } else if (b.bc.pz)
         k_deposit<true><<<wave_grid(k_deposit<true>, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
     else
         k_deposit<false><<<wave_grid(k_deposit<false>, b), kThreads, 0, s>>>(b.bc, b.x, b.y, b.z, b.st, b.nacc);
@@ -1788,9 +1913,9 @@ void launch_assemble_rho(const DevBunch& b, cudaStream_t s) {
     const long long M = (long long)b.bc.n[0] * b.bc.n[1] * b.bc.n[2];
     const int g = grid_for(M, 148 * 16);
     if (b.precision == 0)
-        k_assemble_rho<double><<<g, kThreads, 0, s>>>(b.bc, b.st, b.nacc, (double*)b.rho);
+        k_assemble_rho<double><<<g, kThreads, 0, s>>>(b.bc, b.st, b.nacc, (double*)b.rho, b.dep_weights);
     else
-        k_assemble_rho<float><<<g, kThreads, 0, s>>>(b.bc, b.st, b.nacc, (float*)b.rho);
+        k_assemble_rho<float><<<g, kThreads, 0, s>>>(b.bc, b.st, b.nacc, (float*)b.rho, b.dep_weights);
 }
 
 void launch_igf(const DevBunch& b, const double* hr_host, cudaStream_t s) {
