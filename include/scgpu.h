@@ -18,7 +18,8 @@
  *       virtual void PoissonSolver::computePotential(Field_t& rho, Vector_t hr)
  *       (src/Solvers/PoissonSolver.h:28; FFTPoissonSolver.cpp:337-382)
  *   scgpu_add_solenoid, scgpu_add_rfcavity, scgpu_clear_elements,
- *   scgpu_fieldmap_astra1d, scgpu_fieldmap_astra1d_dynamic, scgpu_fieldmap_2d
+ *   scgpu_fieldmap_astra1d, scgpu_fieldmap_astra1d_dynamic, scgpu_fieldmap_2d,
+ *   scgpu_fieldmap_3d
  *       ParallelTTracker::computeExternalFields (ParallelTTracker.cpp:595-643)
  *       with Solenoid::apply / Astra1DMagnetoStatic and RFCavity::apply /
  *       Astra1DDynamic (see below)
@@ -261,6 +262,24 @@ int scgpu_fieldmap_astra1d_dynamic(const char* path, double* coefs, int max_coef
  * (c, z i, r j) at values[(c nr + j) nz + i]; capacity counts doubles. */
 int scgpu_fieldmap_2d(const char* path, int* dynamic, int* nz, int* nr, double* ranges, double* frequency_mhz,
                       double* values, long long capacity);
+
+/* 3D field maps of RF cavities in OPAL's own format: scgpu_add_rfcavity
+ * takes a 3DDynamic map (src/Classic/Fields/FM3DDynamic.cpp), chosen by the
+ * file's first word.  Header "3DDynamic [TRUE|FALSE]", the frequency [MHz],
+ * "xbegin xend nx", "ybegin yend ny", "zbegin zend nz" [cm, intervals], then
+ * (nx+1)(ny+1)(nz+1) lines "Ex Ey Ez Hx Hy Hz" [MV/m, A/m], x outer, z
+ * inner.  The field is the reference's trilinear interpolation
+ * (FM3DDynamic::getFieldstrength) with E = VOLT cos(omega t + LAG) E_map and
+ * B -= VOLT sin(omega t + LAG) B_map; none in the last two grid planes along
+ * any axis (the reference loses a particle there transversely).  A 3D
+ * magnetostatic map (FM3DMagnetoStatic) is refused: SCGPU_ERR_UNSUPPORTED.
+ * scgpu_fieldmap_3d reads a map as the element does: the grid points n =
+ * {nx, ny, nz}, ranges = {xbegin, xend, ybegin, yend, zbegin, zend} [m], the
+ * frequency [MHz] and, when values is not NULL, the normalised values
+ * component-major (Ex, Ey, Ez [V/m], Bx, By, Bz [T]), value (c, x i, y j,
+ * z k) at values[c nx ny nz + (i ny + j) nz + k]; capacity counts doubles. */
+int scgpu_fieldmap_3d(const char* path, int* n, double* ranges, double* frequency_mhz, double* values,
+                      long long capacity);
 
 /* MULTIPOLE (src/Elements/OpalMultipole.cpp:127-166 attributes L, KN, DKN,
  * KS, DKS and ELEMEDGE; src/Classic/AbsBeamline/Multipole.cpp): a straight

@@ -13,6 +13,7 @@ into ``oracle/_ref/libfftpack_ref.so`` by ``oracle/Makefile``.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -61,7 +62,9 @@ class Solenoid(C.Structure):
                 ("period", C.c_double), ("accuracy", C.c_int), ("kind", C.c_int), ("omega", C.c_double),
                 ("phase", C.c_double), ("xlrep", C.c_double), ("nskew", C.c_int), ("map2d", C.c_int),
                 ("aperture", C.c_double * 2), ("nz", C.c_int), ("nr", C.c_int), ("hz", C.c_double),
-                ("hr", C.c_double), ("grid", _dp), ("coefs", C.c_double * 255)]
+                ("hr", C.c_double), ("grid", _dp), ("map3d", C.c_int), ("nx", C.c_int), ("ny", C.c_int),
+                ("pad3_", C.c_int), ("hx", C.c_double), ("hy", C.c_double), ("xbegin", C.c_double),
+                ("ybegin", C.c_double), ("coefs", C.c_double * 255)]
 
 
 class BeamParams(C.Structure):
@@ -376,13 +379,79 @@ def make_rfcavity2d(m, edge, volt, freq_mhz, lag):
     return _attach_map2d(e, m)
 
 
+def read_map3d(path):
+    """A 3D dynamic map as FM3DDynamic reads it (FM3DDynamic.cpp:17-220),
+    restated: dict with nx, ny, nz (grid points), xbegin, xend, ybegin, yend,
+    zbegin, zend [m], freq_mhz and values [component, x, y, z] (Ex, Ey, Ez
+    [V/m], Bx, By, Bz [T]), normalised to the largest |Ez| on the grid line
+    nearest the axis unless the header says FALSE."""
+    keep = set(".-+\x89")
+    with open(path) as f:
+        lines = []
+        for raw in f:  # Fieldmap::getLine
+            line = raw.split("#", 1)[0]
+            idx = [i for i, ch in enumerate(line) if ch.isalnum() or ch in keep]
+            if idx:
+                lines.append(line[idx[0]:idx[-1] + 1])
+    head = lines[0].split()
+    if not head[0].startswith("3DDy"):
+        raise ValueError("not a 3D dynamic map")
+    normalize = len(head) < 2 or head[1].upper() == "TRUE"
+    freq = float(lines[1])
+    (xb, xe, nxi), (yb, ye, nyi), (zb, ze, nzi) = [(float(a), float(b), int(n)) for a, b, n in
+                                                   (l.split() for l in lines[2:5])]
+    nx, ny, nz = nxi + 1, nyi + 1, nzi + 1
+    rows = np.array([[float(x) for x in l.split()] for l in lines[5:5 + nx * ny * nz]])
+    v = np.ascontiguousarray(rows.T.reshape(6, nx, ny, nz))
+    xb, xe, yb, ye, zb, ze = (q / 100.0 for q in (xb, xe, yb, ye, zb, ze))
+    hx, hy = (xe - xb) / nxi, (ye - yb) / nyi
+    ezmax = 1.0
+    if normalize:
+        ix = int(math.ceil(-xb / hx))
+        if ix * hx + xb > 0.5:
+            ix -= 1
+        iy = int(math.ceil(-yb / hy))
+        if iy * hy + yb > 0.5:
+            iy -= 1
+        ezmax = float(np.max(np.abs(v[2, ix, iy, :])))
+    mu_0 = 1.256637061e-06
+    v[:3] *= 1e6 / ezmax
+    v[3:] *= mu_0 / ezmax
+    return dict(nx=nx, ny=ny, nz=nz, xbegin=xb, xend=xe, ybegin=yb, yend=ye, zbegin=zb, zend=ze, freq_mhz=freq,
+                values=v)
+
+
+def make_rfcavity3d(m, edge, volt, freq_mhz, lag):
+    """RFCAVITY with a 3D dynamic map (read_map3d): VOLT [MV/m], FREQ [MHz],
+    LAG [rad]; the map's frequency replaces FREQ beyond 1 % (RFCavity.cpp:294-305)."""
+    e = Solenoid()
+    two_pi = 2 * 3.14159265358979323846
+    omega_map = m["freq_mhz"] * (two_pi * 1e6)
+    omega = 1e6 * two_pi * freq_mhz
+    if abs((omega - omega_map) / omega) > 0.01:
+        omega = omega_map
+    e.kind, e.edge, e.scale, e.omega, e.phase = 1, edge, volt, omega, lag
+    grid = np.ascontiguousarray(m["values"], dtype=np.float64)
+    e.map3d, e.nx, e.ny, e.nz = 1, m["nx"], m["ny"], m["nz"]
+    e.hx = (m["xend"] - m["xbegin"]) / (m["nx"] - 1)
+    e.hy = (m["yend"] - m["ybegin"]) / (m["ny"] - 1)
+    e.hz = (m["zend"] - m["zbegin"]) / (m["nz"] - 1)
+    e.xbegin, e.ybegin = m["xbegin"], m["ybegin"]
+    e.grid = _ptr(grid)
+    e.zbegin, e.range = m["zbegin"], m["zend"] - m["zbegin"]
+    e._keep = grid  # the grid must outlive the element
+    return e
+
+
 def element_fields(element, R, t=0.0):
-    """E, B of one SOLENOID / RFCAVITY element with a 2D map at points R (element frame)."""
+    """E, B of one SOLENOID / RFCAVITY element with a 2D or 3D map at points R (element frame)."""
     R = _f64(R)
     E, B = np.zeros_like(R), np.zeros_like(R)
     for i in range(R.shape[0]):
         e, b = (C.c_double * 3)(), (C.c_double * 3)()
-        if element.kind == 1:
+        if element.kind == 1 and element.map3d:
+            lib().sco_rfcavity3d_field(C.byref(element), R[i].ctypes.data_as(_dp), C.c_double(t), e, b)
+        elif element.kind == 1:
             lib().sco_rfcavity2d_field(C.byref(element), R[i].ctypes.data_as(_dp), C.c_double(t), e, b)
         else:
             lib().sco_solenoid2d_field(C.byref(element), R[i].ctypes.data_as(_dp), b)

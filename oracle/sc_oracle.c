@@ -1735,12 +1735,62 @@ void sco_rfcavity2d_field(const sco_solenoid* e, const double* R, double t, doub
     }
 }
 
+/* FM3DDynamic::getFieldstrength (FM3DDynamic.cpp:242-315): the floored
+ * coordinates kept as unsigned ints, the 8-term trilinear sums per component
+ * in the reference's order; then RFCavity::apply's scaling (RFCavity.cpp:
+ * 237-248).  No field from the last two z planes on; none (a lost particle
+ * in the reference) from the last two x or y planes on. */
+static unsigned idx3d(double u) {
+    const double f = floor(u);
+    if (!(f >= -2147483648.0 && f < 2147483647.0)) return 0xffffffffu;
+    return (unsigned)(int)f;
+}
+void sco_rfcavity3d_field(const sco_solenoid* e, const double* R, double t, double* E, double* B) {
+    const double tmpR[3] = {R[0], R[1], R[2] - e->zbegin};
+    if (!(tmpR[2] >= 0.0 && tmpR[2] < e->range)) return;
+    const unsigned index_x = idx3d((tmpR[0] - e->xbegin) / e->hx);
+    const unsigned index_y = idx3d((tmpR[1] - e->ybegin) / e->hy);
+    const unsigned index_z = idx3d(tmpR[2] / e->hz);
+    if (index_z >= (unsigned)e->nz - 2u) return;
+    if (index_x >= (unsigned)e->nx - 2u || index_y >= (unsigned)e->ny - 2u) return;
+    const double lever_x = (tmpR[0] - e->xbegin) / e->hx - index_x;
+    const double lever_y = (tmpR[1] - e->ybegin) / e->hy - index_y;
+    const double lever_z = tmpR[2] / e->hz - index_z;
+    const size_t deltaX = (size_t)e->ny * e->nz, deltaY = (size_t)e->nz, deltaZ = 1;
+    const size_t index1 = index_x * deltaX + index_y * deltaY + index_z * deltaZ;
+    const size_t np = (size_t)e->nx * deltaX;
+    double tmpE[3] = {0.0, 0.0, 0.0}, tmpB[3] = {0.0, 0.0, 0.0};
+    for (int c = 0; c < 6; ++c) {
+        const double* F = e->grid + c * np;
+        const double v = (1.0 - lever_x) * (1.0 - lever_y) * (1.0 - lever_z) * F[index1]
+                       + lever_x         * (1.0 - lever_y) * (1.0 - lever_z) * F[index1 + deltaX]
+                       + (1.0 - lever_x) * lever_y         * (1.0 - lever_z) * F[index1 + deltaY]
+                       + lever_x         * lever_y         * (1.0 - lever_z) * F[index1 + deltaX + deltaY]
+                       + (1.0 - lever_x) * (1.0 - lever_y) * lever_z         * F[index1 + deltaZ]
+                       + lever_x         * (1.0 - lever_y) * lever_z         * F[index1 + deltaX + deltaZ]
+                       + (1.0 - lever_x) * lever_y         * lever_z         * F[index1 + deltaY + deltaZ]
+                       + lever_x         * lever_y         * lever_z         * F[index1 + deltaX + deltaY + deltaZ];
+        if (c < 3)
+            tmpE[c] += v;
+        else
+            tmpB[c - 3] += v;
+    }
+    const double cs = e->scale * cos(e->omega * t + e->phase);
+    const double sn = e->scale * sin(e->omega * t + e->phase);
+    for (int d = 0; d < 3; ++d) {
+        E[d] += cs * tmpE[d];
+        B[d] -= sn * tmpB[d];
+    }
+}
+
 /* one element's E (RF cavities) and B at R (element frame), time t */
 static void element_field(const sco_solenoid* e, const double* R, double t, int ref_particle, double* E, double* B) {
     E[0] = E[1] = E[2] = 0.0;
     if (e->kind == 1) {
         B[0] = B[1] = B[2] = 0.0;
-        if (e->map2d)
+        if (e->map3d)
+            sco_rfcavity3d_field(e, R, t, E, B);
+        else if (e->map2d)
             sco_rfcavity2d_field(e, R, t, E, B);
         else
             sco_rfcavity_field(e, R, t, E, B);

@@ -157,7 +157,10 @@ typedef struct {
     double aperture[2]; /* MULTIPOLE: elliptical aperture semi-axes [m] */
     int nz, nr;         /* 2D map: grid points along z and r */
     double hz, hr;      /* 2D map: spacings [m] */
-    const double* grid; /* 2D map: Bz, Br or Ez, Er, Bt, each nz nr values, z fastest */
+    const double* grid; /* 2D map: Bz, Br or Ez, Er, Bt, each nz nr values, z fastest;
+                           3D map: Ex, Ey, Ez, Bx, By, Bz, each nx ny nz values, (i ny + j) nz + k */
+    int map3d, nx, ny, pad3_; /* RFCAVITY: 1 = a 3D (x, y, z) grid map; its points along x, y (nz above) */
+    double hx, hy, xbegin, ybegin; /* 3D map: spacings and first grid x, y [m] */
     double coefs[255];  /* map coefficients; MULTIPOLE: normal, normal errors, skew, skew errors */
 } sco_solenoid;
 int sco_set_solenoids(const sco_solenoid* s, int n);
@@ -172,6 +175,9 @@ void sco_multipole_field(const sco_solenoid* e, const double* R, int ref_particl
  * 185-221 with RFCavity::apply): B (set) and E, B (added) at R, element frame */
 void sco_solenoid2d_field(const sco_solenoid* e, const double* R, double* B);
 void sco_rfcavity2d_field(const sco_solenoid* e, const double* R, double t, double* E, double* B);
+/* RFCAVITY with a 3D dynamic map (FM3DDynamic.cpp:242-315 with
+ * RFCavity::apply, RFCavity.cpp:232-250): E, B added at R, element frame */
+void sco_rfcavity3d_field(const sco_solenoid* e, const double* R, double t, double* E, double* B);
 /* Multipole::setNormalComponent / setSkewComponent (Multipole.cpp:106-163):
  * the stored component of order n (1 = dipole) from KN (or KS) and its error;
  * *err receives the stored error. */

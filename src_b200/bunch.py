@@ -280,3 +280,44 @@ def write_2d_rfcavity_map(path, orientation="XZ", normalize=None, freq_mhz=1300.
                 for j in range(nr + 1):
                     f.write(f"{ER[j, i]:.17g} {EZ[j, i]:.17g} {HT[j, i]:.17g} {EA[j, i]:.17g}\n")
     return z, r, EZ, ER, HT
+
+
+def write_3d_rfcavity_map(path, normalize=None, freq_mhz=1300.0, cells=2, half_width=0.02, nx=16, ny=12, nz=80,
+                          seed=3, comment=True):
+    """A seeded synthetic standing-wave cavity in OPAL's 3DDynamic format on
+    an (x, y, z) grid (cm; E in MV/m, H in A/m): the field of
+    write_2d_rfcavity_map in Cartesian components (Ez = sin(pi z / cell)
+    (1 - (k r)^2 / 4), E_perp = -(x, y)/2 dEz/dz, H = (omega eps0 / 2)
+    (-y, x, 0) Ez) plus a seeded perturbation of 1e-3 of each component's
+    scale, so that no two grid axes are interchangeable; x in [-w, w] with nx
+    intervals, y with ny, z over `cells` cells with nz.  Returns x, y, z [m]
+    and the six arrays [component, x, y, z] as written."""
+    c = 299792458.0
+    cell = c / (2.0 * freq_mhz * 1e6)
+    length = cells * cell
+    k = 2 * np.pi * freq_mhz * 1e6 / c
+    x = np.linspace(-half_width, half_width, nx + 1)
+    y = np.linspace(-half_width, half_width, ny + 1)
+    z = np.linspace(0.0, length, nz + 1)
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    ez0 = np.sin(np.pi * Z / cell)
+    dez0 = np.pi / cell * np.cos(np.pi * Z / cell)
+    w_eps = 2 * np.pi * freq_mhz * 1e6 * 8.854187817e-12 * 1e6  # A/m per MV/m per m
+    F = np.stack([-X / 2 * dez0, -Y / 2 * dez0, ez0 * (1 - k ** 2 * (X ** 2 + Y ** 2) / 4),
+                  -w_eps * Y / 2 * ez0, w_eps * X / 2 * ez0, np.zeros_like(Z)])
+    rng = np.random.default_rng(seed)
+    scale = np.maximum(np.abs(F).reshape(6, -1).max(axis=1), 1e-3 * w_eps * half_width)
+    F = F + 1e-3 * scale[:, None, None, None] * rng.standard_normal(F.shape)
+    flag = "" if normalize is None else (" TRUE" if normalize else " FALSE")
+    with open(path, "w") as f:
+        f.write(f"3DDynamic{flag}\n")
+        if comment:
+            f.write("# synthetic cavity: x, y, z in cm, E in MV/m, H in A/m\n")
+        f.write(f"{freq_mhz:.17g}\n")
+        f.write(f"{-100 * half_width:.17g} {100 * half_width:.17g} {nx}\n")
+        f.write(f"{-100 * half_width:.17g} {100 * half_width:.17g} {ny}\n")
+        f.write(f"{0.0:.17g} {100 * length:.17g} {nz}\n")
+        rows = F.reshape(6, -1).T
+        for r in rows:
+            f.write(" ".join(f"{v:.17g}" for v in r) + "\n")
+    return x, y, z, F

@@ -848,10 +848,44 @@ static int attach_map2d(scgpu_ctx* c, const char* path, bool want_dynamic, MapEl
     return SCGPU_OK;
 }
 
+// A 3D dynamic map's grid on the device (FM3DDynamic), referenced by the
+// element as attach_map2d does.
+static int attach_map3d(scgpu_ctx* c, const char* path, MapElem& e, double* freq_mhz) {
+    int n[3] = {0, 0, 0};
+    double r[6] = {0, 0, 0, 0, 0, 0}, f = 0.0;
+    std::vector<double> v;
+    int rc = fieldmap_3d(path, n, r, &f, &v);
+    if (rc) return fail(c, rc, std::string("cannot read the field map ") + path);
+    if (n[0] < 2 || n[1] < 2 || n[2] < 2 || !(r[1] > r[0]) || !(r[3] > r[2]) || !(r[5] > r[4]))
+        return fail(c, SCGPU_ERR_ARG, "a 3D map needs two points per axis and increasing ranges");
+    CK(cudaSetDevice(c->device));
+    double* d = nullptr;
+    rc = dalloc(c, &d, v.size() * sizeof(double));
+    if (rc) return rc;
+    CK(cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->map_grids.push_back(d);
+    e.map3d = 1;
+    e.nx = n[0];
+    e.ny = n[1];
+    e.nz = n[2];
+    e.hx = (r[1] - r[0]) / (n[0] - 1);  // FM3DDynamic: (end - begin) / intervals
+    e.hy = (r[3] - r[2]) / (n[1] - 1);
+    e.hz = (r[5] - r[4]) / (n[2] - 1);
+    e.xbegin = r[0];
+    e.ybegin = r[2];
+    e.grid = d;
+    e.zbegin = r[4];  // RFCavity::initialise: startField = zbegin, length = zend - zbegin
+    e.range = r[5] - r[4];
+    *freq_mhz = f;
+    return SCGPU_OK;
+}
+
 int scgpu_add_solenoid(scgpu_ctx* c, const char* fieldmap, double elemedge, double ks) {
     if (!c || !fieldmap) return fail(c, SCGPU_ERR_ARG, "null argument");
     if (!std::isfinite(elemedge) || !std::isfinite(ks)) return fail(c, SCGPU_ERR_ARG, "ELEMEDGE and KS must be finite");
     if ((int)c->elements.size() >= kMaxElements) return fail(c, SCGPU_ERR_UNSUPPORTED, "at most 8 elements");
+    if (fieldmap_kind_3d(fieldmap) != 0)
+        return fail(c, SCGPU_ERR_UNSUPPORTED, "3D magnetostatic maps are not supported (FM3DMagnetoStatic)");
     MapElem e{};
     if (fieldmap_is_2d(fieldmap)) {
         int rc = attach_map2d(c, fieldmap, false, e, nullptr);
@@ -891,7 +925,13 @@ int scgpu_add_rfcavity(scgpu_ctx* c, const char* fieldmap, double elemedge, doub
     if ((int)c->elements.size() >= kMaxElements) return fail(c, SCGPU_ERR_UNSUPPORTED, "at most 8 elements");
     MapElem e{};
     double fmap = 0.0;
-    if (fieldmap_is_2d(fieldmap)) {
+    const int kind3d = fieldmap_kind_3d(fieldmap);
+    if (kind3d == 2) return fail(c, SCGPU_ERR_ARG, std::string("the field map ") + fieldmap + " is not a dynamic map");
+    if (kind3d == 1) {
+        int rc = attach_map3d(c, fieldmap, e, &fmap);
+        if (rc) return rc;
+        if (!(fmap > 0.0)) return fail(c, SCGPU_ERR_ARG, "the 3D map's frequency must be positive");
+    } else if (fieldmap_is_2d(fieldmap)) {
         int rc = attach_map2d(c, fieldmap, true, e, &fmap);
         if (rc) return rc;
         if (!(fmap > 0.0)) return fail(c, SCGPU_ERR_ARG, "the 2D map's frequency must be positive");

@@ -128,6 +128,12 @@ struct MapElem {
     int nz, nr;
     double hz, hr;
     const double* grid;
+    // 3D map of an RFCAVITY (FM3DDynamic): 1, the grid points along x and y
+    // (nz above), spacings and the map's first x and y; the grid holds Ex, Ey,
+    // Ez [V/m], Bx, By, Bz [T], each nx ny nz values, (x i, y j, z k) at
+    // (i ny + j) nz + k
+    int map3d, nx, ny, pad3_;
+    double hx, hy, xbegin, ybegin;
     // map: Fourier coefficients; MULTIPOLE: normal components, their errors,
     // skew components, their errors (accuracy, accuracy, nskew, nskew values)
     double coefs[kMaxSolCoefs];
@@ -453,6 +459,52 @@ SC_HD void rfcavity2d_field(const MapElem& e, const double* R, double t, double*
     B[2] -= sb * tB[2];
 }
 
+// The floored grid coordinate as the reference's unsigned index
+// (static_cast<int>(floor(u)) stored in an unsigned int): a point before the
+// grid's start becomes a huge index, which the range checks reject.
+SC_HD unsigned grid3d_index(double u) {
+    const double f = floor(u);
+    if (!(f >= -2147483648.0 && f < 2147483647.0)) return 0xffffffffu;
+    return (unsigned)(int)f;
+}
+// FM3DDynamic's trilinear interpolation of one component, its terms in the
+// reference's order (FM3DDynamic.cpp:262-270; x steps by dX, y by dY, z by 1)
+SC_HD double grid3d_value(const double* F, size_t i1, size_t dX, size_t dY, double lx, double ly, double lz) {
+    return (1.0 - lx) * (1.0 - ly) * (1.0 - lz) * F[i1] + lx * (1.0 - ly) * (1.0 - lz) * F[i1 + dX] +
+           (1.0 - lx) * ly * (1.0 - lz) * F[i1 + dY] + lx * ly * (1.0 - lz) * F[i1 + dX + dY] +
+           (1.0 - lx) * (1.0 - ly) * lz * F[i1 + 1] + lx * (1.0 - ly) * lz * F[i1 + dX + 1] +
+           (1.0 - lx) * ly * lz * F[i1 + dY + 1] + lx * ly * lz * F[i1 + dX + dY + 1];
+}
+
+// FM3DDynamic::getFieldstrength (FM3DDynamic.cpp:242-315) with RFCavity::apply
+// (RFCavity.cpp:232-250): E += VOLT cos(omega t + LAG) E_map and B -= VOLT
+// sin(omega t + LAG) B_map, the map field interpolated at (x, y, z - zbegin)
+// inside [zbegin, zbegin + range).  No field from the last two z planes on;
+// none from the last two x or y planes on either (there the reference loses
+// the particle).
+SC_HD void rfcavity3d_field(const MapElem& e, const double* R, double t, double* E, double* B) {
+    const double tz = R[2] - e.zbegin;
+    if (!(tz >= 0.0 && tz < e.range)) return;
+    const double ux = (R[0] - e.xbegin) / e.hx, uy = (R[1] - e.ybegin) / e.hy, uz = tz / e.hz;
+    const unsigned ix = grid3d_index(ux), iy = grid3d_index(uy), iz = grid3d_index(uz);
+    if (iz >= (unsigned)e.nz - 2u) return;
+    if (ix >= (unsigned)e.nx - 2u || iy >= (unsigned)e.ny - 2u) return;
+    const double lx = ux - ix, ly = uy - iy, lz = uz - iz;
+    const size_t dX = (size_t)e.ny * e.nz, dY = (size_t)e.nz;
+    const size_t i1 = ix * dX + iy * dY + iz, np = (size_t)e.nx * dX;
+    double v[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) v[c] = grid3d_value(e.grid + c * np, i1, dX, dY, lx, ly, lz);
+    const double arg = e.omega * t + e.phase;
+    const double ce = e.scale * cos(arg), sb = e.scale * sin(arg);
+    E[0] += ce * v[0];
+    E[1] += ce * v[1];
+    E[2] += ce * v[2];
+    B[0] -= sb * v[3];
+    B[1] -= sb * v[4];
+    B[2] -= sb * v[5];
+}
+
 // Multipole::computeField (Multipole.cpp:229-349): the normal components
 // c[0..nn), then the skew components s[0..ns), each order's term added to
 // B_x, B_y in the reference's expression order (special forms for the
@@ -575,7 +627,9 @@ SC_HD void add_external_fields(const MapElem* el, int n, const Trafo& ref_to_lab
         loc[1] = lab[1] - 0.0;
         loc[2] = lab[2] - el[k].edge;
         if (el[k].kind == kElemRfCavity) {
-            if (el[k].map2d)
+            if (el[k].map3d)
+                rfcavity3d_field(el[k], loc, t, El, Bl);
+            else if (el[k].map2d)
                 rfcavity2d_field(el[k], loc, t, El, Bl);
             else
                 rfcavity_field(el[k], loc, t, El, Bl);

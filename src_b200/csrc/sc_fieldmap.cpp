@@ -14,7 +14,8 @@
 // frequency in MHz, then lines "z Ez(z)"; the same resampling, mirroring and
 // series, normalised to the largest |Ez| and scaled by 1e6 (MV/m to V/m).
 //
-// 2D maps on an (r, z) grid: see read_map2d.
+// 2D maps on an (r, z) grid: see read_map2d; 3D maps of RF cavities: see
+// read_map3d.
 //
 // Host C++ only (no CUDA); the evaluation is in sc_common.cuh.
 #include <cctype>
@@ -319,9 +320,114 @@ int read_map2d(const char* path, Map2D& m) {
     return SCGPU_OK;
 }
 
+// 3D maps of RF cavities, as FM3DDynamic reads them
+// (src/Classic/Fields/FM3DDynamic.cpp: constructor :17-107, readMap
+// :113-220): a header "3DDynamic [TRUE|FALSE]", the frequency in MHz, the
+// lines "xbegin xend nx", "ybegin yend ny", "zbegin zend nz" in cm and
+// intervals, then (nx+1)(ny+1)(nz+1) lines "Ex Ey Ez Hx Hy Hz" [MV/m, A/m],
+// x outer, y, z inner.  Lengths become m, counts grid points; unless FALSE
+// the values are divided by the largest |Ez| on the grid line along z
+// nearest the axis (the x index ceil(-xbegin / hx), one less when that grid
+// x exceeds 0.5, likewise y); E is scaled by 1e6 / Ezmax (MV/m to V/m) and H
+// by mu_0 / Ezmax (to B).  values: component c (Ex, Ey, Ez, Bx, By, Bz) at
+// (x i, y j, z k) at values[c nx ny nz + (i ny + j) nz + k].
+struct Map3D {
+    int nx = 0, ny = 0, nz = 0;  // grid points
+    double xbegin = 0, xend = 0, ybegin = 0, yend = 0, zbegin = 0, zend = 0, freq_mhz = 0;
+    std::vector<double> v;
+};
+
+int read_map3d(const char* path, Map3D& m) {
+    if (!path) return SCGPU_ERR_ARG;
+    std::ifstream in(path);
+    if (!in) return SCGPU_ERR_ARG;
+    std::string line;
+    if (!content_line(in, line)) return SCGPU_ERR_ARG;
+    std::istringstream hs(line);
+    std::string name, flag, rest;
+    if (!(hs >> name) || name.compare(0, 4, "3DDy") != 0) return SCGPU_ERR_ARG;
+    bool normalize = true;
+    if (hs >> flag) {
+        for (char& ch : flag) ch = (char)std::toupper((unsigned char)ch);
+        if (flag != "TRUE" && flag != "FALSE") return SCGPU_ERR_ARG;
+        normalize = flag == "TRUE";
+        if (hs >> rest) return SCGPU_ERR_ARG;
+    }
+    int nxi = 0, nyi = 0, nzi = 0;
+    if (!content_line(in, line) || !numbers(line, &m.freq_mhz, 1)) return SCGPU_ERR_ARG;
+    if (!range_line(in, m.xbegin, m.xend, nxi) || !range_line(in, m.ybegin, m.yend, nyi) ||
+        !range_line(in, m.zbegin, m.zend, nzi))
+        return SCGPU_ERR_ARG;
+    m.nx = nxi + 1;
+    m.ny = nyi + 1;
+    m.nz = nzi + 1;
+    const size_t np = (size_t)m.nx * m.ny * m.nz;
+    if ((size_t)m.nx * m.ny > ((size_t)1 << 26) || np > ((size_t)1 << 26)) return SCGPU_ERR_ARG;
+    m.v.assign(6 * np, 0.0);
+    double x[6];
+    for (size_t k = 0; k < np; ++k) {  // (i ny + j) nz + k in file order
+        if (!content_line(in, line) || !numbers(line, x, 6)) return SCGPU_ERR_ARG;
+        for (int c = 0; c < 6; ++c) m.v[c * np + k] = x[c];
+    }
+    if (content_line(in, line)) return SCGPU_ERR_ARG;  // interpreteEOF: nothing after the values
+    m.xbegin /= 100.0;
+    m.xend /= 100.0;
+    m.ybegin /= 100.0;
+    m.yend /= 100.0;
+    m.zbegin /= 100.0;
+    m.zend /= 100.0;
+    const double hx = (m.xend - m.xbegin) / nxi, hy = (m.yend - m.ybegin) / nyi;
+    double ezmax = 1.0;
+    if (normalize) {
+        int ix = (int)std::ceil(-m.xbegin / hx);
+        if (ix * hx + m.xbegin > 0.5) --ix;
+        int iy = (int)std::ceil(-m.ybegin / hy);
+        if (iy * hy + m.ybegin > 0.5) --iy;
+        // a map whose axis line lies outside the grid has no reference value
+        if (ix < 0 || ix >= m.nx || iy < 0 || iy >= m.ny) return SCGPU_ERR_ARG;
+        const double* ez = m.v.data() + 2 * np + ((size_t)ix * m.ny + iy) * m.nz;
+        ezmax = 0.0;
+        for (int k = 0; k < m.nz; ++k)
+            if (std::abs(ez[k]) > ezmax) ezmax = std::abs(ez[k]);
+        if (!(ezmax > 0.0)) return SCGPU_ERR_ARG;
+    }
+    const double mu_0 = 1.256637061e-06;
+    for (size_t k = 0; k < 3 * np; ++k) m.v[k] *= 1e6 / ezmax;
+    for (size_t k = 3 * np; k < 6 * np; ++k) m.v[k] *= mu_0 / ezmax;
+    return SCGPU_OK;
+}
+
 }  // namespace
 
 namespace sc {
+// true when the map file's first word names a 3D dynamic map (3DDynamic);
+// a 3D magnetostatic map ("3DMa") answers 2
+int fieldmap_kind_3d(const char* path) {
+    if (!path) return 0;
+    std::ifstream in(path);
+    std::string line;
+    if (!in || !content_line(in, line)) return 0;
+    if (line.compare(0, 4, "3DDy") == 0) return 1;
+    if (line.compare(0, 4, "3DMa") == 0) return 2;
+    return 0;
+}
+
+// the 3D map for the element table (sc_api.cu): grid points {nx, ny, nz},
+// ranges {xbegin, xend, ybegin, yend, zbegin, zend} [m], frequency [MHz]
+int fieldmap_3d(const char* path, int* n, double* ranges, double* freq_mhz, std::vector<double>* values) {
+    Map3D m;
+    const int rc = read_map3d(path, m);
+    if (rc) return rc;
+    n[0] = m.nx;
+    n[1] = m.ny;
+    n[2] = m.nz;
+    const double r[6] = {m.xbegin, m.xend, m.ybegin, m.yend, m.zbegin, m.zend};
+    for (int k = 0; k < 6; ++k) ranges[k] = r[k];
+    *freq_mhz = m.freq_mhz;
+    values->swap(m.v);
+    return SCGPU_OK;
+}
+
 // the map's type from its first word, as Fieldmap::readHeader does
 // (Fieldmap.cpp:296-335, the first four characters)
 bool fieldmap_is_2d(const char* path) {
@@ -370,6 +476,19 @@ int scgpu_fieldmap_2d(const char* path, int* dynamic, int* nz, int* nr, double* 
     if (values) {
         if (capacity < (long long)m.v.size()) return SCGPU_ERR_ARG;
         for (size_t k = 0; k < m.v.size(); ++k) values[k] = m.v[k];
+    }
+    return SCGPU_OK;
+}
+
+int scgpu_fieldmap_3d(const char* path, int* n, double* ranges, double* frequency_mhz, double* values,
+                      long long capacity) {
+    if (!path || !n || !ranges || !frequency_mhz) return SCGPU_ERR_ARG;
+    std::vector<double> v;
+    const int rc = sc::fieldmap_3d(path, n, ranges, frequency_mhz, &v);
+    if (rc) return rc;
+    if (values) {
+        if (capacity < (long long)v.size()) return SCGPU_ERR_ARG;
+        for (size_t k = 0; k < v.size(); ++k) values[k] = v[k];
     }
     return SCGPU_OK;
 }

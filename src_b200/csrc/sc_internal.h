@@ -93,6 +93,13 @@ int fieldmap_2d(const char* path, bool* dynamic, int* nz, int* nr, double* zbegi
                 double* rend, double* freq_mhz, std::vector<double>* values);
 // true when the map file's first word names a 2D map (2DMagnetoStatic / 2DDynamic)
 bool fieldmap_is_2d(const char* path);
+// 1 when the map file's first word names a 3D dynamic map (3DDynamic), 2 for
+// a 3D magnetostatic one, else 0
+int fieldmap_kind_3d(const char* path);
+// a 3D dynamic map (sc_fieldmap.cpp): grid points {nx, ny, nz}, ranges
+// {xbegin, xend, ybegin, yend, zbegin, zend} [m], the frequency [MHz] and the
+// values (Ex, Ey, Ez [V/m], Bx, By, Bz [T], each (i ny + j) nz + k)
+int fieldmap_3d(const char* path, int* n, double* ranges, double* freq_mhz, std::vector<double>* values);
 int particle_grid(const DevBunch& b);
 void prime_particle_grids();  // occupancy of the particle kernels, before any capture
 

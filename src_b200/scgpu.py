@@ -119,6 +119,7 @@ def lib():
         L.scgpu_add_rfcavity.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double]
         L.scgpu_fieldmap_2d.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), _dp,
                                         _dp, _dp, C.c_longlong]
+        L.scgpu_fieldmap_3d.argtypes = [C.c_char_p, C.POINTER(C.c_int), _dp, _dp, _dp, C.c_longlong]
         L.scgpu_add_multipole.argtypes = [C.c_void_p, C.c_double, C.c_double, _dp, C.c_int, _dp, _dp, C.c_int, _dp]
         L.scgpu_fieldmap_astra1d_dynamic.argtypes = [C.c_char_p, _dp, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp, _dp]
         L.scgpu_stat_row.argtypes = [C.c_void_p, _dp]
@@ -147,6 +148,7 @@ EXPORTED = [
     "scgpu_set_periodic_z", "scgpu_set_exchange", "scgpu_add_solenoid", "scgpu_clear_elements",
     "scgpu_fieldmap_astra1d", "scgpu_add_rfcavity", "scgpu_fieldmap_astra1d_dynamic", "scgpu_set_reorder_interval",
     "scgpu_launch_count", "scgpu_set_beam_frequency", "scgpu_add_multipole", "scgpu_fieldmap_2d",
+    "scgpu_fieldmap_3d",
 ]
 STAT_COLUMNS = 48
 MAX_BINS = 64
@@ -632,6 +634,24 @@ def fieldmap_2d(path):
         raise ScgpuError(rc, f"fieldmap_2d: cannot read {path}")
     return dict(dynamic=bool(dyn.value), nz=nz.value, nr=nr.value, zbegin=ranges[0], zend=ranges[1], rbegin=ranges[2],
                 rend=ranges[3], freq_mhz=f.value, values=v)
+
+
+def fieldmap_3d(path):
+    """A 3D dynamic map as the library reads it: dict with nx, ny, nz (grid
+    points), xbegin, xend, ybegin, yend, zbegin, zend [m], freq_mhz and values
+    [component, x, y, z] (Ex, Ey, Ez [V/m], Bx, By, Bz [T])."""
+    n = (C.c_int * 3)()
+    ranges = (C.c_double * 6)()
+    f = C.c_double()
+    rc = lib().scgpu_fieldmap_3d(os.fsencode(path), n, ranges, C.byref(f), None, 0)
+    if rc:
+        raise ScgpuError(rc, f"fieldmap_3d: cannot read {path}")
+    v = np.empty((6, n[0], n[1], n[2]))
+    rc = lib().scgpu_fieldmap_3d(os.fsencode(path), n, ranges, C.byref(f), _p(v), v.size)
+    if rc:
+        raise ScgpuError(rc, f"fieldmap_3d: cannot read {path}")
+    keys = ("xbegin", "xend", "ybegin", "yend", "zbegin", "zend")
+    return dict(nx=n[0], ny=n[1], nz=n[2], freq_mhz=f.value, values=v, **{k: ranges[i] for i, k in enumerate(keys)})
 
 
 def fieldmap_astra1d_dynamic(path):

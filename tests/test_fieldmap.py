@@ -244,3 +244,76 @@ def test_2d_fields_against_bilinear(oracle, tmp_path):
     # outside the z range and beyond the last radial cell: no field
     out = np.array([[0.0, 0.0, ms["zend"] + 1e-6], [0.05, 0.0, 0.1]])
     assert np.all(oracle.element_fields(es, out)[1] == 0)
+
+
+# ---------------------------------------------------------------- 3D maps
+# FM3DDynamic (src/Classic/Fields/FM3DDynamic.cpp): the library's reader
+# against the oracle's restatement, and the oracle's trilinear field against
+# numpy, including the reference's edge rules.
+
+@pytest.mark.parametrize("normalize", [None, True, False])
+def test_3d_readers_agree(sg, oracle, tmp_path, normalize):
+    from src_b200.bunch import write_3d_rfcavity_map
+    path = tmp_path / "c3d.txt"
+    write_3d_rfcavity_map(path, normalize)
+    a, b = sg.fieldmap_3d(path), oracle.read_map3d(path)
+    for key in ("nx", "ny", "nz", "xbegin", "xend", "ybegin", "yend", "zbegin", "zend", "freq_mhz"):
+        assert a[key] == b[key], key
+    np.testing.assert_array_equal(a["values"], b["values"])
+    assert (a["nx"], a["ny"], a["nz"]) == (17, 13, 81)
+    if normalize is not False:  # the largest |Ez| on the axis line is 1 MV/m in V/m
+        assert np.abs(a["values"][2, 8, 6]).max() == 1e6
+
+
+def test_3d_reader_errors(sg, tmp_path):
+    path = tmp_path / "bad.txt"
+    rows = "\n".join(["1 0 0 0 0 0"] * 8)
+    for text in (f"3DDynamic MAYBE\n1300\n-1 1 1\n-1 1 1\n0 1 1\n{rows}\n",   # flag
+                 f"3DDynamic\n1300\n-1 1 1\n-1 1 1\n0 1 1\n{rows}\n1 0 0 0 0 0\n",  # one too many
+                 "3DDynamic\n1300\n-1 1 1\n-1 1 1\n0 1 1\n" + "\n".join(["1 0 0 0 0 0"] * 7) + "\n",  # short
+                 f"3DDynamic\n1300\n-1 1 1\n-1 1 1\n0 1 1\n" + rows.replace("1 0 0 0 0 0", "1 0 0 0 0", 1) + "\n",
+                 f"3DDynamic\n1300\n1 2 1\n-1 1 1\n0 1 1\n{rows}\n",  # axis outside the grid (normalised)
+                 f"2DDynamic XZ\n0 1 1\n1300\n0 1 1\n{rows}\n"):
+        path.write_text(text)
+        with pytest.raises(sg.ScgpuError):
+            sg.fieldmap_3d(path)
+
+
+def _trilinear(F, h, X):
+    u = X / h
+    i = np.floor(u).astype(int)
+    l = u - i
+    out = 0.0
+    for a in (0, 1):
+        for b in (0, 1):
+            for c in (0, 1):
+                w = (l[:, 0] if a else 1 - l[:, 0]) * (l[:, 1] if b else 1 - l[:, 1]) * (l[:, 2] if c else 1 - l[:, 2])
+                out = out + w * F[i[:, 0] + a, i[:, 1] + b, i[:, 2] + c]
+    return out
+
+
+def test_3d_field_against_trilinear(oracle, tmp_path):
+    from src_b200.bunch import write_3d_rfcavity_map
+    rng = np.random.default_rng(4)
+    path = tmp_path / "c3d.txt"
+    write_3d_rfcavity_map(path)
+    m = oracle.read_map3d(path)
+    e = oracle.make_rfcavity3d(m, 0.0, 20.0, 1300.0, 0.3)
+    h = np.array([e.hx, e.hy, e.hz])
+    lo = np.array([m["xbegin"], m["ybegin"], m["zbegin"]])
+    # inside: below the last two grid planes of every axis
+    top = lo + h * (np.array([m["nx"], m["ny"], m["nz"]]) - 2)
+    R = lo + (top - lo) * rng.uniform(0, 0.999, (300, 3))
+    t = 1.1e-10
+    E, B = oracle.element_fields(e, R, t)
+    ce, sb = 20.0 * np.cos(e.omega * t + 0.3), 20.0 * np.sin(e.omega * t + 0.3)
+    v = m["values"]
+    for c in range(3):
+        np.testing.assert_allclose(E[:, c], ce * _trilinear(v[c], h, R - lo), rtol=1e-12, atol=1e-6)
+        np.testing.assert_allclose(B[:, c], -sb * _trilinear(v[3 + c], h, R - lo), rtol=1e-12, atol=1e-18)
+    assert np.abs(E).min() > 0
+    # the last two planes of each axis, before the start, outside z: no field
+    out = np.array([[top[0] + 1e-9, 0.0, 0.1], [0.0, top[1] + 1e-9, 0.1], [0.0, 0.0, top[2] + 1e-9],
+                    [lo[0] - 1e-9, 0.0, 0.1], [0.0, 0.0, -1e-9], [0.0, 0.0, m["zend"] + 1e-6]])
+    E, B = oracle.element_fields(e, out, t)
+    assert np.all(E == 0) and np.all(B == 0)

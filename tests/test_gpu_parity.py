@@ -677,6 +677,46 @@ def test_tracking_with_2d_field_maps_vs_oracle(oracle, gpu, tmp_path):
     assert rel(Pg[:, :2], Pn[:, :2]) > 1e-3  # the solenoid acts
 
 
+def test_tracking_with_3d_rfcavity_map_vs_oracle(oracle, gpu, tmp_path):
+    """RFCAVITY with a 3DDynamic map (FM3DDynamic::getFieldstrength, the
+    trilinear (x, y, z) interpolation of E and B): the bunch inside the
+    cavity, 20 steps against the oracle; a 3D magnetostatic map is refused."""
+    from src_b200.bunch import write_3d_rfcavity_map
+    N, nr, steps = 50_000, (32, 32, 32), 20
+    cav = tmp_path / "cav3d.txt"
+    write_3d_rfcavity_map(cav, normalize=True)
+    R, P = gaussian_bunch(N, bunch_id=16)
+    Q = -1e-9 / N
+    edge, volt, freq, lag = -0.05, 25.0, 1300.0, 0.7
+    m = oracle.read_map3d(cav)
+    oracle.set_solenoids([oracle.make_rfcavity3d(m, edge, volt, freq, lag)])
+    try:
+        tr = oracle.OracleTracker(oracle.make_params(nr, 1e-12), Q)
+        Ro, Po = R.copy(), P.copy()
+        tr.track(Ro, Po, steps)
+    finally:
+        oracle.set_solenoids([])
+    mag = tmp_path / "mag3d.txt"
+    mag.write_text("3DMagnetoStatic\n-1 1 1\n-1 1 1\n0 1 1\n" + "\n".join(["0 0 1"] * 8) + "\n")
+    with gpu.Context(nr) as ctx:
+        with pytest.raises(gpu.ScgpuError):  # FM3DMagnetoStatic is not built
+            ctx.add_solenoid(mag, 0.0, 1.0)
+        ctx.add_rfcavity(cav, edge, volt, freq, lag)
+        ctx.upload(R, P, 1e-12, Q, oracle.electron_mass_ev())
+        ctx.track(steps)
+        Rg, Pg = ctx.download()
+        st = ctx.tracker_state()
+        ctx.clear_elements()
+        ctx.upload(R, P, 1e-12, Q, oracle.electron_mass_ev())
+        ctx.track(steps)
+        Rn, Pn = ctx.download()
+    assert rel(Rg, Ro) < STATE_TOL and rel(Pg, Po) < STATE_TOL
+    assert abs(st["path_length"] - tr.path_length) <= 1e-14 * abs(tr.path_length)
+    np.testing.assert_allclose(st["ref_P"], tr.ref_P, rtol=1e-13, atol=1e-18)
+    assert rel(Pg[:, 2], Pn[:, 2]) > 1e-4  # the cavity acts
+    assert rel(Pg[:, :2], Pn[:, :2]) > 1e-4  # and its transverse fields
+
+
 def test_tracking_with_multipole_vs_oracle(oracle, gpu):
     """MULTIPOLE elements (Multipole::computeField, the component scaling of
     setNormalComponent / setSkewComponent): a quadrupole with dipole,
