@@ -483,6 +483,12 @@ int scgpu_batch_track(scgpu_batch* batch, int nsteps);
  * device errors.  Removing a slot waits for steps in flight. */
 int scgpu_batch_launch(scgpu_batch* batch, int nsteps);
 int scgpu_batch_wait(scgpu_batch* batch);
+/* 1 when the launched steps have finished on the device (or none are in
+ * flight), 0 while they run; never blocks.  A serving loop admits arriving
+ * bunches while this is 0 and launches the next steps once it is 1, so the
+ * device does not idle behind a long admission.  (No counterpart in the
+ * reference: OPAL runs one simulation per process.) */
+int scgpu_batch_done(scgpu_batch* batch);
 /* Removed bunches leave their contexts (device buffers) parked for reuse by
  * later bunches on the same mesh; trim frees the parked ones. */
 int scgpu_batch_trim(scgpu_batch* batch);

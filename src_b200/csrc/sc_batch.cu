@@ -492,6 +492,16 @@ int scgpu_batch_wait(scgpu_batch* b) {
     return wait(b);
 }
 
+int scgpu_batch_done(scgpu_batch* b) {
+    if (!b) return SCGPU_ERR_ARG;
+    if (!b->in_flight || b->members.empty()) return 1;
+    cudaSetDevice(b->device);
+    const cudaError_t e = cudaEventQuery(b->ev_t1);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) return 0;
+    return bfail(b, SCGPU_ERR_CUDA, std::string("batch_done: ") + cudaGetErrorString(e));
+}
+
 scgpu_ctx* scgpu_batch_member(scgpu_batch* b, int slot) {
     if (!b || slot < 0 || slot >= (int)b->slots.size()) return nullptr;
     return b->slots[slot];

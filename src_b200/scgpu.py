@@ -428,6 +428,7 @@ def _batch_lib():
         L.scgpu_batch_autotune.argtypes = [C.c_void_p, C.c_int]
         L.scgpu_batch_launch.argtypes = [C.c_void_p, C.c_int]
         L.scgpu_batch_wait.argtypes = [C.c_void_p]
+        L.scgpu_batch_done.argtypes = [C.c_void_p]
         L.scgpu_batch_trim.argtypes = [C.c_void_p]
         L._batch_ready = True
     return L
@@ -438,7 +439,7 @@ EXPORTED += [
     "scgpu_batch_create", "scgpu_batch_destroy", "scgpu_batch_last_error", "scgpu_batch_add", "scgpu_batch_remove",
     "scgpu_batch_member", "scgpu_batch_size", "scgpu_batch_track", "scgpu_batch_last_track_ms",
     "scgpu_batch_set_tuning", "scgpu_batch_get_tuning", "scgpu_batch_autotune", "scgpu_batch_launch",
-    "scgpu_batch_wait", "scgpu_batch_trim",
+    "scgpu_batch_wait", "scgpu_batch_trim", "scgpu_batch_done",
 ]
 
 
@@ -538,6 +539,13 @@ class Batch:
         """Finishes launched steps; returns their device milliseconds."""
         self._check(_batch_lib().scgpu_batch_wait(self.h), "batch_wait")
         return _batch_lib().scgpu_batch_last_track_ms(self.h)
+
+    def done(self):
+        """True when the launched steps have finished on the device (never blocks)."""
+        rc = _batch_lib().scgpu_batch_done(self.h)
+        if rc < 0:
+            self._check(rc, "batch_done")
+        return rc == 1
 
     def trim(self):
         """Frees the parked contexts of removed bunches."""

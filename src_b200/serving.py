@@ -196,7 +196,9 @@ class Server:
         Each round launches k steps for the current slots and, while the
         device works, admits the jobs that have arrived (their bunches were
         prepared in pinned memory by the Preparer thread and are uploaded
-        meanwhile; they join at the next round).  prepare_ahead = 0 prepares
+        meanwhile; they join at the next round) until the round has
+        finished on the device; jobs not yet admitted wait for the next
+        round.  prepare_ahead = 0 prepares
         each bunch on the serving thread at admission instead."""
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival_s))
         active = {}   # slot -> [job, remaining steps, admitted_s, footprint]
@@ -209,9 +211,14 @@ class Server:
             prep = Preparer(self.masters, max(j.particles for j in pending), depth=prepare_ahead, realtime=realtime)
             prep.start(pending, t0)
 
-        def admit():
+        def admit(in_round):
+            # While a round runs, admit until it has finished on the device:
+            # an admission waits for its upload, and a round left finished
+            # behind a long admission would idle the device.
             t = now()
             while pending and (not realtime or pending[0].arrival_s <= t):
+                if in_round and self.batch.done():
+                    break
                 job = pending[0]
                 fp = job.footprint_bytes(self.precision)
                 if (active or joining) and self.used + fp > self.budget:
@@ -237,7 +244,7 @@ class Server:
                 tt = time.perf_counter()
                 self.batch.launch(k)
                 self.time["track_wall_s"] += time.perf_counter() - tt
-            admit()
+            admit(k > 0)
             if k:
                 tt = time.perf_counter()
                 gpu_ms = self.batch.wait()

@@ -7,13 +7,20 @@ from src_b200.workloads import Job, batched_jobs, serving_jobs
 
 
 class FakeBatch:
-    def __init__(self):
+    """done_after: the round in flight reports itself finished on the device
+    once that many bunches were admitted during it (None: never)."""
+
+    def __init__(self, done_after=None):
         self.slots = {}
         self.steps = {}
         self.tracked = []
         self.peak = 0
+        self.done_after = done_after
+        self.in_round = 0
+        self.admits_per_round = []
 
     def add(self, nr, R, P, dT, q, mass, **kw):
+        self.in_round += 1
         slot = min(set(range(len(self.slots) + 1)) - set(self.slots))
         self.slots[slot] = R.shape[0]
         self.steps[slot] = 0
@@ -23,7 +30,12 @@ class FakeBatch:
     def remove(self, slot):
         del self.slots[slot]
 
+    def done(self):
+        return self.done_after is not None and self.in_round >= self.done_after
+
     def launch(self, k):
+        self.admits_per_round.append(self.in_round)
+        self.in_round = 0
         self.tracked.append((k, len(self.slots)))
         for s in self.slots:
             self.steps[s] += k
@@ -118,3 +130,23 @@ def test_preparer_thread_matches_inline_preparation():
         res = srv.run(jobs, realtime=False, prepare_ahead=ahead)
         out.append(([r.job.job_id for r in res], fb.tracked))
     assert out[0] == out[1]
+
+
+def test_admission_stops_when_the_round_has_finished():
+    """While a round runs, jobs are admitted until the device reports the
+    round finished; the rest wait for the next round, and every job still
+    takes exactly its steps.  The HBM budget holds three jobs, so all but
+    the first three are admitted during rounds."""
+    jobs = [job(i, steps=2 + (i % 4)) for i in range(12)]
+    fp = jobs[0].footprint_bytes(0)
+    for done_after, bound in ((1, 1), (2, 2), (None, 3)):
+        fb = FakeBatch(done_after=done_after)
+        srv = Server(hbm_budget_bytes=3 * fp, batch=fb, masters=FakeMasters())
+        res = srv.run(jobs, realtime=False)
+        assert sorted(r.job.job_id for r in res) == list(range(12))
+        assert srv.particle_steps == sum(j.particles * j.steps for j in jobs)
+        assert fb.admits_per_round[0] == 3  # no round in flight yet: as many as fit
+        assert sum(fb.admits_per_round) + fb.in_round == 12
+        assert max(fb.admits_per_round[1:]) <= bound
+        if done_after is not None:
+            assert max(fb.admits_per_round[1:]) == bound
