@@ -4,8 +4,9 @@ sums and the momentum / moment sums are exact integers, so no result depends
 on which rank holds which particle.
 
 Only one GPU is available to these tests: the ranks are host threads with one
-context each (HostExchange), or two processes on the same GPU that exchange
-through gloo (TorchExchange).  No kernel waits on another rank; the ranks
+context each (HostExchange), two processes on the same GPU that exchange
+through gloo (TorchExchange), or one rank of an NCCL group (TorchExchange's
+device all-reduces).  No kernel waits on another rank; the ranks
 meet on the host between kernels.
 """
 import os
@@ -80,14 +81,21 @@ def test_shards_equal_whole_bunch(gpu, N, nr, steps, cuts):
         np.testing.assert_array_equal(row_r[:42], row[:42])
 
 
-def _gloo_rank(rank, world, port, path):
+def _gloo_rank(rank, world, port, path, backend="gloo"):
+    import datetime
+
+    import torch
     import torch.distributed as dist
     from src_b200 import scgpu
     from src_b200.sharding import TorchExchange, attach
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    kw = {}
+    if backend == "nccl":
+        torch.cuda.set_device(0)
+        kw["device_id"] = torch.device("cuda", 0)
+    dist.init_process_group(backend, rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120), **kw)
     try:
         d = np.load(path)
         R, P, cuts = d["R"], d["P"], d["cuts"]
@@ -121,6 +129,30 @@ def test_two_processes_over_gloo(gpu, tmp_path):
     parts = [np.load(path.replace(".npz", f"_r{r}.npz")) for r in range(2)]
     np.testing.assert_array_equal(np.concatenate([p["R"] for p in parts]), Rs)
     np.testing.assert_array_equal(np.concatenate([p["P"] for p in parts]), Ps)
+
+
+def test_one_rank_over_nccl(gpu, tmp_path):
+    """TorchExchange's NCCL branch on the hardware: one rank of an NCCL
+    process group (the only GPU these tests have) runs the exchanges -- the
+    bounds' min and the exact integer sums as device all-reduces on the
+    context's stream -- and must give the single context's bits."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    N = 20_000
+    R, P = gaussian_bunch(N, bunch_id=10)
+    Rs, Ps, *_ = _single(gpu, R, P, (16, 16, 16), 6, -1e-9 / N)
+    path = str(tmp_path / "bunch.npz")
+    np.savez(path, R=R, P=P, cuts=np.array([0, N]))
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    mp.start_processes(_gloo_rank, args=(1, port, path, "nccl"), nprocs=1, start_method="spawn", join=True)
+    d = np.load(path.replace(".npz", "_r0.npz"))
+    np.testing.assert_array_equal(d["R"], Rs)
+    np.testing.assert_array_equal(d["P"], Ps)
 
 
 def test_shard_limits(gpu):
