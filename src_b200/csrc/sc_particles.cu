@@ -561,10 +561,10 @@ __device__ __forceinline__ long long join(long long hi, long long lo) { return h
 constexpr int kMaxGroupPasses = 4;
 
 // Node accumulator: two 64-bit words (L, H) holding the value H 2^32 + L.
-// A group sum v (|v| < 2^56) adds its low 32 bits to L and its arithmetic
-// high part v >> 32 to H, both as fire-and-forget atomics (no returned value
-// is waited for).  L stays below 2^64 for fewer than 2^32 additions; H is a
-// signed sum of terms below 2^24.  Integer additions commute, so the value
+// A group sum v (|v| < 2^57: up to 64 charges below 2^51) adds its low 32
+// bits to L and its arithmetic high part v >> 32 to H, both as
+// fire-and-forget atomics (no returned value is waited for).  L stays below
+// 2^64 for fewer than 2^32 additions; H is a signed sum of terms below 2^25.  Integer additions commute, so the value
 // is the same in any order.
 __device__ __forceinline__ void acc_add(unsigned long long* a, long long v) {
     atomicAdd(a, (unsigned long long)v & 0xffffffffull);
@@ -678,11 +678,126 @@ __device__ __forceinline__ void deposit_body(const BunchConst& bc, const double*
     }
     if (bad) atomicOr(&st->err, kFlagGuard);
 }
+// The charge deposit of a bunch without bins or periodic z, two particles per
+// lane: a warp takes 64 consecutive (cell-ordered) particles, lane l the
+// pair 2l, 2l + 1 (one 16-byte load per coordinate).  A pair in one cell
+// enters the warp's group reduction as the sum of its two fixed-point
+// charges (|t_a + t_b| < 2^52, split into a 27-bit low limb and the signed
+// rest, so 32 lanes' limb sums fit 32 bits), which halves the reduction
+// passes per particle where cells are dense; the second particle of a pair
+// that straddles a cell boundary adds its own charges.  The node values are
+// the same integer sums as deposit_body's, so rho has the same bits.
+__device__ __forceinline__ void deposit_pairs_body(const BunchConst& bc, const double* __restrict__ x,
+                                                   const double* __restrict__ y, const double* __restrict__ z,
+                                                   StepState* st, unsigned long long* __restrict__ acc, VB g) {
+    __shared__ MeshConsts ms;
+    __shared__ double qdt_s, to_int_s;
+    load_mesh_consts(ms, st);
+    if (threadIdx.x == 0) {
+        qdt_s = st->qdt;
+        to_int_s = ldexp(1.0, kFxFrac - fx_exponent(st->qdt));
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nx = bc.n[0], nxy = bc.n[0] * bc.n[1];
+    const long long span = 2ll * blockDim.x;
+    bool bad = false;
+    for (long long i0 = (long long)g.blk * span; i0 < bc.N; i0 += (long long)g.nblk * span) {
+        const long long ia = i0 + 64ll * warp + 2 * lane, ib = ia + 1;
+        const bool va = ia < bc.N, vb = ib < bc.N;
+        double Xa[3] = {0.0, 0.0, 0.0}, Xb[3] = {0.0, 0.0, 0.0};
+        if (vb) {  // ia is even: the pair is one aligned 16-byte load per coordinate
+            const double2 px = *reinterpret_cast<const double2*>(x + ia);
+            const double2 py = *reinterpret_cast<const double2*>(y + ia);
+            const double2 pz = *reinterpret_cast<const double2*>(z + ia);
+            Xa[0] = px.x, Xa[1] = py.x, Xa[2] = pz.x;
+            Xb[0] = px.y, Xb[1] = py.y, Xb[2] = pz.y;
+        } else if (va) {
+            Xa[0] = x[ia], Xa[1] = y[ia], Xa[2] = z[ia];
+        }
+        uint32_t ka = 0xffffffffu, kb = 0xfffffffeu;
+        int la[3], lb[3];
+        double da[3], db[3];
+        const MeshConsts* m = fresh(&ms);
+        if (va) {
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, Xa, la, da)) bad = true;
+            ka = (uint32_t)(la[0] + nx * la[1] + nxy * la[2]);
+        }
+        if (vb) {
+            if (!cic_locate_r(m->hr, m->rhr, m->org, bc.n, Xb, lb, db)) bad = true;
+            kb = (uint32_t)(lb[0] + nx * lb[1] + nxy * lb[2]);
+        }
+        const bool same = vb && ka == kb;
+        const double q = *fresh(&qdt_s), to_int = *fresh(&to_int_s);
+        long long T[8];
+        {
+            double c[8];
+            if (va) {
+                cic_charge(da, q, c);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) c[k] = 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) T[k] = __double2ll_rn(c[k] * to_int);
+        }
+        if (vb) {
+            double c[8];
+            cic_charge(db, q, c);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const long long t = __double2ll_rn(c[k] * to_int);
+                if (same) {
+                    T[k] += t;
+                } else {
+                    const int node = (int)kb + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
+                    acc_add(acc + 2 * (long long)node, t);
+                }
+            }
+        }
+        const unsigned group = __match_any_sync(kFull, ka);
+        const int gsize = __popc(group);
+        const bool leader = lane == __ffs(group) - 1;
+        unsigned multi = __ballot_sync(kFull, leader && gsize > 1);
+        const bool passes = __popc(multi) <= kMaxGroupPasses;
+        if (va && (gsize == 1 || !passes)) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int node = (int)ka + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
+                acc_add(acc + 2 * (long long)node, T[k]);
+            }
+        }
+        while (passes && multi) {
+            const int ld = __ffs(multi) - 1;
+            multi &= multi - 1;
+            const bool in = (__shfl_sync(kFull, group, ld) >> lane) & 1u;
+            long long sum[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int hi = __reduce_add_sync(kFull, in ? (int)(T[k] >> 27) : 0);
+                const unsigned lo = __reduce_add_sync(kFull, in ? (unsigned)(T[k] & 0x7ffffffll) : 0u);
+                sum[k] = (long long)hi * (1ll << 27) + (long long)lo;
+            }
+            if (va && lane == ld) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int node = (int)ka + (k & 1) + ((k >> 1) & 1) * nx + ((k >> 2) & 1) * nxy;
+                    acc_add(acc + 2 * (long long)node, sum[k]);
+                }
+            }
+        }
+    }
+    if (bad) atomicOr(&st->err, kFlagGuard);
+}
+
 template <bool PZ>
 __global__ void __launch_bounds__(kThreads) k_deposit(BunchConst bc, const double* __restrict__ x, const double* __restrict__ y,
                                                       double* __restrict__ z, StepState* st,
                                                       unsigned long long* __restrict__ acc) {
-    deposit_body<false, PZ>(bc, x, y, z, nullptr, 0, st, acc, vb_grid());
+    if constexpr (PZ)
+        deposit_body<false, true>(bc, x, y, z, nullptr, 0, st, acc, vb_grid());
+    else
+        deposit_pairs_body(bc, x, y, z, st, acc, vb_grid());
 }
 __global__ void __launch_bounds__(kThreads) k_deposit_bins(BunchConst bc, const double* __restrict__ x,
                                                            const double* __restrict__ y, double* __restrict__ z,
@@ -1712,7 +1827,7 @@ __global__ void __launch_bounds__(NT) k_deposit_batch(const DevBunch* __restrict
     if constexpr (MIXED)
         deposit_mixed_body<false>(d.bc, d.x, d.y, d.z, d.st, d.nacc, VB{w.y, w.w});
     else
-        deposit_body<false>(d.bc, d.x, d.y, d.z, nullptr, 0, d.st, d.nacc, VB{w.y, w.w});
+        deposit_pairs_body(d.bc, d.x, d.y, d.z, d.st, d.nacc, VB{w.y, w.w});
 }
 
 template <typename T>
