@@ -219,7 +219,7 @@ bool range_line(std::ifstream& in, double& a, double& b, int& n) {
     std::istringstream is(line);
     std::string rest;
     if (!(is >> a >> b >> n) || (is >> rest)) return false;
-    return n >= 1;
+    return n >= 1 && n <= (1 << 26);  // interval counts; the grid sizes are checked by the callers
 }
 
 int read_map2d(const char* path, Map2D& m) {
