@@ -58,6 +58,29 @@ def test_batch_equals_alone(gpu, precision):
         assert st["path_length"] == sta["path_length"] and st["t"] == sta["t"]
 
 
+def test_batch_done_reports_the_round(gpu):
+    """scgpu_batch_done never blocks: true with nothing in flight, and true
+    once launched steps have finished (polled with a bounded wait); the
+    steps' results are those of a plain track."""
+    import time
+
+    b = make(0, BUNCHES[2])
+    with gpu.Batch(precision=0) as bt:
+        assert bt.done()
+        s = bt.add(b["nr"], b["R"], b["P"], DT, b["Q"], MASS, bz_ext=b["bz"], ref_P=b["ref_P"])
+        bt.launch(6)
+        t0 = time.perf_counter()
+        while not bt.done() and time.perf_counter() - t0 < 30.0:
+            time.sleep(1e-3)
+        assert bt.done()
+        bt.wait()
+        assert bt.done()
+        R, P = bt.member(s).download()
+    Ra, Pa, _, _ = alone(gpu, b, 6, 0)
+    np.testing.assert_array_equal(R, Ra)
+    np.testing.assert_array_equal(P, Pa)
+
+
 def test_batch_membership_changes_and_autotune(gpu):
     """Bunches join and leave between steps (continuous batching) and the
     autotuner switches launch shapes; each bunch still matches its alone run
