@@ -285,8 +285,8 @@ void enqueue_bins_fields(scgpu_ctx* c, cudaStream_t s) {
     for (int k = 0; k < b.nactive; ++k) {
         const DevBunch v = bin_view(c, k);
         if (k >= 2) cudaStreamWaitEvent(c->side, c->ev_used[k - 2], 0);
-        launch_igf(v, nullptr, c->side);
-        launch_green_transform(v, c->side);
+        launch_igf_tmp(v, c->side);
+        launch_green_transform_from_tmp(v, c->side);
         launch_igf_image(v, c->side);
         launch_green_transform_image(v, c->side);
         cudaEventRecord(c->ev_bin[k], c->side);
@@ -376,11 +376,13 @@ void enqueue_reorder(scgpu_ctx* c, cudaStream_t s) {
 // The Green's function and its spectrum (open or periodic z), shared by the
 // step and the solver entry points.
 void enqueue_green(scgpu_ctx* c, cudaStream_t s) {
-    launch_igf(c->b, nullptr, s);
-    if (c->b.periodic_z)
+    if (c->b.periodic_z) {
+        launch_igf(c->b, nullptr, s);
         launch_green_transform_periodic(c->b, s);
-    else
-        launch_green_transform(c->b, s);
+    } else {
+        launch_igf_tmp(c->b, s);
+        launch_green_transform_from_tmp(c->b, s);
+    }
 }
 
 // one ParallelTTracker step on the context's stream

@@ -176,9 +176,7 @@ int rebuild(scgpu_batch* b) {
     add_per_bunch(1, kBatchIgfTmp, [](const DevBunch& d) {
         return blocks_for((long long)(d.bc.n[0] + 2) * (d.bc.n[1] + 2) * (d.bc.n[2] + 2), 256, kCellGridCap);
     });
-    add_per_bunch(1, kBatchIgfG, [](const DevBunch& d) {
-        return blocks_for((long long)(d.bc.n[0] + 1) * (d.bc.n[1] + 1) * (d.bc.n[2] + 1), 256, kCellGridCap);
-    });
+    // G is formed from the antiderivative inside the z cosine transforms
     add_pass(1, kPassDctZ);
     add_pass(1, kPassDctY);
     add_pass(1, kPassDctX);

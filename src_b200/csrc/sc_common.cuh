@@ -689,6 +689,25 @@ SC_HD void kick_one(double* P, const double* Ef, const double* Bf, double dt, do
     P[2] += ke * Ef[2];
 }
 
+// ---------------------------------------------------------------- Green's function
+// G at grid point (i, j, k) from the IGF antiderivative tmp on the (n0+2) x
+// (n1+2) x (n2+2) grid: the 8-corner difference of FFTPoissonSolver.cpp
+// :508-516 in its order, with G[0,0,0] <- G[0,0,1] (mirrorRhoField, :657).
+// t0 = n0 + 2, t1 = n1 + 2.
+SC_HD double igf_G_at(const double* __restrict__ tmp, int t0, int t1, int i, int j, int k) {
+    if (i == 0 && j == 0 && k == 0) k = 1;
+    auto T = [&](int a, int b, int e) { return tmp[(size_t)a + (size_t)t0 * ((size_t)b + (size_t)t1 * e)]; };
+    double g = T(i + 1, j + 1, k + 1);
+    g += T(i + 1, j, k);
+    g += T(i, j + 1, k);
+    g += T(i, j, k + 1);
+    g -= T(i + 1, j + 1, k);
+    g -= T(i + 1, j, k + 1);
+    g -= T(i, j + 1, k + 1);
+    g -= T(i, j, k);
+    return g;
+}
+
 // ---------------------------------------------------------------- division
 // a / b, correctly rounded, from rb = RN(1/b): one product, then the
 // remainder a - q0 b (exact with an FMA) corrects q0 (Markstein, IBM J. Res.

@@ -917,10 +917,14 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_fft_z_c2r(const Cx<T>* __rest
 // Cosine transform of every line along one axis: Y[m] = sum over the even
 // extension (length L = 2(len-1)) of g, m in [0, len-1].  Lines are addressed
 // as in[b * sb + o * so + e * se]; 2 NC lines per block (two per complex FFT).
-template <typename TO, int LT, int NC, int NT>
+// FROM_TMP (the z lines, b = x, o = y, e = z): in is the IGF antiderivative
+// on the (t0 = n0+2) x (t1 = n1+2) grid and each element of G is formed from
+// it as it is staged (igf_G_at), so G itself is never stored.
+template <typename TO, int LT, int NC, int NT, bool FROM_TMP = false>
 __device__ __forceinline__ void dct_lines_body(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
                                                long long sb, long long so, long long se, const FftPlan& pl,
-                                               const double2* __restrict__ twd, int bx, int by) {
+                                               const double2* __restrict__ twd, int bx, int by, int t0 = 0,
+                                               int t1 = 0) {
     constexpr int RC = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L = LT > 0 ? LT : pl.L;
@@ -938,9 +942,15 @@ __device__ __forceinline__ void dct_lines_body(const double* __restrict__ in, TO
         const bool inner = m >= 1 && m <= len - 2;
         double* mir = reinterpret_cast<double*>(&buf[(li >> 1) * CS + sk(inner ? L - m : m)]) + (li & 1);
         if (b < nb) {
-            const double* src = in + (long long)b * sb + obase + (long long)m * se;
-            cp_elem(slot, src);
-            if (inner) cp_elem(mir, src);
+            if constexpr (FROM_TMP) {
+                const double v = igf_G_at(in, t0, t1, b, by, m);
+                *slot = v;
+                if (inner) *mir = v;
+            } else {
+                const double* src = in + (long long)b * sb + obase + (long long)m * se;
+                cp_elem(slot, src);
+                if (inner) cp_elem(mir, src);
+            }
         } else {
             *slot = 0.0;
             if (inner) *mir = 0.0;
@@ -957,11 +967,11 @@ __device__ __forceinline__ void dct_lines_body(const double* __restrict__ in, TO
         out[(long long)b * sb + obase + (long long)m * se] = (TO)((li & 1) ? v.y : v.x);
     }
 }
-template <typename TO, int LT, int NC, int NT>
+template <typename TO, int LT, int NC, int NT, bool FROM_TMP = false>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_dct_lines(const double* __restrict__ in, TO* __restrict__ out, int len, int nb,
                                                   long long sb, long long so, long long se, FftPlan pl,
-                                                  const double2* __restrict__ twd) {
-    dct_lines_body<TO, LT, NC, NT>(in, out, len, nb, sb, so, se, pl, twd, blockIdx.x, blockIdx.y);
+                                                  const double2* __restrict__ twd, int t0, int t1) {
+    dct_lines_body<TO, LT, NC, NT, FROM_TMP>(in, out, len, nb, sb, so, se, pl, twd, blockIdx.x, blockIdx.y, t0, t1);
 }
 
 // Full real transform of lines of length L along z (stride se), 2 NC lines
@@ -1232,7 +1242,7 @@ struct LaunchE {
     }
 };
 
-template <typename TO>
+template <typename TO, bool FROM_TMP = false>
 struct LaunchDct {
     const double* in;
     TO* out;
@@ -1241,6 +1251,7 @@ struct LaunchDct {
     FftPlan pl;
     const double2* tw;
     cudaStream_t s;
+    int t0 = 0, t1 = 0;
     template <int LT>
     void run() {
         with_variant<LT>(*this);
@@ -1249,7 +1260,8 @@ struct LaunchDct {
     void go() {
         constexpr int NC = Geo<LT, V>::NC, NT = Geo<LT, V>::NT;
         dim3 g((unsigned)((nb + 2 * NC - 1) / (2 * NC)), (unsigned)outer);
-        k_dct_lines<TO, LT, NC, NT><<<g, NT, smem_of<double2>(pl.L, NC), s>>>(in, out, len, nb, sb, so, se, pl, tw);
+        k_dct_lines<TO, LT, NC, NT, FROM_TMP><<<g, NT, smem_of<double2>(pl.L, NC), s>>>(in, out, len, nb, sb, so, se, pl,
+                                                                                     tw, t0, t1);
     }
 };
 
@@ -1282,6 +1294,7 @@ struct SetLimits {
         allow(k_fft_z_c2r<double, false, LT, NC, NT>);
         allow(k_dct_lines<double, LT, NC, NT>);
         allow(k_dct_lines<float, LT, NC, NT>);
+        allow(k_dct_lines<double, LT, NC, NT, true>);
         allow(k_fft_x_conv<double, double, LT, NC, NT, true>);
         allow(k_fft_x_conv<float, double, LT, NC, NT, true>);
         allow(k_fft_z_c2r<double, true, LT, NC, NT, true>);
@@ -1348,14 +1361,16 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_fft_pass_batch(const DevBunch
                                                  normFact, d.bc.coupling, w.y, w.z);
     } else {
         const long long g0 = n0 + 1, g1 = n1 + 1, g2 = n2 + 1;
+        // G formed from the antiderivative in the z pass (gtmp -> gline ->
+        // gtmp -> ghat), as launch_green_transform_from_tmp
         if constexpr (PASS == kPassDctZ)
-            dct_lines_body<double, LT, NC, NT>(d.gline, d.gtmp, (int)g2, (int)g0, 1, g0, g0 * g1, plan_dev(L2),
-                                               tw_dev<double>(d, 2), w.y, w.z);
+            dct_lines_body<double, LT, NC, NT, true>(d.gtmp, d.gline, (int)g2, (int)g0, 1, g0, g0 * g1, plan_dev(L2),
+                                                     tw_dev<double>(d, 2), w.y, w.z, n0 + 2, n1 + 2);
         else if constexpr (PASS == kPassDctY)
-            dct_lines_body<double, LT, NC, NT>(d.gtmp, d.gline, (int)g1, (int)g0, 1, g0 * g1, g0, plan_dev(L1),
+            dct_lines_body<double, LT, NC, NT>(d.gline, d.gtmp, (int)g1, (int)g0, 1, g0 * g1, g0, plan_dev(L1),
                                                tw_dev<double>(d, 1), w.y, w.z);
         else
-            dct_lines_body<T, LT, NC, NT>(d.gline, (T*)d.ghat, (int)g0, (int)g1, g0, g0 * g1, 1, plan_dev(L0),
+            dct_lines_body<T, LT, NC, NT>(d.gtmp, (T*)d.ghat, (int)g0, (int)g1, g0, g0 * g1, 1, plan_dev(L0),
                                           tw_dev<double>(d, 0), w.y, w.z);
     }
 }
@@ -1605,6 +1620,29 @@ void launch_green_transform(const DevBunch& b, cudaStream_t s) {
         with_length(2 * n0, LaunchDct<double>{b.gline, (double*)b.ghat, (int)g0, (int)g1, (int)g2, g0, g0 * g1, 1, p0, tw0, s});
     else
         with_length(2 * n0, LaunchDct<float>{b.gline, (float*)b.ghat, (int)g0, (int)g1, (int)g2, g0, g0 * g1, 1, p0, tw0, s});
+}
+
+// The same spectrum from the antiderivative (b.gtmp, launch_igf_tmp): the
+// z transforms form G as they stage it and write gline, the y transforms
+// gline -> gtmp, the x transforms gtmp -> ghat.  G's values and every
+// transform are those of launch_igf + launch_green_transform, so Ĝ has the
+// same bits; G is never stored.
+void launch_green_transform_from_tmp(const DevBunch& b, cudaStream_t s) {
+    const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    const long long g0 = n0 + 1, g1 = n1 + 1, g2 = n2 + 1;
+    const FftPlan p0 = make_plan(2 * n0), p1 = make_plan(2 * n1), p2 = make_plan(2 * n2);
+    const double2* tw0 = reinterpret_cast<const double2*>(b.tw[0]);
+    const double2* tw1 = reinterpret_cast<const double2*>(b.tw[1]);
+    const double2* tw2 = reinterpret_cast<const double2*>(b.tw[2]);
+    LaunchDct<double, true> z{b.gtmp, b.gline, (int)g2, (int)g0, (int)g1, 1, g0, g0 * g1, p2, tw2, s};
+    z.t0 = n0 + 2;
+    z.t1 = n1 + 2;
+    with_length(2 * n2, z);
+    with_length(2 * n1, LaunchDct<double>{b.gline, b.gtmp, (int)g1, (int)g0, (int)g2, 1, g0 * g1, g0, p1, tw1, s});
+    if (b.precision == 0)
+        with_length(2 * n0, LaunchDct<double>{b.gtmp, (double*)b.ghat, (int)g0, (int)g1, (int)g2, g0, g0 * g1, 1, p0, tw0, s});
+    else
+        with_length(2 * n0, LaunchDct<float>{b.gtmp, (float*)b.ghat, (int)g0, (int)g1, (int)g2, g0, g0 * g1, 1, p0, tw0, s});
 }
 
 // Spectrum of the image's shifted G (b.gimg, (n0+1)(n1+1)(2 n2), FP64):

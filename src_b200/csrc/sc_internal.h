@@ -112,6 +112,7 @@ void launch_cell_keys(const DevBunch& b, int digit_bits, cudaStream_t s);
 void launch_deposit(const DevBunch& b, cudaStream_t s);
 void launch_assemble_rho(const DevBunch& b, cudaStream_t s);
 void launch_igf(const DevBunch& b, const double* hr_host, cudaStream_t s);
+void launch_igf_tmp(const DevBunch& b, cudaStream_t s);  // the antiderivative alone
 void launch_grad(const DevBunch& b, cudaStream_t s);
 void launch_gather_kick_push(const DevBunch& b, bool stats, cudaStream_t s);
 void launch_gather_fields(const DevBunch& b, cudaStream_t s);
@@ -221,6 +222,9 @@ void launch_sort(const DevBunch& b, cudaStream_t s);
 
 // FFT TU (sc_fft.cu)
 void launch_green_transform(const DevBunch& b, cudaStream_t s);
+// Ĝ from the antiderivative alone (launch_igf_tmp): G is formed inside the
+// first cosine transform; the same bits as launch_igf + launch_green_transform
+void launch_green_transform_from_tmp(const DevBunch& b, cudaStream_t s);
 void launch_convolution(const DevBunch& b, int mode, cudaStream_t s);
 // the forward passes (A, B) need rho only; the rest (C, D, E) also the spectrum of G.
 // The image part runs C, D, E with the shifted G's complex spectrum and

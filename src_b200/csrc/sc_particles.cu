@@ -980,19 +980,8 @@ __device__ __forceinline__ void igf_G_body(int n0, int n1, int n2, const double*
     const int g0 = n0 + 1, g1 = n1 + 1, g2 = n2 + 1;
     const int t0 = n0 + 2, t1 = n1 + 2;
     for (int c = g.blk * blockDim.x + threadIdx.x; c < g0 * g1 * g2; c += g.nblk * blockDim.x) {
-        int i = c % g0, j = (c / g0) % g1, k = c / (g0 * g1);
-        if (c == 0) k = 1;
-#define TG(a, b, e) tmp[(a) + t0 * ((b) + t1 * (e))]
-        double g = TG(i + 1, j + 1, k + 1);
-        g += TG(i + 1, j, k);
-        g += TG(i, j + 1, k);
-        g += TG(i, j, k + 1);
-        g -= TG(i + 1, j + 1, k);
-        g -= TG(i + 1, j, k + 1);
-        g -= TG(i, j + 1, k + 1);
-        g -= TG(i, j, k);
-#undef TG
-        G[c] = g;
+        const int i = c % g0, j = (c / g0) % g1, k = c / (g0 * g1);
+        G[c] = igf_G_at(tmp, t0, t1, i, j, k);
     }
 }
 __global__ void __launch_bounds__(kThreads) k_igf_G(int n0, int n1, int n2, const double* __restrict__ tmp,
@@ -2043,6 +2032,17 @@ void launch_igf(const DevBunch& b, const double* hr_host, cudaStream_t s) {
     else
         k_igf_tmp<false><<<grid_for(T3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.st, b.gtmp);
     k_igf_G<<<grid_for(G3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.gtmp, b.gline);
+}
+
+// The antiderivative alone (b.gtmp): launch_green_transform_from_tmp forms G
+// from it inside its first cosine transform.
+void launch_igf_tmp(const DevBunch& b, cudaStream_t s) {
+    const int n0 = b.bc.n[0], n1 = b.bc.n[1], n2 = b.bc.n[2];
+    const long long T3 = (long long)(n0 + 2) * (n1 + 2) * (n2 + 2);
+    if (b.precision == 0)
+        k_igf_tmp<true><<<grid_for(T3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.st, b.gtmp);
+    else
+        k_igf_tmp<false><<<grid_for(T3, 148 * 16), kThreads, 0, s>>>(n0, n1, n2, b.st, b.gtmp);
 }
 
 void launch_grad(const DevBunch& b, cudaStream_t s) {
