@@ -713,8 +713,10 @@ SC_HD double igf_G_at(const double* __restrict__ tmp, int t0, int t1, int i, int
 // remainder a - q0 b (exact with an FMA) corrects q0 (Markstein, IBM J. Res.
 // Dev. 34(1), 1990).  With rb correctly rounded the result equals the IEEE
 // quotient; operands near the ends of the exponent range take the division.
-// Callers pass divisors in the normal range (mesh spacings, c dt, gamma), so
-// only the quotient is checked: a tiny, zero or huge q0 takes the division.
+// Callers pass divisors of at least 2^-70 (mesh spacings, c dt, gamma), so
+// only the quotient is checked: a tiny, zero or huge q0 takes the division,
+// and a fast quotient (|q0| >= 2^-899) has |a| >= 2^-969, where the FMA
+// remainder is exact (a subnormal dividend never reaches the product path).
 // The range test reads the biased exponent of q0 from its high word on the
 // integer units: |q0| in [2^-899, 2^900) (exponent field 124 .. 1922; zero,
 // subnormals, infinities and NaN fall outside).
